@@ -1,0 +1,180 @@
+"""ctypes binding for the CPU oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and
+by bench.py's CPU-baseline leg, always as the checker, never as the thing
+measured for the GPU path.  The product (hl2sdk_tools_sharp_b200) never
+imports this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+
+CLOSEST = 1
+ISOLATED = 2
+SKY_PASS = 4
+FULL_WALK = 8
+TRACE_ID_SKY = 0x01000000
+
+# KdTriangle, 48 bytes (MapTools/Tracing/KdTree.cs:120-167).
+TRI_DTYPE = np.dtype([
+    ("n", "<f4", (3,)), ("d", "<f4"), ("id", "<i4"), ("e", "<f4", (6,)),
+    ("cs0", "u1"), ("cs1", "u1"), ("flags", "u1"), ("unused", "u1"),
+])
+assert TRI_DTYPE.itemsize == 48
+NODE_DTYPE = np.dtype([("children", "<i4"), ("split", "<f4")])
+
+
+def build(force: bool = False) -> None:
+    """Compile liboracle.so with the committed Makefile."""
+    if force or not LIB_PATH.exists() or any(
+            p.stat().st_mtime > LIB_PATH.stat().st_mtime
+            for p in HERE.glob("*.[ch]*") if p.suffix in (".cpp", ".h")):
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        _lib = ctypes.CDLL(str(LIB_PATH))
+        P = ctypes.c_void_p
+        i32 = ctypes.c_int32
+        f32 = ctypes.c_float
+        _lib.orc_tri_prepare.argtypes = [P, P, P, i32, P]
+        _lib.orc_kd_trace.argtypes = [P, i32, P, i32, P, i32, P, P, i32, f32, i32, i32, P, P, P]
+        _lib.orc_brute_trace.argtypes = [P, i32, P, i32, f32, i32, i32, P, P, P, i32]
+        _lib.orc_fp64_classify.argtypes = [P, i32, P, i32, ctypes.c_double, P, i32]
+        for name in ("orc_tri_prepare", "orc_kd_trace", "orc_brute_trace", "orc_fp64_classify"):
+            getattr(_lib, name).restype = ctypes.c_int
+        if hasattr(_lib, "orc_kd_build"):
+            _lib.orc_kd_build.argtypes = [P, P, P, i32, P]
+            _lib.orc_kd_build.restype = ctypes.c_int
+            _lib.orc_kd_free.argtypes = [P]
+            _lib.orc_kd_free.restype = None
+    return _lib
+
+
+def _p(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def default_threads() -> int:
+    return max(1, os.cpu_count() or 1)
+
+
+def prepare_triangles(verts: np.ndarray, ids: np.ndarray | None = None,
+                      flags: np.ndarray | None = None) -> np.ndarray:
+    """Correct-mode intersection format for (n, 9) float32 vertices."""
+    verts = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 9)
+    n = verts.shape[0]
+    ids = None if ids is None else np.ascontiguousarray(ids, dtype=np.int32)
+    flags = None if flags is None else np.ascontiguousarray(flags, dtype=np.uint8)
+    out = np.zeros(n, dtype=TRI_DTYPE)
+    rc = lib().orc_tri_prepare(_p(verts), _p(ids), _p(flags), n, _p(out))
+    if rc != 0:
+        raise RuntimeError(f"orc_tri_prepare failed: {rc}")
+    return out
+
+
+def kd_trace(tree: dict, rays: np.ndarray, tmin: float = 0.0, skip_id: int = -1,
+             flags: int = 0):
+    """Restated KdRayTracer over a tree dict (nodes, indices, tris, bounds)."""
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 7)
+    n = rays.shape[0]
+    tri = np.empty(n, dtype=np.int32)
+    dist = np.empty(n, dtype=np.float32)
+    bits = np.zeros((n + 63) // 64, dtype=np.uint64)
+    nodes = np.ascontiguousarray(tree["nodes"], dtype=NODE_DTYPE)
+    idx = np.ascontiguousarray(tree["indices"], dtype=np.int32)
+    tris = np.ascontiguousarray(tree["tris"], dtype=TRI_DTYPE)
+    bounds = np.ascontiguousarray(tree["bounds"], dtype=np.float32)
+    rc = lib().orc_kd_trace(_p(nodes), len(nodes), _p(idx), len(idx), _p(tris), len(tris),
+                            _p(bounds), _p(rays), n, tmin, skip_id, flags, _p(tri), _p(dist),
+                            _p(bits))
+    if rc != 0:
+        raise RuntimeError(f"orc_kd_trace failed: {rc}")
+    return tri, dist, bits
+
+
+def brute_trace(tris: np.ndarray, rays: np.ndarray, tmin: float = 0.0, skip_id: int = -1,
+                flags: int = 0, threads: int | None = None):
+    """The CUDA tracer's exact semantic, by brute force (see vrad_oracle.h)."""
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 7)
+    tris = np.ascontiguousarray(tris, dtype=TRI_DTYPE)
+    n = rays.shape[0]
+    tri = np.empty(n, dtype=np.int32)
+    dist = np.empty(n, dtype=np.float32)
+    bits = np.zeros((n + 63) // 64, dtype=np.uint64)
+    rc = lib().orc_brute_trace(_p(tris), len(tris), _p(rays), n, tmin, skip_id, flags,
+                               _p(tri), _p(dist), _p(bits),
+                               threads if threads is not None else default_threads())
+    if rc != 0:
+        raise RuntimeError(f"orc_brute_trace failed: {rc}")
+    return tri, dist, bits
+
+
+def kd_build(verts: np.ndarray, ids: np.ndarray | None = None,
+             flags: np.ndarray | None = None) -> dict:
+    """Restated KdTreeBuilder (SAH); returns a tree dict for kd_trace."""
+    L = lib()
+    if not hasattr(L, "orc_kd_build"):
+        raise NotImplementedError("orc_kd_build is not in this oracle build")
+
+    class _Tree(ctypes.Structure):
+        _fields_ = [("nodes", ctypes.c_void_p), ("nnodes", ctypes.c_int32),
+                    ("indices", ctypes.c_void_p), ("nindices", ctypes.c_int32),
+                    ("tris", ctypes.c_void_p), ("ntris", ctypes.c_int32),
+                    ("bounds", ctypes.c_float * 6)]
+
+    verts = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 9)
+    ids = None if ids is None else np.ascontiguousarray(ids, dtype=np.int32)
+    flags = None if flags is None else np.ascontiguousarray(flags, dtype=np.uint8)
+    t = _Tree()
+    rc = L.orc_kd_build(_p(verts), _p(ids), _p(flags), verts.shape[0], ctypes.byref(t))
+    if rc != 0:
+        raise RuntimeError(f"orc_kd_build failed: {rc}")
+    try:
+        def arr(ptr, count, dtype):
+            nbytes = count * np.dtype(dtype).itemsize
+            buf = (ctypes.c_char * nbytes).from_address(ptr) if count else b""
+            return np.frombuffer(bytes(buf), dtype=dtype).copy()
+        tree = {
+            "nodes": arr(t.nodes, t.nnodes, NODE_DTYPE),
+            "indices": arr(t.indices, t.nindices, np.int32),
+            "tris": arr(t.tris, t.ntris, TRI_DTYPE),
+            "bounds": np.array(list(t.bounds), dtype=np.float32),
+        }
+    finally:
+        L.orc_kd_free(ctypes.byref(t))
+    return tree
+
+
+def fp64_classify(verts: np.ndarray, rays: np.ndarray, rel_margin: float = 1e-6,
+                  threads: int | None = None) -> np.ndarray:
+    """1 blocked, 0 clear, 2 within the margin of a boundary."""
+    verts = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 9)
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 7)
+    out = np.empty(rays.shape[0], dtype=np.int8)
+    rc = lib().orc_fp64_classify(_p(verts), verts.shape[0], _p(rays), rays.shape[0],
+                                 rel_margin, _p(out),
+                                 threads if threads is not None else default_threads())
+    if rc != 0:
+        raise RuntimeError(f"orc_fp64_classify failed: {rc}")
+    return out
+
+
+def bits_to_bool(bits: np.ndarray, n: int) -> np.ndarray:
+    """Unpack LSB-first u64 words into n booleans."""
+    b = np.ascontiguousarray(bits, dtype="<u8").view(np.uint8)
+    return np.unpackbits(b, bitorder="little")[:n].astype(bool)

@@ -1,0 +1,103 @@
+/*
+ * vrad_oracle.h -- CPU oracle for the vrad lighting path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product (the CUDA library, its
+ * C ABI, the Python host layer) links, loads or calls anything declared here.
+ * Only the tests, the smoke check and the CPU-baseline leg of the benchmark
+ * use it, and only as the checker.
+ *
+ * This is a plain C++17 restatement of the reference's CPU arithmetic
+ * (SourceSharp.MapTools, Correct compliance).  Each function names the
+ * reference file and lines it follows.  Parity is pinned against the
+ * reference's own stock-tracer fixtures (kd-scene / kd-boxes answers), see
+ * tests/test_oracle_fixtures.py.
+ */
+#ifndef VRAD_ORACLE_H
+#define VRAD_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* KdTriangle (MapTools/Tracing/KdTree.cs:120-167): 48 bytes. */
+typedef struct orc_tri {
+    float nx, ny, nz, d;
+    int32_t id;
+    float e[6];
+    uint8_t cs0, cs1, flags, unused;
+} orc_tri;
+
+/* Ray (MapTools/Tracing/IRayTracer.cs:32): 28 bytes. */
+typedef struct orc_ray {
+    float ox, oy, oz, dx, dy, dz, reach;
+} orc_ray;
+
+/* KdNode (MapTools/Tracing/KdTree.cs:60-100): 8 bytes. */
+typedef struct orc_kdnode {
+    int32_t children;
+    float split;
+} orc_kdnode;
+
+enum {
+    ORC_CLOSEST = 1,    /* closest hit (else visibility)            */
+    ORC_ISOLATED = 2,   /* RayTraceOptions.IsolatedRays             */
+    ORC_SKY_PASS = 4,   /* RayTraceOptions.SkyDoesNotBlock          */
+    ORC_FULL_WALK = 8,  /* KdRayTracer.WithFullVisibilityWalk       */
+};
+
+/* TraceId.Sky (MapTools/Rad/TraceId.cs). */
+#define ORC_TRACE_ID_SKY 0x01000000
+
+/* Correct-mode KdTreeBuilder.ToIntersectionFormat for n triangles given as
+ * nine floats each (v0, v1, v2). */
+int orc_tri_prepare(const float *verts9, const int32_t *ids, const uint8_t *flags,
+                    int32_t n, orc_tri *out);
+
+/* KdRayTracer.TraceVisibility / TraceClosest over an already-built tree.
+ * out_tri receives the tree's triangle INDEX (-1 on a miss), out_dist the
+ * raw hit distance, out_bits (visibility only) one bit per ray. */
+int orc_kd_trace(const orc_kdnode *nodes, int32_t nnodes, const int32_t *indices,
+                 int32_t nindices, const orc_tri *tris, int32_t ntris,
+                 const float *bounds6, const orc_ray *rays, int32_t nrays,
+                 float tmin, int32_t skip_id, int32_t flags, int32_t *out_tri,
+                 float *out_dist, uint64_t *out_bits);
+
+/* The semantic the CUDA tracer implements, by brute force over every
+ * triangle with the same FP32 predicate: visibility = any accepted hit with
+ * tmin <= t < reach; closest = lexicographic minimum of (t, triangle index)
+ * over accepted hits with tmin <= t < reach.  out_tri = triangle index or -1,
+ * out_dist = t. */
+int orc_brute_trace(const orc_tri *tris, int32_t ntris, const orc_ray *rays,
+                    int32_t nrays, float tmin, int32_t skip_id, int32_t flags,
+                    int32_t *out_tri, float *out_dist, uint64_t *out_bits,
+                    int32_t threads);
+
+/* KdTreeBuilder (MapTools/Tracing/KdTreeBuilder.cs): SAH KD build.
+ * Returns the node / index counts through the pointers; the arrays are
+ * owned by the oracle until orc_kd_free. */
+typedef struct orc_kdtree {
+    orc_kdnode *nodes;
+    int32_t nnodes;
+    int32_t *indices;
+    int32_t nindices;
+    orc_tri *tris;
+    int32_t ntris;
+    float bounds[6];
+} orc_kdtree;
+
+int orc_kd_build(const float *verts9, const int32_t *ids, const uint8_t *flags, int32_t n,
+                 orc_kdtree *out);
+void orc_kd_free(orc_kdtree *tree);
+
+/* FP64 classification of each ray against the triangles' true geometry:
+ * 1 = blocked by a margin, 0 = clear by a margin, 2 = within margin (ambiguous). */
+int orc_fp64_classify(const float *verts9, int32_t ntris, const orc_ray *rays, int32_t nrays,
+                      double rel_margin, int8_t *out_class, int32_t threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
