@@ -1,0 +1,416 @@
+"""Benchmark: vrad's direct-lighting ray tracing on the seeded 8x8 room grid.
+
+One step = one pass of the tracer over every direct-lighting segment of the
+map (see hl2sdk_tools_sharp_b200/workload.py): a visibility segment from each
+luxel sample to each light in its PVS it faces, a sun sky-test and one sky
+test per ambient direction in front of the face (162 directions).  Light
+segments are any-hit visibility; sun and sky segments are visibility with
+sky pass-through (a first hit on a sky triangle does not block).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  `value` is rays/s over all ranks with the
+rays already in HBM; `e2e` is the same through the C ABI's host-buffer entry
+points (pinned host rays in, hit bits out, copies inside the timed region).
+`--impl reference` times the reference's algorithm on the host CPU (the
+restated KD tracer, all host threads) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "vrad direct-lighting rays/s (8x8 room grid, 1 B200)"
+UNIT = "rays/s"
+BYTES_PER_RAY = 28.0 + 0.125        # 28-byte ray record in, one hit bit out
+CONFIG_SEED = 1
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--side", type=int, default=8, help=argparse.SUPPRESS)
+    ap.add_argument("--no-e2e", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--no-cpu", action="store_true", help=argparse.SUPPRESS)
+    return ap.parse_args()
+
+
+def world_for(side: int):
+    from hl2sdk_tools_sharp_b200 import roomgrid as rg
+    cfg = rg.config_8x8(CONFIG_SEED) if side == 8 else rg.config_3x3(CONFIG_SEED)
+    if side not in (3, 8):
+        cfg.side = side
+    return rg.generate(cfg)
+
+
+def device_rays(world, device):
+    """The full direct-light ray set, built on the device with torch."""
+    import torch
+    from hl2sdk_tools_sharp_b200 import workload as wl
+    s = wl.luxel_samples(world)
+    P = torch.from_numpy(s.points).to(device)
+    N = torch.from_numpy(s.normals).to(device)
+    C = torch.from_numpy(s.cluster.astype(np.int64)).to(device)
+    pvs = torch.from_numpy(world.pvs).to(device)
+    L = torch.from_numpy(world.light_origin).to(device)
+    LC = torch.from_numpy(world.light_cluster.astype(np.int64)).to(device)
+    Ln = torch.from_numpy(world.light_normal).to(device)
+    cos_outer = torch.from_numpy(np.cos(np.radians(world.light_cone[:, 1])).astype(np.float32)).to(device)
+    spot = torch.from_numpy(world.light_type == 2).to(device)
+
+    def seg(a, b):
+        r = torch.empty((a.shape[0], 7), dtype=torch.float32, device=device)
+        r[:, 0:3] = a
+        r[:, 3:6] = b - a
+        r[:, 6] = 1.0
+        return r
+
+    light_parts = []
+    chunk = 1 << 20
+    for b in range(0, P.shape[0], chunk):
+        p, n, c = P[b:b + chunk], N[b:b + chunk], C[b:b + chunk]
+        delta = L[None, :, :] - p[:, None, :]
+        dot = (delta * n[:, None, :]).sum(-1)
+        ok = pvs[c][:, LC] & (dot > 0)
+        dist = delta.norm(dim=-1).clamp_min(1e-6)
+        cos_to = -(delta * Ln[None]).sum(-1) / dist
+        ok &= ~spot[None, :] | (cos_to > cos_outer[None, :])
+        si, li = torch.nonzero(ok, as_tuple=True)
+        light_parts.append(seg(p[si], L[li]))
+    light = torch.cat(light_parts)
+
+    sun_dir = torch.from_numpy(world.sun_direction).to(device)
+    faces = -(N @ sun_dir) > 0
+    sp = P[faces]
+    sun = seg(sp, sp + sun_dir * -float(wl.MAX_TRACE_LENGTH))
+
+    dirs = torch.from_numpy(wl.ambient_directions()).to(device)
+    sky_parts = []
+    for b in range(0, P.shape[0], chunk):
+        p, n = P[b:b + chunk], N[b:b + chunk]
+        si, di = torch.nonzero(-(n @ dirs.T) > float(wl.EQUAL_EPSILON), as_tuple=True)
+        sky_parts.append(seg(p[si], p[si] + dirs[di] * -float(wl.MAX_TRACE_LENGTH)))
+    sky = torch.cat(sky_parts)
+    del sky_parts, light_parts
+    return {"light": light.contiguous(), "sun": sun.contiguous(), "sky": sky.contiguous(),
+            "luxels": int(P.shape[0])}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        rows = [[c.strip() for c in r] for r in rows if len(r) >= 9]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        for r in rows:
+            for name, col in (("hw_slowdown", 5), ("hw_thermal_slowdown", 6), ("sw_thermal_slowdown", 7),
+                              ("sw_power_cap", 8)):
+                if r[col].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def dist_setup(gpus: int):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def host_sample(rays: dict, total: int, cap: int = 16_000_000) -> dict:
+    """Every k-th ray of each kind (the same k for all), at most `cap` rays,
+    copied to host memory; the CPU leg samples within this."""
+    stride = max(1, -(-total // cap))
+    return {k: rays[k][::stride].cpu().numpy() for k in ("light", "sun", "sky")}
+
+
+def cpu_reference(world_map, rays_np: dict, total: int, budget_s: float = 20.0):
+    """The reference's algorithm on the host: the restated KD build and
+    packet walk (oracle), all host threads, on a bounded sample of each ray
+    kind in proportion to the full workload."""
+    from oracle import oracle as O
+    threads = O.default_threads()
+    tree = O.kd_build(world_map.tri_verts, world_map.tri_ids)
+    pool = sum(len(v) for v in rays_np.values())
+    # Calibrate on a small sample, then size the timed sample to the budget.
+    def run(frac):
+        n = 0
+        t0 = time.perf_counter()
+        for kind, rays in rays_np.items():
+            k = max(64, int(len(rays) * frac))
+            sel = rays[:: max(1, len(rays) // k)][:k]
+            flags = 0 if kind == "light" else O.SKY_PASS
+            O.kd_trace(tree, sel, flags=flags, threads=threads)
+            n += len(sel)
+        return n, time.perf_counter() - t0
+    n, dt = run(min(1.0, 2e5 / pool))
+    frac = min(1.0, (2e5 / pool) * budget_s / max(dt, 1e-3))
+    n, dt = run(frac)
+    return {"value": n / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} rays ({100.0 * n / total:.2f}% of each ray kind, strided) of the "
+                      f"8x8 direct-light workload; restated KD build + 4-ray packet walk"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import torch
+    w = world_for(args.side)
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    rays = device_rays(w, dev)
+    total = sum(int(rays[k].shape[0]) for k in ("light", "sun", "sky"))
+    rays_np = host_sample(rays, total)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_reference(w, rays_np, total, budget_s=max(3.0, 60.0 / max(1, args.warmup + args.steps)))
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded room grid)",
+        "config": {"workload": "8x8 room grid direct-lighting rays (light + sun + 162-dir sky)",
+                   "rays_per_step": total, "seed": CONFIG_SEED},
+        "cpu_baseline": {**cb, "value": value},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    from hl2sdk_tools_sharp_b200 import tracer as T
+    rank, world_size, local = dist_setup(args.gpus)
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+
+    w = world_for(args.side)
+    tr = T.CudaRayTracer(T.make_triangles(w.tri_verts, w.tri_ids), device=local)
+    info = tr.scene_info()
+    rays = device_rays(w, device)
+    kinds = [("light", T.RayTraceOptions.stock_exact()),
+             ("sun", T.RayTraceOptions(0.0, sky_does_not_block=True)),
+             ("sky", T.RayTraceOptions(0.0, sky_does_not_block=True))]
+    bits = {k: torch.zeros((rays[k].shape[0] + 63) // 64 + 1, dtype=torch.int64, device=device)
+            for k, _ in kinds}
+    total = sum(rays[k].shape[0] for k, _ in kinds)
+
+    def step():
+        for k, o in kinds:
+            tr.trace_visibility(rays[k], bits[k], o)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+
+    # Spot-check the resident results against the oracle on a sample.
+    check = None
+    if rank == 0 and not args.no_cpu:
+        from oracle import oracle as O
+        tris = O.prepare_triangles(w.tri_verts, w.tri_ids)
+        bad = 0
+        checked = 0
+        for k, o in kinds:
+            n = rays[k].shape[0]
+            idx = np.arange(0, n, max(1, n // 20000))[:20000]
+            sel = rays[k][torch.from_numpy(idx).to(device)].cpu().numpy()
+            _, _, bb = O.brute_trace(tris, sel, flags=O.SKY_PASS if o.sky_does_not_block else 0)
+            want = O.bits_to_bool(bb, len(sel))
+            allbits = bits[k].cpu().numpy().view(np.uint64)
+            got = O.bits_to_bool(allbits, n)[idx]
+            bad += int((got != want).sum())
+            checked += len(sel)
+        check = {"rays": checked, "mismatches": bad}
+
+    # Timed region: K steps, events on the launching (current) stream.
+    stream = torch.cuda.current_stream(device)
+    barrier(world_size)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps)]
+    with ClockSampler(local) as clocks:
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for s in range(args.steps):
+            ev[2 * s].record(stream)
+            step()
+            ev[2 * s + 1].record(stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world_size)
+    elapsed_ms = t0.elapsed_time(t1)
+    elapsed_ms = max_over_ranks(elapsed_ms, world_size)
+    per_step = [ev[2 * s].elapsed_time(ev[2 * s + 1]) for s in range(args.steps)]
+    ms_per_step = elapsed_ms / args.steps
+    value = world_size * total / (ms_per_step / 1000.0)
+
+    # Per-kind kernel times (one launch per kind) for the roofline.
+    kt = {}
+    for k, o in kinds:
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(3):
+            tr.trace_visibility(rays[k], bits[k], o)
+        b.record(stream)
+        torch.cuda.synchronize()
+        kt[k] = a.elapsed_time(b) / 3.0
+
+    # End to end through the host-buffer C ABI: pinned host rays in, bits out.
+    e2e = None
+    if not args.no_e2e:
+        host = {k: torch.empty(rays[k].shape, dtype=torch.float32, pin_memory=True) for k, _ in kinds}
+        hbits = {k: torch.zeros(((rays[k].shape[0] + 63) // 64,), dtype=torch.int64, pin_memory=True)
+                 for k, _ in kinds}
+        for k, _ in kinds:
+            host[k].copy_(rays[k])
+        hv = {k: host[k].numpy().view(T.RAY_DTYPE).reshape(-1) for k, _ in kinds}
+        hb = {k: hbits[k].numpy().view(np.uint64) for k, _ in kinds}
+        def e2e_step():
+            for k, o in kinds:
+                tr.trace_visibility(hv[k], hb[k], o)
+        e2e_step()
+        torch.cuda.synchronize()
+        barrier(world_size)
+        t = time.perf_counter()
+        e2e_steps = max(1, min(args.steps, 3))
+        for _ in range(e2e_steps):
+            e2e_step()
+        e2e_s = (time.perf_counter() - t) / e2e_steps
+        e2e_s = max_over_ranks(e2e_s, world_size)
+        e2e = {"value": world_size * total / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(sum(host[k].numel() * 4 for k, _ in kinds)),
+               "d2h_bytes_per_step": int(sum(8 * ((rays[k].shape[0] + 63) // 64) for k, _ in kinds))}
+        del host, hbits
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu:
+        cpu = cpu_reference(w, host_sample(rays, total), total, budget_s=15.0)
+
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    sky_ms = kt["sky"]
+    achieved = BYTES_PER_RAY * rays["sky"].shape[0] / (sky_ms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None,
+                "kernel": "k_trace<kModeSkyPass> (sky segments)",
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded room grid, rays built on the device)",
+            "config": {"workload": "8x8 room grid direct-lighting rays (light + sun + 162-dir sky)",
+                       "side": args.side, "seed": CONFIG_SEED, "luxels": rays["luxels"],
+                       "triangles": info.triangles, "rays_per_step": total,
+                       "rays": {k: int(rays[k].shape[0]) for k, _ in kinds},
+                       "l2": "inputs larger than L2 (rays ~%.1f GB per step)" % (28 * total / 1e9),
+                       "parallelism": f"replicas{world_size}"},
+            "e2e": e2e,
+            "gpu_launches": 3 * args.steps,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "kernel_ms": kt,
+            "step_ms": per_step,
+            "bvh": {"nodes": info.bvh_nodes, "leaves": info.bvh_leaves, "max_leaf": info.max_leaf,
+                    "build_ms": info.build_ms, "pad": info.box_pad},
+            "check": check,
+        }
+        print(json.dumps(line), flush=True)
+    tr.close()
+    if world_size > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

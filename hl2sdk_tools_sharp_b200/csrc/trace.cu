@@ -1,0 +1,263 @@
+// trace.cu -- ray traversal kernels: any-hit visibility, closest hit, and
+// sky-passing visibility, over the BVH built in scene.cu.
+//
+// Per-triangle arithmetic is the reference's KdRayTracer.IntersectTriangle
+// (MapTools/Tracing/KdRayTracer.cs:1194-1267) operation for operation, each
+// an explicitly rounded intrinsic, so an accepted/rejected decision and a
+// hit distance are the CPU's bits.  What the traversal adds is only WHICH
+// triangles get tested: every triangle whose padded box the segment meets,
+// which includes every triangle the predicate can accept (the pad is far
+// above the rounding of the box test and of the predicate's hit point).
+//
+// Work distribution: one ray per thread, 128-thread CTAs scheduled by the
+// hardware (no shared work counter, so launches on different streams never
+// interfere); a warp's 32 visibility bits are one 32-bit word written with
+// a single store after a ballot.  The traversal stack lives in shared
+// memory, one column per thread.
+
+#include <cfloat>
+
+#include "scene.cuh"
+
+namespace vrad {
+
+namespace {
+
+constexpr int kBlock = 128;
+constexpr uint32_t kFull = 0xffffffffu;
+
+struct RayState {
+    float ox, oy, oz, dx, dy, dz;
+    float ix, iy, iz;      // 1/d with zeros saturated to +-2^60
+    float nox, noy, noz;   // -o/d, for the FMA slab test
+};
+
+__device__ inline float recip_saturate(float a) {
+    // ReciprocalSaturateExact (KdRayTracer.cs:1446): a zero keeps its sign
+    // and becomes 2^-60 before the divide.
+    if (a == 0.0f) a = __uint_as_float(__float_as_uint(a) | 0x21800000u);
+    return __frcp_rn(a);
+}
+
+__device__ inline float sel3(int axis, float x, float y, float z) {
+    return axis == 0 ? x : (axis == 1 ? y : z);
+}
+
+// The predicate.  Returns true with the exact t when the triangle accepts
+// the ray (|d.n| > eps, eps < t < 1e23, both edge values >= eps, their sum
+// <= 1).
+__device__ __forceinline__ bool kd_hit(const DeviceScene &s, int k, const RayState &r, float &t_out,
+                                       uint32_t &meta_out, int32_t &orig_out) {
+    const float4 A = __ldg(&s.tri0[k]);
+    float ddotn = __fmul_rn(r.dx, A.x);
+    ddotn = __fadd_rn(__fmul_rn(r.dy, A.y), ddotn);
+    ddotn = __fadd_rn(__fmul_rn(r.dz, A.z), ddotn);
+    float odotn = __fmul_rn(r.ox, A.x);
+    odotn = __fadd_rn(__fmul_rn(r.oy, A.y), odotn);
+    odotn = __fadd_rn(__fmul_rn(r.oz, A.z), odotn);
+    const float num = __fsub_rn(A.w, odotn);
+    // t > eps needs num and ddotn of one sign; this rejects without the
+    // divide exactly where the divide's sign would (|ddotn| > eps > 0).
+    if (!(ddotn > kKdEps || ddotn < -kKdEps)) return false;
+    if ((__float_as_uint(num) ^ __float_as_uint(ddotn)) & 0x80000000u) return false;
+    const float t = __fdiv_rn(num, ddotn);
+    if (!(t > kKdEps) || !(t < kKdHuge)) return false;
+    const float4 B = __ldg(&s.tri1[k]);
+    const float4 C = __ldg(&s.tri2[k]);
+    const uint32_t meta = __float_as_uint(C.w);
+    const int drop = meta & 3;
+    const int c0 = drop == 2 ? 0 : drop + 1;
+    const int c1 = drop == 0 ? 2 : drop - 1;
+    const float h1 = __fadd_rn(sel3(c0, r.ox, r.oy, r.oz), __fmul_rn(t, sel3(c0, r.dx, r.dy, r.dz)));
+    const float h2 = __fadd_rn(sel3(c1, r.ox, r.oy, r.oz), __fmul_rn(t, sel3(c1, r.dx, r.dy, r.dz)));
+    float b0 = __fmul_rn(B.x, h1);
+    b0 = __fadd_rn(b0, __fmul_rn(B.y, h2));
+    b0 = __fadd_rn(b0, B.z);
+    if (!(b0 >= kKdEps)) return false;
+    float b1 = __fmul_rn(B.w, h1);
+    b1 = __fadd_rn(b1, __fmul_rn(C.x, h2));
+    b1 = __fadd_rn(b1, C.y);
+    if (!(b1 >= kKdEps)) return false;
+    if (!(__fadd_rn(b1, b0) <= 1.0f)) return false;
+    t_out = t;
+    meta_out = meta;
+    orig_out = __float_as_int(C.z);
+    return true;
+}
+
+__device__ __forceinline__ void slab2(const float4 &a, const float4 &b, const float4 &c,
+                                      const RayState &r, float tlo, float thi, bool &h0, bool &h1,
+                                      float &n0, float &n1) {
+    // child 0: x (a.x, a.y), y (a.z, a.w), z (c.x, c.y); child 1: x (b.x, b.y), y (b.z, b.w), z (c.z, c.w)
+    float x0 = fmaf(a.x, r.ix, r.nox), x1 = fmaf(a.y, r.ix, r.nox);
+    float y0 = fmaf(a.z, r.iy, r.noy), y1 = fmaf(a.w, r.iy, r.noy);
+    float z0 = fmaf(c.x, r.iz, r.noz), z1 = fmaf(c.y, r.iz, r.noz);
+    float tn0 = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tlo));
+    float tf0 = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), thi));
+    float u0 = fmaf(b.x, r.ix, r.nox), u1 = fmaf(b.y, r.ix, r.nox);
+    float v0 = fmaf(b.z, r.iy, r.noy), v1 = fmaf(b.w, r.iy, r.noy);
+    float w0 = fmaf(c.z, r.iz, r.noz), w1 = fmaf(c.w, r.iz, r.noz);
+    float tn1 = fmaxf(fmaxf(fminf(u0, u1), fminf(v0, v1)), fmaxf(fminf(w0, w1), tlo));
+    float tf1 = fminf(fminf(fmaxf(u0, u1), fmaxf(v0, v1)), fminf(fmaxf(w0, w1), thi));
+    h0 = tn0 <= tf0;
+    h1 = tn1 <= tf1;
+    n0 = tn0;
+    n1 = tn1;
+}
+
+// One ray.  MODE kModeAny stops at the first accepted hit in
+// [tmin, reach); the other modes find the lexicographically smallest
+// (t, original index) in that window.
+template <int MODE>
+__device__ __forceinline__ void trace_ray(const DeviceScene &s, const RayState &r, float tmin,
+                                          float reach, int32_t skip_id, int *stack,
+                                          uint32_t *overflow, bool &hit, float &best_t,
+                                          int32_t &best_orig, uint32_t &best_meta) {
+    hit = false;
+    best_t = reach;
+    best_orig = 0x7fffffff;
+    best_meta = 0;
+    int sp = 0;
+    int ref = s.root_ref;
+    // The box window: [tmin, reach] for any-hit, [tmin, best] once a
+    // closest candidate exists (a tie at best may still win on index).
+    while (true) {
+        if (ref >= 0) {
+            const float4 *nd = s.nodes + 4 * ref;
+            const float4 a = __ldg(nd), b = __ldg(nd + 1), c = __ldg(nd + 2), d = __ldg(nd + 3);
+            bool h0, h1;
+            float n0, n1;
+            slab2(a, b, c, r, tmin, best_t, h0, h1, n0, n1);
+            const int r0 = __float_as_int(d.x), r1 = __float_as_int(d.y);
+            if (h0 && h1) {
+                int near_ref = r0, far_ref = r1;
+                if (n1 < n0) {
+                    near_ref = r1;
+                    far_ref = r0;
+                }
+                if (sp < kStackDepth) {
+                    stack[sp * kBlock] = far_ref;
+                    sp++;
+                } else {
+                    atomicOr(overflow, 1u);
+                }
+                ref = near_ref;
+                continue;
+            }
+            if (h0) {
+                ref = r0;
+                continue;
+            }
+            if (h1) {
+                ref = r1;
+                continue;
+            }
+        } else {
+            const int packed = ~ref;
+            const int first = packed >> 3;
+            const int count = (packed & 7) + 1;
+            for (int k = first; k < first + count; k++) {
+                float t;
+                uint32_t meta;
+                int32_t orig;
+                if (!kd_hit(s, k, r, t, meta, orig)) continue;
+                if (!(t >= tmin)) continue;
+                if (skip_id != -1 && __ldg(&s.tri_id[orig]) == skip_id) continue;
+                if (MODE == kModeAny) {
+                    if (t < reach) {
+                        hit = true;
+                        return;
+                    }
+                } else {
+                    const bool better = hit ? (t < best_t || (t == best_t && orig < best_orig)) : (t < reach);
+                    if (better) {
+                        hit = true;
+                        best_t = t;
+                        best_orig = orig;
+                        best_meta = meta;
+                    }
+                }
+            }
+        }
+        if (sp == 0) return;
+        sp--;
+        ref = stack[sp * kBlock];
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) k_trace(DeviceScene s, const vrad_ray *__restrict__ rays,
+                                                  int64_t n, TraceParams p, uint32_t *__restrict__ bits,
+                                                  vrad_hit *__restrict__ hits,
+                                                  uint32_t *__restrict__ overflow) {
+    __shared__ int stack_mem[kStackDepth * kBlock];
+    int *stack = stack_mem + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+    if (i - lane >= n) return;  // whole warp past the end
+    bool hit = false;
+    float best_t = 0.0f, reach = 1.0f;
+    int32_t best_orig = -1;
+    uint32_t best_meta = 0;
+    if (i < n) {
+        const float *f = reinterpret_cast<const float *>(rays + i);
+        RayState r;
+        r.ox = __ldg(f + 0);
+        r.oy = __ldg(f + 1);
+        r.oz = __ldg(f + 2);
+        r.dx = __ldg(f + 3);
+        r.dy = __ldg(f + 4);
+        r.dz = __ldg(f + 5);
+        reach = __ldg(f + 6);
+        r.ix = recip_saturate(r.dx);
+        r.iy = recip_saturate(r.dy);
+        r.iz = recip_saturate(r.dz);
+        r.nox = -r.ox * r.ix;
+        r.noy = -r.oy * r.iy;
+        r.noz = -r.oz * r.iz;
+        trace_ray<MODE>(s, r, p.tmin, reach, p.skip_id, stack, overflow, hit, best_t, best_orig,
+                        best_meta);
+    }
+    if (MODE == kModeClosest) {
+        if (i < n) {
+            vrad_hit h;
+            if (hit) {
+                h.surface = __ldg(&s.tri_id[best_orig]);
+                h.fraction = reach == 1.0f ? best_t : __fdiv_rn(best_t, reach);
+            } else {
+                h.surface = -1;
+                h.fraction = 1.0f;
+            }
+            hits[i] = h;
+        }
+    } else {
+        bool blocked = hit;
+        if (MODE == kModeSkyPass) blocked = hit && !(best_meta & 4u);
+        const uint32_t word = __ballot_sync(kFull, blocked);
+        if (lane == 0) bits[i >> 5] = word;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_trace(const DeviceScene &scene, const vrad_ray *d_rays, int64_t n,
+                         const TraceParams &p, uint32_t *d_bits, vrad_hit *d_hits,
+                         uint32_t *d_overflow, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    const int64_t grid = (n + kBlock - 1) / kBlock;
+    if (grid > 0x7fffffffLL) return cudaErrorInvalidValue;
+    switch (p.mode) {
+        case kModeAny:
+            k_trace<kModeAny><<<(unsigned)grid, kBlock, 0, stream>>>(scene, d_rays, n, p, d_bits, d_hits, d_overflow);
+            break;
+        case kModeClosest:
+            k_trace<kModeClosest><<<(unsigned)grid, kBlock, 0, stream>>>(scene, d_rays, n, p, d_bits, d_hits, d_overflow);
+            break;
+        default:
+            k_trace<kModeSkyPass><<<(unsigned)grid, kBlock, 0, stream>>>(scene, d_rays, n, p, d_bits, d_hits, d_overflow);
+            break;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace vrad

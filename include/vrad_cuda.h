@@ -1,0 +1,165 @@
+/*
+ * vrad_cuda.h -- C ABI of libvrad_cuda.so, the B200 (sm_100a) implementation
+ * of the ray-tracing seam of vrad's lighting stage.
+ *
+ * Plain pointers and sizes only.  Every call returns an int32 status
+ * (VRAD_OK or a negative VRAD_ERR_*); vrad_last_error() gives the message.
+ * The caller owns every buffer it passes; the library owns the device state
+ * behind the opaque context.  Calls on one context are serialised inside the
+ * library, so a host may call from many threads.
+ *
+ * Reference interfaces replaced (paths inside muflub/hl2sdk_tools_sharp):
+ *   IRayTracer                 src/SourceSharp.MapTools/Tracing/IRayTracer.cs:128-230
+ *   Ray (28-byte record)       src/SourceSharp.MapTools/Tracing/IRayTracer.cs:32-42
+ *   HitId (8-byte record)      src/SourceSharp.MapTools/Tracing/HitId.cs:70
+ *   RayTraceOptions            src/SourceSharp.MapTools/Tracing/RayTraceOptions.cs:65-145
+ *   TracedTriangle             src/SourceSharp.MapTools/Tracing/KdTree.cs:30-38
+ *   KdTriangle (48-byte form)  src/SourceSharp.MapTools/Tracing/KdTree.cs:120-167
+ *   IGpuTracerFactory offer    src/SourceSharp.MapTools/Rad/GpuTracing.cs:28-75
+ */
+#ifndef VRAD_CUDA_H
+#define VRAD_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VRAD_ABI_VERSION 1
+
+/* Status codes. */
+#define VRAD_OK 0
+#define VRAD_ERR_ARG (-1)          /* bad argument (ArgumentException in the reference) */
+#define VRAD_ERR_CUDA (-2)         /* a CUDA runtime call failed                         */
+#define VRAD_ERR_OOM (-3)          /* device allocation failed                           */
+#define VRAD_ERR_TIMEOUT (-4)      /* a bounded device wait ran out                      */
+#define VRAD_ERR_NO_SCENE (-5)     /* trace before vrad_scene_upload                     */
+#define VRAD_ERR_UNSUPPORTED (-6)  /* option this tracer cannot honour (NotSupported)    */
+#define VRAD_ERR_NO_DEVICE (-7)    /* no CUDA device / wrong architecture                */
+
+/* Ray: origin, direction (need not be unit length), reach in units of the
+ * direction's length.  28 bytes, the reference's wire format. */
+typedef struct vrad_ray {
+    float origin[3];
+    float direction[3];
+    float max_distance;
+} vrad_ray;
+
+/* HitId: the caller's triangle id (-1 = miss) and the hit's position along
+ * the ray in units of max_distance (t when max_distance is 1, else
+ * t / max_distance).  A miss is (-1, 1.0f). */
+typedef struct vrad_hit {
+    int32_t surface;
+    float fraction;
+} vrad_hit;
+
+/* TracedTriangle: caller id (several triangles may share one), three
+ * vertices, FCACHETRI flags.  The id's 0x01000000 bit is TraceId.Sky. */
+typedef struct vrad_triangle {
+    int32_t id;
+    float v0[3];
+    float v1[3];
+    float v2[3];
+    uint8_t flags;
+    uint8_t pad[3];
+} vrad_triangle;
+
+/* KdTriangle: the intersection form (plane, two pre-scaled edge equations,
+ * projection axes).  Only needed to trace with coefficients computed by a
+ * normalise other than the library's (e.g. stock's reciprocal estimate). */
+typedef struct vrad_kd_triangle {
+    float n[3];
+    float d;
+    int32_t id;
+    float e[6];
+    uint8_t cs0, cs1, flags, unused;
+} vrad_kd_triangle;
+
+/* RayTraceOptions.  min_distance: hits with t < min_distance are ignored
+ * (StockExact = 0, SelfIntersectionSafe = 1e-3).  skip_id: triangles with
+ * this id are ignored (-1 = none).  sky_does_not_block: visibility only; a
+ * ray whose first hit is a sky triangle is not blocked.  isolated_rays: the
+ * GPU traces every ray alone, so it is accepted and changes nothing. */
+typedef struct vrad_trace_options {
+    float min_distance;
+    int32_t skip_id;
+    int32_t sky_does_not_block;
+    int32_t isolated_rays;
+} vrad_trace_options;
+
+typedef struct vrad_scene_info {
+    int32_t triangles;
+    int32_t bvh_nodes;
+    int32_t bvh_leaves;
+    int32_t max_leaf;
+    float bounds_min[3];
+    float bounds_max[3];
+    float box_pad;
+    float build_ms;
+    int64_t device_bytes;
+} vrad_scene_info;
+
+typedef struct vrad_ctx vrad_ctx;
+
+/* Context on one CUDA device.  Fails with VRAD_ERR_NO_DEVICE when the device
+ * is absent or is not compute capability 10.0 (the library holds sm_100a
+ * code only).  Replaces IGpuTracerFactory.TryCreateAsync's device probe. */
+int32_t vrad_create(int32_t device, vrad_ctx **out);
+int32_t vrad_destroy(vrad_ctx *ctx);
+
+/* Builds the scene on the device: intersection form (Correct-mode
+ * normalise, bit-identical to KdTreeBuilder.ToIntersectionFormat), padded
+ * boxes and a BVH built on the GPU.  Replaces ShadowCasterSet.BuildTracerAsync
+ * (src/SourceSharp.MapTools/Rad/ShadowCasterSet.cs) for the device tracer. */
+int32_t vrad_scene_upload(vrad_ctx *ctx, const vrad_triangle *tris, int32_t n);
+
+/* As vrad_scene_upload, but the intersection form is given (one per
+ * triangle, same order); the vertices still define the boxes. */
+int32_t vrad_scene_upload_prepared(vrad_ctx *ctx, const vrad_triangle *tris,
+                                   const vrad_kd_triangle *prepared, int32_t n);
+
+int32_t vrad_scene_get_info(vrad_ctx *ctx, vrad_scene_info *out);
+
+/* IRayTracer.Supports: 1 when the options are honoured (all are, except a
+ * NaN or negative min_distance), else 0. */
+int32_t vrad_supports(const vrad_trace_options *opts);
+
+/* IRayTracer.TraceVisibilityAsync with HOST buffers: one bit per ray,
+ * least-significant first, set when an accepted hit lies in
+ * [min_distance, max_distance).  hit_bits must hold (n + 63) / 64 words;
+ * every word is overwritten.  Blocks until the bits are written. */
+int32_t vrad_trace_visibility(vrad_ctx *ctx, const vrad_ray *rays, int64_t n,
+                              const vrad_trace_options *opts, uint64_t *hit_bits);
+
+/* IRayTracer.TraceClosestAsync with HOST buffers: the nearest accepted hit
+ * in [min_distance, max_distance), ties to the lower triangle index. */
+int32_t vrad_trace_closest(vrad_ctx *ctx, const vrad_ray *rays, int64_t n,
+                           const vrad_trace_options *opts, vrad_hit *hits);
+
+/* The same two operations on DEVICE buffers, enqueued on `stream`
+ * (a cudaStream_t; NULL = the context's own stream).  Asynchronous: the
+ * results are ready when the stream reaches this point.  d_hit_bits must be
+ * 4-byte aligned and hold (n + 63) / 64 words. */
+int32_t vrad_trace_visibility_device(vrad_ctx *ctx, const vrad_ray *d_rays, int64_t n,
+                                     const vrad_trace_options *opts, uint64_t *d_hit_bits,
+                                     void *stream);
+int32_t vrad_trace_closest_device(vrad_ctx *ctx, const vrad_ray *d_rays, int64_t n,
+                                  const vrad_trace_options *opts, vrad_hit *d_hits,
+                                  void *stream);
+
+/* IRayTracer.TracerIdentity: backend, device and build, one token. */
+int32_t vrad_tracer_identity(vrad_ctx *ctx, char *buf, int32_t cap);
+
+/* The last error message on this context (or the last context-less error
+ * when ctx is NULL).  Returns the message length. */
+int32_t vrad_last_error(vrad_ctx *ctx, char *buf, int32_t cap);
+
+/* Library version, for a loader's sanity check. */
+int32_t vrad_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VRAD_CUDA_H */

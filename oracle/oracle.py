@@ -52,7 +52,7 @@ def lib() -> ctypes.CDLL:
         i32 = ctypes.c_int32
         f32 = ctypes.c_float
         _lib.orc_tri_prepare.argtypes = [P, P, P, i32, P]
-        _lib.orc_kd_trace.argtypes = [P, i32, P, i32, P, i32, P, P, i32, f32, i32, i32, P, P, P]
+        _lib.orc_kd_trace.argtypes = [P, i32, P, i32, P, i32, P, P, i32, f32, i32, i32, P, P, P, i32]
         _lib.orc_brute_trace.argtypes = [P, i32, P, i32, f32, i32, i32, P, P, P, i32]
         _lib.orc_fp64_classify.argtypes = [P, i32, P, i32, ctypes.c_double, P, i32]
         for name in ("orc_tri_prepare", "orc_kd_trace", "orc_brute_trace", "orc_fp64_classify"):
@@ -88,7 +88,7 @@ def prepare_triangles(verts: np.ndarray, ids: np.ndarray | None = None,
 
 
 def kd_trace(tree: dict, rays: np.ndarray, tmin: float = 0.0, skip_id: int = -1,
-             flags: int = 0):
+             flags: int = 0, threads: int = 1):
     """Restated KdRayTracer over a tree dict (nodes, indices, tris, bounds)."""
     rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 7)
     n = rays.shape[0]
@@ -101,7 +101,7 @@ def kd_trace(tree: dict, rays: np.ndarray, tmin: float = 0.0, skip_id: int = -1,
     bounds = np.ascontiguousarray(tree["bounds"], dtype=np.float32)
     rc = lib().orc_kd_trace(_p(nodes), len(nodes), _p(idx), len(idx), _p(tris), len(tris),
                             _p(bounds), _p(rays), n, tmin, skip_id, flags, _p(tri), _p(dist),
-                            _p(bits))
+                            _p(bits), threads)
     if rc != 0:
         raise RuntimeError(f"orc_kd_trace failed: {rc}")
     return tri, dist, bits

@@ -370,7 +370,7 @@ extern "C" int orc_kd_trace(const orc_kdnode *nodes, int32_t nnodes, const int32
                             int32_t nindices, const orc_tri *tris, int32_t ntris,
                             const float *bounds6, const orc_ray *rays, int32_t nrays, float tmin,
                             int32_t skip_id, int32_t flags, int32_t *out_tri, float *out_dist,
-                            uint64_t *out_bits) {
+                            uint64_t *out_bits, int32_t threads) {
     if (nnodes <= 0 || !nodes || !tris || !bounds6 || nrays < 0) return -1;
     (void)nindices;
     (void)ntris;
@@ -382,31 +382,35 @@ extern "C" int orc_kd_trace(const orc_kdnode *nodes, int32_t nnodes, const int32
     const bool full_walk = flags & ORC_FULL_WALK;
     if (out_bits)
         std::memset(out_bits, 0, sizeof(uint64_t) * (size_t)((nrays + 63) / 64));
-    std::vector<StackEntry> stack;
-    stack.reserve(64);
     const int step = isolated ? 1 : 4;
-    float tmin4[4] = {tmin, tmin, tmin, tmin};
-    for (int32_t i = 0; i < nrays; i += step) {
-        Packet p;
-        float reach[4];
-        load_packet(rays, nrays, i, isolated, p, reach);
-        // settle: visibility without sky pass-through stops once blocked
-        // (KdRayTracer.cs:730-737, 590-596); closest never settles.
-        bool settle = !closest && !full_walk && !sky;
-        float dist[4];
-        int ids[4];
-        trace4(s, p, tmin4, reach, skip_id, settle, dist, ids, stack);
-        for (int l = 0; l < step && i + l < nrays; l++) {
-            int id = ids[l];
-            if (out_tri) out_tri[i + l] = id;
-            if (out_dist) out_dist[i + l] = dist[l];
-            if (!closest && out_bits) {
-                bool blocked = id > -1 && dist[l] < reach[l];
-                if (sky && id >= 0 && (tris[id].id & ORC_TRACE_ID_SKY)) blocked = false;
-                if (blocked) out_bits[(i + l) >> 6] |= 1ull << ((i + l) & 63);
+    // Workers take whole 64-ray words, so packets of four never straddle
+    // two workers and no bit word is shared.
+    parallel_for(nrays, threads, [&](int32_t b, int32_t e) {
+        std::vector<StackEntry> stack;
+        stack.reserve(64);
+        float tmin4[4] = {tmin, tmin, tmin, tmin};
+        for (int32_t i = b; i < e; i += step) {
+            Packet p;
+            float reach[4];
+            load_packet(rays, e, i, isolated, p, reach);
+            // settle: visibility without sky pass-through stops once blocked
+            // (KdRayTracer.cs:730-737, 590-596); closest never settles.
+            bool settle = !closest && !full_walk && !sky;
+            float dist[4];
+            int ids[4];
+            trace4(s, p, tmin4, reach, skip_id, settle, dist, ids, stack);
+            for (int l = 0; l < step && i + l < e; l++) {
+                int id = ids[l];
+                if (out_tri) out_tri[i + l] = id;
+                if (out_dist) out_dist[i + l] = dist[l];
+                if (!closest && out_bits) {
+                    bool blocked = id > -1 && dist[l] < reach[l];
+                    if (sky && id >= 0 && (tris[id].id & ORC_TRACE_ID_SKY)) blocked = false;
+                    if (blocked) out_bits[(i + l) >> 6] |= 1ull << ((i + l) & 63);
+                }
             }
         }
-    }
+    });
     return 0;
 }
 

@@ -62,7 +62,7 @@ int orc_kd_trace(const orc_kdnode *nodes, int32_t nnodes, const int32_t *indices
                  int32_t nindices, const orc_tri *tris, int32_t ntris,
                  const float *bounds6, const orc_ray *rays, int32_t nrays,
                  float tmin, int32_t skip_id, int32_t flags, int32_t *out_tri,
-                 float *out_dist, uint64_t *out_bits);
+                 float *out_dist, uint64_t *out_bits, int32_t threads);
 
 /* The semantic the CUDA tracer implements, by brute force over every
  * triangle with the same FP32 predicate: visibility = any accepted hit with
