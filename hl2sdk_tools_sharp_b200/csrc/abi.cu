@@ -290,7 +290,7 @@ int32_t vrad_trace_visibility_device(vrad_ctx *ctx, const vrad_ray *d_rays, int6
     if (((uintptr_t)d_hit_bits & 3) != 0) return fail(ctx, VRAD_ERR_ARG, "hit bits not 4-byte aligned");
     if (n == 0) return VRAD_OK;
     std::lock_guard<std::mutex> g(ctx->mu);
-    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    cudaStream_t s = (cudaStream_t)stream;  // NULL is the CUDA default stream
     const size_t words32 = (size_t)((n + 31) / 32);
     if (words32 & 1) {
         cudaError_t e = cudaMemsetAsync((uint32_t *)d_hit_bits + words32, 0, 4, s);
@@ -309,7 +309,7 @@ int32_t vrad_trace_closest_device(vrad_ctx *ctx, const vrad_ray *d_rays, int64_t
                     "sky pass-through is a visibility option; a closest-hit trace reports the sky hit itself");
     if (n == 0) return VRAD_OK;
     std::lock_guard<std::mutex> g(ctx->mu);
-    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    cudaStream_t s = (cudaStream_t)stream;  // NULL is the CUDA default stream
     return trace_device(ctx, d_rays, n, opts, nullptr, d_hits, vrad::kModeClosest, s);
 }
 

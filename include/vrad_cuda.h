@@ -138,9 +138,10 @@ int32_t vrad_trace_closest(vrad_ctx *ctx, const vrad_ray *rays, int64_t n,
                            const vrad_trace_options *opts, vrad_hit *hits);
 
 /* The same two operations on DEVICE buffers, enqueued on `stream`
- * (a cudaStream_t; NULL = the context's own stream).  Asynchronous: the
- * results are ready when the stream reaches this point.  d_hit_bits must be
- * 4-byte aligned and hold (n + 63) / 64 words. */
+ * (a cudaStream_t; NULL is the CUDA default stream, as everywhere in CUDA).
+ * Asynchronous: the results are ready when the stream reaches this point.
+ * d_hit_bits must be 4-byte aligned and hold (n + 63) / 64 words.  Launches
+ * on different streams may overlap; they share no device scratch. */
 int32_t vrad_trace_visibility_device(vrad_ctx *ctx, const vrad_ray *d_rays, int64_t n,
                                      const vrad_trace_options *opts, uint64_t *d_hit_bits,
                                      void *stream);
