@@ -59,56 +59,10 @@ def world_for(side: int):
 
 
 def device_rays(world, device):
-    """The full direct-light ray set, built on the device with torch."""
-    import torch
+    """The full direct-light ray set, built on the device with torch, in
+    face-coherent order (see workload.direct_rays)."""
     from hl2sdk_tools_sharp_b200 import workload as wl
-    s = wl.luxel_samples(world)
-    P = torch.from_numpy(s.points).to(device)
-    N = torch.from_numpy(s.normals).to(device)
-    C = torch.from_numpy(s.cluster.astype(np.int64)).to(device)
-    pvs = torch.from_numpy(world.pvs).to(device)
-    L = torch.from_numpy(world.light_origin).to(device)
-    LC = torch.from_numpy(world.light_cluster.astype(np.int64)).to(device)
-    Ln = torch.from_numpy(world.light_normal).to(device)
-    cos_outer = torch.from_numpy(np.cos(np.radians(world.light_cone[:, 1])).astype(np.float32)).to(device)
-    spot = torch.from_numpy(world.light_type == 2).to(device)
-
-    def seg(a, b):
-        r = torch.empty((a.shape[0], 7), dtype=torch.float32, device=device)
-        r[:, 0:3] = a
-        r[:, 3:6] = b - a
-        r[:, 6] = 1.0
-        return r
-
-    light_parts = []
-    chunk = 1 << 20
-    for b in range(0, P.shape[0], chunk):
-        p, n, c = P[b:b + chunk], N[b:b + chunk], C[b:b + chunk]
-        delta = L[None, :, :] - p[:, None, :]
-        dot = (delta * n[:, None, :]).sum(-1)
-        ok = pvs[c][:, LC] & (dot > 0)
-        dist = delta.norm(dim=-1).clamp_min(1e-6)
-        cos_to = -(delta * Ln[None]).sum(-1) / dist
-        ok &= ~spot[None, :] | (cos_to > cos_outer[None, :])
-        si, li = torch.nonzero(ok, as_tuple=True)
-        light_parts.append(seg(p[si], L[li]))
-    light = torch.cat(light_parts)
-
-    sun_dir = torch.from_numpy(world.sun_direction).to(device)
-    faces = -(N @ sun_dir) > 0
-    sp = P[faces]
-    sun = seg(sp, sp + sun_dir * -float(wl.MAX_TRACE_LENGTH))
-
-    dirs = torch.from_numpy(wl.ambient_directions()).to(device)
-    sky_parts = []
-    for b in range(0, P.shape[0], chunk):
-        p, n = P[b:b + chunk], N[b:b + chunk]
-        si, di = torch.nonzero(-(n @ dirs.T) > float(wl.EQUAL_EPSILON), as_tuple=True)
-        sky_parts.append(seg(p[si], p[si] + dirs[di] * -float(wl.MAX_TRACE_LENGTH)))
-    sky = torch.cat(sky_parts)
-    del sky_parts, light_parts
-    return {"light": light.contiguous(), "sun": sun.contiguous(), "sky": sky.contiguous(),
-            "luxels": int(P.shape[0])}
+    return wl.direct_rays_device(world, wl.luxel_samples(world), device)
 
 
 class ClockSampler:

@@ -20,6 +20,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "scene.cuh"
 
@@ -110,11 +111,44 @@ int32_t upload(vrad_ctx *ctx, const vrad_triangle *tris, const vrad_kd_triangle 
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
     ctx->has_scene = false;
-    e = vrad::build_scene(ctx->scene, tris, prep, n, ctx->stream, &ctx->report);
-    if (e == cudaErrorInvalidValue && prep)
-        return fail(ctx, VRAD_ERR_ARG,
-                    "a supplied triangle's projection axes are not the successors of its drop axis");
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "scene build");
+    ctx->scene.release();
+    ctx->report = vrad::SceneBuildReport();
+    // Split by the id's sky bit (TraceId.Sky): two BVHs, so a sky test can
+    // find the nearest sky hit in the small one and then ask the large one
+    // only whether anything opaque lies before it.
+    std::vector<vrad_triangle> part[2];
+    std::vector<vrad_kd_triangle> ppart[2];
+    std::vector<int32_t> orig[2];
+    std::vector<int32_t> ids((size_t)n);
+    for (int32_t i = 0; i < n; i++) {
+        const int32_t id = prep ? prep[i].id : tris[i].id;
+        const int k = ((uint32_t)id & vrad::kTraceIdSky) ? 1 : 0;
+        ids[(size_t)i] = id;
+        part[k].push_back(tris[i]);
+        if (prep) ppart[k].push_back(prep[i]);
+        orig[k].push_back(i);
+    }
+    e = cudaMalloc(&ctx->scene.tri_id, sizeof(int32_t) * (size_t)n);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(ctx->scene.tri_id, ids.data(), sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        ctx->scene.release();
+        return cuda_fail(ctx, e, "scene ids");
+    }
+    ctx->scene.ntris = n;
+    vrad::BvhBuffers *dst[2] = {&ctx->scene.opaque, &ctx->scene.sky};
+    for (int k = 0; k < 2; k++) {
+        e = vrad::build_bvh(*dst[k], part[k].data(), prep ? ppart[k].data() : nullptr, orig[k].data(),
+                            (int)part[k].size(), ctx->stream, &ctx->report);
+        if (e != cudaSuccess) {
+            ctx->scene.release();
+            if (e == cudaErrorInvalidValue && prep)
+                return fail(ctx, VRAD_ERR_ARG,
+                            "a supplied triangle's projection axes are not the successors of its drop axis");
+            return cuda_fail(ctx, e, "scene build");
+        }
+    }
+    ctx->report.device_bytes += (int64_t)n * 4;
     ctx->has_scene = true;
     return VRAD_OK;
 }

@@ -53,9 +53,9 @@ __device__ inline void edge_equation(const float p1[3], const float p2[3], int c
 }
 
 __global__ void k_prepare(const vrad_triangle *__restrict__ in,
-                          const vrad_kd_triangle *__restrict__ prepared, int n,
-                          float4 *__restrict__ t0, float4 *__restrict__ t1,
-                          float4 *__restrict__ t2, int32_t *__restrict__ ids,
+                          const vrad_kd_triangle *__restrict__ prepared,
+                          const int32_t *__restrict__ orig, int n, float4 *__restrict__ t0,
+                          float4 *__restrict__ t1, float4 *__restrict__ t2,
                           float *__restrict__ box) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -115,8 +115,7 @@ __global__ void k_prepare(const vrad_triangle *__restrict__ in,
     uint32_t meta = (uint32_t)(drop & 3) | (((uint32_t)id & kTraceIdSky) ? 4u : 0u) | (flags << 8);
     t0[i] = make_float4(nrm[0], nrm[1], nrm[2], d);
     t1[i] = make_float4(eq1[0], eq1[1], eq1[2], eq2[0]);
-    t2[i] = make_float4(eq2[1], eq2[2], __int_as_float(i), __uint_as_float(meta));
-    ids[i] = id;
+    t2[i] = make_float4(eq2[1], eq2[2], __int_as_float(orig[i]), __uint_as_float(meta));
     for (int a = 0; a < 3; a++) {
         box[6 * i + a] = dmin(dmin(p1[a], p2[a]), p3[a]);
         box[6 * i + 3 + a] = dmax(dmax(p1[a], p2[a]), p3[a]);
@@ -379,14 +378,15 @@ inline int blocks(int n, int b) { return (n + b - 1) / b; }
         }                                                \
     } while (0)
 
-cudaError_t build_scene(SceneBuffers &sb, const vrad_triangle *h_tris,
-                        const vrad_kd_triangle *h_prepared, int n, cudaStream_t stream,
-                        SceneBuildReport *report) {
+cudaError_t build_bvh(BvhBuffers &sb, const vrad_triangle *h_tris,
+                      const vrad_kd_triangle *h_prepared, const int32_t *h_orig, int n,
+                      cudaStream_t stream, SceneBuildReport *report) {
     cudaError_t err = cudaSuccess;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // Scratch (freed at the end of the build).
     vrad_triangle *d_in = nullptr;
     vrad_kd_triangle *d_prep = nullptr;
+    int32_t *d_orig = nullptr;
     float4 *u0 = nullptr, *u1 = nullptr, *u2 = nullptr;
     float *tri_box = nullptr, *d_bounds = nullptr, *node_box = nullptr, *node_cost = nullptr,
           *leaf_box = nullptr;
@@ -403,6 +403,7 @@ cudaError_t build_scene(SceneBuffers &sb, const vrad_triangle *h_tris,
     const int inner = n > 1 ? n - 1 : 1;
 
     sb.release();
+    if (n <= 0) return cudaSuccess;  // an empty subset: no BVH, never traversed
     VRAD_TRY(cudaEventCreate(&ev0));
     VRAD_TRY(cudaEventCreate(&ev1));
     VRAD_TRY(cudaEventRecord(ev0, stream));
@@ -414,6 +415,8 @@ cudaError_t build_scene(SceneBuffers &sb, const vrad_triangle *h_tris,
         VRAD_TRY(cudaMemcpyAsync(d_prep, h_prepared, sizeof(vrad_kd_triangle) * n,
                                  cudaMemcpyHostToDevice, stream));
     }
+    VRAD_TRY(cudaMalloc(&d_orig, sizeof(int32_t) * n));
+    VRAD_TRY(cudaMemcpyAsync(d_orig, h_orig, sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream));
     VRAD_TRY(cudaMalloc(&u0, sizeof(float4) * n));
     VRAD_TRY(cudaMalloc(&u1, sizeof(float4) * n));
     VRAD_TRY(cudaMalloc(&u2, sizeof(float4) * n));
@@ -422,13 +425,12 @@ cudaError_t build_scene(SceneBuffers &sb, const vrad_triangle *h_tris,
     VRAD_TRY(cudaMalloc(&sb.tri0, sizeof(float4) * n));
     VRAD_TRY(cudaMalloc(&sb.tri1, sizeof(float4) * n));
     VRAD_TRY(cudaMalloc(&sb.tri2, sizeof(float4) * n));
-    VRAD_TRY(cudaMalloc(&sb.tri_id, sizeof(int32_t) * n));
     VRAD_TRY(cudaMalloc(&sb.nodes, sizeof(float4) * 4 * inner));
     VRAD_TRY(cudaMalloc(&leaf_box, sizeof(float) * 6 * n));
     VRAD_TRY(cudaMalloc(&d_stats, sizeof(int) * 4));
     VRAD_TRY(cudaMemsetAsync(d_stats, 0, sizeof(int) * 4, stream));
 
-    k_prepare<<<blocks(n, 128), 128, 0, stream>>>(d_in, d_prep, n, u0, u1, u2, sb.tri_id, tri_box);
+    k_prepare<<<blocks(n, 128), 128, 0, stream>>>(d_in, d_prep, d_orig, n, u0, u1, u2, tri_box);
     VRAD_TRY(cudaGetLastError());
     k_bounds<<<1, 256, 0, stream>>>(tri_box, n, d_bounds);
     VRAD_TRY(cudaGetLastError());
@@ -512,22 +514,26 @@ cudaError_t build_scene(SceneBuffers &sb, const vrad_triangle *h_tris,
         goto fail;
     }
     sb.ntris = n;
-    sb.root_ref = 0;
     if (report) {
-        report->nodes = stats[0];
-        report->leaves = stats[1];
-        report->max_leaf = stats[2];
-        for (int a = 0; a < 6; a++) report->bounds[a] = bounds[a];
-        report->pad = ldexpf(bounds[6], -16) + 1e-6f;
+        const bool first = report->nodes == 0 && report->leaves == 0;
+        report->nodes += stats[0];
+        report->leaves += stats[1];
+        report->max_leaf = stats[2] > report->max_leaf ? stats[2] : report->max_leaf;
+        for (int a = 0; a < 3; a++) {
+            report->bounds[a] = first ? bounds[a] : fminf(report->bounds[a], bounds[a]);
+            report->bounds[3 + a] = first ? bounds[3 + a] : fmaxf(report->bounds[3 + a], bounds[3 + a]);
+        }
+        report->pad = fmaxf(report->pad, ldexpf(bounds[6], -16) + 1e-6f);
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, ev0, ev1);
-        report->build_ms = ms;
-        report->device_bytes = (int64_t)n * (48 + 4) + (int64_t)inner * 64;
+        report->build_ms += ms;
+        report->device_bytes += (int64_t)n * 48 + (int64_t)inner * 64;
     }
 
 fail:
     cudaFree(d_in);
     cudaFree(d_prep);
+    cudaFree(d_orig);
     cudaFree(u0);
     cudaFree(u1);
     cudaFree(u2);
@@ -554,17 +560,22 @@ fail:
     return err;
 }
 
-void SceneBuffers::release() {
+void BvhBuffers::release() {
     cudaFree(tri0);
     cudaFree(tri1);
     cudaFree(tri2);
-    cudaFree(tri_id);
     cudaFree(nodes);
     tri0 = tri1 = tri2 = nullptr;
-    tri_id = nullptr;
     nodes = nullptr;
     ntris = 0;
-    root_ref = 0;
+}
+
+void SceneBuffers::release() {
+    opaque.release();
+    sky.release();
+    cudaFree(tri_id);
+    tri_id = nullptr;
+    ntris = 0;
 }
 
 }  // namespace vrad

@@ -7,17 +7,26 @@
 
 namespace vrad {
 
-struct SceneBuffers {
+// One BVH over a subset of the scene's triangles.
+struct BvhBuffers {
     float4 *tri0 = nullptr;
     float4 *tri1 = nullptr;
     float4 *tri2 = nullptr;
-    int32_t *tri_id = nullptr;
     float4 *nodes = nullptr;
     int32_t ntris = 0;
-    int32_t root_ref = 0;
 
     void release();
-    DeviceScene view() const { return DeviceScene{tri0, tri1, tri2, tri_id, nodes, root_ref, ntris}; }
+    DeviceBvh view() const { return DeviceBvh{tri0, tri1, tri2, nodes, ntris}; }
+};
+
+struct SceneBuffers {
+    BvhBuffers opaque;
+    BvhBuffers sky;
+    int32_t *tri_id = nullptr;  // caller ids by original index
+    int32_t ntris = 0;
+
+    void release();
+    DeviceScene view() const { return DeviceScene{opaque.view(), sky.view(), tri_id}; }
 };
 
 struct SceneBuildReport {
@@ -30,11 +39,13 @@ struct SceneBuildReport {
     int64_t device_bytes = 0;
 };
 
-// Builds `sb` from n host triangles (and, optionally, their intersection
-// form).  Synchronises `stream` before returning.
-cudaError_t build_scene(SceneBuffers &sb, const vrad_triangle *h_tris,
-                        const vrad_kd_triangle *h_prepared, int n, cudaStream_t stream,
-                        SceneBuildReport *report);
+// Builds one BVH from n host triangles (and, optionally, their
+// intersection form); h_orig gives each triangle's original index in the
+// whole scene.  Synchronises `stream` before returning.  report is
+// accumulated into (counts added, bounds merged).
+cudaError_t build_bvh(BvhBuffers &bb, const vrad_triangle *h_tris,
+                      const vrad_kd_triangle *h_prepared, const int32_t *h_orig, int n,
+                      cudaStream_t stream, SceneBuildReport *report);
 
 // Traversal launches (trace.cu).  d_bits is written as 32-bit words.
 cudaError_t launch_trace(const DeviceScene &scene, const vrad_ray *d_rays, int64_t n,

@@ -46,7 +46,7 @@ __device__ inline float sel3(int axis, float x, float y, float z) {
 // The predicate.  Returns true with the exact t when the triangle accepts
 // the ray (|d.n| > eps, eps < t < 1e23, both edge values >= eps, their sum
 // <= 1).
-__device__ __forceinline__ bool kd_hit(const DeviceScene &s, int k, const RayState &r, float &t_out,
+__device__ __forceinline__ bool kd_hit(const DeviceBvh &s, int k, const RayState &r, float &t_out,
                                        uint32_t &meta_out, int32_t &orig_out) {
     const float4 A = __ldg(&s.tri0[k]);
     float ddotn = __fmul_rn(r.dx, A.x);
@@ -105,29 +105,26 @@ __device__ __forceinline__ void slab2(const float4 &a, const float4 &b, const fl
     n1 = tn1;
 }
 
-// One ray.  MODE kModeAny stops at the first accepted hit in
-// [tmin, reach); the other modes find the lexicographically smallest
-// (t, original index) in that window.
-template <int MODE>
-__device__ __forceinline__ void trace_ray(const DeviceScene &s, const RayState &r, float tmin,
-                                          float reach, int32_t skip_id, int *stack,
-                                          uint32_t *overflow, bool &hit, float &best_t,
-                                          int32_t &best_orig, uint32_t &best_meta) {
-    hit = false;
-    best_t = reach;
-    best_orig = 0x7fffffff;
-    best_meta = 0;
+// One walk of one BVH.  Accepts a triangle hit (t, orig) when
+// t >= tmin and (t, orig) is lexicographically below the current best
+// (thi, best_orig); best_orig = -1 makes the window half-open, [tmin, thi).
+// ANY stops at the first acceptance; otherwise the best is kept and the
+// box window shrinks to [tmin, thi].  Returns whether anything was accepted.
+template <bool ANY>
+__device__ __forceinline__ bool walk(const DeviceBvh &s, const int32_t *__restrict__ tri_id,
+                                     const RayState &r, float tmin, int32_t skip_id, int *stack,
+                                     uint32_t *overflow, float &thi, int32_t &best_orig,
+                                     uint32_t &best_meta) {
+    bool hit = false;
     int sp = 0;
-    int ref = s.root_ref;
-    // The box window: [tmin, reach] for any-hit, [tmin, best] once a
-    // closest candidate exists (a tie at best may still win on index).
+    int ref = 0;
     while (true) {
         if (ref >= 0) {
             const float4 *nd = s.nodes + 4 * ref;
             const float4 a = __ldg(nd), b = __ldg(nd + 1), c = __ldg(nd + 2), d = __ldg(nd + 3);
             bool h0, h1;
             float n0, n1;
-            slab2(a, b, c, r, tmin, best_t, h0, h1, n0, n1);
+            slab2(a, b, c, r, tmin, thi, h0, h1, n0, n1);
             const int r0 = __float_as_int(d.x), r1 = __float_as_int(d.y);
             if (h0 && h1) {
                 int near_ref = r0, far_ref = r1;
@@ -162,26 +159,53 @@ __device__ __forceinline__ void trace_ray(const DeviceScene &s, const RayState &
                 int32_t orig;
                 if (!kd_hit(s, k, r, t, meta, orig)) continue;
                 if (!(t >= tmin)) continue;
-                if (skip_id != -1 && __ldg(&s.tri_id[orig]) == skip_id) continue;
-                if (MODE == kModeAny) {
-                    if (t < reach) {
-                        hit = true;
-                        return;
-                    }
-                } else {
-                    const bool better = hit ? (t < best_t || (t == best_t && orig < best_orig)) : (t < reach);
-                    if (better) {
-                        hit = true;
-                        best_t = t;
-                        best_orig = orig;
-                        best_meta = meta;
-                    }
-                }
+                if (!(t < thi || (t == thi && orig < best_orig))) continue;
+                if (skip_id != -1 && __ldg(&tri_id[orig]) == skip_id) continue;
+                hit = true;
+                thi = t;
+                best_orig = orig;
+                best_meta = meta;
+                if (ANY) return true;
             }
         }
-        if (sp == 0) return;
+        if (sp == 0) return hit;
         sp--;
         ref = stack[sp * kBlock];
+    }
+}
+
+// One ray against the scene.  Modes:
+//   kModeAny      any accepted hit in [tmin, reach), opaque or sky;
+//   kModeClosest  the smallest (t, original index) in [tmin, reach);
+//   kModeSkyPass  blocked iff that smallest hit exists and is opaque: the
+//                 nearest sky hit (t_s, i_s) is found first, then any
+//                 opaque hit below it decides, so the opaque walk stops at
+//                 its first acceptance.
+template <int MODE>
+__device__ __forceinline__ void trace_ray(const DeviceScene &s, const RayState &r, float tmin,
+                                          float reach, int32_t skip_id, int *stack,
+                                          uint32_t *overflow, bool &hit, float &best_t,
+                                          int32_t &best_orig, uint32_t &best_meta) {
+    best_t = reach;
+    best_orig = -1;
+    best_meta = 0;
+    hit = false;
+    if (MODE == kModeAny) {
+        if (s.opaque.ntris)
+            hit = walk<true>(s.opaque, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
+        if (!hit && s.sky.ntris)
+            hit = walk<true>(s.sky, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
+    } else if (MODE == kModeClosest) {
+        if (s.opaque.ntris)
+            hit = walk<false>(s.opaque, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
+        if (s.sky.ntris)
+            hit |= walk<false>(s.sky, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
+    } else {
+        if (s.sky.ntris)
+            walk<false>(s.sky, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
+        // Blocked iff an opaque hit sorts before the nearest sky hit.
+        if (s.opaque.ntris)
+            hit = walk<true>(s.opaque, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
     }
 }
 
@@ -231,9 +255,7 @@ __global__ void __launch_bounds__(kBlock) k_trace(DeviceScene s, const vrad_ray 
             hits[i] = h;
         }
     } else {
-        bool blocked = hit;
-        if (MODE == kModeSkyPass) blocked = hit && !(best_meta & 4u);
-        const uint32_t word = __ballot_sync(kFull, blocked);
+        const uint32_t word = __ballot_sync(kFull, hit);
         if (lane == 0) bits[i >> 5] = word;
     }
 }

@@ -1,8 +1,10 @@
 // vrad_internal.cuh -- device-side layout shared by the scene build and the
 // traversal kernels of libvrad_cuda.
 //
-// Scene layout in HBM (structure of arrays, every record 16-byte aligned so
-// each is one or more 128-bit loads):
+// Scene layout in HBM.  The triangles are split by the sky bit of their id
+// into two BVHs, opaque and sky, each laid out as below (structure of
+// arrays, every record 16-byte aligned so each is one or more 128-bit
+// loads); tri_id is shared and indexed by the original triangle index.
 //
 //   tri0[i]  float4 (nx, ny, nz, d)          plane of the i-th triangle in
 //   tri1[i]  float4 (e0, e1, e2, e3)         BVH leaf order: the reference's
@@ -32,14 +34,18 @@ constexpr uint32_t kTraceIdSky = 0x01000000u;   // TraceId.Sky (MapTools/Rad/Tra
 constexpr float kKdEps = 1.0e-10f;              // KdRayTracer.cs:1209-1230
 constexpr float kKdHuge = 1.0e23f;              // KdRayTracer.cs:985
 
-struct DeviceScene {
+struct DeviceBvh {
     const float4 *tri0;
     const float4 *tri1;
     const float4 *tri2;
-    const int32_t *tri_id;
     const float4 *nodes;
-    int32_t root_ref;
-    int32_t ntris;
+    int32_t ntris;  // 0: empty, never traversed
+};
+
+struct DeviceScene {
+    DeviceBvh opaque;
+    DeviceBvh sky;
+    const int32_t *tri_id;
 };
 
 enum TraceMode : int { kModeAny = 0, kModeClosest = 1, kModeSkyPass = 2 };

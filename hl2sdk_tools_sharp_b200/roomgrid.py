@@ -17,6 +17,8 @@ generator returns is what vrad's lighting stage reads from a compiled BSP:
 * a PVS with one cluster per room: a room sees itself and the rooms up to
   two steps away along its row or column (straight lines through doors).
 
+Every room has its own floor and ceiling brush, as an authored map would.
+
 There is no BSP tree, no vbsp CSG and no visibility compile: those are
 outside the lighting stage.  Floor faces are not split around pillars; the
 luxels under a pillar are simply in its shadow.
@@ -128,14 +130,17 @@ def _door_span(i: int) -> tuple[float, float]:
 
 def _brushes(cfg: Config, rng: np.random.Generator):
     R = cfg.side
-    extent = R * PITCH + WALL
     boxes = []     # (min, max)
     sky = []       # index of the brush side (in _box_sides order) that is sky, or -1
-    # Floor and ceiling slabs (the ceiling's underside is sky).
-    boxes.append(((0.0, 0.0, -WALL), (extent, extent, 0.0)))
-    sky.append(-1)
-    boxes.append(((0.0, 0.0, ROOM), (extent, extent, ROOM + WALL)))
-    sky.append(0)
+    # A floor slab and a ceiling slab per room, each overlapping the wall
+    # footprints around the room; the ceiling's underside is sky.
+    for i in range(R):
+        for j in range(R):
+            x0, y0 = i * PITCH, j * PITCH
+            boxes.append(((x0, y0, -WALL), (x0 + PITCH + WALL, y0 + PITCH + WALL, 0.0)))
+            sky.append(-1)
+            boxes.append(((x0, y0, ROOM), (x0 + PITCH + WALL, y0 + PITCH + WALL, ROOM + WALL)))
+            sky.append(0)
     # Corner posts.
     for i in range(R + 1):
         for j in range(R + 1):

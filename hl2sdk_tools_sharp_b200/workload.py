@@ -125,45 +125,124 @@ def _segments(starts: np.ndarray, ends: np.ndarray) -> np.ndarray:
     return r
 
 
+def _face_runs(face: np.ndarray):
+    """Start and length of each face's run of consecutive samples."""
+    change = np.flatnonzero(np.diff(face)) + 1
+    starts = np.concatenate([[0], change])
+    counts = np.diff(np.concatenate([starts, [len(face)]]))
+    return starts, counts, face[starts]
+
+
 def direct_rays(world: World, samples: Samples, ambient: bool | None = None,
                 directions: np.ndarray | None = None) -> DirectRays:
+    """Rays in the order a warp-per-32-luxels emitter produces them: face by
+    face, and within a face light by light (or direction by direction),
+    sample by sample, so neighbouring rays share a target and a direction."""
     P, N, C = samples.points, samples.normals, samples.cluster
-    # Lights in the PVS that the sample faces.
-    li_s, li_l = [], []
+    starts, counts, fids = _face_runs(samples.face)
+    run_of = np.repeat(np.arange(len(starts)), counts)
+
+    # Lights in the PVS that the sample faces; a spot's cone must reach it.
+    ok = np.zeros((len(P), len(world.light_origin)), bool)
     for l in range(len(world.light_origin)):
-        vis = world.pvs[C, world.light_cluster[l]]
         delta = world.light_origin[l][None, :] - P
-        dot = np.einsum("ij,ij->i", delta, N)
-        ok = vis & (dot > 0)
+        m = world.pvs[C, world.light_cluster[l]] & (np.einsum("ij,ij->i", delta, N) > 0)
         if world.light_type[l] == 2:
-            dist = np.linalg.norm(delta, axis=1)
-            cos_to = -np.einsum("ij,j->i", delta, world.light_normal[l]) / np.maximum(dist, 1e-6)
-            ok &= cos_to > np.cos(np.radians(world.light_cone[l, 1]))
-        idx = np.nonzero(ok)[0]
-        li_s.append(idx)
-        li_l.append(np.full(len(idx), l, np.int32))
-    li_s = np.concatenate(li_s) if li_s else np.zeros(0, np.int64)
-    li_l = np.concatenate(li_l) if li_l else np.zeros(0, np.int32)
-    order = np.lexsort((li_l, li_s))     # sample-major, light order within a sample
-    li_s, li_l = li_s[order], li_l[order]
+            dist = np.maximum(np.linalg.norm(delta, axis=1), 1e-6)
+            cos_to = -np.einsum("ij,j->i", delta, world.light_normal[l]) / dist
+            m &= cos_to > np.cos(np.radians(world.light_cone[l, 1]))
+        ok[:, l] = m
+    si, li = np.nonzero(ok)
+    order = np.lexsort((si, li, run_of[si]))        # face, then light, then sample
+    li_s, li_l = si[order], li[order].astype(np.int32)
     light = _segments(P[li_s], world.light_origin[li_l])
 
-    # Sun.
+    # Sun: every sample of a face that faces it.
     sun_dir = world.sun_direction
     faces_sun = -(N @ sun_dir) > 0
     sp = P[faces_sun]
     sun = _segments(sp, sp + (sun_dir * -MAX_TRACE_LENGTH)[None, :])
 
-    # Sky ambient.
+    # Sky ambient: per face, per direction in front of it, every sample.
     if ambient is None:
         ambient = bool(np.any(world.sky_intensity > 0))
     if ambient:
         dirs = ambient_directions() if directions is None else directions
-        dots = -(N @ dirs.T)                           # (N, D)
-        si, di = np.nonzero(dots > EQUAL_EPSILON)
-        starts = P[si]
-        ends = starts + (dirs[di] * -MAX_TRACE_LENGTH)
-        sky = _segments(starts, ends)
+        valid = -(world.face_normal[fids] @ dirs.T) > EQUAL_EPSILON      # (runs, D)
+        pr, pd = np.nonzero(valid)
+        reps = counts[pr]
+        pair = np.repeat(np.arange(len(pr)), reps)
+        first = np.concatenate([[0], np.cumsum(reps)[:-1]])
+        sample = starts[pr][pair] + (np.arange(len(pair)) - first[pair])
+        st = P[sample]
+        sky = _segments(st, st + dirs[pd][pair] * -MAX_TRACE_LENGTH)
     else:
         sky = np.zeros(0, RAY_DTYPE)
     return DirectRays(light, sun, sky, li_s.astype(np.int64), li_l)
+
+
+def direct_rays_device(world: World, samples: Samples, device) -> dict:
+    """direct_rays built on a CUDA device with torch, same rays in the same
+    order, as (n, 7) float32 tensors."""
+    import torch
+    P = torch.from_numpy(samples.points).to(device)
+    N = torch.from_numpy(samples.normals).to(device)
+    C = torch.from_numpy(samples.cluster.astype(np.int64)).to(device)
+    starts, counts, fids = _face_runs(samples.face)
+    run_of = torch.from_numpy(np.repeat(np.arange(len(starts)), counts)).to(device)
+    pvs = torch.from_numpy(world.pvs).to(device)
+    Lo = torch.from_numpy(world.light_origin).to(device)
+    LC = torch.from_numpy(world.light_cluster.astype(np.int64)).to(device)
+    Ln = torch.from_numpy(world.light_normal).to(device)
+    cos_outer = torch.from_numpy(np.cos(np.radians(world.light_cone[:, 1])).astype(np.float32)).to(device)
+    spot = torch.from_numpy(world.light_type == 2).to(device)
+    nl = len(world.light_origin)
+
+    def seg(a, b):
+        r = torch.empty((a.shape[0], 7), dtype=torch.float32, device=device)
+        r[:, 0:3] = a
+        r[:, 3:6] = b - a
+        r[:, 6] = 1.0
+        return r
+
+    keys = []
+    chunk = 1 << 20
+    for b in range(0, P.shape[0], chunk):
+        p, n, c = P[b:b + chunk], N[b:b + chunk], C[b:b + chunk]
+        delta = Lo[None, :, :] - p[:, None, :]
+        ok = pvs[c][:, LC] & ((delta * n[:, None, :]).sum(-1) > 0)
+        dist = delta.norm(dim=-1).clamp_min(1e-6)
+        cos_to = -(delta * Ln[None]).sum(-1) / dist
+        ok &= ~spot[None, :] | (cos_to > cos_outer[None, :])
+        si, li = torch.nonzero(ok, as_tuple=True)
+        si = si + b
+        keys.append((run_of[si] * nl + li) * P.shape[0] + si)
+    key = torch.sort(torch.cat(keys)).values
+    si = key % P.shape[0]
+    li = (key // P.shape[0]) % nl
+    light = seg(P[si], Lo[li])
+    del keys, key
+
+    sun_dir = torch.from_numpy(world.sun_direction).to(device)
+    sp = P[-(N @ sun_dir) > 0]
+    sun = seg(sp, sp + sun_dir * -float(MAX_TRACE_LENGTH))
+
+    dirs = torch.from_numpy(ambient_directions()).to(device)
+    fn = torch.from_numpy(world.face_normal[fids]).to(device)
+    pr, pd = torch.nonzero(-(fn @ dirs.T) > float(EQUAL_EPSILON), as_tuple=True)
+    cnt = torch.from_numpy(counts).to(device)
+    st0 = torch.from_numpy(starts).to(device)
+    reps = cnt[pr]
+    sky_parts = []
+    pair_chunk = 1 << 16
+    for b in range(0, pr.shape[0], pair_chunk):
+        r = reps[b:b + pair_chunk]
+        pair = torch.repeat_interleave(torch.arange(r.shape[0], device=device), r)
+        first = torch.cumsum(r, 0) - r
+        sample = st0[pr[b:b + pair_chunk]][pair] + (torch.arange(pair.shape[0], device=device) - first[pair])
+        st = P[sample]
+        sky_parts.append(seg(st, st + dirs[pd[b:b + pair_chunk]][pair] * -float(MAX_TRACE_LENGTH)))
+    sky = torch.cat(sky_parts)
+    del sky_parts
+    return {"light": light.contiguous(), "sun": sun.contiguous(), "sky": sky.contiguous(),
+            "luxels": int(P.shape[0])}

@@ -23,8 +23,8 @@ def test_shadow_casters_follow_brush_shadow_casters(world3):
     ids = world3.tri_ids
     assert set(np.unique(ids)) == {rg.TRACE_ID_OPAQUE, rg.TRACE_ID_SKY}
     assert (ids == rg.TRACE_ID_SKY).sum() == 2 * 9        # one sky quad per room
-    # every brush is a box: 12 triangles, minus the ceiling's sky side
-    assert (ids == rg.TRACE_ID_OPAQUE).sum() == 12 * len(world3.brushes) - 2
+    # every brush is a box: 12 triangles, minus each ceiling's sky side
+    assert (ids == rg.TRACE_ID_OPAQUE).sum() == 12 * len(world3.brushes) - 2 * 9
 
 
 def test_lightmaps_respect_the_maximum_dimension(world3):
