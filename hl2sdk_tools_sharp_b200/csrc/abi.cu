@@ -347,6 +347,27 @@ int32_t vrad_trace_closest_device(vrad_ctx *ctx, const vrad_ray *d_rays, int64_t
     return trace_device(ctx, d_rays, n, opts, nullptr, d_hits, vrad::kModeClosest, s);
 }
 
+int32_t vrad_trace_visibility_static(vrad_ctx *ctx, const vrad_ray *rays, int64_t n,
+                                     const vrad_trace_options *opts, uint64_t *hit_bits) {
+    int32_t rc = validate(ctx, rays, n, opts, hit_bits);
+    if (rc != VRAD_OK) return rc;
+    if (n > VRAD_STATIC_MAX_RAYS)
+        return fail(ctx, VRAD_ERR_ARG,
+                    "%lld rays exceed the %d this allocation-free entry point stages; split the batch",
+                    (long long)n, VRAD_STATIC_MAX_RAYS);
+    if (n == 0) return VRAD_OK;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+    const int mode = (opts && opts->sky_does_not_block) ? vrad::kModeSkyPass : vrad::kModeAny;
+    e = vrad::trace_visibility_static(ctx->scene.view(), ctx->device, ctx->stream, rays, n,
+                                      params_of(opts, mode), hit_bits);
+    if (e == cudaErrorLaunchOutOfResources)
+        return fail(ctx, VRAD_ERR_CUDA, "traversal stack overflow (BVH deeper than %d)", vrad::kStackDepth);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "allocation-free visibility trace");
+    return VRAD_OK;
+}
+
 int32_t vrad_tracer_identity(vrad_ctx *ctx, char *buf, int32_t cap) {
     if (!ctx) return fail(nullptr, VRAD_ERR_ARG, "null context");
     if (buf && cap > 0) snprintf(buf, (size_t)cap, "%s", ctx->identity.c_str());

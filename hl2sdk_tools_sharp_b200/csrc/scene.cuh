@@ -52,4 +52,10 @@ cudaError_t launch_trace(const DeviceScene &scene, const vrad_ray *d_rays, int64
                          const TraceParams &p, uint32_t *d_bits, vrad_hit *d_hits,
                          uint32_t *d_overflow, cudaStream_t stream);
 
+// Host-buffer visibility through the library's fixed staging array
+// (noalloc.cu); allocates nothing.  n <= VRAD_STATIC_MAX_RAYS.
+cudaError_t trace_visibility_static(const DeviceScene &scene, int device, cudaStream_t stream,
+                                    const vrad_ray *h_rays, int64_t n, const TraceParams &p,
+                                    uint64_t *h_bits);
+
 }  // namespace vrad

@@ -149,6 +149,28 @@ int32_t vrad_trace_closest_device(vrad_ctx *ctx, const vrad_ray *d_rays, int64_t
                                   const vrad_trace_options *opts, vrad_hit *d_hits,
                                   void *stream);
 
+/* Largest batch vrad_trace_visibility_static accepts: four of the
+ * reference's 16,384-ray batches. */
+#define VRAD_STATIC_MAX_RAYS 65536
+
+/* vrad_trace_visibility for callers that must not allocate device memory
+ * during a run: hosts recording work into a CUDA graph, where an
+ * allocation's implicit synchronisation is not allowed, or processes that
+ * reserve all their device memory at start-up.  No counterpart in the
+ * reference.  Same arguments, answers and errors as vrad_trace_visibility,
+ * but rays and bits are staged through one fixed array inside the library
+ * (about 1.8 MB, held on every GPU that loads it until the process exits)
+ * instead of buffers grown with cudaMalloc, so the call makes no allocation.
+ * n above VRAD_STATIC_MAX_RAYS is refused with VRAD_ERR_ARG.
+ *
+ * The first call on a device looks up the array's address on that device;
+ * make that first call before any stream capture begins.  All calls on one
+ * device share the array: calls that overlap on the GPU (two contexts on one
+ * device, driven from two threads) race and must be serialised by the
+ * caller.  The call blocks until the bits are written. */
+int32_t vrad_trace_visibility_static(vrad_ctx *ctx, const vrad_ray *rays, int64_t n,
+                                     const vrad_trace_options *opts, uint64_t *hit_bits);
+
 /* IRayTracer.TracerIdentity: backend, device and build, one token. */
 int32_t vrad_tracer_identity(vrad_ctx *ctx, char *buf, int32_t cap);
 
