@@ -32,7 +32,7 @@ def nvcc() -> str:
 
 
 def sources() -> list[pathlib.Path]:
-    return sorted(CSRC.glob("*.cu"))
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
 
 
 def stale() -> bool:
@@ -52,7 +52,10 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     extra = ["-Xptxas", "-v"] if ptxas_info else []
     for src in sources():
         obj = objdir / (src.stem + ".o")
-        cmd = [nvcc(), *ARCH, *FLAGS, *extra, "-dc" if False else "-c", str(src), "-o", str(obj)]
+        # Host code rounds every float operation on its own (no FMA), as the
+        # reference's set-up does.
+        host = ["-Xcompiler", "-ffp-contract=off"]
+        cmd = [nvcc(), *ARCH, *FLAGS, *host, *extra, "-c", str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

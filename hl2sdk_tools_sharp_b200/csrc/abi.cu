@@ -22,24 +22,7 @@
 #include <string>
 #include <vector>
 
-#include "scene.cuh"
-
-struct vrad_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::mutex mu;
-    vrad::SceneBuffers scene;
-    vrad::SceneBuildReport report;
-    bool has_scene = false;
-    uint32_t *status = nullptr;   // [0] traversal stack overflow flag (sticky)
-    // Staging for the host-buffer entry points, grown on demand.
-    void *d_rays = nullptr;
-    size_t d_rays_cap = 0;
-    void *d_out = nullptr;
-    size_t d_out_cap = 0;
-    std::string last_error;
-    std::string identity;
-};
+#include "context.cuh"
 
 namespace {
 
@@ -176,6 +159,17 @@ int32_t validate(vrad_ctx *ctx, const void *rays, int64_t n, const vrad_trace_op
 
 }  // namespace
 
+int32_t vrad_fail(vrad_ctx *ctx, int32_t code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    return fail(ctx, code, "%s", buf);
+}
+
+int32_t vrad_cuda_fail(vrad_ctx *ctx, cudaError_t e, const char *what) { return cuda_fail(ctx, e, what); }
+
 extern "C" {
 
 int32_t vrad_abi_version(void) { return VRAD_ABI_VERSION; }
@@ -223,6 +217,7 @@ int32_t vrad_destroy(vrad_ctx *ctx) {
         cudaSetDevice(ctx->device);
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         ctx->scene.release();
+        ctx->world.release();
         cudaFree(ctx->status);
         cudaFree(ctx->d_rays);
         cudaFree(ctx->d_out);

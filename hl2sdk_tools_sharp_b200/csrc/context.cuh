@@ -1,0 +1,33 @@
+// context.cuh -- the opaque vrad_ctx behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+
+#include "direct.cuh"
+#include "scene.cuh"
+
+struct vrad_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    vrad::SceneBuffers scene;
+    vrad::SceneBuildReport report;
+    bool has_scene = false;
+    uint32_t *status = nullptr;   // [0] traversal stack overflow flag (sticky)
+    // Staging for the host-buffer entry points, grown on demand.
+    void *d_rays = nullptr;
+    size_t d_rays_cap = 0;
+    void *d_out = nullptr;
+    size_t d_out_cap = 0;
+    vrad::WorldBuffers world;
+    std::string last_error;
+    std::string identity;
+};
+
+
+// Shared error reporting (abi.cu).
+int32_t vrad_fail(vrad_ctx *ctx, int32_t code, const char *fmt, ...);
+int32_t vrad_cuda_fail(vrad_ctx *ctx, cudaError_t e, const char *what);

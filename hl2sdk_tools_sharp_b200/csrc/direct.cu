@@ -1,0 +1,470 @@
+// direct.cu -- the fused direct-lighting gather: per luxel sample, every
+// light of its cluster's list in gather order, each shadow, sun and sky
+// segment traced in-thread, accumulated into the sample's LightingValue.
+//
+// Reference behaviour restated (muflub/hl2sdk_tools_sharp, MapTools/Rad/Light):
+//   FaceLightJob.ComputeIlluminationPointAndNormals (FaceLightJob.cs:237-320):
+//       the point is the sample position plus the face normal;
+//   FaceLightJob.EmitGroup / ResolveGroup (FaceLightJob.cs:329-460): lights in
+//       list order, fxdot = (mask ? dot : 0) * falloff, a light skipped when
+//       every lane of the four-sample group has fxdot 0, AddLight otherwise;
+//   DirectLightGatherer.GatherPointFour (:1308-1420), GatherStandardLane
+//       (:1169-1306, spotlights), EmitSkyLight / ResolveSkyLight (:536-640),
+//       AmbientSky (:642-815), Resolve's dot clamp (:441-478),
+//       InverseQuadratic (:1579).
+// Every float operation is an explicitly rounded intrinsic in the
+// reference's order, so a sample's result is the CPU's bits whenever the
+// rays answer as the CPU's do.  The four-sample group is four adjacent
+// lanes; its "every lane zero" tests are shuffles within the group.
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "context.cuh"
+#include "traverse.cuh"
+
+namespace vrad {
+
+namespace {
+
+constexpr float kMaxTraceLength = (float)(1.732050807569 * (2 * 16384));  // LightConstants.MaxTraceLength
+constexpr float kEqualEpsilon = 0.001f;                                   // LightConstants.EqualEpsilon
+
+enum : int { kSurface = 0, kPoint = 1, kSpot = 2, kSkyLight = 3, kSkyAmbient = 4 };
+
+__device__ __forceinline__ float maxps(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ float minps(float a, float b) { return a < b ? a : b; }
+
+// True when any lane of this lane's four-lane group has v set.
+__device__ __forceinline__ bool group_any(bool v, unsigned gmask) {
+    unsigned x = v ? 1u : 0u;
+    x |= __shfl_xor_sync(gmask, x, 1);
+    x |= __shfl_xor_sync(gmask, x, 2);
+    return x != 0;
+}
+
+// The segment start -> stop (LightRayLog.MakeRay: whole segment, reach 1).
+// Visibility blocks on any hit; a sky test blocks only when the first hit
+// is opaque.
+template <int MODE>
+__device__ __forceinline__ bool segment_blocked(const DeviceScene &sc, float sx, float sy, float sz,
+                                                float ex, float ey, float ez, int *stack,
+                                                uint32_t *overflow) {
+    const RayState r = make_ray(sx, sy, sz, __fsub_rn(ex, sx), __fsub_rn(ey, sy), __fsub_rn(ez, sz));
+    bool hit;
+    float t;
+    int32_t orig;
+    uint32_t meta;
+    trace_ray<MODE>(sc, r, 0.0f, 1.0f, -1, stack, overflow, hit, t, orig, meta);
+    return hit;
+}
+
+// QuinticInterpolatingPolynomial fade (GatherPointFour / GatherStandardLane).
+__device__ __forceinline__ float fade(float dist, float start, float span) {
+    float t = __fdiv_rn(__fsub_rn(dist, start), span);
+    t = minps(t, 1.0f);
+    t = maxps(t, 0.0f);
+    t = __fsub_rn(1.0f, t);
+    float mult = __fsub_rn(__fmul_rn(6.0f, t), 15.0f);
+    mult = __fadd_rn(__fmul_rn(mult, t), 10.0f);
+    mult = __fmul_rn(__fmul_rn(t, t), mult);
+    return __fmul_rn(t, mult);
+}
+
+// InverseQuadratic: ((d*d)*q + l*d) + c, then its reciprocal.
+__device__ __forceinline__ float inverse_quadratic(float d, float q, float l, float c) {
+    float f = __fmul_rn(d, d);
+    f = __fmul_rn(f, q);
+    f = __fadd_rn(f, __fmul_rn(l, d));
+    f = __fadd_rn(f, c);
+    return __fdiv_rn(1.0f, f);
+}
+
+__global__ void __launch_bounds__(kBlock) k_direct(DeviceScene sc, DeviceWorld w, float4 *__restrict__ out,
+                                                   unsigned long long *__restrict__ counters,
+                                                   uint32_t *__restrict__ overflow) {
+    __shared__ int stack_mem[kStackDepth * kBlock];
+    int *stack = stack_mem + threadIdx.x;
+    const int64_t slot = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+    if (slot >= w.nslots) return;
+    const int32_t code = __ldg(&w.slots[slot]);
+    if (code == -1) return;  // a whole empty group at the end
+    const int lane = threadIdx.x & 31;
+    const unsigned gmask = 0xFu << (lane & ~3);
+    const bool real = (code & 0x80000000) == 0;
+    const int32_t si = code & 0x7fffffff;
+
+    const float4 sp = __ldg(&w.sample_pos[si]);
+    const int face = __float_as_int(sp.w);
+    const float4 fn = __ldg(&w.face_normal[face]);
+    const int cluster = __float_as_int(fn.w);
+    const float nx = fn.x, ny = fn.y, nz = fn.z;
+    // One unit off the face (ComputeIlluminationPointAndNormals).
+    const float px = __fadd_rn(sp.x, nx), py = __fadd_rn(sp.y, ny), pz = __fadd_rn(sp.z, nz);
+
+    float ax = 0.0f, ay = 0.0f, az = 0.0f, sun = 0.0f;
+    unsigned long long vis_rays = 0, sky_rays = 0;
+
+    const int l0 = __ldg(&w.cl_off[cluster]), l1 = __ldg(&w.cl_off[cluster + 1]);
+    for (int k = l0; k < l1; k++) {
+        const int li = __ldg(&w.cl_list[k]);
+        const float4 *L = w.lights + kLightF4 * li;
+        const float4 A = __ldg(L), B = __ldg(L + 1), C = __ldg(L + 2), D = __ldg(L + 3), E = __ldg(L + 4);
+        const int type = __float_as_int(A.w);
+        float dot = 0.0f, falloff = 0.0f, sun_amount = 0.0f;
+
+        if (type == kPoint || type == kSpot) {
+            const bool hard = E.z > E.y;  // EndFadeDistance > StartFadeDistance
+            float dx = __fsub_rn(A.x, px), dy = __fsub_rn(A.y, py), dz = __fsub_rn(A.z, pz);
+            const float dist2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+            float dist = __fsqrt_rn(dist2);
+            const float rpc = __fdiv_rn(1.0f, dist);
+            dx = __fmul_rn(dx, rpc);
+            dy = __fmul_rn(dy, rpc);
+            dz = __fmul_rn(dz, rpc);
+            float d = __fadd_rn(__fadd_rn(__fmul_rn(dx, nx), __fmul_rn(dy, ny)), __fmul_rn(dz, nz));
+            d = maxps(0.0f, d);
+            bool live = !hard || dist <= E.z;
+            if (type == kPoint) {
+                // GatherPointFour.
+                dist = maxps(dist, 1.0f);
+                const float dd = minps(dist, E.w);
+                float f = inverse_quadratic(dd, E.x, D.w, D.z);
+                if (hard) f = __fmul_rn(fade(dist, E.y, __fsub_rn(E.z, E.y)), f);
+                dot = live ? d : 0.0f;
+                falloff = live ? f : 0.0f;
+            } else if (live) {
+                // GatherStandardLane, Spotlight.
+                dist = maxps(dist, 1.0f);
+                const float fed = minps(dist, E.w);
+                const float dot2 =
+                    -__fadd_rn(__fadd_rn(__fmul_rn(dx, C.x), __fmul_rn(dy, C.y)), __fmul_rn(dz, C.z));
+                if (dot2 > D.y) {
+                    float f = __fmul_rn(inverse_quadratic(fed, E.x, D.w, D.z), dot2);
+                    const bool fringe = dot2 <= D.x;
+                    float mult = __fdiv_rn(__fsub_rn(dot2, D.y), __fsub_rn(D.x, D.y));
+                    mult = minps(mult, 1.0f);
+                    mult = maxps(mult, 0.0f);
+                    if (C.w != 0.0f && C.w != 1.0f) mult = (float)pow((double)mult, (double)C.w);
+                    mult = fringe ? mult : 1.0f;
+                    f = __fmul_rn(mult, f);
+                    if (hard) f = __fmul_rn(fade(dist, E.y, __fsub_rn(E.z, E.y)), f);
+                    dot = d;
+                    falloff = f;
+                }
+            }
+            if (real && dot != 0.0f && falloff != 0.0f) {
+                vis_rays++;
+                if (segment_blocked<kModeAny>(sc, px, py, pz, A.x, A.y, A.z, stack, overflow)) dot = 0.0f;
+            }
+        } else if (type == kSkyLight) {
+            // EmitSkyLight / ResolveSkyLight.
+            float d = -__fadd_rn(__fadd_rn(__fmul_rn(nx, C.x), __fmul_rn(ny, C.y)), __fmul_rn(nz, C.z));
+            d = maxps(d, 0.0f);
+            if (group_any(d != 0.0f, gmask)) {
+                const int ns = w.sun_samples;
+                const float jitter_scale = (float)(1.732050807569 * (2 * 16384) * (double)w.sun_extent);
+                float total = 0.0f;
+                for (int s = 0; s < ns; s++) {
+                    float ex = __fmul_rn(C.x, -kMaxTraceLength), ey = __fmul_rn(C.y, -kMaxTraceLength),
+                          ez = __fmul_rn(C.z, -kMaxTraceLength);
+                    if (s != 0) {
+                        const float4 j = __ldg(&w.jitter[s - 1]);
+                        ex = __fadd_rn(ex, __fmul_rn(j.x, jitter_scale));
+                        ey = __fadd_rn(ey, __fmul_rn(j.y, jitter_scale));
+                        ez = __fadd_rn(ez, __fmul_rn(j.z, jitter_scale));
+                    }
+                    float frac = 1.0f;
+                    if (real) {
+                        sky_rays++;
+                        if (segment_blocked<kModeSkyPass>(sc, px, py, pz, __fadd_rn(ex, px), __fadd_rn(ey, py),
+                                                          __fadd_rn(ez, pz), stack, overflow))
+                            frac = 0.0f;
+                    }
+                    total = __fadd_rn(total, frac);
+                }
+                const float see = __fmul_rn(total, __fdiv_rn(1.0f, (float)ns));
+                dot = __fmul_rn(d, see);
+                falloff = 1.0f;
+                sun_amount = __fmul_rn(see, 10000.0f);
+            }
+        } else if (type == kSkyAmbient) {
+            // AmbientSky: every direction in front of the face, in order.
+            float sumdot = 0.0f, possible = 0.0f, ambient = 0.0f;
+            for (int di = 0; di < w.ndirs; di++) {
+                const float4 an = __ldg(&w.dirs[di]);
+                const float dd = -__fadd_rn(__fadd_rn(__fmul_rn(nx, an.x), __fmul_rn(ny, an.y)), __fmul_rn(nz, an.z));
+                const bool valid = dd > kEqualEpsilon;
+                const float dv = valid ? dd : 0.0f;
+                sumdot = __fadd_rn(dv, sumdot);
+                possible = __fadd_rn(valid ? 1.0f : 0.0f, possible);
+                float frac = 1.0f;
+                if (valid && real) {
+                    // surfacePos = points - anorm * -epsilon, epsilon 0;
+                    // stop = anorm * -MaxTraceLength + points.
+                    const float sx = __fsub_rn(px, __fmul_rn(an.x, -0.0f));
+                    const float sy = __fsub_rn(py, __fmul_rn(an.y, -0.0f));
+                    const float sz = __fsub_rn(pz, __fmul_rn(an.z, -0.0f));
+                    const float ex = __fadd_rn(__fmul_rn(an.x, -kMaxTraceLength), px);
+                    const float ey = __fadd_rn(__fmul_rn(an.y, -kMaxTraceLength), py);
+                    const float ez = __fadd_rn(__fmul_rn(an.z, -kMaxTraceLength), pz);
+                    sky_rays++;
+                    if (segment_blocked<kModeSkyPass>(sc, sx, sy, sz, ex, ey, ez, stack, overflow)) frac = 0.0f;
+                }
+                ambient = __fadd_rn(ambient, __fmul_rn(frac, dv));
+            }
+            const float factor = __fdiv_rn(possible, possible);
+            dot = __fdiv_rn(ambient, __fmul_rn(factor, sumdot));
+            falloff = 1.0f;
+        }
+        // Resolve: a light behind the face lights nothing.
+        dot = maxps(dot, 0.0f);
+        const float fx = __fmul_rn(real ? dot : 0.0f, falloff);
+        if (!group_any(fx != 0.0f, gmask)) continue;
+        if (real) {
+            ax = __fadd_rn(ax, __fmul_rn(fx, B.x));
+            ay = __fadd_rn(ay, __fmul_rn(fx, B.y));
+            az = __fadd_rn(az, __fmul_rn(fx, B.z));
+            sun = __fadd_rn(sun, sun_amount);
+        }
+    }
+    if (real) out[si] = make_float4(ax, ay, az, sun);
+
+    // Ray counts: one atomic per warp.
+    for (int o = 16; o > 0; o >>= 1) {
+        vis_rays += __shfl_xor_sync(__activemask(), vis_rays, o);
+        sky_rays += __shfl_xor_sync(__activemask(), sky_rays, o);
+    }
+    if (lane == (__ffs(__activemask()) - 1)) {
+        atomicAdd(&counters[0], vis_rays);
+        atomicAdd(&counters[1], sky_rays);
+    }
+}
+
+}  // namespace
+
+void WorldBuffers::release() {
+    cudaFree(slots);
+    cudaFree(sample_pos);
+    cudaFree(face_normal);
+    cudaFree(lights);
+    cudaFree(cl_off);
+    cudaFree(cl_list);
+    cudaFree(dirs);
+    cudaFree(jitter);
+    cudaFree(counters);
+    slots = nullptr;
+    sample_pos = face_normal = lights = dirs = jitter = nullptr;
+    cl_off = cl_list = nullptr;
+    counters = nullptr;
+    view = DeviceWorld{};
+    ready = false;
+}
+
+cudaError_t launch_direct(const DeviceScene &scene, const DeviceWorld &world, float4 *out,
+                          unsigned long long *counters, uint32_t *overflow, cudaStream_t stream) {
+    if (world.nslots == 0) return cudaSuccess;
+    const int64_t grid = (world.nslots + kBlock - 1) / kBlock;
+    k_direct<<<(unsigned)grid, kBlock, 0, stream>>>(scene, world, out, counters, overflow);
+    return cudaGetLastError();
+}
+
+}  // namespace vrad
+
+namespace {
+
+template <class T>
+cudaError_t upload_vec(T **dst, const std::vector<T> &v) {
+    cudaError_t e = cudaMalloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
+    if (e == cudaSuccess && !v.empty())
+        e = cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+    return e;
+}
+
+}  // namespace
+
+extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
+    if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
+    if (!w || w->nfaces < 0 || w->nsamples < 0 || w->nlights < 0 || w->nclusters < 0 ||
+        (w->nfaces && !w->faces) || (w->nsamples && !w->samples) || (w->nlights && !w->lights) ||
+        !w->cluster_light_offsets || (w->nsky_directions && !w->sky_directions) ||
+        (w->nsun_jitter && !w->sun_jitter) || w->sun_samples < 1 || w->sun_samples - 1 > w->nsun_jitter)
+        return vrad_fail(ctx, VRAD_ERR_ARG, "invalid world description");
+    const int32_t nl = w->nlights;
+    for (int32_t l = 0; l < nl; l++) {
+        const int t = w->lights[l].type;
+        if (t == 0)
+            return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "surface lights are not supported by this build");
+        if (t < 1 || t > 4) return vrad_fail(ctx, VRAD_ERR_ARG, "light %d has type %d", l, t);
+    }
+    const int32_t total = w->cluster_light_offsets[w->nclusters];
+    for (int32_t c = 0; c < w->nclusters; c++)
+        if (w->cluster_light_offsets[c] > w->cluster_light_offsets[c + 1])
+            return vrad_fail(ctx, VRAD_ERR_ARG, "cluster light offsets decrease at %d", c);
+    for (int32_t k = 0; k < total; k++)
+        if (w->cluster_lights[k] < 0 || w->cluster_lights[k] >= nl)
+            return vrad_fail(ctx, VRAD_ERR_ARG, "cluster light list names light %d", w->cluster_lights[k]);
+
+    // Slots: each face's samples padded to whole groups of four.
+    std::vector<int32_t> slots;
+    slots.reserve((size_t)(w->nsamples + 4 * (int64_t)w->nfaces));
+    std::vector<float4> pos((size_t)w->nsamples);
+    int64_t i = 0;
+    while (i < w->nsamples) {
+        const int32_t face = w->samples[i].face;
+        if (face < 0 || face >= w->nfaces) return vrad_fail(ctx, VRAD_ERR_ARG, "sample %lld names face %d", (long long)i, face);
+        int64_t j = i;
+        while (j < w->nsamples && w->samples[j].face == face) j++;
+        const int32_t cl = w->faces[face].cluster;
+        if (cl < 0 || cl >= w->nclusters)
+            return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "face %d has cluster %d outside the light lists", face, cl);
+        for (int64_t g = i; g < j; g += 4) {
+            for (int l = 0; l < 4; l++) {
+                int64_t s = g + l;
+                slots.push_back(s < j ? (int32_t)s : (int32_t)((j - 1) | 0x80000000LL));
+            }
+        }
+        for (int64_t s = i; s < j; s++) {
+            if (w->samples[s].cluster != cl)
+                return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED,
+                                 "sample %lld is in cluster %d, its face in %d: mixed-cluster groups are not supported",
+                                 (long long)s, w->samples[s].cluster, cl);
+            const vrad_sample &sm = w->samples[s];
+            float4 p;
+            p.x = sm.position[0];
+            p.y = sm.position[1];
+            p.z = sm.position[2];
+            int32_t f = face;
+            memcpy(&p.w, &f, 4);
+            pos[(size_t)s] = p;
+        }
+        i = j;
+    }
+    while (slots.size() % 32) slots.push_back(-1);
+    std::vector<float4> fnorm((size_t)w->nfaces);
+    for (int32_t f = 0; f < w->nfaces; f++) {
+        float4 v;
+        v.x = w->faces[f].normal[0];
+        v.y = w->faces[f].normal[1];
+        v.z = w->faces[f].normal[2];
+        int32_t c = w->faces[f].cluster;
+        memcpy(&v.w, &c, 4);
+        fnorm[(size_t)f] = v;
+    }
+    std::vector<float4> lights((size_t)nl * vrad::kLightF4);
+    for (int32_t l = 0; l < nl; l++) {
+        const vrad_light &s = w->lights[l];
+        float4 *o = &lights[(size_t)l * vrad::kLightF4];
+        int32_t type = s.type, style = s.style;
+        o[0] = make_float4(s.origin[0], s.origin[1], s.origin[2], 0.0f);
+        memcpy(&o[0].w, &type, 4);
+        o[1] = make_float4(s.intensity[0], s.intensity[1], s.intensity[2], 0.0f);
+        memcpy(&o[1].w, &style, 4);
+        o[2] = make_float4(s.normal[0], s.normal[1], s.normal[2], s.exponent);
+        o[3] = make_float4(s.stop_dot, s.stop_dot2, s.constant_attn, s.linear_attn);
+        o[4] = make_float4(s.quadratic_attn, s.start_fade_distance, s.end_fade_distance, s.cap_dist);
+    }
+    std::vector<int32_t> cl_off(w->cluster_light_offsets, w->cluster_light_offsets + w->nclusters + 1);
+    std::vector<int32_t> cl_list(w->cluster_lights, w->cluster_lights + total);
+    std::vector<float4> dirs((size_t)w->nsky_directions), jit((size_t)w->nsun_jitter);
+    for (int32_t d = 0; d < w->nsky_directions; d++)
+        dirs[(size_t)d] = make_float4(w->sky_directions[3 * d], w->sky_directions[3 * d + 1], w->sky_directions[3 * d + 2], 0.0f);
+    for (int32_t d = 0; d < w->nsun_jitter; d++)
+        jit[(size_t)d] = make_float4(w->sun_jitter[3 * d], w->sun_jitter[3 * d + 1], w->sun_jitter[3 * d + 2], 0.0f);
+
+    std::lock_guard<std::mutex> g(ctx->mu);
+    cudaError_t e = cudaSetDevice(ctx->device);
+    vrad::WorldBuffers &wb = ctx->world;
+    wb.release();
+    if (e == cudaSuccess) e = upload_vec(&wb.slots, slots);
+    if (e == cudaSuccess) e = upload_vec(&wb.sample_pos, pos);
+    if (e == cudaSuccess) e = upload_vec(&wb.face_normal, fnorm);
+    if (e == cudaSuccess) e = upload_vec(&wb.lights, lights);
+    if (e == cudaSuccess) e = upload_vec(&wb.cl_off, cl_off);
+    if (e == cudaSuccess) e = upload_vec(&wb.cl_list, cl_list);
+    if (e == cudaSuccess) e = upload_vec(&wb.dirs, dirs);
+    if (e == cudaSuccess) e = upload_vec(&wb.jitter, jit);
+    if (e == cudaSuccess) e = cudaMalloc(&wb.counters, 2 * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        wb.release();
+        return vrad_cuda_fail(ctx, e, "world upload");
+    }
+    wb.view = vrad::DeviceWorld{wb.slots, (int64_t)slots.size(), wb.sample_pos, wb.face_normal, wb.lights, nl,
+                                wb.cl_off, wb.cl_list, w->nclusters, wb.dirs, w->nsky_directions, wb.jitter,
+                                w->nsun_jitter, w->sun_angular_extent, w->sun_samples, w->nsamples};
+    wb.ready = true;
+    return VRAD_OK;
+}
+
+namespace {
+
+int32_t direct_on(vrad_ctx *ctx, float4 *d_out, cudaStream_t s) {
+    if (!ctx->has_scene) return vrad_fail(ctx, VRAD_ERR_NO_SCENE, "no scene uploaded");
+    if (!ctx->world.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no lighting world uploaded");
+    cudaError_t e = cudaMemsetAsync(ctx->world.counters, 0, 2 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess)
+        e = vrad::launch_direct(ctx->scene.view(), ctx->world.view, d_out, ctx->world.counters, ctx->status, s);
+    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "direct lighting launch");
+    return VRAD_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t vrad_direct_lighting_device(vrad_ctx *ctx, vrad_lighting_value *d_out, void *stream) {
+    if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
+    if (!d_out && ctx->world.view.nsamples) return vrad_fail(ctx, VRAD_ERR_ARG, "null output");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
+    return direct_on(ctx, reinterpret_cast<float4 *>(d_out), (cudaStream_t)stream);
+}
+
+extern "C" int32_t vrad_direct_lighting(vrad_ctx *ctx, vrad_lighting_value *out, vrad_direct_stats *stats) {
+    if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    const int64_t n = ctx->world.view.nsamples;
+    if (n && !out) return vrad_fail(ctx, VRAD_ERR_ARG, "null output");
+    cudaError_t e = cudaSetDevice(ctx->device);
+    float4 *d_out = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(float4) * (size_t)(n ? n : 1));
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    if (e == cudaSuccess) e = cudaEventRecord(a, ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(d_out);
+        if (a) cudaEventDestroy(a);
+        return vrad_cuda_fail(ctx, e, "direct lighting set-up");
+    }
+    int32_t rc = direct_on(ctx, d_out, ctx->stream);
+    unsigned long long counts[2] = {0, 0};
+    uint32_t overflow = 0;
+    if (rc == VRAD_OK) {
+        e = cudaEventRecord(b, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(out, d_out, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(counts, ctx->world.counters, sizeof counts, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&overflow, ctx->status, sizeof overflow, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = vrad_cuda_fail(ctx, e, "direct lighting");
+    }
+    if (rc == VRAD_OK && overflow) {
+        cudaMemset(ctx->status, 0, sizeof(uint32_t));
+        rc = vrad_fail(ctx, VRAD_ERR_CUDA, "traversal stack overflow (BVH deeper than %d)", vrad::kStackDepth);
+    }
+    if (rc == VRAD_OK && stats) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, a, b);
+        stats->samples = n;
+        stats->visibility_rays = (int64_t)counts[0];
+        stats->sky_rays = (int64_t)counts[1];
+        stats->kernel_ms = ms;
+    }
+    cudaFree(d_out);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return rc;
+}

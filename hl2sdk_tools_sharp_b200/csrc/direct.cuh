@@ -1,0 +1,69 @@
+// direct.cuh -- the lighting world resident on one device, and the fused
+// direct-gather launch.
+//
+// Layout in HBM:
+//   slots[k]        int32: sample index of thread k; bit 31 marks a padding
+//                   lane (a face's last group of four repeats its last
+//                   sample, as FaceLightJob.EmitGroup pads); -1 = no sample.
+//                   Each face's samples start on a multiple of four, so a
+//                   reference sample group is four adjacent lanes of a warp.
+//   sample_pos[i]   float4 (position xyz, face index bits)
+//   face_normal[f]  float4 (plane normal xyz, cluster bits)
+//   lights[l]       5 x float4, the DirectLight fields:
+//                   (origin, type) (intensity, style) (normal, exponent)
+//                   (stop_dot, stop_dot2, constant, linear)
+//                   (quadratic, start_fade, end_fade, cap_dist)
+//   cl_off, cl_list per-cluster light lists in gather order (CSR)
+//   dirs[d]         float4 sky-ambient directions; jitter[d] sun jitter
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "vrad_internal.cuh"
+
+namespace vrad {
+
+constexpr int kLightF4 = 5;
+
+struct DeviceWorld {
+    const int32_t *slots;
+    int64_t nslots;
+    const float4 *sample_pos;
+    const float4 *face_normal;
+    const float4 *lights;
+    int32_t nlights;
+    const int32_t *cl_off;
+    const int32_t *cl_list;
+    int32_t nclusters;
+    const float4 *dirs;
+    int32_t ndirs;
+    const float4 *jitter;
+    int32_t njitter;
+    float sun_extent;
+    int32_t sun_samples;
+    int64_t nsamples;
+};
+
+struct WorldBuffers {
+    int32_t *slots = nullptr;
+    float4 *sample_pos = nullptr;
+    float4 *face_normal = nullptr;
+    float4 *lights = nullptr;
+    int32_t *cl_off = nullptr;
+    int32_t *cl_list = nullptr;
+    float4 *dirs = nullptr;
+    float4 *jitter = nullptr;
+    unsigned long long *counters = nullptr;  // [0] visibility rays, [1] sky rays
+    DeviceWorld view{};
+    bool ready = false;
+
+    void release();
+};
+
+// Launches the fused gather: out[i] = (lighting xyz, direct sun amount).
+cudaError_t launch_direct(const DeviceScene &scene, const DeviceWorld &world, float4 *out,
+                          unsigned long long *counters, uint32_t *overflow, cudaStream_t stream);
+
+}  // namespace vrad

@@ -1,0 +1,258 @@
+// world.cpp -- host-side set-up of the lighting stage: each face's luxel
+// frame and its light samples, as the reference's RadWorld set-up builds
+// them before any ray is traced.
+//
+//   FaceLightInfo.Build        MapTools/Rad/Light/FaceLightInfo.cs:79-160
+//   FaceSampleBuilder          MapTools/Rad/Light/FaceSampleBuilder.cs:80-367
+//   WindingArena.ClipEpsilon / AreaAndBalancePoint / Bounds /
+//   RemoveColinearPoints       MapTools/Geometry/WindingArena.cs
+//
+// Plain single-precision host arithmetic in the reference's operation order
+// (built with -ffp-contract=off: no fused multiply-add), so sample positions
+// are the reference's bits.  This is set-up, not the hot path: the samples
+// are the input of the device kernels.
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../../include/vrad_cuda.h"
+
+namespace {
+
+struct V3 {
+    float x, y, z;
+};
+inline V3 add(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 mul(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+inline float dot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+inline float length(V3 a) { return std::sqrt((a.x * a.x + a.y * a.y) + a.z * a.z); }
+inline V3 normalise(V3 a) {
+    float l = length(a);
+    if (l == 0.0f) return {0.0f, 0.0f, 0.0f};
+    return {a.x / l, a.y / l, a.z / l};
+}
+
+constexpr float kLightmapOnEpsilon = 0.1f / 16.0f;  // LightConstants.LightmapOnEpsilon
+constexpr double kColinearDot = 0.999;              // GeometryEpsilons.ColinearDotThreshold
+constexpr double kDegenerateDet = 1.0e-20;          // FaceLightInfo.DegenerateDeterminant
+
+struct FaceFrame {
+    V3 normal;
+    float dist;
+    V3 w2l_s, w2l_t, l2w_s, l2w_t, origin;
+    int min_s, min_t, width, height;
+};
+
+// FaceLightInfo.Build (FaceLightInfo.cs:79-160), world model (origin 0).
+FaceFrame face_frame(const vrad_face &f) {
+    FaceFrame fr;
+    fr.normal = {f.normal[0], f.normal[1], f.normal[2]};
+    fr.dist = f.dist;
+    fr.w2l_s = {f.lightmap_vecs[0][0], f.lightmap_vecs[0][1], f.lightmap_vecs[0][2]};
+    fr.w2l_t = {f.lightmap_vecs[1][0], f.lightmap_vecs[1][1], f.lightmap_vecs[1][2]};
+    const float off_s = f.lightmap_vecs[0][3], off_t = f.lightmap_vecs[1][3];
+    const V3 s = fr.w2l_s, t = fr.w2l_t, n = fr.normal;
+    // The 2x2 minors, each written out as the reference pairs them.
+    V3 lsc = {t.y * s.z - t.z * s.y, t.z * s.x - t.x * s.z, t.x * s.y - t.y * s.x};
+    float det = -dot(n, lsc);
+    V3 origin{0.0f, 0.0f, 0.0f};
+    fr.l2w_s = {0.0f, 0.0f, 0.0f};
+    fr.l2w_t = {0.0f, 0.0f, 0.0f};
+    if (!(std::fabs((double)det) < kDegenerateDet)) {
+        fr.l2w_s = {(n.z * t.y - n.y * t.z) / det, (n.x * t.z - n.z * t.x) / det,
+                    (n.y * t.x - n.x * t.y) / det};
+        fr.l2w_t = {(n.y * s.z - n.z * s.y) / det, (n.z * s.x - n.x * s.z) / det,
+                    (n.x * s.y - n.y * s.x) / det};
+        origin = {-(f.dist * lsc.x) / det, -(f.dist * lsc.y) / det, -(f.dist * lsc.z) / det};
+        origin = add(origin, mul(fr.l2w_s, -off_s));
+        origin = add(origin, mul(fr.l2w_t, -off_t));
+    }
+    origin = add(origin, V3{0.0f, 0.0f, 0.0f});  // plus the (zero) model origin
+    fr.origin = origin;
+    fr.min_s = f.lightmap_mins[0];
+    fr.min_t = f.lightmap_mins[1];
+    fr.width = f.lightmap_size[0] + 1;
+    fr.height = f.lightmap_size[1] + 1;
+    return fr;
+}
+
+V3 luxel_to_world(const FaceFrame &fr, float s, float t) {
+    s += (float)fr.min_s;
+    t += (float)fr.min_t;
+    V3 pos = add(fr.origin, mul(fr.l2w_s, s));
+    return add(pos, mul(fr.l2w_t, t));
+}
+
+using Winding = std::vector<V3>;
+
+// WindingArena.RemoveColinearPoints.
+Winding remove_colinear(const Winding &w) {
+    const size_t n = w.size();
+    Winding kept;
+    for (size_t i = 0; i < n; i++) {
+        size_t j = (i + 1) % n, k = (i + n - 1) % n;
+        V3 v1 = normalise(sub(w[j], w[i]));
+        V3 v2 = normalise(sub(w[i], w[k]));
+        if ((double)dot(v1, v2) < kColinearDot) kept.push_back(w[i]);
+    }
+    return kept.size() == n ? w : kept;
+}
+
+// WindingArena.ClipEpsilon against an axis plane (normal = unit axis `ax`).
+// front: dot > dist + eps side, back: the rest.  Empty vector = null.
+void clip_axis(const Winding &in, int ax, float dist, float eps, Winding &front, Winding &back) {
+    front.clear();
+    back.clear();
+    const size_t n = in.size();
+    std::vector<float> dists(n + 1);
+    std::vector<int> sides(n + 1);  // 0 front, 1 back, 2 on
+    int counts[3] = {0, 0, 0};
+    const V3 normal = {ax == 0 ? 1.0f : 0.0f, ax == 1 ? 1.0f : 0.0f, 0.0f};
+    for (size_t i = 0; i < n; i++) {
+        float d = dot(in[i], normal);
+        d -= dist;
+        dists[i] = d;
+        sides[i] = d > eps ? 0 : (d < -eps ? 1 : 2);
+        counts[sides[i]]++;
+    }
+    sides[n] = sides[0];
+    dists[n] = dists[0];
+    if (counts[0] == 0) {
+        back = in;
+        return;
+    }
+    if (counts[1] == 0) {
+        front = in;
+        return;
+    }
+    for (size_t i = 0; i < n; i++) {
+        const V3 p1 = in[i];
+        if (sides[i] == 2) {
+            front.push_back(p1);
+            back.push_back(p1);
+            continue;
+        }
+        if (sides[i] == 0) front.push_back(p1);
+        if (sides[i] == 1) back.push_back(p1);
+        if (sides[i + 1] == 2 || sides[i + 1] == sides[i]) continue;
+        const V3 p2 = in[(i + 1) % n];
+        const float t = dists[i] / (dists[i] - dists[i + 1]);
+        auto axis = [&](float nv, float a, float b) {
+            if (nv == 1.0f) return dist;
+            if (nv == -1.0f) return -dist;
+            return a + t * (b - a);
+        };
+        V3 mid = {axis(normal.x, p1.x, p2.x), axis(normal.y, p1.y, p2.y), axis(normal.z, p1.z, p2.z)};
+        front.push_back(mid);
+        back.push_back(mid);
+    }
+}
+
+// WindingArena.AreaAndBalancePoint.
+float area_and_balance(const Winding &p, V3 &center) {
+    center = {0.0f, 0.0f, 0.0f};
+    float total = 0.0f;
+    for (size_t i = 2; i < p.size(); i++) {
+        V3 d1 = sub(p[i - 1], p[0]);
+        V3 d2 = sub(p[i], p[0]);
+        float area = length(cross(d1, d2));
+        total += area;
+        float third = (float)((double)area / 3.0);
+        center = add(center, mul(p[i - 1], third));
+        center = add(center, mul(p[i], third));
+        center = add(center, mul(p[0], third));
+    }
+    if (total != 0.0f) center = mul(center, (float)(1.0 / (double)total));
+    return total * 0.5f;
+}
+
+float world_area_per_luxel(const vrad_face &f) {
+    const float *a = f.lightmap_vecs[0], *b = f.lightmap_vecs[1];
+    float ss = (a[0] * a[0] + a[1] * a[1]) + a[2] * a[2];
+    float tt = (b[0] * b[0] + b[1] * b[1]) + b[2] * b[2];
+    float product = std::sqrt(ss) * std::sqrt(tt);
+    return (float)(1.0 / (double)product);
+}
+
+}  // namespace
+
+extern "C" int32_t vrad_build_samples(const vrad_face *faces, int32_t nfaces, const float *vertices,
+                                      int64_t nvertices, vrad_sample *out, int64_t capacity,
+                                      int64_t *count, int64_t *face_first) {
+    if (nfaces < 0 || (nfaces > 0 && (!faces || !vertices)) || !count) return VRAD_ERR_ARG;
+    int64_t written = 0;
+    Winding cell_front, cell_back, row_front, row_back;
+    for (int32_t fi = 0; fi < nfaces; fi++) {
+        const vrad_face &f = faces[fi];
+        if (face_first) face_first[fi] = written;
+        if (f.num_vertices < 3 || f.first_vertex < 0 || f.first_vertex + (int64_t)f.num_vertices > nvertices)
+            return VRAD_ERR_ARG;
+        const FaceFrame fr = face_frame(f);
+        const float area_per_luxel = world_area_per_luxel(f);
+        // LightmapCoordWinding: the face's winding in luxel space.
+        Winding w;
+        for (int32_t k = 0; k < f.num_vertices; k++) {
+            const float *v = vertices + 3 * (int64_t)(f.first_vertex + k);
+            w.push_back(add(V3{v[0], v[1], v[2]}, V3{0.0f, 0.0f, 0.0f}));
+        }
+        w = remove_colinear(w);
+        for (V3 &p : w) {
+            V3 pos = sub(p, fr.origin);
+            p = {dot(pos, fr.w2l_s) - (float)fr.min_s, dot(pos, fr.w2l_t) - (float)fr.min_t, 0.0f};
+        }
+        // BuildFacesamples: rows by t, cells by s, sample offset 1.0.
+        Winding lm = w;
+        for (int t = 0; t < fr.height && !lm.empty(); t++) {
+            clip_axis(lm, 1, (float)t + 1.0f, kLightmapOnEpsilon, row_front, row_back);
+            Winding row = row_back;
+            for (int s = 0; s < fr.width && !row.empty(); s++) {
+                clip_axis(row, 0, (float)s + 1.0f, kLightmapOnEpsilon, cell_front, cell_back);
+                if (!cell_back.empty()) {
+                    if (written >= capacity) {
+                        *count = written;
+                        return out ? VRAD_ERR_ARG : VRAD_OK;  // out == NULL: a counting pass
+                    }
+                    V3 center;
+                    float area = area_and_balance(cell_back, center) * area_per_luxel;
+                    float mn[2] = {99999.0f, 99999.0f}, mx[2] = {-99999.0f, -99999.0f};
+                    for (const V3 &p : cell_back) {
+                        if (p.x < mn[0]) mn[0] = p.x;
+                        if (p.x > mx[0]) mx[0] = p.x;
+                        if (p.y < mn[1]) mn[1] = p.y;
+                        if (p.y > mx[1]) mx[1] = p.y;
+                    }
+                    if (out) {
+                        vrad_sample &o = out[written];
+                        V3 pos = luxel_to_world(fr, center.x, center.y);
+                        o.position[0] = pos.x;
+                        o.position[1] = pos.y;
+                        o.position[2] = pos.z;
+                        o.area = area;
+                        o.coord[0] = center.x;
+                        o.coord[1] = center.y;
+                        o.mins[0] = mn[0];
+                        o.mins[1] = mn[1];
+                        o.maxs[0] = mx[0];
+                        o.maxs[1] = mx[1];
+                        o.s = s;
+                        o.t = t;
+                        o.face = fi;
+                        o.cluster = f.cluster;
+                    }
+                    written++;
+                }
+                row = cell_front;
+            }
+            lm = row_front;
+        }
+    }
+    if (face_first) face_first[nfaces] = written;
+    *count = written;
+    return VRAD_OK;
+}

@@ -1,0 +1,307 @@
+"""Host side of vrad's lighting stage over libvrad_cuda.
+
+Builds what the reference's RadWorld set-up builds before any ray is traced
+(muflub/hl2sdk_tools_sharp, src/SourceSharp.MapTools/Rad/Light), from a
+room-grid World:
+
+  faces      vrad_face records (plane, texinfo lightmap vectors, lightmap
+             extents, winding, cluster); the inputs of FaceLightInfo.Build
+  samples    vrad_build_samples (native): FaceSampleBuilder.CalcPoints
+  lights     the DirectLight list in gather order (DirectLightBuilder.Build,
+             DirectLightBuilder.cs:43-505): ParseIntensity's gamma and
+             brightness (MapFormats/Text/RadLightFile.cs:344-410), literal
+             attenuation and its normalisation (LightFalloff.cs:40-90), spot
+             cones as cosines, the light_environment's sun and its ambient
+             partner; the active list is built by prepending, so it holds the
+             entities in reverse order
+  clusters   per cluster, the lights whose PVS reaches it, in list order
+             (DirectLightGatherer's per-cluster lists)
+
+and runs the fused direct gather on the device (vrad_direct_lighting).
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import math
+
+import numpy as np
+
+from . import tracer as T
+from .roomgrid import World
+from .workload import ambient_directions
+
+FACE_DTYPE = np.dtype([
+    ("normal", "<f4", (3,)), ("dist", "<f4"), ("lightmap_vecs", "<f4", (2, 4)),
+    ("lightmap_mins", "<i4", (2,)), ("lightmap_size", "<i4", (2,)), ("first_vertex", "<i4"),
+    ("num_vertices", "<i4"), ("cluster", "<i4"), ("flags", "<i4"),
+])
+SAMPLE_DTYPE = np.dtype([
+    ("position", "<f4", (3,)), ("area", "<f4"), ("coord", "<f4", (2,)), ("mins", "<f4", (2,)),
+    ("maxs", "<f4", (2,)), ("s", "<i4"), ("t", "<i4"), ("face", "<i4"), ("cluster", "<i4"),
+])
+LIGHT_DTYPE = np.dtype([
+    ("type", "<i4"), ("style", "<i4"), ("origin", "<f4", (3,)), ("intensity", "<f4", (3,)),
+    ("normal", "<f4", (3,)), ("stop_dot", "<f4"), ("stop_dot2", "<f4"), ("exponent", "<f4"),
+    ("constant_attn", "<f4"), ("linear_attn", "<f4"), ("quadratic_attn", "<f4"),
+    ("start_fade_distance", "<f4"), ("end_fade_distance", "<f4"), ("cap_dist", "<f4"),
+])
+LIGHTING_DTYPE = np.dtype([("lighting", "<f4", (3,)), ("direct_sun_amount", "<f4")])
+assert FACE_DTYPE.itemsize == 80 and SAMPLE_DTYPE.itemsize == 56 and LIGHT_DTYPE.itemsize == 80
+
+EMIT_POINT, EMIT_SPOT, EMIT_SKY, EMIT_AMBIENT = 1, 2, 3, 4
+EQUAL_EPSILON = np.float32(0.001)
+
+
+class _WorldDesc(ctypes.Structure):
+    _fields_ = [("faces", ctypes.c_void_p), ("nfaces", ctypes.c_int32),
+                ("samples", ctypes.c_void_p), ("nsamples", ctypes.c_int64),
+                ("lights", ctypes.c_void_p), ("nlights", ctypes.c_int32),
+                ("cluster_light_offsets", ctypes.c_void_p), ("cluster_lights", ctypes.c_void_p),
+                ("nclusters", ctypes.c_int32), ("sky_directions", ctypes.c_void_p),
+                ("nsky_directions", ctypes.c_int32), ("sun_jitter", ctypes.c_void_p),
+                ("nsun_jitter", ctypes.c_int32), ("sun_angular_extent", ctypes.c_float),
+                ("sun_samples", ctypes.c_int32)]
+
+
+class DirectStats(ctypes.Structure):
+    _fields_ = [("samples", ctypes.c_int64), ("visibility_rays", ctypes.c_int64),
+                ("sky_rays", ctypes.c_int64), ("kernel_ms", ctypes.c_float)]
+
+
+def _lib():
+    lib = T.load_library()
+    if not getattr(lib, "_lighting_bound", False):
+        P, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+        lib.vrad_build_samples.argtypes = [P, i32, P, i64, P, i64, ctypes.POINTER(i64), P]
+        lib.vrad_build_samples.restype = i32
+        lib.vrad_world_upload.argtypes = [P, ctypes.POINTER(_WorldDesc)]
+        lib.vrad_world_upload.restype = i32
+        lib.vrad_direct_lighting.argtypes = [P, P, ctypes.POINTER(DirectStats)]
+        lib.vrad_direct_lighting.restype = i32
+        lib.vrad_direct_lighting_device.argtypes = [P, P, P]
+        lib.vrad_direct_lighting_device.restype = i32
+        lib._lighting_bound = True
+    return lib
+
+
+# ---------------------------------------------------------------- faces
+
+def faces_of(world: World):
+    """vrad_face records and the shared vertex array."""
+    nf = world.face_count
+    faces = np.zeros(nf, FACE_DTYPE)
+    counts = np.array([len(v) for v in world.face_verts], np.int32)
+    first = np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.int32)
+    faces["normal"] = world.face_normal
+    faces["dist"] = world.face_dist
+    faces["lightmap_vecs"][:, 0] = world.face_s
+    faces["lightmap_vecs"][:, 1] = world.face_t
+    faces["lightmap_mins"] = world.face_mins
+    faces["lightmap_size"] = world.face_extents
+    faces["first_vertex"] = first
+    faces["num_vertices"] = counts
+    faces["cluster"] = world.face_cluster
+    verts = np.concatenate(world.face_verts).astype(np.float32)
+    return faces, verts
+
+
+def build_samples(faces: np.ndarray, verts: np.ndarray):
+    """FaceSampleBuilder.CalcPoints for every face (native); returns the
+    samples and face_first (index of each face's first sample)."""
+    lib = _lib()
+    faces = np.ascontiguousarray(faces, FACE_DTYPE)
+    verts = np.ascontiguousarray(verts, np.float32)
+    count = ctypes.c_int64()
+    rc = lib.vrad_build_samples(faces.ctypes.data, len(faces), verts.ctypes.data, len(verts), None,
+                                1 << 62, ctypes.byref(count), None)
+    if rc != 0:
+        raise ValueError(f"vrad_build_samples failed ({rc})")
+    out = np.zeros(count.value, SAMPLE_DTYPE)
+    first = np.zeros(len(faces) + 1, np.int64)
+    rc = lib.vrad_build_samples(faces.ctypes.data, len(faces), verts.ctypes.data, len(verts),
+                                out.ctypes.data, len(out), ctypes.byref(count), first.ctypes.data)
+    if rc != 0:
+        raise ValueError(f"vrad_build_samples failed ({rc})")
+    return out, first
+
+
+# ---------------------------------------------------------------- lights
+
+def parse_intensity(color, light_scale: float = 1.0) -> np.ndarray:
+    """RadLightFile.ParseIntensity for a four-field "_light" (r g b
+    brightness): gamma 2.2 in double, narrowed to float, times
+    (float)(brightness / 255)."""
+    r, g, b, scaler = (float(c) for c in color)
+    if r < 0 or g < 0 or b < 0 or scaler < 0:
+        return np.zeros(3, np.float32)
+    x = np.float32(math.pow(r / 255.0, 2.2) * 255)
+    y = np.float32(math.pow(g / 255.0, 2.2) * 255)
+    z = np.float32(math.pow(b / 255.0, 2.2) * 255)
+    v = np.array([x, y, z], np.float32) * np.float32(scaler / 255.0)
+    return (v * np.float32(light_scale)).astype(np.float32)
+
+
+def _normalise(v) -> np.ndarray:
+    """Vec3.Normalise: sqrt((x*x + y*y) + z*z) in float, three divides."""
+    v = np.asarray(v, np.float32)
+    ln = np.float32(math.sqrt(float(np.float32(np.float32(v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]))))
+    if ln == 0:
+        return np.zeros(3, np.float32)
+    return np.array([v[0] / ln, v[1] / ln, v[2] / ln], np.float32)
+
+
+def _cone_cos(deg: float) -> np.float32:
+    """DetMath.CosToSingle(LightNormals.Radians(deg)): (deg / 180) in float,
+    times pi in double, cosine rounded to float."""
+    rad = float(np.float32(np.float32(deg) / np.float32(180))) * math.pi
+    return np.float32(math.cos(rad))
+
+
+def _literal_falloff(light, attn) -> None:
+    """LightFalloff.ApplyLiteralCoefficients (no _fifty_percent_distance)."""
+    c, l, q = (np.float32(a) for a in attn)
+    c = np.float32(0) if c < EQUAL_EPSILON else c
+    l = np.float32(0) if l < EQUAL_EPSILON else l
+    q = np.float32(0) if q < EQUAL_EPSILON else q
+    if c < EQUAL_EPSILON and l < EQUAL_EPSILON and q < EQUAL_EPSILON:
+        c = np.float32(1)
+    ratio = np.float32(np.float32(c + np.float32(100.0) * l) + np.float32(np.float32(100.0) * np.float32(100.0)) * q)
+    light["constant_attn"], light["linear_attn"], light["quadratic_attn"] = c, l, q
+    light["start_fade_distance"] = 0.0
+    light["end_fade_distance"] = -1.0
+    light["cap_dist"] = np.float32(1.0e22)
+    if ratio > 0:
+        light["intensity"] = (light["intensity"] * ratio).astype(np.float32)
+
+
+def build_lights(world: World):
+    """The active DirectLight list and the per-cluster light lists.
+
+    Entity order: the light_environment, then each light / light_spot.
+    Returns (lights, cluster_offsets, cluster_lights)."""
+    entities = []
+    for l in range(len(world.light_origin)):
+        e = np.zeros((), LIGHT_DTYPE)
+        e["type"] = EMIT_SPOT if world.light_type[l] == 2 else EMIT_POINT
+        e["origin"] = world.light_origin[l]
+        e["intensity"] = parse_intensity(world.light_color[l])
+        if world.light_type[l] == 2:
+            e["normal"] = _normalise(np.asarray(world.light_target[l], np.float32) - world.light_origin[l])
+            inner, outer, expo = (float(x) for x in world.light_cone[l])
+            sd = inner if inner != 0 else 10.0
+            sd2 = outer if outer != 0 else sd
+            sd2 = max(sd2, sd)
+            sd, sd2 = min(sd, 90.0), min(sd2, 90.0)
+            e["stop_dot2"] = _cone_cos(sd2)
+            e["stop_dot"] = _cone_cos(sd)
+            e["exponent"] = expo
+        _literal_falloff(e, world.light_attn[l])
+        entities.append((e, int(world.light_cluster[l])))
+    # light_environment at the origin, aimed at its target.
+    sun = np.zeros((), LIGHT_DTYPE)
+    sun["type"] = EMIT_SKY
+    sun["intensity"] = parse_intensity(world.sun_color)
+    sun["normal"] = _normalise(world.sun_target)
+    sun["cap_dist"] = np.float32(1.0e22)
+    sun["end_fade_distance"] = -1.0
+    amb = np.zeros((), LIGHT_DTYPE)
+    amb["type"] = EMIT_AMBIENT
+    amb["intensity"] = parse_intensity(world.ambient_color)
+    amb["cap_dist"] = np.float32(1.0e22)
+    amb["end_fade_distance"] = -1.0
+    # Active list: prepend in entity order (environment first: sun, then
+    # ambient), then each light.
+    active = [(sun, -1), ]
+    active.insert(0, (amb, -1))
+    for e in entities:
+        active.insert(0, e)
+    lights = np.stack([a for a, _ in active]).astype(LIGHT_DTYPE)
+    home = [c for _, c in active]
+    C = world.pvs.shape[0]
+    lists = []
+    for c in range(C):
+        # Sun and ambient reach every cluster that sees sky: every room here.
+        lists.append([k for k, h in enumerate(home) if h < 0 or world.pvs[h, c]])
+    offsets = np.zeros(C + 1, np.int32)
+    offsets[1:] = np.cumsum([len(x) for x in lists])
+    flat = np.array([k for x in lists for k in x], np.int32)
+    return lights, offsets, flat
+
+
+# ---------------------------------------------------------------- stage
+
+@dataclasses.dataclass
+class LightingInputs:
+    faces: np.ndarray
+    verts: np.ndarray
+    samples: np.ndarray
+    face_first: np.ndarray
+    lights: np.ndarray
+    cluster_offsets: np.ndarray
+    cluster_lights: np.ndarray
+    sky_directions: np.ndarray
+    sun_jitter: np.ndarray
+    sun_samples: int = 1
+    sun_angular_extent: float = 0.0
+
+
+def prepare(world: World) -> LightingInputs:
+    faces, verts = faces_of(world)
+    samples, first = build_samples(faces, verts)
+    lights, off, flat = build_lights(world)
+    return LightingInputs(faces, verts, samples, first, lights, off, flat,
+                          ambient_directions().astype(np.float32), np.zeros((0, 3), np.float32))
+
+
+class LightingStage:
+    """The lighting stage of one map on one device: the shadow casters and
+    the lighting world resident, the direct gather on demand."""
+
+    def __init__(self, world: World, inputs: LightingInputs | None = None, device: int = 0):
+        self.inputs = inputs if inputs is not None else prepare(world)
+        self.tracer = T.CudaRayTracer(T.make_triangles(world.tri_verts, world.tri_ids), device=device)
+        self._ctx = self.tracer._ctx
+        self.upload_world(self.inputs)
+
+    def upload_world(self, i: LightingInputs) -> None:
+        """vrad_world_upload: faces, samples, lights, cluster lists, tables."""
+        keep = [np.ascontiguousarray(a) for a in (i.faces, i.samples, i.lights, i.cluster_offsets,
+                                                  i.cluster_lights, i.sky_directions, i.sun_jitter)]
+        f, s, l, off, cl, dirs, jit = keep
+        d = _WorldDesc(f.ctypes.data, len(f), s.ctypes.data, len(s), l.ctypes.data, len(l),
+                       off.ctypes.data, cl.ctypes.data, len(off) - 1, dirs.ctypes.data, len(dirs),
+                       jit.ctypes.data if len(jit) else None, len(jit), i.sun_angular_extent, i.sun_samples)
+        T._check(_lib().vrad_world_upload(self._ctx, ctypes.byref(d)), self._ctx)
+        self.inputs = i
+
+    def close(self):
+        self.tracer.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def direct(self):
+        """Every sample's LightingValue (style 0), and the kernel's stats."""
+        out = np.zeros(len(self.inputs.samples), LIGHTING_DTYPE)
+        st = DirectStats()
+        T._check(_lib().vrad_direct_lighting(self._ctx, out.ctypes.data, ctypes.byref(st)), self._ctx)
+        return out, st
+
+    def direct_into(self, out: np.ndarray):
+        """vrad_direct_lighting into a caller's host buffer (LIGHTING_DTYPE)."""
+        st = DirectStats()
+        T._check(_lib().vrad_direct_lighting(self._ctx, out.ctypes.data, ctypes.byref(st)), self._ctx)
+        return st
+
+    def direct_device(self, d_out, stream=None):
+        """Into a CUDA tensor of nsamples * 16 bytes, on `stream` (default:
+        torch's current stream)."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        T._check(_lib().vrad_direct_lighting_device(self._ctx, d_out.data_ptr(), ctypes.c_void_p(s)),
+                 self._ctx)
+        return d_out

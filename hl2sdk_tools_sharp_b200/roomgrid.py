@@ -13,7 +13,9 @@ generator returns is what vrad's lighting stage reads from a compiled BSP:
   lightmapVecs at the map's luxel scale) and lightmap extents, split so no
   face's lightmap exceeds 32 luxels per axis (vbsp's maximum lightmap
   dimension), a material reflectivity, and the room (cluster) it lies in;
-* lights (point and spot) placed inside rooms, a sun and a sky;
+* lights as the entity keys vrad reads (light / light_spot with "_light",
+  attenuation, cone and target; a light_environment with "_light" and
+  "_ambient" aimed by a target), placed inside rooms;
 * a PVS with one cluster per room: a room sees itself and the rooms up to
   two steps away along its row or column (straight lines through doors).
 
@@ -84,15 +86,19 @@ class World:
     face_cluster: np.ndarray     # (F,) int32
     face_material: np.ndarray    # (F,) int32
     reflectivity: np.ndarray     # (M, 3) float32
-    light_type: np.ndarray       # (L,) int32: 1 point, 2 spot
+    light_type: np.ndarray       # (L,) int32: 1 point (light), 2 spot (light_spot)
     light_origin: np.ndarray     # (L, 3) float32
-    light_intensity: np.ndarray  # (L, 3) float32
-    light_normal: np.ndarray     # (L, 3) float32 (spot direction)
-    light_cone: np.ndarray       # (L, 3) float32 (inner deg, outer deg, exponent)
+    light_color: np.ndarray      # (L, 4) float64 "_light" r g b brightness
+    light_attn: np.ndarray       # (L, 3) float64 _constant_attn, _linear_attn, _quadratic_attn
+    light_target: np.ndarray     # (L, 3) float32 origin of the spot's target entity
+    light_normal: np.ndarray     # (L, 3) float32 unit spot direction (for workload culling)
+    light_cone: np.ndarray       # (L, 3) float32 _inner_cone, _cone (degrees), _exponent
     light_cluster: np.ndarray    # (L,) int32
     sun_direction: np.ndarray    # (3,) float32, from the sun towards the world
-    sun_intensity: np.ndarray    # (3,) float32
-    sky_intensity: np.ndarray    # (3,) float32
+    sun_target: np.ndarray       # (3,) float32 target point of the light_environment (origin 0)
+    sun_color: np.ndarray        # (4,) float64 "_light" of the light_environment
+    ambient_color: np.ndarray    # (4,) float64 "_ambient" of the light_environment
+    sky_intensity: np.ndarray    # (3,) float32 nonzero when the sky ambient is on
     pvs: np.ndarray              # (C, C) bool
 
     @property
@@ -337,19 +343,30 @@ def generate(cfg: Config) -> World:
     pos = np.zeros((L, 3), np.float32)
     pos[:, 0:2] = lo + rng.uniform(64.0, ROOM - 64.0, size=(L, 2))
     pos[:, 2] = rng.uniform(128.0, ROOM - 128.0, size=L)
-    inten = rng.uniform(cfg.intensity[0], cfg.intensity[1], size=(L, 1)) * rng.uniform(0.6, 1.0, size=(L, 3))
+    # "_light" r g b brightness: a warm-to-white colour, brightness in the
+    # configured range; Hammer's default falloff (_quadratic_attn 1).
+    color = np.zeros((L, 4))
+    color[:, 0:3] = np.round(rng.uniform(180.0, 255.0, size=(L, 3)))
+    color[:, 3] = np.round(rng.uniform(cfg.intensity[0], cfg.intensity[1], size=L))
+    attn = np.zeros((L, 3))
+    attn[:, 2] = 1.0
     ltype = np.where(rng.uniform(size=L) < cfg.spot_fraction, 2, 1).astype(np.int32)
     ldir = rng.normal(size=(L, 3))
     ldir[:, 2] = -np.abs(ldir[:, 2]) - 0.5
     ldir /= np.linalg.norm(ldir, axis=1, keepdims=True)
-    inner = rng.uniform(20.0, 45.0, size=L)
-    outer = inner + rng.uniform(5.0, 30.0, size=L)
+    target = (pos + 256.0 * ldir).astype(np.float32)
+    ldir = (target - pos) / np.linalg.norm(target - pos, axis=1, keepdims=True)
+    inner = np.round(rng.uniform(20.0, 45.0, size=L))
+    outer = inner + np.round(rng.uniform(5.0, 30.0, size=L))
     expo = rng.choice([0.0, 1.0, 2.0, 5.0], size=L)
 
-    # Sun: from high above at a seeded azimuth and 35-70 degrees elevation.
+    # Sun: from high above at a seeded azimuth and 35-70 degrees elevation,
+    # aimed by a target entity (light_environment at the origin).
     az = rng.uniform(0, 2 * np.pi)
     el = np.radians(rng.uniform(35.0, 70.0))
-    sun_dir = -np.array([np.cos(el) * np.cos(az), np.cos(el) * np.sin(az), np.sin(el)], np.float32)
+    sun_dir = -np.array([np.cos(el) * np.cos(az), np.cos(el) * np.sin(az), np.sin(el)])
+    sun_target = (sun_dir * 1000.0).astype(np.float32)
+    sun_dir = (sun_target / np.linalg.norm(sun_target)).astype(np.float32)
 
     # PVS: self, and two steps along the row or the column.
     C = R * R
@@ -377,12 +394,16 @@ def generate(cfg: Config) -> World:
         reflectivity=refl,
         light_type=ltype,
         light_origin=pos,
-        light_intensity=inten.astype(np.float32),
+        light_color=color,
+        light_attn=attn,
+        light_target=target,
         light_normal=ldir.astype(np.float32),
         light_cone=np.stack([inner, outer, expo], 1).astype(np.float32),
         light_cluster=room_of.astype(np.int32),
         sun_direction=sun_dir,
-        sun_intensity=np.array([255.0, 240.0, 200.0], np.float32),
-        sky_intensity=np.array([40.0, 60.0, 90.0], np.float32) if cfg.sky_ambient else np.zeros(3, np.float32),
+        sun_target=sun_target,
+        sun_color=np.array([255.0, 240.0, 200.0, 220.0]),
+        ambient_color=np.array([120.0, 150.0, 210.0, 60.0]) if cfg.sky_ambient else np.zeros(4),
+        sky_intensity=np.array([1.0, 1.0, 1.0], np.float32) if cfg.sky_ambient else np.zeros(3, np.float32),
         pvs=pvs,
     )

@@ -149,6 +149,124 @@ int32_t vrad_trace_closest_device(vrad_ctx *ctx, const vrad_ray *d_rays, int64_t
                                   const vrad_trace_options *opts, vrad_hit *d_hits,
                                   void *stream);
 
+/* ---- Lighting stage ------------------------------------------------------
+ *
+ * The direct-lighting gather of vrad's lighting stage (the reference's
+ * RadWorld.LightFacesAsync, MapTools/Rad/Light/RadWorld.Facelights.cs:194,
+ * FaceLightJob.EmitGroup / ResolveGroup, FaceLightJob.cs:329-460, and
+ * DirectLightGatherer, DirectLightGatherer.cs:405-1634), fused with its
+ * rays: one kernel computes every sample's light from every light in its
+ * cluster's list, tracing each shadow, sun and sky segment in-thread. */
+
+/* One lit face: the inputs of FaceLightInfo.Build (FaceLightInfo.cs:79-160).
+ * lightmap_vecs are the texinfo's lightmapVecsLuxelsPerWorldUnits rows (s,
+ * t), lightmap_mins / lightmap_size the face's LightmapTextureMinsInLuxels /
+ * LightmapTextureSizeInLuxels.  The winding is num_vertices points starting
+ * at first_vertex of a shared xyz array.  cluster is the cluster of the
+ * face's samples. */
+typedef struct vrad_face {
+    float normal[3];
+    float dist;
+    float lightmap_vecs[2][4];
+    int32_t lightmap_mins[2];
+    int32_t lightmap_size[2];
+    int32_t first_vertex;
+    int32_t num_vertices;
+    int32_t cluster;
+    int32_t flags;
+} vrad_face;
+
+/* LightSample (MapTools/Rad/Light/FaceLight.cs:30-70): one per lightmap cell
+ * the face covers; coord is the cell's balance point in luxel space. */
+typedef struct vrad_sample {
+    float position[3];
+    float area;
+    float coord[2];
+    float mins[2];
+    float maxs[2];
+    int32_t s, t;
+    int32_t face;
+    int32_t cluster;
+} vrad_sample;
+
+/* DirectLight (MapTools/Rad/Light/DirectLight.cs), EmitType numbering:
+ * 0 surface, 1 point, 2 spotlight, 3 sky light (sun), 4 sky ambient. */
+typedef struct vrad_light {
+    int32_t type;
+    int32_t style;
+    float origin[3];
+    float intensity[3];
+    float normal[3];
+    float stop_dot;
+    float stop_dot2;
+    float exponent;
+    float constant_attn;
+    float linear_attn;
+    float quadratic_attn;
+    float start_fade_distance;
+    float end_fade_distance;
+    float cap_dist;
+} vrad_light;
+
+/* LightingValue (MapTools/Rad/Light/LightingValue.cs). */
+typedef struct vrad_lighting_value {
+    float lighting[3];
+    float direct_sun_amount;
+} vrad_lighting_value;
+
+/* What the lighting stage reads.  samples are face-major, each face's in
+ * the order vrad_build_samples writes them.  lights are the active list in
+ * gather order; cluster_lights lists, per cluster, the lights whose PVS
+ * reaches it, in list order (DirectLightGatherer's per-cluster lists).
+ * sky_directions are the DirectionalSampler prefix (xyz each) the sky
+ * ambient uses; sun_jitter the prefix the sun's jittered rays use (entry
+ * d-1 for ray d); sun_samples is 1 with no angular extent. */
+typedef struct vrad_world_desc {
+    const vrad_face *faces;
+    int32_t nfaces;
+    const vrad_sample *samples;
+    int64_t nsamples;
+    const vrad_light *lights;
+    int32_t nlights;
+    const int32_t *cluster_light_offsets;  /* nclusters + 1 */
+    const int32_t *cluster_lights;
+    int32_t nclusters;
+    const float *sky_directions;
+    int32_t nsky_directions;
+    const float *sun_jitter;
+    int32_t nsun_jitter;
+    float sun_angular_extent;
+    int32_t sun_samples;
+} vrad_world_desc;
+
+typedef struct vrad_direct_stats {
+    int64_t samples;
+    int64_t visibility_rays;   /* shadow segments to point and spot lights */
+    int64_t sky_rays;          /* sun and sky-ambient sky tests */
+    float kernel_ms;
+} vrad_direct_stats;
+
+/* FaceSampleBuilder.CalcPoints without -fast (FaceSampleBuilder.cs:80-367):
+ * host-side set-up, no device needed.  Writes each face's samples into out
+ * (capacity entries) and face_first[f] (nfaces + 1 entries) = index of face
+ * f's first sample.  With out = NULL it only counts. */
+int32_t vrad_build_samples(const vrad_face *faces, int32_t nfaces, const float *vertices,
+                           int64_t nvertices, vrad_sample *out, int64_t capacity, int64_t *count,
+                           int64_t *face_first);
+
+/* Uploads the lighting world to the context's device (kept until the next
+ * upload or vrad_destroy).  The scene (vrad_scene_upload) is the shadow
+ * casters.  VRAD_ERR_UNSUPPORTED for a surface light (type 0) or for a
+ * group of four samples that spans two clusters. */
+int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *world);
+
+/* The direct gather of every sample, style 0, flat normals: out[i] is
+ * sample i's LightingValue (host buffer, nsamples entries).  Blocks. */
+int32_t vrad_direct_lighting(vrad_ctx *ctx, vrad_lighting_value *out, vrad_direct_stats *stats);
+
+/* The same into a device buffer on `stream` (NULL = default stream). */
+int32_t vrad_direct_lighting_device(vrad_ctx *ctx, vrad_lighting_value *d_out, void *stream);
+
 /* Largest batch vrad_trace_visibility_static accepts: four of the
  * reference's 16,384-ray batches. */
 #define VRAD_STATIC_MAX_RAYS 65536

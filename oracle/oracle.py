@@ -57,6 +57,10 @@ def lib() -> ctypes.CDLL:
         _lib.orc_fp64_classify.argtypes = [P, i32, P, i32, ctypes.c_double, P, i32]
         for name in ("orc_tri_prepare", "orc_kd_trace", "orc_brute_trace", "orc_fp64_classify"):
             getattr(_lib, name).restype = ctypes.c_int
+        _lib.orc_build_samples.argtypes = [P, i32, P, P, ctypes.c_int64, P, P]
+        _lib.orc_build_samples.restype = ctypes.c_int
+        _lib.orc_direct.argtypes = [P, P, P, P, P, i32, P, P, P, P, P, P, i32, P, i32, f32, P, i32, P]
+        _lib.orc_direct.restype = ctypes.c_int
         if hasattr(_lib, "orc_kd_build"):
             _lib.orc_kd_build.argtypes = [P, P, P, i32, P]
             _lib.orc_kd_build.restype = ctypes.c_int
@@ -178,3 +182,50 @@ def bits_to_bool(bits: np.ndarray, n: int) -> np.ndarray:
     """Unpack LSB-first u64 words into n booleans."""
     b = np.ascontiguousarray(bits, dtype="<u8").view(np.uint8)
     return np.unpackbits(b, bitorder="little")[:n].astype(bool)
+
+
+def build_samples(faces: np.ndarray, verts: np.ndarray):
+    """FaceSampleBuilder restated: (samples as a 56-byte record array viewed
+    through the caller's dtype, face_first)."""
+    faces = np.ascontiguousarray(faces)
+    verts = np.ascontiguousarray(verts, np.float32)
+    count = ctypes.c_int64()
+    rc = lib().orc_build_samples(_p(faces), len(faces), _p(verts), None, 0, ctypes.byref(count), None)
+    if rc != 0:
+        raise RuntimeError(f"orc_build_samples failed: {rc}")
+    out = np.zeros(count.value * 56, np.uint8)
+    first = np.zeros(len(faces) + 1, np.int64)
+    rc = lib().orc_build_samples(_p(faces), len(faces), _p(verts), _p(out), count.value,
+                                 ctypes.byref(count), _p(first))
+    if rc != 0:
+        raise RuntimeError(f"orc_build_samples failed: {rc}")
+    return out, first
+
+
+def direct(tree: dict, faces, samples, face_first, lights, cl_off, cl_list, dirs,
+           jitter=None, sun_samples: int = 1, sun_extent: float = 0.0,
+           threads: int | None = None, count_rays: bool = False):
+    """The direct gather restated; (nsamples, 4) float32: lighting xyz, sun
+    (and the number of segments traced, with count_rays)."""
+    nodes = np.ascontiguousarray(tree["nodes"], dtype=NODE_DTYPE)
+    idx = np.ascontiguousarray(tree["indices"], dtype=np.int32)
+    tris = np.ascontiguousarray(tree["tris"], dtype=TRI_DTYPE)
+    bounds = np.ascontiguousarray(tree["bounds"], dtype=np.float32)
+    faces = np.ascontiguousarray(faces)
+    samples = np.ascontiguousarray(samples)
+    face_first = np.ascontiguousarray(face_first, np.int64)
+    lights = np.ascontiguousarray(lights)
+    cl_off = np.ascontiguousarray(cl_off, np.int32)
+    cl_list = np.ascontiguousarray(cl_list, np.int32)
+    dirs = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+    jit = np.ascontiguousarray(jitter if jitter is not None else np.zeros((1, 3)), np.float32)
+    n = int(face_first[-1])
+    out = np.zeros((n, 4), np.float32)
+    rays = ctypes.c_int64()
+    rc = lib().orc_direct(_p(nodes), _p(idx), _p(tris), _p(bounds), _p(faces), len(faces), _p(samples),
+                          _p(face_first), _p(lights), _p(cl_off), _p(cl_list), _p(dirs), len(dirs),
+                          _p(jit), sun_samples, sun_extent, _p(out),
+                          threads if threads is not None else default_threads(), ctypes.byref(rays))
+    if rc != 0:
+        raise RuntimeError(f"orc_direct failed: {rc}")
+    return (out, rays.value) if count_rays else out

@@ -7,6 +7,7 @@
 // does; the order of operations below is the reference's.
 
 #include "vrad_oracle.h"
+#include "oracle_internal.h"
 
 #include <cmath>
 #include <cstring>
@@ -324,6 +325,25 @@ void parallel_for(int32_t n, int32_t threads, F &&f) {
 }
 
 }  // namespace
+
+// One segment, traced alone (a packet of four copies, as the reference's
+// TraceIsolated does, KdRayTracer.cs:609-625); true when blocked short of
+// its reach (sky_pass: when its first hit is opaque).
+bool orc_kd_segment_blocked(const OrcKd &kd, const orc_ray &r, bool sky_pass) {
+    thread_local std::vector<StackEntry> stack;
+    KdScene s{kd.nodes, kd.indices, kd.tris, {kd.bounds[0], kd.bounds[1], kd.bounds[2]},
+              {kd.bounds[3], kd.bounds[4], kd.bounds[5]}};
+    Packet p;
+    float reach[4];
+    load_packet(&r, 1, 0, true, p, reach);
+    float tmin4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    float dist[4];
+    int ids[4];
+    trace4(s, p, tmin4, reach, -1, !sky_pass, dist, ids, stack);
+    bool blocked = ids[0] > -1 && dist[0] < r.reach;
+    if (sky_pass && blocked && (kd.tris[ids[0]].id & ORC_TRACE_ID_SKY)) blocked = false;
+    return blocked;
+}
 
 extern "C" int orc_tri_prepare(const float *v9, const int32_t *ids, const uint8_t *flags,
                                int32_t n, orc_tri *out) {

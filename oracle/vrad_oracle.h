@@ -96,6 +96,59 @@ void orc_kd_free(orc_kdtree *tree);
 int orc_fp64_classify(const float *verts9, int32_t ntris, const orc_ray *rays, int32_t nrays,
                       double rel_margin, int8_t *out_class, int32_t threads);
 
+/* ---- lighting stage ---------------------------------------------------- */
+
+/* A lit face (the inputs of FaceLightInfo.Build).  Same layout as the
+ * library's vrad_face so a test can hand one buffer to both. */
+typedef struct orc_face {
+    float normal[3];
+    float dist;
+    float vecs[2][4];
+    int32_t mins[2];
+    int32_t size[2];
+    int32_t first_vertex;
+    int32_t num_vertices;
+    int32_t cluster;
+    int32_t flags;
+} orc_face;
+
+/* LightSample (FaceLight.cs:30-70).  Same layout as vrad_sample. */
+typedef struct orc_sample {
+    float position[3];
+    float area;
+    float coord[2];
+    float mins[2];
+    float maxs[2];
+    int32_t s, t;
+    int32_t face;
+    int32_t cluster;
+} orc_sample;
+
+/* DirectLight fields (DirectLight.cs).  Same layout as vrad_light. */
+typedef struct orc_light {
+    int32_t type;
+    int32_t style;
+    float origin[3];
+    float intensity[3];
+    float normal[3];
+    float stop_dot, stop_dot2, exponent;
+    float constant, linear, quadratic;
+    float start_fade, end_fade, cap_dist;
+} orc_light;
+
+/* FaceSampleBuilder.BuildFacesamples over every face. */
+int orc_build_samples(const orc_face *faces, int32_t nfaces, const float *verts, orc_sample *out,
+                      int64_t capacity, int64_t *count, int64_t *first);
+
+/* The direct gather (style 0, flat faces) over every sample, in four-sample
+ * groups per face; out is 4 floats per sample (lighting xyz, sun amount). */
+int orc_direct(const orc_kdnode *nodes, const int32_t *indices, const orc_tri *tris,
+               const float *bounds6, const orc_face *faces, int32_t nfaces,
+               const orc_sample *samples, const int64_t *face_first, const orc_light *lights,
+               const int32_t *cl_off, const int32_t *cl_list, const float *dirs, int32_t ndirs,
+               const float *jitter, int32_t sun_samples, float sun_extent, float *out,
+               int32_t threads, int64_t *rays_out);
+
 #ifdef __cplusplus
 }
 #endif
