@@ -449,6 +449,7 @@ def main_stage(args):
     stage = L.LightingStage(w, inp, device=local)
     info = stage.tracer.scene_info()
     d_out = torch.empty(n * 4, dtype=torch.float32, device=device)
+    block, tune_ms = stage.autotune()                # picks the launch shape (untimed)
     host, stats = stage.direct()                     # counts the segments of one step
     rays_per_step = int(stats.visibility_rays + stats.sky_rays)
     for _ in range(max(3, args.warmup)):
@@ -552,6 +553,7 @@ def main_stage(args):
             "step_ms": per_step,
             "bvh": {"nodes": info.bvh_nodes, "leaves": info.bvh_leaves, "max_leaf": info.max_leaf,
                     "build_ms": info.build_ms, "pad": info.box_pad},
+            "autotune": {"threads_per_cta": block, "ms": tune_ms},
             "check": check,
         }
         print(json.dumps(line), flush=True)

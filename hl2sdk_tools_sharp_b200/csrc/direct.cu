@@ -47,7 +47,7 @@ __device__ __forceinline__ bool group_any(bool v, unsigned gmask) {
 // The segment start -> stop (LightRayLog.MakeRay: whole segment, reach 1).
 // Visibility blocks on any hit; a sky test blocks only when the first hit
 // is opaque.
-template <int MODE>
+template <int MODE, int STRIDE>
 __device__ __forceinline__ bool segment_blocked(const DeviceScene &sc, float sx, float sy, float sz,
                                                 float ex, float ey, float ez, int *stack,
                                                 uint32_t *overflow) {
@@ -56,7 +56,7 @@ __device__ __forceinline__ bool segment_blocked(const DeviceScene &sc, float sx,
     float t;
     int32_t orig;
     uint32_t meta;
-    trace_ray<MODE>(sc, r, 0.0f, 1.0f, -1, stack, overflow, hit, t, orig, meta);
+    trace_ray<MODE, STRIDE>(sc, r, 0.0f, 1.0f, -1, stack, overflow, hit, t, orig, meta);
     return hit;
 }
 
@@ -81,19 +81,24 @@ __device__ __forceinline__ float inverse_quadratic(float d, float q, float l, fl
     return __fdiv_rn(1.0f, f);
 }
 
-__global__ void __launch_bounds__(kBlock) k_direct(DeviceScene sc, DeviceWorld w, float4 *__restrict__ out,
-                                                   unsigned long long *__restrict__ counters,
-                                                   uint32_t *__restrict__ overflow) {
-    __shared__ int stack_mem[kStackDepth * kBlock];
+// BLOCK threads per CTA (32, 64 or 128, chosen by vrad_direct_autotune):
+// every thread traces its samples' whole light list, so a small CTA frees
+// its SM slot as soon as its own warps are done.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_direct(DeviceScene sc, DeviceWorld w, float4 *__restrict__ out,
+                                                  unsigned long long *__restrict__ counters,
+                                                  uint32_t *__restrict__ overflow) {
+    __shared__ int stack_mem[kStackDepth * BLOCK];
     int *stack = stack_mem + threadIdx.x;
-    const int64_t slot = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+    const int64_t slot = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
+    // nslots is a multiple of 32, so a warp is wholly in or out.
     if (slot >= w.nslots) return;
     const int32_t code = __ldg(&w.slots[slot]);
-    if (code == -1) return;  // a whole empty group at the end
+    const bool present = code != -1;  // -1: a whole empty group at the end
     const int lane = threadIdx.x & 31;
     const unsigned gmask = 0xFu << (lane & ~3);
-    const bool real = (code & 0x80000000) == 0;
-    const int32_t si = code & 0x7fffffff;
+    const bool real = present && (code & 0x80000000) == 0;
+    const int32_t si = present ? (code & 0x7fffffff) : 0;
 
     const float4 sp = __ldg(&w.sample_pos[si]);
     const int face = __float_as_int(sp.w);
@@ -106,7 +111,7 @@ __global__ void __launch_bounds__(kBlock) k_direct(DeviceScene sc, DeviceWorld w
     float ax = 0.0f, ay = 0.0f, az = 0.0f, sun = 0.0f;
     unsigned long long vis_rays = 0, sky_rays = 0;
 
-    const int l0 = __ldg(&w.cl_off[cluster]), l1 = __ldg(&w.cl_off[cluster + 1]);
+    const int l0 = __ldg(&w.cl_off[cluster]), l1 = present ? __ldg(&w.cl_off[cluster + 1]) : l0;
     for (int k = l0; k < l1; k++) {
         const int li = __ldg(&w.cl_list[k]);
         const float4 *L = w.lights + kLightF4 * li;
@@ -156,7 +161,7 @@ __global__ void __launch_bounds__(kBlock) k_direct(DeviceScene sc, DeviceWorld w
             }
             if (real && dot != 0.0f && falloff != 0.0f) {
                 vis_rays++;
-                if (segment_blocked<kModeAny>(sc, px, py, pz, A.x, A.y, A.z, stack, overflow)) dot = 0.0f;
+                if (segment_blocked<kModeAny, BLOCK>(sc, px, py, pz, A.x, A.y, A.z, stack, overflow)) dot = 0.0f;
             }
         } else if (type == kSkyLight) {
             // EmitSkyLight / ResolveSkyLight.
@@ -178,7 +183,7 @@ __global__ void __launch_bounds__(kBlock) k_direct(DeviceScene sc, DeviceWorld w
                     float frac = 1.0f;
                     if (real) {
                         sky_rays++;
-                        if (segment_blocked<kModeSkyPass>(sc, px, py, pz, __fadd_rn(ex, px), __fadd_rn(ey, py),
+                        if (segment_blocked<kModeSkyPass, BLOCK>(sc, px, py, pz, __fadd_rn(ex, px), __fadd_rn(ey, py),
                                                           __fadd_rn(ez, pz), stack, overflow))
                             frac = 0.0f;
                     }
@@ -210,7 +215,7 @@ __global__ void __launch_bounds__(kBlock) k_direct(DeviceScene sc, DeviceWorld w
                     const float ey = __fadd_rn(__fmul_rn(an.y, -kMaxTraceLength), py);
                     const float ez = __fadd_rn(__fmul_rn(an.z, -kMaxTraceLength), pz);
                     sky_rays++;
-                    if (segment_blocked<kModeSkyPass>(sc, sx, sy, sz, ex, ey, ez, stack, overflow)) frac = 0.0f;
+                    if (segment_blocked<kModeSkyPass, BLOCK>(sc, sx, sy, sz, ex, ey, ez, stack, overflow)) frac = 0.0f;
                 }
                 ambient = __fadd_rn(ambient, __fmul_rn(frac, dv));
             }
@@ -231,12 +236,14 @@ __global__ void __launch_bounds__(kBlock) k_direct(DeviceScene sc, DeviceWorld w
     }
     if (real) out[si] = make_float4(ax, ay, az, sun);
 
-    // Ray counts: one atomic per warp.
+    // Ray counts: the whole warp is here (no lane returned early), one
+    // atomic per warp.
+    __syncwarp();
     for (int o = 16; o > 0; o >>= 1) {
-        vis_rays += __shfl_xor_sync(__activemask(), vis_rays, o);
-        sky_rays += __shfl_xor_sync(__activemask(), sky_rays, o);
+        vis_rays += __shfl_xor_sync(kFull, vis_rays, o);
+        sky_rays += __shfl_xor_sync(kFull, sky_rays, o);
     }
-    if (lane == (__ffs(__activemask()) - 1)) {
+    if (lane == 0) {
         atomicAdd(&counters[0], vis_rays);
         atomicAdd(&counters[1], sky_rays);
     }
@@ -263,10 +270,20 @@ void WorldBuffers::release() {
 }
 
 cudaError_t launch_direct(const DeviceScene &scene, const DeviceWorld &world, float4 *out,
-                          unsigned long long *counters, uint32_t *overflow, cudaStream_t stream) {
+                          unsigned long long *counters, uint32_t *overflow, cudaStream_t stream,
+                          int block) {
     if (world.nslots == 0) return cudaSuccess;
-    const int64_t grid = (world.nslots + kBlock - 1) / kBlock;
-    k_direct<<<(unsigned)grid, kBlock, 0, stream>>>(scene, world, out, counters, overflow);
+    switch (block) {
+        case 32:
+            k_direct<32><<<(unsigned)((world.nslots + 31) / 32), 32, 0, stream>>>(scene, world, out, counters, overflow);
+            break;
+        case 64:
+            k_direct<64><<<(unsigned)((world.nslots + 63) / 64), 64, 0, stream>>>(scene, world, out, counters, overflow);
+            break;
+        default:
+            k_direct<128><<<(unsigned)((world.nslots + 127) / 128), 128, 0, stream>>>(scene, world, out, counters, overflow);
+            break;
+    }
     return cudaGetLastError();
 }
 
@@ -404,7 +421,8 @@ int32_t direct_on(vrad_ctx *ctx, float4 *d_out, cudaStream_t s) {
     if (!ctx->world.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no lighting world uploaded");
     cudaError_t e = cudaMemsetAsync(ctx->world.counters, 0, 2 * sizeof(unsigned long long), s);
     if (e == cudaSuccess)
-        e = vrad::launch_direct(ctx->scene.view(), ctx->world.view, d_out, ctx->world.counters, ctx->status, s);
+        e = vrad::launch_direct(ctx->scene.view(), ctx->world.view, d_out, ctx->world.counters, ctx->status, s,
+                                ctx->world.block);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "direct lighting launch");
     return VRAD_OK;
 }
@@ -467,4 +485,43 @@ extern "C" int32_t vrad_direct_lighting(vrad_ctx *ctx, vrad_lighting_value *out,
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     return rc;
+}
+
+extern "C" int32_t vrad_direct_autotune(vrad_ctx *ctx, int32_t *chosen_block, float *times_ms) {
+    if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (!ctx->has_scene) return vrad_fail(ctx, VRAD_ERR_NO_SCENE, "no scene uploaded");
+    if (!ctx->world.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no lighting world uploaded");
+    cudaError_t e = cudaSetDevice(ctx->device);
+    const int64_t n = ctx->world.view.nsamples;
+    float4 *d_out = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(float4) * (size_t)(n ? n : 1));
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    const int candidates[3] = {32, 64, 128};
+    float best = 1e30f;
+    int best_block = 128;
+    for (int k = 0; k < 3 && e == cudaSuccess; k++) {
+        e = cudaEventRecord(a, ctx->stream);
+        if (e == cudaSuccess)
+            e = vrad::launch_direct(ctx->scene.view(), ctx->world.view, d_out, ctx->world.counters, ctx->status,
+                                    ctx->stream, candidates[k]);
+        if (e == cudaSuccess) e = cudaEventRecord(b, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        float ms = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+        if (times_ms) times_ms[k] = ms;
+        if (e == cudaSuccess && ms < best) {
+            best = ms;
+            best_block = candidates[k];
+        }
+    }
+    cudaFree(d_out);
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "direct autotune");
+    ctx->world.block = best_block;
+    if (chosen_block) *chosen_block = best_block;
+    return VRAD_OK;
 }

@@ -58,12 +58,14 @@ struct WorldBuffers {
     unsigned long long *counters = nullptr;  // [0] visibility rays, [1] sky rays
     DeviceWorld view{};
     bool ready = false;
+    int block = 64;  // threads per CTA of the gather; vrad_direct_autotune picks it
 
     void release();
 };
 
 // Launches the fused gather: out[i] = (lighting xyz, direct sun amount).
 cudaError_t launch_direct(const DeviceScene &scene, const DeviceWorld &world, float4 *out,
-                          unsigned long long *counters, uint32_t *overflow, cudaStream_t stream);
+                          unsigned long long *counters, uint32_t *overflow, cudaStream_t stream,
+                          int block);
 
 }  // namespace vrad

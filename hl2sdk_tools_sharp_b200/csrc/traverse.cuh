@@ -100,7 +100,7 @@ __device__ __forceinline__ void slab2(const float4 &a, const float4 &b, const fl
 // (thi, best_orig); best_orig = -1 makes the window half-open, [tmin, thi).
 // ANY stops at the first acceptance; otherwise the best is kept and the
 // box window shrinks to [tmin, thi].  Returns whether anything was accepted.
-template <bool ANY>
+template <bool ANY, int STRIDE = kBlock>
 __device__ __forceinline__ bool walk(const DeviceBvh &s, const int32_t *__restrict__ tri_id,
                                      const RayState &r, float tmin, int32_t skip_id, int *stack,
                                      uint32_t *overflow, float &thi, int32_t &best_orig,
@@ -123,7 +123,7 @@ __device__ __forceinline__ bool walk(const DeviceBvh &s, const int32_t *__restri
                     far_ref = r0;
                 }
                 if (sp < kStackDepth) {
-                    stack[sp * kBlock] = far_ref;
+                    stack[sp * STRIDE] = far_ref;
                     sp++;
                 } else {
                     atomicOr(overflow, 1u);
@@ -160,7 +160,7 @@ __device__ __forceinline__ bool walk(const DeviceBvh &s, const int32_t *__restri
         }
         if (sp == 0) return hit;
         sp--;
-        ref = stack[sp * kBlock];
+        ref = stack[sp * STRIDE];
     }
 }
 
@@ -171,7 +171,7 @@ __device__ __forceinline__ bool walk(const DeviceBvh &s, const int32_t *__restri
 //                 nearest sky hit (t_s, i_s) is found first, then any
 //                 opaque hit below it decides, so the opaque walk stops at
 //                 its first acceptance.
-template <int MODE>
+template <int MODE, int STRIDE = kBlock>
 __device__ __forceinline__ void trace_ray(const DeviceScene &s, const RayState &r, float tmin,
                                           float reach, int32_t skip_id, int *stack,
                                           uint32_t *overflow, bool &hit, float &best_t,
@@ -182,20 +182,20 @@ __device__ __forceinline__ void trace_ray(const DeviceScene &s, const RayState &
     hit = false;
     if (MODE == kModeAny) {
         if (s.opaque.ntris)
-            hit = walk<true>(s.opaque, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
+            hit = walk<true, STRIDE>(s.opaque, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
         if (!hit && s.sky.ntris)
-            hit = walk<true>(s.sky, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
+            hit = walk<true, STRIDE>(s.sky, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
     } else if (MODE == kModeClosest) {
         if (s.opaque.ntris)
-            hit = walk<false>(s.opaque, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
+            hit = walk<false, STRIDE>(s.opaque, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
         if (s.sky.ntris)
-            hit |= walk<false>(s.sky, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
+            hit |= walk<false, STRIDE>(s.sky, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
     } else {
         if (s.sky.ntris)
-            walk<false>(s.sky, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
+            walk<false, STRIDE>(s.sky, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
         // Blocked iff an opaque hit sorts before the nearest sky hit.
         if (s.opaque.ntris)
-            hit = walk<true>(s.opaque, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
+            hit = walk<true, STRIDE>(s.opaque, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
     }
 }
 

@@ -81,6 +81,8 @@ def _lib():
         lib.vrad_direct_lighting.restype = i32
         lib.vrad_direct_lighting_device.argtypes = [P, P, P]
         lib.vrad_direct_lighting_device.restype = i32
+        lib.vrad_direct_autotune.argtypes = [P, ctypes.POINTER(i32), P]
+        lib.vrad_direct_autotune.restype = i32
         lib._lighting_bound = True
     return lib
 
@@ -290,6 +292,14 @@ class LightingStage:
         st = DirectStats()
         T._check(_lib().vrad_direct_lighting(self._ctx, out.ctypes.data, ctypes.byref(st)), self._ctx)
         return out, st
+
+    def autotune(self):
+        """vrad_direct_autotune: times each launch shape once on this world
+        and keeps the fastest.  Returns (threads per CTA, {shape: ms})."""
+        chosen = ctypes.c_int32()
+        times = np.zeros(3, np.float32)
+        T._check(_lib().vrad_direct_autotune(self._ctx, ctypes.byref(chosen), times.ctypes.data), self._ctx)
+        return chosen.value, {32: float(times[0]), 64: float(times[1]), 128: float(times[2])}
 
     def direct_into(self, out: np.ndarray):
         """vrad_direct_lighting into a caller's host buffer (LIGHTING_DTYPE)."""

@@ -267,6 +267,12 @@ int32_t vrad_direct_lighting(vrad_ctx *ctx, vrad_lighting_value *out, vrad_direc
 /* The same into a device buffer on `stream` (NULL = default stream). */
 int32_t vrad_direct_lighting_device(vrad_ctx *ctx, vrad_lighting_value *d_out, void *stream);
 
+/* Times the gather once per launch shape (32, 64 and 128 threads per CTA)
+ * on the uploaded world and keeps the fastest for later calls; times_ms
+ * (nullable, 3 entries) receives each shape's time.  No counterpart in the
+ * reference (its CPU work queue has no launch shape). */
+int32_t vrad_direct_autotune(vrad_ctx *ctx, int32_t *chosen_block, float *times_ms);
+
 /* Largest batch vrad_trace_visibility_static accepts: four of the
  * reference's 16,384-ray batches. */
 #define VRAD_STATIC_MAX_RAYS 65536
