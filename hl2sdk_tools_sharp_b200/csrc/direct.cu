@@ -91,14 +91,16 @@ __global__ void __launch_bounds__(BLOCK) k_direct(DeviceScene sc, DeviceWorld w,
     __shared__ int stack_mem[kStackDepth * BLOCK];
     int *stack = stack_mem + threadIdx.x;
     const int64_t slot = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
-    // nslots is a multiple of 32, so a warp is wholly in or out.
+    // nslots is a multiple of 32 and every warp's slots share one cluster
+    // (vrad_world_upload lays them out so), so the light loop is
+    // warp-uniform and the __syncwarp()s below keep the lanes in step: a
+    // warp traces one light (or one sky direction) at a time, coherently.
     if (slot >= w.nslots) return;
     const int32_t code = __ldg(&w.slots[slot]);
-    const bool present = code != -1;  // -1: a whole empty group at the end
     const int lane = threadIdx.x & 31;
     const unsigned gmask = 0xFu << (lane & ~3);
-    const bool real = present && (code & 0x80000000) == 0;
-    const int32_t si = present ? (code & 0x7fffffff) : 0;
+    const bool real = (code & 0x80000000) == 0;
+    const int32_t si = code & 0x7fffffff;
 
     const float4 sp = __ldg(&w.sample_pos[si]);
     const int face = __float_as_int(sp.w);
@@ -111,7 +113,7 @@ __global__ void __launch_bounds__(BLOCK) k_direct(DeviceScene sc, DeviceWorld w,
     float ax = 0.0f, ay = 0.0f, az = 0.0f, sun = 0.0f;
     unsigned long long vis_rays = 0, sky_rays = 0;
 
-    const int l0 = __ldg(&w.cl_off[cluster]), l1 = present ? __ldg(&w.cl_off[cluster + 1]) : l0;
+    const int l0 = __ldg(&w.cl_off[cluster]), l1 = __ldg(&w.cl_off[cluster + 1]);
     for (int k = l0; k < l1; k++) {
         const int li = __ldg(&w.cl_list[k]);
         const float4 *L = w.lights + kLightF4 * li;
@@ -167,7 +169,8 @@ __global__ void __launch_bounds__(BLOCK) k_direct(DeviceScene sc, DeviceWorld w,
             // EmitSkyLight / ResolveSkyLight.
             float d = -__fadd_rn(__fadd_rn(__fmul_rn(nx, C.x), __fmul_rn(ny, C.y)), __fmul_rn(nz, C.z));
             d = maxps(d, 0.0f);
-            if (group_any(d != 0.0f, gmask)) {
+            const bool need = group_any(d != 0.0f, gmask);
+            if (__any_sync(kFull, need)) {
                 const int ns = w.sun_samples;
                 const float jitter_scale = (float)(1.732050807569 * (2 * 16384) * (double)w.sun_extent);
                 float total = 0.0f;
@@ -181,18 +184,22 @@ __global__ void __launch_bounds__(BLOCK) k_direct(DeviceScene sc, DeviceWorld w,
                         ez = __fadd_rn(ez, __fmul_rn(j.z, jitter_scale));
                     }
                     float frac = 1.0f;
-                    if (real) {
+                    if (need && real) {
                         sky_rays++;
-                        if (segment_blocked<kModeSkyPass, BLOCK>(sc, px, py, pz, __fadd_rn(ex, px), __fadd_rn(ey, py),
-                                                          __fadd_rn(ez, pz), stack, overflow))
+                        if (segment_blocked<kModeSkyPass, BLOCK>(sc, px, py, pz, __fadd_rn(ex, px),
+                                                                 __fadd_rn(ey, py), __fadd_rn(ez, pz), stack,
+                                                                 overflow))
                             frac = 0.0f;
                     }
                     total = __fadd_rn(total, frac);
+                    __syncwarp();
                 }
-                const float see = __fmul_rn(total, __fdiv_rn(1.0f, (float)ns));
-                dot = __fmul_rn(d, see);
-                falloff = 1.0f;
-                sun_amount = __fmul_rn(see, 10000.0f);
+                if (need) {
+                    const float see = __fmul_rn(total, __fdiv_rn(1.0f, (float)ns));
+                    dot = __fmul_rn(d, see);
+                    falloff = 1.0f;
+                    sun_amount = __fmul_rn(see, 10000.0f);
+                }
             }
         } else if (type == kSkyAmbient) {
             // AmbientSky: every direction in front of the face, in order.
@@ -218,11 +225,13 @@ __global__ void __launch_bounds__(BLOCK) k_direct(DeviceScene sc, DeviceWorld w,
                     if (segment_blocked<kModeSkyPass, BLOCK>(sc, sx, sy, sz, ex, ey, ez, stack, overflow)) frac = 0.0f;
                 }
                 ambient = __fadd_rn(ambient, __fmul_rn(frac, dv));
+                __syncwarp();
             }
             const float factor = __fdiv_rn(possible, possible);
             dot = __fdiv_rn(ambient, __fmul_rn(factor, sumdot));
             falloff = 1.0f;
         }
+        __syncwarp();
         // Resolve: a light behind the face lights nothing.
         dot = maxps(dot, 0.0f);
         const float fx = __fmul_rn(real ? dot : 0.0f, falloff);
@@ -236,8 +245,7 @@ __global__ void __launch_bounds__(BLOCK) k_direct(DeviceScene sc, DeviceWorld w,
     }
     if (real) out[si] = make_float4(ax, ay, az, sun);
 
-    // Ray counts: the whole warp is here (no lane returned early), one
-    // atomic per warp.
+    // Ray counts: one atomic per warp.
     __syncwarp();
     for (int o = 16; o > 0; o >>= 1) {
         vis_rays += __shfl_xor_sync(kFull, vis_rays, o);
@@ -323,25 +331,20 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
         if (w->cluster_lights[k] < 0 || w->cluster_lights[k] >= nl)
             return vrad_fail(ctx, VRAD_ERR_ARG, "cluster light list names light %d", w->cluster_lights[k]);
 
-    // Slots: each face's samples padded to whole groups of four.
-    std::vector<int32_t> slots;
-    slots.reserve((size_t)(w->nsamples + 4 * (int64_t)w->nfaces));
+    // Samples: positions, and each face's run [start, end).
     std::vector<float4> pos((size_t)w->nsamples);
+    std::vector<int64_t> fstart((size_t)w->nfaces, -1), fend((size_t)w->nfaces, -1);
     int64_t i = 0;
     while (i < w->nsamples) {
         const int32_t face = w->samples[i].face;
         if (face < 0 || face >= w->nfaces) return vrad_fail(ctx, VRAD_ERR_ARG, "sample %lld names face %d", (long long)i, face);
+        if (fstart[(size_t)face] != -1)
+            return vrad_fail(ctx, VRAD_ERR_ARG, "face %d's samples are not contiguous", face);
         int64_t j = i;
         while (j < w->nsamples && w->samples[j].face == face) j++;
         const int32_t cl = w->faces[face].cluster;
         if (cl < 0 || cl >= w->nclusters)
             return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "face %d has cluster %d outside the light lists", face, cl);
-        for (int64_t g = i; g < j; g += 4) {
-            for (int l = 0; l < 4; l++) {
-                int64_t s = g + l;
-                slots.push_back(s < j ? (int32_t)s : (int32_t)((j - 1) | 0x80000000LL));
-            }
-        }
         for (int64_t s = i; s < j; s++) {
             if (w->samples[s].cluster != cl)
                 return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED,
@@ -356,9 +359,32 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
             memcpy(&p.w, &f, 4);
             pos[(size_t)s] = p;
         }
+        fstart[(size_t)face] = i;
+        fend[(size_t)face] = j;
         i = j;
     }
-    while (slots.size() % 32) slots.push_back(-1);
+    // Slots, cluster by cluster: each face's samples in whole groups of
+    // four (the last group repeating its last sample as padding), each
+    // cluster's run padded to whole warps with more padding lanes, so no
+    // warp mixes two light lists.
+    std::vector<int32_t> slots;
+    slots.reserve((size_t)(w->nsamples + 4 * (int64_t)w->nfaces + 32 * (int64_t)w->nclusters));
+    std::vector<std::vector<int32_t>> by_cluster((size_t)w->nclusters);
+    for (int32_t f = 0; f < w->nfaces; f++)
+        if (fstart[(size_t)f] >= 0) by_cluster[(size_t)w->faces[f].cluster].push_back(f);
+    for (int32_t c = 0; c < w->nclusters; c++) {
+        int32_t last = -1;
+        for (int32_t f : by_cluster[(size_t)c]) {
+            const int64_t a = fstart[(size_t)f], b = fend[(size_t)f];
+            for (int64_t g = a; g < b; g += 4)
+                for (int l = 0; l < 4; l++) {
+                    const int64_t s = g + l;
+                    slots.push_back(s < b ? (int32_t)s : (int32_t)((b - 1) | 0x80000000LL));
+                }
+            last = (int32_t)(b - 1);
+        }
+        while (last >= 0 && slots.size() % 32) slots.push_back((int32_t)(last | 0x80000000LL));
+    }
     std::vector<float4> fnorm((size_t)w->nfaces);
     for (int32_t f = 0; f < w->nfaces; f++) {
         float4 v;

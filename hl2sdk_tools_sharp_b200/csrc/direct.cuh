@@ -3,10 +3,13 @@
 //
 // Layout in HBM:
 //   slots[k]        int32: sample index of thread k; bit 31 marks a padding
-//                   lane (a face's last group of four repeats its last
-//                   sample, as FaceLightJob.EmitGroup pads); -1 = no sample.
-//                   Each face's samples start on a multiple of four, so a
-//                   reference sample group is four adjacent lanes of a warp.
+//                   lane, which repeats a sample, traces nothing and writes
+//                   nothing (a face's last group of four repeats its last
+//                   sample, as FaceLightJob.EmitGroup pads).  Slots run
+//                   cluster by cluster, each face's samples starting on a
+//                   multiple of four (a reference sample group is four
+//                   adjacent lanes) and each cluster padded to whole warps,
+//                   so a warp's lanes share one light list.
 //   sample_pos[i]   float4 (position xyz, face index bits)
 //   face_normal[f]  float4 (plane normal xyz, cluster bits)
 //   lights[l]       5 x float4, the DirectLight fields:
