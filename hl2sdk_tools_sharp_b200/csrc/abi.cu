@@ -201,7 +201,7 @@ int32_t vrad_create(int32_t device, vrad_ctx **out) {
         vrad_destroy(ctx);
         return rc;
     }
-    char id[256];
+    char id[320];
     snprintf(id, sizeof id, "cuda-bvh-kdexact-1-%s-sm%d%d", prop.name, prop.major, prop.minor);
     for (char *c = id; *c; c++)
         if (*c == ' ') *c = '-';
