@@ -218,6 +218,8 @@ int32_t vrad_destroy(vrad_ctx *ctx) {
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         ctx->scene.release();
         ctx->world.release();
+        ctx->final_pass.release();
+        cudaFree(ctx->sample_light);
         cudaFree(ctx->status);
         cudaFree(ctx->d_rays);
         cudaFree(ctx->d_out);

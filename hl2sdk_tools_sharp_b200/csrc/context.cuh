@@ -7,6 +7,7 @@
 #include <string>
 
 #include "direct.cuh"
+#include "final.cuh"
 #include "scene.cuh"
 
 struct vrad_ctx {
@@ -23,6 +24,8 @@ struct vrad_ctx {
     void *d_out = nullptr;
     size_t d_out_cap = 0;
     vrad::WorldBuffers world;
+    vrad::FinalBuffers final_pass;
+    float4 *sample_light = nullptr;  // the direct gather's output, one per sample
     std::string last_error;
     std::string identity;
 };

@@ -19,6 +19,7 @@
 
 #include <cuda_runtime.h>
 
+#include <string>
 #include <vector>
 
 #include "context.cuh"
@@ -436,6 +437,27 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     wb.view = vrad::DeviceWorld{wb.slots, (int64_t)slots.size(), wb.sample_pos, wb.face_normal, wb.lights, nl,
                                 wb.cl_off, wb.cl_list, w->nclusters, wb.dirs, w->nsky_directions, wb.jitter,
                                 w->nsun_jitter, w->sun_angular_extent, w->sun_samples, w->nsamples};
+    // The final pass's tables, and the direct gather's output buffer.
+    ctx->final_pass.release();
+    cudaFree(ctx->sample_light);
+    ctx->sample_light = nullptr;
+    if (w->vertices && w->nvertices > 0) {
+        std::string why;
+        e = vrad::build_final(ctx->final_pass, w->faces, w->nfaces, w->samples, w->nsamples, w->vertices,
+                              w->nvertices, why);
+        if (e != cudaSuccess) {
+            wb.release();
+            if (e == cudaErrorInvalidValue) return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "final pass: %s", why.c_str());
+            return vrad_cuda_fail(ctx, e, why.c_str());
+        }
+        ctx->final_pass.view.sample_pos = wb.sample_pos;
+    }
+    e = cudaMalloc(&ctx->sample_light, sizeof(float4) * (size_t)(w->nsamples ? w->nsamples : 1));
+    if (e != cudaSuccess) {
+        wb.release();
+        ctx->final_pass.release();
+        return vrad_cuda_fail(ctx, e, "sample light buffer");
+    }
     wb.ready = true;
     return VRAD_OK;
 }

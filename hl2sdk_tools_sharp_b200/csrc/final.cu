@@ -1,0 +1,496 @@
+// final.cu -- the lighting stage's final pass: each face's luxels from its
+// own and its smoothing neighbours' light samples, minlight, the RGBE
+// encode and the per-face median, written straight into the LIGHTING
+// lump's byte image at the faces' lightofs.
+//
+// Reference behaviour restated (muflub/hl2sdk_tools_sharp, MapTools/Rad):
+//   FinalLightFace.Run / BuildLuxelRadial (Final/FinalLightFace.cs:93-360),
+//       style 0, no bounce (-bounce 0), no macro textures, minlight 0;
+//   LuxelRadial.AddDirect / Sample (Final/LuxelRadial.cs:140-331);
+//   StockLightColor.Encode (Ambient/StockLightColor.cs:136-185);
+//   FinalLightFace.Median: sort, take element count >> 1;
+//   LightmapOffsets.Compute (Light/LightmapOffsets.cs:54-126).
+//
+// Kernels (one launch each per pass):
+//   k_radial  one thread per radial cell: the weighted sum of every sample
+//             whose box covers the cell, in the reference's sample order
+//             (the face's own samples, then each neighbour's)
+//   k_luxel   one thread per luxel: LuxelRadial.Sample at the luxel's own
+//             position, minlight, Encode, store
+//   k_median  one CTA per face: bitonic sort of the sampled luxels per
+//             channel, the median, Encode, store before lightofs
+
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <vector>
+
+#include <string>
+#include <type_traits>
+
+#include "context.cuh"
+#include "final.cuh"
+#include "world.h"
+
+namespace vrad {
+
+namespace {
+
+constexpr int kMedianThreads = 1024;
+constexpr int kMedianMax = 2048;  // luxels per face the median sorts in shared memory
+
+__device__ __forceinline__ void world_to_luxel(const float4 &o, const float4 &ws, const float4 &wt, int mins,
+                                               int mint, float px, float py, float pz, float &s, float &t) {
+    const float x = __fsub_rn(px, o.x), y = __fsub_rn(py, o.y), z = __fsub_rn(pz, o.z);
+    s = __fsub_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, ws.x), __fmul_rn(y, ws.y)), __fmul_rn(z, ws.z)), (float)mins);
+    t = __fsub_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, wt.x), __fmul_rn(y, wt.y)), __fmul_rn(z, wt.z)), (float)mint);
+}
+
+struct Frame {
+    float4 o, ws, wt, ls, lt;
+    int w, h, mins, mint, lightofs;
+};
+
+__device__ __forceinline__ Frame load_frame(const float4 *__restrict__ frames, int f) {
+    Frame fr;
+    fr.o = __ldg(&frames[5 * f + 0]);
+    fr.ws = __ldg(&frames[5 * f + 1]);
+    fr.wt = __ldg(&frames[5 * f + 2]);
+    fr.ls = __ldg(&frames[5 * f + 3]);
+    fr.lt = __ldg(&frames[5 * f + 4]);
+    fr.w = __float_as_int(fr.o.w);
+    fr.h = __float_as_int(fr.ws.w);
+    fr.mins = __float_as_int(fr.wt.w);
+    fr.mint = __float_as_int(fr.ls.w);
+    fr.lightofs = __float_as_int(fr.lt.w);
+    return fr;
+}
+
+// One sample's contribution to cell (s, t): LuxelRadial.AddDirect.
+__device__ __forceinline__ void add_direct(const Frame &fr, int s, int t, const float4 &pos, const float4 &box,
+                                           const float4 &light, float &lx, float &ly, float &lz, float &lsun,
+                                           float &weight) {
+    float cs, ct;
+    world_to_luxel(fr.o, fr.ws, fr.wt, fr.mins, fr.mint, pos.x, pos.y, pos.z, cs, ct);
+    int smin = __float2int_rz(box.x), tmin = __float2int_rz(box.y);
+    int smax = __float2int_rz(__fadd_rn(box.z, 0.9999f)) + 1, tmax = __float2int_rz(__fadd_rn(box.w, 0.9999f)) + 1;
+    smin = max(smin, 0);
+    tmin = max(tmin, 0);
+    smax = min(smax, fr.w);
+    tmax = min(tmax, fr.h);
+    if (s < smin || s >= smax || t < tmin || t >= tmax) return;
+    // max / min against -1 and 1 (compared in double, which changes nothing).
+    const float ds0 = __fsub_rn(box.x, (float)s);
+    const float s0 = ds0 > -1.0f ? ds0 : -1.0f;
+    const float dt0 = __fsub_rn(box.y, (float)t);
+    const float t0 = dt0 > -1.0f ? dt0 : -1.0f;
+    const float ds1 = __fsub_rn(box.z, (float)s);
+    const float s1 = ds1 < 1.0f ? ds1 : 1.0f;
+    const float dt1 = __fsub_rn(box.w, (float)t);
+    const float t1 = dt1 < 1.0f ? dt1 : 1.0f;
+    const float area = __fmul_rn(__fsub_rn(s1, s0), __fsub_rn(t1, t0));
+    if (!((double)area > 0.001)) return;
+    const float ds = fabsf(__fsub_rn(cs, (float)s)), dt = fabsf(__fsub_rn(ct, (float)t));
+    float r = ds > dt ? ds : dt;
+    r = ((double)r < 0.1) ? (float)__ddiv_rn((double)area, 0.1) : __fdiv_rn(area, r);
+    lx = __fadd_rn(lx, __fmul_rn(r, light.x));
+    ly = __fadd_rn(ly, __fmul_rn(r, light.y));
+    lz = __fadd_rn(lz, __fmul_rn(r, light.z));
+    lsun = __fadd_rn(lsun, __fmul_rn(r, light.w));
+    weight = __fadd_rn(weight, r);
+}
+
+__global__ void k_radial(FinalView v, const float4 *__restrict__ sample_light, float4 *__restrict__ rad_light,
+                         float *__restrict__ rad_weight) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= v.ncells) return;
+    const int f = __ldg(&v.cell_face[c]);
+    const Frame fr = load_frame(v.frames, f);
+    const int base = __ldg(&v.face_cells[f]);
+    const int local = (int)(c - base);
+    const int s = local % fr.w, t = local / fr.w;
+    float lx = 0.0f, ly = 0.0f, lz = 0.0f, lsun = 0.0f, weight = 0.0f;
+    // The face's own samples: only cells within two of this one can cover
+    // it, visited in sample order (rows, then columns).
+    for (int tc = t - 2; tc <= t + 1; tc++) {
+        if (tc < 0 || tc >= fr.h) continue;
+        for (int sc = s - 2; sc <= s + 1; sc++) {
+            if (sc < 0 || sc >= fr.w) continue;
+            const int k = __ldg(&v.cell_sample[base + sc + tc * fr.w]);
+            if (k < 0) continue;
+            add_direct(fr, s, t, __ldg(&v.sample_pos[k]), __ldg(&v.sample_box[k]), __ldg(&sample_light[k]), lx, ly,
+                       lz, lsun, weight);
+        }
+    }
+    // Then every neighbour's samples that can reach this face, in order.
+    const int c0 = __ldg(&v.cand_off[f]), c1 = __ldg(&v.cand_off[f + 1]);
+    for (int q = c0; q < c1; q++) {
+        const int k = __ldg(&v.cand_sample[q]);
+        add_direct(fr, s, t, __ldg(&v.sample_pos[k]), __ldg(&v.cand_box[q]), __ldg(&sample_light[k]), lx, ly, lz,
+                   lsun, weight);
+    }
+    rad_light[c] = make_float4(lx, ly, lz, lsun);
+    rad_weight[c] = weight;
+}
+
+// StockLightColor.Encode: ColorRGBExp32 as a little-endian word.
+__device__ __forceinline__ uint32_t encode(float x, float y, float z) {
+    float m;
+    if (x > y)
+        m = x > z ? x : z;
+    else
+        m = y > z ? y : z;
+    int e = 0;
+    if (m != 0.0f) e = (int)((__float_as_uint(m) & 0x7F800000u) >> 23) - (7 + 127);
+    const float scalar = __uint_as_float((uint32_t)(127 - e) << 23);
+    const uint32_t r = (uint8_t)__float2int_rz(__fmul_rn(x, scalar));
+    const uint32_t g = (uint8_t)__float2int_rz(__fmul_rn(y, scalar));
+    const uint32_t b = (uint8_t)__float2int_rz(__fmul_rn(z, scalar));
+    return r | (g << 8) | (b << 16) | ((uint32_t)(uint8_t)(int8_t)e << 24);
+}
+
+__global__ void k_luxel(FinalView v, const float4 *__restrict__ rad_light, const float *__restrict__ rad_weight,
+                        uint32_t *__restrict__ lighting, float4 *__restrict__ flat) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= v.ncells) return;
+    const int f = __ldg(&v.cell_face[c]);
+    const Frame fr = load_frame(v.frames, f);
+    const int base = __ldg(&v.face_cells[f]);
+    const int j = (int)(c - base);
+    const float s = (float)(j % fr.w), t = (float)(j / fr.w);
+    // The luxel's world position (BuildFaceLuxels), back into luxel space.
+    const float ss = __fadd_rn(s, (float)fr.mins), tt = __fadd_rn(t, (float)fr.mint);
+    const float px = __fadd_rn(__fadd_rn(fr.o.x, __fmul_rn(fr.ls.x, ss)), __fmul_rn(fr.lt.x, tt));
+    const float py = __fadd_rn(__fadd_rn(fr.o.y, __fmul_rn(fr.ls.y, ss)), __fmul_rn(fr.lt.y, tt));
+    const float pz = __fadd_rn(__fadd_rn(fr.o.z, __fmul_rn(fr.ls.z, ss)), __fmul_rn(fr.lt.z, tt));
+    float cs, ct;
+    world_to_luxel(fr.o, fr.ws, fr.wt, fr.mins, fr.mint, px, py, pz, cs, ct);
+    const int u = __float2int_rz(__fadd_rn(cs, 0.5f)), w = __float2int_rz(__fadd_rn(ct, 0.5f));
+    float lx = 0.0f, ly = 0.0f, lz = 0.0f;
+    bool ok = true;
+    if (u < 0 || u >= fr.w || w < 0 || w >= fr.h) {
+        lx = 2550.0f;  // LuxelRadial.ErrorRed
+        ok = false;
+    } else {
+        const int i = base + u + w * fr.w;
+        const float wt = rad_weight[i];
+        if (wt > 0.00001f) {
+            const float4 L = rad_light[i];
+            const float scale = (float)__drcp_rn((double)wt);
+            lx = __fmul_rn(L.x, scale);
+            ly = __fmul_rn(L.y, scale);
+            lz = __fmul_rn(L.z, scale);
+        } else {
+            ok = false;
+        }
+    }
+    if (__ldg(&v.face_nsamples[f]) == 0) {
+        lx = 255.0f;
+        ly = 0.0f;
+        lz = 0.0f;
+        ok = false;
+    }
+    // max(value, minlight) with minlight 0.
+    lx = lx > 0.0f ? lx : 0.0f;
+    ly = ly > 0.0f ? ly : 0.0f;
+    lz = lz > 0.0f ? lz : 0.0f;
+    lighting[fr.lightofs / 4 + j] = encode(lx, ly, lz);
+    flat[c] = make_float4(lx, ly, lz, ok ? 1.0f : 0.0f);
+}
+
+__device__ void bitonic(float *a, int n) {
+    for (int k = 2; k <= n; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const bool up = (i & k) == 0;
+                    const float x = a[i], y = a[l];
+                    if ((x > y) == up) {
+                        a[i] = y;
+                        a[l] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kMedianThreads) k_median(FinalView v, const float4 *__restrict__ flat,
+                                                           uint32_t *__restrict__ lighting) {
+    __shared__ float ch[3][kMedianMax];
+    __shared__ int count;
+    const int f = blockIdx.x;
+    const Frame fr = load_frame(v.frames, f);
+    const int base = __ldg(&v.face_cells[f]);
+    const int n = fr.w * fr.h;
+    if (threadIdx.x == 0) count = 0;
+    for (int i = threadIdx.x; i < kMedianMax; i += blockDim.x) ch[0][i] = ch[1][i] = ch[2][i] = FLT_MAX;
+    __syncthreads();
+    // Compact the sampled luxels, in luxel order (their order is irrelevant
+    // to a sort, but the count is what the median index uses).
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float4 q = flat[base + i];
+        if (q.w != 0.0f) {
+            const int slot = atomicAdd(&count, 1);
+            ch[0][slot] = q.x;
+            ch[1][slot] = q.y;
+            ch[2][slot] = q.z;
+        }
+    }
+    __syncthreads();
+    bitonic(ch[0], kMedianMax);
+    bitonic(ch[1], kMedianMax);
+    bitonic(ch[2], kMedianMax);
+    if (threadIdx.x == 0) {
+        const int m = count >> 1;
+        const float x = count ? ch[0][m] : 0.0f, y = count ? ch[1][m] : 0.0f, z = count ? ch[2][m] : 0.0f;
+        lighting[fr.lightofs / 4 - 1] = encode(x, y, z);
+    }
+}
+
+}  // namespace
+
+void FinalBuffers::release() {
+    cudaFree(frames);
+    cudaFree(face_cells);
+    cudaFree(face_nsamples);
+    cudaFree(cell_face);
+    cudaFree(cell_sample);
+    cudaFree(sample_box);
+    cudaFree(cand_off);
+    cudaFree(cand_sample);
+    cudaFree(cand_box);
+    cudaFree(rad_light);
+    cudaFree(rad_weight);
+    cudaFree(flat);
+    *this = FinalBuffers();
+}
+
+cudaError_t launch_final(const FinalView &v, const float4 *sample_light, float4 *rad_light, float *rad_weight,
+                         float4 *flat, uint8_t *lighting, int nfaces, cudaStream_t stream) {
+    if (v.ncells == 0) return cudaSuccess;
+    const unsigned grid = (unsigned)((v.ncells + 255) / 256);
+    k_radial<<<grid, 256, 0, stream>>>(v, sample_light, rad_light, rad_weight);
+    k_luxel<<<grid, 256, 0, stream>>>(v, rad_light, rad_weight, reinterpret_cast<uint32_t *>(lighting), flat);
+    k_median<<<nfaces, kMedianThreads, 0, stream>>>(v, flat, reinterpret_cast<uint32_t *>(lighting));
+    return cudaGetLastError();
+}
+
+// Host-side set-up of the final pass from the uploaded world.
+cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces, const vrad_sample *samples,
+                        int64_t nsamples, const float *vertices, int64_t nvertices, std::string &why) {
+    fb.release();
+    std::vector<FaceFrameOut> fr((size_t)nfaces);
+    for (int32_t f = 0; f < nfaces; f++) face_frame_of(faces[f], fr[(size_t)f]);
+    // Neighbours (FaceNeighbours.Build, DefaultSmoothingThreshold).
+    std::vector<int32_t> noff((size_t)nfaces + 1);
+    int64_t nn = 0;
+    if (vrad_build_neighbours(faces, nfaces, vertices, nvertices, 0.7071067f, noff.data(), nullptr, 0, &nn) != VRAD_OK) {
+        why = "invalid face windings";
+        return cudaErrorInvalidValue;
+    }
+    std::vector<int32_t> nlist((size_t)(nn ? nn : 1));
+    vrad_build_neighbours(faces, nfaces, vertices, nvertices, 0.7071067f, noff.data(), nlist.data(), nn, &nn);
+    std::vector<int32_t> lightofs((size_t)nfaces);
+    int64_t total = 0;
+    vrad_lightmap_layout(faces, nfaces, lightofs.data(), &total);
+    // Each face's sample run.
+    std::vector<int64_t> sfirst((size_t)nfaces + 1, 0), scount((size_t)nfaces, 0);
+    for (int64_t i = 0; i < nsamples; i++) scount[(size_t)samples[i].face]++;
+    for (int32_t f = 0; f < nfaces; f++) sfirst[(size_t)f + 1] = sfirst[(size_t)f] + scount[(size_t)f];
+    // Frames, cells, own-sample cell table.
+    std::vector<float4> frames((size_t)nfaces * 5);
+    std::vector<int32_t> face_cells((size_t)nfaces + 1, 0), face_ns((size_t)nfaces);
+    for (int32_t f = 0; f < nfaces; f++) {
+        const FaceFrameOut &q = fr[(size_t)f];
+        if ((int64_t)q.width * q.height > kMedianMax) {
+            why = "a face's lightmap exceeds the 2048 luxels the median sorts on chip";
+            return cudaErrorInvalidValue;
+        }
+        auto bitsf = [](int32_t x) {
+            float y;
+            memcpy(&y, &x, 4);
+            return y;
+        };
+        frames[5 * (size_t)f + 0] = make_float4(q.origin[0], q.origin[1], q.origin[2], bitsf(q.width));
+        frames[5 * (size_t)f + 1] = make_float4(q.w2l_s[0], q.w2l_s[1], q.w2l_s[2], bitsf(q.height));
+        frames[5 * (size_t)f + 2] = make_float4(q.w2l_t[0], q.w2l_t[1], q.w2l_t[2], bitsf(q.min_s));
+        frames[5 * (size_t)f + 3] = make_float4(q.l2w_s[0], q.l2w_s[1], q.l2w_s[2], bitsf(q.min_t));
+        frames[5 * (size_t)f + 4] = make_float4(q.l2w_t[0], q.l2w_t[1], q.l2w_t[2], bitsf(lightofs[(size_t)f]));
+        face_cells[(size_t)f + 1] = face_cells[(size_t)f] + q.width * q.height;
+        face_ns[(size_t)f] = (int32_t)scount[(size_t)f];
+    }
+    const int64_t ncells = face_cells[(size_t)nfaces];
+    std::vector<int32_t> cell_face((size_t)ncells), cell_sample((size_t)ncells, -1);
+    for (int32_t f = 0; f < nfaces; f++)
+        for (int32_t c = face_cells[(size_t)f]; c < face_cells[(size_t)f + 1]; c++) cell_face[(size_t)c] = f;
+    std::vector<float4> sbox((size_t)nsamples);
+    for (int64_t i = 0; i < nsamples; i++) {
+        const vrad_sample &sm = samples[i];
+        const FaceFrameOut &q = fr[(size_t)sm.face];
+        if (sm.s < 0 || sm.s >= q.width || sm.t < 0 || sm.t >= q.height) {
+            why = "a sample's cell lies outside its face's lightmap";
+            return cudaErrorInvalidValue;
+        }
+        cell_sample[(size_t)(face_cells[(size_t)sm.face] + sm.s + sm.t * q.width)] = (int32_t)i;
+        sbox[(size_t)i] = make_float4(sm.mins[0], sm.mins[1], sm.maxs[0], sm.maxs[1]);
+    }
+    // Neighbour candidates: each neighbour's samples whose box, moved into
+    // this face's luxel space as BuildLuxelRadial moves it, can cover a cell.
+    std::vector<int32_t> cand_off((size_t)nfaces + 1, 0), cand_sample;
+    std::vector<float4> cand_box;
+    for (int32_t f = 0; f < nfaces; f++) {
+        const FaceFrameOut &me = fr[(size_t)f];
+        for (int32_t q = noff[(size_t)f]; q < noff[(size_t)f + 1]; q++) {
+            const int32_t g = nlist[(size_t)q];
+            const FaceFrameOut &l = fr[(size_t)g];
+            for (int64_t k = sfirst[(size_t)g]; k < sfirst[(size_t)g + 1]; k++) {
+                const vrad_sample &sm = samples[k];
+                float tmp[3], mins, mint, maxs, maxt;
+                frame_luxel_to_world(l, sm.mins[0], sm.mins[1], tmp);
+                frame_world_to_luxel(me, tmp, mins, mint);
+                frame_luxel_to_world(l, sm.maxs[0], sm.maxs[1], tmp);
+                frame_world_to_luxel(me, tmp, maxs, maxt);
+                int smin = (int)mins, tmin = (int)mint, smax = (int)(maxs + 0.9999f) + 1, tmax = (int)(maxt + 0.9999f) + 1;
+                smin = smin > 0 ? smin : 0;
+                tmin = tmin > 0 ? tmin : 0;
+                smax = smax < me.width ? smax : me.width;
+                tmax = tmax < me.height ? tmax : me.height;
+                if (smin >= smax || tmin >= tmax) continue;
+                cand_sample.push_back((int32_t)k);
+                cand_box.push_back(make_float4(mins, mint, maxs, maxt));
+            }
+        }
+        cand_off[(size_t)f + 1] = (int32_t)cand_sample.size();
+    }
+    auto up = [](auto **dst, const auto &v) {
+        using T = typename std::remove_reference<decltype(v)>::type::value_type;
+        cudaError_t e = cudaMalloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
+        if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+        return e;
+    };
+    cudaError_t e = up(&fb.frames, frames);
+    if (e == cudaSuccess) e = up(&fb.face_cells, face_cells);
+    if (e == cudaSuccess) e = up(&fb.face_nsamples, face_ns);
+    if (e == cudaSuccess) e = up(&fb.cell_face, cell_face);
+    if (e == cudaSuccess) e = up(&fb.cell_sample, cell_sample);
+    if (e == cudaSuccess) e = up(&fb.sample_box, sbox);
+    if (e == cudaSuccess) e = up(&fb.cand_off, cand_off);
+    if (e == cudaSuccess) e = up(&fb.cand_sample, cand_sample);
+    if (e == cudaSuccess) e = up(&fb.cand_box, cand_box);
+    if (e == cudaSuccess) e = cudaMalloc(&fb.rad_light, sizeof(float4) * (size_t)(ncells ? ncells : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&fb.rad_weight, sizeof(float) * (size_t)(ncells ? ncells : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&fb.flat, sizeof(float4) * (size_t)(ncells ? ncells : 1));
+    if (e != cudaSuccess) {
+        fb.release();
+        why = "final-pass buffers";
+        return e;
+    }
+    fb.lighting_bytes = total;
+    fb.nfaces = nfaces;
+    fb.lightofs = lightofs;
+    fb.view = FinalView{fb.frames, fb.face_cells, fb.face_nsamples, fb.cell_face, fb.cell_sample, nullptr,
+                        fb.sample_box, fb.cand_off, fb.cand_sample, fb.cand_box, ncells};
+    fb.ready = true;
+    return cudaSuccess;
+}
+
+}  // namespace vrad
+
+namespace {
+
+int32_t pass_on(vrad_ctx *ctx, uint8_t *d_lighting, cudaStream_t s, cudaEvent_t mid) {
+    if (!ctx->has_scene) return vrad_fail(ctx, VRAD_ERR_NO_SCENE, "no scene uploaded");
+    if (!ctx->world.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no lighting world uploaded");
+    if (!ctx->final_pass.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without face windings");
+    vrad::FinalBuffers &fb = ctx->final_pass;
+    cudaError_t e = cudaMemsetAsync(ctx->world.counters, 0, 2 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess)
+        e = vrad::launch_direct(ctx->scene.view(), ctx->world.view, ctx->sample_light, ctx->world.counters,
+                                ctx->status, s, ctx->world.block);
+    if (e == cudaSuccess && mid) e = cudaEventRecord(mid, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_lighting, 0, (size_t)fb.lighting_bytes, s);
+    if (e == cudaSuccess)
+        e = vrad::launch_final(fb.view, ctx->sample_light, fb.rad_light, fb.rad_weight, fb.flat, d_lighting, fb.nfaces, s);
+    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "light pass launch");
+    return VRAD_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t vrad_lighting_size(vrad_ctx *ctx, int64_t *bytes) {
+    if (!ctx || !bytes) return vrad_fail(ctx, VRAD_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (!ctx->final_pass.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without face windings");
+    *bytes = ctx->final_pass.lighting_bytes;
+    return VRAD_OK;
+}
+
+extern "C" int32_t vrad_light_pass_device(vrad_ctx *ctx, uint8_t *d_lighting, void *stream) {
+    if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
+    if (!d_lighting || ((uintptr_t)d_lighting & 3)) return vrad_fail(ctx, VRAD_ERR_ARG, "lighting buffer null or not 4-byte aligned");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
+    return pass_on(ctx, d_lighting, (cudaStream_t)stream, nullptr);
+}
+
+extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t capacity, int32_t *lightofs,
+                                   vrad_pass_stats *stats) {
+    if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    vrad::FinalBuffers &fb = ctx->final_pass;
+    if (!fb.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without face windings");
+    if (!lighting || capacity < fb.lighting_bytes)
+        return vrad_fail(ctx, VRAD_ERR_ARG, "the LIGHTING lump needs %lld bytes, %lld given", (long long)fb.lighting_bytes,
+                         (long long)capacity);
+    cudaError_t e = cudaSetDevice(ctx->device);
+    uint8_t *d_lighting = nullptr;
+    cudaEvent_t a = nullptr, m = nullptr, b = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&d_lighting, (size_t)(fb.lighting_bytes ? fb.lighting_bytes : 4));
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&m);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    if (e == cudaSuccess) e = cudaEventRecord(a, ctx->stream);
+    int32_t rc = e == cudaSuccess ? pass_on(ctx, d_lighting, ctx->stream, m) : vrad_cuda_fail(ctx, e, "light pass set-up");
+    unsigned long long counts[2] = {0, 0};
+    uint32_t overflow = 0;
+    if (rc == VRAD_OK) {
+        e = cudaEventRecord(b, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(lighting, d_lighting, (size_t)fb.lighting_bytes, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(counts, ctx->world.counters, sizeof counts, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&overflow, ctx->status, sizeof overflow, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = vrad_cuda_fail(ctx, e, "light pass");
+    }
+    if (rc == VRAD_OK && overflow) {
+        cudaMemset(ctx->status, 0, sizeof(uint32_t));
+        rc = vrad_fail(ctx, VRAD_ERR_CUDA, "traversal stack overflow (BVH deeper than %d)", vrad::kStackDepth);
+    }
+    if (rc == VRAD_OK) {
+        if (lightofs)
+            for (int32_t f = 0; f < fb.nfaces; f++) lightofs[f] = fb.lightofs[(size_t)f];
+        if (stats) {
+            float d_ms = 0.0f, f_ms = 0.0f;
+            cudaEventElapsedTime(&d_ms, a, m);
+            cudaEventElapsedTime(&f_ms, m, b);
+            stats->samples = ctx->world.view.nsamples;
+            stats->luxels = fb.view.ncells;
+            stats->visibility_rays = (int64_t)counts[0];
+            stats->sky_rays = (int64_t)counts[1];
+            stats->lighting_bytes = fb.lighting_bytes;
+            stats->direct_ms = d_ms;
+            stats->final_ms = f_ms;
+        }
+    }
+    cudaFree(d_lighting);
+    if (a) cudaEventDestroy(a);
+    if (m) cudaEventDestroy(m);
+    if (b) cudaEventDestroy(b);
+    return rc;
+}

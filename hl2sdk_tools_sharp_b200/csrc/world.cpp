@@ -12,12 +12,14 @@
 // are the reference's bits.  This is set-up, not the hot path: the samples
 // are the input of the device kernels.
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <vector>
 
 #include "../../include/vrad_cuda.h"
+#include "world.h"
 
 namespace {
 
@@ -256,3 +258,139 @@ extern "C" int32_t vrad_build_samples(const vrad_face *faces, int32_t nfaces, co
     *count = written;
     return VRAD_OK;
 }
+
+// ---- smoothing neighbours and the lightmap layout --------------------------
+
+#include <map>
+#include <tuple>
+
+namespace {
+
+inline uint32_t fbits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
+
+}  // namespace
+
+// FaceNeighbours.Build (MapTools/Rad/Light/FaceNeighbours.cs:80-230) for
+// brush faces with smoothing groups 0: faces sharing a vertex are
+// neighbours when the cosine of their normals is at least the threshold
+// (rule 2).  Vertices are identified by position, as a BSP's vertex lump
+// welds them.  Writes offsets[nfaces + 1] and the lists, in discovery order.
+extern "C" int32_t vrad_build_neighbours(const vrad_face *faces, int32_t nfaces, const float *vertices,
+                                         int64_t nvertices, float smoothing_threshold, int32_t *offsets,
+                                         int32_t *list, int64_t capacity, int64_t *count) {
+    if (nfaces < 0 || (nfaces && (!faces || !vertices)) || !offsets || !count) return VRAD_ERR_ARG;
+    // Weld: one vertex number per distinct position.
+    std::map<std::tuple<uint32_t, uint32_t, uint32_t>, int32_t> weld;
+    std::vector<std::vector<int32_t>> face_verts((size_t)nfaces);
+    for (int32_t i = 0; i < nfaces; i++) {
+        const vrad_face &f = faces[i];
+        if (f.first_vertex < 0 || f.first_vertex + (int64_t)f.num_vertices > nvertices) return VRAD_ERR_ARG;
+        for (int32_t k = 0; k < f.num_vertices; k++) {
+            const float *v = vertices + 3 * (int64_t)(f.first_vertex + k);
+            auto key = std::make_tuple(fbits(v[0] + 0.0f), fbits(v[1] + 0.0f), fbits(v[2] + 0.0f));
+            auto it = weld.find(key);
+            int32_t id;
+            if (it == weld.end()) {
+                id = (int32_t)weld.size();
+                weld.emplace(key, id);
+            } else {
+                id = it->second;
+            }
+            face_verts[(size_t)i].push_back(id);
+        }
+    }
+    // vertexFace: the faces touching each vertex, in face order, once each.
+    std::vector<std::vector<int32_t>> vertex_face(weld.size());
+    for (int32_t i = 0; i < nfaces; i++)
+        for (int32_t v : face_verts[(size_t)i]) {
+            auto &vf = vertex_face[(size_t)v];
+            if (std::find(vf.begin(), vf.end(), i) == vf.end()) vf.push_back(i);
+        }
+    int64_t written = 0;
+    for (int32_t i = 0; i < nfaces; i++) {
+        offsets[i] = (int32_t)written;
+        const V3 ni = {faces[i].normal[0], faces[i].normal[1], faces[i].normal[2]};
+        std::vector<int32_t> found;
+        for (int32_t v : face_verts[(size_t)i]) {
+            for (int32_t other : vertex_face[(size_t)v]) {
+                if (other == i) continue;
+                const V3 no = {faces[other].normal[0], faces[other].normal[1], faces[other].normal[2]};
+                const double c = (double)dot(no, ni);
+                if (c < (double)smoothing_threshold) continue;
+                if (std::find(found.begin(), found.end(), other) == found.end()) {
+                    if (found.size() >= 64) return VRAD_ERR_ARG;  // MaxNeighbours
+                    found.push_back(other);
+                }
+            }
+        }
+        for (int32_t o : found) {
+            if (list) {
+                if (written >= capacity) return VRAD_ERR_ARG;
+                list[written] = o;
+            }
+            written++;
+        }
+    }
+    offsets[nfaces] = (int32_t)written;
+    *count = written;
+    return VRAD_OK;
+}
+
+// LightmapOffsets.Compute (MapTools/Rad/Light/LightmapOffsets.cs:54-126)
+// for faces lit in style 0 only (every lit face has style 0): four bytes of
+// median before each face's lightofs, then (w + 1) * (h + 1) luxels.
+extern "C" int32_t vrad_lightmap_layout(const vrad_face *faces, int32_t nfaces, int32_t *lightofs,
+                                        int64_t *total) {
+    if (nfaces < 0 || (nfaces && !faces) || !lightofs || !total) return VRAD_ERR_ARG;
+    int64_t size = 0;
+    for (int32_t f = 0; f < nfaces; f++) {
+        const int lightstyles = 1;
+        size += lightstyles * 4;
+        lightofs[f] = (int32_t)size;
+        const int64_t luxels = (int64_t)(faces[f].lightmap_size[0] + 1) * (faces[f].lightmap_size[1] + 1);
+        size += luxels * 4 * lightstyles;
+    }
+    *total = size;
+    return VRAD_OK;
+}
+
+// ---- frames for the other translation units --------------------------------
+
+namespace vrad {
+
+void face_frame_of(const vrad_face &f, FaceFrameOut &out) {
+    const FaceFrame fr = face_frame(f);
+    const V3 *src[5] = {&fr.origin, &fr.w2l_s, &fr.w2l_t, &fr.l2w_s, &fr.l2w_t};
+    float *dst[5] = {out.origin, out.w2l_s, out.w2l_t, out.l2w_s, out.l2w_t};
+    for (int k = 0; k < 5; k++) {
+        dst[k][0] = src[k]->x;
+        dst[k][1] = src[k]->y;
+        dst[k][2] = src[k]->z;
+    }
+    out.min_s = fr.min_s;
+    out.min_t = fr.min_t;
+    out.width = fr.width;
+    out.height = fr.height;
+}
+
+void frame_luxel_to_world(const FaceFrameOut &fr, float s, float t, float out[3]) {
+    s += (float)fr.min_s;
+    t += (float)fr.min_t;
+    V3 pos = add(V3{fr.origin[0], fr.origin[1], fr.origin[2]}, mul(V3{fr.l2w_s[0], fr.l2w_s[1], fr.l2w_s[2]}, s));
+    pos = add(pos, mul(V3{fr.l2w_t[0], fr.l2w_t[1], fr.l2w_t[2]}, t));
+    out[0] = pos.x;
+    out[1] = pos.y;
+    out[2] = pos.z;
+}
+
+void frame_world_to_luxel(const FaceFrameOut &fr, const float p[3], float &s, float &t) {
+    const V3 pos = sub(V3{p[0], p[1], p[2]}, V3{fr.origin[0], fr.origin[1], fr.origin[2]});
+    s = dot(pos, V3{fr.w2l_s[0], fr.w2l_s[1], fr.w2l_s[2]}) - (float)fr.min_s;
+    t = dot(pos, V3{fr.w2l_t[0], fr.w2l_t[1], fr.w2l_t[2]}) - (float)fr.min_t;
+}
+
+}  // namespace vrad

@@ -1,0 +1,25 @@
+// world.h -- host-side set-up helpers shared between world.cpp and the
+// CUDA files (face luxel frames, neighbour candidate boxes).
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/vrad_cuda.h"
+
+namespace vrad {
+
+// FaceLightInfo's luxel frame (FaceLightInfo.cs:79-160).
+struct FaceFrameOut {
+    float origin[3];
+    float w2l_s[3], w2l_t[3];
+    float l2w_s[3], l2w_t[3];
+    int32_t min_s, min_t, width, height;
+};
+
+void face_frame_of(const vrad_face &f, FaceFrameOut &out);
+
+// LuxelToWorld / WorldToLuxel in the reference's float order.
+void frame_luxel_to_world(const FaceFrameOut &fr, float s, float t, float out[3]);
+void frame_world_to_luxel(const FaceFrameOut &fr, const float p[3], float &s, float &t);
+
+}  // namespace vrad

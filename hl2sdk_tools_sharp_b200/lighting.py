@@ -61,7 +61,13 @@ class _WorldDesc(ctypes.Structure):
                 ("nclusters", ctypes.c_int32), ("sky_directions", ctypes.c_void_p),
                 ("nsky_directions", ctypes.c_int32), ("sun_jitter", ctypes.c_void_p),
                 ("nsun_jitter", ctypes.c_int32), ("sun_angular_extent", ctypes.c_float),
-                ("sun_samples", ctypes.c_int32)]
+                ("sun_samples", ctypes.c_int32), ("vertices", ctypes.c_void_p), ("nvertices", ctypes.c_int64)]
+
+
+class PassStats(ctypes.Structure):
+    _fields_ = [("samples", ctypes.c_int64), ("luxels", ctypes.c_int64), ("visibility_rays", ctypes.c_int64),
+                ("sky_rays", ctypes.c_int64), ("lighting_bytes", ctypes.c_int64), ("direct_ms", ctypes.c_float),
+                ("final_ms", ctypes.c_float)]
 
 
 class DirectStats(ctypes.Structure):
@@ -83,6 +89,16 @@ def _lib():
         lib.vrad_direct_lighting_device.restype = i32
         lib.vrad_direct_autotune.argtypes = [P, ctypes.POINTER(i32), P]
         lib.vrad_direct_autotune.restype = i32
+        lib.vrad_build_neighbours.argtypes = [P, i32, P, i64, ctypes.c_float, P, P, i64, ctypes.POINTER(i64)]
+        lib.vrad_build_neighbours.restype = i32
+        lib.vrad_lightmap_layout.argtypes = [P, i32, P, ctypes.POINTER(i64)]
+        lib.vrad_lightmap_layout.restype = i32
+        lib.vrad_lighting_size.argtypes = [P, ctypes.POINTER(i64)]
+        lib.vrad_lighting_size.restype = i32
+        lib.vrad_light_pass.argtypes = [P, P, i64, P, ctypes.POINTER(PassStats)]
+        lib.vrad_light_pass.restype = i32
+        lib.vrad_light_pass_device.argtypes = [P, P, P]
+        lib.vrad_light_pass_device.restype = i32
         lib._lighting_bound = True
     return lib
 
@@ -126,6 +142,36 @@ def build_samples(faces: np.ndarray, verts: np.ndarray):
     if rc != 0:
         raise ValueError(f"vrad_build_samples failed ({rc})")
     return out, first
+
+
+def build_neighbours(faces: np.ndarray, verts: np.ndarray, threshold: float = 0.7071067):
+    """vrad_build_neighbours (native): CSR offsets and lists."""
+    lib = _lib()
+    faces = np.ascontiguousarray(faces, FACE_DTYPE)
+    verts = np.ascontiguousarray(verts, np.float32)
+    off = np.zeros(len(faces) + 1, np.int32)
+    count = ctypes.c_int64()
+    rc = lib.vrad_build_neighbours(faces.ctypes.data, len(faces), verts.ctypes.data, len(verts), threshold,
+                                   off.ctypes.data, None, 0, ctypes.byref(count))
+    if rc != 0:
+        raise ValueError(f"vrad_build_neighbours failed ({rc})")
+    lst = np.zeros(max(1, count.value), np.int32)
+    rc = lib.vrad_build_neighbours(faces.ctypes.data, len(faces), verts.ctypes.data, len(verts), threshold,
+                                   off.ctypes.data, lst.ctypes.data, count.value, ctypes.byref(count))
+    if rc != 0:
+        raise ValueError(f"vrad_build_neighbours failed ({rc})")
+    return off, lst[:count.value]
+
+
+def lightmap_layout(faces: np.ndarray):
+    """vrad_lightmap_layout: (lightofs per face, LIGHTING size)."""
+    faces = np.ascontiguousarray(faces, FACE_DTYPE)
+    ofs = np.zeros(len(faces), np.int32)
+    total = ctypes.c_int64()
+    rc = _lib().vrad_lightmap_layout(faces.ctypes.data, len(faces), ofs.ctypes.data, ctypes.byref(total))
+    if rc != 0:
+        raise ValueError(f"vrad_lightmap_layout failed ({rc})")
+    return ofs, total.value
 
 
 # ---------------------------------------------------------------- lights
@@ -269,11 +315,12 @@ class LightingStage:
     def upload_world(self, i: LightingInputs) -> None:
         """vrad_world_upload: faces, samples, lights, cluster lists, tables."""
         keep = [np.ascontiguousarray(a) for a in (i.faces, i.samples, i.lights, i.cluster_offsets,
-                                                  i.cluster_lights, i.sky_directions, i.sun_jitter)]
-        f, s, l, off, cl, dirs, jit = keep
+                                                  i.cluster_lights, i.sky_directions, i.sun_jitter, i.verts)]
+        f, s, l, off, cl, dirs, jit, vv = keep
         d = _WorldDesc(f.ctypes.data, len(f), s.ctypes.data, len(s), l.ctypes.data, len(l),
                        off.ctypes.data, cl.ctypes.data, len(off) - 1, dirs.ctypes.data, len(dirs),
-                       jit.ctypes.data if len(jit) else None, len(jit), i.sun_angular_extent, i.sun_samples)
+                       jit.ctypes.data if len(jit) else None, len(jit), i.sun_angular_extent, i.sun_samples,
+                       vv.ctypes.data, len(vv))
         T._check(_lib().vrad_world_upload(self._ctx, ctypes.byref(d)), self._ctx)
         self.inputs = i
 
@@ -300,6 +347,28 @@ class LightingStage:
         times = np.zeros(3, np.float32)
         T._check(_lib().vrad_direct_autotune(self._ctx, ctypes.byref(chosen), times.ctypes.data), self._ctx)
         return chosen.value, {32: float(times[0]), 64: float(times[1]), 128: float(times[2])}
+
+    def lighting_size(self) -> int:
+        n = ctypes.c_int64()
+        T._check(_lib().vrad_lighting_size(self._ctx, ctypes.byref(n)), self._ctx)
+        return n.value
+
+    def light_pass(self, lighting: np.ndarray | None = None):
+        """vrad_light_pass (bounce 0): the LIGHTING lump bytes, each face's
+        lightofs, and the stats."""
+        if lighting is None:
+            lighting = np.zeros(self.lighting_size(), np.uint8)
+        ofs = np.zeros(len(self.inputs.faces), np.int32)
+        st = PassStats()
+        T._check(_lib().vrad_light_pass(self._ctx, lighting.ctypes.data, len(lighting), ofs.ctypes.data,
+                                        ctypes.byref(st)), self._ctx)
+        return lighting, ofs, st
+
+    def light_pass_device(self, d_lighting, stream=None):
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        T._check(_lib().vrad_light_pass_device(self._ctx, d_lighting.data_ptr(), ctypes.c_void_p(s)), self._ctx)
+        return d_lighting
 
     def direct_into(self, out: np.ndarray):
         """vrad_direct_lighting into a caller's host buffer (LIGHTING_DTYPE)."""

@@ -237,6 +237,8 @@ typedef struct vrad_world_desc {
     int32_t nsun_jitter;
     float sun_angular_extent;
     int32_t sun_samples;
+    const float *vertices;                 /* face windings, xyz each (vrad_face.first_vertex) */
+    int64_t nvertices;
 } vrad_world_desc;
 
 typedef struct vrad_direct_stats {
@@ -254,6 +256,20 @@ int32_t vrad_build_samples(const vrad_face *faces, int32_t nfaces, const float *
                            int64_t nvertices, vrad_sample *out, int64_t capacity, int64_t *count,
                            int64_t *face_first);
 
+/* FaceNeighbours.Build (MapTools/Rad/Light/FaceNeighbours.cs:80-230) for
+ * brush faces with smoothing groups 0: faces sharing a vertex position are
+ * neighbours when the cosine of their normals is at least
+ * smoothing_threshold (the reference's default is 0.7071067).  offsets has
+ * nfaces + 1 entries; with list = NULL it only counts.  Host-side set-up. */
+int32_t vrad_build_neighbours(const vrad_face *faces, int32_t nfaces, const float *vertices,
+                              int64_t nvertices, float smoothing_threshold, int32_t *offsets,
+                              int32_t *list, int64_t capacity, int64_t *count);
+
+/* LightmapOffsets.Compute (MapTools/Rad/Light/LightmapOffsets.cs:54-126)
+ * for faces lit in style 0: each face's lightofs (its median's four bytes
+ * sit just before it) and the LIGHTING lump's total size.  Host-side. */
+int32_t vrad_lightmap_layout(const vrad_face *faces, int32_t nfaces, int32_t *lightofs, int64_t *total);
+
 /* Uploads the lighting world to the context's device (kept until the next
  * upload or vrad_destroy).  The scene (vrad_scene_upload) is the shadow
  * casters.  VRAD_ERR_UNSUPPORTED for a surface light (type 0) or for a
@@ -266,6 +282,34 @@ int32_t vrad_direct_lighting(vrad_ctx *ctx, vrad_lighting_value *out, vrad_direc
 
 /* The same into a device buffer on `stream` (NULL = default stream). */
 int32_t vrad_direct_lighting_device(vrad_ctx *ctx, vrad_lighting_value *d_out, void *stream);
+
+typedef struct vrad_pass_stats {
+    int64_t samples;
+    int64_t luxels;
+    int64_t visibility_rays;
+    int64_t sky_rays;
+    int64_t lighting_bytes;
+    float direct_ms;
+    float final_ms;
+} vrad_pass_stats;
+
+/* Size in bytes of the LIGHTING lump the uploaded world produces
+ * (LightmapOffsets.Compute's LightDataSize). */
+int32_t vrad_lighting_size(vrad_ctx *ctx, int64_t *bytes);
+
+/* The lighting stage with -bounce 0 (the reference's Vrad.RunPassAsync
+ * without the bounce, MapTools/Rad/Vrad.cs:392-530): the direct gather, then
+ * FinalLightFace for every face (LuxelRadial filter over the face's own and
+ * its smoothing neighbours' samples, minlight, StockLightColor.Encode, the
+ * per-face median), written as the LIGHTING lump's bytes.  lighting must
+ * hold vrad_lighting_size bytes (bytes no face owns are zero); lightofs
+ * (nfaces entries, nullable) receives each face's FACES lightofs; styles
+ * are 0 then 255 for every lit face.  Host buffers; blocks. */
+int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t capacity, int32_t *lightofs,
+                        vrad_pass_stats *stats);
+
+/* The same into a device buffer on `stream` (NULL = default stream). */
+int32_t vrad_light_pass_device(vrad_ctx *ctx, uint8_t *d_lighting, void *stream);
 
 /* Times the gather once per launch shape (32, 64 and 128 threads per CTA)
  * on the uploaded world and keeps the fastest for later calls; times_ms

@@ -61,6 +61,10 @@ def lib() -> ctypes.CDLL:
         _lib.orc_build_samples.restype = ctypes.c_int
         _lib.orc_direct.argtypes = [P, P, P, P, P, i32, P, P, P, P, P, P, i32, P, i32, f32, P, i32, P]
         _lib.orc_direct.restype = ctypes.c_int
+        _lib.orc_neighbours.argtypes = [P, i32, P, f32, P, P, ctypes.c_int64, P]
+        _lib.orc_neighbours.restype = ctypes.c_int
+        _lib.orc_final.argtypes = [P, i32, P, P, P, P, P, ctypes.c_int64, P, P]
+        _lib.orc_final.restype = ctypes.c_int
         if hasattr(_lib, "orc_kd_build"):
             _lib.orc_kd_build.argtypes = [P, P, P, i32, P]
             _lib.orc_kd_build.restype = ctypes.c_int
@@ -229,3 +233,34 @@ def direct(tree: dict, faces, samples, face_first, lights, cl_off, cl_list, dirs
     if rc != 0:
         raise RuntimeError(f"orc_direct failed: {rc}")
     return (out, rays.value) if count_rays else out
+
+
+def neighbours(faces, verts, threshold: float = 0.7071067):
+    faces = np.ascontiguousarray(faces)
+    verts = np.ascontiguousarray(verts, np.float32)
+    off = np.zeros(len(faces) + 1, np.int32)
+    count = ctypes.c_int64()
+    lib().orc_neighbours(_p(faces), len(faces), _p(verts), threshold, _p(off), None, 0, ctypes.byref(count))
+    lst = np.zeros(max(1, count.value), np.int32)
+    lib().orc_neighbours(_p(faces), len(faces), _p(verts), threshold, _p(off), _p(lst), count.value,
+                         ctypes.byref(count))
+    return off, lst[:count.value]
+
+
+def final(faces, verts, samples, face_first, sample_light):
+    """FinalLightFace restated: (LIGHTING bytes, lightofs)."""
+    faces = np.ascontiguousarray(faces)
+    verts = np.ascontiguousarray(verts, np.float32)
+    samples = np.ascontiguousarray(samples)
+    face_first = np.ascontiguousarray(face_first, np.int64)
+    light = np.ascontiguousarray(sample_light, np.float32).reshape(-1, 4)
+    total = ctypes.c_int64()
+    ofs = np.zeros(len(faces), np.int32)
+    lib().orc_final(_p(faces), len(faces), _p(verts), _p(samples), _p(face_first), _p(light), None, 0,
+                    _p(ofs), ctypes.byref(total))
+    out = np.zeros(total.value, np.uint8)
+    rc = lib().orc_final(_p(faces), len(faces), _p(verts), _p(samples), _p(face_first), _p(light), _p(out),
+                         len(out), _p(ofs), ctypes.byref(total))
+    if rc != 0:
+        raise RuntimeError(f"orc_final failed: {rc}")
+    return out, ofs

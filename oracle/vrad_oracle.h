@@ -149,6 +149,17 @@ int orc_direct(const orc_kdnode *nodes, const int32_t *indices, const orc_tri *t
                const float *jitter, int32_t sun_samples, float sun_extent, float *out,
                int32_t threads, int64_t *rays_out);
 
+/* FaceNeighbours.Build for smoothing groups 0 (vertices welded by position). */
+int orc_neighbours(const orc_face *faces, int32_t nfaces, const float *verts, float threshold,
+                   int32_t *offsets, int32_t *list, int64_t capacity, int64_t *count);
+
+/* FinalLightFace for every face, bounce 0: the LIGHTING lump bytes (total
+ * size in *total; lighting may be NULL to size it) and each face's lightofs.
+ * sample_light is the direct gather's output, 4 floats per sample. */
+int orc_final(const orc_face *faces, int32_t nfaces, const float *verts, const orc_sample *samples,
+              const int64_t *face_first, const float *sample_light, uint8_t *lighting,
+              int64_t capacity, int32_t *lightofs, int64_t *total);
+
 #ifdef __cplusplus
 }
 #endif

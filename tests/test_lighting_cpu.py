@@ -56,3 +56,44 @@ def test_light_list_order_and_falloff():
         lst = flat[off[c]:off[c + 1]]
         assert len(lights) - 1 in lst and len(lights) - 2 in lst
         assert list(lst) == sorted(lst)
+
+
+@pytest.mark.parametrize("cfg", [rg.config_3x3(seed=2), rg.config_8x8(seed=1)], ids=["3x3", "8x8"])
+def test_neighbours_match_the_oracle(oracle_mod, cfg):
+    w = rg.generate(cfg)
+    faces, verts = L.faces_of(w)
+    off, lst = L.build_neighbours(faces, verts)
+    woff, wlst = oracle_mod.neighbours(faces, verts)
+    assert np.array_equal(off, woff) and np.array_equal(lst, wlst)
+    assert len(lst) > 0
+
+
+def test_layout_puts_the_median_before_lightofs():
+    w = rg.generate(rg.config_3x3(seed=2))
+    faces, _ = L.faces_of(w)
+    ofs, total = L.lightmap_layout(faces)
+    luxels = (faces["lightmap_size"][:, 0] + 1) * (faces["lightmap_size"][:, 1] + 1)
+    assert ofs[0] == 4
+    assert np.array_equal(np.diff(ofs), 4 * luxels[:-1] + 4)
+    assert total == ofs[-1] + 4 * luxels[-1]
+
+
+def test_oracle_encode_known_values(oracle_mod):
+    # StockLightColor.Encode: 1.0 -> exponent -7, mantissa 128 (1 * 2^7);
+    # 0 -> all zero; 255 -> exponent 0, 255.
+    import ctypes
+    faces = np.zeros(1, L.FACE_DTYPE)
+    faces["normal"] = (0, 0, 1)
+    faces["lightmap_vecs"][0, 0] = (1, 0, 0, 0)
+    faces["lightmap_vecs"][0, 1] = (0, 1, 0, 0)
+    faces["lightmap_size"] = (1, 1)
+    faces["first_vertex"] = 0
+    faces["num_vertices"] = 4
+    verts = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0]], np.float32)
+    samples, first = L.build_samples(faces, verts)
+    assert len(samples) == 1
+    for value, word in ((1.0, (128, 128, 128, -7)), (0.0, (0, 0, 0, 0)), (255.0, (255, 255, 255, 0))):
+        light = np.full((1, 4), value, np.float32)
+        lump, _ = oracle_mod.final(faces, verts, samples, first, light)
+        px = lump[4:8].view(np.int8)
+        assert tuple(int(x) & 0xFF for x in px[:3]) == word[:3] and int(px[3]) == word[3], (value, px)
