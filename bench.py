@@ -567,7 +567,7 @@ def main_stage(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded room grid)",
-            "config": {"workload": "8x8 room grid direct-lighting stage (64 point/spot lights, sun, 162-dir sky)",
+            "config": {"workload": "8x8 room grid lighting stage, bounce 0 (64 point/spot lights, sun, 162-dir sky; direct gather + final pass)",
                        "side": args.side, "seed": CONFIG_SEED, "samples": n, "faces": int(len(inp.faces)),
                        "triangles": info.triangles, "lights": int(len(inp.lights)),
                        "rays_per_step": rays_per_step,
