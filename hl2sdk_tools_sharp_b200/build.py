@@ -39,7 +39,7 @@ def stale() -> bool:
     if not LIB.exists():
         return True
     t = LIB.stat().st_mtime
-    deps = sources() + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "vrad_cuda.h", pathlib.Path(__file__)]
+    deps = sources() + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [ROOT / "include" / "vrad_cuda.h", pathlib.Path(__file__)]
     return any(p.stat().st_mtime > t for p in deps)
 
 

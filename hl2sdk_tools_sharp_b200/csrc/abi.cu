@@ -219,6 +219,7 @@ int32_t vrad_destroy(vrad_ctx *ctx) {
         ctx->scene.release();
         ctx->world.release();
         ctx->final_pass.release();
+        ctx->bounce.release();
         cudaFree(ctx->sample_light);
         cudaFree(ctx->status);
         cudaFree(ctx->d_rays);

@@ -1,0 +1,565 @@
+// bounce.cu -- the radiosity bounce: the patches' direct light, the
+// transfers (candidate pairs, their rays and form factors), the bounces,
+// and the tables the final pass reads the bounced light through.
+//
+// Reference behaviour restated (muflub/hl2sdk_tools_sharp, MapTools/Rad):
+//   PatchLighting.BuildPatchLights / AddSampleToPatch  Light/PatchLighting.cs:65-249
+//   Radiosity.MoveDirectLightToEmission / GatherLight /
+//             CollectLight / BounceAsync               Bounce/Radiosity.cs:132-316
+//   VisMatrix.ReceiverOrder / FacesInRow / Enumerator.Run /
+//             TestPatchToFace / TestPatchToPatch /
+//             TransferRay / MakeTransfers / MakeTransfer /
+//             MakeScales                               Bounce/VisMatrix.cs:180-1004
+//   FormFactors.DiffToDiff / PolyToDiff                Bounce/FormFactors.cs:58-140
+//   DetMathF.Asin (correctly rounded)                  MapFormats/Numerics/DetMathF.cs:141-164
+//   FinalLightFace.BuildPatchRadial / AddFacePatches /
+//             PatchLightmapCoordRange                  Final/FinalLightFace.cs:393-540
+// with the reference's default settings: no compliance quirks (the
+// receiver's plane normal in the plane test, true divides in the transfer
+// rays, sines above one clamped), the exact normalise, bounces > 0.
+//
+// Every float operation of those routines is an explicitly rounded
+// intrinsic, in the reference's association order, and every sum runs in
+// the reference's order, so the transfers, the patch light and the stop
+// decision are the reference's bits.
+//
+// Kernels of one light pass (after the direct gather):
+//   k_patch_samples   one thread per patch: the face's samples that overlap
+//                     it, in sample order (AddSampleToPatch)
+//   k_patch_tree      one thread per face: pushes, averages and area blends
+//                     over the face's patch list, then the move to emission
+//   k_candidates      one thread per receiver: the candidate sources in the
+//                     enumerator's order (a counting and a writing launch)
+//   k_transfer        one thread per candidate: the transfer ray, traced
+//                     in-thread, and MakeTransfer for an open pair
+//   k_transfer_count / k_transfer_write  one warp per receiver: the
+//                     accepted pairs compacted in order, capped at
+//                     MaxPatches, and MakeScales' ordered sum
+//   k_gather          one thread per receiver: GatherLight's ordered sum,
+//                     then CollectLight's leaf update
+//   k_collect         one thread per face: CollectLight's parents, bottom up
+//   k_totals          fp64 sums of the light a bounce added, with absolute
+//                     sums that bound the reference's float sum
+//   k_exact_total     one thread: the reference's sequential float sum, run
+//                     only when the bound cannot settle the stop rule
+
+#include <cuda_runtime.h>
+
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bounce.cuh"
+#include "context.cuh"
+#include "detmath.cuh"
+#include "patches.h"
+#include "traverse.cuh"
+#include "world.h"
+
+namespace vrad {
+
+namespace {
+
+constexpr int kBounceBlock = 128;
+constexpr int kEnumStack = 64;  // patch tree depth the candidate walk holds
+
+// ---- float and double-double helpers ----------------------------------------
+
+struct F3 {
+    float x, y, z;
+};
+__device__ __forceinline__ F3 f3(const float4 &a) { return {a.x, a.y, a.z}; }
+__device__ __forceinline__ F3 add3(F3 a, F3 b) { return {__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)}; }
+__device__ __forceinline__ F3 sub3(F3 a, F3 b) { return {__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)}; }
+__device__ __forceinline__ F3 mul3(F3 a, float s) { return {__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s)}; }
+__device__ __forceinline__ float dot3(F3 a, F3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ F3 cross3(F3 a, F3 b) {
+    return {__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+            __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x))};
+}
+// Vec3.Normalise: exact length, three true divides, zero for zero.
+__device__ __forceinline__ F3 normalise3(F3 a, float &len) {
+    len = __fsqrt_rn(dot3(a, a));
+    if (len == 0.0f) return {0.0f, 0.0f, 0.0f};
+    return {__fdiv_rn(a.x, len), __fdiv_rn(a.y, len), __fdiv_rn(a.z, len)};
+}
+
+// ---- the patches' direct light ----------------------------------------------
+
+// AddSampleToPatch for one patch over its face's samples, in sample order:
+// acc = (sample light * area summed, sample area summed).
+__global__ void k_patch_samples(BounceView v, const float4 *__restrict__ sample_light, float4 *__restrict__ acc) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= v.npatches) return;
+    const int4 tr = __ldg(&v.tree[p]);
+    float lx = 0.0f, ly = 0.0f, lz = 0.0f, area = 0.0f;
+    if (tr.y == -1 && tr.w == 0) {
+        const float4 mn = __ldg(&v.mins[p]), mx = __ldg(&v.maxs[p]);
+        const int f = __float_as_int(mn.w);
+        const int2 fs = __ldg(&v.face_samples[f]);
+        for (int k = fs.x; k < fs.x + fs.y; k++) {
+            const float4 L = __ldg(&sample_light[k]);
+            // VectorAvg: a float divide by 3.
+            if (__fdiv_rn(__fadd_rn(__fadd_rn(L.x, L.y), L.z), 3.0f) < 1.0f) continue;
+            const float a = __ldg(&v.sample_area[k]);
+            const float4 P = __ldg(&v.sample_pos[k]);
+            const float radius = (float)__ddiv_rn((double)__fsqrt_rn(a), 2.0);
+            if (mn.x > __fadd_rn(P.x, radius) || mx.x < __fsub_rn(P.x, radius)) continue;
+            if (mn.y > __fadd_rn(P.y, radius) || mx.y < __fsub_rn(P.y, radius)) continue;
+            if (mn.z > __fadd_rn(P.z, radius) || mx.z < __fsub_rn(P.z, radius)) continue;
+            area = __fadd_rn(area, a);
+            lx = __fadd_rn(lx, __fmul_rn(a, L.x));
+            ly = __fadd_rn(ly, __fmul_rn(a, L.y));
+            lz = __fadd_rn(lz, __fmul_rn(a, L.z));
+        }
+    }
+    acc[p] = make_float4(lx, ly, lz, area);
+}
+
+// The face's patch list (FacePatches after RebuildFaceLists): its
+// descendants in descending index order, then its root.
+struct FaceList {
+    int root, first, end;
+    __device__ __forceinline__ int count() const { return root < 0 ? 0 : end - first + 1; }
+    __device__ __forceinline__ int at(int k) const { return k < end - first ? end - 1 - k : root; }
+};
+
+// BuildPatchLights after the samples (pushes to parents, averages, area
+// blends), then MoveDirectLightToEmission for the face's patches.
+__global__ void k_patch_tree(BounceView v, float4 *__restrict__ acc, float4 *__restrict__ direct,
+                             float4 *__restrict__ total, float4 *__restrict__ emit, float4 *__restrict__ shoot) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= v.nfaces) return;
+    const int4 fr = __ldg(&v.face_range[f]);
+    const FaceList L{fr.x, fr.y, fr.z};
+    const int n = L.count();
+    for (int k = 0; k < n; k++) {
+        const int p = L.at(k);
+        const int parent = __ldg(&v.tree[p].x);
+        if (parent == -1) continue;
+        const float4 a = acc[p], b = acc[parent];
+        acc[parent] = make_float4(__fadd_rn(b.x, a.x), __fadd_rn(b.y, a.y), __fadd_rn(b.z, a.z), __fadd_rn(b.w, a.w));
+    }
+    for (int k = 0; k < n; k++) {
+        const int p = L.at(k);
+        const float4 a = acc[p];
+        float4 t = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (a.w != 0.0f) {
+            const float scale = (float)__drcp_rn((double)a.w);
+            t = make_float4(__fadd_rn(0.0f, __fmul_rn(a.x, scale)), __fadd_rn(0.0f, __fmul_rn(a.y, scale)),
+                            __fadd_rn(0.0f, __fmul_rn(a.z, scale)), 0.0f);
+        }
+        total[p] = t;
+        direct[p] = t;
+    }
+    for (int k = 0; k < n; k++) {
+        const int p = L.at(k);
+        const int4 tr = __ldg(&v.tree[p]);
+        if (tr.y == -1) continue;
+        const float a1 = __ldg(&v.origin[tr.y].w), a2 = __ldg(&v.origin[tr.z].w);
+        const float s1 = __fdiv_rn(a1, __fadd_rn(a1, a2)), s2 = __fdiv_rn(a2, __fadd_rn(a1, a2));
+        const float4 c1 = total[tr.y], c2 = total[tr.z];
+        const float4 t = make_float4(__fadd_rn(__fmul_rn(c1.x, s1), __fmul_rn(c2.x, s2)),
+                                     __fadd_rn(__fmul_rn(c1.y, s1), __fmul_rn(c2.y, s2)),
+                                     __fadd_rn(__fmul_rn(c1.z, s1), __fmul_rn(c2.z, s2)), 0.0f);
+        total[p] = t;
+        direct[p] = t;
+    }
+    for (int k = 0; k < n; k++) {
+        const int p = L.at(k);
+        const float4 e = total[p], r = __ldg(&v.refl[p]);
+        emit[p] = e;
+        shoot[p] = make_float4(__fmul_rn(e.x, r.x), __fmul_rn(e.y, r.y), __fmul_rn(e.z, r.z), 0.0f);
+        total[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+// ---- transfers ---------------------------------------------------------------
+
+// Enumerator.Run for one receiver: the faces of its cluster's PVS row
+// other than its own, each tested with TestPatchToFace, then its patch
+// tree walked as TestPatchToPatch recurses (child1's subtree before
+// child2's).  Counts (out == nullptr) or writes the candidates.
+__global__ void k_candidates(BounceView v, const int64_t *__restrict__ cand_off, int64_t *__restrict__ counts,
+                             int32_t *__restrict__ out, uint32_t *__restrict__ overflow) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= v.nreceivers) return;
+    const int p = __ldg(&v.recv[r]);
+    const F3 o = f3(__ldg(&v.origin[p]));
+    const float4 mn = __ldg(&v.mins[p]), mx = __ldg(&v.maxs[p]);
+    const int face = __float_as_int(mn.w), cluster = __float_as_int(mx.w);
+    const float4 pl = __ldg(&v.face_plane[face]);
+    const F3 me_n = {pl.x, pl.y, pl.z};
+    const double me_d = (double)__ldg(&v.normal[p].w) + 0.01;
+    int64_t n = 0;
+    int64_t at = out ? cand_off[r] : 0;
+    int stack[kEnumStack];
+    const int q0 = __ldg(&v.row_off[cluster]), q1 = __ldg(&v.row_off[cluster + 1]);
+    for (int q = q0; q < q1; q++) {
+        const int g = __ldg(&v.row_faces[q]);
+        if (g == face) continue;
+        const int root = __ldg(&v.face_range[g].x);
+        if (root < 0) continue;
+        const float4 rn = __ldg(&v.normal[root]);
+        if (!((double)dot3(o, f3(rn)) > (double)rn.w + 0.01)) continue;
+        int sp = 0;
+        stack[sp++] = root;
+        while (sp > 0) {
+            const int s = stack[--sp];
+            const int4 tr = __ldg(&v.tree[s]);
+            const float4 so = __ldg(&v.origin[s]);
+            if (tr.y != -1) {
+                const F3 d = sub3(o, f3(so));
+                if ((double)dot3(d, d) * 0.0625 < (double)so.w) {
+                    if (sp + 2 > kEnumStack) {
+                        atomicOr(overflow, 2u);
+                        continue;
+                    }
+                    stack[sp++] = tr.z;
+                    stack[sp++] = tr.y;
+                    continue;
+                }
+            }
+            if ((double)dot3(f3(so), me_n) > me_d) {
+                if (out) out[at] = s;
+                at++;
+                n++;
+            }
+        }
+    }
+    if (!out) counts[r] = n;
+}
+
+// FormFactors.PolyToDiff of source s's winding seen from (o, n).
+__device__ float poly_to_diff(const BounceView &v, int s, float area, F3 o, F3 n, unsigned long long *open) {
+    const int2 w = __ldg(&v.wind[s]);
+    float ff = 0.0f;
+    for (int k = 0; k < w.y; k++) {
+        const int k2 = k < w.y - 1 ? k + 1 : 0;
+        float l;
+        const F3 v1 = normalise3(sub3(f3(__ldg(&v.points[w.x + k])), o), l);
+        const F3 v2 = normalise3(sub3(f3(__ldg(&v.points[w.x + k2])), o), l);
+        float sin_alpha;
+        F3 gamma = normalise3(cross3(v1, v2), sin_alpha);
+        if (sin_alpha < -1.0f || sin_alpha > 1.0f) sin_alpha = sin_alpha > 1.0f ? 1.0f : -1.0f;
+        gamma = mul3(gamma, asin_cr(sin_alpha, open));
+        ff = __fadd_rn(ff, dot3(gamma, n));
+    }
+    return __fmul_rn(ff, __fdiv_rn(0.5f, area));
+}
+
+// One candidate pair: VisMatrix.TransferRay traced (StockExact: every
+// triangle blocks, t in (0, len)), then MakeTransfer.  cand_w = the
+// transfer, 0 for none.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_transfer(BounceView v, DeviceScene sc, const int64_t *__restrict__ cand_off,
+                                                    const int32_t *__restrict__ cand_src, float *__restrict__ cand_w,
+                                                    int64_t ncand, unsigned long long *counters, uint32_t *overflow) {
+    __shared__ int stack_mem[kStackDepth * BLOCK];
+    int *stack = stack_mem + threadIdx.x;
+    const int64_t q = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
+    const bool live = q < ncand;
+    float w = 0.0f;
+    bool blocked = false;
+    if (live) {
+        // The receiver whose run holds q.
+        int lo = 0, hi = v.nreceivers;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (__ldg(&cand_off[mid]) <= q) lo = mid;
+            else hi = mid;
+        }
+        const int p = __ldg(&v.recv[lo]);
+        const int s = __ldg(&cand_src[q]);
+        const float4 po = __ldg(&v.origin[p]), pn = __ldg(&v.normal[p]);
+        const float4 so = __ldg(&v.origin[s]), sn = __ldg(&v.normal[s]);
+        const F3 start = add3(f3(po), f3(pn)), end = add3(f3(so), f3(sn));
+        const F3 delta = sub3(end, start);
+        const float len = __fsqrt_rn(dot3(delta, delta));
+        const float safe = len == 0.0f ? 1.1920929e-07f : len;
+        const RayState ray = make_ray(start.x, start.y, start.z, __fdiv_rn(delta.x, safe), __fdiv_rn(delta.y, safe),
+                                      __fdiv_rn(delta.z, safe));
+        float t;
+        int32_t orig;
+        uint32_t meta;
+        trace_ray<kModeAny, BLOCK>(sc, ray, 0.0f, len, -1, stack, overflow, blocked, t, orig, meta);
+        if (!blocked && __ldg(&v.tree[s].w) == 0 && so.w > 0.0f) {
+            // MakeTransfer: DiffToDiff(source, receiver), the polygon form
+            // factor for a near source, trans = area * scale > 1e-7.
+            float dl;
+            const F3 d = normalise3(sub3(f3(so), f3(po)), dl);
+            float scale = __fdiv_rn(__fmul_rn(-dot3(d, f3(sn)), dot3(d, f3(pn))), __fmul_rn(dl, dl));
+            if (!(scale <= 0.0f)) {
+                const F3 dd = sub3(f3(po), f3(so));
+                const float threshold = (float)__dmul_rn(3.141592653589793 * 0.04, (double)dot3(dd, dd));
+                bool ok = true;
+                if (threshold < so.w) {
+                    scale = poly_to_diff(v, s, so.w, f3(po), f3(pn), &counters[2]);
+                    ok = !(scale <= 0.0f);
+                }
+                if (ok) {
+                    const float trans = __fmul_rn(so.w, scale);
+                    if ((double)trans > 0.0000001) w = trans;
+                }
+            }
+        }
+        cand_w[q] = w;
+    }
+    // Ray counts: one warp add each.
+    const unsigned lane = threadIdx.x & 31;
+    const int nlive = __popc(__ballot_sync(kFull, live));
+    const int nblocked = __popc(__ballot_sync(kFull, live && blocked));
+    if (lane == 0) {
+        if (nlive) atomicAdd(&counters[0], (unsigned long long)nlive);
+        if (nblocked) atomicAdd(&counters[1], (unsigned long long)nblocked);
+    }
+}
+
+// MakeTransfers' count per receiver: accepted pairs, at most MaxPatches.
+__global__ void k_transfer_count(int nrecv, const int64_t *__restrict__ cand_off, const float *__restrict__ cand_w,
+                                 int64_t *__restrict__ counts) {
+    const int r = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const unsigned lane = threadIdx.x & 31;
+    if (r >= nrecv) return;
+    const int64_t a = cand_off[r], b = cand_off[r + 1];
+    int64_t n = 0;
+    for (int64_t base = a; base < b; base += 32) {
+        const int64_t q = base + lane;
+        n += __popc(__ballot_sync(kFull, q < b && cand_w[q] > 0.0f));
+    }
+    if (lane == 0) counts[r] = n < kMaxTransfersPerReceiver ? n : kMaxTransfersPerReceiver;
+}
+
+// MakeTransfers' writes in candidate order (the first MaxPatches), then
+// MakeScales: the float sum in order, total > pi ? 1/total : 1/pi, and the
+// weights scaled.
+__global__ void k_transfer_write(int nrecv, const int64_t *__restrict__ cand_off, const int32_t *__restrict__ cand_src,
+                                 const float *__restrict__ cand_w, const int64_t *__restrict__ tr_off,
+                                 int2 *__restrict__ tr) {
+    const int r = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const unsigned lane = threadIdx.x & 31;
+    if (r >= nrecv) return;
+    const int64_t a = cand_off[r], b = cand_off[r + 1];
+    const int64_t o0 = tr_off[r], o1 = tr_off[r + 1];
+    int64_t made = 0;
+    for (int64_t base = a; base < b && o0 + made < o1; base += 32) {
+        const int64_t q = base + lane;
+        const float w = q < b ? cand_w[q] : 0.0f;
+        const unsigned ok = __ballot_sync(kFull, w > 0.0f);
+        const int64_t at = o0 + made + __popc(ok & ((1u << lane) - 1u));
+        if (w > 0.0f && at < o1) tr[at] = make_int2(cand_src[q], __float_as_int(w));
+        made += __popc(ok);
+    }
+    __syncwarp();
+    float scale = 0.0f;
+    if (lane == 0 && o1 > o0) {
+        float total = 0.0f;
+        for (int64_t j = o0; j < o1; j++) total = __fadd_rn(total, __int_as_float(tr[j].y));
+        scale = (double)total > 3.141592653589793 ? __fdiv_rn(1.0f, total) : (float)(1.0 / 3.141592653589793);
+    }
+    scale = __shfl_sync(kFull, scale, 0);
+    __syncwarp();
+    for (int64_t j = o0 + lane; j < o1; j += 32) {
+        const int2 t = tr[j];
+        tr[j] = make_int2(t.x, __float_as_int(__fmul_rn(__int_as_float(t.y), scale)));
+    }
+}
+
+// ---- bounces ---------------------------------------------------------------
+
+// GatherLight for one receiver (the ordered sum over its transfers of the
+// sources' shoot times the weight), then CollectLight's update of that
+// leaf: the light added, emitted and shot on.
+__global__ void k_gather(BounceView v, const int64_t *__restrict__ tr_off, const int2 *__restrict__ tr,
+                         const float4 *__restrict__ shoot_in, float4 *__restrict__ total,
+                         float4 *__restrict__ emit_out, float4 *__restrict__ shoot_out) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= v.nreceivers) return;
+    const int p = __ldg(&v.recv[r]);
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    const int64_t a = __ldg(&tr_off[r]), b = __ldg(&tr_off[r + 1]);
+    for (int64_t j = a; j < b; j++) {
+        const int2 t = __ldg(&tr[j]);
+        const float w = __int_as_float(t.y);
+        const float4 s = __ldg(&shoot_in[t.x]);
+        sx = __fadd_rn(sx, __fmul_rn(s.x, w));
+        sy = __fadd_rn(sy, __fmul_rn(s.y, w));
+        sz = __fadd_rn(sz, __fmul_rn(s.z, w));
+    }
+    if (__ldg(&v.tree[p].w)) {
+        emit_out[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        shoot_out[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        return;
+    }
+    const float4 t = total[p];
+    total[p] = make_float4(__fadd_rn(t.x, sx), __fadd_rn(t.y, sy), __fadd_rn(t.z, sz), 0.0f);
+    emit_out[p] = make_float4(sx, sy, sz, 0.0f);
+    const float4 rf = __ldg(&v.refl[p]);
+    shoot_out[p] = make_float4(__fmul_rn(sx, rf.x), __fmul_rn(sy, rf.y), __fmul_rn(sz, rf.z), 0.0f);
+}
+
+// CollectLight's parents, bottom up within each face (children have
+// higher indices): the area blend of the children's light and emission.
+__global__ void k_collect(BounceView v, float4 *__restrict__ total, float4 *__restrict__ emit_out,
+                          float4 *__restrict__ shoot_out) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= v.nfaces) return;
+    const int4 fr = __ldg(&v.face_range[f]);
+    const FaceList L{fr.x, fr.y, fr.z};
+    const int n = L.count();
+    for (int k = 0; k < n; k++) {
+        const int p = L.at(k);
+        const int4 tr = __ldg(&v.tree[p]);
+        if (tr.w) {
+            emit_out[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            shoot_out[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            continue;
+        }
+        if (tr.y == -1) continue;
+        const float a1 = __ldg(&v.origin[tr.y].w), a2 = __ldg(&v.origin[tr.z].w);
+        const float s1 = __fdiv_rn(a1, __fadd_rn(a1, a2)), s2 = __fdiv_rn(a2, __fadd_rn(a1, a2));
+        const float4 c1 = total[tr.y], c2 = total[tr.z];
+        total[p] = make_float4(__fadd_rn(__fmul_rn(c1.x, s1), __fmul_rn(c2.x, s2)),
+                               __fadd_rn(__fmul_rn(c1.y, s1), __fmul_rn(c2.y, s2)),
+                               __fadd_rn(__fmul_rn(c1.z, s1), __fmul_rn(c2.z, s2)), 0.0f);
+        const float4 e1 = emit_out[tr.y], e2 = emit_out[tr.z];
+        const float4 e = make_float4(__fadd_rn(__fmul_rn(e1.x, s1), __fmul_rn(e2.x, s2)),
+                                     __fadd_rn(__fmul_rn(e1.y, s1), __fmul_rn(e2.y, s2)),
+                                     __fadd_rn(__fmul_rn(e1.z, s1), __fmul_rn(e2.z, s2)), 0.0f);
+        emit_out[p] = e;
+        const float4 rf = __ldg(&v.refl[p]);
+        shoot_out[p] = make_float4(__fmul_rn(e.x, rf.x), __fmul_rn(e.y, rf.y), __fmul_rn(e.z, rf.z), 0.0f);
+    }
+}
+
+// The light a bounce added (the leaves' emission), in fp64, with the sum
+// of absolute values that bounds how far the reference's float sum can
+// lie from it.
+__global__ void k_totals(BounceView v, const float4 *__restrict__ emit, double *__restrict__ sums) {
+    __shared__ double part[6][kBounceBlock / 32];
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    if (p < v.npatches) {
+        const int4 tr = __ldg(&v.tree[p]);
+        if (tr.y == -1 && tr.w == 0) {
+            const float4 e = emit[p];
+            s[0] = e.x, s[1] = e.y, s[2] = e.z;
+            s[3] = fabs((double)e.x), s[4] = fabs((double)e.y), s[5] = fabs((double)e.z);
+        }
+    }
+    for (int k = 0; k < 6; k++)
+        for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_down_sync(kFull, s[k], o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int k = 0; k < 6; k++) part[k][warp] = s[k];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double t = 0.0;
+        for (int w = 0; w < kBounceBlock / 32; w++) t += part[threadIdx.x][w];
+        atomicAdd(&sums[threadIdx.x], t);
+    }
+}
+
+// CollectLight's own total: the leaves' emission summed in float, in
+// descending index order.
+__global__ void k_exact_total(BounceView v, const float4 *__restrict__ emit, float *__restrict__ out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    float x = 0.0f, y = 0.0f, z = 0.0f;
+    for (int p = v.npatches - 1; p >= 0; p--) {
+        const int4 tr = __ldg(&v.tree[p]);
+        if (tr.y != -1 || tr.w) continue;
+        const float4 e = emit[p];
+        x = __fadd_rn(x, e.x);
+        y = __fadd_rn(y, e.y);
+        z = __fadd_rn(z, e.z);
+    }
+    out[0] = x;
+    out[1] = y;
+    out[2] = z;
+}
+
+unsigned blocks(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
+
+}  // namespace
+
+void BounceBuffers::release() {
+    void *ptrs[] = {origin, normal, mins, maxs, refl, tree, wind, points, face_range, face_samples, face_plane,
+                    recv, row_off, row_faces, sample_area, cand_off, cand_src, cand_w, tr_off, tr, scan_tmp,
+                    acc, direct, total, emit[0], emit[1], shoot[0], shoot[1], sums, exact, counters,
+                    pr_off, pr_patch, pr_box, pr_coord, prad_light, prad_weight};
+    for (void *q : ptrs) cudaFree(q);
+    cudaFreeHost(h_sums);
+    cudaFreeHost(h_exact);
+    *this = BounceBuffers();
+}
+
+cudaError_t launch_patch_light(const BounceBuffers &b, const float4 *sample_light, cudaStream_t stream) {
+    if (b.npatches == 0) return cudaSuccess;
+    k_patch_samples<<<blocks(b.npatches, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, sample_light, b.acc);
+    k_patch_tree<<<blocks(b.nfaces, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.acc, b.direct, b.total,
+                                                                              b.emit[0], b.shoot[0]);
+    return cudaGetLastError();
+}
+
+// The transfer build.  count_only: the candidate counts and offsets alone
+// (sizing at upload).  Otherwise the candidates, their rays and form
+// factors, and the transfer lists; counters[0..1] are added to.
+cudaError_t launch_transfers(BounceBuffers &b, const DeviceScene &scene, uint32_t *overflow, cudaStream_t stream,
+                             bool count_only) {
+    const int R = b.nreceivers;
+    if (R == 0) return cudaSuccess;
+    // Candidate counts into cand_off[1..R], then the exclusive scan.
+    k_candidates<<<blocks(R, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, nullptr, b.cand_off + 1, nullptr,
+                                                                       overflow);
+    cudaError_t e = cudaMemsetAsync(b.cand_off, 0, sizeof(int64_t), stream);
+    if (e != cudaSuccess) return e;
+    size_t tmp = b.scan_tmp_bytes;
+    e = cub::DeviceScan::InclusiveSum(b.scan_tmp, tmp, b.cand_off + 1, b.cand_off + 1, R, stream);
+    if (e != cudaSuccess || count_only) return e != cudaSuccess ? e : cudaGetLastError();
+    k_candidates<<<blocks(R, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.cand_off, nullptr, b.cand_src,
+                                                                       overflow);
+    if (b.ncand > 0)
+        k_transfer<kBlock><<<blocks(b.ncand, kBlock), kBlock, 0, stream>>>(b.view, scene, b.cand_off, b.cand_src,
+                                                                           b.cand_w, b.ncand, b.counters, overflow);
+    k_transfer_count<<<blocks((int64_t)R * 32, kBounceBlock), kBounceBlock, 0, stream>>>(R, b.cand_off, b.cand_w,
+                                                                                         b.tr_off + 1);
+    e = cudaMemsetAsync(b.tr_off, 0, sizeof(int64_t), stream);
+    if (e != cudaSuccess) return e;
+    tmp = b.scan_tmp_bytes;
+    e = cub::DeviceScan::InclusiveSum(b.scan_tmp, tmp, b.tr_off + 1, b.tr_off + 1, R, stream);
+    if (e != cudaSuccess) return e;
+    if (b.tr)
+        k_transfer_write<<<blocks((int64_t)R * 32, kBounceBlock), kBounceBlock, 0, stream>>>(
+            R, b.cand_off, b.cand_src, b.cand_w, b.tr_off, b.tr);
+    return cudaGetLastError();
+}
+
+// Bounce number `bounce` (0-based): reads shoot[bounce & 1], writes the
+// other half, then the fp64 totals.
+cudaError_t launch_gather(BounceBuffers &b, int bounce, cudaStream_t stream) {
+    const int in = bounce & 1, out = in ^ 1;
+    if (b.nreceivers)
+        k_gather<<<blocks(b.nreceivers, kBounceBlock), kBounceBlock, 0, stream>>>(
+            b.view, b.tr_off, b.tr, b.shoot[in], b.total, b.emit[out], b.shoot[out]);
+    k_collect<<<blocks(b.nfaces, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.total, b.emit[out], b.shoot[out]);
+    cudaError_t e = cudaMemsetAsync(b.sums, 0, 6 * sizeof(double), stream);
+    if (e != cudaSuccess) return e;
+    if (b.npatches)
+        k_totals<<<blocks(b.npatches, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.emit[out], b.sums);
+    b.last_buffer = out;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_exact_total(BounceBuffers &b, int bounce, cudaStream_t stream) {
+    k_exact_total<<<1, 32, 0, stream>>>(b.view, b.emit[(bounce & 1) ^ 1], b.exact);
+    return cudaGetLastError();
+}
+
+}  // namespace vrad

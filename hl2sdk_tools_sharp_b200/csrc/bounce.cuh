@@ -1,0 +1,120 @@
+// bounce.cuh -- the radiosity bounce resident on one device.
+//
+// Layout in HBM (P patches in the reference's index order, R receivers,
+// F faces, Q candidate pairs, T transfers):
+//   origin[P]    float4 (origin xyz, area)
+//   normal[P]    float4 (shading normal xyz, plane dist)
+//   mins[P]      float4 (winding bounds min xyz, face bits)
+//   maxs[P]      float4 (winding bounds max xyz, cluster bits)
+//   tree[P]      int4   (parent, child1, child2, sky)
+//   refl[P]      float4 (reflectivity xyz, -)
+//   wind[P]      int2   (first point, count) into points[] float4
+//   face_range[F] int4  (root patch, first descendant, end of descendants, -)
+//   face_samples[F] int2 (first sample, count)
+//   face_plane[F] float4 (plane normal xyz, dist)
+//   recv[R]      int32  receiver order (VisMatrix.ReceiverOrder): cluster by
+//                       cluster, each cluster's leaf patches in index order
+//   row_off / row_faces  per cluster, the faces its PVS row reaches, in
+//                       VisMatrix.FacesInRow order
+//   cand_off[R+1] int64, cand_src[Q] int32, cand_w[Q] float: each receiver's
+//                       candidate sources in enumeration order and the
+//                       transfer each earns (0 when blocked or none)
+//   tr_off[R+1] int64, tr[T] int2 (source, weight bits): the transfer lists
+//                       (TransferSet), by receiver
+//   acc[P] float4 (sample light xyz, sample area); direct[P], total[P],
+//   emit[2][P], shoot[2][P] float4: PatchLighting and Radiosity state
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "scene.cuh"
+#include "vrad_internal.cuh"
+
+namespace vrad {
+
+constexpr int64_t kMaxTransfersPerReceiver = 4 * 65536;  // VisMatrix.MaxPatches
+
+struct BounceView {
+    int32_t npatches, nfaces, nreceivers;
+    const float4 *origin;
+    const float4 *normal;
+    const float4 *mins;
+    const float4 *maxs;
+    const int4 *tree;
+    const float4 *refl;
+    const int2 *wind;
+    const float4 *points;
+    const int4 *face_range;
+    const int2 *face_samples;
+    const float4 *face_plane;
+    const int32_t *recv;
+    const int32_t *row_off;
+    const int32_t *row_faces;
+    const float *sample_area;
+    const float4 *sample_pos;  // the world's (xyz, face bits)
+};
+
+struct BounceBuffers {
+    // Geometry and tables, built once by vrad_bounce_upload.
+    float4 *origin = nullptr, *normal = nullptr, *mins = nullptr, *maxs = nullptr, *refl = nullptr;
+    int4 *tree = nullptr;
+    int2 *wind = nullptr;
+    float4 *points = nullptr;
+    int4 *face_range = nullptr;
+    int2 *face_samples = nullptr;
+    float4 *face_plane = nullptr;
+    int32_t *recv = nullptr, *row_off = nullptr, *row_faces = nullptr;
+    float *sample_area = nullptr;
+    // Transfer build.
+    int64_t *cand_off = nullptr;   // R + 1
+    int32_t *cand_src = nullptr;   // Q
+    float *cand_w = nullptr;       // Q
+    int64_t *tr_off = nullptr;     // R + 1
+    int2 *tr = nullptr;            // T
+    void *scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
+    int64_t ncand = 0, ntransfers = 0;
+    // Light state.
+    float4 *acc = nullptr, *direct = nullptr, *total = nullptr;
+    float4 *emit[2] = {nullptr, nullptr}, *shoot[2] = {nullptr, nullptr};
+    double *sums = nullptr;        // fp64 totals of a bounce: 3 sums, 3 absolute sums
+    float *exact = nullptr;        // the sequential float total, when needed
+    unsigned long long *counters = nullptr;  // [0] transfer rays, [1] blocked, [2] asin ties left open
+    double *h_sums = nullptr;      // pinned host copies
+    float *h_exact = nullptr;
+    // Final pass: each face's leaf patches whose radial box reaches it.
+    int32_t *pr_off = nullptr;     // F + 1
+    int32_t *pr_patch = nullptr;
+    int4 *pr_box = nullptr;        // sMin, tMin, sMax, tMax
+    float4 *pr_coord = nullptr;    // coordS, coordT, distS, distT
+    float4 *prad_light = nullptr;  // per cell
+    float *prad_weight = nullptr;
+
+    BounceView view{};
+    std::vector<int32_t> h_recv;     // host copy of the receiver order
+    int32_t npatches = 0, nfaces = 0, nreceivers = 0, nleaves = 0;
+    int32_t max_bounces = 0;
+    float threshold = 1.0f;
+    int32_t last_buffer = 0;         // which emit/shoot half the last bounce wrote
+    bool ready = false;
+    // Statistics of the last pass.
+    int32_t bounces_run = 0, exact_totals = 0;
+    double added[3] = {0, 0, 0};
+    float patch_light_ms = 0, transfer_ms = 0, bounce_ms = 0, final_ms = 0;
+    unsigned long long rays = 0, blocked = 0, open_ties = 0;
+
+    void release();
+};
+
+// Device phases of one bounce pass, all on `stream`.
+cudaError_t launch_patch_light(const BounceBuffers &b, const float4 *sample_light, cudaStream_t stream);
+cudaError_t launch_transfers(BounceBuffers &b, const DeviceScene &scene, uint32_t *overflow, cudaStream_t stream,
+                             bool count_only);
+cudaError_t launch_gather(BounceBuffers &b, int bounce, cudaStream_t stream);
+cudaError_t launch_exact_total(BounceBuffers &b, int bounce, cudaStream_t stream);
+
+}  // namespace vrad

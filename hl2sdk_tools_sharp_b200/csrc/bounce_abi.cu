@@ -1,0 +1,449 @@
+// bounce_abi.cu -- host side of the bounce: vrad_bounce_upload (the patch
+// tree, receiver order, PVS rows and the final pass's patch tables, and
+// the buffers sized by a first transfer build), the bounce loop of a light
+// pass with the reference's stop rule, and the inspection entry points.
+
+#include <cuda_runtime.h>
+
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bounce.cuh"
+#include "bounce_host.h"
+#include "context.cuh"
+#include "patches.h"
+#include "world.h"
+
+namespace vrad {
+
+namespace {
+
+template <class T>
+cudaError_t upload(T **dst, const std::vector<T> &v) {
+    cudaError_t e = cudaMalloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
+    if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+    return e;
+}
+
+inline float bits_f(int32_t x) {
+    float y;
+    std::memcpy(&y, &x, 4);
+    return y;
+}
+
+// The per-face candidate list of the bounced light's radial grid
+// (BuildPatchRadial): the face's own leaf patches, then each smoothing
+// neighbour's, each list in FacePatches order (descendants by descending
+// index, then the root); each kept with its box in this face's cells when
+// that box holds at least one cell.
+void patch_radial_tables(const std::vector<vrad_face> &faces, const PatchTree &tree, const std::vector<int32_t> &noff,
+                         const std::vector<int32_t> &nlist, std::vector<int32_t> &off, std::vector<int32_t> &patch,
+                         std::vector<int4> &box, std::vector<float4> &coord) {
+    const int32_t nf = (int32_t)faces.size();
+    off.assign((size_t)nf + 1, 0);
+    patch.clear();
+    box.clear();
+    coord.clear();
+    auto leaves = [&](int32_t g, std::vector<int32_t> &out) {
+        out.clear();
+        if (tree.face_root[(size_t)g] < 0) return;
+        for (int32_t p = tree.face_end[(size_t)g] - 1; p >= tree.face_first[(size_t)g]; p--)
+            if (tree.patches[(size_t)p].child1 == -1) out.push_back(p);
+        const int32_t r = tree.face_root[(size_t)g];
+        if (tree.patches[(size_t)r].child1 == -1) out.push_back(r);
+    };
+    std::vector<int32_t> list;
+    for (int32_t f = 0; f < nf; f++) {
+        FaceFrameOut me;
+        face_frame_of(faces[(size_t)f], me);
+        std::vector<int32_t> order = {f};
+        for (int32_t q = noff[(size_t)f]; q < noff[(size_t)f + 1]; q++) order.push_back(nlist[(size_t)q]);
+        for (int32_t g : order) {
+            leaves(g, list);
+            for (int32_t p : list) {
+                const vrad_patch &pt = tree.patches[(size_t)p];
+                // PatchLightmapCoordRange.
+                float min_s = 1e30f, min_t = 1e30f, max_s = -1e30f, max_t = -1e30f;
+                for (int32_t k = 0; k < pt.num_points; k++) {
+                    float s, t;
+                    frame_world_to_luxel(me, &tree.points[3 * (size_t)(pt.first_point + k)], s, t);
+                    min_s = min_s < s ? min_s : s;
+                    max_s = max_s > s ? max_s : s;
+                    min_t = min_t < t ? min_t : t;
+                    max_t = max_t > t ? max_t : t;
+                }
+                // LuxelRadial.AddBounced's extent and box.
+                float cs, ct;
+                frame_world_to_luxel(me, pt.origin, cs, ct);
+                float ds = max_s - min_s, dt = max_t - min_t;
+                ds = (float)(1.0 > (double)ds ? 1.0 : (double)ds);
+                dt = (float)(1.0 > (double)dt ? 1.0 : (double)dt);
+                int smin = (int)((double)cs - (double)ds * 1.42);
+                int tmin = (int)((double)ct - (double)dt * 1.42);
+                int smax = (int)((double)cs + (double)ds * 1.42 + 1.0);
+                int tmax = (int)((double)ct + (double)dt * 1.42 + 1.0);
+                smin = std::max(smin, 0);
+                tmin = std::max(tmin, 0);
+                smax = std::min(smax, me.width);
+                tmax = std::min(tmax, me.height);
+                if (smin >= smax || tmin >= tmax) continue;
+                patch.push_back(p);
+                box.push_back(make_int4(smin, tmin, smax, tmax));
+                coord.push_back(make_float4(cs, ct, ds, dt));
+            }
+        }
+        off[(size_t)f + 1] = (int32_t)patch.size();
+    }
+}
+
+}  // namespace
+
+// The bounce of one light pass, after the direct gather wrote
+// sample_light: patch light, transfers, bounces to the stop rule.  Leaves
+// the bounced light in b.total.  Blocks on the stream once per bounce (the
+// stop rule is decided on the host).
+cudaError_t run_bounce(vrad_ctx *ctx, cudaStream_t s, std::string &why) {
+    BounceBuffers &b = ctx->bounce;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 4 && e == cudaSuccess; k++) e = cudaEventCreate(&ev[k]);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[0], s);
+    if (e == cudaSuccess) e = launch_patch_light(b, ctx->sample_light, s);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[1], s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.counters, 0, 3 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = launch_transfers(b, ctx->scene.view(), ctx->status, s, false);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[2], s);
+    b.bounces_run = 0;
+    b.exact_totals = 0;
+    const double u = std::ldexp(1.0, -24);
+    const double nu = (double)b.nleaves * u;
+    const double gamma = nu < 0.5 ? nu / (1.0 - nu) : INFINITY;
+    for (int i = 0; e == cudaSuccess && i < b.max_bounces; i++) {
+        e = launch_gather(b, i, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_sums, b.sums, 6 * sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) break;
+        b.bounces_run = i + 1;
+        // Radiosity.BounceAsync's stop rule on CollectLight's float total:
+        // settled by the fp64 total when the float sum's error bound keeps
+        // it on one side of the threshold, else by the sequential sum.
+        bool below[3], settled = true;
+        for (int c = 0; c < 3; c++) {
+            const double S = b.h_sums[c], bound = gamma * b.h_sums[3 + c] * 1.0001;
+            b.added[c] = S;
+            if (S + bound < (double)b.threshold) below[c] = true;
+            else if (S - bound >= (double)b.threshold) below[c] = false;
+            else settled = false;
+        }
+        if (!settled) {
+            b.exact_totals++;
+            e = launch_exact_total(b, i, s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_exact, b.exact, 3 * sizeof(float), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) break;
+            for (int c = 0; c < 3; c++) {
+                b.added[c] = b.h_exact[c];
+                below[c] = (double)b.h_exact[c] < (double)b.threshold;
+            }
+        }
+        if (below[0] && below[1] && below[2]) break;
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ev[3], s);
+    unsigned long long counts[3] = {0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(counts, b.counters, sizeof counts, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) {
+        cudaEventElapsedTime(&b.patch_light_ms, ev[0], ev[1]);
+        cudaEventElapsedTime(&b.transfer_ms, ev[1], ev[2]);
+        cudaEventElapsedTime(&b.bounce_ms, ev[2], ev[3]);
+        b.rays = counts[0];
+        b.blocked = counts[1];
+        b.open_ties = counts[2];
+    } else {
+        why = "bounce";
+    }
+    for (cudaEvent_t x : ev)
+        if (x) cudaEventDestroy(x);
+    return e;
+}
+
+bool bounce_active(const vrad_ctx *ctx) { return ctx->bounce.ready && ctx->bounce.max_bounces > 0; }
+
+PatchRadialView patch_radial_view(vrad_ctx *ctx) {
+    BounceBuffers &b = ctx->bounce;
+    return PatchRadialView{b.pr_off, b.pr_patch, b.pr_box, b.pr_coord, b.total, b.prad_light, b.prad_weight};
+}
+
+}  // namespace vrad
+
+extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) {
+    using namespace vrad;
+    if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (!ctx->has_scene) return vrad_fail(ctx, VRAD_ERR_NO_SCENE, "no scene uploaded");
+    if (!ctx->world.ready || !ctx->final_pass.ready || ctx->h_vertices.empty())
+        return vrad_fail(ctx, VRAD_ERR_ARG, "upload the world, with face windings, before the bounce");
+    const int32_t nf = (int32_t)ctx->h_faces.size();
+    if (!d || (nf && !d->reflectivity) || !d->pvs_offsets || d->nclusters != ctx->nclusters || d->bounces < 0 ||
+        !(d->max_chop > 0.0f) || !(d->min_chop > 0.0f) || !(d->threshold >= 0.0f))
+        return vrad_fail(ctx, VRAD_ERR_ARG, "invalid bounce description");
+    const int32_t C = d->nclusters;
+    for (int32_t c = 0; c < C; c++) {
+        if (d->pvs_offsets[c] > d->pvs_offsets[c + 1]) return vrad_fail(ctx, VRAD_ERR_ARG, "PVS offsets decrease at %d", c);
+        for (int32_t k = d->pvs_offsets[c]; k < d->pvs_offsets[c + 1]; k++) {
+            const int32_t j = d->pvs_clusters[k];
+            if (j < 0 || j >= C || (k > d->pvs_offsets[c] && j <= d->pvs_clusters[k - 1]))
+                return vrad_fail(ctx, VRAD_ERR_ARG, "PVS row %d is not ascending clusters", c);
+        }
+    }
+    for (int32_t f = 0; f < nf; f++)
+        if (ctx->h_faces[(size_t)f].flags & VRAD_SURF_BUMPLIGHT)
+            return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "face %d is bump-mapped", f);
+
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
+    BounceBuffers &b = ctx->bounce;
+    b.release();
+    PatchTree tree;
+    std::string why;
+    const int64_t nvert = (int64_t)ctx->h_vertices.size() / 3;
+    if (!build_patch_tree(ctx->h_faces.data(), nf, ctx->h_vertices.data(), nvert, d->reflectivity, d->max_chop,
+                          d->min_chop, tree, why))
+        return vrad_fail(ctx, VRAD_ERR_ARG, "patches: %s", why.c_str());
+    const int32_t P = (int32_t)tree.patches.size();
+
+    // Per patch.
+    std::vector<float4> origin((size_t)P), normal((size_t)P), mins((size_t)P), maxs((size_t)P), refl((size_t)P);
+    std::vector<int4> tr((size_t)P);
+    std::vector<int2> wind((size_t)P);
+    int32_t nleaves = 0;
+    for (int32_t i = 0; i < P; i++) {
+        const vrad_patch &p = tree.patches[(size_t)i];
+        if (p.cluster < 0 || p.cluster >= C)
+            return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "patch %d lies outside every cluster", i);
+        origin[(size_t)i] = make_float4(p.origin[0], p.origin[1], p.origin[2], p.area);
+        normal[(size_t)i] = make_float4(p.normal[0], p.normal[1], p.normal[2], p.plane_dist);
+        mins[(size_t)i] = make_float4(p.mins[0], p.mins[1], p.mins[2], bits_f(p.face));
+        maxs[(size_t)i] = make_float4(p.maxs[0], p.maxs[1], p.maxs[2], bits_f(p.cluster));
+        refl[(size_t)i] = make_float4(p.reflectivity[0], p.reflectivity[1], p.reflectivity[2], 0.0f);
+        tr[(size_t)i] = make_int4(p.parent, p.child1, p.child2, p.sky);
+        wind[(size_t)i] = make_int2(p.first_point, p.num_points);
+        if (p.child1 == -1 && !p.sky) nleaves++;
+    }
+    std::vector<float4> points(tree.points.size() / 3);
+    for (size_t k = 0; k < points.size(); k++)
+        points[k] = make_float4(tree.points[3 * k], tree.points[3 * k + 1], tree.points[3 * k + 2], 0.0f);
+    // Per face.
+    std::vector<int4> face_range((size_t)nf);
+    std::vector<int2> face_samples((size_t)nf, make_int2(0, 0));
+    std::vector<float4> face_plane((size_t)nf);
+    for (int32_t f = 0; f < nf; f++) {
+        face_range[(size_t)f] = make_int4(tree.face_root[(size_t)f], tree.face_first[(size_t)f], tree.face_end[(size_t)f], 0);
+        const vrad_face &fc = ctx->h_faces[(size_t)f];
+        face_plane[(size_t)f] = make_float4(fc.normal[0], fc.normal[1], fc.normal[2], fc.dist);
+    }
+    std::vector<float> sample_area(ctx->h_samples.size());
+    for (size_t k = 0; k < ctx->h_samples.size(); k++) {
+        const vrad_sample &sm = ctx->h_samples[k];
+        sample_area[k] = sm.area;
+        int2 &fs = face_samples[(size_t)sm.face];
+        if (fs.y == 0) fs.x = (int32_t)k;
+        fs.y++;
+    }
+    // VisMatrix.ReceiverOrder: cluster by cluster, leaf patches in index order.
+    std::vector<std::vector<int32_t>> by_cluster((size_t)C);
+    for (int32_t i = 0; i < P; i++)
+        if (tree.patches[(size_t)i].child1 == -1) by_cluster[(size_t)tree.patches[(size_t)i].cluster].push_back(i);
+    std::vector<int32_t> recv;
+    for (const auto &v : by_cluster) recv.insert(recv.end(), v.begin(), v.end());
+    // FacesInRow: each visible cluster's faces, in face order (one leaf per
+    // cluster, whose faces are the faces that lie in it).
+    std::vector<std::vector<int32_t>> cluster_faces((size_t)C);
+    for (int32_t f = 0; f < nf; f++) cluster_faces[(size_t)ctx->h_faces[(size_t)f].cluster].push_back(f);
+    std::vector<int32_t> row_off((size_t)C + 1, 0), row_faces;
+    for (int32_t c = 0; c < C; c++) {
+        for (int32_t k = d->pvs_offsets[c]; k < d->pvs_offsets[c + 1]; k++) {
+            const auto &fl = cluster_faces[(size_t)d->pvs_clusters[k]];
+            row_faces.insert(row_faces.end(), fl.begin(), fl.end());
+        }
+        row_off[(size_t)c + 1] = (int32_t)row_faces.size();
+    }
+    // The final pass's patch tables over the smoothing neighbours.
+    std::vector<int32_t> noff((size_t)nf + 1);
+    int64_t nn = 0;
+    if (vrad_build_neighbours(ctx->h_faces.data(), nf, ctx->h_vertices.data(), nvert, 0.7071067f, noff.data(), nullptr, 0,
+                              &nn) != VRAD_OK)
+        return vrad_fail(ctx, VRAD_ERR_ARG, "invalid face windings");
+    std::vector<int32_t> nlist((size_t)(nn ? nn : 1));
+    vrad_build_neighbours(ctx->h_faces.data(), nf, ctx->h_vertices.data(), nvert, 0.7071067f, noff.data(), nlist.data(), nn,
+                          &nn);
+    std::vector<int32_t> pr_off, pr_patch;
+    std::vector<int4> pr_box;
+    std::vector<float4> pr_coord;
+    patch_radial_tables(ctx->h_faces, tree, noff, nlist, pr_off, pr_patch, pr_box, pr_coord);
+
+    const int32_t R = (int32_t)recv.size();
+    const int64_t ncells = ctx->final_pass.view.ncells;
+    if (e == cudaSuccess) e = upload(&b.origin, origin);
+    if (e == cudaSuccess) e = upload(&b.normal, normal);
+    if (e == cudaSuccess) e = upload(&b.mins, mins);
+    if (e == cudaSuccess) e = upload(&b.maxs, maxs);
+    if (e == cudaSuccess) e = upload(&b.refl, refl);
+    if (e == cudaSuccess) e = upload(&b.tree, tr);
+    if (e == cudaSuccess) e = upload(&b.wind, wind);
+    if (e == cudaSuccess) e = upload(&b.points, points);
+    if (e == cudaSuccess) e = upload(&b.face_range, face_range);
+    if (e == cudaSuccess) e = upload(&b.face_samples, face_samples);
+    if (e == cudaSuccess) e = upload(&b.face_plane, face_plane);
+    if (e == cudaSuccess) e = upload(&b.recv, recv);
+    if (e == cudaSuccess) e = upload(&b.row_off, row_off);
+    if (e == cudaSuccess) e = upload(&b.row_faces, row_faces);
+    if (e == cudaSuccess) e = upload(&b.sample_area, sample_area);
+    if (e == cudaSuccess) e = upload(&b.pr_off, pr_off);
+    if (e == cudaSuccess) e = upload(&b.pr_patch, pr_patch);
+    if (e == cudaSuccess) e = upload(&b.pr_box, pr_box);
+    if (e == cudaSuccess) e = upload(&b.pr_coord, pr_coord);
+    const size_t P1 = (size_t)(P ? P : 1), R1 = (size_t)R + 1, N1 = (size_t)(ncells ? ncells : 1);
+    if (e == cudaSuccess) e = cudaMalloc(&b.cand_off, sizeof(int64_t) * R1);
+    if (e == cudaSuccess) e = cudaMalloc(&b.tr_off, sizeof(int64_t) * R1);
+    for (float4 **q : {&b.acc, &b.direct, &b.total, &b.emit[0], &b.emit[1], &b.shoot[0], &b.shoot[1]})
+        if (e == cudaSuccess) e = cudaMalloc(q, sizeof(float4) * P1);
+    if (e == cudaSuccess) e = cudaMalloc(&b.sums, 6 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b.exact, 3 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&b.counters, 3 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMallocHost(&b.h_sums, 6 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&b.h_exact, 3 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&b.prad_light, sizeof(float4) * N1);
+    if (e == cudaSuccess) e = cudaMalloc(&b.prad_weight, sizeof(float) * N1);
+    if (e == cudaSuccess && R > 0) {
+        size_t need = 0;
+        e = cub::DeviceScan::InclusiveSum(nullptr, need, b.cand_off + 1, b.cand_off + 1, R);
+        if (e == cudaSuccess) e = cudaMalloc(&b.scan_tmp, need ? need : 1);
+        b.scan_tmp_bytes = need;
+    }
+    if (e != cudaSuccess) {
+        b.release();
+        return vrad_cuda_fail(ctx, e, "bounce upload");
+    }
+    b.npatches = P;
+    b.nfaces = nf;
+    b.nreceivers = R;
+    b.nleaves = nleaves;
+    b.max_bounces = d->bounces;
+    b.threshold = d->threshold;
+    b.h_recv = recv;
+    b.view = BounceView{P, nf, R, b.origin, b.normal, b.mins, b.maxs, b.tree, b.refl, b.wind, b.points,
+                        b.face_range, b.face_samples, b.face_plane, b.recv, b.row_off, b.row_faces, b.sample_area,
+                        ctx->world.sample_pos};
+    // Size the candidate and transfer arrays by one build.
+    cudaStream_t s = ctx->stream;
+    e = launch_transfers(b, ctx->scene.view(), ctx->status, s, true);
+    int64_t ncand = 0;
+    if (e == cudaSuccess && R > 0) e = cudaMemcpyAsync(&ncand, b.cand_off + R, sizeof ncand, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    b.ncand = ncand;
+    if (e == cudaSuccess) e = cudaMalloc(&b.cand_src, sizeof(int32_t) * (size_t)(ncand ? ncand : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&b.cand_w, sizeof(float) * (size_t)(ncand ? ncand : 1));
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.counters, 0, 3 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = launch_transfers(b, ctx->scene.view(), ctx->status, s, false);
+    int64_t ntr = 0;
+    if (e == cudaSuccess && R > 0) e = cudaMemcpyAsync(&ntr, b.tr_off + R, sizeof ntr, cudaMemcpyDeviceToHost, s);
+    uint32_t overflow = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&overflow, ctx->status, sizeof overflow, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = cudaMalloc(&b.tr, sizeof(int2) * (size_t)(ntr ? ntr : 1));
+    if (e != cudaSuccess) {
+        b.release();
+        return vrad_cuda_fail(ctx, e, "transfer sizing");
+    }
+    if (overflow) {
+        cudaMemset(ctx->status, 0, sizeof(uint32_t));
+        b.release();
+        return vrad_fail(ctx, VRAD_ERR_CUDA, "stack overflow in the transfer build (flags %u)", overflow);
+    }
+    b.ntransfers = ntr;
+    b.ready = true;
+    return VRAD_OK;
+}
+
+extern "C" int32_t vrad_bounce_stats_get(vrad_ctx *ctx, vrad_bounce_stats *st) {
+    if (!ctx || !st) return vrad_fail(ctx, VRAD_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    const vrad::BounceBuffers &b = ctx->bounce;
+    if (!b.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no bounce uploaded");
+    std::memset(st, 0, sizeof *st);
+    st->patches = b.npatches;
+    st->receivers = b.nreceivers;
+    st->transfer_rays = (int64_t)b.rays;
+    st->blocked = (int64_t)b.blocked;
+    st->transfers = b.ntransfers;
+    st->bounces = b.bounces_run;
+    st->exact_totals = b.exact_totals;
+    for (int c = 0; c < 3; c++) st->added[c] = b.added[c];
+    st->patch_light_ms = b.patch_light_ms;
+    st->transfer_ms = b.transfer_ms;
+    st->bounce_ms = b.bounce_ms;
+    st->final_ms = b.final_ms;
+    return VRAD_OK;
+}
+
+extern "C" int32_t vrad_bounce_patch_light(vrad_ctx *ctx, float *total_light, float *direct_light, int64_t npatches) {
+    if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    vrad::BounceBuffers &b = ctx->bounce;
+    if (!b.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no bounce uploaded");
+    if (npatches != b.npatches) return vrad_fail(ctx, VRAD_ERR_ARG, "%d patches, %lld asked", b.npatches, (long long)npatches);
+    std::vector<float4> tmp((size_t)(npatches ? npatches : 1));
+    cudaError_t e = cudaSetDevice(ctx->device);
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) {
+        float *dst = k == 0 ? total_light : direct_light;
+        if (!dst || npatches == 0) continue;
+        e = cudaMemcpy(tmp.data(), k == 0 ? b.total : b.direct, sizeof(float4) * (size_t)npatches, cudaMemcpyDeviceToHost);
+        for (int64_t i = 0; e == cudaSuccess && i < npatches; i++) {
+            dst[3 * i] = tmp[(size_t)i].x;
+            dst[3 * i + 1] = tmp[(size_t)i].y;
+            dst[3 * i + 2] = tmp[(size_t)i].z;
+        }
+    }
+    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "patch light download");
+    return VRAD_OK;
+}
+
+extern "C" int32_t vrad_bounce_transfers(vrad_ctx *ctx, int64_t *offsets, int64_t npatches, vrad_transfer *transfers,
+                                         int64_t capacity, int64_t *count) {
+    if (!ctx || !offsets || !count) return vrad_fail(ctx, VRAD_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    vrad::BounceBuffers &b = ctx->bounce;
+    if (!b.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no bounce uploaded");
+    if (npatches != b.npatches) return vrad_fail(ctx, VRAD_ERR_ARG, "%d patches, %lld asked", b.npatches, (long long)npatches);
+    const int32_t R = b.nreceivers;
+    std::vector<int64_t> off((size_t)R + 1, 0);
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess && R) e = cudaMemcpy(off.data(), b.tr_off, sizeof(int64_t) * ((size_t)R + 1), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "transfer download");
+    std::vector<int64_t> len((size_t)npatches, 0), from((size_t)npatches, 0);
+    for (int32_t r = 0; r < R; r++) {
+        len[(size_t)b.h_recv[(size_t)r]] = off[(size_t)r + 1] - off[(size_t)r];
+        from[(size_t)b.h_recv[(size_t)r]] = off[(size_t)r];
+    }
+    offsets[0] = 0;
+    for (int64_t p = 0; p < npatches; p++) offsets[p + 1] = offsets[p] + len[(size_t)p];
+    *count = offsets[npatches];
+    if (!transfers) return VRAD_OK;
+    if (capacity < *count) return vrad_fail(ctx, VRAD_ERR_ARG, "%lld transfers, room for %lld", (long long)*count, (long long)capacity);
+    std::vector<int2> all((size_t)(off[(size_t)R] ? off[(size_t)R] : 1));
+    if (off[(size_t)R]) e = cudaMemcpy(all.data(), b.tr, sizeof(int2) * (size_t)off[(size_t)R], cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "transfer download");
+    for (int64_t p = 0; p < npatches; p++)
+        for (int64_t k = 0; k < len[(size_t)p]; k++) {
+            const int2 t = all[(size_t)(from[(size_t)p] + k)];
+            transfers[offsets[p] + k].patch = t.x;
+            std::memcpy(&transfers[offsets[p] + k].weight, &t.y, 4);
+        }
+    return VRAD_OK;
+}

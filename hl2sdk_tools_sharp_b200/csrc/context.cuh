@@ -5,7 +5,9 @@
 
 #include <mutex>
 #include <string>
+#include <vector>
 
+#include "bounce.cuh"
 #include "direct.cuh"
 #include "final.cuh"
 #include "scene.cuh"
@@ -26,6 +28,12 @@ struct vrad_ctx {
     vrad::WorldBuffers world;
     vrad::FinalBuffers final_pass;
     float4 *sample_light = nullptr;  // the direct gather's output, one per sample
+    // Host copies of the uploaded world the bounce set-up reads.
+    std::vector<vrad_face> h_faces;
+    std::vector<float> h_vertices;
+    std::vector<vrad_sample> h_samples;
+    int32_t nclusters = 0;
+    vrad::BounceBuffers bounce;
     std::string last_error;
     std::string identity;
 };

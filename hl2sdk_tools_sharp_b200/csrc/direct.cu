@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "context.cuh"
+#include "detmath.cuh"
 #include "traverse.cuh"
 
 namespace vrad {
@@ -154,7 +155,7 @@ __global__ void __launch_bounds__(BLOCK) k_direct(DeviceScene sc, DeviceWorld w,
                     float mult = __fdiv_rn(__fsub_rn(dot2, D.y), __fsub_rn(D.x, D.y));
                     mult = minps(mult, 1.0f);
                     mult = maxps(mult, 0.0f);
-                    if (C.w != 0.0f && C.w != 1.0f) mult = (float)pow((double)mult, (double)C.w);
+                    if (C.w != 0.0f && C.w != 1.0f) mult = pow_cr(mult, C.w, &counters[2]);  // DetMathF.Pow
                     mult = fringe ? mult : 1.0f;
                     f = __fmul_rn(mult, f);
                     if (hard) f = __fmul_rn(fade(dist, E.y, __fsub_rn(E.z, E.y)), f);
@@ -429,7 +430,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     if (e == cudaSuccess) e = upload_vec(&wb.cl_list, cl_list);
     if (e == cudaSuccess) e = upload_vec(&wb.dirs, dirs);
     if (e == cudaSuccess) e = upload_vec(&wb.jitter, jit);
-    if (e == cudaSuccess) e = cudaMalloc(&wb.counters, 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&wb.counters, 3 * sizeof(unsigned long long));
     if (e != cudaSuccess) {
         wb.release();
         return vrad_cuda_fail(ctx, e, "world upload");
@@ -437,7 +438,14 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     wb.view = vrad::DeviceWorld{wb.slots, (int64_t)slots.size(), wb.sample_pos, wb.face_normal, wb.lights, nl,
                                 wb.cl_off, wb.cl_list, w->nclusters, wb.dirs, w->nsky_directions, wb.jitter,
                                 w->nsun_jitter, w->sun_angular_extent, w->sun_samples, w->nsamples};
-    // The final pass's tables, and the direct gather's output buffer.
+    // The final pass's tables, and the direct gather's output buffer.  A
+    // new world drops the old bounce.
+    ctx->bounce.release();
+    ctx->h_faces.assign(w->faces, w->faces + w->nfaces);
+    ctx->h_samples.assign(w->samples, w->samples + w->nsamples);
+    if (w->vertices && w->nvertices > 0) ctx->h_vertices.assign(w->vertices, w->vertices + 3 * w->nvertices);
+    else ctx->h_vertices.clear();
+    ctx->nclusters = w->nclusters;
     ctx->final_pass.release();
     cudaFree(ctx->sample_light);
     ctx->sample_light = nullptr;
@@ -467,7 +475,7 @@ namespace {
 int32_t direct_on(vrad_ctx *ctx, float4 *d_out, cudaStream_t s) {
     if (!ctx->has_scene) return vrad_fail(ctx, VRAD_ERR_NO_SCENE, "no scene uploaded");
     if (!ctx->world.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no lighting world uploaded");
-    cudaError_t e = cudaMemsetAsync(ctx->world.counters, 0, 2 * sizeof(unsigned long long), s);
+    cudaError_t e = cudaMemsetAsync(ctx->world.counters, 0, 3 * sizeof(unsigned long long), s);
     if (e == cudaSuccess)
         e = vrad::launch_direct(ctx->scene.view(), ctx->world.view, d_out, ctx->world.counters, ctx->status, s,
                                 ctx->world.block);

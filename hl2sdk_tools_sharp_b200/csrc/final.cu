@@ -28,6 +28,7 @@
 #include <string>
 #include <type_traits>
 
+#include "bounce_host.h"
 #include "context.cuh"
 #include "final.cuh"
 #include "world.h"
@@ -133,6 +134,37 @@ __global__ void k_radial(FinalView v, const float4 *__restrict__ sample_light, f
     rad_weight[c] = weight;
 }
 
+// The bounced light's radial grid: LuxelRadial.AddBounced for every leaf
+// patch in the face's list whose box holds this cell, in list order.
+__global__ void k_patch_radial(FinalView v, PatchRadialView p) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= v.ncells) return;
+    const int f = __ldg(&v.cell_face[c]);
+    const int base = __ldg(&v.face_cells[f]);
+    const int w = __float_as_int(__ldg(&v.frames[5 * f].w));
+    const int local = (int)(c - base);
+    const int s = local % w, t = local / w;
+    float lx = 0.0f, ly = 0.0f, lz = 0.0f, weight = 0.0f;
+    const int q0 = __ldg(&p.off[f]), q1 = __ldg(&p.off[f + 1]);
+    for (int q = q0; q < q1; q++) {
+        const int4 b = __ldg(&p.box[q]);
+        if (s < b.x || s >= b.z || t < b.y || t >= b.w) continue;
+        const float4 k = __ldg(&p.coord[q]);
+        const float ds = __fdiv_rn(__fsub_rn(k.x, (float)s), k.z);
+        const float dt = __fdiv_rn(__fsub_rn(k.y, (float)t), k.w);
+        const float r = __fsub_rn(2.0f, __fadd_rn(__fmul_rn(ds, ds), __fmul_rn(dt, dt)));
+        if (r > 0.0f) {
+            const float4 L = __ldg(&p.light[__ldg(&p.patch[q])]);
+            lx = __fadd_rn(lx, __fmul_rn(r, L.x));
+            ly = __fadd_rn(ly, __fmul_rn(r, L.y));
+            lz = __fadd_rn(lz, __fmul_rn(r, L.z));
+            weight = __fadd_rn(weight, r);
+        }
+    }
+    p.rad_light[c] = make_float4(lx, ly, lz, 0.0f);
+    p.rad_weight[c] = weight;
+}
+
 // StockLightColor.Encode: ColorRGBExp32 as a little-endian word.
 __device__ __forceinline__ uint32_t encode(float x, float y, float z) {
     float m;
@@ -150,6 +182,7 @@ __device__ __forceinline__ uint32_t encode(float x, float y, float z) {
 }
 
 __global__ void k_luxel(FinalView v, const float4 *__restrict__ rad_light, const float *__restrict__ rad_weight,
+                        const float4 *__restrict__ prad_light, const float *__restrict__ prad_weight,
                         uint32_t *__restrict__ lighting, float4 *__restrict__ flat) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= v.ncells) return;
@@ -183,6 +216,27 @@ __global__ void k_luxel(FinalView v, const float4 *__restrict__ rad_light, const
         } else {
             ok = false;
         }
+    }
+    if (prad_light) {
+        // The bounced light, style 0: the patch grid sampled the same way
+        // (its own off-grid red and weight test), added before minlight.
+        float bx = 0.0f, by = 0.0f, bz = 0.0f;
+        if (u < 0 || u >= fr.w || w < 0 || w >= fr.h) {
+            bx = 2550.0f;
+        } else {
+            const int i = base + u + w * fr.w;
+            const float wt = prad_weight[i];
+            if (wt > 0.00001f) {
+                const float4 L = prad_light[i];
+                const float scale = (float)__drcp_rn((double)wt);
+                bx = __fmul_rn(L.x, scale);
+                by = __fmul_rn(L.y, scale);
+                bz = __fmul_rn(L.z, scale);
+            }
+        }
+        lx = __fadd_rn(lx, bx);
+        ly = __fadd_rn(ly, by);
+        lz = __fadd_rn(lz, bz);
     }
     if (__ldg(&v.face_nsamples[f]) == 0) {
         lx = 255.0f;
@@ -269,11 +323,14 @@ void FinalBuffers::release() {
 }
 
 cudaError_t launch_final(const FinalView &v, const float4 *sample_light, float4 *rad_light, float *rad_weight,
-                         float4 *flat, uint8_t *lighting, int nfaces, cudaStream_t stream) {
+                         float4 *flat, uint8_t *lighting, int nfaces, const PatchRadialView *prad,
+                         cudaStream_t stream) {
     if (v.ncells == 0) return cudaSuccess;
     const unsigned grid = (unsigned)((v.ncells + 255) / 256);
     k_radial<<<grid, 256, 0, stream>>>(v, sample_light, rad_light, rad_weight);
-    k_luxel<<<grid, 256, 0, stream>>>(v, rad_light, rad_weight, reinterpret_cast<uint32_t *>(lighting), flat);
+    if (prad) k_patch_radial<<<grid, 256, 0, stream>>>(v, *prad);
+    k_luxel<<<grid, 256, 0, stream>>>(v, rad_light, rad_weight, prad ? prad->rad_light : nullptr,
+                                      prad ? prad->rad_weight : nullptr, reinterpret_cast<uint32_t *>(lighting), flat);
     k_median<<<nfaces, kMedianThreads, 0, stream>>>(v, flat, reinterpret_cast<uint32_t *>(lighting));
     return cudaGetLastError();
 }
@@ -401,19 +458,30 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
 
 namespace {
 
-int32_t pass_on(vrad_ctx *ctx, uint8_t *d_lighting, cudaStream_t s, cudaEvent_t mid) {
+int32_t pass_on(vrad_ctx *ctx, uint8_t *d_lighting, cudaStream_t s, cudaEvent_t mid, cudaEvent_t bounce_mark) {
     if (!ctx->has_scene) return vrad_fail(ctx, VRAD_ERR_NO_SCENE, "no scene uploaded");
     if (!ctx->world.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no lighting world uploaded");
     if (!ctx->final_pass.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without face windings");
     vrad::FinalBuffers &fb = ctx->final_pass;
-    cudaError_t e = cudaMemsetAsync(ctx->world.counters, 0, 2 * sizeof(unsigned long long), s);
+    cudaError_t e = cudaMemsetAsync(ctx->world.counters, 0, 3 * sizeof(unsigned long long), s);
     if (e == cudaSuccess)
         e = vrad::launch_direct(ctx->scene.view(), ctx->world.view, ctx->sample_light, ctx->world.counters,
                                 ctx->status, s, ctx->world.block);
     if (e == cudaSuccess && mid) e = cudaEventRecord(mid, s);
+    // The bounce (patch light, transfers, bounces), when one is uploaded.
+    vrad::PatchRadialView prad{};
+    const bool bounce = vrad::bounce_active(ctx);
+    if (e == cudaSuccess && bounce) {
+        std::string why;
+        e = vrad::run_bounce(ctx, s, why);
+        if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, why.c_str());
+        prad = vrad::patch_radial_view(ctx);
+    }
+    if (e == cudaSuccess && bounce_mark) e = cudaEventRecord(bounce_mark, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_lighting, 0, (size_t)fb.lighting_bytes, s);
     if (e == cudaSuccess)
-        e = vrad::launch_final(fb.view, ctx->sample_light, fb.rad_light, fb.rad_weight, fb.flat, d_lighting, fb.nfaces, s);
+        e = vrad::launch_final(fb.view, ctx->sample_light, fb.rad_light, fb.rad_weight, fb.flat, d_lighting, fb.nfaces,
+                               bounce ? &prad : nullptr, s);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "light pass launch");
     return VRAD_OK;
 }
@@ -434,7 +502,7 @@ extern "C" int32_t vrad_light_pass_device(vrad_ctx *ctx, uint8_t *d_lighting, vo
     std::lock_guard<std::mutex> g(ctx->mu);
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
-    return pass_on(ctx, d_lighting, (cudaStream_t)stream, nullptr);
+    return pass_on(ctx, d_lighting, (cudaStream_t)stream, nullptr, nullptr);
 }
 
 extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t capacity, int32_t *lightofs,
@@ -448,13 +516,14 @@ extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t cap
                          (long long)capacity);
     cudaError_t e = cudaSetDevice(ctx->device);
     uint8_t *d_lighting = nullptr;
-    cudaEvent_t a = nullptr, m = nullptr, b = nullptr;
+    cudaEvent_t a = nullptr, m = nullptr, bm = nullptr, b = nullptr;
     if (e == cudaSuccess) e = cudaMalloc(&d_lighting, (size_t)(fb.lighting_bytes ? fb.lighting_bytes : 4));
     if (e == cudaSuccess) e = cudaEventCreate(&a);
     if (e == cudaSuccess) e = cudaEventCreate(&m);
+    if (e == cudaSuccess) e = cudaEventCreate(&bm);
     if (e == cudaSuccess) e = cudaEventCreate(&b);
     if (e == cudaSuccess) e = cudaEventRecord(a, ctx->stream);
-    int32_t rc = e == cudaSuccess ? pass_on(ctx, d_lighting, ctx->stream, m) : vrad_cuda_fail(ctx, e, "light pass set-up");
+    int32_t rc = e == cudaSuccess ? pass_on(ctx, d_lighting, ctx->stream, m, bm) : vrad_cuda_fail(ctx, e, "light pass set-up");
     unsigned long long counts[2] = {0, 0};
     uint32_t overflow = 0;
     if (rc == VRAD_OK) {
@@ -473,12 +542,15 @@ extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t cap
         rc = vrad_fail(ctx, VRAD_ERR_CUDA, "traversal stack overflow (BVH deeper than %d)", vrad::kStackDepth);
     }
     if (rc == VRAD_OK) {
+        float f_ms = 0.0f;
+        cudaEventElapsedTime(&f_ms, bm, b);
+        ctx->bounce.final_ms = f_ms;
         if (lightofs)
             for (int32_t f = 0; f < fb.nfaces; f++) lightofs[f] = fb.lightofs[(size_t)f];
         if (stats) {
             float d_ms = 0.0f, f_ms = 0.0f;
             cudaEventElapsedTime(&d_ms, a, m);
-            cudaEventElapsedTime(&f_ms, m, b);
+            cudaEventElapsedTime(&f_ms, bm, b);
             stats->samples = ctx->world.view.nsamples;
             stats->luxels = fb.view.ncells;
             stats->visibility_rays = (int64_t)counts[0];
@@ -491,6 +563,7 @@ extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t cap
     cudaFree(d_lighting);
     if (a) cudaEventDestroy(a);
     if (m) cudaEventDestroy(m);
+    if (bm) cudaEventDestroy(bm);
     if (b) cudaEventDestroy(b);
     return rc;
 }

@@ -62,7 +62,24 @@ struct FinalBuffers {
 cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces, const vrad_sample *samples,
                         int64_t nsamples, const float *vertices, int64_t nvertices, std::string &why);
 
+// The bounced light's radial grid (FinalLightFace.BuildPatchRadial): per
+// face, the leaf patches of the face and of its smoothing neighbours whose
+// radial box reaches it, in the reference's order, with the box and the
+// patch's luxel-space centre and extent; the patches' bounced light; and
+// the per-cell accumulators.
+struct PatchRadialView {
+    const int32_t *off;      // F + 1
+    const int32_t *patch;
+    const int4 *box;         // sMin, tMin, sMax, tMax (clamped to the face)
+    const float4 *coord;     // coordS, coordT, distS, distT
+    const float4 *light;     // TotalLight.Flat per patch
+    float4 *rad_light;       // per cell
+    float *rad_weight;
+};
+
+// prad = nullptr: no bounce (-bounce 0).
 cudaError_t launch_final(const FinalView &v, const float4 *sample_light, float4 *rad_light, float *rad_weight,
-                         float4 *flat, uint8_t *lighting, int nfaces, cudaStream_t stream);
+                         float4 *flat, uint8_t *lighting, int nfaces, const PatchRadialView *prad,
+                         cudaStream_t stream);
 
 }  // namespace vrad

@@ -19,29 +19,14 @@
 #include <vector>
 
 #include "../../include/vrad_cuda.h"
+#include "host_geom.h"
 #include "world.h"
 
 namespace {
 
-struct V3 {
-    float x, y, z;
-};
-inline V3 add(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-inline V3 mul(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
-inline float dot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
-inline V3 cross(V3 a, V3 b) {
-    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
-}
-inline float length(V3 a) { return std::sqrt((a.x * a.x + a.y * a.y) + a.z * a.z); }
-inline V3 normalise(V3 a) {
-    float l = length(a);
-    if (l == 0.0f) return {0.0f, 0.0f, 0.0f};
-    return {a.x / l, a.y / l, a.z / l};
-}
+using namespace vrad::hg;
 
 constexpr float kLightmapOnEpsilon = 0.1f / 16.0f;  // LightConstants.LightmapOnEpsilon
-constexpr double kColinearDot = 0.999;              // GeometryEpsilons.ColinearDotThreshold
 constexpr double kDegenerateDet = 1.0e-20;          // FaceLightInfo.DegenerateDeterminant
 
 struct FaceFrame {
@@ -89,89 +74,6 @@ V3 luxel_to_world(const FaceFrame &fr, float s, float t) {
     t += (float)fr.min_t;
     V3 pos = add(fr.origin, mul(fr.l2w_s, s));
     return add(pos, mul(fr.l2w_t, t));
-}
-
-using Winding = std::vector<V3>;
-
-// WindingArena.RemoveColinearPoints.
-Winding remove_colinear(const Winding &w) {
-    const size_t n = w.size();
-    Winding kept;
-    for (size_t i = 0; i < n; i++) {
-        size_t j = (i + 1) % n, k = (i + n - 1) % n;
-        V3 v1 = normalise(sub(w[j], w[i]));
-        V3 v2 = normalise(sub(w[i], w[k]));
-        if ((double)dot(v1, v2) < kColinearDot) kept.push_back(w[i]);
-    }
-    return kept.size() == n ? w : kept;
-}
-
-// WindingArena.ClipEpsilon against an axis plane (normal = unit axis `ax`).
-// front: dot > dist + eps side, back: the rest.  Empty vector = null.
-void clip_axis(const Winding &in, int ax, float dist, float eps, Winding &front, Winding &back) {
-    front.clear();
-    back.clear();
-    const size_t n = in.size();
-    std::vector<float> dists(n + 1);
-    std::vector<int> sides(n + 1);  // 0 front, 1 back, 2 on
-    int counts[3] = {0, 0, 0};
-    const V3 normal = {ax == 0 ? 1.0f : 0.0f, ax == 1 ? 1.0f : 0.0f, 0.0f};
-    for (size_t i = 0; i < n; i++) {
-        float d = dot(in[i], normal);
-        d -= dist;
-        dists[i] = d;
-        sides[i] = d > eps ? 0 : (d < -eps ? 1 : 2);
-        counts[sides[i]]++;
-    }
-    sides[n] = sides[0];
-    dists[n] = dists[0];
-    if (counts[0] == 0) {
-        back = in;
-        return;
-    }
-    if (counts[1] == 0) {
-        front = in;
-        return;
-    }
-    for (size_t i = 0; i < n; i++) {
-        const V3 p1 = in[i];
-        if (sides[i] == 2) {
-            front.push_back(p1);
-            back.push_back(p1);
-            continue;
-        }
-        if (sides[i] == 0) front.push_back(p1);
-        if (sides[i] == 1) back.push_back(p1);
-        if (sides[i + 1] == 2 || sides[i + 1] == sides[i]) continue;
-        const V3 p2 = in[(i + 1) % n];
-        const float t = dists[i] / (dists[i] - dists[i + 1]);
-        auto axis = [&](float nv, float a, float b) {
-            if (nv == 1.0f) return dist;
-            if (nv == -1.0f) return -dist;
-            return a + t * (b - a);
-        };
-        V3 mid = {axis(normal.x, p1.x, p2.x), axis(normal.y, p1.y, p2.y), axis(normal.z, p1.z, p2.z)};
-        front.push_back(mid);
-        back.push_back(mid);
-    }
-}
-
-// WindingArena.AreaAndBalancePoint.
-float area_and_balance(const Winding &p, V3 &center) {
-    center = {0.0f, 0.0f, 0.0f};
-    float total = 0.0f;
-    for (size_t i = 2; i < p.size(); i++) {
-        V3 d1 = sub(p[i - 1], p[0]);
-        V3 d2 = sub(p[i], p[0]);
-        float area = length(cross(d1, d2));
-        total += area;
-        float third = (float)((double)area / 3.0);
-        center = add(center, mul(p[i - 1], third));
-        center = add(center, mul(p[i], third));
-        center = add(center, mul(p[0], third));
-    }
-    if (total != 0.0f) center = mul(center, (float)(1.0 / (double)total));
-    return total * 0.5f;
 }
 
 float world_area_per_luxel(const vrad_face &f) {
@@ -274,21 +176,16 @@ inline uint32_t fbits(float f) {
 
 }  // namespace
 
-// FaceNeighbours.Build (MapTools/Rad/Light/FaceNeighbours.cs:80-230) for
-// brush faces with smoothing groups 0: faces sharing a vertex are
-// neighbours when the cosine of their normals is at least the threshold
-// (rule 2).  Vertices are identified by position, as a BSP's vertex lump
-// welds them.  Writes offsets[nfaces + 1] and the lists, in discovery order.
-extern "C" int32_t vrad_build_neighbours(const vrad_face *faces, int32_t nfaces, const float *vertices,
-                                         int64_t nvertices, float smoothing_threshold, int32_t *offsets,
-                                         int32_t *list, int64_t capacity, int64_t *count) {
-    if (nfaces < 0 || (nfaces && (!faces || !vertices)) || !offsets || !count) return VRAD_ERR_ARG;
+namespace vrad {
+
+bool weld_faces(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
+                std::vector<std::vector<int32_t>> &face_verts, std::vector<std::vector<int32_t>> &vertex_face) {
     // Weld: one vertex number per distinct position.
     std::map<std::tuple<uint32_t, uint32_t, uint32_t>, int32_t> weld;
-    std::vector<std::vector<int32_t>> face_verts((size_t)nfaces);
+    face_verts.assign((size_t)nfaces, {});
     for (int32_t i = 0; i < nfaces; i++) {
         const vrad_face &f = faces[i];
-        if (f.first_vertex < 0 || f.first_vertex + (int64_t)f.num_vertices > nvertices) return VRAD_ERR_ARG;
+        if (f.first_vertex < 0 || f.num_vertices < 0 || f.first_vertex + (int64_t)f.num_vertices > nvertices) return false;
         for (int32_t k = 0; k < f.num_vertices; k++) {
             const float *v = vertices + 3 * (int64_t)(f.first_vertex + k);
             auto key = std::make_tuple(fbits(v[0] + 0.0f), fbits(v[1] + 0.0f), fbits(v[2] + 0.0f));
@@ -304,12 +201,54 @@ extern "C" int32_t vrad_build_neighbours(const vrad_face *faces, int32_t nfaces,
         }
     }
     // vertexFace: the faces touching each vertex, in face order, once each.
-    std::vector<std::vector<int32_t>> vertex_face(weld.size());
+    vertex_face.assign(weld.size(), {});
     for (int32_t i = 0; i < nfaces; i++)
         for (int32_t v : face_verts[(size_t)i]) {
             auto &vf = vertex_face[(size_t)v];
             if (std::find(vf.begin(), vf.end(), i) == vf.end()) vf.push_back(i);
         }
+    return true;
+}
+
+bool corner_normals(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
+                    float smoothing_threshold, std::vector<std::vector<float>> &out) {
+    std::vector<std::vector<int32_t>> face_verts, vertex_face;
+    if (!weld_faces(faces, nfaces, vertices, nvertices, face_verts, vertex_face)) return false;
+    out.assign((size_t)nfaces, {});
+    for (int32_t i = 0; i < nfaces; i++) {
+        const V3 ni = {faces[i].normal[0], faces[i].normal[1], faces[i].normal[2]};
+        std::vector<float> &o = out[(size_t)i];
+        for (int32_t v : face_verts[(size_t)i]) {
+            V3 sum = {0.0f, 0.0f, 0.0f};
+            for (int32_t other : vertex_face[(size_t)v]) {
+                if (other == i) continue;
+                const V3 no = {faces[other].normal[0], faces[other].normal[1], faces[other].normal[2]};
+                if ((double)dot(no, ni) < (double)smoothing_threshold) continue;
+                sum = add(sum, no);
+            }
+            // The face's own normal last, then the exact normalise.
+            const V3 n = normalise(add(sum, ni));
+            o.push_back(n.x);
+            o.push_back(n.y);
+            o.push_back(n.z);
+        }
+    }
+    return true;
+}
+
+}  // namespace vrad
+
+// FaceNeighbours.Build (MapTools/Rad/Light/FaceNeighbours.cs:80-230) for
+// brush faces with smoothing groups 0: faces sharing a vertex are
+// neighbours when the cosine of their normals is at least the threshold
+// (rule 2).  Vertices are identified by position, as a BSP's vertex lump
+// welds them.  Writes offsets[nfaces + 1] and the lists, in discovery order.
+extern "C" int32_t vrad_build_neighbours(const vrad_face *faces, int32_t nfaces, const float *vertices,
+                                         int64_t nvertices, float smoothing_threshold, int32_t *offsets,
+                                         int32_t *list, int64_t capacity, int64_t *count) {
+    if (nfaces < 0 || (nfaces && (!faces || !vertices)) || !offsets || !count) return VRAD_ERR_ARG;
+    std::vector<std::vector<int32_t>> face_verts, vertex_face;
+    if (!vrad::weld_faces(faces, nfaces, vertices, nvertices, face_verts, vertex_face)) return VRAD_ERR_ARG;
     int64_t written = 0;
     for (int32_t i = 0; i < nfaces; i++) {
         offsets[i] = (int32_t)written;

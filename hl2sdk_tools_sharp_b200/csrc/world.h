@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
 
 #include "../../include/vrad_cuda.h"
 
@@ -21,5 +22,17 @@ void face_frame_of(const vrad_face &f, FaceFrameOut &out);
 // LuxelToWorld / WorldToLuxel in the reference's float order.
 void frame_luxel_to_world(const FaceFrameOut &fr, float s, float t, float out[3]);
 void frame_world_to_luxel(const FaceFrameOut &fr, const float p[3], float &s, float &t);
+
+// The welded vertex numbers of each face's winding (vertices identified by
+// position) and, per vertex, the faces touching it in face order.  False
+// when a face's winding lies outside the vertex array.
+bool weld_faces(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
+                std::vector<std::vector<int32_t>> &face_verts, std::vector<std::vector<int32_t>> &vertex_face);
+
+// FaceNeighbours.Build's corner normals (FaceNeighbours.cs:230-340, rule 2):
+// per face, per winding vertex (xyz each), the normalised sum of the
+// smoothing neighbours' normals and the face's own.
+bool corner_normals(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
+                    float smoothing_threshold, std::vector<std::vector<float>> &out);
 
 }  // namespace vrad

@@ -47,7 +47,16 @@ LIGHT_DTYPE = np.dtype([
     ("start_fade_distance", "<f4"), ("end_fade_distance", "<f4"), ("cap_dist", "<f4"),
 ])
 LIGHTING_DTYPE = np.dtype([("lighting", "<f4", (3,)), ("direct_sun_amount", "<f4")])
+PATCH_DTYPE = np.dtype([
+    ("origin", "<f4", (3,)), ("area", "<f4"), ("normal", "<f4", (3,)), ("plane_dist", "<f4"),
+    ("mins", "<f4", (3,)), ("chop", "<f4"), ("maxs", "<f4", (3,)), ("lux_scale", "<f4"),
+    ("face_mins", "<f4", (3,)), ("face", "<i4"), ("face_maxs", "<f4", (3,)), ("cluster", "<i4"),
+    ("reflectivity", "<f4", (3,)), ("sky", "<i4"), ("parent", "<i4"), ("child1", "<i4"),
+    ("child2", "<i4"), ("first_point", "<i4"), ("num_points", "<i4"), ("pad", "<i4", (3,)),
+])
+TRANSFER_DTYPE = np.dtype([("patch", "<i4"), ("weight", "<f4")])
 assert FACE_DTYPE.itemsize == 80 and SAMPLE_DTYPE.itemsize == 56 and LIGHT_DTYPE.itemsize == 80
+assert PATCH_DTYPE.itemsize == 144 and TRANSFER_DTYPE.itemsize == 8
 
 EMIT_POINT, EMIT_SPOT, EMIT_SKY, EMIT_AMBIENT = 1, 2, 3, 4
 EQUAL_EPSILON = np.float32(0.001)
@@ -68,6 +77,20 @@ class PassStats(ctypes.Structure):
     _fields_ = [("samples", ctypes.c_int64), ("luxels", ctypes.c_int64), ("visibility_rays", ctypes.c_int64),
                 ("sky_rays", ctypes.c_int64), ("lighting_bytes", ctypes.c_int64), ("direct_ms", ctypes.c_float),
                 ("final_ms", ctypes.c_float)]
+
+
+class _BounceDesc(ctypes.Structure):
+    _fields_ = [("reflectivity", ctypes.c_void_p), ("pvs_offsets", ctypes.c_void_p),
+                ("pvs_clusters", ctypes.c_void_p), ("nclusters", ctypes.c_int32), ("max_chop", ctypes.c_float),
+                ("min_chop", ctypes.c_float), ("bounces", ctypes.c_int32), ("threshold", ctypes.c_float)]
+
+
+class BounceStats(ctypes.Structure):
+    _fields_ = [("patches", ctypes.c_int64), ("receivers", ctypes.c_int64), ("transfer_rays", ctypes.c_int64),
+                ("blocked", ctypes.c_int64), ("transfers", ctypes.c_int64), ("bounces", ctypes.c_int32),
+                ("exact_totals", ctypes.c_int32), ("added", ctypes.c_double * 3),
+                ("patch_light_ms", ctypes.c_float), ("transfer_ms", ctypes.c_float),
+                ("bounce_ms", ctypes.c_float), ("final_ms", ctypes.c_float)]
 
 
 class DirectStats(ctypes.Structure):
@@ -99,6 +122,17 @@ def _lib():
         lib.vrad_light_pass.restype = i32
         lib.vrad_light_pass_device.argtypes = [P, P, P]
         lib.vrad_light_pass_device.restype = i32
+        lib.vrad_build_patches.argtypes = [P, i32, P, i64, P, ctypes.c_float, ctypes.c_float, P, i64,
+                                           ctypes.POINTER(i64), P, i64, ctypes.POINTER(i64)]
+        lib.vrad_build_patches.restype = i32
+        lib.vrad_bounce_upload.argtypes = [P, ctypes.POINTER(_BounceDesc)]
+        lib.vrad_bounce_upload.restype = i32
+        lib.vrad_bounce_stats_get.argtypes = [P, ctypes.POINTER(BounceStats)]
+        lib.vrad_bounce_stats_get.restype = i32
+        lib.vrad_bounce_patch_light.argtypes = [P, P, P, i64]
+        lib.vrad_bounce_patch_light.restype = i32
+        lib.vrad_bounce_transfers.argtypes = [P, P, i64, P, i64, ctypes.POINTER(i64)]
+        lib.vrad_bounce_transfers.restype = i32
         lib._lighting_bound = True
     return lib
 
@@ -142,6 +176,43 @@ def build_samples(faces: np.ndarray, verts: np.ndarray):
     if rc != 0:
         raise ValueError(f"vrad_build_samples failed ({rc})")
     return out, first
+
+
+def build_patches(faces: np.ndarray, verts: np.ndarray, reflectivity: np.ndarray, max_chop: float = 4.0,
+                  min_chop: float = 4.0):
+    """PatchBuilder + PatchSubdivider (native): the patch records in the
+    reference's index order and the winding points (n, 3)."""
+    lib = _lib()
+    faces = np.ascontiguousarray(faces, FACE_DTYPE)
+    verts = np.ascontiguousarray(verts, np.float32)
+    refl = np.ascontiguousarray(reflectivity, np.float32).reshape(-1, 3)
+    n, m = ctypes.c_int64(), ctypes.c_int64()
+    rc = lib.vrad_build_patches(faces.ctypes.data, len(faces), verts.ctypes.data, len(verts), refl.ctypes.data,
+                                max_chop, min_chop, None, 0, ctypes.byref(n), None, 0, ctypes.byref(m))
+    if rc != 0:
+        raise ValueError(f"vrad_build_patches failed ({rc})")
+    out = np.zeros(n.value, PATCH_DTYPE)
+    pts = np.zeros((max(1, m.value), 3), np.float32)
+    rc = lib.vrad_build_patches(faces.ctypes.data, len(faces), verts.ctypes.data, len(verts), refl.ctypes.data,
+                                max_chop, min_chop, out.ctypes.data, len(out), ctypes.byref(n), pts.ctypes.data,
+                                m.value, ctypes.byref(m))
+    if rc != 0:
+        raise ValueError(f"vrad_build_patches failed ({rc})")
+    return out, pts[:m.value]
+
+
+def face_reflectivity(world: World) -> np.ndarray:
+    """Each lit face's material reflectivity (F, 3)."""
+    return np.ascontiguousarray(world.reflectivity[world.face_material], np.float32)
+
+
+def pvs_lists(world: World):
+    """The PVS as CSR: per cluster, the clusters its row sets, ascending."""
+    C = world.pvs.shape[0]
+    rows = [np.flatnonzero(world.pvs[c]).astype(np.int32) for c in range(C)]
+    off = np.zeros(C + 1, np.int32)
+    off[1:] = np.cumsum([len(r) for r in rows])
+    return off, (np.concatenate(rows) if rows else np.zeros(0, np.int32)).astype(np.int32)
 
 
 def build_neighbours(faces: np.ndarray, verts: np.ndarray, threshold: float = 0.7071067):
@@ -324,6 +395,45 @@ class LightingStage:
         T._check(_lib().vrad_world_upload(self._ctx, ctypes.byref(d)), self._ctx)
         self.inputs = i
 
+    def upload_bounce(self, reflectivity: np.ndarray, pvs_offsets: np.ndarray, pvs_clusters: np.ndarray,
+                      bounces: int = 100, threshold: float = 1.0, max_chop: float = 4.0,
+                      min_chop: float = 4.0) -> None:
+        """vrad_bounce_upload: the patch tree and the transfer tables; every
+        later light pass bounces (Radiosity.BounceAsync's stop rule: at most
+        `bounces` bounces, or until one adds less than `threshold`)."""
+        refl = np.ascontiguousarray(reflectivity, np.float32).reshape(-1, 3)
+        off = np.ascontiguousarray(pvs_offsets, np.int32)
+        lst = np.ascontiguousarray(pvs_clusters, np.int32)
+        self._bounce_keep = (refl, off, lst)
+        d = _BounceDesc(refl.ctypes.data, off.ctypes.data, lst.ctypes.data if len(lst) else None, len(off) - 1,
+                        max_chop, min_chop, bounces, threshold)
+        T._check(_lib().vrad_bounce_upload(self._ctx, ctypes.byref(d)), self._ctx)
+
+    def bounce_stats(self) -> BounceStats:
+        st = BounceStats()
+        T._check(_lib().vrad_bounce_stats_get(self._ctx, ctypes.byref(st)), self._ctx)
+        return st
+
+    def patch_light(self):
+        """After a light pass: (TotalLight (P, 3), DirectLight (P, 3))."""
+        n = self.bounce_stats().patches
+        total = np.zeros((n, 3), np.float32)
+        direct = np.zeros((n, 3), np.float32)
+        T._check(_lib().vrad_bounce_patch_light(self._ctx, total.ctypes.data, direct.ctypes.data, n), self._ctx)
+        return total, direct
+
+    def transfers(self):
+        """After a light pass: (offsets by patch (P + 1), TRANSFER_DTYPE records)."""
+        n = self.bounce_stats().patches
+        off = np.zeros(n + 1, np.int64)
+        count = ctypes.c_int64()
+        T._check(_lib().vrad_bounce_transfers(self._ctx, off.ctypes.data, n, None, 0, ctypes.byref(count)),
+                 self._ctx)
+        tr = np.zeros(max(1, count.value), TRANSFER_DTYPE)
+        T._check(_lib().vrad_bounce_transfers(self._ctx, off.ctypes.data, n, tr.ctypes.data, len(tr),
+                                              ctypes.byref(count)), self._ctx)
+        return off, tr[:count.value]
+
     def close(self):
         self.tracer.close()
 
@@ -354,8 +464,8 @@ class LightingStage:
         return n.value
 
     def light_pass(self, lighting: np.ndarray | None = None):
-        """vrad_light_pass (bounce 0): the LIGHTING lump bytes, each face's
-        lightofs, and the stats."""
+        """vrad_light_pass: the LIGHTING lump bytes, each face's lightofs, and
+        the stats (with the bounce when upload_bounce ran)."""
         if lighting is None:
             lighting = np.zeros(self.lighting_size(), np.uint8)
         ofs = np.zeros(len(self.inputs.faces), np.int32)

@@ -317,6 +317,120 @@ int32_t vrad_light_pass_device(vrad_ctx *ctx, uint8_t *d_lighting, void *stream)
  * reference (its CPU work queue has no launch shape). */
 int32_t vrad_direct_autotune(vrad_ctx *ctx, int32_t *chosen_block, float *times_ms);
 
+/* ---- Bounce ---------------------------------------------------------------
+ *
+ * The radiosity bounce of the lighting stage (the reference's
+ * RadWorld.BounceAsync, MapTools/Rad/Light/RadWorld.Bounce.cs:240-290):
+ * the patch tree (PatchBuilder, PatchSubdivider), the patches' direct light
+ * (PatchLighting.BuildPatchLights), the transfers (VisMatrix.BuildAsync
+ * with FormFactors), the bounces (Radiosity.BounceAsync) and the bounced
+ * light's radial filter in the final pass (FinalLightFace.BuildPatchRadial).
+ * The replaced stage boundary is IVradBounceStage.BounceAsync
+ * (MapTools/Rad/VradStages.cs:112-183), whose contract is that the
+ * patches' TotalLight holds the bounced light only. */
+
+/* Texinfo surface flags (SurfaceFlags) read from vrad_face.flags. */
+#define VRAD_SURF_LIGHT 0x0001
+#define VRAD_SURF_SKY 0x0004
+#define VRAD_SURF_NOLIGHT 0x0400
+#define VRAD_SURF_BUMPLIGHT 0x0800
+#define VRAD_SURF_NOCHOP 0x4000
+
+/* Patch (MapTools/Rad/Light/Patch.cs:44-234), the fields the bounce reads.
+ * normal is the shading normal (the plane normal for a root, the phong
+ * normal at the origin for a child); plane_dist is the face plane's.
+ * cluster is the cluster of the patch's face; the winding is num_points
+ * points from first_point of the point array vrad_build_patches fills. */
+typedef struct vrad_patch {
+    float origin[3];
+    float area;
+    float normal[3];
+    float plane_dist;
+    float mins[3];
+    float chop;
+    float maxs[3];
+    float lux_scale;
+    float face_mins[3];
+    int32_t face;
+    float face_maxs[3];
+    int32_t cluster;
+    float reflectivity[3];
+    int32_t sky;
+    int32_t parent;
+    int32_t child1;
+    int32_t child2;
+    int32_t first_point;
+    int32_t num_points;
+    int32_t pad[3];
+} vrad_patch;
+
+/* PatchBuilder.Build + PatchSubdivider.Subdivide (bounces > 0, not -fast)
+ * on the host: one root patch per face in face order, then each root's
+ * subtree in creation order, the reference's patch indices.  reflectivity
+ * is nfaces x 3 (the faces' texdata reflectivity, clamped to 0.99 here);
+ * max_chop / min_chop in luxels (the reference's defaults are 4 and 4).
+ * With out and points NULL it only counts. */
+int32_t vrad_build_patches(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
+                           const float *reflectivity, float max_chop, float min_chop, vrad_patch *out,
+                           int64_t capacity, int64_t *count, float *points, int64_t point_capacity,
+                           int64_t *point_count);
+
+/* What the bounce reads beyond the world: per-face reflectivity, the PVS
+ * (per cluster, the clusters its row sets, ascending), the chop sizes and
+ * the stop rule.  Radiosity.BounceAsync stops after `bounces` bounces or
+ * once a bounce adds less than `threshold` in every channel (the
+ * reference's threshold is 1.0). */
+typedef struct vrad_bounce_desc {
+    const float *reflectivity;     /* nfaces x 3 */
+    const int32_t *pvs_offsets;    /* nclusters + 1 */
+    const int32_t *pvs_clusters;
+    int32_t nclusters;
+    float max_chop;
+    float min_chop;
+    int32_t bounces;               /* 0: the light pass does not bounce */
+    float threshold;
+} vrad_bounce_desc;
+
+/* Builds the patch tree for the uploaded world (vrad_world_upload first,
+ * with face windings) and keeps it, with the transfer and final-pass
+ * tables, on the device: every later vrad_light_pass then bounces.
+ * VRAD_ERR_UNSUPPORTED for bumped faces. */
+int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *desc);
+
+typedef struct vrad_bounce_stats {
+    int64_t patches;
+    int64_t receivers;        /* leaf patches in a cluster (VisMatrix.ReceiverOrder) */
+    int64_t transfer_rays;    /* candidate pairs traced (VisMatrixStatistics.Rays) */
+    int64_t blocked;          /* of them, blocked */
+    int64_t transfers;
+    int32_t bounces;          /* bounces run */
+    int32_t exact_totals;     /* stop decisions the bounded fp64 total could not settle */
+    double added[3];          /* light the last bounce added, over leaf patches */
+    float patch_light_ms;
+    float transfer_ms;
+    float bounce_ms;
+    float final_ms;
+} vrad_bounce_stats;
+
+/* The statistics of the last light pass's bounce. */
+int32_t vrad_bounce_stats_get(vrad_ctx *ctx, vrad_bounce_stats *stats);
+
+/* After a light pass: each patch's bounced light (TotalLight.Flat) and
+ * direct light (DirectLight), npatches x 3 each; either may be NULL. */
+int32_t vrad_bounce_patch_light(vrad_ctx *ctx, float *total_light, float *direct_light, int64_t npatches);
+
+/* Transfer (MapTools/Rad/Bounce/TransferSet.cs:26): source patch, weight. */
+typedef struct vrad_transfer {
+    int32_t patch;
+    float weight;
+} vrad_transfer;
+
+/* After a light pass: the transfer lists by receiving patch,
+ * offsets[npatches + 1] (TransferSet.For(patch) = transfers[offsets[p] ..
+ * offsets[p + 1])).  With transfers NULL it only fills offsets and count. */
+int32_t vrad_bounce_transfers(vrad_ctx *ctx, int64_t *offsets, int64_t npatches, vrad_transfer *transfers,
+                              int64_t capacity, int64_t *count);
+
 /* Largest batch vrad_trace_visibility_static accepts: four of the
  * reference's 16,384-ray batches. */
 #define VRAD_STATIC_MAX_RAYS 65536
@@ -338,6 +452,17 @@ int32_t vrad_direct_autotune(vrad_ctx *ctx, int32_t *chosen_block, float *times_
  * caller.  The call blocks until the bits are written. */
 int32_t vrad_trace_visibility_static(vrad_ctx *ctx, const vrad_ray *rays, int64_t n,
                                      const vrad_trace_options *opts, uint64_t *hit_bits);
+
+/* DetMathF.Asin / DetMathF.Pow (MapFormats/Numerics/DetMathF.cs:141-164,
+ * 265-292) as the device computes them inside the transfer build and the
+ * spotlight falloff: the float nearest the exact value.  out[i] = asin a[i]
+ * or a[i]^b[i] (b unused for the arcsine).  open (nullable) receives how
+ * many results sat so near a rounding midpoint that the device could not
+ * settle them (expected 0).  Host buffers; blocks. */
+#define VRAD_DETMATH_ASIN 0
+#define VRAD_DETMATH_POW 1
+int32_t vrad_detmath(vrad_ctx *ctx, int32_t fn, const float *a, const float *b, float *out, int64_t n,
+                     int64_t *open);
 
 /* IRayTracer.TracerIdentity: backend, device and build, one token. */
 int32_t vrad_tracer_identity(vrad_ctx *ctx, char *buf, int32_t cap);

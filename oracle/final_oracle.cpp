@@ -19,6 +19,7 @@
 #include <tuple>
 #include <vector>
 
+#include "oracle_internal.h"
 #include "vrad_oracle.h"
 
 namespace {
@@ -132,6 +133,37 @@ struct Radial {
         }
     }
 
+    // LuxelRadial.AddBounced (LuxelRadial.cs:238-307), unbumped.
+    void add_bounced(P3 point, float minS, float minT, float maxS, float maxT, const float *lv) {
+        float cs, ct;
+        w2l(fr, point, cs, ct);
+        float distS = maxS - minS, distT = maxT - minT;
+        distS = (float)(1.0 > (double)distS ? 1.0 : (double)distS);
+        distT = (float)(1.0 > (double)distT ? 1.0 : (double)distT);
+        int sMin = (int)((double)cs - (double)distS * 1.42);
+        int tMin = (int)((double)ct - (double)distT * 1.42);
+        int sMax = (int)((double)cs + (double)distS * 1.42 + 1.0f);
+        int tMax = (int)((double)ct + (double)distT * 1.42 + 1.0f);
+        sMin = std::max(sMin, 0);
+        tMin = std::max(tMin, 0);
+        sMax = std::min(sMax, fr.w);
+        tMax = std::min(tMax, fr.h);
+        for (int s = sMin; s < sMax; s++) {
+            for (int t = tMin; t < tMax; t++) {
+                float ds = (cs - (float)s) / distS;
+                float dt = (ct - (float)t) / distT;
+                float r = 2.0f - (ds * ds + dt * dt);
+                size_t i = (size_t)(s + t * fr.w);
+                if (r > 0) {
+                    light[4 * i + 0] = light[4 * i + 0] + r * lv[0];
+                    light[4 * i + 1] = light[4 * i + 1] + r * lv[1];
+                    light[4 * i + 2] = light[4 * i + 2] + r * lv[2];
+                    weight[i] += r;
+                }
+            }
+        }
+    }
+
     bool sample(P3 point, float out[3]) const {
         float cs, ct;
         w2l(fr, point, cs, ct);
@@ -204,9 +236,9 @@ extern "C" int orc_neighbours(const orc_face *faces, int32_t nfaces, const float
     return 0;
 }
 
-extern "C" int orc_final(const orc_face *faces, int32_t nfaces, const float *verts, const orc_sample *samples,
-                         const int64_t *face_first, const float *sample_light, uint8_t *lighting,
-                         int64_t capacity, int32_t *lightofs, int64_t *total) {
+int orc_final_impl(const orc_face *faces, int32_t nfaces, const float *verts, const orc_sample *samples,
+                   const int64_t *face_first, const float *sample_light, uint8_t *lighting, int64_t capacity,
+                   int32_t *lightofs, int64_t *total, const OrcBounced *bounced) {
     // LightmapOffsets.Compute: style 0 on every lit face.
     int64_t size = 0;
     std::vector<int32_t> ofs((size_t)nfaces);
@@ -227,7 +259,7 @@ extern "C" int orc_final(const orc_face *faces, int32_t nfaces, const float *ver
     orc_neighbours(faces, nfaces, verts, 0.7071067f, noff.data(), nlist.data(), nn, &nn);
     std::vector<Frame> frames((size_t)nfaces);
     for (int f = 0; f < nfaces; f++) frames[(size_t)f] = frame(faces[f]);
-    Radial rad;
+    Radial rad, prad;
     std::vector<float> red, green, blue;
     for (int f = 0; f < nfaces; f++) {
         const Frame &fr = frames[(size_t)f];
@@ -250,6 +282,27 @@ extern "C" int orc_final(const orc_face *faces, int32_t nfaces, const float *ver
                                sample_light + 4 * k);
             }
         }
+        // BuildPatchRadial: the leaf patches of the face, then of each
+        // neighbour (AddFacePatches), splatted with their bounced light.
+        if (bounced) {
+            prad.reset(fr);
+            std::vector<int> order = {f};
+            for (int q = noff[(size_t)f]; q < noff[(size_t)f + 1]; q++) order.push_back(nlist[(size_t)q]);
+            for (int g : order)
+                for (const OrcBouncedPatch &bp : bounced->face_leaves[(size_t)g]) {
+                    // PatchLightmapCoordRange in this face's luxel space.
+                    float minS = 1e30f, minT = 1e30f, maxS = -1e30f, maxT = -1e30f;
+                    for (size_t k = 0; k + 2 < bp.winding.size(); k += 3) {
+                        float ps, pt;
+                        w2l(fr, {bp.winding[k], bp.winding[k + 1], bp.winding[k + 2]}, ps, pt);
+                        minS = minS < ps ? minS : ps;
+                        maxS = maxS > ps ? maxS : ps;
+                        minT = minT < pt ? minT : pt;
+                        maxT = maxT > pt ? maxT : pt;
+                    }
+                    prad.add_bounced({bp.origin[0], bp.origin[1], bp.origin[2]}, minS, minT, maxS, maxT, bp.light);
+                }
+        }
         // Each luxel: Sample at its own position, minlight 0, encode.
         red.clear();
         green.clear();
@@ -260,6 +313,11 @@ extern "C" int orc_final(const orc_face *faces, int32_t nfaces, const float *ver
             const int s = j % fr.w, t = j / fr.w;
             float lb[3];
             bool ok = rad.sample(l2w(fr, (float)s, (float)t), lb);
+            if (bounced) {
+                float v[3];
+                (void)prad.sample(l2w(fr, (float)s, (float)t), v);
+                for (int c = 0; c < 3; c++) lb[c] = lb[c] + v[c];
+            }
             if (no_samples) {
                 lb[0] = 255.0f;
                 lb[1] = lb[2] = 0.0f;
@@ -287,4 +345,11 @@ extern "C" int orc_final(const orc_face *faces, int32_t nfaces, const float *ver
         std::memcpy(lighting + ofs[(size_t)f] - 4, &w, 4);
     }
     return 0;
+}
+
+extern "C" int orc_final(const orc_face *faces, int32_t nfaces, const float *verts, const orc_sample *samples,
+                         const int64_t *face_first, const float *sample_light, uint8_t *lighting,
+                         int64_t capacity, int32_t *lightofs, int64_t *total) {
+    return orc_final_impl(faces, nfaces, verts, samples, face_first, sample_light, lighting, capacity, lightofs,
+                          total, nullptr);
 }

@@ -264,3 +264,145 @@ def final(faces, verts, samples, face_first, sample_light):
     if rc != 0:
         raise RuntimeError(f"orc_final failed: {rc}")
     return out, ofs
+
+
+# Patch, 144 bytes (the library's vrad_patch layout).
+PATCH_DTYPE = np.dtype([
+    ("origin", "<f4", (3,)), ("area", "<f4"), ("normal", "<f4", (3,)), ("plane_dist", "<f4"),
+    ("mins", "<f4", (3,)), ("chop", "<f4"), ("maxs", "<f4", (3,)), ("lux_scale", "<f4"),
+    ("face_mins", "<f4", (3,)), ("face", "<i4"), ("face_maxs", "<f4", (3,)), ("cluster", "<i4"),
+    ("reflectivity", "<f4", (3,)), ("sky", "<i4"), ("parent", "<i4"), ("child1", "<i4"),
+    ("child2", "<i4"), ("first_point", "<i4"), ("num_points", "<i4"), ("pad", "<i4", (3,)),
+])
+assert PATCH_DTYPE.itemsize == 144
+
+
+class _BounceIn(ctypes.Structure):
+    _fields_ = [
+        ("faces", ctypes.c_void_p), ("nfaces", ctypes.c_int32), ("verts", ctypes.c_void_p),
+        ("samples", ctypes.c_void_p), ("face_first", ctypes.c_void_p), ("reflectivity", ctypes.c_void_p),
+        ("pvs_off", ctypes.c_void_p), ("pvs_list", ctypes.c_void_p), ("nclusters", ctypes.c_int32),
+        ("max_chop", ctypes.c_float), ("min_chop", ctypes.c_float), ("bounces", ctypes.c_int32),
+        ("threshold", ctypes.c_float), ("nodes", ctypes.c_void_p), ("indices", ctypes.c_void_p),
+        ("tris", ctypes.c_void_p), ("bounds6", ctypes.c_void_p), ("threads", ctypes.c_int32),
+    ]
+
+
+def _bounce_lib():
+    L = lib()
+    if not getattr(L, "_bounce_typed", False):
+        P = ctypes.c_void_p
+        i32, i64, f32 = ctypes.c_int32, ctypes.c_int64, ctypes.c_float
+        L.orc_bounce_new.argtypes = [P]
+        L.orc_bounce_new.restype = P
+        L.orc_bounce_free.argtypes = [P]
+        L.orc_bounce_free.restype = None
+        L.orc_bounce_patches.argtypes = [P, P, i64, P, P, i64, P]
+        L.orc_bounce_transfers.argtypes = [P, P, i32, P, P, P, i64, P, P]
+        L.orc_bounce_set_transfers.argtypes = [P, P, P, P]
+        L.orc_bounce_run.argtypes = [P, P, P, P, P, P]
+        L.orc_bounce_final.argtypes = [P, P, P, i64, P, P]
+        L.orc_bounce_stats.argtypes = [P, P]
+        L.orc_bounce_stats.restype = i64
+        L.orc_asin.argtypes = [f32]
+        L.orc_asin.restype = f32
+        L._bounce_typed = True
+    return L
+
+
+def asin(x: float) -> float:
+    """DetMathF.Asin as the oracle computes it."""
+    return _bounce_lib().orc_asin(float(x))
+
+
+class Bounce:
+    """The bounce restated (patches, patch light, transfers, radiosity and
+    the final pass with the bounced light) over one world."""
+
+    def __init__(self, tree: dict, faces, verts, samples, face_first, reflectivity, pvs_off, pvs_list,
+                 max_chop: float = 4.0, min_chop: float = 4.0, bounces: int = 100, threshold: float = 1.0,
+                 threads: int | None = None):
+        self._keep = dict(
+            faces=np.ascontiguousarray(faces), verts=np.ascontiguousarray(verts, np.float32),
+            samples=np.ascontiguousarray(samples), face_first=np.ascontiguousarray(face_first, np.int64),
+            refl=np.ascontiguousarray(reflectivity, np.float32).reshape(-1, 3),
+            pvs_off=np.ascontiguousarray(pvs_off, np.int32), pvs_list=np.ascontiguousarray(pvs_list, np.int32),
+            nodes=np.ascontiguousarray(tree["nodes"], dtype=NODE_DTYPE),
+            idx=np.ascontiguousarray(tree["indices"], dtype=np.int32),
+            tris=np.ascontiguousarray(tree["tris"], dtype=TRI_DTYPE),
+            bounds=np.ascontiguousarray(tree["bounds"], dtype=np.float32))
+        k = self._keep
+        self._in = _BounceIn(_p(k["faces"]), len(k["faces"]), _p(k["verts"]), _p(k["samples"]),
+                             _p(k["face_first"]), _p(k["refl"]), _p(k["pvs_off"]), _p(k["pvs_list"]),
+                             len(k["pvs_off"]) - 1, max_chop, min_chop, bounces, threshold, _p(k["nodes"]),
+                             _p(k["idx"]), _p(k["tris"]), _p(k["bounds"]),
+                             threads if threads is not None else default_threads())
+        self._h = _bounce_lib().orc_bounce_new(ctypes.byref(self._in))
+        self.npatches = len(self.patches()[0])
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _bounce_lib().orc_bounce_free(h)
+            self._h = None
+
+    def patches(self):
+        """(patch records, winding points (n, 3))."""
+        L = _bounce_lib()
+        n, m = ctypes.c_int64(), ctypes.c_int64()
+        L.orc_bounce_patches(self._h, None, 0, ctypes.byref(n), None, 0, ctypes.byref(m))
+        out = np.zeros(n.value, PATCH_DTYPE)
+        pts = np.zeros((max(1, m.value), 3), np.float32)
+        L.orc_bounce_patches(self._h, _p(out), n.value, ctypes.byref(n), _p(pts), m.value, ctypes.byref(m))
+        return out, pts[:m.value]
+
+    def transfers(self, receivers=None):
+        """VisMatrix for the receivers (patch indices; None = all): (offsets by
+        patch, sources, weights, rays traced)."""
+        L = _bounce_lib()
+        recv = None if receivers is None else np.ascontiguousarray(receivers, np.int32)
+        off = np.zeros(self.npatches + 1, np.int64)
+        count, rays = ctypes.c_int64(), ctypes.c_int64()
+        rc = L.orc_bounce_transfers(self._h, _p(recv), 0 if recv is None else len(recv), _p(off), None, None, 0,
+                                    ctypes.byref(count), ctypes.byref(rays))
+        if rc != 0:
+            raise RuntimeError(f"orc_bounce_transfers failed: {rc}")
+        src = np.zeros(max(1, count.value), np.int32)
+        w = np.zeros(max(1, count.value), np.float32)
+        # The lists are kept from the first call; this one only copies them.
+        rc = L.orc_bounce_transfers(self._h, _p(recv), 0 if recv is None else len(recv), _p(off), _p(src), _p(w),
+                                    count.value, ctypes.byref(count), None)
+        if rc != 0:
+            raise RuntimeError(f"orc_bounce_transfers failed: {rc}")
+        return off, src[:count.value], w[:count.value], rays.value
+
+    def set_transfers(self, offsets, src, weight):
+        self._tr = (np.ascontiguousarray(offsets, np.int64), np.ascontiguousarray(src, np.int32),
+                    np.ascontiguousarray(weight, np.float32))
+        _bounce_lib().orc_bounce_set_transfers(self._h, *(_p(a) for a in self._tr))
+
+    def run(self, sample_light):
+        """(TotalLight (P, 3), DirectLight (P, 3), bounces run, last total)."""
+        light = np.ascontiguousarray(sample_light, np.float32).reshape(-1, 4)
+        total = np.zeros((self.npatches, 3), np.float32)
+        direct = np.zeros((self.npatches, 3), np.float32)
+        n = ctypes.c_int32()
+        added = np.zeros(3, np.float32)
+        rc = _bounce_lib().orc_bounce_run(self._h, _p(light), _p(total), _p(direct), ctypes.byref(n), _p(added))
+        if rc != 0:
+            raise RuntimeError(f"orc_bounce_run failed: {rc}")
+        return total, direct, n.value, added
+
+    def final(self, sample_light):
+        """FinalLightFace with the last run's bounced light: (LIGHTING, lightofs)."""
+        L = _bounce_lib()
+        light = np.ascontiguousarray(sample_light, np.float32).reshape(-1, 4)
+        total = ctypes.c_int64()
+        nf = len(self._keep["faces"])
+        ofs = np.zeros(nf, np.int32)
+        L.orc_bounce_final(self._h, _p(light), None, 0, _p(ofs), ctypes.byref(total))
+        out = np.zeros(total.value, np.uint8)
+        rc = L.orc_bounce_final(self._h, _p(light), _p(out), len(out), _p(ofs), ctypes.byref(total))
+        if rc != 0:
+            raise RuntimeError(f"orc_bounce_final failed: {rc}")
+        return out, ofs

@@ -12,3 +12,23 @@ struct OrcKd {
 };
 
 bool orc_kd_segment_blocked(const OrcKd &kd, const orc_ray &r, bool sky_pass);
+
+#include <vector>
+
+// A leaf patch as the final pass's bounced radial reads it
+// (FinalLightFace.AddFacePatches): winding (xyz each), origin, TotalLight.
+struct OrcBouncedPatch {
+    std::vector<float> winding;
+    float origin[3];
+    float light[3];
+};
+
+// Per face, its leaf patches in FacePatches order.
+struct OrcBounced {
+    std::vector<std::vector<OrcBouncedPatch>> face_leaves;
+};
+
+// FinalLightFace over every face; bounced = nullptr for -bounce 0.
+int orc_final_impl(const orc_face *faces, int32_t nfaces, const float *verts, const orc_sample *samples,
+                   const int64_t *face_first, const float *sample_light, uint8_t *lighting, int64_t capacity,
+                   int32_t *lightofs, int64_t *total, const OrcBounced *bounced);

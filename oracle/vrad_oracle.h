@@ -160,6 +160,84 @@ int orc_final(const orc_face *faces, int32_t nfaces, const float *verts, const o
               const int64_t *face_first, const float *sample_light, uint8_t *lighting,
               int64_t capacity, int32_t *lightofs, int64_t *total);
 
+/* ---- bounce ------------------------------------------------------------- */
+
+/* Patch (Patch.cs), the fields compared with the library's vrad_patch;
+ * same layout. */
+typedef struct orc_patch {
+    float origin[3];
+    float area;
+    float normal[3];
+    float plane_dist;
+    float mins[3];
+    float chop;
+    float maxs[3];
+    float lux_scale;
+    float face_mins[3];
+    int32_t face;
+    float face_maxs[3];
+    int32_t cluster;
+    float reflectivity[3];
+    int32_t sky;
+    int32_t parent;
+    int32_t child1;
+    int32_t child2;
+    int32_t first_point;
+    int32_t num_points;
+    int32_t pad[3];
+} orc_patch;
+
+/* A world for the bounce: faces and windings, samples (face-major, with
+ * face_first), per-face reflectivity, the PVS (per cluster, ascending
+ * clusters), chop sizes, the stop rule, the KD scene for the transfer rays
+ * and a thread count. */
+typedef struct orc_bounce_in {
+    const orc_face *faces;
+    int32_t nfaces;
+    const float *verts;
+    const orc_sample *samples;
+    const int64_t *face_first;
+    const float *reflectivity;
+    const int32_t *pvs_off;
+    const int32_t *pvs_list;
+    int32_t nclusters;
+    float max_chop;
+    float min_chop;
+    int32_t bounces;
+    float threshold;
+    const orc_kdnode *nodes;
+    const int32_t *indices;
+    const orc_tri *tris;
+    const float *bounds6;
+    int32_t threads;
+} orc_bounce_in;
+
+/* PatchBuilder + PatchSubdivider; returns a handle. */
+void *orc_bounce_new(const orc_bounce_in *in);
+void orc_bounce_free(void *h);
+/* The patches and their windings (counts only with out and points NULL). */
+int orc_bounce_patches(void *h, orc_patch *out, int64_t capacity, int64_t *count, float *points,
+                       int64_t point_capacity, int64_t *point_count);
+/* VisMatrix for the given receivers (patch indices; NULL = every receiver
+ * in ReceiverOrder), lists by patch index in offsets[npatches + 1]; rays =
+ * candidate rays traced.  src / weight NULL: counts only. */
+int orc_bounce_transfers(void *h, const int32_t *receivers, int32_t nreceivers, int64_t *offsets, int32_t *src,
+                         float *weight, int64_t capacity, int64_t *count, int64_t *rays);
+/* Replaces the transfers (lists by patch index). */
+int orc_bounce_set_transfers(void *h, const int64_t *offsets, const int32_t *src, const float *weight);
+/* BuildPatchLights from the direct sample light (4 floats per sample), then
+ * (building every transfer first unless set) Radiosity.BounceAsync.
+ * Outputs per patch xyz: TotalLight.Flat and DirectLight. */
+int orc_bounce_run(void *h, const float *sample_light, float *total_light, float *direct_light,
+                   int32_t *bounces_run, float *added);
+/* FinalLightFace for every face with the bounced light of the last run. */
+int orc_bounce_final(void *h, const float *sample_light, uint8_t *lighting, int64_t capacity, int32_t *lightofs,
+                     int64_t *total);
+/* Rays traced so far; *blocked of them blocked. */
+int64_t orc_bounce_stats(void *h, int64_t *blocked);
+/* DetMathF.Asin as the oracle computes it. */
+float orc_asin(float x);
+
 #ifdef __cplusplus
 }
 #endif

@@ -77,3 +77,14 @@ def load(prefix: str) -> dict:
         "tree": {"nodes": nodes, "indices": indices, "tris": tri48, "bounds": bounds},
         "stock_tris": tri48, "hit": hit, "dist": dist,
     }
+
+
+def detmath(function: str):
+    """Rows of the reference's DetMath golden table for one function
+    ("Asin" or "Pow"): (a, b, expected) as uint32 bit patterns."""
+    rows = [line.split() for line in (HERE / "detmath-goldens.txt").read_text().splitlines() if line.strip()]
+    sel = [r for r in rows if r[0] == function]
+    a = np.array([int(r[1], 16) for r in sel], np.uint32)
+    b = np.array([int(r[2], 16) for r in sel], np.uint32)
+    e = np.array([int(r[3], 16) for r in sel], np.uint32)
+    return a, b, e

@@ -1,0 +1,127 @@
+"""GPU parity of the bounce against the oracle's restatement of the
+reference's PatchLighting, VisMatrix, FormFactors, Radiosity and
+FinalLightFace.BuildPatchRadial.
+
+The bar is bit-exact: every transfer (source and weight bits), every
+patch's direct and bounced light, the number of bounces the stop rule runs,
+and the LIGHTING lump's bytes."""
+import numpy as np
+import pytest
+
+import fixtures
+from hl2sdk_tools_sharp_b200 import lighting as L, roomgrid as rg, tracer as T
+
+pytestmark = pytest.mark.gpu
+
+
+def _stage(cfg, threshold=1.0, bounces=100):
+    w = rg.generate(cfg)
+    inp = L.prepare(w)
+    st = L.LightingStage(w, inp)
+    off, lst = L.pvs_lists(w)
+    st.upload_bounce(L.face_reflectivity(w), off, lst, bounces=bounces, threshold=threshold)
+    return w, inp, st
+
+
+def _oracle(O, w, inp, threshold=1.0, bounces=100):
+    tree = O.kd_build(w.tri_verts, w.tri_ids)
+    off, lst = L.pvs_lists(w)
+    return O.Bounce(tree, inp.faces, inp.verts, inp.samples, inp.face_first, L.face_reflectivity(w), off, lst,
+                    bounces=bounces, threshold=threshold)
+
+
+def _sample_light(st):
+    s, _ = st.direct()
+    return np.concatenate([s["lighting"], s["direct_sun_amount"][:, None]], 1)
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def test_detmath_asin_and_pow_match_goldens():
+    import ctypes
+    tr = T.CudaRayTracer(T.make_triangles(np.zeros((1, 9), np.float32), np.zeros(1, np.int32)))
+    lib = T.load_library()
+    lib.vrad_detmath.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                 ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
+    for fn, name in ((0, "Asin"), (1, "Pow")):
+        a, b, e = fixtures.detmath(name)
+        out = np.zeros(len(a), np.float32)
+        open_ = ctypes.c_int64()
+        rc = lib.vrad_detmath(tr._ctx, fn, a.ctypes.data, b.ctypes.data, out.ctypes.data, len(a), ctypes.byref(open_))
+        assert rc == 0
+        got = out.view(np.uint32)
+        bad = np.flatnonzero(got != e)
+        assert len(bad) == 0, (name, [(hex(a[i]), hex(b[i]), hex(got[i]), hex(e[i])) for i in bad[:6]])
+    tr.close()
+
+
+@pytest.mark.parametrize("threshold", [1.0, 0.1], ids=["stock-1.0", "config-0.1"])
+def test_3x3_bounce_bit_exact(oracle_mod, threshold):
+    w, inp, st = _stage(rg.config_3x3(seed=2), threshold=threshold)
+    with st:
+        lump, lightofs, _ = st.light_pass()
+        bs = st.bounce_stats()
+        total, direct = st.patch_light()
+        off, tr = st.transfers()
+        light = _sample_light(st)
+    ob = _oracle(oracle_mod, w, inp, threshold=threshold)
+    o_off, o_src, o_w, rays = ob.transfers()
+    assert bs.transfer_rays == rays
+    assert np.array_equal(off, o_off)
+    assert np.array_equal(tr["patch"], o_src)
+    assert np.array_equal(_bits(tr["weight"]), _bits(o_w))
+    o_total, o_direct, o_bounces, o_added = ob.run(light)
+    assert np.array_equal(_bits(direct), _bits(o_direct))
+    assert bs.bounces == o_bounces and bs.bounces > 1
+    assert np.array_equal(_bits(total), _bits(o_total))
+    want, want_ofs = ob.final(light)
+    assert np.array_equal(lightofs, want_ofs)
+    bad = np.flatnonzero(lump.view(np.uint32) != want.view(np.uint32))
+    assert len(bad) == 0, f"{len(bad)} of {len(lump) // 4} RGBE words differ"
+    # The bounce adds light.
+    assert (total > 0).any() and bs.transfers == len(tr) > 0
+
+
+def test_8x8_transfers_sampled_and_bounce_bit_exact(oracle_mod):
+    w, inp, st = _stage(rg.config_8x8(seed=1))
+    with st:
+        lump, lightofs, _ = st.light_pass()
+        bs = st.bounce_stats()
+        total, direct = st.patch_light()
+        off, tr = st.transfers()
+        light = _sample_light(st)
+    ob = _oracle(oracle_mod, w, inp)
+    patches, _ = ob.patches()
+    leaves = np.flatnonzero(patches["child1"] == -1)
+    rng = np.random.default_rng(7)
+    sub = np.sort(rng.choice(leaves, 400, replace=False))
+    o_off, o_src, o_w, _ = ob.transfers(sub)
+    for p in sub:
+        a, b = off[p], off[p + 1]
+        c, d = o_off[p], o_off[p + 1]
+        assert np.array_equal(tr["patch"][a:b], o_src[c:d]), p
+        assert np.array_equal(_bits(tr["weight"][a:b]), _bits(o_w[c:d])), p
+    # The bounce itself over the device's transfers.
+    ob.set_transfers(off, tr["patch"], tr["weight"])
+    o_total, o_direct, o_bounces, _ = ob.run(light)
+    assert np.array_equal(_bits(direct), _bits(o_direct))
+    assert bs.bounces == o_bounces
+    assert np.array_equal(_bits(total), _bits(o_total))
+    want, want_ofs = ob.final(light)
+    bad = np.flatnonzero(lump.view(np.uint32) != want.view(np.uint32))
+    assert len(bad) == 0, f"{len(bad)} of {len(lump) // 4} RGBE words differ"
+
+
+def test_bounce_pass_is_repeatable_and_device_entry_matches():
+    import torch
+    w, inp, st = _stage(rg.config_3x3(seed=2))
+    with st:
+        a, _, _ = st.light_pass()
+        b, _, _ = st.light_pass()
+        d = torch.zeros(len(a), dtype=torch.uint8, device="cuda")
+        st.light_pass_device(d)
+        torch.cuda.synchronize()
+    assert np.array_equal(a, b)
+    assert np.array_equal(d.cpu().numpy(), a)
