@@ -1,11 +1,16 @@
 """Benchmark: vrad's lighting stage on the seeded 8x8 room grid.
 
-One step = one light pass (vrad_light_pass): the fused direct gather over
-every light sample of the map -- for each of its 5.68 M samples, every
-light of its cluster's list in gather order: shadow segments to 64 point
-and spot lights, the sun's sky test and 162 sky-ambient directions, traced
-in-kernel -- then the final pass (luxel radial filter, RGBE encode, medians)
-into the 24.5 MB LIGHTING lump.
+One step = one light pass (vrad_light_pass), the whole stage from the
+uploaded world to the LIGHTING lump:
+  direct  the fused direct gather over every light sample of the map (for
+          each of its 5.68 M samples, every light of its cluster's list in
+          gather order: shadow segments to 64 point and spot lights, the
+          sun's sky test and 162 sky-ambient directions, traced in-kernel);
+  bounce  the patches' direct light, the transfer build (every candidate
+          patch pair's ray traced, form factors, scales) and the radiosity
+          bounces to the stop threshold (0.1, the configuration's);
+  final   the luxel radial filters of the direct and the bounced light,
+          RGBE encode, medians, into the LIGHTING lump.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
     python bench.py --workload seam     # the IRayTracer seam alone, rays in HBM
@@ -38,6 +43,8 @@ METRIC = "vrad lighting stage rays/s (8x8 room grid, 1 B200)"
 UNIT = "rays/s"
 BYTES_PER_RAY = 28.0 + 0.125        # 28-byte ray record in, one hit bit out
 CONFIG_SEED = 1
+BOUNCE_THRESHOLD = 0.1      # the configuration's stop threshold (the reference's own default is 1.0)
+MAX_BOUNCES = 100           # Radiosity.BounceAsync's default bounce limit
 
 
 def parse():
@@ -380,7 +387,7 @@ def oracle_faces_sample(world, inp, stride: int):
 
 
 def cpu_stage(world, inp, budget_s: float = 15.0):
-    """The reference's algorithm on the host: restated KD build + the
+    """The reference's direct gather on the host: restated KD build + the
     four-sample-group gather with the KD walk, all host threads, on a
     strided sample of faces sized to about budget_s."""
     from oracle import oracle as O
@@ -409,29 +416,82 @@ def world_and_inputs(side):
     return w, L.prepare(w)
 
 
+def oracle_bounce(world, inp, tree=None):
+    """The oracle's bounce over the world (patches built, nothing traced)."""
+    from hl2sdk_tools_sharp_b200 import lighting as L
+    from oracle import oracle as O
+    tree = tree if tree is not None else O.kd_build(world.tri_verts, world.tri_ids)
+    off, lst = L.pvs_lists(world)
+    return O.Bounce(tree, inp.faces, inp.verts, inp.samples, inp.face_first, L.face_reflectivity(world), off, lst,
+                    bounces=MAX_BOUNCES, threshold=BOUNCE_THRESHOLD)
+
+
+def cpu_transfers(ob, budget_s: float = 10.0):
+    """The transfer build restated (candidate walk, KD-traced rays, form
+    factors) on a strided sample of receivers: transfer rays per second."""
+    patches, _ = ob.patches()
+    leaves = np.flatnonzero(patches["child1"] == -1)
+
+    def run(stride, phase):
+        sub = leaves[phase::stride]
+        ob.forget_transfers()
+        t0 = time.perf_counter()
+        _, _, _, rays = ob.transfers(sub)
+        return rays, time.perf_counter() - t0, len(sub)
+    rays, dt, n = run(max(1, len(leaves) // 400), 1)
+    stride = max(1, int(len(leaves) / max(1.0, n * budget_s / max(dt, 1e-3))))
+    rays, dt, n = run(stride, 0)
+    return rays / dt, f"{n} of {len(leaves)} receivers (every {stride}th), {rays} transfer rays"
+
+
+WORKLOAD = ("8x8 room grid lighting stage: direct gather (64 point/spot lights, sun, 162-dir sky), "
+            "bounce (patch light, transfer build, radiosity to threshold 0.1), final pass")
+
+
 def run_reference_stage(args):
+    """The reference's algorithm on the host cores: the direct gather and
+    the transfer build restated (KD build, KD walk, four-sample groups,
+    candidate walk, form factors), all host threads, each on a bounded
+    sample of the 8x8 stage.  value = the stage's traced rays over the CPU
+    seconds those two parts take at the sampled rates; the bounce's
+    gathers and the final pass are left out of the CPU time (which only
+    flatters the CPU)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    from oracle import oracle as O
     w, inp = world_and_inputs(args.side)
+    tree = O.kd_build(w.tri_verts, w.tri_ids)
+    ob = oracle_bounce(w, inp, tree)
+    counts = None
     vals = []
     cb = None
     for i in range(args.warmup + args.steps):
-        cb = cpu_stage(w, inp, budget_s=max(3.0, 60.0 / max(1, args.warmup + args.steps)))
+        budget = max(2.0, 40.0 / max(1, args.warmup + args.steps))
+        cb = cpu_stage(w, inp, budget_s=budget)
+        t_rate, t_sample = cpu_transfers(ob, budget_s=budget)
+        if counts is None:
+            # Ray counts of one full step: the direct gather's from the
+            # sampled rate's own sample scaled to every sample; the transfer
+            # build's from the candidate walk (no tracing needed to count).
+            direct_rays = cb["value"] * len(inp.samples) / cb["samples_per_s"]
+            counts = (direct_rays, ob.count_candidates())
+        direct_rays, transfer_rays = counts
+        cpu_s = direct_rays / cb["value"] + transfer_rays / t_rate
         if i >= args.warmup:
-            vals.append(cb["value"])
+            vals.append((direct_rays + transfer_rays) / cpu_s)
     value = statistics.median(vals)
-    # A whole step extrapolated from the sample: every sample of the map at
-    # the sampled samples/s.
-    ms_full = 1000.0 * len(inp.samples) / cb["samples_per_s"]
+    direct_rays, transfer_rays = counts
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_full,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * (direct_rays + transfer_rays) / value,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded room grid)",
-        "config": {"workload": "8x8 room grid direct-lighting stage (64 point/spot lights, sun, 162-dir sky)",
-                   "side": args.side, "seed": CONFIG_SEED, "samples": int(len(inp.samples))},
-        "cpu_baseline": {**cb, "value": value},
+        "config": {"workload": WORKLOAD, "side": args.side, "seed": CONFIG_SEED, "samples": int(len(inp.samples)),
+                   "bounce_threshold": BOUNCE_THRESHOLD},
+        "cpu_baseline": {**cb, "value": value,
+                         "sample": cb["sample"] + f"; transfer build: {t_sample}; bounce gathers and final pass not timed"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -447,40 +507,73 @@ def main_stage(args):
 
     w, inp = world_and_inputs(args.side)
     n = len(inp.samples)
+    refl = L.face_reflectivity(w)
+    pvs_off, pvs_list = L.pvs_lists(w)
     stage = L.LightingStage(w, inp, device=local)
+    stage.upload_bounce(refl, pvs_off, pvs_list, bounces=MAX_BOUNCES, threshold=BOUNCE_THRESHOLD)
     info = stage.tracer.scene_info()
     d_out = torch.empty(n * 4, dtype=torch.float32, device=device)
     block, tune_ms = stage.autotune()                # picks the launch shape (untimed)
-    lump_host, lightofs, pstats = stage.light_pass()   # counts the segments of one step
-    rays_per_step = int(pstats.visibility_rays + pstats.sky_rays)
+    lump_host, lightofs, pstats = stage.light_pass()   # counts the rays of one step
+    bst = stage.bounce_stats()
+    rays_per_step = int(pstats.visibility_rays + pstats.sky_rays + bst.transfer_rays)
     luxels = int(pstats.luxels)
     d_lump = torch.empty(len(lump_host), dtype=torch.uint8, device=device)
     for _ in range(max(3, args.warmup)):
         stage.light_pass_device(d_lump)
-    stage.direct_device(d_out)
     torch.cuda.synchronize()
 
     check = None
+    ob = None
+    cpu_parts = {}
     if rank == 0 and not args.no_cpu:
+        # Parity on this run's own output: a strided sample of faces through
+        # the oracle's direct gather, a sample of receivers through its
+        # transfer build, and the whole lump through its bounce and final
+        # pass fed the device's sample light and transfers (each checked
+        # here or by the sampled comparisons).
         from oracle import oracle as O
         tree = O.kd_build(w.tri_verts, w.tri_ids)
         sel, samples, first, index = oracle_faces_sample(w, inp, 97)
         want = O.direct(tree, inp.faces[sel], samples, first, inp.lights, inp.cluster_offsets,
                         inp.cluster_lights, inp.sky_directions, inp.sun_jitter, inp.sun_samples,
                         inp.sun_angular_extent)
+        stage.direct_device(d_out)
+        torch.cuda.synchronize()
         got_all = d_out.view(n, 4).cpu().numpy()
-        got = got_all[index]
-        lump_want, _ = O.final(inp.faces, inp.verts, inp.samples, inp.face_first, got_all)
+        t_off, t_rec = stage.transfers()
+        ob = oracle_bounce(w, inp, tree)
+        patches, _ = ob.patches()
+        leaves = np.flatnonzero(patches["child1"] == -1)
+        sub = leaves[::max(1, len(leaves) // 200)]
+        o_off, o_src, o_w, _ = ob.transfers(sub)
+        tr_bad = 0
+        for p in sub:
+            a, b = t_off[p], t_off[p + 1]
+            c, d = o_off[p], o_off[p + 1]
+            tr_bad += int(not (np.array_equal(t_rec["patch"][a:b], o_src[c:d])
+                               and np.array_equal(t_rec["weight"][a:b].view(np.uint32), o_w[c:d].view(np.uint32))))
+        ob.set_transfers(t_off, t_rec["patch"], t_rec["weight"])
+        t = time.perf_counter()
+        _, _, o_bounces, _ = ob.run(got_all)
+        cpu_parts["bounce_s"] = time.perf_counter() - t
+        t = time.perf_counter()
+        lump_want, _ = ob.final(got_all)
+        cpu_parts["final_s"] = time.perf_counter() - t
         lump_got = d_lump.cpu().numpy()
         check = {"samples": int(len(index)),
-                 "mismatches": int((got.view(np.uint32) != want.view(np.uint32)).any(1).sum()),
+                 "mismatches": int((got_all[index].view(np.uint32) != want.view(np.uint32)).any(1).sum()),
+                 "receivers": int(len(sub)), "receiver_mismatches": tr_bad,
+                 "bounces": int(bst.bounces), "oracle_bounces": int(o_bounces),
                  "lump_words": int(len(lump_want) // 4),
                  "lump_mismatches": int((lump_got.view(np.uint32) != lump_want.view(np.uint32)).sum())}
+        del t_rec
 
     stream = torch.cuda.current_stream(device)
     barrier(world_size)
     torch.cuda.synchronize()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps)]
+    phases = []
     with ClockSampler(local) as clocks:
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
@@ -489,6 +582,8 @@ def main_stage(args):
             ev[2 * s_].record(stream)
             stage.light_pass_device(d_lump)
             ev[2 * s_ + 1].record(stream)
+            b = stage.bounce_stats()
+            phases.append((b.patch_light_ms, b.transfer_ms, b.bounce_ms, b.bounces))
         t1.record(stream)
         torch.cuda.synchronize()
     barrier(world_size)
@@ -496,9 +591,11 @@ def main_stage(args):
     per_step = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps)]
     ms_per_step = elapsed_ms / args.steps
     value = world_size * rays_per_step / (ms_per_step / 1000.0)
+    bst = stage.bounce_stats()
 
-    # End to end through the host-buffer C ABI: the samples (from pinned
-    # memory) uploaded with the world, the gather, the values read back.
+    # End to end through the host-buffer C ABI: the world (samples from
+    # pinned memory) and the bounce uploaded, the light pass, the lump read
+    # back into pinned memory.
     e2e = None
     if not args.no_e2e:
         pinned = torch.empty(inp.samples.nbytes, dtype=torch.uint8, pin_memory=True)
@@ -509,6 +606,7 @@ def main_stage(args):
 
         def e2e_step():
             stage.upload_world(inp_pinned)
+            stage.upload_bounce(refl, pvs_off, pvs_list, bounces=MAX_BOUNCES, threshold=BOUNCE_THRESHOLD)
             stage.light_pass(outv)
         e2e_step()
         barrier(world_size)
@@ -519,26 +617,26 @@ def main_stage(args):
         e2e_s = max_over_ranks((time.perf_counter() - t) / e2e_steps, world_size)
         e2e = {"value": world_size * rays_per_step / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(inp.samples.nbytes + inp.faces.nbytes + inp.lights.nbytes
-                                         + inp.verts.nbytes),
+                                         + inp.verts.nbytes + refl.nbytes + pvs_off.nbytes + pvs_list.nbytes),
                "d2h_bytes_per_step": int(len(lump_host)), "stage_s": e2e_s,
-               "note": "includes the host-side world upload (slot layout, final-pass tables)"}
+               "note": "includes the host-side set-up of the world and the bounce (slot layout, final-pass "
+                       "tables, the patch tree) and the device tables' uploads"}
         if not np.array_equal(outv, lump_host):
             e2e["mismatch_vs_device"] = True
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu:
-        cpu = cpu_stage(w, inp, budget_s=15.0)
-        # The final pass on the host over the whole map (fed the sample light
-        # the device computed; its cost does not depend on the values).
-        from oracle import oracle as O
-        t = time.perf_counter()
-        O.final(inp.faces, inp.verts, inp.samples, inp.face_first, d_out.view(n, 4).cpu().numpy())
-        cpu_final_s = time.perf_counter() - t
+        cpu = cpu_stage(w, inp, budget_s=12.0)
+        t_rate, t_sample = cpu_transfers(ob, budget_s=12.0)
         cpu_direct_s = n / cpu["samples_per_s"]
-        cpu["stage_s"] = cpu_direct_s + cpu_final_s
-        cpu["final_s"] = cpu_final_s
+        cpu_transfer_s = bst.transfer_rays / t_rate
+        cpu["stage_s"] = cpu_direct_s + cpu_transfer_s + cpu_parts["bounce_s"] + cpu_parts["final_s"]
+        cpu["parts_s"] = {"direct": cpu_direct_s, "transfers": cpu_transfer_s, "bounce": cpu_parts["bounce_s"],
+                          "final": cpu_parts["final_s"]}
         cpu["value"] = rays_per_step / cpu["stage_s"]
-        cpu["sample"] += f"; final pass timed on the whole map ({cpu_final_s:.2f} s, one thread)"
+        cpu["sample"] += (f"; transfer build: {t_sample} ({t_rate:.3g} rays/s); bounce (patch light + "
+                          f"{bst.bounces} bounces over the device's transfers) and final pass timed whole "
+                          f"({cpu_parts['bounce_s']:.2f} s, {cpu_parts['final_s']:.2f} s)")
 
     peaks = {}
     try:
@@ -546,7 +644,8 @@ def main_stage(args):
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    # The dominant kernel (k_direct) timed alone on the launching stream.
+    # The dominant phases timed alone on the launching stream: the direct
+    # gather kernel, and the transfer build (its phase events).
     a_ev = torch.cuda.Event(enable_timing=True)
     b_ev = torch.cuda.Event(enable_timing=True)
     a_ev.record(stream)
@@ -554,32 +653,50 @@ def main_stage(args):
         stage.direct_device(d_out)
     b_ev.record(stream)
     torch.cuda.synchronize()
-    kernel_ms = a_ev.elapsed_time(b_ev) / 3.0
-    alg_bytes = 28.0 * rays_per_step + 32.0 * n
+    direct_ms = a_ev.elapsed_time(b_ev) / 3.0
+    transfer_ms = statistics.median([p[1] for p in phases])
+    direct_rays = int(pstats.visibility_rays + pstats.sky_rays)
+    if direct_ms >= transfer_ms:
+        alg_bytes = 28.0 * direct_rays + 32.0 * n
+        kernel, kernel_ms = "k_direct (fused gather + traversal)", direct_ms
+        alg_note = "28 B per traced segment + 16 B sample in + 16 B value out"
+    else:
+        alg_bytes = 28.0 * bst.transfer_rays + 8.0 * bst.transfers
+        kernel, kernel_ms = "transfer build (k_candidates + k_transfer + compaction)", transfer_ms
+        alg_note = "28 B per candidate ray + 8 B per transfer written"
     achieved = alg_bytes / (kernel_ms / 1000.0) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": "k_direct (fused gather + traversal)", "kernel_ms": kernel_ms,
-                "algorithmic_bytes": "28 B per traced segment + 16 B sample in + 16 B value out",
-                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+                "traffic": None, "kernel": kernel, "kernel_ms": kernel_ms, "algorithmic_bytes": alg_note,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "direct_ms": direct_ms, "transfer_build_ms": transfer_ms}
+    nb = int(statistics.median([p[3] for p in phases]))
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded room grid)",
-            "config": {"workload": "8x8 room grid lighting stage, bounce 0 (64 point/spot lights, sun, 162-dir sky; direct gather + final pass)",
+            "config": {"workload": WORKLOAD,
                        "side": args.side, "seed": CONFIG_SEED, "samples": n, "faces": int(len(inp.faces)),
                        "triangles": info.triangles, "lights": int(len(inp.lights)),
                        "rays_per_step": rays_per_step,
                        "visibility_rays": int(pstats.visibility_rays), "sky_rays": int(pstats.sky_rays),
-                       "luxels": luxels, "lighting_bytes": int(len(lump_host)), "bounce": 0,
-                       "l2": "no L2 flush: the 0.3 GB sample set exceeds L2; the 0.5 MB scene stays on chip",
+                       "transfer_rays": int(bst.transfer_rays), "transfers": int(bst.transfers),
+                       "patches": int(bst.patches), "receivers": int(bst.receivers),
+                       "luxels": luxels, "lighting_bytes": int(len(lump_host)),
+                       "bounce_threshold": BOUNCE_THRESHOLD, "bounces": nb,
+                       "l2": "no L2 flush: the 0.3 GB sample set and 5 GB of candidate pairs exceed L2",
                        "parallelism": f"replicas{world_size}"},
             "samples_per_s": world_size * n / (ms_per_step / 1000.0),
             "luxels_per_s": world_size * luxels / (ms_per_step / 1000.0),
             "stage_s": ms_per_step / 1000.0,
+            "phase_ms": {"direct": direct_ms, "patch_light": statistics.median([p[0] for p in phases]),
+                         "transfers": transfer_ms, "bounces": statistics.median([p[2] for p in phases])},
+            "bounce_iterations": nb,
             "e2e": e2e,
-            "gpu_launches": 4 * args.steps,
+            # direct 1, patch light 2, transfer build 5 + 2 scans (2 each),
+            # 3 per bounce, final 4 (exact totals add one each when needed).
+            "gpu_launches": (1 + 2 + 9 + 3 * nb + 4) * args.steps,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),

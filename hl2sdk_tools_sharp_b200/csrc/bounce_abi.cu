@@ -1,6 +1,6 @@
 // bounce_abi.cu -- host side of the bounce: vrad_bounce_upload (the patch
 // tree, receiver order, PVS rows and the final pass's patch tables, and
-// the buffers sized by a first transfer build), the bounce loop of a light
+// the buffers sized by a candidate count), the bounce loop of a light
 // pass with the reference's stop rule, and the inspection entry points.
 
 #include <cuda_runtime.h>
@@ -155,8 +155,12 @@ cudaError_t run_bounce(vrad_ctx *ctx, cudaStream_t s, std::string &why) {
     }
     if (e == cudaSuccess) e = cudaEventRecord(ev[3], s);
     unsigned long long counts[3] = {0, 0, 0};
+    int64_t ntr = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(counts, b.counters, sizeof counts, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && b.nreceivers)
+        e = cudaMemcpyAsync(&ntr, b.tr_off + b.nreceivers, sizeof ntr, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) b.ntransfers = ntr;
     if (e == cudaSuccess) {
         cudaEventElapsedTime(&b.patch_light_ms, ev[0], ev[1]);
         cudaEventElapsedTime(&b.transfer_ms, ev[1], ev[2]);
@@ -349,14 +353,12 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     b.ncand = ncand;
     if (e == cudaSuccess) e = cudaMalloc(&b.cand_src, sizeof(int32_t) * (size_t)(ncand ? ncand : 1));
     if (e == cudaSuccess) e = cudaMalloc(&b.cand_w, sizeof(float) * (size_t)(ncand ? ncand : 1));
-    if (e == cudaSuccess) e = cudaMemsetAsync(b.counters, 0, 3 * sizeof(unsigned long long), s);
-    if (e == cudaSuccess) e = launch_transfers(b, ctx->scene.view(), ctx->status, s, false);
-    int64_t ntr = 0;
-    if (e == cudaSuccess && R > 0) e = cudaMemcpyAsync(&ntr, b.tr_off + R, sizeof ntr, cudaMemcpyDeviceToHost, s);
+    // Transfers are at most the candidates: the list array takes that
+    // bound, so sizing needs no trace.
     uint32_t overflow = 0;
+    if (e == cudaSuccess) e = cudaMalloc(&b.tr, sizeof(int2) * (size_t)(ncand ? ncand : 1));
     if (e == cudaSuccess) e = cudaMemcpyAsync(&overflow, ctx->status, sizeof overflow, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e == cudaSuccess) e = cudaMalloc(&b.tr, sizeof(int2) * (size_t)(ntr ? ntr : 1));
     if (e != cudaSuccess) {
         b.release();
         return vrad_cuda_fail(ctx, e, "transfer sizing");
@@ -364,8 +366,9 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     if (overflow) {
         cudaMemset(ctx->status, 0, sizeof(uint32_t));
         b.release();
-        return vrad_fail(ctx, VRAD_ERR_CUDA, "stack overflow in the transfer build (flags %u)", overflow);
+        return vrad_fail(ctx, VRAD_ERR_CUDA, "stack overflow in the candidate walk (flags %u)", overflow);
     }
+    const int64_t ntr = 0;
     b.ntransfers = ntr;
     b.ready = true;
     return VRAD_OK;
@@ -389,6 +392,7 @@ extern "C" int32_t vrad_bounce_stats_get(vrad_ctx *ctx, vrad_bounce_stats *st) {
     st->transfer_ms = b.transfer_ms;
     st->bounce_ms = b.bounce_ms;
     st->final_ms = b.final_ms;
+    st->unsettled_asin = (int64_t)b.open_ties;
     return VRAD_OK;
 }
 

@@ -15,10 +15,13 @@
 // by the root.  Single precision in the reference's operation order
 // (-ffp-contract=off), so origins, normals and areas are its bits.
 
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/vrad_cuda.h"
@@ -36,12 +39,13 @@ constexpr float kOnEpsilon = 0.1f;          // LightConstants.OnEpsilon
 constexpr float kMaxReflectivity = 0.99f;   // PatchBuilder.MaxReflectivity
 constexpr float kSmoothing = 0.7071067f;    // LightConstants.DefaultSmoothingThreshold
 
+// One root's subtree under construction: local indices, the root at 0.
 struct Builder {
     const vrad_face *faces;
     const float *vertices;
     float min_chop;
-    std::vector<std::vector<float>> corners;  // per face, xyz per winding vertex
-    std::vector<V3> centroid;                 // PatchSet.Centroids
+    const std::vector<std::vector<float>> *corner_normals;  // per face, xyz per winding vertex
+    const std::vector<V3> *centroids;                       // PatchSet.Centroids
     std::vector<vrad_patch> patches;
     std::vector<Winding> windings;
 
@@ -56,8 +60,8 @@ struct Builder {
     V3 phong(int32_t f, V3 spot) const {
         const vrad_face &fc = faces[f];
         const V3 fn = {fc.normal[0], fc.normal[1], fc.normal[2]};
-        const std::vector<float> &cn = corners[(size_t)f];
-        const V3 c = centroid[(size_t)f];
+        const std::vector<float> &cn = (*corner_normals)[(size_t)f];
+        const V3 c = (*centroids)[(size_t)f];
         const int n = fc.num_vertices;
         for (int j = 0; j < n; j++) {
             const int j2 = (j + 1) % n;
@@ -177,17 +181,15 @@ bool prevent_subdivision(int32_t flags) {
 
 bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
                       const float *reflectivity, float max_chop, float min_chop, PatchTree &out, std::string &why) {
-    Builder b;
-    b.faces = faces;
-    b.vertices = vertices;
-    b.min_chop = min_chop;
-    if (!corner_normals(faces, nfaces, vertices, nvertices, kSmoothing, b.corners)) {
+    std::vector<std::vector<float>> corners;
+    if (!corner_normals(faces, nfaces, vertices, nvertices, kSmoothing, corners)) {
         why = "a face's winding lies outside the vertex array";
         return false;
     }
-    b.centroid.assign((size_t)nfaces, V3{0.0f, 0.0f, 0.0f});
+    std::vector<V3> centroid((size_t)nfaces, V3{0.0f, 0.0f, 0.0f});
     out.face_root.assign((size_t)nfaces, -1);
-    // MakePatchForFace, face by face.
+    // MakePatchForFace, face by face: the roots, in face order.
+    std::vector<Builder> subtree;
     for (int32_t f = 0; f < nfaces; f++) {
         const vrad_face &fc = faces[f];
         if (fc.num_vertices < 3) {
@@ -195,7 +197,10 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
             return false;
         }
         Winding w;
-        for (int32_t k = 0; k < fc.num_vertices; k++) w.push_back(add(b.vertex(f, k), V3{0.0f, 0.0f, 0.0f}));
+        for (int32_t k = 0; k < fc.num_vertices; k++) {
+            const float *v = vertices + 3 * (int64_t)(fc.first_vertex + k);
+            w.push_back(add(V3{v[0], v[1], v[2]}, V3{0.0f, 0.0f, 0.0f}));
+        }
         w = remove_colinear(w);
         const float ar = area(w);
         if (ar <= 0.0f) continue;  // a degenerate face gets no patch
@@ -212,7 +217,7 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
         p.cluster = fc.cluster;
         p.sky = (fc.flags & VRAD_SURF_SKY) ? 1 : 0;
         const V3 c = center(w);
-        b.centroid[(size_t)f] = c;
+        centroid[(size_t)f] = c;
         p.origin[0] = c.x, p.origin[1] = c.y, p.origin[2] = c.z;
         for (int a = 0; a < 3; a++) p.normal[a] = fc.normal[a];
         V3 mn, mx;
@@ -227,34 +232,75 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
             const float r = reflectivity[3 * (int64_t)f + a];
             p.reflectivity[a] = r < kMaxReflectivity ? r : kMaxReflectivity;
         }
-        out.face_root[(size_t)f] = b.add_patch(p, w);
+        out.face_root[(size_t)f] = (int32_t)subtree.size();
+        Builder b;
+        b.faces = faces;
+        b.vertices = vertices;
+        b.min_chop = min_chop;
+        b.corner_normals = &corners;
+        b.centroids = &centroid;
+        b.add_patch(p, w);
+        subtree.push_back(std::move(b));
     }
-    const int32_t roots = (int32_t)b.patches.size();
-    // PatchSubdivider.Subdivide with bounces > 0, not -fast: every root in
-    // index order (one per face, in face order).
+    const int32_t roots = (int32_t)subtree.size();
+    // PatchSubdivider.Subdivide with bounces > 0, not -fast.  Each root's
+    // subtree depends on nothing outside its face, so the roots are split
+    // on worker threads, each into its own arrays.
+    {
+        std::atomic<int32_t> next{0};
+        auto work = [&]() {
+            for (int32_t i; (i = next.fetch_add(1)) < roots;) {
+                Builder &b = subtree[(size_t)i];
+                if (!prevent_subdivision(faces[b.patches[0].face].flags)) b.subdivide(0);
+            }
+        };
+        const unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (unsigned t = 1; t < nt; t++) pool.emplace_back(work);
+        work();
+        for (auto &t : pool) t.join();
+    }
+    // Global indices: the roots 0..roots-1 in face order, then each root's
+    // descendants in creation order (the order SubdividePatch adds them).
+    std::vector<int32_t> base((size_t)roots);
+    int32_t total = roots;
+    for (int32_t i = 0; i < roots; i++) {
+        base[(size_t)i] = total;
+        total += (int32_t)subtree[(size_t)i].patches.size() - 1;
+    }
+    out.patches.resize((size_t)total);
+    std::vector<const Winding *> wind((size_t)total);
     out.face_first.assign((size_t)nfaces, 0);
     out.face_end.assign((size_t)nfaces, 0);
     for (int32_t i = 0; i < roots; i++) {
-        const int32_t f = b.patches[(size_t)i].face;
-        out.face_first[(size_t)f] = (int32_t)b.patches.size();
-        if (!prevent_subdivision(faces[f].flags)) b.subdivide(i);
-        out.face_end[(size_t)f] = (int32_t)b.patches.size();
+        Builder &b = subtree[(size_t)i];
+        auto global = [&](int32_t local) { return local < 0 ? -1 : (local == 0 ? i : base[(size_t)i] + local - 1); };
+        for (size_t k = 0; k < b.patches.size(); k++) {
+            vrad_patch p = b.patches[k];
+            p.parent = global(p.parent);
+            p.child1 = global(p.child1);
+            p.child2 = global(p.child2);
+            const int32_t g = global((int32_t)k);
+            out.patches[(size_t)g] = p;
+            wind[(size_t)g] = &b.windings[k];
+        }
+        const int32_t f = b.patches[0].face;
+        out.face_first[(size_t)f] = base[(size_t)i];
+        out.face_end[(size_t)f] = base[(size_t)i] + (int32_t)b.patches.size() - 1;
+        out.face_root[(size_t)f] = i;
     }
-    for (int32_t f = 0; f < nfaces; f++)
-        if (out.face_root[(size_t)f] < 0) out.face_first[(size_t)f] = out.face_end[(size_t)f] = 0;
     // Windings into one point array.
     out.points.clear();
-    for (size_t i = 0; i < b.patches.size(); i++) {
-        vrad_patch &p = b.patches[i];
+    for (size_t i = 0; i < out.patches.size(); i++) {
+        vrad_patch &p = out.patches[i];
         p.first_point = (int32_t)(out.points.size() / 3);
-        p.num_points = (int32_t)b.windings[i].size();
-        for (const V3 &v : b.windings[i]) {
+        p.num_points = (int32_t)wind[i]->size();
+        for (const V3 &v : *wind[i]) {
             out.points.push_back(v.x);
             out.points.push_back(v.y);
             out.points.push_back(v.z);
         }
     }
-    out.patches = std::move(b.patches);
     out.roots = roots;
     return true;
 }

@@ -410,6 +410,7 @@ typedef struct vrad_bounce_stats {
     float transfer_ms;
     float bounce_ms;
     float final_ms;
+    int64_t unsettled_asin;   /* form-factor arcsines left at the plain rounding (expected 0) */
 } vrad_bounce_stats;
 
 /* The statistics of the last light pass's bounce. */

@@ -890,4 +890,41 @@ int64_t orc_bounce_stats(void *h, int64_t *blocked) {
 
 float orc_asin(float x) { return AsinCR(x); }
 
+// Drops every built transfer list, so the next build traces again.
+void orc_bounce_forget_transfers(void *h) {
+    World &w = *static_cast<World *>(h);
+    w.transfers.assign(w.patches.size(), {});
+    w.computed.assign(w.patches.size(), 0);
+    w.have_transfers = false;
+}
+
+// The candidate pairs of every receiver (the transfer rays one full build
+// traces), counted by the enumerator alone.
+int64_t orc_bounce_count_candidates(void *h) {
+    World &w = *static_cast<World *>(h);
+    std::vector<int> recv = ReceiverOrder(w);
+    std::atomic<size_t> next{0};
+    std::atomic<int64_t> total{0};
+    auto work = [&]() {
+        int last = -1;
+        std::vector<int> row;
+        int64_t n = 0;
+        for (;;) {
+            size_t k = next.fetch_add(1);
+            if (k >= recv.size()) break;
+            int c = w.patches[(size_t)recv[k]].cluster;
+            if (c != last) {
+                row = FacesInRow(w, c);
+                last = c;
+            }
+            n += (int64_t)Candidates(w, recv[k], row).size();
+        }
+        total += n;
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < std::max(1, w.threads); t++) pool.emplace_back(work);
+    for (auto &t : pool) t.join();
+    return total;
+}
+
 }  // extern "C"

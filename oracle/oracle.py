@@ -304,6 +304,10 @@ def _bounce_lib():
         L.orc_bounce_final.argtypes = [P, P, P, i64, P, P]
         L.orc_bounce_stats.argtypes = [P, P]
         L.orc_bounce_stats.restype = i64
+        L.orc_bounce_forget_transfers.argtypes = [P]
+        L.orc_bounce_forget_transfers.restype = None
+        L.orc_bounce_count_candidates.argtypes = [P]
+        L.orc_bounce_count_candidates.restype = i64
         L.orc_asin.argtypes = [f32]
         L.orc_asin.restype = f32
         L._bounce_typed = True
@@ -375,6 +379,14 @@ class Bounce:
         if rc != 0:
             raise RuntimeError(f"orc_bounce_transfers failed: {rc}")
         return off, src[:count.value], w[:count.value], rays.value
+
+    def forget_transfers(self) -> None:
+        """Drop the built lists: the next transfers() call traces again."""
+        _bounce_lib().orc_bounce_forget_transfers(self._h)
+
+    def count_candidates(self) -> int:
+        """Every receiver's candidate pairs (one full build's transfer rays)."""
+        return int(_bounce_lib().orc_bounce_count_candidates(self._h))
 
     def set_transfers(self, offsets, src, weight):
         self._tr = (np.ascontiguousarray(offsets, np.int64), np.ascontiguousarray(src, np.int32),

@@ -235,6 +235,10 @@ int orc_bounce_final(void *h, const float *sample_light, uint8_t *lighting, int6
                      int64_t *total);
 /* Rays traced so far; *blocked of them blocked. */
 int64_t orc_bounce_stats(void *h, int64_t *blocked);
+/* Drops the built transfer lists (the next build traces again). */
+void orc_bounce_forget_transfers(void *h);
+/* Every receiver's candidate pairs, counted without tracing. */
+int64_t orc_bounce_count_candidates(void *h);
 /* DetMathF.Asin as the oracle computes it. */
 float orc_asin(float x);
 
