@@ -40,7 +40,7 @@
 //   k_collect         one thread per face: CollectLight's parents, bottom up
 //   k_totals          fp64 sums of the light a bounce added, with absolute
 //                     sums that bound the reference's float sum
-//   k_exact_total     one thread: the reference's sequential float sum, run
+//   k_exact_total     one block: the reference's sequential float sum, run
 //                     only when the bound cannot settle the stop rule
 
 #include <cuda_runtime.h>
@@ -268,14 +268,24 @@ __global__ void __launch_bounds__(BLOCK) k_transfer(BounceView v, DeviceScene sc
     const bool live = q < ncand;
     float w = 0.0f;
     bool blocked = false;
-    if (live) {
-        // The receiver whose run holds q.
+    // The receiver whose run holds q: one binary search per warp, for its
+    // first candidate, then each lane steps forward (a warp's 32
+    // candidates seldom span more than one or two receivers).
+    const int64_t q0 = (int64_t)blockIdx.x * BLOCK + (threadIdx.x & ~31);
+    int r0 = 0;
+    if ((threadIdx.x & 31) == 0 && q0 < ncand) {
         int lo = 0, hi = v.nreceivers;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (__ldg(&cand_off[mid]) <= q) lo = mid;
+            if (__ldg(&cand_off[mid]) <= q0) lo = mid;
             else hi = mid;
         }
+        r0 = lo;
+    }
+    r0 = __shfl_sync(kFull, r0, 0);
+    if (live) {
+        int lo = r0;
+        while (__ldg(&cand_off[lo + 1]) <= q) lo++;
         const int p = __ldg(&v.recv[lo]);
         const int s = __ldg(&cand_src[q]);
         const float4 po = __ldg(&v.origin[p]), pn = __ldg(&v.normal[p]);
@@ -468,21 +478,49 @@ __global__ void k_totals(BounceView v, const float4 *__restrict__ emit, double *
 }
 
 // CollectLight's own total: the leaves' emission summed in float, in
-// descending index order.
-__global__ void k_exact_total(BounceView v, const float4 *__restrict__ emit, float *__restrict__ out) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+// descending index order (leaf_desc lists the sky-free leaves that way).
+// The sum is one chain of dependent adds; one block keeps it fed: all of
+// its threads stage the next tile of values in shared memory while warp 0
+// adds up the current one, every lane of it the same chain.
+constexpr int kExactThreads = 1024;
+constexpr int kExactTile = 2048;  // two tiles of float3: 48 KB of shared memory
+
+__global__ void __launch_bounds__(kExactThreads) k_exact_total(const int32_t *__restrict__ leaf_desc, int32_t n,
+                                                               const float4 *__restrict__ emit, float *__restrict__ out) {
+    __shared__ float3 tile[2][kExactTile];
     float x = 0.0f, y = 0.0f, z = 0.0f;
-    for (int p = v.npatches - 1; p >= 0; p--) {
-        const int4 tr = __ldg(&v.tree[p]);
-        if (tr.y != -1 || tr.w) continue;
-        const float4 e = emit[p];
-        x = __fadd_rn(x, e.x);
-        y = __fadd_rn(y, e.y);
-        z = __fadd_rn(z, e.z);
+    auto stage = [&](int buf, int base) {
+        for (int k = threadIdx.x; k < kExactTile; k += kExactThreads) {
+            const int i = base + k;
+            float3 v = make_float3(0.0f, 0.0f, 0.0f);
+            if (i < n) {
+                const float4 e = __ldg(&emit[__ldg(&leaf_desc[i])]);
+                v = make_float3(e.x, e.y, e.z);
+            }
+            tile[buf][k] = v;
+        }
+    };
+    stage(0, 0);
+    __syncthreads();
+    for (int base = 0, buf = 0; base < n; base += kExactTile, buf ^= 1) {
+        if (threadIdx.x >= 32) {
+            stage(buf ^ 1, base + kExactTile);
+        } else {
+            const int m = min(kExactTile, n - base);
+            for (int k = 0; k < m; k++) {
+                const float3 v = tile[buf][k];
+                x = __fadd_rn(x, v.x);
+                y = __fadd_rn(y, v.y);
+                z = __fadd_rn(z, v.z);
+            }
+        }
+        __syncthreads();
     }
-    out[0] = x;
-    out[1] = y;
-    out[2] = z;
+    if (threadIdx.x == 0) {
+        out[0] = x;
+        out[1] = y;
+        out[2] = z;
+    }
 }
 
 unsigned blocks(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
@@ -492,7 +530,7 @@ unsigned blocks(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
 void BounceBuffers::release() {
     void *ptrs[] = {origin, normal, mins, maxs, refl, tree, wind, points, face_range, face_samples, face_plane,
                     recv, row_off, row_faces, sample_area, cand_off, cand_src, cand_w, tr_off, tr, scan_tmp,
-                    acc, direct, total, emit[0], emit[1], shoot[0], shoot[1], sums, exact, counters,
+                    acc, direct, total, emit[0], emit[1], shoot[0], shoot[1], sums, exact, counters, leaf_desc,
                     pr_off, pr_patch, pr_box, pr_coord, prad_light, prad_weight};
     for (void *q : ptrs) cudaFree(q);
     cudaFreeHost(h_sums);
@@ -558,7 +596,7 @@ cudaError_t launch_gather(BounceBuffers &b, int bounce, cudaStream_t stream) {
 }
 
 cudaError_t launch_exact_total(BounceBuffers &b, int bounce, cudaStream_t stream) {
-    k_exact_total<<<1, 32, 0, stream>>>(b.view, b.emit[(bounce & 1) ^ 1], b.exact);
+    k_exact_total<<<1, kExactThreads, 0, stream>>>(b.leaf_desc, b.nleaves, b.emit[(bounce & 1) ^ 1], b.exact);
     return cudaGetLastError();
 }
 

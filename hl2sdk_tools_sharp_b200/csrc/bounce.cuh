@@ -83,6 +83,7 @@ struct BounceBuffers {
     float4 *emit[2] = {nullptr, nullptr}, *shoot[2] = {nullptr, nullptr};
     double *sums = nullptr;        // fp64 totals of a bounce: 3 sums, 3 absolute sums
     float *exact = nullptr;        // the sequential float total, when needed
+    int32_t *leaf_desc = nullptr;  // the sky-free leaves, descending index (CollectLight's total order)
     unsigned long long *counters = nullptr;  // [0] transfer rays, [1] blocked, [2] asin ties left open
     double *h_sums = nullptr;      // pinned host copies
     float *h_exact = nullptr;

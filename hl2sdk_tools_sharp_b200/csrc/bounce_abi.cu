@@ -265,6 +265,9 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
         if (tree.patches[(size_t)i].child1 == -1) by_cluster[(size_t)tree.patches[(size_t)i].cluster].push_back(i);
     std::vector<int32_t> recv;
     for (const auto &v : by_cluster) recv.insert(recv.end(), v.begin(), v.end());
+    std::vector<int32_t> leaf_desc;
+    for (int32_t i = P - 1; i >= 0; i--)
+        if (tree.patches[(size_t)i].child1 == -1 && !tree.patches[(size_t)i].sky) leaf_desc.push_back(i);
     // FacesInRow: each visible cluster's faces, in face order (one leaf per
     // cluster, whose faces are the faces that lie in it).
     std::vector<std::vector<int32_t>> cluster_faces((size_t)C);
@@ -305,6 +308,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     if (e == cudaSuccess) e = upload(&b.face_samples, face_samples);
     if (e == cudaSuccess) e = upload(&b.face_plane, face_plane);
     if (e == cudaSuccess) e = upload(&b.recv, recv);
+    if (e == cudaSuccess) e = upload(&b.leaf_desc, leaf_desc);
     if (e == cudaSuccess) e = upload(&b.row_off, row_off);
     if (e == cudaSuccess) e = upload(&b.row_faces, row_faces);
     if (e == cudaSuccess) e = upload(&b.sample_area, sample_area);
