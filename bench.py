@@ -399,7 +399,7 @@ def cpu_stage(world, inp, budget_s: float = 15.0):
         t0 = time.perf_counter()
         _, rays = O.direct(tree, inp.faces[sel], samples, first, inp.lights, inp.cluster_offsets,
                            inp.cluster_lights, inp.sky_directions, inp.sun_jitter, inp.sun_samples,
-                           inp.sun_angular_extent, threads=threads, count_rays=True)
+                           inp.sun_angular_extent, threads=threads, count_rays=True, verts=inp.verts)
         return rays, len(samples), time.perf_counter() - t0, len(sel)
     rays, n, dt, nf = run(max(1, len(inp.faces) // 64))
     stride = max(1, int(len(inp.faces) / max(1.0, nf * budget_s / max(dt, 1e-3))))
@@ -537,7 +537,7 @@ def main_stage(args):
         sel, samples, first, index = oracle_faces_sample(w, inp, 97)
         want = O.direct(tree, inp.faces[sel], samples, first, inp.lights, inp.cluster_offsets,
                         inp.cluster_lights, inp.sky_directions, inp.sun_jitter, inp.sun_samples,
-                        inp.sun_angular_extent)
+                        inp.sun_angular_extent, verts=inp.verts)
         stage.direct_device(d_out)
         torch.cuda.synchronize()
         got_all = d_out.view(n, 4).cpu().numpy()

@@ -220,6 +220,7 @@ int32_t vrad_destroy(vrad_ctx *ctx) {
         ctx->world.release();
         ctx->final_pass.release();
         ctx->bounce.release();
+        ctx->supersample.release();
         cudaFree(ctx->sample_light);
         cudaFree(ctx->status);
         cudaFree(ctx->d_rays);

@@ -11,6 +11,7 @@
 #include "direct.cuh"
 #include "final.cuh"
 #include "scene.cuh"
+#include "supersample.cuh"
 
 struct vrad_ctx {
     int device = 0;
@@ -34,10 +35,17 @@ struct vrad_ctx {
     std::vector<vrad_sample> h_samples;
     int32_t nclusters = 0;
     vrad::BounceBuffers bounce;
+    vrad::SupersampleBuffers supersample;
+    std::string supersample_why;     // why the world's samples cannot be supersampled
     std::string last_error;
     std::string identity;
 };
 
+
+// The direct gather with its supersampling passes into d_out (direct.cu).
+namespace vrad {
+int32_t direct_pass(vrad_ctx *ctx, float4 *d_out, cudaStream_t s);
+}
 
 // Shared error reporting (abi.cu).
 int32_t vrad_fail(vrad_ctx *ctx, int32_t code, const char *fmt, ...);

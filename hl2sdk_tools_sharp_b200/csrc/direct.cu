@@ -23,65 +23,12 @@
 #include <vector>
 
 #include "context.cuh"
-#include "detmath.cuh"
-#include "traverse.cuh"
+#include "gather.cuh"
+#include "supersample.cuh"
 
 namespace vrad {
 
 namespace {
-
-constexpr float kMaxTraceLength = (float)(1.732050807569 * (2 * 16384));  // LightConstants.MaxTraceLength
-constexpr float kEqualEpsilon = 0.001f;                                   // LightConstants.EqualEpsilon
-
-enum : int { kSurface = 0, kPoint = 1, kSpot = 2, kSkyLight = 3, kSkyAmbient = 4 };
-
-__device__ __forceinline__ float maxps(float a, float b) { return a > b ? a : b; }
-__device__ __forceinline__ float minps(float a, float b) { return a < b ? a : b; }
-
-// True when any lane of this lane's four-lane group has v set.
-__device__ __forceinline__ bool group_any(bool v, unsigned gmask) {
-    unsigned x = v ? 1u : 0u;
-    x |= __shfl_xor_sync(gmask, x, 1);
-    x |= __shfl_xor_sync(gmask, x, 2);
-    return x != 0;
-}
-
-// The segment start -> stop (LightRayLog.MakeRay: whole segment, reach 1).
-// Visibility blocks on any hit; a sky test blocks only when the first hit
-// is opaque.
-template <int MODE, int STRIDE>
-__device__ __forceinline__ bool segment_blocked(const DeviceScene &sc, float sx, float sy, float sz,
-                                                float ex, float ey, float ez, int *stack,
-                                                uint32_t *overflow) {
-    const RayState r = make_ray(sx, sy, sz, __fsub_rn(ex, sx), __fsub_rn(ey, sy), __fsub_rn(ez, sz));
-    bool hit;
-    float t;
-    int32_t orig;
-    uint32_t meta;
-    trace_ray<MODE, STRIDE>(sc, r, 0.0f, 1.0f, -1, stack, overflow, hit, t, orig, meta);
-    return hit;
-}
-
-// QuinticInterpolatingPolynomial fade (GatherPointFour / GatherStandardLane).
-__device__ __forceinline__ float fade(float dist, float start, float span) {
-    float t = __fdiv_rn(__fsub_rn(dist, start), span);
-    t = minps(t, 1.0f);
-    t = maxps(t, 0.0f);
-    t = __fsub_rn(1.0f, t);
-    float mult = __fsub_rn(__fmul_rn(6.0f, t), 15.0f);
-    mult = __fadd_rn(__fmul_rn(mult, t), 10.0f);
-    mult = __fmul_rn(__fmul_rn(t, t), mult);
-    return __fmul_rn(t, mult);
-}
-
-// InverseQuadratic: ((d*d)*q + l*d) + c, then its reciprocal.
-__device__ __forceinline__ float inverse_quadratic(float d, float q, float l, float c) {
-    float f = __fmul_rn(d, d);
-    f = __fmul_rn(f, q);
-    f = __fadd_rn(f, __fmul_rn(l, d));
-    f = __fadd_rn(f, c);
-    return __fdiv_rn(1.0f, f);
-}
 
 // BLOCK threads per CTA (32, 64 or 128, chosen by vrad_direct_autotune):
 // every thread traces its samples' whole light list, so a small CTA frees
@@ -112,139 +59,10 @@ __global__ void __launch_bounds__(BLOCK) k_direct(DeviceScene sc, DeviceWorld w,
     // One unit off the face (ComputeIlluminationPointAndNormals).
     const float px = __fadd_rn(sp.x, nx), py = __fadd_rn(sp.y, ny), pz = __fadd_rn(sp.z, nz);
 
-    float ax = 0.0f, ay = 0.0f, az = 0.0f, sun = 0.0f;
     unsigned long long vis_rays = 0, sky_rays = 0;
-
-    const int l0 = __ldg(&w.cl_off[cluster]), l1 = __ldg(&w.cl_off[cluster + 1]);
-    for (int k = l0; k < l1; k++) {
-        const int li = __ldg(&w.cl_list[k]);
-        const float4 *L = w.lights + kLightF4 * li;
-        const float4 A = __ldg(L), B = __ldg(L + 1), C = __ldg(L + 2), D = __ldg(L + 3), E = __ldg(L + 4);
-        const int type = __float_as_int(A.w);
-        float dot = 0.0f, falloff = 0.0f, sun_amount = 0.0f;
-
-        if (type == kPoint || type == kSpot) {
-            const bool hard = E.z > E.y;  // EndFadeDistance > StartFadeDistance
-            float dx = __fsub_rn(A.x, px), dy = __fsub_rn(A.y, py), dz = __fsub_rn(A.z, pz);
-            const float dist2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-            float dist = __fsqrt_rn(dist2);
-            const float rpc = __fdiv_rn(1.0f, dist);
-            dx = __fmul_rn(dx, rpc);
-            dy = __fmul_rn(dy, rpc);
-            dz = __fmul_rn(dz, rpc);
-            float d = __fadd_rn(__fadd_rn(__fmul_rn(dx, nx), __fmul_rn(dy, ny)), __fmul_rn(dz, nz));
-            d = maxps(0.0f, d);
-            bool live = !hard || dist <= E.z;
-            if (type == kPoint) {
-                // GatherPointFour.
-                dist = maxps(dist, 1.0f);
-                const float dd = minps(dist, E.w);
-                float f = inverse_quadratic(dd, E.x, D.w, D.z);
-                if (hard) f = __fmul_rn(fade(dist, E.y, __fsub_rn(E.z, E.y)), f);
-                dot = live ? d : 0.0f;
-                falloff = live ? f : 0.0f;
-            } else if (live) {
-                // GatherStandardLane, Spotlight.
-                dist = maxps(dist, 1.0f);
-                const float fed = minps(dist, E.w);
-                const float dot2 =
-                    -__fadd_rn(__fadd_rn(__fmul_rn(dx, C.x), __fmul_rn(dy, C.y)), __fmul_rn(dz, C.z));
-                if (dot2 > D.y) {
-                    float f = __fmul_rn(inverse_quadratic(fed, E.x, D.w, D.z), dot2);
-                    const bool fringe = dot2 <= D.x;
-                    float mult = __fdiv_rn(__fsub_rn(dot2, D.y), __fsub_rn(D.x, D.y));
-                    mult = minps(mult, 1.0f);
-                    mult = maxps(mult, 0.0f);
-                    if (C.w != 0.0f && C.w != 1.0f) mult = pow_cr(mult, C.w, &counters[2]);  // DetMathF.Pow
-                    mult = fringe ? mult : 1.0f;
-                    f = __fmul_rn(mult, f);
-                    if (hard) f = __fmul_rn(fade(dist, E.y, __fsub_rn(E.z, E.y)), f);
-                    dot = d;
-                    falloff = f;
-                }
-            }
-            if (real && dot != 0.0f && falloff != 0.0f) {
-                vis_rays++;
-                if (segment_blocked<kModeAny, BLOCK>(sc, px, py, pz, A.x, A.y, A.z, stack, overflow)) dot = 0.0f;
-            }
-        } else if (type == kSkyLight) {
-            // EmitSkyLight / ResolveSkyLight.
-            float d = -__fadd_rn(__fadd_rn(__fmul_rn(nx, C.x), __fmul_rn(ny, C.y)), __fmul_rn(nz, C.z));
-            d = maxps(d, 0.0f);
-            const bool need = group_any(d != 0.0f, gmask);
-            if (__any_sync(kFull, need)) {
-                const int ns = w.sun_samples;
-                const float jitter_scale = (float)(1.732050807569 * (2 * 16384) * (double)w.sun_extent);
-                float total = 0.0f;
-                for (int s = 0; s < ns; s++) {
-                    float ex = __fmul_rn(C.x, -kMaxTraceLength), ey = __fmul_rn(C.y, -kMaxTraceLength),
-                          ez = __fmul_rn(C.z, -kMaxTraceLength);
-                    if (s != 0) {
-                        const float4 j = __ldg(&w.jitter[s - 1]);
-                        ex = __fadd_rn(ex, __fmul_rn(j.x, jitter_scale));
-                        ey = __fadd_rn(ey, __fmul_rn(j.y, jitter_scale));
-                        ez = __fadd_rn(ez, __fmul_rn(j.z, jitter_scale));
-                    }
-                    float frac = 1.0f;
-                    if (need && real) {
-                        sky_rays++;
-                        if (segment_blocked<kModeSkyPass, BLOCK>(sc, px, py, pz, __fadd_rn(ex, px),
-                                                                 __fadd_rn(ey, py), __fadd_rn(ez, pz), stack,
-                                                                 overflow))
-                            frac = 0.0f;
-                    }
-                    total = __fadd_rn(total, frac);
-                    __syncwarp();
-                }
-                if (need) {
-                    const float see = __fmul_rn(total, __fdiv_rn(1.0f, (float)ns));
-                    dot = __fmul_rn(d, see);
-                    falloff = 1.0f;
-                    sun_amount = __fmul_rn(see, 10000.0f);
-                }
-            }
-        } else if (type == kSkyAmbient) {
-            // AmbientSky: every direction in front of the face, in order.
-            float sumdot = 0.0f, possible = 0.0f, ambient = 0.0f;
-            for (int di = 0; di < w.ndirs; di++) {
-                const float4 an = __ldg(&w.dirs[di]);
-                const float dd = -__fadd_rn(__fadd_rn(__fmul_rn(nx, an.x), __fmul_rn(ny, an.y)), __fmul_rn(nz, an.z));
-                const bool valid = dd > kEqualEpsilon;
-                const float dv = valid ? dd : 0.0f;
-                sumdot = __fadd_rn(dv, sumdot);
-                possible = __fadd_rn(valid ? 1.0f : 0.0f, possible);
-                float frac = 1.0f;
-                if (valid && real) {
-                    // surfacePos = points - anorm * -epsilon, epsilon 0;
-                    // stop = anorm * -MaxTraceLength + points.
-                    const float sx = __fsub_rn(px, __fmul_rn(an.x, -0.0f));
-                    const float sy = __fsub_rn(py, __fmul_rn(an.y, -0.0f));
-                    const float sz = __fsub_rn(pz, __fmul_rn(an.z, -0.0f));
-                    const float ex = __fadd_rn(__fmul_rn(an.x, -kMaxTraceLength), px);
-                    const float ey = __fadd_rn(__fmul_rn(an.y, -kMaxTraceLength), py);
-                    const float ez = __fadd_rn(__fmul_rn(an.z, -kMaxTraceLength), pz);
-                    sky_rays++;
-                    if (segment_blocked<kModeSkyPass, BLOCK>(sc, sx, sy, sz, ex, ey, ez, stack, overflow)) frac = 0.0f;
-                }
-                ambient = __fadd_rn(ambient, __fmul_rn(frac, dv));
-                __syncwarp();
-            }
-            const float factor = __fdiv_rn(possible, possible);
-            dot = __fdiv_rn(ambient, __fmul_rn(factor, sumdot));
-            falloff = 1.0f;
-        }
-        __syncwarp();
-        // Resolve: a light behind the face lights nothing.
-        dot = maxps(dot, 0.0f);
-        const float fx = __fmul_rn(real ? dot : 0.0f, falloff);
-        if (!group_any(fx != 0.0f, gmask)) continue;
-        if (real) {
-            ax = __fadd_rn(ax, __fmul_rn(fx, B.x));
-            ay = __fadd_rn(ay, __fmul_rn(fx, B.y));
-            az = __fadd_rn(az, __fmul_rn(fx, B.z));
-            sun = __fadd_rn(sun, sun_amount);
-        }
-    }
+    const float4 r = gather_point<BLOCK>(sc, w, cluster, px, py, pz, nx, ny, nz, real, gmask, kAllLights, stack,
+                                         overflow, counters, vis_rays, sky_rays);
+    const float ax = r.x, ay = r.y, az = r.z, sun = r.w;
     if (real) out[si] = make_float4(ax, ay, az, sun);
 
     // Ray counts: one atomic per warp.
@@ -459,6 +277,18 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
             return vrad_cuda_fail(ctx, e, why.c_str());
         }
         ctx->final_pass.view.sample_pos = wb.sample_pos;
+        bool have = false;
+        e = vrad::build_supersample(ctx->supersample, ctx->h_faces, ctx->h_vertices, ctx->h_samples, ctx->final_pass,
+                                    w->nclusters, have, why);
+        if (e != cudaSuccess) {
+            wb.release();
+            ctx->final_pass.release();
+            return vrad_cuda_fail(ctx, e, why.c_str());
+        }
+        ctx->supersample_why = have ? std::string() : why;
+    } else {
+        ctx->supersample.release();
+        ctx->supersample_why = "the world was uploaded without face windings";
     }
     e = cudaMalloc(&ctx->sample_light, sizeof(float4) * (size_t)(w->nsamples ? w->nsamples : 1));
     if (e != cudaSuccess) {
@@ -479,11 +309,23 @@ int32_t direct_on(vrad_ctx *ctx, float4 *d_out, cudaStream_t s) {
     if (e == cudaSuccess)
         e = vrad::launch_direct(ctx->scene.view(), ctx->world.view, d_out, ctx->world.counters, ctx->status, s,
                                 ctx->world.block);
+    // The supersampling passes (FaceLightJob's rounds after the first).
+    if (e == cudaSuccess && ctx->supersample.extra_passes > 0 && !ctx->supersample.ready && ctx->world.view.nsamples)
+        return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "supersampling: %s (vrad_set_extra_passes 0 turns it off)",
+                         ctx->supersample_why.c_str());
+    if (e == cudaSuccess)
+        e = vrad::run_supersample(ctx->supersample, ctx->scene.view(), ctx->world.view, ctx->final_pass.view, d_out,
+                                  ctx->world.counters, ctx->status, s);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "direct lighting launch");
     return VRAD_OK;
 }
 
 }  // namespace
+
+namespace vrad {
+// The direct gather with its supersampling passes (the light pass's first step).
+int32_t direct_pass(vrad_ctx *ctx, float4 *d_out, cudaStream_t s) { return direct_on(ctx, d_out, s); }
+}  // namespace vrad
 
 extern "C" int32_t vrad_direct_lighting_device(vrad_ctx *ctx, vrad_lighting_value *d_out, void *stream) {
     if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
@@ -536,6 +378,8 @@ extern "C" int32_t vrad_direct_lighting(vrad_ctx *ctx, vrad_lighting_value *out,
         stats->visibility_rays = (int64_t)counts[0];
         stats->sky_rays = (int64_t)counts[1];
         stats->kernel_ms = ms;
+        stats->extra_passes_run = ctx->supersample.passes_run;
+        stats->supersampled = ctx->supersample.supersampled;
     }
     cudaFree(d_out);
     cudaEventDestroy(a);
@@ -579,5 +423,13 @@ extern "C" int32_t vrad_direct_autotune(vrad_ctx *ctx, int32_t *chosen_block, fl
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "direct autotune");
     ctx->world.block = best_block;
     if (chosen_block) *chosen_block = best_block;
+    return VRAD_OK;
+}
+
+extern "C" int32_t vrad_set_extra_passes(vrad_ctx *ctx, int32_t passes) {
+    if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
+    if (passes < 0) return vrad_fail(ctx, VRAD_ERR_ARG, "extra passes %d < 0", passes);
+    std::lock_guard<std::mutex> g(ctx->mu);
+    ctx->supersample.extra_passes = passes;
     return VRAD_OK;
 }

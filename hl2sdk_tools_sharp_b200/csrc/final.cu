@@ -463,10 +463,9 @@ int32_t pass_on(vrad_ctx *ctx, uint8_t *d_lighting, cudaStream_t s, cudaEvent_t 
     if (!ctx->world.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no lighting world uploaded");
     if (!ctx->final_pass.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without face windings");
     vrad::FinalBuffers &fb = ctx->final_pass;
-    cudaError_t e = cudaMemsetAsync(ctx->world.counters, 0, 3 * sizeof(unsigned long long), s);
-    if (e == cudaSuccess)
-        e = vrad::launch_direct(ctx->scene.view(), ctx->world.view, ctx->sample_light, ctx->world.counters,
-                                ctx->status, s, ctx->world.block);
+    const int32_t rc = vrad::direct_pass(ctx, ctx->sample_light, s);
+    if (rc != VRAD_OK) return rc;
+    cudaError_t e = cudaSuccess;
     if (e == cudaSuccess && mid) e = cudaEventRecord(mid, s);
     // The bounce (patch light, transfers, bounces), when one is uploaded.
     vrad::PatchRadialView prad{};
@@ -558,6 +557,9 @@ extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t cap
             stats->lighting_bytes = fb.lighting_bytes;
             stats->direct_ms = d_ms;
             stats->final_ms = f_ms;
+            stats->extra_passes_run = ctx->supersample.passes_run;
+            stats->supersampled = ctx->supersample.supersampled;
+            stats->supersample_ms = ctx->supersample.ms;
         }
     }
     cudaFree(d_lighting);

@@ -86,9 +86,16 @@ float world_area_per_luxel(const vrad_face &f) {
 
 }  // namespace
 
-extern "C" int32_t vrad_build_samples(const vrad_face *faces, int32_t nfaces, const float *vertices,
-                                      int64_t nvertices, vrad_sample *out, int64_t capacity,
-                                      int64_t *count, int64_t *face_first) {
+namespace {
+
+// FaceSampleBuilder.BuildFacesamples over every face.  With wind set, it
+// also keeps each partial sample's cell winding in world space (the
+// reference keeps them for supersampling, MakeSample with do_extra:
+// FaceSampleBuilder.cs:325-367): wind gets (first point, count) per sample,
+// count 0 for a whole cell, and pts the points (xyz each).
+int32_t build_samples_core(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
+                           vrad_sample *out, int64_t capacity, int64_t *count, int64_t *face_first,
+                           std::vector<int32_t> *wind, std::vector<float> *pts) {
     if (nfaces < 0 || (nfaces > 0 && (!faces || !vertices)) || !count) return VRAD_ERR_ARG;
     int64_t written = 0;
     Winding cell_front, cell_back, row_front, row_back;
@@ -131,6 +138,21 @@ extern "C" int32_t vrad_build_samples(const vrad_face *faces, int32_t nfaces, co
                         if (p.y < mn[1]) mn[1] = p.y;
                         if (p.y > mx[1]) mx[1] = p.y;
                     }
+                    if (wind) {
+                        // EQUAL_EPSILON is a double literal: the test is in double.
+                        int32_t first = (int32_t)(pts->size() / 3), n = 0;
+                        if ((double)area < (double)area_per_luxel - 0.001) {
+                            for (const V3 &p : cell_back) {
+                                const V3 q = luxel_to_world(fr, p.x, p.y);
+                                pts->push_back(q.x);
+                                pts->push_back(q.y);
+                                pts->push_back(q.z);
+                                n++;
+                            }
+                        }
+                        wind->push_back(n ? first : 0);
+                        wind->push_back(n);
+                    }
                     if (out) {
                         vrad_sample &o = out[written];
                         V3 pos = luxel_to_world(fr, center.x, center.y);
@@ -160,6 +182,33 @@ extern "C" int32_t vrad_build_samples(const vrad_face *faces, int32_t nfaces, co
     *count = written;
     return VRAD_OK;
 }
+
+}  // namespace
+
+extern "C" int32_t vrad_build_samples(const vrad_face *faces, int32_t nfaces, const float *vertices,
+                                      int64_t nvertices, vrad_sample *out, int64_t capacity,
+                                      int64_t *count, int64_t *face_first) {
+    return build_samples_core(faces, nfaces, vertices, nvertices, out, capacity, count, face_first, nullptr, nullptr);
+}
+
+namespace vrad {
+
+bool sample_windings(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
+                     const vrad_sample *given, int64_t ngiven, std::vector<int32_t> &wind, std::vector<float> &pts) {
+    int64_t n = 0;
+    if (build_samples_core(faces, nfaces, vertices, nvertices, nullptr, INT64_MAX, &n, nullptr, nullptr, nullptr) !=
+            VRAD_OK ||
+        n != ngiven)
+        return false;
+    std::vector<vrad_sample> mine((size_t)(n ? n : 1));
+    wind.clear();
+    pts.clear();
+    if (build_samples_core(faces, nfaces, vertices, nvertices, mine.data(), n, &n, nullptr, &wind, &pts) != VRAD_OK)
+        return false;
+    return n == 0 || std::memcmp(mine.data(), given, sizeof(vrad_sample) * (size_t)n) == 0;
+}
+
+}  // namespace vrad
 
 // ---- smoothing neighbours and the lightmap layout --------------------------
 

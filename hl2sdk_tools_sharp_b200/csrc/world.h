@@ -23,6 +23,14 @@ void face_frame_of(const vrad_face &f, FaceFrameOut &out);
 void frame_luxel_to_world(const FaceFrameOut &fr, float s, float t, float out[3]);
 void frame_world_to_luxel(const FaceFrameOut &fr, const float p[3], float &s, float &t);
 
+// The cell windings (world space) of the partial samples, as
+// FaceSampleBuilder keeps them for supersampling: wind holds (first point,
+// count) per sample, count 0 for a sample whose cell the face covers
+// whole; pts the points (xyz each).  False unless the samples the builder
+// makes from these faces are exactly `given`.
+bool sample_windings(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
+                     const vrad_sample *given, int64_t ngiven, std::vector<int32_t> &wind, std::vector<float> &pts);
+
 // The welded vertex numbers of each face's winding (vertices identified by
 // position) and, per vertex, the faces touching it in face order.  False
 // when a face's winding lies outside the vertex array.

@@ -76,7 +76,8 @@ class _WorldDesc(ctypes.Structure):
 class PassStats(ctypes.Structure):
     _fields_ = [("samples", ctypes.c_int64), ("luxels", ctypes.c_int64), ("visibility_rays", ctypes.c_int64),
                 ("sky_rays", ctypes.c_int64), ("lighting_bytes", ctypes.c_int64), ("direct_ms", ctypes.c_float),
-                ("final_ms", ctypes.c_float)]
+                ("final_ms", ctypes.c_float), ("extra_passes_run", ctypes.c_int32), ("supersampled", ctypes.c_int64),
+                ("supersample_ms", ctypes.c_float)]
 
 
 class _BounceDesc(ctypes.Structure):
@@ -95,7 +96,8 @@ class BounceStats(ctypes.Structure):
 
 class DirectStats(ctypes.Structure):
     _fields_ = [("samples", ctypes.c_int64), ("visibility_rays", ctypes.c_int64),
-                ("sky_rays", ctypes.c_int64), ("kernel_ms", ctypes.c_float)]
+                ("sky_rays", ctypes.c_int64), ("kernel_ms", ctypes.c_float), ("extra_passes_run", ctypes.c_int32),
+                ("supersampled", ctypes.c_int64)]
 
 
 def _lib():
@@ -122,6 +124,8 @@ def _lib():
         lib.vrad_light_pass.restype = i32
         lib.vrad_light_pass_device.argtypes = [P, P, P]
         lib.vrad_light_pass_device.restype = i32
+        lib.vrad_set_extra_passes.argtypes = [P, i32]
+        lib.vrad_set_extra_passes.restype = i32
         lib.vrad_build_patches.argtypes = [P, i32, P, i64, P, ctypes.c_float, ctypes.c_float, P, i64,
                                            ctypes.POINTER(i64), P, i64, ctypes.POINTER(i64)]
         lib.vrad_build_patches.restype = i32
@@ -394,6 +398,10 @@ class LightingStage:
                        vv.ctypes.data, len(vv))
         T._check(_lib().vrad_world_upload(self._ctx, ctypes.byref(d)), self._ctx)
         self.inputs = i
+
+    def set_extra_passes(self, passes: int) -> None:
+        """vrad_set_extra_passes: supersampling passes (4 default, 0 off)."""
+        T._check(_lib().vrad_set_extra_passes(self._ctx, passes), self._ctx)
 
     def upload_bounce(self, reflectivity: np.ndarray, pvs_offsets: np.ndarray, pvs_clusters: np.ndarray,
                       bounces: int = 100, threshold: float = 1.0, max_chop: float = 4.0,

@@ -246,6 +246,8 @@ typedef struct vrad_direct_stats {
     int64_t visibility_rays;   /* shadow segments to point and spot lights */
     int64_t sky_rays;          /* sun and sky-ambient sky tests */
     float kernel_ms;
+    int32_t extra_passes_run;  /* supersampling passes that selected samples */
+    int64_t supersampled;      /* samples supersampled, over all passes */
 } vrad_direct_stats;
 
 /* FaceSampleBuilder.CalcPoints without -fast (FaceSampleBuilder.cs:80-367):
@@ -277,7 +279,15 @@ int32_t vrad_lightmap_layout(const vrad_face *faces, int32_t nfaces, int32_t *li
 int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *world);
 
 /* The direct gather of every sample, style 0, flat normals: out[i] is
- * sample i's LightingValue (host buffer, nsamples entries).  Blocks. */
+ * sample i's LightingValue (host buffer, nsamples entries), after the
+ * supersampling passes (FaceLightJob's rounds after the first,
+ * FaceLightJob.cs:553-930: samples whose perceptual light differs from a
+ * neighbour's by 1/16 or more are gathered again on 4x4 and 2x2 grids
+ * across their cell, up to vrad_set_extra_passes passes).  Supersampling
+ * needs the world uploaded with face windings and samples exactly as
+ * vrad_build_samples makes them (their partial cells' windings are rebuilt
+ * from the faces); otherwise, with extra passes above 0, the call fails
+ * with VRAD_ERR_UNSUPPORTED.  Blocks. */
 int32_t vrad_direct_lighting(vrad_ctx *ctx, vrad_lighting_value *out, vrad_direct_stats *stats);
 
 /* The same into a device buffer on `stream` (NULL = default stream). */
@@ -291,6 +301,9 @@ typedef struct vrad_pass_stats {
     int64_t lighting_bytes;
     float direct_ms;
     float final_ms;
+    int32_t extra_passes_run;
+    int64_t supersampled;
+    float supersample_ms;     /* of direct_ms */
 } vrad_pass_stats;
 
 /* Size in bytes of the LIGHTING lump the uploaded world produces
@@ -310,6 +323,11 @@ int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t capacity, int3
 
 /* The same into a device buffer on `stream` (NULL = default stream). */
 int32_t vrad_light_pass_device(vrad_ctx *ctx, uint8_t *d_lighting, void *stream);
+
+/* DirectLightingSettings.ExtraPasses: how many supersampling passes the
+ * direct gather may run (the reference's default, and this library's, is
+ * 4; 0 is -noextra, no supersampling). */
+int32_t vrad_set_extra_passes(vrad_ctx *ctx, int32_t passes);
 
 /* Times the gather once per launch shape (32, 64 and 128 threads per CTA)
  * on the uploaded world and keeps the fastest for later calls; times_ms

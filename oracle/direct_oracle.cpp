@@ -126,90 +126,117 @@ void clip(const W &w, int axis, float d, float eps, W &front, W &back) {
 
 }  // namespace
 
+namespace {
+
+// FaceSampleBuilder.BuildFacesamples for one face, appending its samples;
+// with wind set, each partial sample's cell winding in world space
+// (MakeSample keeps it when area < worldAreaPerLuxel - EQUAL_EPSILON, in
+// double), an empty one for a whole cell.
+void face_samples(const orc_face &f, int32_t fi, const float *verts, std::vector<orc_sample> &out,
+                  std::vector<W> *wind) {
+    const float eps = 0.1f / 16.0f;
+    Info in = face_info(f);
+    float ss = (f.vecs[0][0] * f.vecs[0][0] + f.vecs[0][1] * f.vecs[0][1]) + f.vecs[0][2] * f.vecs[0][2];
+    float tt = (f.vecs[1][0] * f.vecs[1][0] + f.vecs[1][1] * f.vecs[1][1]) + f.vecs[1][2] * f.vecs[1][2];
+    float apl = (float)(1.0 / (double)(std::sqrt(ss) * std::sqrt(tt)));
+    W w;
+    for (int v = 0; v < f.num_vertices; v++) {
+        const float *p = verts + 3 * (f.first_vertex + v);
+        w.push_back(F3{p[0], p[1], p[2]} + F3{0, 0, 0});
+    }
+    // RemoveColinearPoints.
+    {
+        W kept;
+        int n = (int)w.size();
+        for (int i = 0; i < n; i++) {
+            F3 v1 = Normalise(w[(i + 1) % n] - w[i]);
+            F3 v2 = Normalise(w[i] - w[(i + n - 1) % n]);
+            if ((double)Dot(v1, v2) < 0.999) kept.push_back(w[i]);
+        }
+        if ((int)kept.size() != n) w = kept;
+    }
+    for (F3 &p : w) {
+        F3 q = p - in.origin;
+        p = {Dot(q, in.ws) - (float)in.mins, Dot(q, in.wt) - (float)in.mint, 0.0f};
+    }
+    auto l2w = [&](float s, float t) {
+        float su = s + (float)in.mins, tv = t + (float)in.mint;
+        F3 pos = in.origin + in.ls * su;
+        return pos + in.lt * tv;
+    };
+    W rest = w, rowf, rowb, cf, cb;
+    for (int t = 0; t < in.height && !rest.empty(); t++) {
+        clip(rest, 1, (float)t + 1.0f, eps, rowf, rowb);
+        W row = rowb;
+        for (int s = 0; s < in.width && !row.empty(); s++) {
+            clip(row, 0, (float)s + 1.0f, eps, cf, cb);
+            if (!cb.empty()) {
+                // AreaAndBalancePoint.
+                F3 c = {0, 0, 0};
+                float total = 0.0f;
+                for (size_t i = 2; i < cb.size(); i++) {
+                    float a = Len(Cross(cb[i - 1] - cb[0], cb[i] - cb[0]));
+                    total += a;
+                    float third = (float)((double)a / 3.0);
+                    c = c + cb[i - 1] * third;
+                    c = c + cb[i] * third;
+                    c = c + cb[0] * third;
+                }
+                if (total != 0.0f) c = c * (float)(1.0 / (double)total);
+                float area = total * 0.5f * apl;
+                orc_sample o;
+                o.area = area;
+                o.coord[0] = c.x;
+                o.coord[1] = c.y;
+                float mn[2] = {99999.0f, 99999.0f}, mx[2] = {-99999.0f, -99999.0f};
+                for (const F3 &p : cb) {
+                    if (p.x < mn[0]) mn[0] = p.x;
+                    if (p.x > mx[0]) mx[0] = p.x;
+                    if (p.y < mn[1]) mn[1] = p.y;
+                    if (p.y > mx[1]) mx[1] = p.y;
+                }
+                o.mins[0] = mn[0];
+                o.mins[1] = mn[1];
+                o.maxs[0] = mx[0];
+                o.maxs[1] = mx[1];
+                F3 pos = l2w(c.x, c.y);
+                o.position[0] = pos.x;
+                o.position[1] = pos.y;
+                o.position[2] = pos.z;
+                o.s = s;
+                o.t = t;
+                o.face = fi;
+                o.cluster = f.cluster;
+                out.push_back(o);
+                if (wind) {
+                    W cell;
+                    if ((double)area < (double)apl - 0.001)
+                        for (const F3 &p : cb) cell.push_back(l2w(p.x, p.y));
+                    wind->push_back(cell);
+                }
+            }
+            row = cf;
+        }
+        rest = rowf;
+    }
+}
+
+}  // namespace
+
 extern "C" int orc_build_samples(const orc_face *faces, int32_t nfaces, const float *verts,
                                  orc_sample *out, int64_t capacity, int64_t *count, int64_t *first) {
     int64_t k = 0;
-    const float eps = 0.1f / 16.0f;
+    std::vector<orc_sample> tmp;
     for (int32_t fi = 0; fi < nfaces; fi++) {
-        const orc_face &f = faces[fi];
         if (first) first[fi] = k;
-        Info in = face_info(f);
-        float ss = (f.vecs[0][0] * f.vecs[0][0] + f.vecs[0][1] * f.vecs[0][1]) + f.vecs[0][2] * f.vecs[0][2];
-        float tt = (f.vecs[1][0] * f.vecs[1][0] + f.vecs[1][1] * f.vecs[1][1]) + f.vecs[1][2] * f.vecs[1][2];
-        float apl = (float)(1.0 / (double)(std::sqrt(ss) * std::sqrt(tt)));
-        W w;
-        for (int v = 0; v < f.num_vertices; v++) {
-            const float *p = verts + 3 * (f.first_vertex + v);
-            w.push_back(F3{p[0], p[1], p[2]} + F3{0, 0, 0});
-        }
-        // RemoveColinearPoints.
-        {
-            W kept;
-            int n = (int)w.size();
-            for (int i = 0; i < n; i++) {
-                F3 v1 = Normalise(w[(i + 1) % n] - w[i]);
-                F3 v2 = Normalise(w[i] - w[(i + n - 1) % n]);
-                if ((double)Dot(v1, v2) < 0.999) kept.push_back(w[i]);
+        tmp.clear();
+        face_samples(faces[fi], fi, verts, tmp, nullptr);
+        for (const orc_sample &o : tmp) {
+            if (out) {
+                if (k >= capacity) return -1;
+                out[k] = o;
             }
-            if ((int)kept.size() != n) w = kept;
-        }
-        for (F3 &p : w) {
-            F3 q = p - in.origin;
-            p = {Dot(q, in.ws) - (float)in.mins, Dot(q, in.wt) - (float)in.mint, 0.0f};
-        }
-        W rest = w, rowf, rowb, cf, cb;
-        for (int t = 0; t < in.height && !rest.empty(); t++) {
-            clip(rest, 1, (float)t + 1.0f, eps, rowf, rowb);
-            W row = rowb;
-            for (int s = 0; s < in.width && !row.empty(); s++) {
-                clip(row, 0, (float)s + 1.0f, eps, cf, cb);
-                if (!cb.empty()) {
-                    if (out && k >= capacity) return -1;
-                    if (out) {
-                        // AreaAndBalancePoint.
-                        F3 c = {0, 0, 0};
-                        float total = 0.0f;
-                        for (size_t i = 2; i < cb.size(); i++) {
-                            float a = Len(Cross(cb[i - 1] - cb[0], cb[i] - cb[0]));
-                            total += a;
-                            float third = (float)((double)a / 3.0);
-                            c = c + cb[i - 1] * third;
-                            c = c + cb[i] * third;
-                            c = c + cb[0] * third;
-                        }
-                        if (total != 0.0f) c = c * (float)(1.0 / (double)total);
-                        float area = total * 0.5f * apl;
-                        orc_sample &o = out[k];
-                        o.area = area;
-                        o.coord[0] = c.x;
-                        o.coord[1] = c.y;
-                        float mn[2] = {99999.0f, 99999.0f}, mx[2] = {-99999.0f, -99999.0f};
-                        for (const F3 &p : cb) {
-                            if (p.x < mn[0]) mn[0] = p.x;
-                            if (p.x > mx[0]) mx[0] = p.x;
-                            if (p.y < mn[1]) mn[1] = p.y;
-                            if (p.y > mx[1]) mx[1] = p.y;
-                        }
-                        o.mins[0] = mn[0];
-                        o.mins[1] = mn[1];
-                        o.maxs[0] = mx[0];
-                        o.maxs[1] = mx[1];
-                        float su = c.x + (float)in.mins, tv = c.y + (float)in.mint;
-                        F3 pos = in.origin + in.ls * su;
-                        pos = pos + in.lt * tv;
-                        o.position[0] = pos.x;
-                        o.position[1] = pos.y;
-                        o.position[2] = pos.z;
-                        o.s = s;
-                        o.t = t;
-                        o.face = fi;
-                        o.cluster = f.cluster;
-                    }
-                    k++;
-                }
-                row = cf;
-            }
-            rest = rowf;
+            k++;
         }
     }
     if (first) first[nfaces] = k;
@@ -247,6 +274,13 @@ bool visible(const Ctx &c, F3 a, F3 b, bool sky) {
     orc_ray r{a.x, a.y, a.z, d.x, d.y, d.z, 1.0f};
     return !orc_kd_segment_blocked(c.kd, r, sky);
 }
+
+// DetMathF.Pow: the correctly rounded float power, here the x87 extended
+// power rounded once.
+float PowF(float x, float y) { return (float)powl((long double)x, (long double)y); }
+
+// DetMath.PowToSingle: x^y rounded to double, then to float.
+float PowToSingle(double x, double y) { return (float)(double)powl((long double)x, (long double)y); }
 
 float inv_quadratic(const orc_light &L, float d) {
     float f = d * d;
@@ -316,7 +350,7 @@ void gather(const Ctx &c, const orc_light &L, const F3 pts[4], const F3 nrm[4], 
             float mult = (dot2 - L.stop_dot2) / (L.stop_dot - L.stop_dot2);
             mult = MinPs(mult, 1.0f);
             mult = MaxPs(mult, 0.0f);
-            if (L.exponent != 0.0f && L.exponent != 1.0f) mult = (float)std::pow((double)mult, (double)L.exponent);
+            if (L.exponent != 0.0f && L.exponent != 1.0f) mult = PowF(mult, L.exponent);
             mult = fringe ? mult : 1.0f;
             fall = mult * fall;
             if (hard) fall = quintic(dist, L) * fall;
@@ -397,13 +431,199 @@ void gather(const Ctx &c, const orc_light &L, const F3 pts[4], const F3 nrm[4], 
 
 }  // namespace
 
+namespace {
+
+// PointsInWinding (FaceLightJob.cs:902-940).
+bool PointsInWinding(const F3 pts[4], const W &winding, int &invalidBits) {
+    invalidBits = 0;
+    const int n = (int)winding.size();
+    F3 test[4];
+    bool invalid[4] = {false, false, false, false};
+    for (int l = 0; l < 4; l++) test[l] = Normalise(Cross(winding[1 % n] - winding[0], pts[l] - winding[0]));
+    for (int k = 1; k < n; k++) {
+        F3 p0 = winding[k], p1 = winding[(k + 1) % n];
+        F3 edge = p1 - p0;
+        invalidBits = 0;
+        for (int l = 0; l < 4; l++) {
+            F3 cr = Normalise(Cross(edge, pts[l] - p0));
+            float dot = Dot(cr, test[l]);
+            invalid[l] |= dot < 0.0f;
+            invalidBits |= invalid[l] ? 1 << l : 0;
+        }
+        if (invalidBits == 0xF) return false;
+    }
+    return true;
+}
+
+// EmitResample + ResolveResample for one row of four points: the ambient
+// light alone or every other light, each added with AddLight (no skip).
+void Resample(const Ctx &c, const F3 pts[4], F3 n, int cl, const int32_t *cl_off, const int32_t *cl_list,
+              bool ambientOnly, float result[4][4]) {
+    std::memset(result, 0, sizeof(float) * 16);
+    F3 nrm[4] = {n, n, n, n};
+    for (int k = cl_off[cl]; k < cl_off[cl + 1]; k++) {
+        const orc_light &L = c.lights[cl_list[k]];
+        if (ambientOnly && L.type != 4) continue;
+        if (!ambientOnly && L.type == 4) continue;
+        Out4 o;
+        gather(c, L, pts, nrm, 4, o);
+        for (int l = 0; l < 4; l++) {
+            float f = o.falloff[l] * o.dot[l];
+            result[l][0] = result[l][0] + (f * L.intensity[0]);
+            result[l][1] = result[l][1] + (f * L.intensity[1]);
+            result[l][2] = result[l][2] + (f * L.intensity[2]);
+            result[l][3] += o.sun[l];
+        }
+    }
+}
+
+// The supersampling passes of one face (FaceLightJob.AdvanceAfterRound and
+// StyleSupersample), over its samples' light (4 floats each).
+int64_t Supersample(const Ctx &c, const orc_face &f, const orc_sample *samples, int64_t nsamp, const std::vector<W> &wind,
+                    const int32_t *cl_off, const int32_t *cl_list, int extra_passes, float *light) {
+    const Info in = face_info(f);
+    const int w = in.width, h = in.height, size = w * h;
+    std::vector<float> inten((size_t)size, 0.0f);
+    std::vector<char> has((size_t)size, 0), processed((size_t)nsamp, 0);
+    std::vector<float> grad((size_t)nsamp, 0.0f);
+    auto intensity = [&](int64_t i) {
+        const float *v = light + 4 * i;
+        float sum = v[0] + v[1] + v[2];
+        inten[(size_t)(samples[i].s + samples[i].t * w)] = PowToSingle(sum / 256.0, 1.0 / 2.2);
+    };
+    for (int64_t i = 0; i < nsamp; i++) has[(size_t)(samples[i].s + samples[i].t * w)] = 1;
+    for (int64_t i = 0; i < nsamp; i++) intensity(i);
+    const F3 n = {f.normal[0], f.normal[1], f.normal[2]};
+    auto w2l = [&](F3 p, float &s, float &t) {
+        F3 q = p - in.origin;
+        s = Dot(q, in.ws) - (float)in.mins;
+        t = Dot(q, in.wt) - (float)in.mint;
+    };
+    auto l2w = [&](float s, float t) {
+        float su = s + (float)in.mins, tv = t + (float)in.mint;
+        F3 pos = in.origin + in.ls * su;
+        return pos + in.lt * tv;
+    };
+    int64_t done = 0;
+    int pass = 1;
+    bool another = true;
+    std::vector<int64_t> selected;
+    for (;;) {
+        if (!another || pass > extra_passes) break;
+        // ComputeGradients, then the selection.
+        for (int64_t i = 0; i < nsamp; i++) {
+            if (processed[(size_t)i]) continue;
+            float g = 0.0f;
+            const int j = samples[i].s + samples[i].t * w;
+            const float cv = inten[(size_t)j];
+            auto step = [&](int idx) {
+                if (!has[(size_t)idx]) return;
+                float d = std::fabs(cv - inten[(size_t)idx]);
+                g = g > d ? g : d;
+            };
+            const int S = samples[i].s, T = samples[i].t;
+            if (T > 0) {
+                if (S > 0) step(j - 1 - w);
+                step(j - w);
+                if (S < w - 1) step(j + 1 - w);
+            }
+            if (T < h - 1) {
+                if (S > 0) step(j - 1 + w);
+                step(j + w);
+                if (S < w - 1) step(j + 1 + w);
+            }
+            if (S > 0) step(j - 1);
+            if (S < w - 1) step(j + 1);
+            grad[(size_t)i] = g;
+        }
+        selected.clear();
+        for (int64_t i = 0; i < nsamp; i++) {
+            if (processed[(size_t)i]) continue;
+            if (grad[(size_t)i] < 0.0625f) continue;
+            processed[(size_t)i] = 1;
+            selected.push_back(i);
+        }
+        another = !selected.empty();
+        if (!another) break;
+        for (int64_t i : selected) {
+            const orc_sample &sm = samples[i];
+            float os, ot;
+            w2l(F3{sm.position[0], sm.position[1], sm.position[2]}, os, ot);
+            const W &wd = wind[(size_t)i];
+            float amb[4] = {0, 0, 0, 0}, dir[4] = {0, 0, 0, 0};
+            int ac = 0, dc = 0;
+            for (int pt = 0; pt < 2; pt++) {
+                const bool ambientOnly = pt == 0;
+                const float width = ambientOnly ? 2.0f : 4.0f;
+                const float cscale = 1.0f / width;
+                const float csshift = (float)(-((width - 1) * cscale) / 2.0);
+                float aRow[4];
+                for (int k = 0; k < 4; k++) aRow[k] = csshift + (k * cscale);
+                const int rows = ambientOnly ? 1 : 4;
+                for (int r = 0; r < rows; r++) {
+                    F3 pos[4];
+                    for (int l = 0; l < 4; l++) {
+                        float cs, ct;
+                        if (ambientOnly) {
+                            cs = os + (l < 2 ? csshift : csshift + cscale);
+                            ct = ot + ((l & 1) == 0 ? csshift : csshift + cscale);
+                        } else {
+                            cs = os + aRow[r];
+                            ct = ot + aRow[l];
+                        }
+                        pos[l] = l2w(cs, ct);
+                    }
+                    int bits = 0;
+                    if (!wd.empty() && !PointsInWinding(pos, wd, bits)) {
+                        if (ambientOnly) break;
+                        continue;
+                    }
+                    F3 pts[4];
+                    for (int l = 0; l < 4; l++) pts[l] = pos[l] + n;
+                    float res[4][4];
+                    Resample(c, pts, n, f.cluster, cl_off, cl_list, ambientOnly, res);
+                    float *acc = ambientOnly ? amb : dir;
+                    int &cnt = ambientOnly ? ac : dc;
+                    for (int l = 0; l < 4; l++) {
+                        if ((bits >> l) & 1) continue;
+                        acc[0] = acc[0] + res[l][0];
+                        acc[1] = acc[1] + res[l][1];
+                        acc[2] = acc[2] + res[l][2];
+                        acc[3] += res[l][3];
+                        cnt++;
+                    }
+                }
+            }
+            if (ac > 0 && dc > 0) {
+                float *v = light + 4 * i;
+                float wdir = 1.0f / dc, wamb = 1.0f / ac;
+                v[0] = 0.0f + wdir * dir[0];
+                v[1] = 0.0f + wdir * dir[1];
+                v[2] = 0.0f + wdir * dir[2];
+                v[3] = 0.0f + wdir * dir[3];
+                v[0] = v[0] + wamb * amb[0];
+                v[1] = v[1] + wamb * amb[1];
+                v[2] = v[2] + wamb * amb[2];
+                v[3] += wamb * amb[3];
+                intensity(i);
+            }
+        }
+        done += (int64_t)selected.size();
+        pass++;
+    }
+    return done;
+}
+
+}  // namespace
+
 extern "C" int orc_direct(const orc_kdnode *nodes, const int32_t *indices, const orc_tri *tris,
-                          const float *bounds6, const orc_face *faces, int32_t nfaces,
+                          const float *bounds6, const orc_face *faces, int32_t nfaces, const float *verts,
                           const orc_sample *samples, const int64_t *face_first, const orc_light *lights,
                           const int32_t *cl_off, const int32_t *cl_list, const float *dirs, int32_t ndirs,
-                          const float *jitter, int32_t sun_samples, float sun_extent, float *out,
-                          int32_t threads, int64_t *rays_out) {
-    std::atomic<int64_t> rays(0);
+                          const float *jitter, int32_t sun_samples, float sun_extent, int32_t extra_passes,
+                          float *out, int32_t threads, int64_t *rays_out, int64_t *supersampled_out) {
+    std::atomic<int64_t> rays(0), supersampled(0);
+    std::atomic<bool> mismatch(false);
     Ctx c;
     c.kd = OrcKd{nodes, indices, tris, {bounds6[0], bounds6[1], bounds6[2], bounds6[3], bounds6[4], bounds6[5]}};
     c.lights = lights;
@@ -449,6 +669,25 @@ extern "C" int orc_direct(const orc_kdnode *nodes, const int32_t *indices, const
                 }
                 for (int l = 0; l < count; l++) std::memcpy(out + 4 * (g + l), acc[l], 16);
             }
+            if (extra_passes > 0 && b > a) {
+                // The face's own samples and their windings (the caller's
+                // samples must be the builder's: checked, not assumed).
+                std::vector<orc_sample> mine;
+                std::vector<W> wind;
+                face_samples(faces[fi], fi, verts, mine, &wind);
+                bool same = (int64_t)mine.size() == b - a;
+                for (int64_t k = 0; same && k < b - a; k++) {
+                    orc_sample x = mine[(size_t)k];
+                    x.face = samples[a + k].face;
+                    same = std::memcmp(&x, &samples[a + k], sizeof x) == 0;
+                }
+                if (!same) {
+                    mismatch = true;
+                    continue;
+                }
+                supersampled += Supersample(c, faces[fi], samples + a, b - a, wind, cl_off, cl_list, extra_passes,
+                                            out + 4 * a);
+            }
         }
         rays += t_rays;
     };
@@ -469,5 +708,6 @@ extern "C" int orc_direct(const orc_kdnode *nodes, const int32_t *indices, const
         for (auto &th : pool) th.join();
     }
     if (rays_out) *rays_out = rays.load();
-    return 0;
+    if (supersampled_out) *supersampled_out = supersampled.load();
+    return mismatch ? -2 : 0;
 }

@@ -59,7 +59,7 @@ def lib() -> ctypes.CDLL:
             getattr(_lib, name).restype = ctypes.c_int
         _lib.orc_build_samples.argtypes = [P, i32, P, P, ctypes.c_int64, P, P]
         _lib.orc_build_samples.restype = ctypes.c_int
-        _lib.orc_direct.argtypes = [P, P, P, P, P, i32, P, P, P, P, P, P, i32, P, i32, f32, P, i32, P]
+        _lib.orc_direct.argtypes = [P, P, P, P, P, i32, P, P, P, P, P, P, P, i32, P, i32, f32, i32, P, i32, P, P]
         _lib.orc_direct.restype = ctypes.c_int
         _lib.orc_neighbours.argtypes = [P, i32, P, f32, P, P, ctypes.c_int64, P]
         _lib.orc_neighbours.restype = ctypes.c_int
@@ -208,9 +208,12 @@ def build_samples(faces: np.ndarray, verts: np.ndarray):
 
 def direct(tree: dict, faces, samples, face_first, lights, cl_off, cl_list, dirs,
            jitter=None, sun_samples: int = 1, sun_extent: float = 0.0,
-           threads: int | None = None, count_rays: bool = False):
+           threads: int | None = None, count_rays: bool = False, verts=None, extra_passes: int = 4,
+           stats: dict | None = None):
     """The direct gather restated; (nsamples, 4) float32: lighting xyz, sun
-    (and the number of segments traced, with count_rays)."""
+    (and the number of segments traced, with count_rays).  With verts, up to
+    extra_passes supersampling passes follow (the reference's default is 4);
+    without verts, none."""
     nodes = np.ascontiguousarray(tree["nodes"], dtype=NODE_DTYPE)
     idx = np.ascontiguousarray(tree["indices"], dtype=np.int32)
     tris = np.ascontiguousarray(tree["tris"], dtype=TRI_DTYPE)
@@ -222,16 +225,22 @@ def direct(tree: dict, faces, samples, face_first, lights, cl_off, cl_list, dirs
     cl_off = np.ascontiguousarray(cl_off, np.int32)
     cl_list = np.ascontiguousarray(cl_list, np.int32)
     dirs = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
-    jit = np.ascontiguousarray(jitter if jitter is not None else np.zeros((1, 3)), np.float32)
+    jit = np.ascontiguousarray(jitter if jitter is not None and len(jitter) else np.zeros((1, 3)), np.float32)
+    vv = None if verts is None else np.ascontiguousarray(verts, np.float32)
     n = int(face_first[-1])
     out = np.zeros((n, 4), np.float32)
     rays = ctypes.c_int64()
-    rc = lib().orc_direct(_p(nodes), _p(idx), _p(tris), _p(bounds), _p(faces), len(faces), _p(samples),
+    ss = ctypes.c_int64()
+    rc = lib().orc_direct(_p(nodes), _p(idx), _p(tris), _p(bounds), _p(faces), len(faces), _p(vv), _p(samples),
                           _p(face_first), _p(lights), _p(cl_off), _p(cl_list), _p(dirs), len(dirs),
-                          _p(jit), sun_samples, sun_extent, _p(out),
-                          threads if threads is not None else default_threads(), ctypes.byref(rays))
+                          _p(jit), sun_samples, sun_extent, extra_passes if vv is not None else 0, _p(out),
+                          threads if threads is not None else default_threads(), ctypes.byref(rays),
+                          ctypes.byref(ss))
     if rc != 0:
         raise RuntimeError(f"orc_direct failed: {rc}")
+    if stats is not None:
+        stats["rays"] = rays.value
+        stats["supersampled"] = ss.value
     return (out, rays.value) if count_rays else out
 
 

@@ -141,13 +141,15 @@ int orc_build_samples(const orc_face *faces, int32_t nfaces, const float *verts,
                       int64_t capacity, int64_t *count, int64_t *first);
 
 /* The direct gather (style 0, flat faces) over every sample, in four-sample
- * groups per face; out is 4 floats per sample (lighting xyz, sun amount). */
+ * groups per face, then up to extra_passes supersampling passes per face
+ * (the samples must be the builder's own for the faces and verts given:
+ * -2 otherwise); out is 4 floats per sample (lighting xyz, sun amount). */
 int orc_direct(const orc_kdnode *nodes, const int32_t *indices, const orc_tri *tris,
-               const float *bounds6, const orc_face *faces, int32_t nfaces,
+               const float *bounds6, const orc_face *faces, int32_t nfaces, const float *verts,
                const orc_sample *samples, const int64_t *face_first, const orc_light *lights,
                const int32_t *cl_off, const int32_t *cl_list, const float *dirs, int32_t ndirs,
-               const float *jitter, int32_t sun_samples, float sun_extent, float *out,
-               int32_t threads, int64_t *rays_out);
+               const float *jitter, int32_t sun_samples, float sun_extent, int32_t extra_passes,
+               float *out, int32_t threads, int64_t *rays_out, int64_t *supersampled_out);
 
 /* FaceNeighbours.Build for smoothing groups 0 (vertices welded by position). */
 int orc_neighbours(const orc_face *faces, int32_t nfaces, const float *verts, float threshold,

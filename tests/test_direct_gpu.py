@@ -18,7 +18,7 @@ def oracle_direct(O, world, inp, faces=None):
     if faces is None:
         return O.direct(tree, inp.faces, inp.samples, inp.face_first, inp.lights, inp.cluster_offsets,
                         inp.cluster_lights, inp.sky_directions, inp.sun_jitter, inp.sun_samples,
-                        inp.sun_angular_extent)
+                        inp.sun_angular_extent, verts=inp.verts)
     # A subset of faces: their samples, renumbered.
     sel = np.asarray(faces)
     ff = inp.face_first
@@ -29,7 +29,7 @@ def oracle_direct(O, world, inp, faces=None):
     samples["face"] = np.repeat(np.arange(len(sel)), counts)
     out = O.direct(tree, inp.faces[sel], samples, first, inp.lights, inp.cluster_offsets,
                    inp.cluster_lights, inp.sky_directions, inp.sun_jitter, inp.sun_samples,
-                   inp.sun_angular_extent)
+                   inp.sun_angular_extent, verts=inp.verts)
     index = np.concatenate([np.arange(ff[f], ff[f + 1]) for f in sel])
     return out, index
 
@@ -95,3 +95,30 @@ def test_device_output_matches_host_output():
         torch.cuda.synchronize()
     assert np.array_equal(d.cpu().numpy().view(np.uint32),
                           np.ascontiguousarray(host).view(np.uint32).reshape(-1))
+
+
+def test_3x3_supersampling_counts_and_noextra(oracle_mod):
+    # The supersampling passes select the same samples as the oracle's
+    # (their count), change their light, and -noextra (0 passes) is the
+    # plain four-sample-group gather bit for bit.
+    w = rg.generate(rg.config_3x3(seed=2))
+    inp = L.prepare(w)
+    tree = oracle_mod.kd_build(w.tri_verts, w.tri_ids)
+    args = (tree, inp.faces, inp.samples, inp.face_first, inp.lights, inp.cluster_offsets, inp.cluster_lights,
+            inp.sky_directions, inp.sun_jitter, inp.sun_samples, inp.sun_angular_extent)
+    with L.LightingStage(w, inp) as st:
+        ss, ss_stats = st.direct()
+        st.set_extra_passes(0)
+        plain, plain_stats = st.direct()
+    o_stats = {}
+    want_ss = oracle_mod.direct(*args, verts=inp.verts, extra_passes=4, stats=o_stats)
+    want_plain = oracle_mod.direct(*args, verts=inp.verts, extra_passes=0)
+    g_ss = np.concatenate([ss["lighting"], ss["direct_sun_amount"][:, None]], 1)
+    g_plain = np.concatenate([plain["lighting"], plain["direct_sun_amount"][:, None]], 1)
+    assert np.array_equal(bits(g_plain), bits(want_plain))
+    assert np.array_equal(bits(g_ss), bits(want_ss))
+    assert ss_stats.supersampled == o_stats["supersampled"] > 100
+    assert plain_stats.supersampled == 0 and ss_stats.extra_passes_run >= 1
+    changed = (bits(g_ss) != bits(g_plain)).any(1)
+    assert changed.sum() > 0.5 * ss_stats.supersampled
+    assert ss_stats.visibility_rays + ss_stats.sky_rays > plain_stats.visibility_rays + plain_stats.sky_rays

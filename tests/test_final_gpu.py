@@ -17,7 +17,7 @@ def test_3x3_lighting_lump_byte_identical(oracle_mod):
         lump, lightofs, stats = st.light_pass()
     tree = oracle_mod.kd_build(w.tri_verts, w.tri_ids)
     light = oracle_mod.direct(tree, inp.faces, inp.samples, inp.face_first, inp.lights, inp.cluster_offsets,
-                              inp.cluster_lights, inp.sky_directions)
+                              inp.cluster_lights, inp.sky_directions, verts=inp.verts)
     want, want_ofs = oracle_mod.final(inp.faces, inp.verts, inp.samples, inp.face_first, light)
     assert np.array_equal(lightofs, want_ofs)
     assert len(lump) == len(want) == stats.lighting_bytes
