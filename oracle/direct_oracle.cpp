@@ -711,3 +711,6 @@ extern "C" int orc_direct(const orc_kdnode *nodes, const int32_t *indices, const
     if (supersampled_out) *supersampled_out = supersampled.load();
     return mismatch ? -2 : 0;
 }
+
+// DetMathF.Pow as the oracle computes it (the spotlight cone's power).
+extern "C" float orc_powf(float x, float y) { return PowF(x, y); }

@@ -323,6 +323,14 @@ def _bounce_lib():
     return L
 
 
+def powf(x: float, y: float) -> float:
+    """DetMathF.Pow as the oracle computes it."""
+    L = lib()
+    L.orc_powf.argtypes = [ctypes.c_float, ctypes.c_float]
+    L.orc_powf.restype = ctypes.c_float
+    return L.orc_powf(float(x), float(y))
+
+
 def asin(x: float) -> float:
     """DetMathF.Asin as the oracle computes it."""
     return _bounce_lib().orc_asin(float(x))

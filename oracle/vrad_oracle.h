@@ -241,6 +241,8 @@ int64_t orc_bounce_stats(void *h, int64_t *blocked);
 void orc_bounce_forget_transfers(void *h);
 /* Every receiver's candidate pairs, counted without tracing. */
 int64_t orc_bounce_count_candidates(void *h);
+/* DetMathF.Pow as the oracle computes it. */
+float orc_powf(float x, float y);
 /* DetMathF.Asin as the oracle computes it. */
 float orc_asin(float x);
 

@@ -69,6 +69,14 @@ def test_oracle_asin_matches_detmath_goldens(oracle_mod):
     assert len(bad) == 0, [(hex(a[i]), hex(got.view(np.uint32)[i]), hex(e[i])) for i in bad[:5]]
 
 
+def test_oracle_pow_matches_detmath_goldens(oracle_mod):
+    a, b, e = fixtures.detmath("Pow")
+    assert len(a) > 100
+    got = np.array([oracle_mod.powf(x, y) for x, y in zip(a.view(np.float32), b.view(np.float32))], np.float32)
+    bad = np.flatnonzero(got.view(np.uint32) != e)
+    assert len(bad) == 0, [(hex(a[i]), hex(b[i]), hex(got.view(np.uint32)[i]), hex(e[i])) for i in bad[:5]]
+
+
 def test_pvs_lists_are_rows_of_the_pvs():
     w, _ = _world(rg.config_3x3(seed=2))
     off, lst = L.pvs_lists(w)
