@@ -489,8 +489,9 @@ __global__ void __launch_bounds__(kExactThreads) k_exact_total(const int32_t *__
                                                                const float4 *__restrict__ emit, float *__restrict__ out) {
     __shared__ float3 tile[2][kExactTile];
     float x = 0.0f, y = 0.0f, z = 0.0f;
-    auto stage = [&](int buf, int base) {
-        for (int k = threadIdx.x; k < kExactTile; k += kExactThreads) {
+    // Stages tile `buf` with threads [first, kExactThreads).
+    auto stage = [&](int buf, int base, int first) {
+        for (int k = (int)threadIdx.x - first; k < kExactTile; k += kExactThreads - first) {
             const int i = base + k;
             float3 v = make_float3(0.0f, 0.0f, 0.0f);
             if (i < n) {
@@ -500,11 +501,11 @@ __global__ void __launch_bounds__(kExactThreads) k_exact_total(const int32_t *__
             tile[buf][k] = v;
         }
     };
-    stage(0, 0);
+    stage(0, 0, 0);
     __syncthreads();
     for (int base = 0, buf = 0; base < n; base += kExactTile, buf ^= 1) {
         if (threadIdx.x >= 32) {
-            stage(buf ^ 1, base + kExactTile);
+            stage(buf ^ 1, base + kExactTile, 32);
         } else {
             const int m = min(kExactTile, n - base);
             for (int k = 0; k < m; k++) {

@@ -455,3 +455,17 @@ extern "C" int32_t vrad_bounce_transfers(vrad_ctx *ctx, int64_t *offsets, int64_
         }
     return VRAD_OK;
 }
+
+extern "C" int32_t vrad_bounce_last_total(vrad_ctx *ctx, float *total) {
+    if (!ctx || !total) return vrad_fail(ctx, VRAD_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    vrad::BounceBuffers &b = ctx->bounce;
+    if (!b.ready || b.bounces_run == 0) return vrad_fail(ctx, VRAD_ERR_ARG, "no bounce has run");
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess) e = vrad::launch_exact_total(b, b.bounces_run - 1, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_exact, b.exact, 3 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "bounce total");
+    for (int c = 0; c < 3; c++) total[c] = b.h_exact[c];
+    return VRAD_OK;
+}

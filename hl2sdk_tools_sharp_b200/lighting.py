@@ -135,6 +135,8 @@ def _lib():
         lib.vrad_bounce_stats_get.restype = i32
         lib.vrad_bounce_patch_light.argtypes = [P, P, P, i64]
         lib.vrad_bounce_patch_light.restype = i32
+        lib.vrad_bounce_last_total.argtypes = [P, P]
+        lib.vrad_bounce_last_total.restype = i32
         lib.vrad_bounce_transfers.argtypes = [P, P, i64, P, i64, ctypes.POINTER(i64)]
         lib.vrad_bounce_transfers.restype = i32
         lib._lighting_bound = True
@@ -429,6 +431,12 @@ class LightingStage:
         direct = np.zeros((n, 3), np.float32)
         T._check(_lib().vrad_bounce_patch_light(self._ctx, total.ctypes.data, direct.ctypes.data, n), self._ctx)
         return total, direct
+
+    def last_total(self) -> np.ndarray:
+        """After a light pass: CollectLight's float total of the last bounce."""
+        out = np.zeros(3, np.float32)
+        T._check(_lib().vrad_bounce_last_total(self._ctx, out.ctypes.data), self._ctx)
+        return out
 
     def transfers(self):
         """After a light pass: (offsets by patch (P + 1), TRANSFER_DTYPE records)."""

@@ -438,6 +438,11 @@ int32_t vrad_bounce_stats_get(vrad_ctx *ctx, vrad_bounce_stats *stats);
  * direct light (DirectLight), npatches x 3 each; either may be NULL. */
 int32_t vrad_bounce_patch_light(vrad_ctx *ctx, float *total_light, float *direct_light, int64_t npatches);
 
+/* After a light pass: the light the last bounce added, summed as
+ * Radiosity.CollectLight sums it (float, descending patch index; the
+ * value its stop rule compares), xyz. */
+int32_t vrad_bounce_last_total(vrad_ctx *ctx, float *total);
+
 /* Transfer (MapTools/Rad/Bounce/TransferSet.cs:26): source patch, weight. */
 typedef struct vrad_transfer {
     int32_t patch;

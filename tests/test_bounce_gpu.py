@@ -65,6 +65,7 @@ def test_3x3_bounce_bit_exact(oracle_mod, threshold):
         bs = st.bounce_stats()
         total, direct = st.patch_light()
         off, tr = st.transfers()
+        last = st.last_total()
         light = _sample_light(st)
     ob = _oracle(oracle_mod, w, inp, threshold=threshold)
     o_off, o_src, o_w, rays = ob.transfers()
@@ -75,6 +76,7 @@ def test_3x3_bounce_bit_exact(oracle_mod, threshold):
     o_total, o_direct, o_bounces, o_added = ob.run(light)
     assert np.array_equal(_bits(direct), _bits(o_direct))
     assert bs.bounces == o_bounces and bs.bounces > 1
+    assert np.array_equal(_bits(last), _bits(o_added))
     assert np.array_equal(_bits(total), _bits(o_total))
     want, want_ofs = ob.final(light)
     assert np.array_equal(lightofs, want_ofs)
@@ -91,6 +93,7 @@ def test_8x8_transfers_sampled_and_bounce_bit_exact(oracle_mod):
         bs = st.bounce_stats()
         total, direct = st.patch_light()
         off, tr = st.transfers()
+        last = st.last_total()
         light = _sample_light(st)
     ob = _oracle(oracle_mod, w, inp)
     patches, _ = ob.patches()
@@ -105,10 +108,13 @@ def test_8x8_transfers_sampled_and_bounce_bit_exact(oracle_mod):
         assert np.array_equal(_bits(tr["weight"][a:b]), _bits(o_w[c:d])), p
     # The bounce itself over the device's transfers.
     ob.set_transfers(off, tr["patch"], tr["weight"])
-    o_total, o_direct, o_bounces, _ = ob.run(light)
+    o_total, o_direct, o_bounces, o_added = ob.run(light)
     assert np.array_equal(_bits(direct), _bits(o_direct))
     assert bs.bounces == o_bounces
     assert np.array_equal(_bits(total), _bits(o_total))
+    # CollectLight's sequential float total over the million leaves, as the
+    # device's exact-sum kernel computes it when the fp64 bound is unsure.
+    assert np.array_equal(_bits(last), _bits(o_added))
     want, want_ofs = ob.final(light)
     bad = np.flatnonzero(lump.view(np.uint32) != want.view(np.uint32))
     assert len(bad) == 0, f"{len(bad)} of {len(lump) // 4} RGBE words differ"
