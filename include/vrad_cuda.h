@@ -455,6 +455,49 @@ typedef struct vrad_transfer {
 int32_t vrad_bounce_transfers(vrad_ctx *ctx, int64_t *offsets, int64_t npatches, vrad_transfer *transfers,
                               int64_t capacity, int64_t *count);
 
+/* ---- Learned warm start ---------------------------------------------------
+ *
+ * A small network (32 -> 128 -> 128 -> 3, ReLU, BF16 weights and
+ * activations, FP32 accumulation) that predicts a patch's converged bounced
+ * light from per-patch features; the bounce can start from its guess
+ * (vrad_bounce_set_model).  No counterpart in the reference: its bounce
+ * always starts from zero, and that plain bounce stays the default here.
+ * Training and inference run on the context's device, on tensor cores.
+ * A network is not safe to use from two threads at once. */
+
+#define VRAD_MLP_INPUTS 32
+#define VRAD_MLP_HIDDEN 128
+#define VRAD_MLP_OUTPUTS 3
+/* Parameters in order: w1 [32][128], b1 [128], w2 [128][128], b2 [128],
+ * w3 [128][3], b3 [3]; w[k][n] maps input k to output n. */
+#define VRAD_MLP_PARAMS (32 * 128 + 128 + 128 * 128 + 128 + 128 * 3 + 3)
+
+typedef struct vrad_mlp vrad_mlp;
+
+/* A new network on ctx's device, He-initialised from `seed`. */
+int32_t vrad_mlp_create(vrad_ctx *ctx, uint64_t seed, vrad_mlp **out);
+int32_t vrad_mlp_destroy(vrad_mlp *m);
+
+/* Reads (get) and/or replaces (set) the FP32 parameters, host arrays of
+ * VRAD_MLP_PARAMS floats. */
+int32_t vrad_mlp_params(vrad_mlp *m, float *get, const float *set);
+
+/* y[n][3] = the network on x[n][32] (BF16 bit patterns), device buffers,
+ * on `stream` (NULL = default stream). */
+int32_t vrad_mlp_forward_device(vrad_mlp *m, const uint16_t *x, int64_t n, float *y, void *stream);
+
+/* The gradient of the mean squared error against target[n][3] (device
+ * buffers): grad (host, VRAD_MLP_PARAMS floats, nullable) and the loss
+ * (host, nullable).  Blocks. */
+int32_t vrad_mlp_gradient_device(vrad_mlp *m, const uint16_t *x, const float *target, int64_t n, float *grad,
+                                 float *loss, void *stream);
+
+/* One Adam step (beta1 0.9, beta2 0.999) on that gradient, learning rate
+ * lr, on `stream`; vrad_mlp_loss reads the step's loss. */
+int32_t vrad_mlp_train_step_device(vrad_mlp *m, const uint16_t *x, const float *target, int64_t n, float lr,
+                                   void *stream);
+int32_t vrad_mlp_loss(vrad_mlp *m, float *loss);
+
 /* Largest batch vrad_trace_visibility_static accepts: four of the
  * reference's 16,384-ray batches. */
 #define VRAD_STATIC_MAX_RAYS 65536

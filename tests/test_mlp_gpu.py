@@ -1,0 +1,72 @@
+"""The learned warm start's network: the library's tensor-core forward and
+backward kernels against the numpy oracle (which mirrors the device's BF16
+roundings; the tolerance covers FP32 summation order), and training."""
+import numpy as np
+import pytest
+
+from hl2sdk_tools_sharp_b200 import learned as LN, tracer as T
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def net():
+    import torch
+    tr = T.CudaRayTracer(T.make_triangles(np.zeros((1, 9), np.float32), np.zeros(1, np.int32)))
+    n = LN.Network(tr, seed=3)
+    yield n, torch
+    n.close()
+    tr.close()
+
+
+def _data(torch, n, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(size=(n, LN.INPUTS)).astype(np.float32)
+    xt = torch.from_numpy(x).to("cuda").to(torch.bfloat16).contiguous()
+    bits = xt.cpu().view(torch.int16).numpy().view(np.uint16)
+    t = rng.normal(size=(n, LN.OUTPUTS)).astype(np.float32)
+    return xt, bits, torch.from_numpy(t).cuda(), t
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def test_forward_matches_oracle(net):
+    from oracle import mlp_oracle as MO
+    n, torch = net
+    xt, bits, _, _ = _data(torch, 1000, 1)       # not a multiple of the 128-row tile
+    y = n.forward(xt).cpu().numpy()
+    want, _, _ = MO.forward(n.params(), bits)
+    assert _rel(y, want) < 2e-3
+
+
+def test_gradient_matches_oracle(net):
+    from oracle import mlp_oracle as MO
+    n, torch = net
+    xt, bits, tt, t = _data(torch, 777, 2)
+    g, loss = n.gradient(xt, tt)
+    want, want_loss = MO.gradient(n.params(), bits, t)
+    assert abs(loss - want_loss) < 1e-3 * want_loss
+    gs, ws = LN.split(g), LN.split(want.astype(np.float32))
+    for name in ("w1", "b1", "w2", "b2", "w3", "b3"):
+        assert _rel(gs[name], ws[name]) < 1e-2, name
+    # Two calls give the same gradient but for the atomics' order.
+    g2, _ = n.gradient(xt, tt)
+    assert _rel(g2, g) < 1e-5
+
+
+def test_training_fits_a_function(net):
+    import torch
+    n, _ = net
+    rng = np.random.default_rng(5)
+    x = rng.uniform(-1, 1, size=(20000, LN.INPUTS)).astype(np.float32)
+    t = np.stack([np.sin(2 * x[:, 0]) + x[:, 1] * x[:, 2], np.abs(x[:, 3]) - 0.5, x[:, 4] ** 2], 1).astype(np.float32)
+    xt = torch.from_numpy(x).cuda().to(torch.bfloat16).contiguous()
+    tt = torch.from_numpy(t).cuda()
+    _, first = n.gradient(xt, tt)
+    for step in range(400):
+        n.train_step(xt, tt, 3e-3)
+    torch.cuda.synchronize()
+    last = n.loss()
+    assert last < first / 10, (first, last)
