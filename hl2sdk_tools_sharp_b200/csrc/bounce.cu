@@ -43,6 +43,7 @@
 //   k_exact_total     one block: the reference's sequential float sum, run
 //                     only when the bound cannot settle the stop rule
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cub/device/device_scan.cuh>
@@ -57,6 +58,7 @@
 #include "bounce.cuh"
 #include "context.cuh"
 #include "detmath.cuh"
+#include "mlp.cuh"
 #include "patches.h"
 #include "traverse.cuh"
 #include "world.h"
@@ -524,6 +526,113 @@ __global__ void __launch_bounds__(kExactThreads) k_exact_total(const int32_t *__
     }
 }
 
+// ---- the learned warm start --------------------------------------------------
+
+// Per receiver, the network's 32 inputs (BF16): the shading normal, log2 of
+// the area over 16, the reflectivity, log1p of the direct and of the
+// first-bounce light over 8, log2(1 + d) over 16 of the distances d to the
+// eight nearest point and spot lights (1 when there are fewer), zeros.
+__global__ void k_features(BounceView v, const float4 *__restrict__ direct, const float4 *__restrict__ first,
+                           const float4 *__restrict__ lights, int32_t nlights, uint16_t *__restrict__ x) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= v.nreceivers) return;
+    const int p = __ldg(&v.recv[r]);
+    const float4 o = __ldg(&v.origin[p]), nrm = __ldg(&v.normal[p]), rf = __ldg(&v.refl[p]);
+    const float4 d = direct[p], b1 = first[p];
+    float f[kFeatures];
+    f[0] = nrm.x, f[1] = nrm.y, f[2] = nrm.z;
+    f[3] = log2f(fmaxf(o.w, 1e-6f)) / 16.0f;
+    f[4] = rf.x, f[5] = rf.y, f[6] = rf.z;
+    f[7] = log1pf(fmaxf(d.x, 0.0f)) / 8.0f, f[8] = log1pf(fmaxf(d.y, 0.0f)) / 8.0f, f[9] = log1pf(fmaxf(d.z, 0.0f)) / 8.0f;
+    f[10] = log1pf(fmaxf(b1.x, 0.0f)) / 8.0f, f[11] = log1pf(fmaxf(b1.y, 0.0f)) / 8.0f;
+    f[12] = log1pf(fmaxf(b1.z, 0.0f)) / 8.0f;
+    float best[8];
+    for (int k = 0; k < 8; k++) best[k] = INFINITY;
+    for (int l = 0; l < nlights; l++) {
+        const float4 a = __ldg(&lights[5 * l]);
+        const int type = __float_as_int(a.w);
+        if (type != 1 && type != 2) continue;
+        const float dx = a.x - o.x, dy = a.y - o.y, dz = a.z - o.z;
+        float q = dx * dx + dy * dy + dz * dz;
+        for (int k = 0; k < 8; k++) {
+            if (q < best[k]) {
+                const float tmp = best[k];
+                best[k] = q;
+                q = tmp;
+            }
+        }
+    }
+    for (int k = 0; k < 8; k++) f[13 + k] = isinf(best[k]) ? 1.0f : log2f(1.0f + sqrtf(best[k])) / 16.0f;
+    for (int k = 21; k < kFeatures; k++) f[k] = 0.0f;
+    for (int k = 0; k < kFeatures; k++) x[(int64_t)r * kFeatures + k] = __bfloat16_as_ushort(__float2bfloat16_rn(f[k]));
+}
+
+// The network's guess as light per patch: expm1 of its output, at least
+// zero, on the non-sky receivers (everything else zero).
+__global__ void k_guess(BounceView v, const float *__restrict__ y, float4 *__restrict__ guess) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= v.nreceivers) return;
+    const int p = __ldg(&v.recv[r]);
+    float4 gv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (!__ldg(&v.tree[p].w)) {
+        gv.x = fmaxf(expm1f(y[3 * (int64_t)r]), 0.0f);
+        gv.y = fmaxf(expm1f(y[3 * (int64_t)r + 1]), 0.0f);
+        gv.z = fmaxf(expm1f(y[3 * (int64_t)r + 2]), 0.0f);
+    }
+    guess[p] = gv;
+}
+
+// A per-patch quantity of the parents as the area blend of their children,
+// bottom up within each face (as CollectLight blends the light).
+__global__ void k_blend(BounceView v, float4 *__restrict__ a) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= v.nfaces) return;
+    const int4 fr = __ldg(&v.face_range[f]);
+    const FaceList L{fr.x, fr.y, fr.z};
+    for (int k = 0; k < L.count(); k++) {
+        const int p = L.at(k);
+        const int4 tr = __ldg(&v.tree[p]);
+        if (tr.y == -1) continue;
+        const float a1 = __ldg(&v.origin[tr.y].w), a2 = __ldg(&v.origin[tr.z].w);
+        const float s1 = a1 / (a1 + a2), s2 = a2 / (a1 + a2);
+        const float4 c1 = a[tr.y], c2 = a[tr.z];
+        a[p] = make_float4(c1.x * s1 + c2.x * s2, c1.y * s1 + c2.y * s2, c1.z * s1 + c2.z * s2, 0.0f);
+    }
+}
+
+// The first warm step for each receiver: A = the transfers' gather of the
+// guess's shot light, then light = B1 + A (the Jacobi step from the guess),
+// emission = light - guess (the change, which later bounces carry on).
+__global__ void k_warm_combine(BounceView v, const int64_t *__restrict__ tr_off, const int2 *__restrict__ tr,
+                               const float4 *__restrict__ guess, const float4 *__restrict__ first,
+                               float4 *__restrict__ total, float4 *__restrict__ emit_out, float4 *__restrict__ shoot_out) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= v.nreceivers) return;
+    const int p = __ldg(&v.recv[r]);
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    const int64_t a = __ldg(&tr_off[r]), b = __ldg(&tr_off[r + 1]);
+    for (int64_t j = a; j < b; j++) {
+        const int2 t = __ldg(&tr[j]);
+        const float w = __int_as_float(t.y);
+        const float4 gs = guess[t.x], rf = __ldg(&v.refl[t.x]);
+        sx += gs.x * rf.x * w;
+        sy += gs.y * rf.y * w;
+        sz += gs.z * rf.z * w;
+    }
+    if (__ldg(&v.tree[p].w)) {
+        emit_out[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        shoot_out[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        return;
+    }
+    const float4 b1 = first[p], gv = guess[p];
+    const float4 t = make_float4(b1.x + sx, b1.y + sy, b1.z + sz, 0.0f);
+    total[p] = t;
+    const float4 d = make_float4(t.x - gv.x, t.y - gv.y, t.z - gv.z, 0.0f);
+    emit_out[p] = d;
+    const float4 rf = __ldg(&v.refl[p]);
+    shoot_out[p] = make_float4(d.x * rf.x, d.y * rf.y, d.z * rf.z, 0.0f);
+}
+
 unsigned blocks(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
 
 }  // namespace
@@ -532,6 +641,7 @@ void BounceBuffers::release() {
     void *ptrs[] = {origin, normal, mins, maxs, refl, tree, wind, points, face_range, face_samples, face_plane,
                     recv, row_off, row_faces, sample_area, cand_off, cand_src, cand_w, tr_off, tr, scan_tmp,
                     acc, direct, total, emit[0], emit[1], shoot[0], shoot[1], sums, exact, counters, leaf_desc,
+                    first, guess, feat, pred,
                     pr_off, pr_patch, pr_box, pr_coord, prad_light, prad_weight};
     for (void *q : ptrs) cudaFree(q);
     cudaFreeHost(h_sums);
@@ -593,6 +703,35 @@ cudaError_t launch_gather(BounceBuffers &b, int bounce, cudaStream_t stream) {
     if (b.npatches)
         k_totals<<<blocks(b.npatches, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.emit[out], b.sums);
     b.last_buffer = out;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_features(BounceBuffers &b, const DeviceWorld &w, cudaStream_t stream) {
+    if (!b.nreceivers) return cudaSuccess;
+    k_features<<<blocks(b.nreceivers, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.direct, b.first, w.lights,
+                                                                                w.nlights, b.feat);
+    return cudaGetLastError();
+}
+
+// The warm start after bounce 0 (which left B1 in b.first): the guess from
+// the network, blended to the parents, the first warm step into the other
+// emit/shoot half, the parents' light and emission, and the totals.
+cudaError_t launch_warm_start(BounceBuffers &b, const DeviceWorld &w, const vrad_mlp &m, cudaStream_t stream) {
+    if (!b.nreceivers) return cudaSuccess;
+    cudaError_t e = launch_features(b, w, stream);
+    if (e == cudaSuccess) e = mlp_forward(m, b.feat, b.nreceivers, b.pred, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.guess, 0, sizeof(float4) * (size_t)b.npatches, stream);
+    if (e != cudaSuccess) return e;
+    k_guess<<<blocks(b.nreceivers, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.pred, b.guess);
+    k_blend<<<blocks(b.nfaces, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.guess);
+    // Bounce 0 wrote half 1; the warm step writes half 0, as bounce 1 would.
+    k_warm_combine<<<blocks(b.nreceivers, kBounceBlock), kBounceBlock, 0, stream>>>(
+        b.view, b.tr_off, b.tr, b.guess, b.first, b.total, b.emit[0], b.shoot[0]);
+    k_collect<<<blocks(b.nfaces, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.total, b.emit[0], b.shoot[0]);
+    e = cudaMemsetAsync(b.sums, 0, 6 * sizeof(double), stream);
+    if (e != cudaSuccess) return e;
+    k_totals<<<blocks(b.npatches, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.emit[0], b.sums);
+    b.last_buffer = 0;
     return cudaGetLastError();
 }
 

@@ -31,12 +31,16 @@
 #include <string>
 #include <vector>
 
+#include "direct.cuh"
 #include "scene.cuh"
 #include "vrad_internal.cuh"
+
+struct vrad_mlp;
 
 namespace vrad {
 
 constexpr int64_t kMaxTransfersPerReceiver = 4 * 65536;  // VisMatrix.MaxPatches
+constexpr int kFeatures = 32;                            // the warm start network's inputs
 
 struct BounceView {
     int32_t npatches, nfaces, nreceivers;
@@ -84,6 +88,12 @@ struct BounceBuffers {
     double *sums = nullptr;        // fp64 totals of a bounce: 3 sums, 3 absolute sums
     float *exact = nullptr;        // the sequential float total, when needed
     int32_t *leaf_desc = nullptr;  // the sky-free leaves, descending index (CollectLight's total order)
+    // Learned warm start.
+    float4 *first = nullptr;       // the first bounce's light per patch (bounce 0's total)
+    float4 *guess = nullptr;       // the network's guess per patch
+    uint16_t *feat = nullptr;      // R x 32 BF16 inputs
+    float *pred = nullptr;         // R x 3 outputs
+    const vrad_mlp *model = nullptr;
     unsigned long long *counters = nullptr;  // [0] transfer rays, [1] blocked, [2] asin ties left open
     double *h_sums = nullptr;      // pinned host copies
     float *h_exact = nullptr;
@@ -117,5 +127,7 @@ cudaError_t launch_transfers(BounceBuffers &b, const DeviceScene &scene, uint32_
                              bool count_only);
 cudaError_t launch_gather(BounceBuffers &b, int bounce, cudaStream_t stream);
 cudaError_t launch_exact_total(BounceBuffers &b, int bounce, cudaStream_t stream);
+cudaError_t launch_features(BounceBuffers &b, const DeviceWorld &w, cudaStream_t stream);
+cudaError_t launch_warm_start(BounceBuffers &b, const DeviceWorld &w, const vrad_mlp &m, cudaStream_t stream);
 
 }  // namespace vrad

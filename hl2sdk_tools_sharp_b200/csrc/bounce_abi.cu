@@ -123,12 +123,25 @@ cudaError_t run_bounce(vrad_ctx *ctx, cudaStream_t s, std::string &why) {
     const double u = std::ldexp(1.0, -24);
     const double nu = (double)b.nleaves * u;
     const double gamma = nu < 0.5 ? nu / (1.0 - nu) : INFINITY;
+    const vrad_mlp *model = ctx->bounce_model;
     for (int i = 0; e == cudaSuccess && i < b.max_bounces; i++) {
-        e = launch_gather(b, i, s);
+        // With a network attached, the second step starts from its guess
+        // (launch_warm_start) instead of bouncing the first bounce's light.
+        e = (model && i == 1) ? launch_warm_start(b, ctx->world.view, *model, s) : launch_gather(b, i, s);
+        if (e == cudaSuccess && i == 0)
+            e = cudaMemcpyAsync(b.first, b.total, sizeof(float4) * (size_t)b.npatches, cudaMemcpyDeviceToDevice, s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_sums, b.sums, 6 * sizeof(double), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) break;
         b.bounces_run = i + 1;
+        if (model) {
+            // The warm iteration's changes can be negative: it stops on the
+            // sum of their magnitudes.
+            for (int c = 0; c < 3; c++) b.added[c] = b.h_sums[3 + c];
+            if (b.added[0] < (double)b.threshold && b.added[1] < (double)b.threshold && b.added[2] < (double)b.threshold)
+                break;
+            continue;
+        }
         // Radiosity.BounceAsync's stop rule on CollectLight's float total:
         // settled by the fp64 total when the float sum's error bound keeps
         // it on one side of the threshold, else by the sequential sum.
@@ -326,6 +339,10 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     if (e == cudaSuccess) e = cudaMalloc(&b.counters, 3 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMallocHost(&b.h_sums, 6 * sizeof(double));
     if (e == cudaSuccess) e = cudaMallocHost(&b.h_exact, 3 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&b.first, sizeof(float4) * P1);
+    if (e == cudaSuccess) e = cudaMalloc(&b.guess, sizeof(float4) * P1);
+    if (e == cudaSuccess) e = cudaMalloc(&b.feat, sizeof(uint16_t) * kFeatures * (size_t)(R ? R : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&b.pred, sizeof(float) * 3 * (size_t)(R ? R : 1));
     if (e == cudaSuccess) e = cudaMalloc(&b.prad_light, sizeof(float4) * N1);
     if (e == cudaSuccess) e = cudaMalloc(&b.prad_weight, sizeof(float) * N1);
     if (e == cudaSuccess && R > 0) {
@@ -467,5 +484,47 @@ extern "C" int32_t vrad_bounce_last_total(vrad_ctx *ctx, float *total) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "bounce total");
     for (int c = 0; c < 3; c++) total[c] = b.h_exact[c];
+    return VRAD_OK;
+}
+
+namespace {
+
+__global__ void k_targets(vrad::BounceView v, const float4 *__restrict__ total, float *__restrict__ t) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= v.nreceivers) return;
+    const float4 x = total[__ldg(&v.recv[r])];
+    t[3 * (int64_t)r] = log1pf(fmaxf(x.x, 0.0f));
+    t[3 * (int64_t)r + 1] = log1pf(fmaxf(x.y, 0.0f));
+    t[3 * (int64_t)r + 2] = log1pf(fmaxf(x.z, 0.0f));
+}
+
+}  // namespace
+
+extern "C" int32_t vrad_bounce_set_model(vrad_ctx *ctx, const vrad_mlp *model) {
+    if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    ctx->bounce_model = model;
+    return VRAD_OK;
+}
+
+extern "C" int32_t vrad_bounce_features_device(vrad_ctx *ctx, uint16_t *x, float *target, int64_t capacity,
+                                               int64_t *count, void *stream) {
+    if (!ctx || !count) return vrad_fail(ctx, VRAD_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    vrad::BounceBuffers &b = ctx->bounce;
+    if (!b.ready || b.bounces_run == 0) return vrad_fail(ctx, VRAD_ERR_ARG, "no bounce has run");
+    *count = b.nreceivers;
+    if (!x && !target) return VRAD_OK;
+    if (capacity < b.nreceivers) return vrad_fail(ctx, VRAD_ERR_ARG, "%d receivers, room for %lld", b.nreceivers, (long long)capacity);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess && x) e = vrad::launch_features(b, ctx->world.view, s);
+    if (e == cudaSuccess && x)
+        e = cudaMemcpyAsync(x, b.feat, sizeof(uint16_t) * vrad::kFeatures * (size_t)b.nreceivers, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess && target && b.nreceivers) {
+        k_targets<<<(b.nreceivers + 127) / 128, 128, 0, s>>>(b.view, b.total, target);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "bounce features");
     return VRAD_OK;
 }

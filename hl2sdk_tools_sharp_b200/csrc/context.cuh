@@ -35,6 +35,7 @@ struct vrad_ctx {
     std::vector<vrad_sample> h_samples;
     int32_t nclusters = 0;
     vrad::BounceBuffers bounce;
+    const vrad_mlp *bounce_model = nullptr;  // the warm start's network, or none
     vrad::SupersampleBuffers supersample;
     std::string supersample_why;     // why the world's samples cannot be supersampled
     std::string last_error;

@@ -112,3 +112,59 @@ class Network:
         v = np.zeros(1, np.float32)
         T._check(_lib().vrad_mlp_loss(self._h, v.ctypes.data), None)
         return float(v[0])
+
+
+def training_config(k: int, seed0: int = 100):
+    """The k-th training map: an 8x8-style room grid (pillars, point and
+    spot lights, sun and sky) of 2 to 6 rooms a side, one light per room."""
+    import dataclasses
+    from . import roomgrid as rg
+    side = 2 + k % 5
+    return dataclasses.replace(rg.config_8x8(seed0 + k), side=side, lights=side * side)
+
+
+def collect(configs, threshold: float = 0.1, bounces: int = 100):
+    """Plain light passes over the maps: the receivers' features and the
+    log1p of their converged bounced light, concatenated (CUDA tensors)."""
+    import torch
+    from . import lighting as L, roomgrid as rg
+    xs, ts = [], []
+    for cfg in configs:
+        w = rg.generate(cfg)
+        with L.LightingStage(w) as st:
+            off, lst = L.pvs_lists(w)
+            st.upload_bounce(L.face_reflectivity(w), off, lst, bounces=bounces, threshold=threshold)
+            st.light_pass()
+            x, t = st.bounce_features()
+            xs.append(x.clone())
+            ts.append(t.clone())
+    return torch.cat(xs), torch.cat(ts)
+
+
+def train(net: Network, x, t, steps: int = 3000, batch: int = 32768, lr: float = 2e-3, seed: int = 0,
+          log=None) -> float:
+    """Adam on random minibatches (the rate drops 4x for the last third);
+    returns the last step's loss."""
+    import torch
+    g = torch.Generator(device=x.device)
+    g.manual_seed(seed)
+    n = len(x)
+    for step in range(steps):
+        idx = torch.randint(0, n, (min(batch, n),), device=x.device, generator=g)
+        net.train_step(x[idx].contiguous(), t[idx].contiguous(), lr if step < 2 * steps // 3 else lr / 4)
+        if log is not None and step % 500 == 0:
+            log(step, net.loss())
+    return net.loss()
+
+
+def within_one_lsb(a: np.ndarray, b: np.ndarray) -> float:
+    """The fraction of RGBE words of two LIGHTING lumps whose three channels
+    differ by at most one unit of the larger word's last place."""
+    va = a.view(np.uint8).reshape(-1, 4).astype(np.int64)
+    vb = b.view(np.uint8).reshape(-1, 4).astype(np.int64)
+    ea = va[:, 3].astype(np.int8).astype(np.int64)
+    eb = vb[:, 3].astype(np.int8).astype(np.int64)
+    fa = va[:, :3] * np.exp2(ea)[:, None]
+    fb = vb[:, :3] * np.exp2(eb)[:, None]
+    lsb = np.exp2(np.maximum(ea, eb))[:, None]
+    return float((np.abs(fa - fb) <= lsb).all(1).mean())

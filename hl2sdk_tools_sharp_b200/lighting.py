@@ -135,6 +135,10 @@ def _lib():
         lib.vrad_bounce_stats_get.restype = i32
         lib.vrad_bounce_patch_light.argtypes = [P, P, P, i64]
         lib.vrad_bounce_patch_light.restype = i32
+        lib.vrad_bounce_set_model.argtypes = [P, P]
+        lib.vrad_bounce_set_model.restype = i32
+        lib.vrad_bounce_features_device.argtypes = [P, P, P, i64, ctypes.POINTER(i64), P]
+        lib.vrad_bounce_features_device.restype = i32
         lib.vrad_bounce_last_total.argtypes = [P, P]
         lib.vrad_bounce_last_total.restype = i32
         lib.vrad_bounce_transfers.argtypes = [P, P, i64, P, i64, ctypes.POINTER(i64)]
@@ -431,6 +435,25 @@ class LightingStage:
         direct = np.zeros((n, 3), np.float32)
         T._check(_lib().vrad_bounce_patch_light(self._ctx, total.ctypes.data, direct.ctypes.data, n), self._ctx)
         return total, direct
+
+    def set_bounce_model(self, net) -> None:
+        """vrad_bounce_set_model: later light passes start their bounce from
+        the network's guess (None: the plain bounce)."""
+        self._model = net
+        T._check(_lib().vrad_bounce_set_model(self._ctx, net.handle if net is not None else None), self._ctx)
+
+    def bounce_features(self):
+        """After a light pass: (x (R, 32) bfloat16, log1p of the converged
+        bounced light (R, 3) float32), CUDA tensors, per receiver."""
+        import torch
+        n = ctypes.c_int64()
+        T._check(_lib().vrad_bounce_features_device(self._ctx, None, None, 0, ctypes.byref(n), None), self._ctx)
+        x = torch.empty((n.value, 32), dtype=torch.bfloat16, device="cuda")
+        t = torch.empty((n.value, 3), dtype=torch.float32, device="cuda")
+        s = torch.cuda.current_stream().cuda_stream
+        T._check(_lib().vrad_bounce_features_device(self._ctx, x.data_ptr(), t.data_ptr(), n.value, ctypes.byref(n),
+                                                    ctypes.c_void_p(s)), self._ctx)
+        return x, t
 
     def last_total(self) -> np.ndarray:
         """After a light pass: CollectLight's float total of the last bounce."""

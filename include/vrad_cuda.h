@@ -498,6 +498,22 @@ int32_t vrad_mlp_train_step_device(vrad_mlp *m, const uint16_t *x, const float *
                                    void *stream);
 int32_t vrad_mlp_loss(vrad_mlp *m, float *loss);
 
+/* Attaches a network to the bounce (NULL detaches it: the plain bounce).
+ * With one attached, a light pass bounces once from the direct light (B1),
+ * asks the network for each patch's converged bounced light G from its
+ * features, and then iterates T <- B1 + gather(G) and T_next = T + the
+ * bounced change from there, stopping when the summed magnitude of a
+ * step's change is below the threshold.  The network must outlive its
+ * use; the context does not own it. */
+int32_t vrad_bounce_set_model(vrad_ctx *ctx, const vrad_mlp *model);
+
+/* After a light pass: per receiver (VisMatrix.ReceiverOrder), the network's
+ * 32 BF16 inputs (x, nullable) and log1p of the bounced light the pass
+ * converged to (target, 3 floats, nullable), device buffers of `capacity`
+ * rows; *count = the receivers.  The training set of the warm start. */
+int32_t vrad_bounce_features_device(vrad_ctx *ctx, uint16_t *x, float *target, int64_t capacity, int64_t *count,
+                                    void *stream);
+
 /* Largest batch vrad_trace_visibility_static accepts: four of the
  * reference's 16,384-ray batches. */
 #define VRAD_STATIC_MAX_RAYS 65536
