@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--workload", default="stage", choices=["stage", "seam"])
     ap.add_argument("--no-e2e", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-cpu", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--no-learned", action="store_true", help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -126,7 +127,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def dist_setup(gpus: int):
+def dist_setup(gpus: int, backend: str = "nccl"):
+    """One process per GPU (torchrun's environment); the process group is
+    only the barrier and the max-over-ranks time: the ranks are replicas,
+    each lighting its own map, with no data-path exchange."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -134,8 +138,9 @@ def dist_setup(gpus: int):
         import datetime
         import torch.distributed as dist
         import torch
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return rank, world, local
 
 
@@ -144,9 +149,15 @@ def max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_value(units_per_rank: float, ms_per_step: float, world: int) -> float:
+    """Whole-job throughput: every rank's units over the slowest rank's time."""
+    return world * units_per_rank / (ms_per_step / 1000.0)
 
 
 def barrier(world: int):
@@ -335,6 +346,50 @@ def main_seam(args):
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
+
+    # The learned warm start: a network trained on the device on plain
+    # bounce solutions of eight small seeded maps (2 to 6 rooms a side),
+    # then this map bounced from its guess, against the plain bounce.
+    learned = None
+    if rank == 0 and not args.no_learned:
+        from hl2sdk_tools_sharp_b200 import learned as LN
+        t = time.perf_counter()
+        lx, lt = LN.collect([LN.training_config(k) for k in range(8)], threshold=BOUNCE_THRESHOLD)
+        collect_s = time.perf_counter() - t
+        net = LN.Network(stage.tracer, seed=7)
+        ta, tb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ta.record(stream)
+        loss = LN.train(net, lx, lt, steps=3000)
+        tb.record(stream)
+        torch.cuda.synchronize()
+        train_ms = ta.elapsed_time(tb)
+        stage.set_bounce_model(net)
+        warm_lump, _, _ = stage.light_pass()
+        bw = stage.bounce_stats()
+        stage.set_bounce_model(None)
+        hx, ht = stage.bounce_features()
+        for _ in range(3):
+            net.forward(hx)
+        ta.record(stream)
+        for _ in range(10):
+            y = net.forward(hx)
+        tb.record(stream)
+        torch.cuda.synchronize()
+        fwd_ms = ta.elapsed_time(tb) / 10
+        flops = 2.0 * (32 * 128 + 128 * 128 + 128 * 8) * len(hx)
+        tpeak = float(peaks.get("bf16_tflops", 1590.0))
+        learned = {"plain_bounces": int(bst.bounces), "warm_bounces": int(bw.bounces),
+                   "plain_bounce_ms": statistics.median([p[2] for p in phases]), "warm_bounce_ms": bw.bounce_ms,
+                   "iteration_ratio": bst.bounces / max(1, bw.bounces),
+                   "lightmap_within_1_lsb": LN.within_one_lsb(warm_lump, lump_host),
+                   "guess_abs_error_log1p": float((y - ht).abs().mean().item()),
+                   "training": {"maps": 8, "rows": int(len(lx)), "steps": 3000, "batch": 32768,
+                                "collect_s": collect_s, "train_ms": train_ms, "final_loss": loss},
+                   "roofline": {"bound": "tensor", "kernel": "k_mlp_forward (mma.sync bf16, fp32 accumulate)",
+                                "achieved": flops / (fwd_ms / 1000.0) / 1e12, "peak": tpeak, "unit": "TFLOP/s",
+                                "frac": flops / (fwd_ms / 1000.0) / 1e12 / tpeak, "rows": int(len(hx)),
+                                "ms": fwd_ms, "flops_per_row": flops / len(hx)}}
+        net.close()
     sky_ms = kt["sky"]
     achieved = BYTES_PER_RAY * rays["sky"].shape[0] / (sky_ms / 1000.0) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -364,6 +419,7 @@ def main_seam(args):
             "bvh": {"nodes": info.bvh_nodes, "leaves": info.bvh_leaves, "max_leaf": info.max_leaf,
                     "build_ms": info.build_ms, "pad": info.box_pad},
             "check": check,
+            "learned": learned,
         }
         print(json.dumps(line), flush=True)
     tr.close()
@@ -590,7 +646,7 @@ def main_stage(args):
     elapsed_ms = max_over_ranks(t0.elapsed_time(t1), world_size)
     per_step = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps)]
     ms_per_step = elapsed_ms / args.steps
-    value = world_size * rays_per_step / (ms_per_step / 1000.0)
+    value = job_value(rays_per_step, ms_per_step, world_size)
     bst = stage.bounce_stats()
 
     # End to end through the host-buffer C ABI: the world (samples from
@@ -644,6 +700,50 @@ def main_stage(args):
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
+
+    # The learned warm start: a network trained on the device on plain
+    # bounce solutions of eight small seeded maps (2 to 6 rooms a side),
+    # then this map bounced from its guess, against the plain bounce.
+    learned = None
+    if rank == 0 and not args.no_learned:
+        from hl2sdk_tools_sharp_b200 import learned as LN
+        t = time.perf_counter()
+        lx, lt = LN.collect([LN.training_config(k) for k in range(8)], threshold=BOUNCE_THRESHOLD)
+        collect_s = time.perf_counter() - t
+        net = LN.Network(stage.tracer, seed=7)
+        ta, tb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ta.record(stream)
+        loss = LN.train(net, lx, lt, steps=3000)
+        tb.record(stream)
+        torch.cuda.synchronize()
+        train_ms = ta.elapsed_time(tb)
+        stage.set_bounce_model(net)
+        warm_lump, _, _ = stage.light_pass()
+        bw = stage.bounce_stats()
+        stage.set_bounce_model(None)
+        hx, ht = stage.bounce_features()
+        for _ in range(3):
+            net.forward(hx)
+        ta.record(stream)
+        for _ in range(10):
+            y = net.forward(hx)
+        tb.record(stream)
+        torch.cuda.synchronize()
+        fwd_ms = ta.elapsed_time(tb) / 10
+        flops = 2.0 * (32 * 128 + 128 * 128 + 128 * 8) * len(hx)
+        tpeak = float(peaks.get("bf16_tflops", 1590.0))
+        learned = {"plain_bounces": int(bst.bounces), "warm_bounces": int(bw.bounces),
+                   "plain_bounce_ms": statistics.median([p[2] for p in phases]), "warm_bounce_ms": bw.bounce_ms,
+                   "iteration_ratio": bst.bounces / max(1, bw.bounces),
+                   "lightmap_within_1_lsb": LN.within_one_lsb(warm_lump, lump_host),
+                   "guess_abs_error_log1p": float((y - ht).abs().mean().item()),
+                   "training": {"maps": 8, "rows": int(len(lx)), "steps": 3000, "batch": 32768,
+                                "collect_s": collect_s, "train_ms": train_ms, "final_loss": loss},
+                   "roofline": {"bound": "tensor", "kernel": "k_mlp_forward (mma.sync bf16, fp32 accumulate)",
+                                "achieved": flops / (fwd_ms / 1000.0) / 1e12, "peak": tpeak, "unit": "TFLOP/s",
+                                "frac": flops / (fwd_ms / 1000.0) / 1e12 / tpeak, "rows": int(len(hx)),
+                                "ms": fwd_ms, "flops_per_row": flops / len(hx)}}
+        net.close()
     # The dominant phases timed alone on the launching stream: the direct
     # gather kernel, and the transfer build (its phase events).
     a_ev = torch.cuda.Event(enable_timing=True)
@@ -705,6 +805,7 @@ def main_stage(args):
                     "build_ms": info.build_ms, "pad": info.box_pad},
             "autotune": {"threads_per_cta": block, "ms": tune_ms},
             "check": check,
+            "learned": learned,
         }
         print(json.dumps(line), flush=True)
     stage.close()
