@@ -416,7 +416,7 @@ def main_seam(args):
             "clocks": clocks.summary(),
             "kernel_ms": kt,
             "step_ms": per_step,
-            "bvh": {"nodes": info.bvh_nodes, "leaves": info.bvh_leaves, "max_leaf": info.max_leaf,
+            "bvh": {"nodes": info.bvh_nodes, "leaves": info.bvh_leaves, "max_leaf": info.max_leaf, "depth": info.bvh_depth,
                     "build_ms": info.build_ms, "pad": info.box_pad},
             "check": check,
             "learned": learned,
@@ -801,7 +801,7 @@ def main_stage(args):
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
             "step_ms": per_step,
-            "bvh": {"nodes": info.bvh_nodes, "leaves": info.bvh_leaves, "max_leaf": info.max_leaf,
+            "bvh": {"nodes": info.bvh_nodes, "leaves": info.bvh_leaves, "max_leaf": info.max_leaf, "depth": info.bvh_depth,
                     "build_ms": info.build_ms, "pad": info.box_pad},
             "autotune": {"threads_per_cta": block, "ms": tune_ms},
             "check": check,

@@ -249,6 +249,7 @@ int32_t vrad_scene_get_info(vrad_ctx *ctx, vrad_scene_info *out) {
     out->bvh_nodes = ctx->report.nodes;
     out->bvh_leaves = ctx->report.leaves;
     out->max_leaf = ctx->report.max_leaf;
+    out->bvh_depth = ctx->report.max_depth;
     for (int a = 0; a < 3; a++) {
         out->bounds_min[a] = ctx->report.bounds[a];
         out->bounds_max[a] = ctx->report.bounds[3 + a];

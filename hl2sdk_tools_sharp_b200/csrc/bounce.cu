@@ -264,7 +264,7 @@ template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_transfer(BounceView v, DeviceScene sc, const int64_t *__restrict__ cand_off,
                                                     const int32_t *__restrict__ cand_src, float *__restrict__ cand_w,
                                                     int64_t ncand, unsigned long long *counters, uint32_t *overflow) {
-    __shared__ int stack_mem[kStackDepth * BLOCK];
+    extern __shared__ int stack_mem[];  // sc.stack_depth() entries per thread
     int *stack = stack_mem + threadIdx.x;
     const int64_t q = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
     const bool live = q < ncand;
@@ -675,7 +675,7 @@ cudaError_t launch_transfers(BounceBuffers &b, const DeviceScene &scene, uint32_
     k_candidates<<<blocks(R, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.cand_off, nullptr, b.cand_src,
                                                                        overflow);
     if (b.ncand > 0)
-        k_transfer<kBlock><<<blocks(b.ncand, kBlock), kBlock, 0, stream>>>(b.view, scene, b.cand_off, b.cand_src,
+        k_transfer<kBlock><<<blocks(b.ncand, kBlock), kBlock, sizeof(int) * scene.stack_depth() * kBlock, stream>>>(b.view, scene, b.cand_off, b.cand_src,
                                                                            b.cand_w, b.ncand, b.counters, overflow);
     k_transfer_count<<<blocks((int64_t)R * 32, kBounceBlock), kBounceBlock, 0, stream>>>(R, b.cand_off, b.cand_w,
                                                                                          b.tr_off + 1);

@@ -37,7 +37,7 @@ template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_direct(DeviceScene sc, DeviceWorld w, float4 *__restrict__ out,
                                                   unsigned long long *__restrict__ counters,
                                                   uint32_t *__restrict__ overflow) {
-    __shared__ int stack_mem[kStackDepth * BLOCK];
+    extern __shared__ int stack_mem[];  // sc.stack_depth() entries per thread
     int *stack = stack_mem + threadIdx.x;
     const int64_t slot = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
     // nslots is a multiple of 32 and every warp's slots share one cluster
@@ -101,15 +101,16 @@ cudaError_t launch_direct(const DeviceScene &scene, const DeviceWorld &world, fl
                           unsigned long long *counters, uint32_t *overflow, cudaStream_t stream,
                           int block) {
     if (world.nslots == 0) return cudaSuccess;
+    const size_t smem = sizeof(int) * (size_t)scene.stack_depth();  // per thread
     switch (block) {
         case 32:
-            k_direct<32><<<(unsigned)((world.nslots + 31) / 32), 32, 0, stream>>>(scene, world, out, counters, overflow);
+            k_direct<32><<<(unsigned)((world.nslots + 31) / 32), 32, smem * 32, stream>>>(scene, world, out, counters, overflow);
             break;
         case 64:
-            k_direct<64><<<(unsigned)((world.nslots + 63) / 64), 64, 0, stream>>>(scene, world, out, counters, overflow);
+            k_direct<64><<<(unsigned)((world.nslots + 63) / 64), 64, smem * 64, stream>>>(scene, world, out, counters, overflow);
             break;
         default:
-            k_direct<128><<<(unsigned)((world.nslots + 127) / 128), 128, 0, stream>>>(scene, world, out, counters, overflow);
+            k_direct<128><<<(unsigned)((world.nslots + 127) / 128), 128, smem * 128, stream>>>(scene, world, out, counters, overflow);
             break;
     }
     return cudaGetLastError();

@@ -21,6 +21,9 @@
 
 #include <cfloat>
 #include <cmath>
+#include <cstring>
+#include <utility>
+#include <vector>
 
 #include "scene.cuh"
 
@@ -514,7 +517,31 @@ cudaError_t build_bvh(BvhBuffers &sb, const vrad_triangle *h_tris,
         goto fail;
     }
     sb.ntris = n;
+    // The tree's depth in inner nodes, from the emitted nodes: the deepest
+    // stack a walk can build (each inner node pushes at most one entry).
+    // Nodes sit at their inner-node numbers (0 .. n-2, the root at 0); the
+    // collapsed subtrees' nodes stay in the array, unreachable.
+    if (n > 1 && stats[0] > 0) {
+        std::vector<float4> nodes((size_t)inner * 4);
+        VRAD_TRY(cudaMemcpy(nodes.data(), sb.nodes, sizeof(float4) * nodes.size(), cudaMemcpyDeviceToHost));
+        std::vector<std::pair<int32_t, int32_t>> todo = {{0, 1}};
+        int32_t depth = 0;
+        while (!todo.empty()) {
+            const auto [node, d] = todo.back();
+            todo.pop_back();
+            depth = d > depth ? d : depth;
+            if (d > kStackDepth) break;  // the walk's limit: deeper is an error either way
+            int32_t refs[2];
+            std::memcpy(refs, &nodes[(size_t)node * 4 + 3], sizeof refs);
+            for (int32_t r : refs)
+                if (r >= 0 && r < inner) todo.push_back({r, d + 1});
+        }
+        sb.depth = depth > kStackDepth ? kStackDepth : depth;  // deeper: walks report an overflow
+    } else {
+        sb.depth = n > 0 ? 1 : 0;
+    }
     if (report) {
+        report->max_depth = sb.depth > report->max_depth ? sb.depth : report->max_depth;
         const bool first = report->nodes == 0 && report->leaves == 0;
         report->nodes += stats[0];
         report->leaves += stats[1];
@@ -568,6 +595,7 @@ void BvhBuffers::release() {
     tri0 = tri1 = tri2 = nullptr;
     nodes = nullptr;
     ntris = 0;
+    depth = 0;
 }
 
 void SceneBuffers::release() {

@@ -14,9 +14,10 @@ struct BvhBuffers {
     float4 *tri2 = nullptr;
     float4 *nodes = nullptr;
     int32_t ntris = 0;
+    int32_t depth = 0;  // inner nodes on the longest root-to-leaf path
 
     void release();
-    DeviceBvh view() const { return DeviceBvh{tri0, tri1, tri2, nodes, ntris}; }
+    DeviceBvh view() const { return DeviceBvh{tri0, tri1, tri2, nodes, ntris, depth}; }
 };
 
 struct SceneBuffers {
@@ -33,6 +34,7 @@ struct SceneBuildReport {
     int32_t nodes = 0;
     int32_t leaves = 0;
     int32_t max_leaf = 0;
+    int32_t max_depth = 0;
     float bounds[6] = {0, 0, 0, 0, 0, 0};
     float pad = 0;
     float build_ms = 0;

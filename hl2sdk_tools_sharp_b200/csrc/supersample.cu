@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(BLOCK) k_resample(DeviceScene sc, DeviceWorld 
                                                     const float4 *__restrict__ points, float4 *__restrict__ row_out,
                                                     int32_t *__restrict__ row_bits, unsigned long long *counters,
                                                     uint32_t *overflow) {
-    __shared__ int stack_mem[kStackDepth * BLOCK];
+    extern __shared__ int stack_mem[];  // sc.stack_depth() entries per thread
     int *stack = stack_mem + threadIdx.x;
     const int64_t tid = (int64_t)blockIdx.x * BLOCK + threadIdx.x;
     const int g = (int)(tid >> 2), l4 = (int)(tid & 3);
@@ -425,7 +425,8 @@ cudaError_t run_supersample(SupersampleBuffers &ss, const DeviceScene &scene, co
         if (e == cudaSuccess)
             k_ss_place<<<grid_of(nsel, 256), 256, 0, s>>>(nsel, world, ss.selected, ss.base, ss.counts + 1 + C, ss.rows);
         if (e == cudaSuccess && g > 0)
-            k_resample<kSsBlock><<<grid_of(4 * (int64_t)g, kSsBlock), kSsBlock, 0, s>>>(
+            k_resample<kSsBlock><<<grid_of(4 * (int64_t)g, kSsBlock), kSsBlock,
+                                  sizeof(int) * scene.stack_depth() * kSsBlock, s>>>(
                 scene, world, fv, g, 2 * C + 1, ss.base, ss.rows, ss.selected, ss.origin_st, ss.wind, ss.points,
                 ss.row_out, ss.row_bits, counters, overflow);
         if (e == cudaSuccess)

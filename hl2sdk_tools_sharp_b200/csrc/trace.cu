@@ -29,7 +29,7 @@ __global__ void __launch_bounds__(kBlock) k_trace(DeviceScene s, const vrad_ray 
                                                   int64_t n, TraceParams p, uint32_t *__restrict__ bits,
                                                   vrad_hit *__restrict__ hits,
                                                   uint32_t *__restrict__ overflow) {
-    __shared__ int stack_mem[kStackDepth * kBlock];
+    extern __shared__ int stack_mem[];  // sc.stack_depth() entries per thread
     int *stack = stack_mem + threadIdx.x;
     const int lane = threadIdx.x & 31;
     const int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x;
@@ -83,15 +83,16 @@ cudaError_t launch_trace(const DeviceScene &scene, const vrad_ray *d_rays, int64
     if (n <= 0) return cudaSuccess;
     const int64_t grid = (n + kBlock - 1) / kBlock;
     if (grid > 0x7fffffffLL) return cudaErrorInvalidValue;
+    const size_t smem = sizeof(int) * (size_t)scene.stack_depth() * kBlock;
     switch (p.mode) {
         case kModeAny:
-            k_trace<kModeAny><<<(unsigned)grid, kBlock, 0, stream>>>(scene, d_rays, n, p, d_bits, d_hits, d_overflow);
+            k_trace<kModeAny><<<(unsigned)grid, kBlock, smem, stream>>>(scene, d_rays, n, p, d_bits, d_hits, d_overflow);
             break;
         case kModeClosest:
-            k_trace<kModeClosest><<<(unsigned)grid, kBlock, 0, stream>>>(scene, d_rays, n, p, d_bits, d_hits, d_overflow);
+            k_trace<kModeClosest><<<(unsigned)grid, kBlock, smem, stream>>>(scene, d_rays, n, p, d_bits, d_hits, d_overflow);
             break;
         default:
-            k_trace<kModeSkyPass><<<(unsigned)grid, kBlock, 0, stream>>>(scene, d_rays, n, p, d_bits, d_hits, d_overflow);
+            k_trace<kModeSkyPass><<<(unsigned)grid, kBlock, smem, stream>>>(scene, d_rays, n, p, d_bits, d_hits, d_overflow);
             break;
     }
     return cudaGetLastError();

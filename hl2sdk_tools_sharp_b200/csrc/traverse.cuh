@@ -122,7 +122,7 @@ __device__ __forceinline__ bool walk(const DeviceBvh &s, const int32_t *__restri
                     near_ref = r1;
                     far_ref = r0;
                 }
-                if (sp < kStackDepth) {
+                if (sp < s.depth) {
                     stack[sp * STRIDE] = far_ref;
                     sp++;
                 } else {

@@ -40,12 +40,19 @@ struct DeviceBvh {
     const float4 *tri2;
     const float4 *nodes;
     int32_t ntris;  // 0: empty, never traversed
+    int32_t depth;  // stack entries a walk can need: the tree's depth in inner nodes
 };
 
 struct DeviceScene {
     DeviceBvh opaque;
     DeviceBvh sky;
     const int32_t *tri_id;
+    // The traversal stack's entries per thread (kernels size their shared
+    // memory by it): the deeper tree's depth, at least 1, at most kStackDepth.
+    __host__ __device__ int32_t stack_depth() const {
+        const int32_t d = opaque.depth > sky.depth ? opaque.depth : sky.depth;
+        return d < 1 ? 1 : (d > kStackDepth ? kStackDepth : d);
+    }
 };
 
 enum TraceMode : int { kModeAny = 0, kModeClosest = 1, kModeSkyPass = 2 };

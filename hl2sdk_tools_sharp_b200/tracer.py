@@ -75,7 +75,7 @@ class SceneInfo(ctypes.Structure):
                 ("bvh_leaves", ctypes.c_int32), ("max_leaf", ctypes.c_int32),
                 ("bounds_min", ctypes.c_float * 3), ("bounds_max", ctypes.c_float * 3),
                 ("box_pad", ctypes.c_float), ("build_ms", ctypes.c_float),
-                ("device_bytes", ctypes.c_int64)]
+                ("device_bytes", ctypes.c_int64), ("bvh_depth", ctypes.c_int32)]
 
 
 @dataclasses.dataclass(frozen=True)

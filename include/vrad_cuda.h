@@ -98,6 +98,7 @@ typedef struct vrad_scene_info {
     float box_pad;
     float build_ms;
     int64_t device_bytes;
+    int32_t bvh_depth;      /* inner nodes on the deepest path: the traversal stack's size */
 } vrad_scene_info;
 
 typedef struct vrad_ctx vrad_ctx;
