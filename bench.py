@@ -660,10 +660,19 @@ def main_stage(args):
         out_pinned = torch.empty(len(lump_host), dtype=torch.uint8, pin_memory=True)
         outv = out_pinned.numpy()
 
+        parts = {"upload_world": [], "upload_bounce": [], "light_pass": []}
+
         def e2e_step():
+            t0 = time.perf_counter()
             stage.upload_world(inp_pinned)
+            t1 = time.perf_counter()
             stage.upload_bounce(refl, pvs_off, pvs_list, bounces=MAX_BOUNCES, threshold=BOUNCE_THRESHOLD)
+            t2 = time.perf_counter()
             stage.light_pass(outv)
+            t3 = time.perf_counter()
+            parts["upload_world"].append(t1 - t0)
+            parts["upload_bounce"].append(t2 - t1)
+            parts["light_pass"].append(t3 - t2)
         e2e_step()
         barrier(world_size)
         t = time.perf_counter()
@@ -675,6 +684,7 @@ def main_stage(args):
                "h2d_bytes_per_step": int(inp.samples.nbytes + inp.faces.nbytes + inp.lights.nbytes
                                          + inp.verts.nbytes + refl.nbytes + pvs_off.nbytes + pvs_list.nbytes),
                "d2h_bytes_per_step": int(len(lump_host)), "stage_s": e2e_s,
+               "parts_s": {k: statistics.median(v[1:]) for k, v in parts.items()},
                "note": "includes the host-side set-up of the world and the bounce (slot layout, final-pass "
                        "tables, the patch tree) and the device tables' uploads"}
         if not np.array_equal(outv, lump_host):

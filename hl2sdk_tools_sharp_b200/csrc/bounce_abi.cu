@@ -17,6 +17,7 @@
 #include "bounce_host.h"
 #include "context.cuh"
 #include "patches.h"
+#include "setup_clock.h"
 #include "world.h"
 
 namespace vrad {
@@ -222,10 +223,12 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
         if (ctx->h_faces[(size_t)f].flags & VRAD_SURF_BUMPLIGHT)
             return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "face %d is bump-mapped", f);
 
+    SetupClock clock("bounce_upload");
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
     BounceBuffers &b = ctx->bounce;
     b.release();
+    clock.mark("release");
     PatchTree tree;
     std::string why;
     const int64_t nvert = (int64_t)ctx->h_vertices.size() / 3;
@@ -233,6 +236,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
                           d->min_chop, tree, why))
         return vrad_fail(ctx, VRAD_ERR_ARG, "patches: %s", why.c_str());
     const int32_t P = (int32_t)tree.patches.size();
+    clock.mark("patch tree");
 
     // Per patch.
     std::vector<float4> origin((size_t)P), normal((size_t)P), mins((size_t)P), maxs((size_t)P), refl((size_t)P);
@@ -272,6 +276,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
         if (fs.y == 0) fs.x = (int32_t)k;
         fs.y++;
     }
+    clock.mark("patch tables");
     // VisMatrix.ReceiverOrder: cluster by cluster, leaf patches in index order.
     std::vector<std::vector<int32_t>> by_cluster((size_t)C);
     for (int32_t i = 0; i < P; i++)
@@ -293,6 +298,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
         }
         row_off[(size_t)c + 1] = (int32_t)row_faces.size();
     }
+    clock.mark("receivers and rows");
     // The final pass's patch tables over the smoothing neighbours.
     std::vector<int32_t> noff((size_t)nf + 1);
     int64_t nn = 0;
@@ -302,11 +308,13 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     std::vector<int32_t> nlist((size_t)(nn ? nn : 1));
     vrad_build_neighbours(ctx->h_faces.data(), nf, ctx->h_vertices.data(), nvert, 0.7071067f, noff.data(), nlist.data(), nn,
                           &nn);
+    clock.mark("neighbours");
     std::vector<int32_t> pr_off, pr_patch;
     std::vector<int4> pr_box;
     std::vector<float4> pr_coord;
     patch_radial_tables(ctx->h_faces, tree, noff, nlist, pr_off, pr_patch, pr_box, pr_coord);
 
+    clock.mark("patch radial tables");
     const int32_t R = (int32_t)recv.size();
     const int64_t ncells = ctx->final_pass.view.ncells;
     if (e == cudaSuccess) e = upload(&b.origin, origin);
@@ -355,6 +363,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
         b.release();
         return vrad_cuda_fail(ctx, e, "bounce upload");
     }
+    clock.mark("device buffers");
     b.npatches = P;
     b.nfaces = nf;
     b.nreceivers = R;
@@ -389,6 +398,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
         b.release();
         return vrad_fail(ctx, VRAD_ERR_CUDA, "stack overflow in the candidate walk (flags %u)", overflow);
     }
+    clock.mark("candidate sizing");
     const int64_t ntr = 0;
     b.ntransfers = ntr;
     b.ready = true;

@@ -24,6 +24,7 @@
 
 #include "context.cuh"
 #include "gather.cuh"
+#include "setup_clock.h"
 #include "supersample.cuh"
 
 namespace vrad {
@@ -137,6 +138,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
         !w->cluster_light_offsets || (w->nsky_directions && !w->sky_directions) ||
         (w->nsun_jitter && !w->sun_jitter) || w->sun_samples < 1 || w->sun_samples - 1 > w->nsun_jitter)
         return vrad_fail(ctx, VRAD_ERR_ARG, "invalid world description");
+    vrad::SetupClock clock("world_upload");
     const int32_t nl = w->nlights;
     for (int32_t l = 0; l < nl; l++) {
         const int t = w->lights[l].type;
@@ -184,6 +186,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
         fend[(size_t)face] = j;
         i = j;
     }
+    clock.mark("samples");
     // Slots, cluster by cluster: each face's samples in whole groups of
     // four (the last group repeating its last sample as padding), each
     // cluster's run padded to whole warps with more padding lanes, so no
@@ -237,6 +240,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     for (int32_t d = 0; d < w->nsun_jitter; d++)
         jit[(size_t)d] = make_float4(w->sun_jitter[3 * d], w->sun_jitter[3 * d + 1], w->sun_jitter[3 * d + 2], 0.0f);
 
+    clock.mark("slots and lights");
     std::lock_guard<std::mutex> g(ctx->mu);
     cudaError_t e = cudaSetDevice(ctx->device);
     vrad::WorldBuffers &wb = ctx->world;
@@ -257,6 +261,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     wb.view = vrad::DeviceWorld{wb.slots, (int64_t)slots.size(), wb.sample_pos, wb.face_normal, wb.lights, nl,
                                 wb.cl_off, wb.cl_list, w->nclusters, wb.dirs, w->nsky_directions, wb.jitter,
                                 w->nsun_jitter, w->sun_angular_extent, w->sun_samples, w->nsamples};
+    clock.mark("world buffers");
     // The final pass's tables, and the direct gather's output buffer.  A
     // new world drops the old bounce.
     ctx->bounce.release();
@@ -277,6 +282,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
             if (e == cudaErrorInvalidValue) return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "final pass: %s", why.c_str());
             return vrad_cuda_fail(ctx, e, why.c_str());
         }
+        clock.mark("final pass tables");
         ctx->final_pass.view.sample_pos = wb.sample_pos;
         bool have = false;
         e = vrad::build_supersample(ctx->supersample, ctx->h_faces, ctx->h_vertices, ctx->h_samples, ctx->final_pass,
@@ -287,6 +293,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
             return vrad_cuda_fail(ctx, e, why.c_str());
         }
         ctx->supersample_why = have ? std::string() : why;
+        clock.mark("supersample tables");
     } else {
         ctx->supersample.release();
         ctx->supersample_why = "the world was uploaded without face windings";

@@ -31,6 +31,7 @@
 #include "bounce_host.h"
 #include "context.cuh"
 #include "final.cuh"
+#include "setup_clock.h"
 #include "world.h"
 
 namespace vrad {
@@ -339,6 +340,7 @@ cudaError_t launch_final(const FinalView &v, const float4 *sample_light, float4 
 cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces, const vrad_sample *samples,
                         int64_t nsamples, const float *vertices, int64_t nvertices, std::string &why) {
     fb.release();
+    SetupClock clock("final_tables");
     std::vector<FaceFrameOut> fr((size_t)nfaces);
     for (int32_t f = 0; f < nfaces; f++) face_frame_of(faces[f], fr[(size_t)f]);
     // Neighbours (FaceNeighbours.Build, DefaultSmoothingThreshold).
@@ -350,6 +352,7 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
     }
     std::vector<int32_t> nlist((size_t)(nn ? nn : 1));
     vrad_build_neighbours(faces, nfaces, vertices, nvertices, 0.7071067f, noff.data(), nlist.data(), nn, &nn);
+    clock.mark("neighbours");
     std::vector<int32_t> lightofs((size_t)nfaces);
     int64_t total = 0;
     vrad_lightmap_layout(faces, nfaces, lightofs.data(), &total);
@@ -394,6 +397,7 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
         cell_sample[(size_t)(face_cells[(size_t)sm.face] + sm.s + sm.t * q.width)] = (int32_t)i;
         sbox[(size_t)i] = make_float4(sm.mins[0], sm.mins[1], sm.maxs[0], sm.maxs[1]);
     }
+    clock.mark("frames and cells");
     // Neighbour candidates: each neighbour's samples whose box, moved into
     // this face's luxel space as BuildLuxelRadial moves it, can cover a cell.
     std::vector<int32_t> cand_off((size_t)nfaces + 1, 0), cand_sample;
@@ -422,6 +426,7 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
         }
         cand_off[(size_t)f + 1] = (int32_t)cand_sample.size();
     }
+    clock.mark("candidates");
     auto up = [](auto **dst, const auto &v) {
         using T = typename std::remove_reference<decltype(v)>::type::value_type;
         cudaError_t e = cudaMalloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
@@ -445,6 +450,7 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
         why = "final-pass buffers";
         return e;
     }
+    clock.mark("upload");
     fb.lighting_bytes = total;
     fb.nfaces = nfaces;
     fb.lightofs = lightofs;

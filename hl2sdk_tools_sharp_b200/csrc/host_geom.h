@@ -61,8 +61,20 @@ inline void clip_axis(const Winding &in, int ax, float dist, float eps, Winding 
     front.clear();
     back.clear();
     const size_t n = in.size();
-    std::vector<float> dists(n + 1);
-    std::vector<int> sides(n + 1);  // 0 front, 1 back, 2 on
+    // Windings here have a handful of points: local arrays, a heap
+    // fallback only past 63.
+    float dist_buf[64];
+    int side_buf[64];
+    std::vector<float> dist_big;
+    std::vector<int> side_big;
+    float *dists = dist_buf;
+    int *sides = side_buf;  // 0 front, 1 back, 2 on
+    if (n + 1 > 64) {
+        dist_big.resize(n + 1);
+        side_big.resize(n + 1);
+        dists = dist_big.data();
+        sides = side_big.data();
+    }
     int counts[3] = {0, 0, 0};
     const V3 normal = {ax == 0 ? 1.0f : 0.0f, ax == 1 ? 1.0f : 0.0f, ax == 2 ? 1.0f : 0.0f};
     for (size_t i = 0; i < n; i++) {

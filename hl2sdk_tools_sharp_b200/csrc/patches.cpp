@@ -27,6 +27,7 @@
 #include "../../include/vrad_cuda.h"
 #include "host_geom.h"
 #include "patches.h"
+#include "setup_clock.h"
 #include "world.h"
 
 namespace vrad {
@@ -181,11 +182,13 @@ bool prevent_subdivision(int32_t flags) {
 
 bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
                       const float *reflectivity, float max_chop, float min_chop, PatchTree &out, std::string &why) {
+    SetupClock clock("patch_tree");
     std::vector<std::vector<float>> corners;
     if (!corner_normals(faces, nfaces, vertices, nvertices, kSmoothing, corners)) {
         why = "a face's winding lies outside the vertex array";
         return false;
     }
+    clock.mark("corner normals");
     std::vector<V3> centroid((size_t)nfaces, V3{0.0f, 0.0f, 0.0f});
     out.face_root.assign((size_t)nfaces, -1);
     // MakePatchForFace, face by face: the roots, in face order.
@@ -243,6 +246,7 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
         subtree.push_back(std::move(b));
     }
     const int32_t roots = (int32_t)subtree.size();
+    clock.mark("roots");
     // PatchSubdivider.Subdivide with bounces > 0, not -fast.  Each root's
     // subtree depends on nothing outside its face, so the roots are split
     // on worker threads, each into its own arrays.
@@ -260,6 +264,7 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
         work();
         for (auto &t : pool) t.join();
     }
+    clock.mark("subdivide");
     // Global indices: the roots 0..roots-1 in face order, then each root's
     // descendants in creation order (the order SubdividePatch adds them).
     std::vector<int32_t> base((size_t)roots);
@@ -272,7 +277,21 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
     std::vector<const Winding *> wind((size_t)total);
     out.face_first.assign((size_t)nfaces, 0);
     out.face_end.assign((size_t)nfaces, 0);
-    for (int32_t i = 0; i < roots; i++) {
+    const unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    auto parallel = [&](int64_t n, auto &&body) {
+        std::atomic<int64_t> next{0};
+        auto work = [&]() {
+            for (int64_t i; (i = next.fetch_add(1024)) < n;)
+                for (int64_t k = i; k < std::min(n, i + 1024); k++) body(k);
+        };
+        std::vector<std::thread> pool;
+        for (unsigned t = 1; t < nt; t++) pool.emplace_back(work);
+        work();
+        for (auto &t : pool) t.join();
+    };
+    // Each root's block of patches, renumbered, in parallel.
+    parallel(roots, [&](int64_t ii) {
+        const int32_t i = (int32_t)ii;
         Builder &b = subtree[(size_t)i];
         auto global = [&](int32_t local) { return local < 0 ? -1 : (local == 0 ? i : base[(size_t)i] + local - 1); };
         for (size_t k = 0; k < b.patches.size(); k++) {
@@ -284,23 +303,32 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
             out.patches[(size_t)g] = p;
             wind[(size_t)g] = &b.windings[k];
         }
+    });
+    for (int32_t i = 0; i < roots; i++) {
+        const Builder &b = subtree[(size_t)i];
         const int32_t f = b.patches[0].face;
         out.face_first[(size_t)f] = base[(size_t)i];
         out.face_end[(size_t)f] = base[(size_t)i] + (int32_t)b.patches.size() - 1;
         out.face_root[(size_t)f] = i;
     }
-    // Windings into one point array.
-    out.points.clear();
-    for (size_t i = 0; i < out.patches.size(); i++) {
-        vrad_patch &p = out.patches[i];
-        p.first_point = (int32_t)(out.points.size() / 3);
-        p.num_points = (int32_t)wind[i]->size();
-        for (const V3 &v : *wind[i]) {
-            out.points.push_back(v.x);
-            out.points.push_back(v.y);
-            out.points.push_back(v.z);
+    clock.mark("merge");
+    // Windings into one point array: offsets by a prefix sum, points copied
+    // in parallel.
+    std::vector<int64_t> first((size_t)total + 1, 0);
+    for (int32_t i = 0; i < total; i++) first[(size_t)i + 1] = first[(size_t)i] + (int64_t)wind[(size_t)i]->size();
+    out.points.assign((size_t)first[(size_t)total] * 3, 0.0f);
+    parallel(total, [&](int64_t i) {
+        vrad_patch &p = out.patches[(size_t)i];
+        p.first_point = (int32_t)first[(size_t)i];
+        p.num_points = (int32_t)wind[(size_t)i]->size();
+        float *dst = &out.points[(size_t)first[(size_t)i] * 3];
+        for (const V3 &v : *wind[(size_t)i]) {
+            *dst++ = v.x;
+            *dst++ = v.y;
+            *dst++ = v.z;
         }
-    }
+    });
+    clock.mark("points");
     out.roots = roots;
     return true;
 }

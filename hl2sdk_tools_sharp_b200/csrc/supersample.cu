@@ -35,6 +35,7 @@
 #include <vector>
 
 #include "gather.cuh"
+#include "setup_clock.h"
 #include "supersample.cuh"
 #include "world.h"
 
@@ -327,6 +328,7 @@ cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_fac
                               const FinalBuffers &fb, int32_t nclusters, bool &have, std::string &why) {
     ss.release();
     have = false;
+    SetupClock clock("supersample_tables");
     std::vector<int32_t> wind_flat;
     std::vector<float> pts;
     if (!sample_windings(faces.data(), (int32_t)faces.size(), vertices.data(), (int64_t)vertices.size() / 3,
@@ -334,6 +336,7 @@ cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_fac
         why = "the samples are not the face sample builder's own, so their cell windings are unknown";
         return cudaSuccess;
     }
+    clock.mark("windings");
     const size_t S = samples.size();
     std::vector<FaceFrameOut> fr(faces.size());
     std::vector<int32_t> face_cells(faces.size() + 1, 0);
@@ -353,6 +356,7 @@ cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_fac
     }
     std::vector<float4> p4(pts.size() / 3);
     for (size_t k = 0; k < p4.size(); k++) p4[k] = make_float4(pts[3 * k], pts[3 * k + 1], pts[3 * k + 2], 0.0f);
+    clock.mark("sample tables");
     const size_t S1 = S ? S : 1;
     const size_t groups = 5 * S1 + 16 * (size_t)(nclusters + 1);
     cudaError_t e = upload(&ss.origin_st, origin_st);
@@ -373,6 +377,7 @@ cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_fac
         why = "supersampling buffers";
         return e;
     }
+    clock.mark("upload");
     (void)fb;
     ss.nsamples = (int64_t)S;
     ss.nclusters = nclusters;

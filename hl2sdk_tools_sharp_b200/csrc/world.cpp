@@ -13,6 +13,8 @@
 // are the input of the device kernels.
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -88,99 +90,116 @@ float world_area_per_luxel(const vrad_face &f) {
 
 namespace {
 
-// FaceSampleBuilder.BuildFacesamples over every face.  With wind set, it
-// also keeps each partial sample's cell winding in world space (the
-// reference keeps them for supersampling, MakeSample with do_extra:
-// FaceSampleBuilder.cs:325-367): wind gets (first point, count) per sample,
-// count 0 for a whole cell, and pts the points (xyz each).
-int32_t build_samples_core(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
-                           vrad_sample *out, int64_t capacity, int64_t *count, int64_t *face_first,
-                           std::vector<int32_t> *wind, std::vector<float> *pts) {
-    if (nfaces < 0 || (nfaces > 0 && (!faces || !vertices)) || !count) return VRAD_ERR_ARG;
-    int64_t written = 0;
+// FaceSampleBuilder.BuildFacesamples for one face (number fi): its samples
+// appended to `out`.  With wind set, also each partial sample's cell winding
+// in world space (the reference keeps them for supersampling, MakeSample
+// with do_extra: FaceSampleBuilder.cs:325-367): wind gets (first point,
+// count) per sample, count 0 for a whole cell, points indexing pts.
+int32_t face_samples(const vrad_face &f, int32_t fi, const float *vertices, int64_t nvertices,
+                     std::vector<vrad_sample> &out, std::vector<int32_t> *wind, std::vector<float> *pts) {
+    if (f.num_vertices < 3 || f.first_vertex < 0 || f.first_vertex + (int64_t)f.num_vertices > nvertices)
+        return VRAD_ERR_ARG;
     Winding cell_front, cell_back, row_front, row_back;
-    for (int32_t fi = 0; fi < nfaces; fi++) {
-        const vrad_face &f = faces[fi];
-        if (face_first) face_first[fi] = written;
-        if (f.num_vertices < 3 || f.first_vertex < 0 || f.first_vertex + (int64_t)f.num_vertices > nvertices)
-            return VRAD_ERR_ARG;
-        const FaceFrame fr = face_frame(f);
-        const float area_per_luxel = world_area_per_luxel(f);
-        // LightmapCoordWinding: the face's winding in luxel space.
-        Winding w;
-        for (int32_t k = 0; k < f.num_vertices; k++) {
-            const float *v = vertices + 3 * (int64_t)(f.first_vertex + k);
-            w.push_back(add(V3{v[0], v[1], v[2]}, V3{0.0f, 0.0f, 0.0f}));
-        }
-        w = remove_colinear(w);
-        for (V3 &p : w) {
-            V3 pos = sub(p, fr.origin);
-            p = {dot(pos, fr.w2l_s) - (float)fr.min_s, dot(pos, fr.w2l_t) - (float)fr.min_t, 0.0f};
-        }
-        // BuildFacesamples: rows by t, cells by s, sample offset 1.0.
-        Winding lm = w;
-        for (int t = 0; t < fr.height && !lm.empty(); t++) {
-            clip_axis(lm, 1, (float)t + 1.0f, kLightmapOnEpsilon, row_front, row_back);
-            Winding row = row_back;
-            for (int s = 0; s < fr.width && !row.empty(); s++) {
-                clip_axis(row, 0, (float)s + 1.0f, kLightmapOnEpsilon, cell_front, cell_back);
-                if (!cell_back.empty()) {
-                    if (written >= capacity) {
-                        *count = written;
-                        return out ? VRAD_ERR_ARG : VRAD_OK;  // out == NULL: a counting pass
-                    }
-                    V3 center;
-                    float area = area_and_balance(cell_back, center) * area_per_luxel;
-                    float mn[2] = {99999.0f, 99999.0f}, mx[2] = {-99999.0f, -99999.0f};
-                    for (const V3 &p : cell_back) {
-                        if (p.x < mn[0]) mn[0] = p.x;
-                        if (p.x > mx[0]) mx[0] = p.x;
-                        if (p.y < mn[1]) mn[1] = p.y;
-                        if (p.y > mx[1]) mx[1] = p.y;
-                    }
-                    if (wind) {
-                        // EQUAL_EPSILON is a double literal: the test is in double.
-                        int32_t first = (int32_t)(pts->size() / 3), n = 0;
-                        if ((double)area < (double)area_per_luxel - 0.001) {
-                            for (const V3 &p : cell_back) {
-                                const V3 q = luxel_to_world(fr, p.x, p.y);
-                                pts->push_back(q.x);
-                                pts->push_back(q.y);
-                                pts->push_back(q.z);
-                                n++;
-                            }
-                        }
-                        wind->push_back(n ? first : 0);
-                        wind->push_back(n);
-                    }
-                    if (out) {
-                        vrad_sample &o = out[written];
-                        V3 pos = luxel_to_world(fr, center.x, center.y);
-                        o.position[0] = pos.x;
-                        o.position[1] = pos.y;
-                        o.position[2] = pos.z;
-                        o.area = area;
-                        o.coord[0] = center.x;
-                        o.coord[1] = center.y;
-                        o.mins[0] = mn[0];
-                        o.mins[1] = mn[1];
-                        o.maxs[0] = mx[0];
-                        o.maxs[1] = mx[1];
-                        o.s = s;
-                        o.t = t;
-                        o.face = fi;
-                        o.cluster = f.cluster;
-                    }
-                    written++;
-                }
-                row = cell_front;
-            }
-            lm = row_front;
-        }
+    const FaceFrame fr = face_frame(f);
+    const float area_per_luxel = world_area_per_luxel(f);
+    // LightmapCoordWinding: the face's winding in luxel space.
+    Winding w;
+    for (int32_t k = 0; k < f.num_vertices; k++) {
+        const float *v = vertices + 3 * (int64_t)(f.first_vertex + k);
+        w.push_back(add(V3{v[0], v[1], v[2]}, V3{0.0f, 0.0f, 0.0f}));
     }
-    if (face_first) face_first[nfaces] = written;
-    *count = written;
+    w = remove_colinear(w);
+    for (V3 &p : w) {
+        V3 pos = sub(p, fr.origin);
+        p = {dot(pos, fr.w2l_s) - (float)fr.min_s, dot(pos, fr.w2l_t) - (float)fr.min_t, 0.0f};
+    }
+    // BuildFacesamples: rows by t, cells by s, sample offset 1.0.
+    Winding lm = w;
+    for (int t = 0; t < fr.height && !lm.empty(); t++) {
+        clip_axis(lm, 1, (float)t + 1.0f, kLightmapOnEpsilon, row_front, row_back);
+        Winding row = row_back;
+        for (int s = 0; s < fr.width && !row.empty(); s++) {
+            clip_axis(row, 0, (float)s + 1.0f, kLightmapOnEpsilon, cell_front, cell_back);
+            if (!cell_back.empty()) {
+                V3 center;
+                float area = area_and_balance(cell_back, center) * area_per_luxel;
+                float mn[2] = {99999.0f, 99999.0f}, mx[2] = {-99999.0f, -99999.0f};
+                for (const V3 &p : cell_back) {
+                    if (p.x < mn[0]) mn[0] = p.x;
+                    if (p.x > mx[0]) mx[0] = p.x;
+                    if (p.y < mn[1]) mn[1] = p.y;
+                    if (p.y > mx[1]) mx[1] = p.y;
+                }
+                if (wind) {
+                    // EQUAL_EPSILON is a double literal: the test is in double.
+                    int32_t first = (int32_t)(pts->size() / 3), n = 0;
+                    if ((double)area < (double)area_per_luxel - 0.001) {
+                        for (const V3 &p : cell_back) {
+                            const V3 q = luxel_to_world(fr, p.x, p.y);
+                            pts->push_back(q.x);
+                            pts->push_back(q.y);
+                            pts->push_back(q.z);
+                            n++;
+                        }
+                    }
+                    wind->push_back(n ? first : 0);
+                    wind->push_back(n);
+                }
+                vrad_sample o;
+                V3 pos = luxel_to_world(fr, center.x, center.y);
+                o.position[0] = pos.x;
+                o.position[1] = pos.y;
+                o.position[2] = pos.z;
+                o.area = area;
+                o.coord[0] = center.x;
+                o.coord[1] = center.y;
+                o.mins[0] = mn[0];
+                o.mins[1] = mn[1];
+                o.maxs[0] = mx[0];
+                o.maxs[1] = mx[1];
+                o.s = s;
+                o.t = t;
+                o.face = fi;
+                o.cluster = f.cluster;
+                out.push_back(o);
+            }
+            row = cell_front;
+        }
+        lm = row_front;
+    }
     return VRAD_OK;
+}
+
+// Every face's samples, faces built in parallel (each face's samples
+// depend on that face alone), concatenated in face order.
+struct AllSamples {
+    std::vector<std::vector<vrad_sample>> samples;
+    std::vector<std::vector<int32_t>> wind;
+    std::vector<std::vector<float>> pts;
+};
+
+int32_t build_all_samples(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
+                          bool windings, AllSamples &all) {
+    if (nfaces < 0 || (nfaces > 0 && (!faces || !vertices))) return VRAD_ERR_ARG;
+    all.samples.assign((size_t)nfaces, {});
+    all.wind.assign(windings ? (size_t)nfaces : 0, {});
+    all.pts.assign(windings ? (size_t)nfaces : 0, {});
+    std::atomic<int32_t> next{0};
+    std::atomic<int32_t> rc{VRAD_OK};
+    auto work = [&]() {
+        for (int32_t f; (f = next.fetch_add(1)) < nfaces;) {
+            const int32_t r = face_samples(faces[f], f, vertices, nvertices, all.samples[(size_t)f],
+                                           windings ? &all.wind[(size_t)f] : nullptr,
+                                           windings ? &all.pts[(size_t)f] : nullptr);
+            if (r != VRAD_OK) rc = r;
+        }
+    };
+    const unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < nt && (int32_t)t < nfaces; t++) pool.emplace_back(work);
+    work();
+    for (auto &t : pool) t.join();
+    return rc;
 }
 
 }  // namespace
@@ -188,24 +207,51 @@ int32_t build_samples_core(const vrad_face *faces, int32_t nfaces, const float *
 extern "C" int32_t vrad_build_samples(const vrad_face *faces, int32_t nfaces, const float *vertices,
                                       int64_t nvertices, vrad_sample *out, int64_t capacity,
                                       int64_t *count, int64_t *face_first) {
-    return build_samples_core(faces, nfaces, vertices, nvertices, out, capacity, count, face_first, nullptr, nullptr);
+    if (!count) return VRAD_ERR_ARG;
+    AllSamples all;
+    const int32_t rc = build_all_samples(faces, nfaces, vertices, nvertices, false, all);
+    if (rc != VRAD_OK) return rc;
+    int64_t written = 0;
+    for (int32_t f = 0; f < nfaces; f++) {
+        if (face_first) face_first[f] = written;
+        const auto &v = all.samples[(size_t)f];
+        if (out) {
+            if (written + (int64_t)v.size() > capacity) {
+                *count = written;
+                return VRAD_ERR_ARG;
+            }
+            std::memcpy(out + written, v.data(), sizeof(vrad_sample) * v.size());
+        }
+        written += (int64_t)v.size();
+    }
+    if (face_first) face_first[nfaces] = written;
+    *count = written;
+    return VRAD_OK;
 }
 
 namespace vrad {
 
 bool sample_windings(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
                      const vrad_sample *given, int64_t ngiven, std::vector<int32_t> &wind, std::vector<float> &pts) {
-    int64_t n = 0;
-    if (build_samples_core(faces, nfaces, vertices, nvertices, nullptr, INT64_MAX, &n, nullptr, nullptr, nullptr) !=
-            VRAD_OK ||
-        n != ngiven)
-        return false;
-    std::vector<vrad_sample> mine((size_t)(n ? n : 1));
+    AllSamples all;
+    if (build_all_samples(faces, nfaces, vertices, nvertices, true, all) != VRAD_OK) return false;
     wind.clear();
     pts.clear();
-    if (build_samples_core(faces, nfaces, vertices, nvertices, mine.data(), n, &n, nullptr, &wind, &pts) != VRAD_OK)
-        return false;
-    return n == 0 || std::memcmp(mine.data(), given, sizeof(vrad_sample) * (size_t)n) == 0;
+    int64_t k = 0;
+    for (int32_t f = 0; f < nfaces; f++) {
+        const auto &v = all.samples[(size_t)f];
+        if (k + (int64_t)v.size() > ngiven) return false;
+        if (!v.empty() && std::memcmp(v.data(), given + k, sizeof(vrad_sample) * v.size()) != 0) return false;
+        const int32_t base = (int32_t)(pts.size() / 3);
+        const auto &wf = all.wind[(size_t)f];
+        for (size_t i = 0; i < wf.size(); i += 2) {
+            wind.push_back(wf[i + 1] ? wf[i] + base : 0);
+            wind.push_back(wf[i + 1]);
+        }
+        pts.insert(pts.end(), all.pts[(size_t)f].begin(), all.pts[(size_t)f].end());
+        k += (int64_t)v.size();
+    }
+    return k == ngiven;
 }
 
 }  // namespace vrad
