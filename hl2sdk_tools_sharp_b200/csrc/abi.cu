@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "context.cuh"
+#include "device_pool.h"
 
 namespace {
 
@@ -215,17 +216,19 @@ int32_t vrad_destroy(vrad_ctx *ctx) {
     {
         std::lock_guard<std::mutex> g(ctx->mu);
         cudaSetDevice(ctx->device);
-        if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+        // Kernels of this context may run on callers' streams too.
+        cudaDeviceSynchronize();
         ctx->scene.release();
         ctx->world.release();
         ctx->final_pass.release();
         ctx->bounce.release();
         ctx->supersample.release();
-        cudaFree(ctx->sample_light);
+        vrad::dev_free(ctx->sample_light);
         cudaFree(ctx->status);
         cudaFree(ctx->d_rays);
         cudaFree(ctx->d_out);
         if (ctx->stream) cudaStreamDestroy(ctx->stream);
+        vrad::dev_trim(ctx->device);
     }
     delete ctx;
     return VRAD_OK;

@@ -56,6 +56,7 @@
 #include <vector>
 
 #include "bounce.cuh"
+#include "device_pool.h"
 #include "context.cuh"
 #include "detmath.cuh"
 #include "mlp.cuh"
@@ -643,7 +644,7 @@ void BounceBuffers::release() {
                     acc, direct, total, emit[0], emit[1], shoot[0], shoot[1], sums, exact, counters, leaf_desc,
                     first, guess, feat, pred,
                     pr_off, pr_patch, pr_box, pr_coord, prad_light, prad_weight};
-    for (void *q : ptrs) cudaFree(q);
+    for (void *q : ptrs) dev_free(q);
     cudaFreeHost(h_sums);
     cudaFreeHost(h_exact);
     *this = BounceBuffers();

@@ -8,6 +8,8 @@
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
+#include <atomic>
+#include <cstdint>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -16,6 +18,8 @@
 #include "bounce.cuh"
 #include "bounce_host.h"
 #include "context.cuh"
+#include "device_pool.h"
+#include "host_parallel.h"
 #include "patches.h"
 #include "setup_clock.h"
 #include "world.h"
@@ -24,9 +28,10 @@ namespace vrad {
 
 namespace {
 
-template <class T>
-cudaError_t upload(T **dst, const std::vector<T> &v) {
-    cudaError_t e = cudaMalloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
+template <class T, class V>
+cudaError_t upload(T **dst, const V &v) {
+    static_assert(sizeof(typename V::value_type) == sizeof(T), "element size");
+    cudaError_t e = dev_alloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
     if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
     return e;
 }
@@ -41,65 +46,77 @@ inline float bits_f(int32_t x) {
 // (BuildPatchRadial): the face's own leaf patches, then each smoothing
 // neighbour's, each list in FacePatches order (descendants by descending
 // index, then the root); each kept with its box in this face's cells when
-// that box holds at least one cell.
+// that box holds at least one cell.  Faces are independent: each builds its
+// list on a worker thread, the lists are concatenated in face order.
 void patch_radial_tables(const std::vector<vrad_face> &faces, const PatchTree &tree, const std::vector<int32_t> &noff,
-                         const std::vector<int32_t> &nlist, std::vector<int32_t> &off, std::vector<int32_t> &patch,
-                         std::vector<int4> &box, std::vector<float4> &coord) {
+                         const std::vector<int32_t> &nlist, std::vector<int32_t> &off, uvector<int32_t> &patch,
+                         uvector<int4> &box, uvector<float4> &coord) {
     const int32_t nf = (int32_t)faces.size();
-    off.assign((size_t)nf + 1, 0);
-    patch.clear();
-    box.clear();
-    coord.clear();
-    auto leaves = [&](int32_t g, std::vector<int32_t> &out) {
-        out.clear();
-        if (tree.face_root[(size_t)g] < 0) return;
-        for (int32_t p = tree.face_end[(size_t)g] - 1; p >= tree.face_first[(size_t)g]; p--)
-            if (tree.patches[(size_t)p].child1 == -1) out.push_back(p);
-        const int32_t r = tree.face_root[(size_t)g];
-        if (tree.patches[(size_t)r].child1 == -1) out.push_back(r);
+    struct Entry {
+        int32_t patch;
+        int4 box;
+        float4 coord;
     };
-    std::vector<int32_t> list;
-    for (int32_t f = 0; f < nf; f++) {
+    std::vector<std::vector<Entry>> lists((size_t)nf);
+    parallel_for(nf, 8, [&](int64_t fi) {
+        const int32_t f = (int32_t)fi;
         FaceFrameOut me;
         face_frame_of(faces[(size_t)f], me);
-        std::vector<int32_t> order = {f};
-        for (int32_t q = noff[(size_t)f]; q < noff[(size_t)f + 1]; q++) order.push_back(nlist[(size_t)q]);
-        for (int32_t g : order) {
-            leaves(g, list);
-            for (int32_t p : list) {
-                const vrad_patch &pt = tree.patches[(size_t)p];
-                // PatchLightmapCoordRange.
-                float min_s = 1e30f, min_t = 1e30f, max_s = -1e30f, max_t = -1e30f;
-                for (int32_t k = 0; k < pt.num_points; k++) {
-                    float s, t;
-                    frame_world_to_luxel(me, &tree.points[3 * (size_t)(pt.first_point + k)], s, t);
-                    min_s = min_s < s ? min_s : s;
-                    max_s = max_s > s ? max_s : s;
-                    min_t = min_t < t ? min_t : t;
-                    max_t = max_t > t ? max_t : t;
-                }
-                // LuxelRadial.AddBounced's extent and box.
-                float cs, ct;
-                frame_world_to_luxel(me, pt.origin, cs, ct);
-                float ds = max_s - min_s, dt = max_t - min_t;
-                ds = (float)(1.0 > (double)ds ? 1.0 : (double)ds);
-                dt = (float)(1.0 > (double)dt ? 1.0 : (double)dt);
-                int smin = (int)((double)cs - (double)ds * 1.42);
-                int tmin = (int)((double)ct - (double)dt * 1.42);
-                int smax = (int)((double)cs + (double)ds * 1.42 + 1.0);
-                int tmax = (int)((double)ct + (double)dt * 1.42 + 1.0);
-                smin = std::max(smin, 0);
-                tmin = std::max(tmin, 0);
-                smax = std::min(smax, me.width);
-                tmax = std::min(tmax, me.height);
-                if (smin >= smax || tmin >= tmax) continue;
-                patch.push_back(p);
-                box.push_back(make_int4(smin, tmin, smax, tmax));
-                coord.push_back(make_float4(cs, ct, ds, dt));
+        std::vector<Entry> &out = lists[(size_t)f];
+        auto visit = [&](int32_t p) {
+            const vrad_patch &pt = tree.patches[(size_t)p];
+            if (pt.child1 != -1) return;
+            // PatchLightmapCoordRange.
+            float min_s = 1e30f, min_t = 1e30f, max_s = -1e30f, max_t = -1e30f;
+            for (int32_t k = 0; k < pt.num_points; k++) {
+                float s, t;
+                frame_world_to_luxel(me, &tree.points[3 * (size_t)(pt.first_point + k)], s, t);
+                min_s = min_s < s ? min_s : s;
+                max_s = max_s > s ? max_s : s;
+                min_t = min_t < t ? min_t : t;
+                max_t = max_t > t ? max_t : t;
             }
+            // LuxelRadial.AddBounced's extent and box.
+            float cs, ct;
+            frame_world_to_luxel(me, pt.origin, cs, ct);
+            float ds = max_s - min_s, dt = max_t - min_t;
+            ds = (float)(1.0 > (double)ds ? 1.0 : (double)ds);
+            dt = (float)(1.0 > (double)dt ? 1.0 : (double)dt);
+            int smin = (int)((double)cs - (double)ds * 1.42);
+            int tmin = (int)((double)ct - (double)dt * 1.42);
+            int smax = (int)((double)cs + (double)ds * 1.42 + 1.0);
+            int tmax = (int)((double)ct + (double)dt * 1.42 + 1.0);
+            smin = std::max(smin, 0);
+            tmin = std::max(tmin, 0);
+            smax = std::min(smax, me.width);
+            tmax = std::min(tmax, me.height);
+            if (smin >= smax || tmin >= tmax) return;
+            out.push_back(Entry{p, make_int4(smin, tmin, smax, tmax), make_float4(cs, ct, ds, dt)});
+        };
+        auto face_leaves = [&](int32_t g) {
+            const int32_t r = tree.face_root[(size_t)g];
+            if (r < 0) return;
+            for (int32_t p = tree.face_end[(size_t)g] - 1; p >= tree.face_first[(size_t)g]; p--) visit(p);
+            visit(r);
+        };
+        face_leaves(f);
+        for (int32_t q = noff[(size_t)f]; q < noff[(size_t)f + 1]; q++) face_leaves(nlist[(size_t)q]);
+    });
+    off.assign((size_t)nf + 1, 0);
+    for (int32_t f = 0; f < nf; f++) off[(size_t)f + 1] = off[(size_t)f] + (int32_t)lists[(size_t)f].size();
+    const size_t total = (size_t)off[(size_t)nf];
+    patch.resize(total);
+    box.resize(total);
+    coord.resize(total);
+    parallel_for(nf, 8, [&](int64_t f) {
+        size_t k = (size_t)off[(size_t)f];
+        for (const Entry &e : lists[(size_t)f]) {
+            patch[k] = e.patch;
+            box[k] = e.box;
+            coord[k] = e.coord;
+            k++;
         }
-        off[(size_t)f + 1] = (int32_t)patch.size();
-    }
+    });
 }
 
 }  // namespace
@@ -225,6 +242,9 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
 
     SetupClock clock("bounce_upload");
     cudaError_t e = cudaSetDevice(ctx->device);
+    // The old bounce's blocks go back to the device pool: no kernel of
+    // this context, on any stream, may still read them.
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
     BounceBuffers &b = ctx->bounce;
     b.release();
@@ -238,27 +258,37 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     const int32_t P = (int32_t)tree.patches.size();
     clock.mark("patch tree");
 
-    // Per patch.
-    std::vector<float4> origin((size_t)P), normal((size_t)P), mins((size_t)P), maxs((size_t)P), refl((size_t)P);
-    std::vector<int4> tr((size_t)P);
-    std::vector<int2> wind((size_t)P);
-    int32_t nleaves = 0;
-    for (int32_t i = 0; i < P; i++) {
-        const vrad_patch &p = tree.patches[(size_t)i];
-        if (p.cluster < 0 || p.cluster >= C)
-            return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "patch %d lies outside every cluster", i);
-        origin[(size_t)i] = make_float4(p.origin[0], p.origin[1], p.origin[2], p.area);
-        normal[(size_t)i] = make_float4(p.normal[0], p.normal[1], p.normal[2], p.plane_dist);
-        mins[(size_t)i] = make_float4(p.mins[0], p.mins[1], p.mins[2], bits_f(p.face));
-        maxs[(size_t)i] = make_float4(p.maxs[0], p.maxs[1], p.maxs[2], bits_f(p.cluster));
-        refl[(size_t)i] = make_float4(p.reflectivity[0], p.reflectivity[1], p.reflectivity[2], 0.0f);
-        tr[(size_t)i] = make_int4(p.parent, p.child1, p.child2, p.sky);
-        wind[(size_t)i] = make_int2(p.first_point, p.num_points);
-        if (p.child1 == -1 && !p.sky) nleaves++;
-    }
-    std::vector<float4> points(tree.points.size() / 3);
-    for (size_t k = 0; k < points.size(); k++)
-        points[k] = make_float4(tree.points[3 * k], tree.points[3 * k + 1], tree.points[3 * k + 2], 0.0f);
+    // Per patch, in parallel: the device's SoA rows, and each leaf's
+    // cluster for the receiver order.
+    uvector<float4> origin((size_t)P), normal((size_t)P), mins((size_t)P), maxs((size_t)P), refl((size_t)P);
+    uvector<int4> tr((size_t)P);
+    uvector<int2> wind((size_t)P);
+    uvector<int32_t> leaf_cluster((size_t)P);
+    std::atomic<int32_t> bad{INT32_MAX};
+    parallel_for(P, 4096, [&](int64_t ii) {
+        const size_t i = (size_t)ii;
+        const vrad_patch &p = tree.patches[i];
+        if (p.cluster < 0 || p.cluster >= C) {
+            int32_t cur = bad.load();
+            while ((int32_t)ii < cur && !bad.compare_exchange_weak(cur, (int32_t)ii)) {
+            }
+        }
+        origin[i] = make_float4(p.origin[0], p.origin[1], p.origin[2], p.area);
+        normal[i] = make_float4(p.normal[0], p.normal[1], p.normal[2], p.plane_dist);
+        mins[i] = make_float4(p.mins[0], p.mins[1], p.mins[2], bits_f(p.face));
+        maxs[i] = make_float4(p.maxs[0], p.maxs[1], p.maxs[2], bits_f(p.cluster));
+        refl[i] = make_float4(p.reflectivity[0], p.reflectivity[1], p.reflectivity[2], 0.0f);
+        tr[i] = make_int4(p.parent, p.child1, p.child2, p.sky);
+        wind[i] = make_int2(p.first_point, p.num_points);
+        leaf_cluster[i] = p.child1 == -1 ? p.cluster : -1;
+    });
+    if (bad.load() != INT32_MAX)
+        return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "patch %d lies outside every cluster", bad.load());
+    uvector<float4> points(tree.points.size() / 3);
+    parallel_for((int64_t)points.size(), 1 << 16, [&](int64_t k) {
+        const float *q = &tree.points[3 * (size_t)k];
+        points[(size_t)k] = make_float4(q[0], q[1], q[2], 0.0f);
+    });
     // Per face.
     std::vector<int4> face_range((size_t)nf);
     std::vector<int2> face_samples((size_t)nf, make_int2(0, 0));
@@ -268,24 +298,37 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
         const vrad_face &fc = ctx->h_faces[(size_t)f];
         face_plane[(size_t)f] = make_float4(fc.normal[0], fc.normal[1], fc.normal[2], fc.dist);
     }
-    std::vector<float> sample_area(ctx->h_samples.size());
-    for (size_t k = 0; k < ctx->h_samples.size(); k++) {
-        const vrad_sample &sm = ctx->h_samples[k];
-        sample_area[k] = sm.area;
-        int2 &fs = face_samples[(size_t)sm.face];
-        if (fs.y == 0) fs.x = (int32_t)k;
-        fs.y++;
-    }
+    // Each face's sample run (the world upload checked that a face's
+    // samples are contiguous): its first sample and count.
+    const int64_t S = (int64_t)ctx->h_samples.size();
+    const vrad_sample *sm = ctx->h_samples.data();
+    uvector<float> sample_area((size_t)S);
+    parallel_for(S, 1 << 15, [&](int64_t k) {
+        sample_area[(size_t)k] = sm[k].area;
+        const int32_t f = sm[k].face;
+        if (k == 0 || sm[k - 1].face != f) face_samples[(size_t)f].x = (int32_t)k;
+        if (k + 1 == S || sm[k + 1].face != f) face_samples[(size_t)f].y = (int32_t)(k + 1);
+    });
+    for (int32_t f = 0; f < nf; f++)
+        if (face_samples[(size_t)f].y) face_samples[(size_t)f].y -= face_samples[(size_t)f].x;
     clock.mark("patch tables");
-    // VisMatrix.ReceiverOrder: cluster by cluster, leaf patches in index order.
-    std::vector<std::vector<int32_t>> by_cluster((size_t)C);
+    // VisMatrix.ReceiverOrder: cluster by cluster, leaf patches in index
+    // order (a stable counting sort on the leaves' clusters).
+    std::vector<int32_t> cstart((size_t)C + 1, 0);
     for (int32_t i = 0; i < P; i++)
-        if (tree.patches[(size_t)i].child1 == -1) by_cluster[(size_t)tree.patches[(size_t)i].cluster].push_back(i);
-    std::vector<int32_t> recv;
-    for (const auto &v : by_cluster) recv.insert(recv.end(), v.begin(), v.end());
+        if (leaf_cluster[(size_t)i] >= 0) cstart[(size_t)leaf_cluster[(size_t)i] + 1]++;
+    for (int32_t c = 0; c < C; c++) cstart[(size_t)c + 1] += cstart[(size_t)c];
+    std::vector<int32_t> recv((size_t)cstart[(size_t)C]);
+    {
+        std::vector<int32_t> at(cstart.begin(), cstart.end() - 1);
+        for (int32_t i = 0; i < P; i++)
+            if (leaf_cluster[(size_t)i] >= 0) recv[(size_t)at[(size_t)leaf_cluster[(size_t)i]]++] = i;
+    }
     std::vector<int32_t> leaf_desc;
+    leaf_desc.reserve(recv.size());
     for (int32_t i = P - 1; i >= 0; i--)
-        if (tree.patches[(size_t)i].child1 == -1 && !tree.patches[(size_t)i].sky) leaf_desc.push_back(i);
+        if (tr[(size_t)i].y == -1 && !tr[(size_t)i].w) leaf_desc.push_back(i);
+    const int32_t nleaves = (int32_t)leaf_desc.size();
     // FacesInRow: each visible cluster's faces, in face order (one leaf per
     // cluster, whose faces are the faces that lie in it).
     std::vector<std::vector<int32_t>> cluster_faces((size_t)C);
@@ -299,19 +342,15 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
         row_off[(size_t)c + 1] = (int32_t)row_faces.size();
     }
     clock.mark("receivers and rows");
-    // The final pass's patch tables over the smoothing neighbours.
-    std::vector<int32_t> noff((size_t)nf + 1);
-    int64_t nn = 0;
-    if (vrad_build_neighbours(ctx->h_faces.data(), nf, ctx->h_vertices.data(), nvert, 0.7071067f, noff.data(), nullptr, 0,
-                              &nn) != VRAD_OK)
-        return vrad_fail(ctx, VRAD_ERR_ARG, "invalid face windings");
-    std::vector<int32_t> nlist((size_t)(nn ? nn : 1));
-    vrad_build_neighbours(ctx->h_faces.data(), nf, ctx->h_vertices.data(), nvert, 0.7071067f, noff.data(), nlist.data(), nn,
-                          &nn);
+    // The final pass's patch tables over the smoothing neighbours (the
+    // world upload's).
+    if (ctx->h_noff.size() != (size_t)nf + 1) return vrad_fail(ctx, VRAD_ERR_ARG, "the world has no smoothing neighbours");
+    const std::vector<int32_t> &noff = ctx->h_noff, &nlist = ctx->h_nlist;
     clock.mark("neighbours");
-    std::vector<int32_t> pr_off, pr_patch;
-    std::vector<int4> pr_box;
-    std::vector<float4> pr_coord;
+    std::vector<int32_t> pr_off;
+    uvector<int32_t> pr_patch;
+    uvector<int4> pr_box;
+    uvector<float4> pr_coord;
     patch_radial_tables(ctx->h_faces, tree, noff, nlist, pr_off, pr_patch, pr_box, pr_coord);
 
     clock.mark("patch radial tables");
@@ -337,26 +376,27 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     if (e == cudaSuccess) e = upload(&b.pr_patch, pr_patch);
     if (e == cudaSuccess) e = upload(&b.pr_box, pr_box);
     if (e == cudaSuccess) e = upload(&b.pr_coord, pr_coord);
+    clock.mark("tables copied");
     const size_t P1 = (size_t)(P ? P : 1), R1 = (size_t)R + 1, N1 = (size_t)(ncells ? ncells : 1);
-    if (e == cudaSuccess) e = cudaMalloc(&b.cand_off, sizeof(int64_t) * R1);
-    if (e == cudaSuccess) e = cudaMalloc(&b.tr_off, sizeof(int64_t) * R1);
+    if (e == cudaSuccess) e = dev_alloc(&b.cand_off, sizeof(int64_t) * R1);
+    if (e == cudaSuccess) e = dev_alloc(&b.tr_off, sizeof(int64_t) * R1);
     for (float4 **q : {&b.acc, &b.direct, &b.total, &b.emit[0], &b.emit[1], &b.shoot[0], &b.shoot[1]})
-        if (e == cudaSuccess) e = cudaMalloc(q, sizeof(float4) * P1);
-    if (e == cudaSuccess) e = cudaMalloc(&b.sums, 6 * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&b.exact, 3 * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&b.counters, 3 * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = dev_alloc(q, sizeof(float4) * P1);
+    if (e == cudaSuccess) e = dev_alloc(&b.sums, 6 * sizeof(double));
+    if (e == cudaSuccess) e = dev_alloc(&b.exact, 3 * sizeof(float));
+    if (e == cudaSuccess) e = dev_alloc(&b.counters, 3 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMallocHost(&b.h_sums, 6 * sizeof(double));
     if (e == cudaSuccess) e = cudaMallocHost(&b.h_exact, 3 * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&b.first, sizeof(float4) * P1);
-    if (e == cudaSuccess) e = cudaMalloc(&b.guess, sizeof(float4) * P1);
-    if (e == cudaSuccess) e = cudaMalloc(&b.feat, sizeof(uint16_t) * kFeatures * (size_t)(R ? R : 1));
-    if (e == cudaSuccess) e = cudaMalloc(&b.pred, sizeof(float) * 3 * (size_t)(R ? R : 1));
-    if (e == cudaSuccess) e = cudaMalloc(&b.prad_light, sizeof(float4) * N1);
-    if (e == cudaSuccess) e = cudaMalloc(&b.prad_weight, sizeof(float) * N1);
+    if (e == cudaSuccess) e = dev_alloc(&b.first, sizeof(float4) * P1);
+    if (e == cudaSuccess) e = dev_alloc(&b.guess, sizeof(float4) * P1);
+    if (e == cudaSuccess) e = dev_alloc(&b.feat, sizeof(uint16_t) * kFeatures * (size_t)(R ? R : 1));
+    if (e == cudaSuccess) e = dev_alloc(&b.pred, sizeof(float) * 3 * (size_t)(R ? R : 1));
+    if (e == cudaSuccess) e = dev_alloc(&b.prad_light, sizeof(float4) * N1);
+    if (e == cudaSuccess) e = dev_alloc(&b.prad_weight, sizeof(float) * N1);
     if (e == cudaSuccess && R > 0) {
         size_t need = 0;
         e = cub::DeviceScan::InclusiveSum(nullptr, need, b.cand_off + 1, b.cand_off + 1, R);
-        if (e == cudaSuccess) e = cudaMalloc(&b.scan_tmp, need ? need : 1);
+        if (e == cudaSuccess) e = dev_alloc(&b.scan_tmp, need ? need : 1);
         b.scan_tmp_bytes = need;
     }
     if (e != cudaSuccess) {
@@ -381,12 +421,13 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     if (e == cudaSuccess && R > 0) e = cudaMemcpyAsync(&ncand, b.cand_off + R, sizeof ncand, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     b.ncand = ncand;
-    if (e == cudaSuccess) e = cudaMalloc(&b.cand_src, sizeof(int32_t) * (size_t)(ncand ? ncand : 1));
-    if (e == cudaSuccess) e = cudaMalloc(&b.cand_w, sizeof(float) * (size_t)(ncand ? ncand : 1));
+    clock.mark("candidate count");
+    if (e == cudaSuccess) e = dev_alloc(&b.cand_src, sizeof(int32_t) * (size_t)(ncand ? ncand : 1));
+    if (e == cudaSuccess) e = dev_alloc(&b.cand_w, sizeof(float) * (size_t)(ncand ? ncand : 1));
     // Transfers are at most the candidates: the list array takes that
     // bound, so sizing needs no trace.
     uint32_t overflow = 0;
-    if (e == cudaSuccess) e = cudaMalloc(&b.tr, sizeof(int2) * (size_t)(ncand ? ncand : 1));
+    if (e == cudaSuccess) e = dev_alloc(&b.tr, sizeof(int2) * (size_t)(ncand ? ncand : 1));
     if (e == cudaSuccess) e = cudaMemcpyAsync(&overflow, ctx->status, sizeof overflow, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {

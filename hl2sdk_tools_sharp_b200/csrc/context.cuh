@@ -10,6 +10,7 @@
 #include "bounce.cuh"
 #include "direct.cuh"
 #include "final.cuh"
+#include "host_parallel.h"
 #include "scene.cuh"
 #include "supersample.cuh"
 
@@ -32,7 +33,10 @@ struct vrad_ctx {
     // Host copies of the uploaded world the bounce set-up reads.
     std::vector<vrad_face> h_faces;
     std::vector<float> h_vertices;
-    std::vector<vrad_sample> h_samples;
+    vrad::uvector<vrad_sample> h_samples;
+    // The smoothing neighbours (FaceNeighbours, threshold 0.7071067) of
+    // h_faces: face f's are h_nlist[h_noff[f] .. h_noff[f + 1]).
+    std::vector<int32_t> h_noff, h_nlist;
     int32_t nclusters = 0;
     vrad::BounceBuffers bounce;
     const vrad_mlp *bounce_model = nullptr;  // the warm start's network, or none

@@ -19,11 +19,16 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <cstdint>
+#include <cstring>
 #include <string>
 #include <vector>
 
 #include "context.cuh"
+#include "device_pool.h"
 #include "gather.cuh"
+#include "host_parallel.h"
 #include "setup_clock.h"
 #include "supersample.cuh"
 
@@ -81,15 +86,15 @@ __global__ void __launch_bounds__(BLOCK) k_direct(DeviceScene sc, DeviceWorld w,
 }  // namespace
 
 void WorldBuffers::release() {
-    cudaFree(slots);
-    cudaFree(sample_pos);
-    cudaFree(face_normal);
-    cudaFree(lights);
-    cudaFree(cl_off);
-    cudaFree(cl_list);
-    cudaFree(dirs);
-    cudaFree(jitter);
-    cudaFree(counters);
+    dev_free(slots);
+    dev_free(sample_pos);
+    dev_free(face_normal);
+    dev_free(lights);
+    dev_free(cl_off);
+    dev_free(cl_list);
+    dev_free(dirs);
+    dev_free(jitter);
+    dev_free(counters);
     slots = nullptr;
     sample_pos = face_normal = lights = dirs = jitter = nullptr;
     cl_off = cl_list = nullptr;
@@ -121,9 +126,9 @@ cudaError_t launch_direct(const DeviceScene &scene, const DeviceWorld &world, fl
 
 namespace {
 
-template <class T>
-cudaError_t upload_vec(T **dst, const std::vector<T> &v) {
-    cudaError_t e = cudaMalloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
+template <class T, class A>
+cudaError_t upload_vec(T **dst, const std::vector<T, A> &v) {
+    cudaError_t e = vrad::dev_alloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
     if (e == cudaSuccess && !v.empty())
         e = cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
     return e;
@@ -154,26 +159,44 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
         if (w->cluster_lights[k] < 0 || w->cluster_lights[k] >= nl)
             return vrad_fail(ctx, VRAD_ERR_ARG, "cluster light list names light %d", w->cluster_lights[k]);
 
-    // Samples: positions, and each face's run [start, end).
-    std::vector<float4> pos((size_t)w->nsamples);
+    // Samples: the runs of one face (marked in parallel, walked in one
+    // scan), then the runs' cluster checks and positions in parallel.
+    const int64_t ns = w->nsamples;
+    vrad::uvector<uint8_t> run_start((size_t)ns + 1);
+    vrad::parallel_for(ns, 1 << 16, [&](int64_t k) {
+        run_start[(size_t)k] = k == 0 || w->samples[k - 1].face != w->samples[k].face;
+    });
+    run_start[(size_t)ns] = 1;
     std::vector<int64_t> fstart((size_t)w->nfaces, -1), fend((size_t)w->nfaces, -1);
+    std::vector<int32_t> run_face;
     int64_t i = 0;
-    while (i < w->nsamples) {
+    while (i < ns) {
         const int32_t face = w->samples[i].face;
         if (face < 0 || face >= w->nfaces) return vrad_fail(ctx, VRAD_ERR_ARG, "sample %lld names face %d", (long long)i, face);
         if (fstart[(size_t)face] != -1)
             return vrad_fail(ctx, VRAD_ERR_ARG, "face %d's samples are not contiguous", face);
-        int64_t j = i;
-        while (j < w->nsamples && w->samples[j].face == face) j++;
+        const uint8_t *next = static_cast<const uint8_t *>(memchr(&run_start[(size_t)i + 1], 1, (size_t)(ns - i)));
+        const int64_t j = next - run_start.data();
         const int32_t cl = w->faces[face].cluster;
         if (cl < 0 || cl >= w->nclusters)
             return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "face %d has cluster %d outside the light lists", face, cl);
-        for (int64_t s = i; s < j; s++) {
-            if (w->samples[s].cluster != cl)
-                return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED,
-                                 "sample %lld is in cluster %d, its face in %d: mixed-cluster groups are not supported",
-                                 (long long)s, w->samples[s].cluster, cl);
+        fstart[(size_t)face] = i;
+        fend[(size_t)face] = j;
+        run_face.push_back(face);
+        i = j;
+    }
+    vrad::uvector<float4> pos((size_t)w->nsamples);
+    std::atomic<int64_t> mixed{INT64_MAX};
+    vrad::parallel_for((int64_t)run_face.size(), 16, [&](int64_t r) {
+        const int32_t face = run_face[(size_t)r];
+        const int32_t cl = w->faces[face].cluster;
+        for (int64_t s = fstart[(size_t)face]; s < fend[(size_t)face]; s++) {
             const vrad_sample &sm = w->samples[s];
+            if (sm.cluster != cl) {
+                int64_t cur = mixed.load();
+                while (s < cur && !mixed.compare_exchange_weak(cur, s)) {
+                }
+            }
             float4 p;
             p.x = sm.position[0];
             p.y = sm.position[1];
@@ -182,9 +205,12 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
             memcpy(&p.w, &f, 4);
             pos[(size_t)s] = p;
         }
-        fstart[(size_t)face] = i;
-        fend[(size_t)face] = j;
-        i = j;
+    });
+    if (mixed.load() != INT64_MAX) {
+        const int64_t s = mixed.load();
+        return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED,
+                         "sample %lld is in cluster %d, its face in %d: mixed-cluster groups are not supported",
+                         (long long)s, w->samples[s].cluster, w->faces[w->samples[s].face].cluster);
     }
     clock.mark("samples");
     // Slots, cluster by cluster: each face's samples in whole groups of
@@ -243,6 +269,9 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     clock.mark("slots and lights");
     std::lock_guard<std::mutex> g(ctx->mu);
     cudaError_t e = cudaSetDevice(ctx->device);
+    // The old world's blocks go back to the device pool: no kernel of this
+    // context, on any stream, may still read them.
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     vrad::WorldBuffers &wb = ctx->world;
     wb.release();
     if (e == cudaSuccess) e = upload_vec(&wb.slots, slots);
@@ -253,7 +282,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     if (e == cudaSuccess) e = upload_vec(&wb.cl_list, cl_list);
     if (e == cudaSuccess) e = upload_vec(&wb.dirs, dirs);
     if (e == cudaSuccess) e = upload_vec(&wb.jitter, jit);
-    if (e == cudaSuccess) e = cudaMalloc(&wb.counters, 3 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = vrad::dev_alloc(&wb.counters, 3 * sizeof(unsigned long long));
     if (e != cudaSuccess) {
         wb.release();
         return vrad_cuda_fail(ctx, e, "world upload");
@@ -265,18 +294,23 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     // The final pass's tables, and the direct gather's output buffer.  A
     // new world drops the old bounce.
     ctx->bounce.release();
+    clock.mark("bounce released");
     ctx->h_faces.assign(w->faces, w->faces + w->nfaces);
-    ctx->h_samples.assign(w->samples, w->samples + w->nsamples);
+    ctx->h_samples.resize((size_t)w->nsamples);
+    vrad::parallel_for(w->nsamples, 1 << 16, [&](int64_t k) { ctx->h_samples[(size_t)k] = w->samples[k]; });
+    ctx->h_noff.clear();
+    ctx->h_nlist.clear();
     if (w->vertices && w->nvertices > 0) ctx->h_vertices.assign(w->vertices, w->vertices + 3 * w->nvertices);
     else ctx->h_vertices.clear();
     ctx->nclusters = w->nclusters;
     ctx->final_pass.release();
-    cudaFree(ctx->sample_light);
+    vrad::dev_free(ctx->sample_light);
     ctx->sample_light = nullptr;
+    clock.mark("host copies");
     if (w->vertices && w->nvertices > 0) {
         std::string why;
         e = vrad::build_final(ctx->final_pass, w->faces, w->nfaces, w->samples, w->nsamples, w->vertices,
-                              w->nvertices, why);
+                              w->nvertices, ctx->h_noff, ctx->h_nlist, why);
         if (e != cudaSuccess) {
             wb.release();
             if (e == cudaErrorInvalidValue) return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "final pass: %s", why.c_str());
@@ -298,7 +332,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
         ctx->supersample.release();
         ctx->supersample_why = "the world was uploaded without face windings";
     }
-    e = cudaMalloc(&ctx->sample_light, sizeof(float4) * (size_t)(w->nsamples ? w->nsamples : 1));
+    e = vrad::dev_alloc(&ctx->sample_light, sizeof(float4) * (size_t)(w->nsamples ? w->nsamples : 1));
     if (e != cudaSuccess) {
         wb.release();
         ctx->final_pass.release();
@@ -352,12 +386,12 @@ extern "C" int32_t vrad_direct_lighting(vrad_ctx *ctx, vrad_lighting_value *out,
     cudaError_t e = cudaSetDevice(ctx->device);
     float4 *d_out = nullptr;
     cudaEvent_t a = nullptr, b = nullptr;
-    if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(float4) * (size_t)(n ? n : 1));
+    if (e == cudaSuccess) e = vrad::dev_alloc(&d_out, sizeof(float4) * (size_t)(n ? n : 1));
     if (e == cudaSuccess) e = cudaEventCreate(&a);
     if (e == cudaSuccess) e = cudaEventCreate(&b);
     if (e == cudaSuccess) e = cudaEventRecord(a, ctx->stream);
     if (e != cudaSuccess) {
-        cudaFree(d_out);
+        vrad::dev_free(d_out);
         if (a) cudaEventDestroy(a);
         return vrad_cuda_fail(ctx, e, "direct lighting set-up");
     }
@@ -389,7 +423,7 @@ extern "C" int32_t vrad_direct_lighting(vrad_ctx *ctx, vrad_lighting_value *out,
         stats->extra_passes_run = ctx->supersample.passes_run;
         stats->supersampled = ctx->supersample.supersampled;
     }
-    cudaFree(d_out);
+    vrad::dev_free(d_out);
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     return rc;
@@ -404,7 +438,7 @@ extern "C" int32_t vrad_direct_autotune(vrad_ctx *ctx, int32_t *chosen_block, fl
     const int64_t n = ctx->world.view.nsamples;
     float4 *d_out = nullptr;
     cudaEvent_t a = nullptr, b = nullptr;
-    if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(float4) * (size_t)(n ? n : 1));
+    if (e == cudaSuccess) e = vrad::dev_alloc(&d_out, sizeof(float4) * (size_t)(n ? n : 1));
     if (e == cudaSuccess) e = cudaEventCreate(&a);
     if (e == cudaSuccess) e = cudaEventCreate(&b);
     const int candidates[3] = {32, 64, 128};
@@ -425,7 +459,7 @@ extern "C" int32_t vrad_direct_autotune(vrad_ctx *ctx, int32_t *chosen_block, fl
             best_block = candidates[k];
         }
     }
-    cudaFree(d_out);
+    vrad::dev_free(d_out);
     if (a) cudaEventDestroy(a);
     if (b) cudaEventDestroy(b);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "direct autotune");

@@ -22,6 +22,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cfloat>
 #include <vector>
 
@@ -30,7 +31,9 @@
 
 #include "bounce_host.h"
 #include "context.cuh"
+#include "device_pool.h"
 #include "final.cuh"
+#include "host_parallel.h"
 #include "setup_clock.h"
 #include "world.h"
 
@@ -308,18 +311,18 @@ __global__ void __launch_bounds__(kMedianThreads) k_median(FinalView v, const fl
 }  // namespace
 
 void FinalBuffers::release() {
-    cudaFree(frames);
-    cudaFree(face_cells);
-    cudaFree(face_nsamples);
-    cudaFree(cell_face);
-    cudaFree(cell_sample);
-    cudaFree(sample_box);
-    cudaFree(cand_off);
-    cudaFree(cand_sample);
-    cudaFree(cand_box);
-    cudaFree(rad_light);
-    cudaFree(rad_weight);
-    cudaFree(flat);
+    dev_free(frames);
+    dev_free(face_cells);
+    dev_free(face_nsamples);
+    dev_free(cell_face);
+    dev_free(cell_sample);
+    dev_free(sample_box);
+    dev_free(cand_off);
+    dev_free(cand_sample);
+    dev_free(cand_box);
+    dev_free(rad_light);
+    dev_free(rad_weight);
+    dev_free(flat);
     *this = FinalBuffers();
 }
 
@@ -338,28 +341,35 @@ cudaError_t launch_final(const FinalView &v, const float4 *sample_light, float4 
 
 // Host-side set-up of the final pass from the uploaded world.
 cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces, const vrad_sample *samples,
-                        int64_t nsamples, const float *vertices, int64_t nvertices, std::string &why) {
+                        int64_t nsamples, const float *vertices, int64_t nvertices, std::vector<int32_t> &noff,
+                        std::vector<int32_t> &nlist, std::string &why) {
     fb.release();
     SetupClock clock("final_tables");
     std::vector<FaceFrameOut> fr((size_t)nfaces);
     for (int32_t f = 0; f < nfaces; f++) face_frame_of(faces[f], fr[(size_t)f]);
-    // Neighbours (FaceNeighbours.Build, DefaultSmoothingThreshold).
-    std::vector<int32_t> noff((size_t)nfaces + 1);
+    // Neighbours (FaceNeighbours.Build, DefaultSmoothingThreshold), kept
+    // for the bounce's set-up.
+    noff.assign((size_t)nfaces + 1, 0);
     int64_t nn = 0;
     if (vrad_build_neighbours(faces, nfaces, vertices, nvertices, 0.7071067f, noff.data(), nullptr, 0, &nn) != VRAD_OK) {
         why = "invalid face windings";
         return cudaErrorInvalidValue;
     }
-    std::vector<int32_t> nlist((size_t)(nn ? nn : 1));
+    nlist.assign((size_t)(nn ? nn : 1), 0);
     vrad_build_neighbours(faces, nfaces, vertices, nvertices, 0.7071067f, noff.data(), nlist.data(), nn, &nn);
     clock.mark("neighbours");
     std::vector<int32_t> lightofs((size_t)nfaces);
     int64_t total = 0;
     vrad_lightmap_layout(faces, nfaces, lightofs.data(), &total);
-    // Each face's sample run.
-    std::vector<int64_t> sfirst((size_t)nfaces + 1, 0), scount((size_t)nfaces, 0);
-    for (int64_t i = 0; i < nsamples; i++) scount[(size_t)samples[i].face]++;
-    for (int32_t f = 0; f < nfaces; f++) sfirst[(size_t)f + 1] = sfirst[(size_t)f] + scount[(size_t)f];
+    // Each face's sample run [sfirst, send) (the world upload checked
+    // that a face's samples are contiguous; runs need not be in face order).
+    std::vector<int64_t> sfirst((size_t)nfaces, 0), send((size_t)nfaces, 0), scount((size_t)nfaces, 0);
+    parallel_for(nsamples, 1 << 16, [&](int64_t k) {
+        const int32_t f = samples[k].face;
+        if (k == 0 || samples[k - 1].face != f) sfirst[(size_t)f] = k;
+        if (k + 1 == nsamples || samples[k + 1].face != f) send[(size_t)f] = k + 1;
+    });
+    for (int32_t f = 0; f < nfaces; f++) scount[(size_t)f] = send[(size_t)f] - sfirst[(size_t)f];
     // Frames, cells, own-sample cell table.
     std::vector<float4> frames((size_t)nfaces * 5);
     std::vector<int32_t> face_cells((size_t)nfaces + 1, 0), face_ns((size_t)nfaces);
@@ -383,31 +393,45 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
         face_ns[(size_t)f] = (int32_t)scount[(size_t)f];
     }
     const int64_t ncells = face_cells[(size_t)nfaces];
-    std::vector<int32_t> cell_face((size_t)ncells), cell_sample((size_t)ncells, -1);
-    for (int32_t f = 0; f < nfaces; f++)
-        for (int32_t c = face_cells[(size_t)f]; c < face_cells[(size_t)f + 1]; c++) cell_face[(size_t)c] = f;
-    std::vector<float4> sbox((size_t)nsamples);
-    for (int64_t i = 0; i < nsamples; i++) {
+    uvector<int32_t> cell_face((size_t)ncells), cell_sample((size_t)ncells);
+    parallel_for(nfaces, 16, [&](int64_t f) {
+        for (int32_t c = face_cells[(size_t)f]; c < face_cells[(size_t)f + 1]; c++) {
+            cell_face[(size_t)c] = (int32_t)f;
+            cell_sample[(size_t)c] = -1;
+        }
+    });
+    uvector<float4> sbox((size_t)nsamples);
+    std::atomic<bool> outside{false};
+    parallel_for(nsamples, 1 << 15, [&](int64_t i) {
         const vrad_sample &sm = samples[i];
         const FaceFrameOut &q = fr[(size_t)sm.face];
         if (sm.s < 0 || sm.s >= q.width || sm.t < 0 || sm.t >= q.height) {
-            why = "a sample's cell lies outside its face's lightmap";
-            return cudaErrorInvalidValue;
+            outside = true;
+            return;
         }
         cell_sample[(size_t)(face_cells[(size_t)sm.face] + sm.s + sm.t * q.width)] = (int32_t)i;
         sbox[(size_t)i] = make_float4(sm.mins[0], sm.mins[1], sm.maxs[0], sm.maxs[1]);
+    });
+    if (outside) {
+        why = "a sample's cell lies outside its face's lightmap";
+        return cudaErrorInvalidValue;
     }
     clock.mark("frames and cells");
     // Neighbour candidates: each neighbour's samples whose box, moved into
-    // this face's luxel space as BuildLuxelRadial moves it, can cover a cell.
-    std::vector<int32_t> cand_off((size_t)nfaces + 1, 0), cand_sample;
-    std::vector<float4> cand_box;
-    for (int32_t f = 0; f < nfaces; f++) {
-        const FaceFrameOut &me = fr[(size_t)f];
-        for (int32_t q = noff[(size_t)f]; q < noff[(size_t)f + 1]; q++) {
+    // this face's luxel space as BuildLuxelRadial moves it, can cover a
+    // cell.  Faces on worker threads, lists joined in face order.
+    struct Cand {
+        int32_t sample;
+        float4 box;
+    };
+    std::vector<std::vector<Cand>> lists((size_t)nfaces);
+    parallel_for(nfaces, 4, [&](int64_t fi) {
+        const FaceFrameOut &me = fr[(size_t)fi];
+        std::vector<Cand> &out = lists[(size_t)fi];
+        for (int32_t q = noff[(size_t)fi]; q < noff[(size_t)fi + 1]; q++) {
             const int32_t g = nlist[(size_t)q];
             const FaceFrameOut &l = fr[(size_t)g];
-            for (int64_t k = sfirst[(size_t)g]; k < sfirst[(size_t)g + 1]; k++) {
+            for (int64_t k = sfirst[(size_t)g]; k < send[(size_t)g]; k++) {
                 const vrad_sample &sm = samples[k];
                 float tmp[3], mins, mint, maxs, maxt;
                 frame_luxel_to_world(l, sm.mins[0], sm.mins[1], tmp);
@@ -420,16 +444,26 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
                 smax = smax < me.width ? smax : me.width;
                 tmax = tmax < me.height ? tmax : me.height;
                 if (smin >= smax || tmin >= tmax) continue;
-                cand_sample.push_back((int32_t)k);
-                cand_box.push_back(make_float4(mins, mint, maxs, maxt));
+                out.push_back(Cand{(int32_t)k, make_float4(mins, mint, maxs, maxt)});
             }
         }
-        cand_off[(size_t)f + 1] = (int32_t)cand_sample.size();
-    }
+    });
+    std::vector<int32_t> cand_off((size_t)nfaces + 1, 0);
+    for (int32_t f = 0; f < nfaces; f++) cand_off[(size_t)f + 1] = cand_off[(size_t)f] + (int32_t)lists[(size_t)f].size();
+    uvector<int32_t> cand_sample((size_t)cand_off[(size_t)nfaces]);
+    uvector<float4> cand_box((size_t)cand_off[(size_t)nfaces]);
+    parallel_for(nfaces, 16, [&](int64_t f) {
+        size_t k = (size_t)cand_off[(size_t)f];
+        for (const Cand &c : lists[(size_t)f]) {
+            cand_sample[k] = c.sample;
+            cand_box[k] = c.box;
+            k++;
+        }
+    });
     clock.mark("candidates");
     auto up = [](auto **dst, const auto &v) {
         using T = typename std::remove_reference<decltype(v)>::type::value_type;
-        cudaError_t e = cudaMalloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
+        cudaError_t e = vrad::dev_alloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
         if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
         return e;
     };
@@ -442,9 +476,9 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
     if (e == cudaSuccess) e = up(&fb.cand_off, cand_off);
     if (e == cudaSuccess) e = up(&fb.cand_sample, cand_sample);
     if (e == cudaSuccess) e = up(&fb.cand_box, cand_box);
-    if (e == cudaSuccess) e = cudaMalloc(&fb.rad_light, sizeof(float4) * (size_t)(ncells ? ncells : 1));
-    if (e == cudaSuccess) e = cudaMalloc(&fb.rad_weight, sizeof(float) * (size_t)(ncells ? ncells : 1));
-    if (e == cudaSuccess) e = cudaMalloc(&fb.flat, sizeof(float4) * (size_t)(ncells ? ncells : 1));
+    if (e == cudaSuccess) e = vrad::dev_alloc(&fb.rad_light, sizeof(float4) * (size_t)(ncells ? ncells : 1));
+    if (e == cudaSuccess) e = vrad::dev_alloc(&fb.rad_weight, sizeof(float) * (size_t)(ncells ? ncells : 1));
+    if (e == cudaSuccess) e = vrad::dev_alloc(&fb.flat, sizeof(float4) * (size_t)(ncells ? ncells : 1));
     if (e != cudaSuccess) {
         fb.release();
         why = "final-pass buffers";
@@ -522,7 +556,7 @@ extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t cap
     cudaError_t e = cudaSetDevice(ctx->device);
     uint8_t *d_lighting = nullptr;
     cudaEvent_t a = nullptr, m = nullptr, bm = nullptr, b = nullptr;
-    if (e == cudaSuccess) e = cudaMalloc(&d_lighting, (size_t)(fb.lighting_bytes ? fb.lighting_bytes : 4));
+    if (e == cudaSuccess) e = vrad::dev_alloc(&d_lighting, (size_t)(fb.lighting_bytes ? fb.lighting_bytes : 4));
     if (e == cudaSuccess) e = cudaEventCreate(&a);
     if (e == cudaSuccess) e = cudaEventCreate(&m);
     if (e == cudaSuccess) e = cudaEventCreate(&bm);
@@ -568,7 +602,7 @@ extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t cap
             stats->supersample_ms = ctx->supersample.ms;
         }
     }
-    cudaFree(d_lighting);
+    vrad::dev_free(d_lighting);
     if (a) cudaEventDestroy(a);
     if (m) cudaEventDestroy(m);
     if (bm) cudaEventDestroy(bm);

@@ -60,7 +60,8 @@ struct FinalBuffers {
 };
 
 cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces, const vrad_sample *samples,
-                        int64_t nsamples, const float *vertices, int64_t nvertices, std::string &why);
+                        int64_t nsamples, const float *vertices, int64_t nvertices, std::vector<int32_t> &noff,
+                        std::vector<int32_t> &nlist, std::string &why);
 
 // The bounced light's radial grid (FinalLightFace.BuildPatchRadial): per
 // face, the leaf patches of the face and of its smoothing neighbours whose

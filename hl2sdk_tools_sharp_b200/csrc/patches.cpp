@@ -250,20 +250,10 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
     // PatchSubdivider.Subdivide with bounces > 0, not -fast.  Each root's
     // subtree depends on nothing outside its face, so the roots are split
     // on worker threads, each into its own arrays.
-    {
-        std::atomic<int32_t> next{0};
-        auto work = [&]() {
-            for (int32_t i; (i = next.fetch_add(1)) < roots;) {
-                Builder &b = subtree[(size_t)i];
-                if (!prevent_subdivision(faces[b.patches[0].face].flags)) b.subdivide(0);
-            }
-        };
-        const unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-        std::vector<std::thread> pool;
-        for (unsigned t = 1; t < nt; t++) pool.emplace_back(work);
-        work();
-        for (auto &t : pool) t.join();
-    }
+    parallel_for(roots, 1, [&](int64_t i) {
+        Builder &b = subtree[(size_t)i];
+        if (!prevent_subdivision(faces[b.patches[0].face].flags)) b.subdivide(0);
+    });
     clock.mark("subdivide");
     // Global indices: the roots 0..roots-1 in face order, then each root's
     // descendants in creation order (the order SubdividePatch adds them).
@@ -274,23 +264,12 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
         total += (int32_t)subtree[(size_t)i].patches.size() - 1;
     }
     out.patches.resize((size_t)total);
-    std::vector<const Winding *> wind((size_t)total);
+    uvector<const Winding *> wind((size_t)total);
+    uvector<int64_t> first((size_t)total + 1);
     out.face_first.assign((size_t)nfaces, 0);
     out.face_end.assign((size_t)nfaces, 0);
-    const unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-    auto parallel = [&](int64_t n, auto &&body) {
-        std::atomic<int64_t> next{0};
-        auto work = [&]() {
-            for (int64_t i; (i = next.fetch_add(1024)) < n;)
-                for (int64_t k = i; k < std::min(n, i + 1024); k++) body(k);
-        };
-        std::vector<std::thread> pool;
-        for (unsigned t = 1; t < nt; t++) pool.emplace_back(work);
-        work();
-        for (auto &t : pool) t.join();
-    };
     // Each root's block of patches, renumbered, in parallel.
-    parallel(roots, [&](int64_t ii) {
+    parallel_for(roots, 8, [&](int64_t ii) {
         const int32_t i = (int32_t)ii;
         Builder &b = subtree[(size_t)i];
         auto global = [&](int32_t local) { return local < 0 ? -1 : (local == 0 ? i : base[(size_t)i] + local - 1); };
@@ -302,6 +281,7 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
             const int32_t g = global((int32_t)k);
             out.patches[(size_t)g] = p;
             wind[(size_t)g] = &b.windings[k];
+            first[(size_t)g + 1] = (int64_t)b.windings[k].size();
         }
     });
     for (int32_t i = 0; i < roots; i++) {
@@ -314,13 +294,13 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
     clock.mark("merge");
     // Windings into one point array: offsets by a prefix sum, points copied
     // in parallel.
-    std::vector<int64_t> first((size_t)total + 1, 0);
-    for (int32_t i = 0; i < total; i++) first[(size_t)i + 1] = first[(size_t)i] + (int64_t)wind[(size_t)i]->size();
-    out.points.assign((size_t)first[(size_t)total] * 3, 0.0f);
-    parallel(total, [&](int64_t i) {
+    first[0] = 0;
+    for (int32_t i = 0; i < total; i++) first[(size_t)i + 1] += first[(size_t)i];
+    out.points.resize((size_t)first[(size_t)total] * 3);
+    parallel_for(total, 4096, [&](int64_t i) {
         vrad_patch &p = out.patches[(size_t)i];
         p.first_point = (int32_t)first[(size_t)i];
-        p.num_points = (int32_t)wind[(size_t)i]->size();
+        p.num_points = (int32_t)(first[(size_t)i + 1] - first[(size_t)i]);
         float *dst = &out.points[(size_t)first[(size_t)i] * 3];
         for (const V3 &v : *wind[(size_t)i]) {
             *dst++ = v.x;
@@ -329,6 +309,10 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
         }
     });
     clock.mark("points");
+    // The builders' windings (one small vector per patch) freed in
+    // parallel rather than by one thread on return.
+    parallel_for(roots, 8, [&](int64_t i) { Builder gone = std::move(subtree[(size_t)i]); });
+    clock.mark("free");
     out.roots = roots;
     return true;
 }

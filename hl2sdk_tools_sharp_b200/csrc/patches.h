@@ -7,12 +7,13 @@
 #include <vector>
 
 #include "../../include/vrad_cuda.h"
+#include "host_parallel.h"
 
 namespace vrad {
 
 struct PatchTree {
-    std::vector<vrad_patch> patches;   // the reference's patch indices
-    std::vector<float> points;         // windings, xyz each (vrad_patch.first_point)
+    uvector<vrad_patch> patches;       // the reference's patch indices
+    uvector<float> points;             // windings, xyz each (vrad_patch.first_point)
     std::vector<int32_t> face_root;    // per face: its root patch, -1 for none
     std::vector<int32_t> face_first;   // per face: its descendants are [face_first, face_end)
     std::vector<int32_t> face_end;

@@ -34,7 +34,9 @@
 #include <string>
 #include <vector>
 
+#include "device_pool.h"
 #include "gather.cuh"
+#include "host_parallel.h"
 #include "setup_clock.h"
 #include "supersample.cuh"
 #include "world.h"
@@ -305,9 +307,9 @@ __global__ void k_ss_resolve(int32_t nsel, const int32_t *__restrict__ selected,
 
 unsigned grid_of(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
 
-template <class T>
-cudaError_t upload(T **dst, const std::vector<T> &v) {
-    cudaError_t e = cudaMalloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
+template <class T, class A>
+cudaError_t upload(T **dst, const std::vector<T, A> &v) {
+    cudaError_t e = dev_alloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
     if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
     return e;
 }
@@ -316,7 +318,7 @@ cudaError_t upload(T **dst, const std::vector<T> &v) {
 
 void SupersampleBuffers::release() {
     void *ptrs[] = {origin_st, cell, wind, points, intensity, processed, selected, counts, base, rows, row_out, row_bits};
-    for (void *p : ptrs) cudaFree(p);
+    for (void *p : ptrs) dev_free(p);
     cudaFreeHost(h_counts);
     const int32_t keep = extra_passes;
     *this = SupersampleBuffers();
@@ -324,13 +326,13 @@ void SupersampleBuffers::release() {
 }
 
 cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_face> &faces,
-                              const std::vector<float> &vertices, const std::vector<vrad_sample> &samples,
+                              const std::vector<float> &vertices, const uvector<vrad_sample> &samples,
                               const FinalBuffers &fb, int32_t nclusters, bool &have, std::string &why) {
     ss.release();
     have = false;
     SetupClock clock("supersample_tables");
-    std::vector<int32_t> wind_flat;
-    std::vector<float> pts;
+    uvector<int32_t> wind_flat;
+    uvector<float> pts;
     if (!sample_windings(faces.data(), (int32_t)faces.size(), vertices.data(), (int64_t)vertices.size() / 3,
                          samples.data(), (int64_t)samples.size(), wind_flat, pts)) {
         why = "the samples are not the face sample builder's own, so their cell windings are unknown";
@@ -344,18 +346,21 @@ cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_fac
         face_frame_of(faces[f], fr[f]);
         face_cells[f + 1] = face_cells[f] + fr[f].width * fr[f].height;
     }
-    std::vector<float2> origin_st(S);
-    std::vector<int32_t> cell(S);
-    std::vector<int2> wind(S);
-    for (size_t i = 0; i < S; i++) {
+    uvector<float2> origin_st(S);
+    uvector<int32_t> cell(S);
+    uvector<int2> wind(S);
+    parallel_for((int64_t)S, 1 << 15, [&](int64_t ii) {
+        const size_t i = (size_t)ii;
         const vrad_sample &sm = samples[i];
         const FaceFrameOut &q = fr[(size_t)sm.face];
         frame_world_to_luxel(q, sm.position, origin_st[i].x, origin_st[i].y);
         cell[i] = face_cells[(size_t)sm.face] + sm.s + sm.t * q.width;
         wind[i] = make_int2(wind_flat[2 * i], wind_flat[2 * i + 1]);
-    }
-    std::vector<float4> p4(pts.size() / 3);
-    for (size_t k = 0; k < p4.size(); k++) p4[k] = make_float4(pts[3 * k], pts[3 * k + 1], pts[3 * k + 2], 0.0f);
+    });
+    uvector<float4> p4(pts.size() / 3);
+    parallel_for((int64_t)p4.size(), 1 << 16, [&](int64_t k) {
+        p4[(size_t)k] = make_float4(pts[3 * k], pts[3 * k + 1], pts[3 * k + 2], 0.0f);
+    });
     clock.mark("sample tables");
     const size_t S1 = S ? S : 1;
     const size_t groups = 5 * S1 + 16 * (size_t)(nclusters + 1);
@@ -363,14 +368,14 @@ cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_fac
     if (e == cudaSuccess) e = upload(&ss.cell, cell);
     if (e == cudaSuccess) e = upload(&ss.wind, wind);
     if (e == cudaSuccess) e = upload(&ss.points, p4);
-    if (e == cudaSuccess) e = cudaMalloc(&ss.intensity, sizeof(float) * S1);
-    if (e == cudaSuccess) e = cudaMalloc(&ss.processed, S1);
-    if (e == cudaSuccess) e = cudaMalloc(&ss.selected, sizeof(int32_t) * S1);
-    if (e == cudaSuccess) e = cudaMalloc(&ss.counts, sizeof(int32_t) * (1 + 2 * (size_t)nclusters));
-    if (e == cudaSuccess) e = cudaMalloc(&ss.base, sizeof(int32_t) * (2 * (size_t)nclusters + 1));
-    if (e == cudaSuccess) e = cudaMalloc(&ss.rows, sizeof(int32_t) * groups);
-    if (e == cudaSuccess) e = cudaMalloc(&ss.row_out, sizeof(float4) * 20 * S1);
-    if (e == cudaSuccess) e = cudaMalloc(&ss.row_bits, sizeof(int32_t) * 5 * S1);
+    if (e == cudaSuccess) e = dev_alloc(&ss.intensity, sizeof(float) * S1);
+    if (e == cudaSuccess) e = dev_alloc(&ss.processed, S1);
+    if (e == cudaSuccess) e = dev_alloc(&ss.selected, sizeof(int32_t) * S1);
+    if (e == cudaSuccess) e = dev_alloc(&ss.counts, sizeof(int32_t) * (1 + 2 * (size_t)nclusters));
+    if (e == cudaSuccess) e = dev_alloc(&ss.base, sizeof(int32_t) * (2 * (size_t)nclusters + 1));
+    if (e == cudaSuccess) e = dev_alloc(&ss.rows, sizeof(int32_t) * groups);
+    if (e == cudaSuccess) e = dev_alloc(&ss.row_out, sizeof(float4) * 20 * S1);
+    if (e == cudaSuccess) e = dev_alloc(&ss.row_bits, sizeof(int32_t) * 5 * S1);
     if (e == cudaSuccess) e = cudaMallocHost(&ss.h_counts, sizeof(int32_t) * (1 + (size_t)nclusters));
     if (e != cudaSuccess) {
         ss.release();

@@ -27,6 +27,7 @@
 
 #include "direct.cuh"
 #include "final.cuh"
+#include "host_parallel.h"
 #include "scene.cuh"
 
 namespace vrad {
@@ -62,7 +63,7 @@ struct SupersampleBuffers {
 // and false returned when the samples are not the builder's own (their
 // windings cannot be known).
 cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_face> &faces,
-                              const std::vector<float> &vertices, const std::vector<vrad_sample> &samples,
+                              const std::vector<float> &vertices, const uvector<vrad_sample> &samples,
                               const FinalBuffers &fb, int32_t nclusters, bool &have, std::string &why);
 
 // The supersampling passes over `light` (the direct gather's output, one

@@ -232,26 +232,33 @@ extern "C" int32_t vrad_build_samples(const vrad_face *faces, int32_t nfaces, co
 namespace vrad {
 
 bool sample_windings(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
-                     const vrad_sample *given, int64_t ngiven, std::vector<int32_t> &wind, std::vector<float> &pts) {
+                     const vrad_sample *given, int64_t ngiven, uvector<int32_t> &wind, uvector<float> &pts) {
     AllSamples all;
     if (build_all_samples(faces, nfaces, vertices, nvertices, true, all) != VRAD_OK) return false;
-    wind.clear();
-    pts.clear();
-    int64_t k = 0;
+    // Each face's first sample and first point, then the comparison and the
+    // copies face by face in parallel.
+    std::vector<int64_t> s0((size_t)nfaces + 1, 0), p0((size_t)nfaces + 1, 0);
     for (int32_t f = 0; f < nfaces; f++) {
-        const auto &v = all.samples[(size_t)f];
-        if (k + (int64_t)v.size() > ngiven) return false;
-        if (!v.empty() && std::memcmp(v.data(), given + k, sizeof(vrad_sample) * v.size()) != 0) return false;
-        const int32_t base = (int32_t)(pts.size() / 3);
-        const auto &wf = all.wind[(size_t)f];
-        for (size_t i = 0; i < wf.size(); i += 2) {
-            wind.push_back(wf[i + 1] ? wf[i] + base : 0);
-            wind.push_back(wf[i + 1]);
-        }
-        pts.insert(pts.end(), all.pts[(size_t)f].begin(), all.pts[(size_t)f].end());
-        k += (int64_t)v.size();
+        s0[(size_t)f + 1] = s0[(size_t)f] + (int64_t)all.samples[(size_t)f].size();
+        p0[(size_t)f + 1] = p0[(size_t)f] + (int64_t)all.pts[(size_t)f].size();
     }
-    return k == ngiven;
+    if (s0[(size_t)nfaces] != ngiven) return false;
+    wind.resize(2 * (size_t)ngiven);
+    pts.resize((size_t)p0[(size_t)nfaces]);
+    std::atomic<bool> same{true};
+    parallel_for(nfaces, 16, [&](int64_t f) {
+        const auto &v = all.samples[(size_t)f];
+        if (!v.empty() && std::memcmp(v.data(), given + s0[(size_t)f], sizeof(vrad_sample) * v.size()) != 0) same = false;
+        const int32_t base = (int32_t)(p0[(size_t)f] / 3);
+        const auto &wf = all.wind[(size_t)f];
+        int32_t *w = &wind[2 * (size_t)s0[(size_t)f]];
+        for (size_t i = 0; i < wf.size(); i += 2) {
+            *w++ = wf[i + 1] ? wf[i] + base : 0;
+            *w++ = wf[i + 1];
+        }
+        std::copy(all.pts[(size_t)f].begin(), all.pts[(size_t)f].end(), pts.begin() + p0[(size_t)f]);
+    });
+    return same.load();
 }
 
 }  // namespace vrad

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "../../include/vrad_cuda.h"
+#include "host_parallel.h"
 
 namespace vrad {
 
@@ -29,7 +30,7 @@ void frame_world_to_luxel(const FaceFrameOut &fr, const float p[3], float &s, fl
 // whole; pts the points (xyz each).  False unless the samples the builder
 // makes from these faces are exactly `given`.
 bool sample_windings(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
-                     const vrad_sample *given, int64_t ngiven, std::vector<int32_t> &wind, std::vector<float> &pts);
+                     const vrad_sample *given, int64_t ngiven, uvector<int32_t> &wind, uvector<float> &pts);
 
 // The welded vertex numbers of each face's winding (vertices identified by
 // position) and, per vertex, the faces touching it in face order.  False

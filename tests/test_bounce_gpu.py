@@ -131,3 +131,28 @@ def test_bounce_pass_is_repeatable_and_device_entry_matches():
         torch.cuda.synchronize()
     assert np.array_equal(a, b)
     assert np.array_equal(d.cpu().numpy(), a)
+
+
+def test_sample_runs_in_any_face_order_light_the_same_lump():
+    """The world upload takes each face's samples as one contiguous run, the
+    runs in any order of faces: an upload with the runs permuted lights the
+    same lump, bounce included (supersampling off in both, since it needs
+    the sample builder's own order)."""
+    w = rg.generate(rg.config_3x3(seed=2))
+    inp = L.prepare(w)
+    off, lst = L.pvs_lists(w)
+    refl = L.face_reflectivity(w)
+    ff = inp.face_first
+    order = np.random.default_rng(5).permutation(len(inp.faces))
+    idx = np.concatenate([np.arange(ff[f], ff[f + 1]) for f in order])
+    perm = L.LightingInputs(**{**inp.__dict__, "samples": inp.samples[idx].copy()})
+    lumps, stats = [], []
+    for i in (inp, perm):
+        with L.LightingStage(w, i) as st:
+            st.set_extra_passes(0)
+            st.upload_bounce(refl, off, lst, threshold=1.0)
+            lump, _, _ = st.light_pass()
+            lumps.append(lump)
+            stats.append(st.bounce_stats().bounces)
+    assert stats[0] == stats[1] and stats[0] > 1
+    assert np.array_equal(lumps[0], lumps[1])
