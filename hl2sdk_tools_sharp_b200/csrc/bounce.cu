@@ -37,7 +37,8 @@
 //                     MaxPatches, and MakeScales' ordered sum
 //   k_gather          one thread per receiver: GatherLight's ordered sum,
 //                     then CollectLight's leaf update
-//   k_collect         one thread per face: CollectLight's parents, bottom up
+//   k_collect_level   one thread per parent of one tree level: CollectLight's
+//                     parents, one launch per level, bottom up
 //   k_totals          fp64 sums of the light a bounce added, with absolute
 //                     sums that bound the reference's float sum
 //   k_exact_total     one block: the reference's sequential float sum, run
@@ -418,38 +419,34 @@ __global__ void k_gather(BounceView v, const int64_t *__restrict__ tr_off, const
     shoot_out[p] = make_float4(__fmul_rn(sx, rf.x), __fmul_rn(sy, rf.y), __fmul_rn(sz, rf.z), 0.0f);
 }
 
-// CollectLight's parents, bottom up within each face (children have
-// higher indices): the area blend of the children's light and emission.
-__global__ void k_collect(BounceView v, float4 *__restrict__ total, float4 *__restrict__ emit_out,
-                          float4 *__restrict__ shoot_out) {
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= v.nfaces) return;
-    const int4 fr = __ldg(&v.face_range[f]);
-    const FaceList L{fr.x, fr.y, fr.z};
-    const int n = L.count();
-    for (int k = 0; k < n; k++) {
-        const int p = L.at(k);
-        const int4 tr = __ldg(&v.tree[p]);
-        if (tr.w) {
-            emit_out[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            shoot_out[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            continue;
-        }
-        if (tr.y == -1) continue;
-        const float a1 = __ldg(&v.origin[tr.y].w), a2 = __ldg(&v.origin[tr.z].w);
-        const float s1 = __fdiv_rn(a1, __fadd_rn(a1, a2)), s2 = __fdiv_rn(a2, __fadd_rn(a1, a2));
-        const float4 c1 = total[tr.y], c2 = total[tr.z];
-        total[p] = make_float4(__fadd_rn(__fmul_rn(c1.x, s1), __fmul_rn(c2.x, s2)),
-                               __fadd_rn(__fmul_rn(c1.y, s1), __fmul_rn(c2.y, s2)),
-                               __fadd_rn(__fmul_rn(c1.z, s1), __fmul_rn(c2.z, s2)), 0.0f);
-        const float4 e1 = emit_out[tr.y], e2 = emit_out[tr.z];
-        const float4 e = make_float4(__fadd_rn(__fmul_rn(e1.x, s1), __fmul_rn(e2.x, s2)),
-                                     __fadd_rn(__fmul_rn(e1.y, s1), __fmul_rn(e2.y, s2)),
-                                     __fadd_rn(__fmul_rn(e1.z, s1), __fmul_rn(e2.z, s2)), 0.0f);
-        emit_out[p] = e;
-        const float4 rf = __ldg(&v.refl[p]);
-        shoot_out[p] = make_float4(__fmul_rn(e.x, rf.x), __fmul_rn(e.y, rf.y), __fmul_rn(e.z, rf.z), 0.0f);
+// CollectLight's parents for one level of the patch trees: every parent
+// whose subtree is `level` deep, each the area blend of its children's
+// light and emission (the children, one level lower, are final).  Run for
+// levels 1, 2, ... this is CollectLight's bottom-up order within each face.
+__global__ void k_collect_level(BounceView v, const int32_t *__restrict__ parents, int n, float4 *__restrict__ total,
+                                float4 *__restrict__ emit_out, float4 *__restrict__ shoot_out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int p = __ldg(&parents[i]);
+    const int4 tr = __ldg(&v.tree[p]);
+    if (tr.w) {
+        emit_out[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        shoot_out[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        return;
     }
+    const float a1 = __ldg(&v.origin[tr.y].w), a2 = __ldg(&v.origin[tr.z].w);
+    const float s1 = __fdiv_rn(a1, __fadd_rn(a1, a2)), s2 = __fdiv_rn(a2, __fadd_rn(a1, a2));
+    const float4 c1 = total[tr.y], c2 = total[tr.z];
+    total[p] = make_float4(__fadd_rn(__fmul_rn(c1.x, s1), __fmul_rn(c2.x, s2)),
+                           __fadd_rn(__fmul_rn(c1.y, s1), __fmul_rn(c2.y, s2)),
+                           __fadd_rn(__fmul_rn(c1.z, s1), __fmul_rn(c2.z, s2)), 0.0f);
+    const float4 e1 = emit_out[tr.y], e2 = emit_out[tr.z];
+    const float4 e = make_float4(__fadd_rn(__fmul_rn(e1.x, s1), __fmul_rn(e2.x, s2)),
+                                 __fadd_rn(__fmul_rn(e1.y, s1), __fmul_rn(e2.y, s2)),
+                                 __fadd_rn(__fmul_rn(e1.z, s1), __fmul_rn(e2.z, s2)), 0.0f);
+    emit_out[p] = e;
+    const float4 rf = __ldg(&v.refl[p]);
+    shoot_out[p] = make_float4(__fmul_rn(e.x, rf.x), __fmul_rn(e.y, rf.y), __fmul_rn(e.z, rf.z), 0.0f);
 }
 
 // The light a bounce added (the leaves' emission), in fp64, with the sum
@@ -642,6 +639,7 @@ void BounceBuffers::release() {
     void *ptrs[] = {origin, normal, mins, maxs, refl, tree, wind, points, face_range, face_samples, face_plane,
                     recv, row_off, row_faces, sample_area, cand_off, cand_src, cand_w, tr_off, tr, scan_tmp,
                     acc, direct, total, emit[0], emit[1], shoot[0], shoot[1], sums, exact, counters, leaf_desc,
+                    level_patch,
                     first, guess, feat, pred,
                     pr_off, pr_patch, pr_box, pr_coord, prad_light, prad_weight};
     for (void *q : ptrs) dev_free(q);
@@ -691,6 +689,17 @@ cudaError_t launch_transfers(BounceBuffers &b, const DeviceScene &scene, uint32_
     return cudaGetLastError();
 }
 
+// CollectLight's parents, level by level.
+cudaError_t launch_collect(const BounceBuffers &b, float4 *emit_out, float4 *shoot_out, cudaStream_t stream) {
+    for (size_t h = 1; h + 1 < b.h_level_off.size(); h++) {
+        const int32_t a = b.h_level_off[h], n = b.h_level_off[h + 1] - a;
+        if (n > 0)
+            k_collect_level<<<blocks(n, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.level_patch + a, n, b.total,
+                                                                                  emit_out, shoot_out);
+    }
+    return cudaGetLastError();
+}
+
 // Bounce number `bounce` (0-based): reads shoot[bounce & 1], writes the
 // other half, then the fp64 totals.
 cudaError_t launch_gather(BounceBuffers &b, int bounce, cudaStream_t stream) {
@@ -698,8 +707,8 @@ cudaError_t launch_gather(BounceBuffers &b, int bounce, cudaStream_t stream) {
     if (b.nreceivers)
         k_gather<<<blocks(b.nreceivers, kBounceBlock), kBounceBlock, 0, stream>>>(
             b.view, b.tr_off, b.tr, b.shoot[in], b.total, b.emit[out], b.shoot[out]);
-    k_collect<<<blocks(b.nfaces, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.total, b.emit[out], b.shoot[out]);
-    cudaError_t e = cudaMemsetAsync(b.sums, 0, 6 * sizeof(double), stream);
+    cudaError_t e = launch_collect(b, b.emit[out], b.shoot[out], stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.sums, 0, 6 * sizeof(double), stream);
     if (e != cudaSuccess) return e;
     if (b.npatches)
         k_totals<<<blocks(b.npatches, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.emit[out], b.sums);
@@ -728,8 +737,8 @@ cudaError_t launch_warm_start(BounceBuffers &b, const DeviceWorld &w, const vrad
     // Bounce 0 wrote half 1; the warm step writes half 0, as bounce 1 would.
     k_warm_combine<<<blocks(b.nreceivers, kBounceBlock), kBounceBlock, 0, stream>>>(
         b.view, b.tr_off, b.tr, b.guess, b.first, b.total, b.emit[0], b.shoot[0]);
-    k_collect<<<blocks(b.nfaces, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.total, b.emit[0], b.shoot[0]);
-    e = cudaMemsetAsync(b.sums, 0, 6 * sizeof(double), stream);
+    e = launch_collect(b, b.emit[0], b.shoot[0], stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.sums, 0, 6 * sizeof(double), stream);
     if (e != cudaSuccess) return e;
     k_totals<<<blocks(b.npatches, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.emit[0], b.sums);
     b.last_buffer = 0;

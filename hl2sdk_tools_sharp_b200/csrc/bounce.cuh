@@ -88,6 +88,10 @@ struct BounceBuffers {
     double *sums = nullptr;        // fp64 totals of a bounce: 3 sums, 3 absolute sums
     float *exact = nullptr;        // the sequential float total, when needed
     int32_t *leaf_desc = nullptr;  // the sky-free leaves, descending index (CollectLight's total order)
+    // CollectLight's parents by level (the depth of the subtree below):
+    // level h's are level_patch[h_level_off[h] .. h_level_off[h + 1]).
+    int32_t *level_patch = nullptr;
+    std::vector<int32_t> h_level_off;
     // Learned warm start.
     float4 *first = nullptr;       // the first bounce's light per patch (bounce 0's total)
     float4 *guess = nullptr;       // the network's guess per patch

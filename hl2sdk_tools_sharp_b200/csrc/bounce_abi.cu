@@ -329,6 +329,29 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     for (int32_t i = P - 1; i >= 0; i--)
         if (tr[(size_t)i].y == -1 && !tr[(size_t)i].w) leaf_desc.push_back(i);
     const int32_t nleaves = (int32_t)leaf_desc.size();
+    // Each parent's level (1 + its deeper child's; leaves 0): children
+    // have higher indices than their parent, so one descending pass; then
+    // the parents grouped by level, index order within a level.
+    std::vector<uint8_t> level((size_t)P, 0);
+    int32_t top = 0;
+    for (int32_t i = P - 1; i >= 0; i--) {
+        const int4 t = tr[(size_t)i];
+        if (t.y == -1) continue;
+        const int h = 1 + std::max(level[(size_t)t.y], level[(size_t)t.z]);
+        if (h > 255) return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "patch %d's subtree is deeper than 255 levels", i);
+        level[(size_t)i] = (uint8_t)h;
+        top = std::max(top, h);
+    }
+    std::vector<int32_t> level_off((size_t)top + 2, 0);
+    for (int32_t i = 0; i < P; i++)
+        if (level[(size_t)i]) level_off[(size_t)level[(size_t)i] + 1]++;
+    for (int32_t h = 0; h <= top; h++) level_off[(size_t)h + 1] += level_off[(size_t)h];
+    std::vector<int32_t> level_patch((size_t)level_off[(size_t)top + 1]);
+    {
+        std::vector<int32_t> at(level_off.begin(), level_off.end() - 1);
+        for (int32_t i = 0; i < P; i++)
+            if (level[(size_t)i]) level_patch[(size_t)at[level[(size_t)i]]++] = i;
+    }
     // FacesInRow: each visible cluster's faces, in face order (one leaf per
     // cluster, whose faces are the faces that lie in it).
     std::vector<std::vector<int32_t>> cluster_faces((size_t)C);
@@ -369,6 +392,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     if (e == cudaSuccess) e = upload(&b.face_plane, face_plane);
     if (e == cudaSuccess) e = upload(&b.recv, recv);
     if (e == cudaSuccess) e = upload(&b.leaf_desc, leaf_desc);
+    if (e == cudaSuccess) e = upload(&b.level_patch, level_patch);
     if (e == cudaSuccess) e = upload(&b.row_off, row_off);
     if (e == cudaSuccess) e = upload(&b.row_faces, row_faces);
     if (e == cudaSuccess) e = upload(&b.sample_area, sample_area);
@@ -411,6 +435,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     b.max_bounces = d->bounces;
     b.threshold = d->threshold;
     b.h_recv = recv;
+    b.h_level_off = level_off;
     b.view = BounceView{P, nf, R, b.origin, b.normal, b.mins, b.maxs, b.tree, b.refl, b.wind, b.points,
                         b.face_range, b.face_samples, b.face_plane, b.recv, b.row_off, b.row_faces, b.sample_area,
                         ctx->world.sample_pos};
