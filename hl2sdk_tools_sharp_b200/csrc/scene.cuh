@@ -38,6 +38,7 @@ struct SceneBuildReport {
     float bounds[6] = {0, 0, 0, 0, 0, 0};
     float pad = 0;
     float build_ms = 0;
+    double sah_cost = 0;       // the SAH trees' expected cost per ray (node visits + triangle tests)
     int64_t device_bytes = 0;
 };
 
