@@ -35,8 +35,11 @@
 //   k_transfer_count / k_transfer_write  one warp per receiver: the
 //                     accepted pairs compacted in order, capped at
 //                     MaxPatches, and MakeScales' ordered sum
-//   k_gather          one thread per receiver: GatherLight's ordered sum,
-//                     then CollectLight's leaf update
+//   k_sell_*          the transfer lists copied into slices of 32 receivers
+//                     sorted by count (SELL-32), once per pass
+//   k_gather          one thread per receiver (in count order): GatherLight's
+//                     ordered sum from its slice lane, then CollectLight's
+//                     leaf update
 //   k_collect_level   one thread per parent of one tree level: CollectLight's
 //                     parents, one launch per level, bottom up
 //   k_totals          fp64 sums of the light a bounce added, with absolute
@@ -47,6 +50,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
@@ -388,19 +392,51 @@ __global__ void k_transfer_write(int nrecv, const int64_t *__restrict__ cand_off
 
 // ---- bounces ---------------------------------------------------------------
 
+// The gather's slices (SELL-32) of the transfer lists: each receiver's
+// count and index for the sort by count.
+__global__ void k_sell_keys(int nrecv, const int64_t *__restrict__ tr_off, int32_t *__restrict__ key,
+                            int32_t *__restrict__ idx) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrecv) return;
+    key[r] = (int32_t)(tr_off[r + 1] - tr_off[r]);
+    idx[r] = r;
+}
+
+// Slice s's size: 32 times its first (largest) count.
+__global__ void k_sell_width(int nrecv, int nslices, const int32_t *__restrict__ count, int64_t *__restrict__ width) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslices) return;
+    width[s] = 32 * (int64_t)count[32 * s];
+}
+
+// Copies each receiver's transfers into its lane of its slice.
+__global__ void k_sell_pack(int nrecv, const int32_t *__restrict__ order, const int32_t *__restrict__ count,
+                            const int64_t *__restrict__ sell_off, const int64_t *__restrict__ tr_off,
+                            const int2 *__restrict__ tr, int2 *__restrict__ sell) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrecv) return;
+    const int r = order[i], n = count[i];
+    const int2 *src = tr + tr_off[r];
+    int2 *dst = sell + sell_off[i >> 5] + (i & 31);
+    for (int j = 0; j < n; j++) dst[32 * (int64_t)j] = __ldg(&src[j]);
+}
+
 // GatherLight for one receiver (the ordered sum over its transfers of the
 // sources' shoot times the weight), then CollectLight's update of that
-// leaf: the light added, emitted and shot on.
-__global__ void k_gather(BounceView v, const int64_t *__restrict__ tr_off, const int2 *__restrict__ tr,
+// leaf: the light added, emitted and shot on.  Thread i takes the i-th
+// receiver of the count order, its transfers from its lane of its slice.
+__global__ void k_gather(BounceView v, const int32_t *__restrict__ order, const int32_t *__restrict__ count,
+                         const int64_t *__restrict__ sell_off, const int2 *__restrict__ sell,
                          const float4 *__restrict__ shoot_in, float4 *__restrict__ total,
                          float4 *__restrict__ emit_out, float4 *__restrict__ shoot_out) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= v.nreceivers) return;
-    const int p = __ldg(&v.recv[r]);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= v.nreceivers) return;
+    const int p = __ldg(&v.recv[__ldg(&order[i])]);
+    const int n = __ldg(&count[i]);
+    const int2 *src = sell + __ldg(&sell_off[i >> 5]) + (i & 31);
     float sx = 0.0f, sy = 0.0f, sz = 0.0f;
-    const int64_t a = __ldg(&tr_off[r]), b = __ldg(&tr_off[r + 1]);
-    for (int64_t j = a; j < b; j++) {
-        const int2 t = __ldg(&tr[j]);
+    for (int j = 0; j < n; j++) {
+        const int2 t = __ldg(&src[32 * (int64_t)j]);
         const float w = __int_as_float(t.y);
         const float4 s = __ldg(&shoot_in[t.x]);
         sx = __fadd_rn(sx, __fmul_rn(s.x, w));
@@ -449,28 +485,34 @@ __global__ void k_collect_level(BounceView v, const int32_t *__restrict__ parent
     shoot_out[p] = make_float4(__fmul_rn(e.x, rf.x), __fmul_rn(e.y, rf.y), __fmul_rn(e.z, rf.z), 0.0f);
 }
 
-// The light a bounce added (the leaves' emission), in fp64, with the sum
-// of absolute values that bounds how far the reference's float sum can
-// lie from it.
-__global__ void k_totals(BounceView v, const float4 *__restrict__ emit, double *__restrict__ sums) {
-    __shared__ double part[6][kBounceBlock / 32];
+// The light a bounce added (the leaves' emission), in fp64, with two sums
+// that bound how far the reference's float sum (CollectLight's, in
+// leaf_desc order) can lie from it: the absolute values, and the absolute
+// values each weighted by the number of terms from it to the end of that
+// order (n - rank).  Recursive summation's error is at most
+// u * sum_k |partial sum k| <= u * sum_i |x_i| (n - rank_i), over 1 - n u.
+__global__ void k_totals(BounceView v, const float4 *__restrict__ emit, const int32_t *__restrict__ leaf_rank,
+                         int32_t nleaves, double *__restrict__ sums) {
+    __shared__ double part[kSums][kBounceBlock / 32];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    double s[6] = {0, 0, 0, 0, 0, 0};
+    double s[kSums] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     if (p < v.npatches) {
         const int4 tr = __ldg(&v.tree[p]);
         if (tr.y == -1 && tr.w == 0) {
             const float4 e = emit[p];
+            const double w = (double)(nleaves - __ldg(&leaf_rank[p]));
             s[0] = e.x, s[1] = e.y, s[2] = e.z;
             s[3] = fabs((double)e.x), s[4] = fabs((double)e.y), s[5] = fabs((double)e.z);
+            s[6] = s[3] * w, s[7] = s[4] * w, s[8] = s[5] * w;
         }
     }
-    for (int k = 0; k < 6; k++)
+    for (int k = 0; k < kSums; k++)
         for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_down_sync(kFull, s[k], o);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0)
-        for (int k = 0; k < 6; k++) part[k][warp] = s[k];
+        for (int k = 0; k < kSums; k++) part[k][warp] = s[k];
     __syncthreads();
-    if (threadIdx.x < 6) {
+    if (threadIdx.x < kSums) {
         double t = 0.0;
         for (int w = 0; w < kBounceBlock / 32; w++) t += part[threadIdx.x][w];
         atomicAdd(&sums[threadIdx.x], t);
@@ -483,22 +525,17 @@ __global__ void k_totals(BounceView v, const float4 *__restrict__ emit, double *
 // its threads stage the next tile of values in shared memory while warp 0
 // adds up the current one, every lane of it the same chain.
 constexpr int kExactThreads = 1024;
-constexpr int kExactTile = 2048;  // two tiles of float3: 48 KB of shared memory
+constexpr int kExactTile = 1024;  // two tiles of float4: 32 KB of shared memory
 
 __global__ void __launch_bounds__(kExactThreads) k_exact_total(const int32_t *__restrict__ leaf_desc, int32_t n,
                                                                const float4 *__restrict__ emit, float *__restrict__ out) {
-    __shared__ float3 tile[2][kExactTile];
+    __shared__ float4 tile[2][kExactTile];
     float x = 0.0f, y = 0.0f, z = 0.0f;
     // Stages tile `buf` with threads [first, kExactThreads).
     auto stage = [&](int buf, int base, int first) {
         for (int k = (int)threadIdx.x - first; k < kExactTile; k += kExactThreads - first) {
             const int i = base + k;
-            float3 v = make_float3(0.0f, 0.0f, 0.0f);
-            if (i < n) {
-                const float4 e = __ldg(&emit[__ldg(&leaf_desc[i])]);
-                v = make_float3(e.x, e.y, e.z);
-            }
-            tile[buf][k] = v;
+            tile[buf][k] = i < n ? __ldg(&emit[__ldg(&leaf_desc[i])]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
     };
     stage(0, 0, 0);
@@ -507,9 +544,13 @@ __global__ void __launch_bounds__(kExactThreads) k_exact_total(const int32_t *__
         if (threadIdx.x >= 32) {
             stage(buf ^ 1, base + kExactTile, 32);
         } else {
+            // The three chains of dependent adds; unrolled so the tile's
+            // loads run ahead of them.
             const int m = min(kExactTile, n - base);
+            const float4 *t = tile[buf];
+#pragma unroll 16
             for (int k = 0; k < m; k++) {
-                const float3 v = tile[buf][k];
+                const float4 v = t[k];
                 x = __fadd_rn(x, v.x);
                 y = __fadd_rn(y, v.y);
                 z = __fadd_rn(z, v.z);
@@ -639,7 +680,7 @@ void BounceBuffers::release() {
     void *ptrs[] = {origin, normal, mins, maxs, refl, tree, wind, points, face_range, face_samples, face_plane,
                     recv, row_off, row_faces, sample_area, cand_off, cand_src, cand_w, tr_off, tr, scan_tmp,
                     acc, direct, total, emit[0], emit[1], shoot[0], shoot[1], sums, exact, counters, leaf_desc,
-                    level_patch,
+                    level_patch, leaf_rank, sell_key, sell_idx, sell_count, sell_order, sell_off, sell, sort_tmp,
                     first, guess, feat, pred,
                     pr_off, pr_patch, pr_box, pr_coord, prad_light, prad_weight};
     for (void *q : ptrs) dev_free(q);
@@ -683,9 +724,23 @@ cudaError_t launch_transfers(BounceBuffers &b, const DeviceScene &scene, uint32_
     tmp = b.scan_tmp_bytes;
     e = cub::DeviceScan::InclusiveSum(b.scan_tmp, tmp, b.tr_off + 1, b.tr_off + 1, R, stream);
     if (e != cudaSuccess) return e;
-    if (b.tr)
-        k_transfer_write<<<blocks((int64_t)R * 32, kBounceBlock), kBounceBlock, 0, stream>>>(
-            R, b.cand_off, b.cand_src, b.cand_w, b.tr_off, b.tr);
+    if (!b.tr) return cudaGetLastError();
+    k_transfer_write<<<blocks((int64_t)R * 32, kBounceBlock), kBounceBlock, 0, stream>>>(
+        R, b.cand_off, b.cand_src, b.cand_w, b.tr_off, b.tr);
+    // The gather's slices.
+    const int nslices = (R + 31) / 32;
+    k_sell_keys<<<blocks(R, kBounceBlock), kBounceBlock, 0, stream>>>(R, b.tr_off, b.sell_key, b.sell_idx);
+    tmp = b.sort_tmp_bytes;
+    e = cub::DeviceRadixSort::SortPairsDescending(b.sort_tmp, tmp, b.sell_key, b.sell_count, b.sell_idx, b.sell_order,
+                                                  R, 0, 20, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.sell_off, 0, sizeof(int64_t), stream);
+    if (e != cudaSuccess) return e;
+    k_sell_width<<<blocks(nslices, kBounceBlock), kBounceBlock, 0, stream>>>(R, nslices, b.sell_count, b.sell_off + 1);
+    tmp = b.scan_tmp_bytes;
+    e = cub::DeviceScan::InclusiveSum(b.scan_tmp, tmp, b.sell_off + 1, b.sell_off + 1, nslices, stream);
+    if (e != cudaSuccess) return e;
+    k_sell_pack<<<blocks(R, kBounceBlock), kBounceBlock, 0, stream>>>(R, b.sell_order, b.sell_count, b.sell_off,
+                                                                      b.tr_off, b.tr, b.sell);
     return cudaGetLastError();
 }
 
@@ -706,12 +761,13 @@ cudaError_t launch_gather(BounceBuffers &b, int bounce, cudaStream_t stream) {
     const int in = bounce & 1, out = in ^ 1;
     if (b.nreceivers)
         k_gather<<<blocks(b.nreceivers, kBounceBlock), kBounceBlock, 0, stream>>>(
-            b.view, b.tr_off, b.tr, b.shoot[in], b.total, b.emit[out], b.shoot[out]);
+            b.view, b.sell_order, b.sell_count, b.sell_off, b.sell, b.shoot[in], b.total, b.emit[out], b.shoot[out]);
     cudaError_t e = launch_collect(b, b.emit[out], b.shoot[out], stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(b.sums, 0, 6 * sizeof(double), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.sums, 0, kSums * sizeof(double), stream);
     if (e != cudaSuccess) return e;
     if (b.npatches)
-        k_totals<<<blocks(b.npatches, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.emit[out], b.sums);
+        k_totals<<<blocks(b.npatches, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.emit[out], b.leaf_rank,
+                                                                                b.nleaves, b.sums);
     b.last_buffer = out;
     return cudaGetLastError();
 }
@@ -738,9 +794,10 @@ cudaError_t launch_warm_start(BounceBuffers &b, const DeviceWorld &w, const vrad
     k_warm_combine<<<blocks(b.nreceivers, kBounceBlock), kBounceBlock, 0, stream>>>(
         b.view, b.tr_off, b.tr, b.guess, b.first, b.total, b.emit[0], b.shoot[0]);
     e = launch_collect(b, b.emit[0], b.shoot[0], stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(b.sums, 0, 6 * sizeof(double), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.sums, 0, kSums * sizeof(double), stream);
     if (e != cudaSuccess) return e;
-    k_totals<<<blocks(b.npatches, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.emit[0], b.sums);
+    k_totals<<<blocks(b.npatches, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.emit[0], b.leaf_rank, b.nleaves,
+                                                                            b.sums);
     b.last_buffer = 0;
     return cudaGetLastError();
 }

@@ -40,6 +40,7 @@ struct vrad_mlp;
 namespace vrad {
 
 constexpr int64_t kMaxTransfersPerReceiver = 4 * 65536;  // VisMatrix.MaxPatches
+constexpr int kSums = 9;  // doubles in BounceBuffers::sums
 constexpr int kFeatures = 32;                            // the warm start network's inputs
 
 struct BounceView {
@@ -81,13 +82,25 @@ struct BounceBuffers {
     int2 *tr = nullptr;            // T
     void *scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
+    // The transfers again, in slices for the gather (SELL-32): receivers
+    // sorted by transfer count, descending (stable), 32 to a slice; entry j
+    // of lane l of slice s at sell[sell_off[s] + 32 j + l], so a warp's
+    // loads of step j are one contiguous 256 B row.
+    int32_t *sell_key = nullptr, *sell_idx = nullptr;      // R: counts and receivers before the sort
+    int32_t *sell_count = nullptr, *sell_order = nullptr;  // R: after it
+    int64_t *sell_off = nullptr;   // slices + 1
+    int2 *sell = nullptr;          // at most T + 32 * (the largest count) entries
+    void *sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
     int64_t ncand = 0, ntransfers = 0;
     // Light state.
     float4 *acc = nullptr, *direct = nullptr, *total = nullptr;
     float4 *emit[2] = {nullptr, nullptr}, *shoot[2] = {nullptr, nullptr};
-    double *sums = nullptr;        // fp64 totals of a bounce: 3 sums, 3 absolute sums
+    double *sums = nullptr;        // fp64 totals of a bounce (kSums): 3 sums, 3 absolute sums,
+                                   // 3 absolute sums weighted by the terms left in CollectLight's order
     float *exact = nullptr;        // the sequential float total, when needed
     int32_t *leaf_desc = nullptr;  // the sky-free leaves, descending index (CollectLight's total order)
+    int32_t *leaf_rank = nullptr;  // per patch: its position in leaf_desc, -1 off it
     // CollectLight's parents by level (the depth of the subtree below):
     // level h's are level_patch[h_level_off[h] .. h_level_off[h + 1]).
     int32_t *level_patch = nullptr;

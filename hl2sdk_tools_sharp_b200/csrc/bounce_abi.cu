@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
@@ -138,9 +139,11 @@ cudaError_t run_bounce(vrad_ctx *ctx, cudaStream_t s, std::string &why) {
     if (e == cudaSuccess) e = cudaEventRecord(ev[2], s);
     b.bounces_run = 0;
     b.exact_totals = 0;
+    // The float sum's error bound: u / (1 - n u) times the rank-weighted
+    // absolute sum (k_totals).
     const double u = std::ldexp(1.0, -24);
     const double nu = (double)b.nleaves * u;
-    const double gamma = nu < 0.5 ? nu / (1.0 - nu) : INFINITY;
+    const double scale = nu < 0.5 ? u / (1.0 - nu) : INFINITY;
     const vrad_mlp *model = ctx->bounce_model;
     for (int i = 0; e == cudaSuccess && i < b.max_bounces; i++) {
         // With a network attached, the second step starts from its guess
@@ -148,7 +151,7 @@ cudaError_t run_bounce(vrad_ctx *ctx, cudaStream_t s, std::string &why) {
         e = (model && i == 1) ? launch_warm_start(b, ctx->world.view, *model, s) : launch_gather(b, i, s);
         if (e == cudaSuccess && i == 0)
             e = cudaMemcpyAsync(b.first, b.total, sizeof(float4) * (size_t)b.npatches, cudaMemcpyDeviceToDevice, s);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_sums, b.sums, 6 * sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_sums, b.sums, kSums * sizeof(double), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) break;
         b.bounces_run = i + 1;
@@ -162,10 +165,11 @@ cudaError_t run_bounce(vrad_ctx *ctx, cudaStream_t s, std::string &why) {
         }
         // Radiosity.BounceAsync's stop rule on CollectLight's float total:
         // settled by the fp64 total when the float sum's error bound keeps
-        // it on one side of the threshold, else by the sequential sum.
+        // it on one side of the threshold, else by the sequential sum.  The
+        // 1.0001 covers the fp64 sums' own rounding.
         bool below[3], settled = true;
         for (int c = 0; c < 3; c++) {
-            const double S = b.h_sums[c], bound = gamma * b.h_sums[3 + c] * 1.0001;
+            const double S = b.h_sums[c], bound = scale * b.h_sums[6 + c] * 1.0001;
             b.added[c] = S;
             if (S + bound < (double)b.threshold) below[c] = true;
             else if (S - bound >= (double)b.threshold) below[c] = false;
@@ -329,6 +333,8 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     for (int32_t i = P - 1; i >= 0; i--)
         if (tr[(size_t)i].y == -1 && !tr[(size_t)i].w) leaf_desc.push_back(i);
     const int32_t nleaves = (int32_t)leaf_desc.size();
+    std::vector<int32_t> leaf_rank((size_t)P, -1);
+    for (int32_t k = 0; k < nleaves; k++) leaf_rank[(size_t)leaf_desc[(size_t)k]] = k;
     // Each parent's level (1 + its deeper child's; leaves 0): children
     // have higher indices than their parent, so one descending pass; then
     // the parents grouped by level, index order within a level.
@@ -392,6 +398,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     if (e == cudaSuccess) e = upload(&b.face_plane, face_plane);
     if (e == cudaSuccess) e = upload(&b.recv, recv);
     if (e == cudaSuccess) e = upload(&b.leaf_desc, leaf_desc);
+    if (e == cudaSuccess) e = upload(&b.leaf_rank, leaf_rank);
     if (e == cudaSuccess) e = upload(&b.level_patch, level_patch);
     if (e == cudaSuccess) e = upload(&b.row_off, row_off);
     if (e == cudaSuccess) e = upload(&b.row_faces, row_faces);
@@ -406,10 +413,10 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     if (e == cudaSuccess) e = dev_alloc(&b.tr_off, sizeof(int64_t) * R1);
     for (float4 **q : {&b.acc, &b.direct, &b.total, &b.emit[0], &b.emit[1], &b.shoot[0], &b.shoot[1]})
         if (e == cudaSuccess) e = dev_alloc(q, sizeof(float4) * P1);
-    if (e == cudaSuccess) e = dev_alloc(&b.sums, 6 * sizeof(double));
+    if (e == cudaSuccess) e = dev_alloc(&b.sums, kSums * sizeof(double));
     if (e == cudaSuccess) e = dev_alloc(&b.exact, 3 * sizeof(float));
     if (e == cudaSuccess) e = dev_alloc(&b.counters, 3 * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMallocHost(&b.h_sums, 6 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&b.h_sums, kSums * sizeof(double));
     if (e == cudaSuccess) e = cudaMallocHost(&b.h_exact, 3 * sizeof(float));
     if (e == cudaSuccess) e = dev_alloc(&b.first, sizeof(float4) * P1);
     if (e == cudaSuccess) e = dev_alloc(&b.guess, sizeof(float4) * P1);
@@ -417,12 +424,26 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     if (e == cudaSuccess) e = dev_alloc(&b.pred, sizeof(float) * 3 * (size_t)(R ? R : 1));
     if (e == cudaSuccess) e = dev_alloc(&b.prad_light, sizeof(float4) * N1);
     if (e == cudaSuccess) e = dev_alloc(&b.prad_weight, sizeof(float) * N1);
+    const int32_t nslices = (R + 31) / 32;
     if (e == cudaSuccess && R > 0) {
-        size_t need = 0;
+        // One scan buffer for the receiver scans and the slice scan; one
+        // sort buffer for the slices' count order.
+        size_t need = 0, need2 = 0;
         e = cub::DeviceScan::InclusiveSum(nullptr, need, b.cand_off + 1, b.cand_off + 1, R);
+        if (e == cudaSuccess) e = cub::DeviceScan::InclusiveSum(nullptr, need2, b.cand_off + 1, b.cand_off + 1, nslices);
+        need = std::max(need, need2);
         if (e == cudaSuccess) e = dev_alloc(&b.scan_tmp, need ? need : 1);
         b.scan_tmp_bytes = need;
+        size_t sort = 0;
+        if (e == cudaSuccess)
+            e = cub::DeviceRadixSort::SortPairsDescending(nullptr, sort, (const int32_t *)nullptr, (int32_t *)nullptr,
+                                                          (const int32_t *)nullptr, (int32_t *)nullptr, R, 0, 20);
+        if (e == cudaSuccess) e = dev_alloc(&b.sort_tmp, sort ? sort : 1);
+        b.sort_tmp_bytes = sort;
     }
+    for (int32_t **q : {&b.sell_key, &b.sell_idx, &b.sell_count, &b.sell_order})
+        if (e == cudaSuccess) e = dev_alloc(q, sizeof(int32_t) * (size_t)(R ? R : 1));
+    if (e == cudaSuccess) e = dev_alloc(&b.sell_off, sizeof(int64_t) * ((size_t)nslices + 1));
     if (e != cudaSuccess) {
         b.release();
         return vrad_cuda_fail(ctx, e, "bounce upload");
@@ -453,6 +474,10 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     // bound, so sizing needs no trace.
     uint32_t overflow = 0;
     if (e == cudaSuccess) e = dev_alloc(&b.tr, sizeof(int2) * (size_t)(ncand ? ncand : 1));
+    // The slices hold the transfers and at most 32 times the largest count
+    // of padding.
+    const int64_t sell_cap = ncand + 32 * std::min<int64_t>(kMaxTransfersPerReceiver, ncand);
+    if (e == cudaSuccess) e = dev_alloc(&b.sell, sizeof(int2) * (size_t)(sell_cap ? sell_cap : 1));
     if (e == cudaSuccess) e = cudaMemcpyAsync(&overflow, ctx->status, sizeof overflow, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
