@@ -621,37 +621,35 @@ __global__ void k_guess(BounceView v, const float *__restrict__ y, float4 *__res
     guess[p] = gv;
 }
 
-// A per-patch quantity of the parents as the area blend of their children,
-// bottom up within each face (as CollectLight blends the light).
-__global__ void k_blend(BounceView v, float4 *__restrict__ a) {
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= v.nfaces) return;
-    const int4 fr = __ldg(&v.face_range[f]);
-    const FaceList L{fr.x, fr.y, fr.z};
-    for (int k = 0; k < L.count(); k++) {
-        const int p = L.at(k);
-        const int4 tr = __ldg(&v.tree[p]);
-        if (tr.y == -1) continue;
-        const float a1 = __ldg(&v.origin[tr.y].w), a2 = __ldg(&v.origin[tr.z].w);
-        const float s1 = a1 / (a1 + a2), s2 = a2 / (a1 + a2);
-        const float4 c1 = a[tr.y], c2 = a[tr.z];
-        a[p] = make_float4(c1.x * s1 + c2.x * s2, c1.y * s1 + c2.y * s2, c1.z * s1 + c2.z * s2, 0.0f);
-    }
+// A per-patch quantity of one level's parents as the area blend of their
+// children (as CollectLight blends the light); run level by level.
+__global__ void k_blend_level(BounceView v, const int32_t *__restrict__ parents, int n, float4 *__restrict__ a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int p = __ldg(&parents[i]);
+    const int4 tr = __ldg(&v.tree[p]);
+    const float a1 = __ldg(&v.origin[tr.y].w), a2 = __ldg(&v.origin[tr.z].w);
+    const float s1 = a1 / (a1 + a2), s2 = a2 / (a1 + a2);
+    const float4 c1 = a[tr.y], c2 = a[tr.z];
+    a[p] = make_float4(c1.x * s1 + c2.x * s2, c1.y * s1 + c2.y * s2, c1.z * s1 + c2.z * s2, 0.0f);
 }
 
-// The first warm step for each receiver: A = the transfers' gather of the
-// guess's shot light, then light = B1 + A (the Jacobi step from the guess),
-// emission = light - guess (the change, which later bounces carry on).
-__global__ void k_warm_combine(BounceView v, const int64_t *__restrict__ tr_off, const int2 *__restrict__ tr,
+// The first warm step for each receiver (in count order, its transfers
+// from its slice lane): A = the transfers' gather of the guess's shot
+// light, then light = B1 + A (the Jacobi step from the guess), emission =
+// light - guess (the change, which later bounces carry on).
+__global__ void k_warm_combine(BounceView v, const int32_t *__restrict__ order, const int32_t *__restrict__ count,
+                               const int64_t *__restrict__ sell_off, const int2 *__restrict__ sell,
                                const float4 *__restrict__ guess, const float4 *__restrict__ first,
                                float4 *__restrict__ total, float4 *__restrict__ emit_out, float4 *__restrict__ shoot_out) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= v.nreceivers) return;
-    const int p = __ldg(&v.recv[r]);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= v.nreceivers) return;
+    const int p = __ldg(&v.recv[__ldg(&order[i])]);
+    const int n = __ldg(&count[i]);
+    const int2 *src = sell + __ldg(&sell_off[i >> 5]) + (i & 31);
     float sx = 0.0f, sy = 0.0f, sz = 0.0f;
-    const int64_t a = __ldg(&tr_off[r]), b = __ldg(&tr_off[r + 1]);
-    for (int64_t j = a; j < b; j++) {
-        const int2 t = __ldg(&tr[j]);
+    for (int j = 0; j < n; j++) {
+        const int2 t = __ldg(&src[32 * (int64_t)j]);
         const float w = __int_as_float(t.y);
         const float4 gs = guess[t.x], rf = __ldg(&v.refl[t.x]);
         sx += gs.x * rf.x * w;
@@ -789,10 +787,14 @@ cudaError_t launch_warm_start(BounceBuffers &b, const DeviceWorld &w, const vrad
     if (e == cudaSuccess) e = cudaMemsetAsync(b.guess, 0, sizeof(float4) * (size_t)b.npatches, stream);
     if (e != cudaSuccess) return e;
     k_guess<<<blocks(b.nreceivers, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.pred, b.guess);
-    k_blend<<<blocks(b.nfaces, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.guess);
+    for (size_t h = 1; h + 1 < b.h_level_off.size(); h++) {
+        const int32_t a = b.h_level_off[h], n = b.h_level_off[h + 1] - a;
+        if (n > 0)
+            k_blend_level<<<blocks(n, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.level_patch + a, n, b.guess);
+    }
     // Bounce 0 wrote half 1; the warm step writes half 0, as bounce 1 would.
     k_warm_combine<<<blocks(b.nreceivers, kBounceBlock), kBounceBlock, 0, stream>>>(
-        b.view, b.tr_off, b.tr, b.guess, b.first, b.total, b.emit[0], b.shoot[0]);
+        b.view, b.sell_order, b.sell_count, b.sell_off, b.sell, b.guess, b.first, b.total, b.emit[0], b.shoot[0]);
     e = launch_collect(b, b.emit[0], b.shoot[0], stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b.sums, 0, kSums * sizeof(double), stream);
     if (e != cudaSuccess) return e;
