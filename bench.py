@@ -685,6 +685,7 @@ def main_stage(args):
                                          + inp.verts.nbytes + refl.nbytes + pvs_off.nbytes + pvs_list.nbytes),
                "d2h_bytes_per_step": int(len(lump_host)), "stage_s": e2e_s,
                "parts_s": {k: statistics.median(v[1:]) for k, v in parts.items()},
+               "step_parts_s": [[round(parts[k][i], 4) for k in parts] for i in range(1, len(parts["light_pass"]))],
                "note": "includes the host-side set-up of the world and the bounce (slot layout, final-pass "
                        "tables, the patch tree) and the device tables' uploads"}
         if not np.array_equal(outv, lump_host):

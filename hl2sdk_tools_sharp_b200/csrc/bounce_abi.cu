@@ -29,14 +29,6 @@ namespace vrad {
 
 namespace {
 
-template <class T, class V>
-cudaError_t upload(T **dst, const V &v) {
-    static_assert(sizeof(typename V::value_type) == sizeof(T), "element size");
-    cudaError_t e = dev_alloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
-    if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
-    return e;
-}
-
 inline float bits_f(int32_t x) {
     float y;
     std::memcpy(&y, &x, 4);
@@ -385,28 +377,28 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     clock.mark("patch radial tables");
     const int32_t R = (int32_t)recv.size();
     const int64_t ncells = ctx->final_pass.view.ncells;
-    if (e == cudaSuccess) e = upload(&b.origin, origin);
-    if (e == cudaSuccess) e = upload(&b.normal, normal);
-    if (e == cudaSuccess) e = upload(&b.mins, mins);
-    if (e == cudaSuccess) e = upload(&b.maxs, maxs);
-    if (e == cudaSuccess) e = upload(&b.refl, refl);
-    if (e == cudaSuccess) e = upload(&b.tree, tr);
-    if (e == cudaSuccess) e = upload(&b.wind, wind);
-    if (e == cudaSuccess) e = upload(&b.points, points);
-    if (e == cudaSuccess) e = upload(&b.face_range, face_range);
-    if (e == cudaSuccess) e = upload(&b.face_samples, face_samples);
-    if (e == cudaSuccess) e = upload(&b.face_plane, face_plane);
-    if (e == cudaSuccess) e = upload(&b.recv, recv);
-    if (e == cudaSuccess) e = upload(&b.leaf_desc, leaf_desc);
-    if (e == cudaSuccess) e = upload(&b.leaf_rank, leaf_rank);
-    if (e == cudaSuccess) e = upload(&b.level_patch, level_patch);
-    if (e == cudaSuccess) e = upload(&b.row_off, row_off);
-    if (e == cudaSuccess) e = upload(&b.row_faces, row_faces);
-    if (e == cudaSuccess) e = upload(&b.sample_area, sample_area);
-    if (e == cudaSuccess) e = upload(&b.pr_off, pr_off);
-    if (e == cudaSuccess) e = upload(&b.pr_patch, pr_patch);
-    if (e == cudaSuccess) e = upload(&b.pr_box, pr_box);
-    if (e == cudaSuccess) e = upload(&b.pr_coord, pr_coord);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.origin, origin);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.normal, normal);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.mins, mins);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.maxs, maxs);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.refl, refl);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.tree, tr);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.wind, wind);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.points, points);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.face_range, face_range);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.face_samples, face_samples);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.face_plane, face_plane);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.recv, recv);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.leaf_desc, leaf_desc);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.leaf_rank, leaf_rank);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.level_patch, level_patch);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.row_off, row_off);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.row_faces, row_faces);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.sample_area, sample_area);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.pr_off, pr_off);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.pr_patch, pr_patch);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.pr_box, pr_box);
+    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.pr_coord, pr_coord);
     clock.mark("tables copied");
     const size_t P1 = (size_t)(P ? P : 1), R1 = (size_t)R + 1, N1 = (size_t)(ncells ? ncells : 1);
     if (e == cudaSuccess) e = dev_alloc(&b.cand_off, sizeof(int64_t) * R1);
@@ -445,6 +437,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
         if (e == cudaSuccess) e = dev_alloc(q, sizeof(int32_t) * (size_t)(R ? R : 1));
     if (e == cudaSuccess) e = dev_alloc(&b.sell_off, sizeof(int64_t) * ((size_t)nslices + 1));
     if (e != cudaSuccess) {
+        ctx->stager.finish(ctx->stream);  // no copy in flight into a released block
         b.release();
         return vrad_cuda_fail(ctx, e, "bounce upload");
     }
@@ -481,13 +474,20 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     if (e == cudaSuccess) e = cudaMemcpyAsync(&overflow, ctx->status, sizeof overflow, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
+        ctx->stager.finish(ctx->stream);  // no copy in flight into a released block
         b.release();
         return vrad_cuda_fail(ctx, e, "transfer sizing");
     }
     if (overflow) {
         cudaMemset(ctx->status, 0, sizeof(uint32_t));
+        ctx->stager.finish(ctx->stream);  // no copy in flight into a released block
         b.release();
         return vrad_fail(ctx, VRAD_ERR_CUDA, "stack overflow in the candidate walk (flags %u)", overflow);
+    }
+    e = ctx->stager.finish(s);
+    if (e != cudaSuccess) {
+        b.release();
+        return vrad_cuda_fail(ctx, e, "bounce upload");
     }
     clock.mark("candidate sizing");
     const int64_t ntr = 0;

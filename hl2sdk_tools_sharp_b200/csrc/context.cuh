@@ -12,6 +12,7 @@
 #include "final.cuh"
 #include "host_parallel.h"
 #include "scene.cuh"
+#include "staging.h"
 #include "supersample.cuh"
 
 struct vrad_ctx {
@@ -42,6 +43,7 @@ struct vrad_ctx {
     const vrad_mlp *bounce_model = nullptr;  // the warm start's network, or none
     vrad::SupersampleBuffers supersample;
     std::string supersample_why;     // why the world's samples cannot be supersampled
+    vrad::Stager stager;             // pinned staging of the uploads' tables
     std::string last_error;
     std::string identity;
 };

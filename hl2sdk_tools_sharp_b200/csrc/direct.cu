@@ -124,18 +124,6 @@ cudaError_t launch_direct(const DeviceScene &scene, const DeviceWorld &world, fl
 
 }  // namespace vrad
 
-namespace {
-
-template <class T, class A>
-cudaError_t upload_vec(T **dst, const std::vector<T, A> &v) {
-    cudaError_t e = vrad::dev_alloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
-    if (e == cudaSuccess && !v.empty())
-        e = cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
-    return e;
-}
-
-}  // namespace
-
 extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
     if (!w || w->nfaces < 0 || w->nsamples < 0 || w->nlights < 0 || w->nclusters < 0 ||
@@ -274,16 +262,17 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     vrad::WorldBuffers &wb = ctx->world;
     wb.release();
-    if (e == cudaSuccess) e = upload_vec(&wb.slots, slots);
-    if (e == cudaSuccess) e = upload_vec(&wb.sample_pos, pos);
-    if (e == cudaSuccess) e = upload_vec(&wb.face_normal, fnorm);
-    if (e == cudaSuccess) e = upload_vec(&wb.lights, lights);
-    if (e == cudaSuccess) e = upload_vec(&wb.cl_off, cl_off);
-    if (e == cudaSuccess) e = upload_vec(&wb.cl_list, cl_list);
-    if (e == cudaSuccess) e = upload_vec(&wb.dirs, dirs);
-    if (e == cudaSuccess) e = upload_vec(&wb.jitter, jit);
+    if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.slots, slots);
+    if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.sample_pos, pos);
+    if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.face_normal, fnorm);
+    if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.lights, lights);
+    if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.cl_off, cl_off);
+    if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.cl_list, cl_list);
+    if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.dirs, dirs);
+    if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.jitter, jit);
     if (e == cudaSuccess) e = vrad::dev_alloc(&wb.counters, 3 * sizeof(unsigned long long));
     if (e != cudaSuccess) {
+        ctx->stager.finish(ctx->stream);  // no copy in flight into a released block
         wb.release();
         return vrad_cuda_fail(ctx, e, "world upload");
     }
@@ -310,9 +299,10 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     if (w->vertices && w->nvertices > 0) {
         std::string why;
         e = vrad::build_final(ctx->final_pass, w->faces, w->nfaces, w->samples, w->nsamples, w->vertices,
-                              w->nvertices, ctx->h_noff, ctx->h_nlist, why);
+                              w->nvertices, ctx->h_noff, ctx->h_nlist, ctx->stager, ctx->stream, why);
         if (e != cudaSuccess) {
-            wb.release();
+            ctx->stager.finish(ctx->stream);  // no copy in flight into a released block
+        wb.release();
             if (e == cudaErrorInvalidValue) return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "final pass: %s", why.c_str());
             return vrad_cuda_fail(ctx, e, why.c_str());
         }
@@ -320,9 +310,10 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
         ctx->final_pass.view.sample_pos = wb.sample_pos;
         bool have = false;
         e = vrad::build_supersample(ctx->supersample, ctx->h_faces, ctx->h_vertices, ctx->h_samples, ctx->final_pass,
-                                    w->nclusters, have, why);
+                                    w->nclusters, ctx->stager, ctx->stream, have, why);
         if (e != cudaSuccess) {
-            wb.release();
+            ctx->stager.finish(ctx->stream);  // no copy in flight into a released block
+        wb.release();
             ctx->final_pass.release();
             return vrad_cuda_fail(ctx, e, why.c_str());
         }
@@ -334,9 +325,16 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     }
     e = vrad::dev_alloc(&ctx->sample_light, sizeof(float4) * (size_t)(w->nsamples ? w->nsamples : 1));
     if (e != cudaSuccess) {
+        ctx->stager.finish(ctx->stream);  // no copy in flight into a released block
         wb.release();
         ctx->final_pass.release();
         return vrad_cuda_fail(ctx, e, "sample light buffer");
+    }
+    e = ctx->stager.finish(ctx->stream);
+    if (e != cudaSuccess) {
+        wb.release();
+        ctx->final_pass.release();
+        return vrad_cuda_fail(ctx, e, "world upload");
     }
     wb.ready = true;
     return VRAD_OK;

@@ -342,7 +342,7 @@ cudaError_t launch_final(const FinalView &v, const float4 *sample_light, float4 
 // Host-side set-up of the final pass from the uploaded world.
 cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces, const vrad_sample *samples,
                         int64_t nsamples, const float *vertices, int64_t nvertices, std::vector<int32_t> &noff,
-                        std::vector<int32_t> &nlist, std::string &why) {
+                        std::vector<int32_t> &nlist, Stager &stager, cudaStream_t stream, std::string &why) {
     fb.release();
     SetupClock clock("final_tables");
     std::vector<FaceFrameOut> fr((size_t)nfaces);
@@ -461,12 +461,7 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
         }
     });
     clock.mark("candidates");
-    auto up = [](auto **dst, const auto &v) {
-        using T = typename std::remove_reference<decltype(v)>::type::value_type;
-        cudaError_t e = vrad::dev_alloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
-        if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
-        return e;
-    };
+    auto up = [&](auto **dst, const auto &v) { return stage_table(stager, stream, dst, v); };
     cudaError_t e = up(&fb.frames, frames);
     if (e == cudaSuccess) e = up(&fb.face_cells, face_cells);
     if (e == cudaSuccess) e = up(&fb.face_nsamples, face_ns);

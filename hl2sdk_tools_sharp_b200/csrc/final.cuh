@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../include/vrad_cuda.h"
+#include "staging.h"
 
 namespace vrad {
 
@@ -61,7 +62,7 @@ struct FinalBuffers {
 
 cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces, const vrad_sample *samples,
                         int64_t nsamples, const float *vertices, int64_t nvertices, std::vector<int32_t> &noff,
-                        std::vector<int32_t> &nlist, std::string &why);
+                        std::vector<int32_t> &nlist, Stager &stager, cudaStream_t stream, std::string &why);
 
 // The bounced light's radial grid (FinalLightFace.BuildPatchRadial): per
 // face, the leaf patches of the face and of its smoothing neighbours whose

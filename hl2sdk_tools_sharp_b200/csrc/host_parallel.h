@@ -1,13 +1,17 @@
-// host_parallel.h -- the host set-up's two tools for large tables:
-// parallel_for over an index range on the host's cores, and vectors whose
+// host_parallel.h -- the host set-up's tools for large tables:
+// parallel_for over an index range on a persistent pool of worker threads
+// (started on first use, one per host core, at most 32), and vectors whose
 // elements start uninitialised (a resize writes nothing, so the pages are
 // first touched by the parallel writers, not by one thread's zero fill).
 #pragma once
 
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
 #include <cstdint>
+#include <functional>
 #include <memory>
+#include <mutex>
 #include <thread>
 #include <type_traits>
 #include <utility>
@@ -21,8 +25,72 @@ inline unsigned host_threads() {
     return std::max(1u, std::min(32u, hw));
 }
 
+// The workers behind parallel_for.  One job at a time (a second caller
+// waits); the calling thread works on the job too.
+class HostPool {
+public:
+    static HostPool &get() {
+        static HostPool *p = new HostPool(host_threads() - 1);  // never destroyed: workers may outlive statics
+        return *p;
+    }
+
+    // fn() on `workers` pool threads and on the caller.
+    void run(unsigned workers, const std::function<void()> &fn) {
+        std::lock_guard<std::mutex> one(job_mu_);
+        workers = std::min<unsigned>(workers, (unsigned)threads_.size());
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            fn_ = &fn;
+            want_ = workers;
+            taken_ = 0;
+            done_ = 0;
+            gen_++;
+        }
+        cv_.notify_all();
+        fn();
+        std::unique_lock<std::mutex> g(mu_);
+        done_cv_.wait(g, [&] { return done_ == want_; });
+        fn_ = nullptr;
+    }
+
+private:
+    explicit HostPool(unsigned n) {
+        for (unsigned i = 0; i < n; i++) threads_.emplace_back([this] { loop(); });
+        for (auto &t : threads_) t.detach();
+    }
+
+    void loop() {
+        uint64_t seen = 0;
+        std::unique_lock<std::mutex> g(mu_);
+        while (true) {
+            cv_.wait(g, [&] { return gen_ != seen && taken_ < want_; });
+            seen = gen_;
+            taken_++;
+            const std::function<void()> *fn = fn_;
+            g.unlock();
+            (*fn)();
+            g.lock();
+            if (++done_ == want_) done_cv_.notify_one();
+        }
+    }
+
+    std::vector<std::thread> threads_;
+    std::mutex job_mu_, mu_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void()> *fn_ = nullptr;
+    unsigned want_ = 0, taken_ = 0, done_ = 0;
+    uint64_t gen_ = 0;
+};
+
+// Whether this thread is running a parallel_for body.
+inline bool &in_parallel_body() {
+    thread_local bool inside = false;
+    return inside;
+}
+
 // body(i) for every i in [0, n), chunks of `grain` indices handed out from a
-// shared counter; the calling thread works too.  Bodies must not throw.
+// shared counter to the pool's workers and the calling thread.  Bodies must
+// not throw.  A call from inside a body runs serially.
 template <class F>
 void parallel_for(int64_t n, int64_t grain, F &&body) {
     if (n <= 0) return;
@@ -36,15 +104,18 @@ void parallel_for(int64_t n, int64_t grain, F &&body) {
             for (int64_t k = i; k < end; k++) body(k);
         }
     };
-    if (nt <= 1) {
+    if (nt <= 1 || in_parallel_body()) {
         work();
         return;
     }
-    std::vector<std::thread> pool;
-    pool.reserve(nt - 1);
-    for (unsigned t = 1; t < nt; t++) pool.emplace_back(work);
-    work();
-    for (auto &t : pool) t.join();
+    const std::function<void()> job = [&]() {
+        bool &inside = in_parallel_body();
+        const bool was = inside;
+        inside = true;
+        work();
+        inside = was;
+    };
+    HostPool::get().run(nt - 1, job);
 }
 
 // An allocator whose value-initialising construct() default-initialises

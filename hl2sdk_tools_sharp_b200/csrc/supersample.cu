@@ -307,13 +307,6 @@ __global__ void k_ss_resolve(int32_t nsel, const int32_t *__restrict__ selected,
 
 unsigned grid_of(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
 
-template <class T, class A>
-cudaError_t upload(T **dst, const std::vector<T, A> &v) {
-    cudaError_t e = dev_alloc(dst, sizeof(T) * (v.empty() ? 1 : v.size()));
-    if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
-    return e;
-}
-
 }  // namespace
 
 void SupersampleBuffers::release() {
@@ -327,7 +320,8 @@ void SupersampleBuffers::release() {
 
 cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_face> &faces,
                               const std::vector<float> &vertices, const uvector<vrad_sample> &samples,
-                              const FinalBuffers &fb, int32_t nclusters, bool &have, std::string &why) {
+                              const FinalBuffers &fb, int32_t nclusters, Stager &stager, cudaStream_t stream,
+                              bool &have, std::string &why) {
     ss.release();
     have = false;
     SetupClock clock("supersample_tables");
@@ -364,10 +358,10 @@ cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_fac
     clock.mark("sample tables");
     const size_t S1 = S ? S : 1;
     const size_t groups = 5 * S1 + 16 * (size_t)(nclusters + 1);
-    cudaError_t e = upload(&ss.origin_st, origin_st);
-    if (e == cudaSuccess) e = upload(&ss.cell, cell);
-    if (e == cudaSuccess) e = upload(&ss.wind, wind);
-    if (e == cudaSuccess) e = upload(&ss.points, p4);
+    cudaError_t e = stage_table(stager, stream, &ss.origin_st, origin_st);
+    if (e == cudaSuccess) e = stage_table(stager, stream, &ss.cell, cell);
+    if (e == cudaSuccess) e = stage_table(stager, stream, &ss.wind, wind);
+    if (e == cudaSuccess) e = stage_table(stager, stream, &ss.points, p4);
     if (e == cudaSuccess) e = dev_alloc(&ss.intensity, sizeof(float) * S1);
     if (e == cudaSuccess) e = dev_alloc(&ss.processed, S1);
     if (e == cudaSuccess) e = dev_alloc(&ss.selected, sizeof(int32_t) * S1);

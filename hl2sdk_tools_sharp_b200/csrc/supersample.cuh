@@ -64,7 +64,8 @@ struct SupersampleBuffers {
 // windings cannot be known).
 cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_face> &faces,
                               const std::vector<float> &vertices, const uvector<vrad_sample> &samples,
-                              const FinalBuffers &fb, int32_t nclusters, bool &have, std::string &why);
+                              const FinalBuffers &fb, int32_t nclusters, Stager &stager, cudaStream_t stream,
+                              bool &have, std::string &why);
 
 // The supersampling passes over `light` (the direct gather's output, one
 // float4 per sample), on `stream`.  Blocks once per pass.

@@ -184,21 +184,13 @@ int32_t build_all_samples(const vrad_face *faces, int32_t nfaces, const float *v
     all.samples.assign((size_t)nfaces, {});
     all.wind.assign(windings ? (size_t)nfaces : 0, {});
     all.pts.assign(windings ? (size_t)nfaces : 0, {});
-    std::atomic<int32_t> next{0};
     std::atomic<int32_t> rc{VRAD_OK};
-    auto work = [&]() {
-        for (int32_t f; (f = next.fetch_add(1)) < nfaces;) {
-            const int32_t r = face_samples(faces[f], f, vertices, nvertices, all.samples[(size_t)f],
-                                           windings ? &all.wind[(size_t)f] : nullptr,
-                                           windings ? &all.pts[(size_t)f] : nullptr);
-            if (r != VRAD_OK) rc = r;
-        }
-    };
-    const unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-    std::vector<std::thread> pool;
-    for (unsigned t = 1; t < nt && (int32_t)t < nfaces; t++) pool.emplace_back(work);
-    work();
-    for (auto &t : pool) t.join();
+    vrad::parallel_for(nfaces, 1, [&](int64_t f) {
+        const int32_t r = face_samples(faces[f], (int32_t)f, vertices, nvertices, all.samples[(size_t)f],
+                                       windings ? &all.wind[(size_t)f] : nullptr,
+                                       windings ? &all.pts[(size_t)f] : nullptr);
+        if (r != VRAD_OK) rc = r;
+    });
     return rc;
 }
 
