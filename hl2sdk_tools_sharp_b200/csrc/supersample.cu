@@ -325,44 +325,24 @@ cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_fac
     ss.release();
     have = false;
     SetupClock clock("supersample_tables");
-    uvector<int32_t> wind_flat;
-    uvector<float> pts;
-    if (!sample_windings(faces.data(), (int32_t)faces.size(), vertices.data(), (int64_t)vertices.size() / 3,
-                         samples.data(), (int64_t)samples.size(), wind_flat, pts)) {
-        why = "the samples are not the face sample builder's own, so their cell windings are unknown";
+    // The faces' row strips on the host, their cells on the device, which
+    // checks that the world's samples are the builder's own.
+    RowStrips rs;
+    if (!face_row_strips(faces.data(), (int32_t)faces.size(), vertices.data(), (int64_t)vertices.size() / 3, rs, why))
         return cudaSuccess;
+    clock.mark("row strips");
+    bool match = false;
+    cudaError_t e = device_windings(ss, rs, fb.view, samples, stager, stream, match, why);
+    if (e != cudaSuccess || !match) {
+        ss.release();
+        if (e != cudaSuccess) why = "supersampling windings";
+        return e;
     }
     clock.mark("windings");
     const size_t S = samples.size();
-    std::vector<FaceFrameOut> fr(faces.size());
-    std::vector<int32_t> face_cells(faces.size() + 1, 0);
-    for (size_t f = 0; f < faces.size(); f++) {
-        face_frame_of(faces[f], fr[f]);
-        face_cells[f + 1] = face_cells[f] + fr[f].width * fr[f].height;
-    }
-    uvector<float2> origin_st(S);
-    uvector<int32_t> cell(S);
-    uvector<int2> wind(S);
-    parallel_for((int64_t)S, 1 << 15, [&](int64_t ii) {
-        const size_t i = (size_t)ii;
-        const vrad_sample &sm = samples[i];
-        const FaceFrameOut &q = fr[(size_t)sm.face];
-        frame_world_to_luxel(q, sm.position, origin_st[i].x, origin_st[i].y);
-        cell[i] = face_cells[(size_t)sm.face] + sm.s + sm.t * q.width;
-        wind[i] = make_int2(wind_flat[2 * i], wind_flat[2 * i + 1]);
-    });
-    uvector<float4> p4(pts.size() / 3);
-    parallel_for((int64_t)p4.size(), 1 << 16, [&](int64_t k) {
-        p4[(size_t)k] = make_float4(pts[3 * k], pts[3 * k + 1], pts[3 * k + 2], 0.0f);
-    });
-    clock.mark("sample tables");
     const size_t S1 = S ? S : 1;
     const size_t groups = 5 * S1 + 16 * (size_t)(nclusters + 1);
-    cudaError_t e = stage_table(stager, stream, &ss.origin_st, origin_st);
-    if (e == cudaSuccess) e = stage_table(stager, stream, &ss.cell, cell);
-    if (e == cudaSuccess) e = stage_table(stager, stream, &ss.wind, wind);
-    if (e == cudaSuccess) e = stage_table(stager, stream, &ss.points, p4);
-    if (e == cudaSuccess) e = dev_alloc(&ss.intensity, sizeof(float) * S1);
+    e = dev_alloc(&ss.intensity, sizeof(float) * S1);
     if (e == cudaSuccess) e = dev_alloc(&ss.processed, S1);
     if (e == cudaSuccess) e = dev_alloc(&ss.selected, sizeof(int32_t) * S1);
     if (e == cudaSuccess) e = dev_alloc(&ss.counts, sizeof(int32_t) * (1 + 2 * (size_t)nclusters));
@@ -376,8 +356,7 @@ cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_fac
         why = "supersampling buffers";
         return e;
     }
-    clock.mark("upload");
-    (void)fb;
+    clock.mark("buffers");
     ss.nsamples = (int64_t)S;
     ss.nclusters = nclusters;
     ss.ready = true;

@@ -29,6 +29,7 @@
 #include "final.cuh"
 #include "host_parallel.h"
 #include "scene.cuh"
+#include "world.h"
 
 namespace vrad {
 
@@ -66,6 +67,14 @@ cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_fac
                               const std::vector<float> &vertices, const uvector<vrad_sample> &samples,
                               const FinalBuffers &fb, int32_t nclusters, Stager &stager, cudaStream_t stream,
                               bool &have, std::string &why);
+
+// The partial cells' windings, the samples' luxel origins and cells,
+// rebuilt on the device from the faces' row strips (windings.cu) into
+// ss.wind, ss.points, ss.cell and ss.origin_st; match = the world's
+// samples are the builder's own (else `why`).  Synchronises `stream`.
+cudaError_t device_windings(SupersampleBuffers &ss, const RowStrips &rs, const FinalView &fv,
+                            const uvector<vrad_sample> &samples, Stager &stager, cudaStream_t stream, bool &match,
+                            std::string &why);
 
 // The supersampling passes over `light` (the direct gather's output, one
 // float4 per sample), on `stream`.  Blocks once per pass.

@@ -90,20 +90,11 @@ float world_area_per_luxel(const vrad_face &f) {
 
 namespace {
 
-// FaceSampleBuilder.BuildFacesamples for one face (number fi): its samples
-// appended to `out`.  With wind set, also each partial sample's cell winding
-// in world space (the reference keeps them for supersampling, MakeSample
-// with do_extra: FaceSampleBuilder.cs:325-367): wind gets (first point,
-// count) per sample, count 0 for a whole cell, points indexing pts.
-int32_t face_samples(const vrad_face &f, int32_t fi, const float *vertices, int64_t nvertices,
-                     std::vector<vrad_sample> &out, std::vector<int32_t> *wind, std::vector<float> *pts) {
-    if (f.num_vertices < 3 || f.first_vertex < 0 || f.first_vertex + (int64_t)f.num_vertices > nvertices)
-        return VRAD_ERR_ARG;
-    Winding cell_front, cell_back, row_front, row_back;
-    const FaceFrame fr = face_frame(f);
-    const float area_per_luxel = world_area_per_luxel(f);
-    // LightmapCoordWinding: the face's winding in luxel space.
-    Winding w;
+// LightmapCoordWinding: face f's winding, colinear points removed, in
+// luxel space (z 0).  False when it lies outside the vertex array.
+bool luxel_winding(const vrad_face &f, const float *vertices, int64_t nvertices, const FaceFrame &fr, Winding &w) {
+    if (f.num_vertices < 3 || f.first_vertex < 0 || f.first_vertex + (int64_t)f.num_vertices > nvertices) return false;
+    w.clear();
     for (int32_t k = 0; k < f.num_vertices; k++) {
         const float *v = vertices + 3 * (int64_t)(f.first_vertex + k);
         w.push_back(add(V3{v[0], v[1], v[2]}, V3{0.0f, 0.0f, 0.0f}));
@@ -113,6 +104,17 @@ int32_t face_samples(const vrad_face &f, int32_t fi, const float *vertices, int6
         V3 pos = sub(p, fr.origin);
         p = {dot(pos, fr.w2l_s) - (float)fr.min_s, dot(pos, fr.w2l_t) - (float)fr.min_t, 0.0f};
     }
+    return true;
+}
+
+// FaceSampleBuilder.BuildFacesamples for one face (number fi): its samples
+// appended to `out`.
+int32_t face_samples(const vrad_face &f, int32_t fi, const float *vertices, int64_t nvertices,
+                     std::vector<vrad_sample> &out) {
+    Winding cell_front, cell_back, row_front, row_back, w;
+    const FaceFrame fr = face_frame(f);
+    const float area_per_luxel = world_area_per_luxel(f);
+    if (!luxel_winding(f, vertices, nvertices, fr, w)) return VRAD_ERR_ARG;
     // BuildFacesamples: rows by t, cells by s, sample offset 1.0.
     Winding lm = w;
     for (int t = 0; t < fr.height && !lm.empty(); t++) {
@@ -129,21 +131,6 @@ int32_t face_samples(const vrad_face &f, int32_t fi, const float *vertices, int6
                     if (p.x > mx[0]) mx[0] = p.x;
                     if (p.y < mn[1]) mn[1] = p.y;
                     if (p.y > mx[1]) mx[1] = p.y;
-                }
-                if (wind) {
-                    // EQUAL_EPSILON is a double literal: the test is in double.
-                    int32_t first = (int32_t)(pts->size() / 3), n = 0;
-                    if ((double)area < (double)area_per_luxel - 0.001) {
-                        for (const V3 &p : cell_back) {
-                            const V3 q = luxel_to_world(fr, p.x, p.y);
-                            pts->push_back(q.x);
-                            pts->push_back(q.y);
-                            pts->push_back(q.z);
-                            n++;
-                        }
-                    }
-                    wind->push_back(n ? first : 0);
-                    wind->push_back(n);
                 }
                 vrad_sample o;
                 V3 pos = luxel_to_world(fr, center.x, center.y);
@@ -171,24 +158,14 @@ int32_t face_samples(const vrad_face &f, int32_t fi, const float *vertices, int6
 }
 
 // Every face's samples, faces built in parallel (each face's samples
-// depend on that face alone), concatenated in face order.
-struct AllSamples {
-    std::vector<std::vector<vrad_sample>> samples;
-    std::vector<std::vector<int32_t>> wind;
-    std::vector<std::vector<float>> pts;
-};
-
+// depend on that face alone), one list per face.
 int32_t build_all_samples(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
-                          bool windings, AllSamples &all) {
+                          std::vector<std::vector<vrad_sample>> &all) {
     if (nfaces < 0 || (nfaces > 0 && (!faces || !vertices))) return VRAD_ERR_ARG;
-    all.samples.assign((size_t)nfaces, {});
-    all.wind.assign(windings ? (size_t)nfaces : 0, {});
-    all.pts.assign(windings ? (size_t)nfaces : 0, {});
+    all.assign((size_t)nfaces, {});
     std::atomic<int32_t> rc{VRAD_OK};
     vrad::parallel_for(nfaces, 1, [&](int64_t f) {
-        const int32_t r = face_samples(faces[f], (int32_t)f, vertices, nvertices, all.samples[(size_t)f],
-                                       windings ? &all.wind[(size_t)f] : nullptr,
-                                       windings ? &all.pts[(size_t)f] : nullptr);
+        const int32_t r = face_samples(faces[f], (int32_t)f, vertices, nvertices, all[(size_t)f]);
         if (r != VRAD_OK) rc = r;
     });
     return rc;
@@ -200,57 +177,102 @@ extern "C" int32_t vrad_build_samples(const vrad_face *faces, int32_t nfaces, co
                                       int64_t nvertices, vrad_sample *out, int64_t capacity,
                                       int64_t *count, int64_t *face_first) {
     if (!count) return VRAD_ERR_ARG;
-    AllSamples all;
-    const int32_t rc = build_all_samples(faces, nfaces, vertices, nvertices, false, all);
+    std::vector<std::vector<vrad_sample>> all;
+    const int32_t rc = build_all_samples(faces, nfaces, vertices, nvertices, all);
     if (rc != VRAD_OK) return rc;
-    int64_t written = 0;
-    for (int32_t f = 0; f < nfaces; f++) {
-        if (face_first) face_first[f] = written;
-        const auto &v = all.samples[(size_t)f];
-        if (out) {
-            if (written + (int64_t)v.size() > capacity) {
-                *count = written;
-                return VRAD_ERR_ARG;
-            }
-            std::memcpy(out + written, v.data(), sizeof(vrad_sample) * v.size());
-        }
-        written += (int64_t)v.size();
+    std::vector<int64_t> first((size_t)nfaces + 1, 0);
+    for (int32_t f = 0; f < nfaces; f++) first[(size_t)f + 1] = first[(size_t)f] + (int64_t)all[(size_t)f].size();
+    const int64_t total = first[(size_t)nfaces];
+    if (face_first) std::copy(first.begin(), first.end(), face_first);
+    *count = total;
+    if (out) {
+        if (total > capacity) return VRAD_ERR_ARG;
+        vrad::parallel_for(nfaces, 16, [&](int64_t f) {
+            const auto &v = all[(size_t)f];
+            if (!v.empty()) std::memcpy(out + first[(size_t)f], v.data(), sizeof(vrad_sample) * v.size());
+        });
     }
-    if (face_first) face_first[nfaces] = written;
-    *count = written;
     return VRAD_OK;
 }
 
 namespace vrad {
 
-bool sample_windings(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
-                     const vrad_sample *given, int64_t ngiven, uvector<int32_t> &wind, uvector<float> &pts) {
-    AllSamples all;
-    if (build_all_samples(faces, nfaces, vertices, nvertices, true, all) != VRAD_OK) return false;
-    // Each face's first sample and first point, then the comparison and the
-    // copies face by face in parallel.
-    std::vector<int64_t> s0((size_t)nfaces + 1, 0), p0((size_t)nfaces + 1, 0);
-    for (int32_t f = 0; f < nfaces; f++) {
-        s0[(size_t)f + 1] = s0[(size_t)f] + (int64_t)all.samples[(size_t)f].size();
-        p0[(size_t)f + 1] = p0[(size_t)f] + (int64_t)all.pts[(size_t)f].size();
-    }
-    if (s0[(size_t)nfaces] != ngiven) return false;
-    wind.resize(2 * (size_t)ngiven);
-    pts.resize((size_t)p0[(size_t)nfaces]);
-    std::atomic<bool> same{true};
-    parallel_for(nfaces, 16, [&](int64_t f) {
-        const auto &v = all.samples[(size_t)f];
-        if (!v.empty() && std::memcmp(v.data(), given + s0[(size_t)f], sizeof(vrad_sample) * v.size()) != 0) same = false;
-        const int32_t base = (int32_t)(p0[(size_t)f] / 3);
-        const auto &wf = all.wind[(size_t)f];
-        int32_t *w = &wind[2 * (size_t)s0[(size_t)f]];
-        for (size_t i = 0; i < wf.size(); i += 2) {
-            *w++ = wf[i + 1] ? wf[i] + base : 0;
-            *w++ = wf[i + 1];
+bool face_row_strips(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices, RowStrips &out,
+                     std::string &why) {
+    struct Rows {
+        std::vector<int32_t> t;
+        std::vector<int32_t> n;
+        std::vector<float> xy;
+        bool ok = true, big = false;
+    };
+    std::vector<Rows> per((size_t)nfaces);
+    out.apl.assign((size_t)nfaces, 0.0f);
+    parallel_for(nfaces, 4, [&](int64_t fi) {
+        const vrad_face &f = faces[fi];
+        Rows &r = per[(size_t)fi];
+        const FaceFrame fr = face_frame(f);
+        out.apl[(size_t)fi] = world_area_per_luxel(f);
+        Winding w, row_front, row_back;
+        if (!luxel_winding(f, vertices, nvertices, fr, w)) {
+            r.ok = false;
+            return;
         }
-        std::copy(all.pts[(size_t)f].begin(), all.pts[(size_t)f].end(), pts.begin() + p0[(size_t)f]);
+        if ((int32_t)w.size() > kStripMax) {
+            r.big = true;
+            return;
+        }
+        // BuildFacesamples' rows: the winding's part between t and t + 1,
+        // the rest carried to the next row.
+        Winding lm = w;
+        for (int t = 0; t < fr.height && !lm.empty(); t++) {
+            clip_axis(lm, 1, (float)t + 1.0f, kLightmapOnEpsilon, row_front, row_back);
+            if (!row_back.empty()) {
+                r.t.push_back(t);
+                r.n.push_back((int32_t)row_back.size());
+                for (const V3 &p : row_back) {
+                    r.xy.push_back(p.x);
+                    r.xy.push_back(p.y);
+                }
+            }
+            lm = row_front;
+        }
     });
-    return same.load();
+    size_t nrows = 0, npts = 0;
+    for (const Rows &r : per) {
+        if (!r.ok) {
+            why = "a face's winding lies outside the vertex array";
+            return false;
+        }
+        if (r.big) {
+            why = "a face's winding has more than 56 points";
+            return false;
+        }
+        nrows += r.t.size();
+        npts += r.xy.size() / 2;
+    }
+    out.face.resize(nrows);
+    out.t.resize(nrows);
+    out.first.resize(nrows + 1);
+    out.xy.resize(2 * npts);
+    std::vector<size_t> row0((size_t)nfaces + 1, 0), pt0((size_t)nfaces + 1, 0);
+    for (int32_t f = 0; f < nfaces; f++) {
+        row0[(size_t)f + 1] = row0[(size_t)f] + per[(size_t)f].t.size();
+        pt0[(size_t)f + 1] = pt0[(size_t)f] + per[(size_t)f].xy.size() / 2;
+    }
+    out.first[nrows] = (int64_t)npts;
+    parallel_for(nfaces, 16, [&](int64_t f) {
+        const Rows &r = per[(size_t)f];
+        size_t k = row0[(size_t)f];
+        int64_t p = (int64_t)pt0[(size_t)f];
+        for (size_t i = 0; i < r.t.size(); i++, k++) {
+            out.face[k] = (int32_t)f;
+            out.t[k] = r.t[i];
+            out.first[k] = p;
+            p += r.n[i];
+        }
+        std::copy(r.xy.begin(), r.xy.end(), out.xy.begin() + 2 * pt0[(size_t)f]);
+    });
+    return true;
 }
 
 }  // namespace vrad

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "../../include/vrad_cuda.h"
@@ -24,13 +25,22 @@ void face_frame_of(const vrad_face &f, FaceFrameOut &out);
 void frame_luxel_to_world(const FaceFrameOut &fr, float s, float t, float out[3]);
 void frame_world_to_luxel(const FaceFrameOut &fr, const float p[3], float &s, float &t);
 
-// The cell windings (world space) of the partial samples, as
-// FaceSampleBuilder keeps them for supersampling: wind holds (first point,
-// count) per sample, count 0 for a sample whose cell the face covers
-// whole; pts the points (xyz each).  False unless the samples the builder
-// makes from these faces are exactly `given`.
-bool sample_windings(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
-                     const vrad_sample *given, int64_t ngiven, uvector<int32_t> &wind, uvector<float> &pts);
+// BuildFacesamples' row strips of every face, for the cell clipping on the
+// device (windings.cu): row k is face[k]'s strip t[k], the luxel-space
+// winding's part between t and t + 1 as the builder cuts it, its points
+// (luxel x, y; z is 0) at xy[2 first[k] ..] (first[nrows] = the point
+// count); apl = each face's world area per luxel.  Rows the builder leaves
+// empty are left out.  False, with `why`, when a face's winding lies
+// outside the vertex array or has more than kStripMax points.
+constexpr int kStripMax = 56;
+struct RowStrips {
+    std::vector<int32_t> face, t;
+    std::vector<int64_t> first;
+    uvector<float> xy;
+    std::vector<float> apl;
+};
+bool face_row_strips(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices, RowStrips &out,
+                     std::string &why);
 
 // The welded vertex numbers of each face's winding (vertices identified by
 // position) and, per vertex, the faces touching it in face order.  False

@@ -122,3 +122,37 @@ def test_3x3_supersampling_counts_and_noextra(oracle_mod):
     changed = (bits(g_ss) != bits(g_plain)).any(1)
     assert changed.sum() > 0.5 * ss_stats.supersampled
     assert ss_stats.visibility_rays + ss_stats.sky_rays > plain_stats.visibility_rays + plain_stats.sky_rays
+
+
+@pytest.mark.parametrize("change", ["area", "coord", "mins", "position", "swap"])
+def test_supersampling_refuses_samples_not_the_builders(change):
+    # Supersampling needs each partial sample's cell winding, which the
+    # library rebuilds from the faces; it accepts the world's samples only
+    # when they are the sample builder's own, bit for bit.  One changed
+    # field (or two samples of a face swapped) makes the gather refuse the
+    # passes; with them off it still runs.
+    w = rg.generate(rg.config_3x3(seed=2))
+    inp = L.prepare(w)
+    s = inp.samples.copy()
+    ff = inp.face_first
+    face = int(np.argmax(np.diff(ff)))
+    k = int(ff[face]) + 1
+    if change == "area":
+        s["area"][k] = np.nextafter(s["area"][k], np.float32(np.inf))
+    elif change == "coord":
+        s["coord"][k, 1] = np.nextafter(s["coord"][k, 1], np.float32(-np.inf))
+    elif change == "mins":
+        s["mins"][k, 0] = np.nextafter(s["mins"][k, 0], np.float32(-np.inf))
+    elif change == "position":
+        s["position"][k, 2] = np.nextafter(s["position"][k, 2], np.float32(np.inf))
+    else:
+        s[[k, k + 1]] = s[[k + 1, k]]
+    changed = L.LightingInputs(**{**inp.__dict__, "samples": s})
+    with L.LightingStage(w, changed) as st:
+        with pytest.raises(NotImplementedError, match="builder's own"):
+            st.direct()
+        st.set_extra_passes(0)
+        plain, stats = st.direct()
+        assert stats.supersampled == 0 and len(plain) == len(s)
+    with L.LightingStage(w, inp) as st:
+        st.direct()
