@@ -327,19 +327,30 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     const int32_t nleaves = (int32_t)leaf_desc.size();
     std::vector<int32_t> leaf_rank((size_t)P, -1);
     for (int32_t k = 0; k < nleaves; k++) leaf_rank[(size_t)leaf_desc[(size_t)k]] = k;
-    // Each parent's level (1 + its deeper child's; leaves 0): children
-    // have higher indices than their parent, so one descending pass; then
-    // the parents grouped by level, index order within a level.
+    // Each parent's level (1 + its deeper child's; leaves 0): a face's
+    // tree is its root and its descendants, children numbered above their
+    // parent, so one descending pass per face, faces in parallel; then the
+    // parents grouped by level, index order within a level.
     std::vector<uint8_t> level((size_t)P, 0);
+    std::vector<int32_t> face_top((size_t)nf, 0);
+    parallel_for(nf, 16, [&](int64_t f) {
+        const int32_t root = tree.face_root[(size_t)f];
+        if (root < 0) return;
+        int32_t top_f = 0;
+        auto visit = [&](int32_t i) {
+            const int4 t = tr[(size_t)i];
+            if (t.y == -1) return;
+            const int h = 1 + std::max(level[(size_t)t.y], level[(size_t)t.z]);
+            level[(size_t)i] = (uint8_t)std::min(h, 255);
+            top_f = std::max(top_f, h);
+        };
+        for (int32_t i = tree.face_end[(size_t)f] - 1; i >= tree.face_first[(size_t)f]; i--) visit(i);
+        visit(root);
+        face_top[(size_t)f] = top_f;
+    });
     int32_t top = 0;
-    for (int32_t i = P - 1; i >= 0; i--) {
-        const int4 t = tr[(size_t)i];
-        if (t.y == -1) continue;
-        const int h = 1 + std::max(level[(size_t)t.y], level[(size_t)t.z]);
-        if (h > 255) return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "patch %d's subtree is deeper than 255 levels", i);
-        level[(size_t)i] = (uint8_t)h;
-        top = std::max(top, h);
-    }
+    for (int32_t f = 0; f < nf; f++) top = std::max(top, face_top[(size_t)f]);
+    if (top > 255) return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "a patch's subtree is deeper than 255 levels");
     std::vector<int32_t> level_off((size_t)top + 2, 0);
     for (int32_t i = 0; i < P; i++)
         if (level[(size_t)i]) level_off[(size_t)level[(size_t)i] + 1]++;

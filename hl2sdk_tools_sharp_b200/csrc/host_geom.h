@@ -54,13 +54,13 @@ inline Winding remove_colinear(const Winding &w) {
     return kept.size() == n ? w : kept;
 }
 
-// WindingArena.ClipEpsilon against the axis plane p[ax] = dist (normal the
-// unit axis).  front: the d > eps side; back: d < -eps; points within eps
-// go to both.  An empty vector is the reference's null winding.
-inline void clip_axis(const Winding &in, int ax, float dist, float eps, Winding &front, Winding &back) {
+// WindingArena.ClipEpsilon of the n points at `in` against the axis plane
+// p[ax] = dist (normal the unit axis).  front: the d > eps side; back:
+// d < -eps; points within eps go to both.  An empty vector is the
+// reference's null winding.  `in` must not alias either output.
+inline void clip_axis(const V3 *in, size_t n, int ax, float dist, float eps, Winding &front, Winding &back) {
     front.clear();
     back.clear();
-    const size_t n = in.size();
     // Windings here have a handful of points: local arrays, a heap
     // fallback only past 63.
     float dist_buf[64];
@@ -88,11 +88,11 @@ inline void clip_axis(const Winding &in, int ax, float dist, float eps, Winding 
     sides[n] = sides[0];
     dists[n] = dists[0];
     if (counts[0] == 0) {
-        back = in;
+        back.assign(in, in + n);
         return;
     }
     if (counts[1] == 0) {
-        front = in;
+        front.assign(in, in + n);
         return;
     }
     for (size_t i = 0; i < n; i++) {
@@ -116,6 +116,10 @@ inline void clip_axis(const Winding &in, int ax, float dist, float eps, Winding 
         front.push_back(mid);
         back.push_back(mid);
     }
+}
+
+inline void clip_axis(const Winding &in, int ax, float dist, float eps, Winding &front, Winding &back) {
+    clip_axis(in.data(), in.size(), ax, dist, eps, front, back);
 }
 
 // WindingArena.Area: fan from point 0, cross lengths summed, halved once.

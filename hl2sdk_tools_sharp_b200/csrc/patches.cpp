@@ -48,7 +48,11 @@ struct Builder {
     const std::vector<std::vector<float>> *corner_normals;  // per face, xyz per winding vertex
     const std::vector<V3> *centroids;                       // PatchSet.Centroids
     std::vector<vrad_patch> patches;
-    std::vector<Winding> windings;
+    // The patches' windings, one flat array: patch k's points are
+    // pts[wfirst[k] .. wfirst[k] + wcount[k]).
+    std::vector<V3> pts;
+    std::vector<int32_t> wfirst, wcount;
+    Winding o1, o2;  // SubdividePatch's halves (scratch)
 
     V3 vertex(int32_t f, int32_t k) const {
         const vrad_face &fc = faces[f];
@@ -83,9 +87,11 @@ struct Builder {
         return fn;
     }
 
-    int32_t add_patch(const vrad_patch &p, Winding w) {
+    int32_t add_patch(const vrad_patch &p, const Winding &w) {
         patches.push_back(p);
-        windings.push_back(std::move(w));
+        wfirst.push_back((int32_t)pts.size());
+        wcount.push_back((int32_t)w.size());
+        pts.insert(pts.end(), w.begin(), w.end());
         return (int32_t)patches.size() - 1;
     }
 
@@ -156,8 +162,7 @@ struct Builder {
         }
         if (!split) return;
         const float dist = (comp(mn, widest_axis) + comp(mx, widest_axis)) * 0.5f;
-        Winding o1, o2;
-        clip_axis(windings[(size_t)i], widest_axis, dist, kOnEpsilon, o1, o2);
+        clip_axis(pts.data() + wfirst[(size_t)i], (size_t)wcount[(size_t)i], widest_axis, dist, kOnEpsilon, o1, o2);
         V3 c1, c2;
         const float a1 = area_and_balance(o1, c1);
         const float a2 = area_and_balance(o2, c2);
@@ -264,7 +269,7 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
         total += (int32_t)subtree[(size_t)i].patches.size() - 1;
     }
     out.patches.resize((size_t)total);
-    uvector<const Winding *> wind((size_t)total);
+    uvector<const V3 *> wind((size_t)total);  // each patch's points in its builder's array
     uvector<int64_t> first((size_t)total + 1);
     out.face_first.assign((size_t)nfaces, 0);
     out.face_end.assign((size_t)nfaces, 0);
@@ -280,8 +285,8 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
             p.child2 = global(p.child2);
             const int32_t g = global((int32_t)k);
             out.patches[(size_t)g] = p;
-            wind[(size_t)g] = &b.windings[k];
-            first[(size_t)g + 1] = (int64_t)b.windings[k].size();
+            wind[(size_t)g] = b.pts.data() + b.wfirst[k];
+            first[(size_t)g + 1] = (int64_t)b.wcount[k];
         }
     });
     for (int32_t i = 0; i < roots; i++) {
@@ -302,17 +307,14 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
         p.first_point = (int32_t)first[(size_t)i];
         p.num_points = (int32_t)(first[(size_t)i + 1] - first[(size_t)i]);
         float *dst = &out.points[(size_t)first[(size_t)i] * 3];
-        for (const V3 &v : *wind[(size_t)i]) {
-            *dst++ = v.x;
-            *dst++ = v.y;
-            *dst++ = v.z;
+        const V3 *src = wind[(size_t)i];
+        for (int32_t k = 0; k < p.num_points; k++) {
+            *dst++ = src[k].x;
+            *dst++ = src[k].y;
+            *dst++ = src[k].z;
         }
     });
     clock.mark("points");
-    // The builders' windings (one small vector per patch) freed in
-    // parallel rather than by one thread on return.
-    parallel_for(roots, 8, [&](int64_t i) { Builder gone = std::move(subtree[(size_t)i]); });
-    clock.mark("free");
     out.roots = roots;
     return true;
 }
