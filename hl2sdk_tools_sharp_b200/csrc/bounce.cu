@@ -265,9 +265,12 @@ __device__ float poly_to_diff(const BounceView &v, int s, float area, F3 o, F3 n
 
 // One candidate pair: VisMatrix.TransferRay traced (StockExact: every
 // triangle blocks, t in (0, len)), then MakeTransfer.  cand_w = the
-// transfer, 0 for none.
+// transfer, 0 for none.  Twelve CTAs per SM (40 registers, a few spilled
+// to L1): the walk is latency-bound, and the extra resident warps hide
+// more of it than the spills cost (measured 66 against 72 ms at 64
+// registers and 8 CTAs on the 8x8 map).
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_transfer(BounceView v, DeviceScene sc, const int64_t *__restrict__ cand_off,
+__global__ void __launch_bounds__(BLOCK, 12) k_transfer(BounceView v, DeviceScene sc, const int64_t *__restrict__ cand_off,
                                                     const int32_t *__restrict__ cand_src, float *__restrict__ cand_w,
                                                     int64_t ncand, unsigned long long *counters, uint32_t *overflow) {
     extern __shared__ int stack_mem[];  // sc.stack_depth() entries per thread

@@ -100,7 +100,10 @@ __device__ __forceinline__ void slab2(const float4 &a, const float4 &b, const fl
 // (thi, best_orig); best_orig = -1 makes the window half-open, [tmin, thi).
 // ANY stops at the first acceptance; otherwise the best is kept and the
 // box window shrinks to [tmin, thi].  Returns whether anything was accepted.
-template <bool ANY, int STRIDE = kBlock>
+// Of two children the segment meets, the nearer is entered first, or with
+// FAR the farther (an any-hit walk may find its blocker sooner from the far
+// end; which order pays is measured per caller).
+template <bool ANY, int STRIDE = kBlock, bool FAR = false>
 __device__ __forceinline__ bool walk(const DeviceBvh &s, const int32_t *__restrict__ tri_id,
                                      const RayState &r, float tmin, int32_t skip_id, int *stack,
                                      uint32_t *overflow, float &thi, int32_t &best_orig,
@@ -118,7 +121,7 @@ __device__ __forceinline__ bool walk(const DeviceBvh &s, const int32_t *__restri
             const int r0 = __float_as_int(d.x), r1 = __float_as_int(d.y);
             if (h0 && h1) {
                 int near_ref = r0, far_ref = r1;
-                if (n1 < n0) {
+                if (FAR ? (n1 > n0) : (n1 < n0)) {
                     near_ref = r1;
                     far_ref = r0;
                 }
@@ -171,7 +174,8 @@ __device__ __forceinline__ bool walk(const DeviceBvh &s, const int32_t *__restri
 //                 nearest sky hit (t_s, i_s) is found first, then any
 //                 opaque hit below it decides, so the opaque walk stops at
 //                 its first acceptance.
-template <int MODE, int STRIDE = kBlock>
+// FAR_ANY: the any-hit walks enter the farther child first (walk's FAR).
+template <int MODE, int STRIDE = kBlock, bool FAR_ANY = false>
 __device__ __forceinline__ void trace_ray(const DeviceScene &s, const RayState &r, float tmin,
                                           float reach, int32_t skip_id, int *stack,
                                           uint32_t *overflow, bool &hit, float &best_t,
@@ -182,9 +186,9 @@ __device__ __forceinline__ void trace_ray(const DeviceScene &s, const RayState &
     hit = false;
     if (MODE == kModeAny) {
         if (s.opaque.ntris)
-            hit = walk<true, STRIDE>(s.opaque, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
+            hit = walk<true, STRIDE, FAR_ANY>(s.opaque, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
         if (!hit && s.sky.ntris)
-            hit = walk<true, STRIDE>(s.sky, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
+            hit = walk<true, STRIDE, FAR_ANY>(s.sky, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
     } else if (MODE == kModeClosest) {
         if (s.opaque.ntris)
             hit = walk<false, STRIDE>(s.opaque, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
@@ -195,7 +199,7 @@ __device__ __forceinline__ void trace_ray(const DeviceScene &s, const RayState &
             walk<false, STRIDE>(s.sky, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
         // Blocked iff an opaque hit sorts before the nearest sky hit.
         if (s.opaque.ntris)
-            hit = walk<true, STRIDE>(s.opaque, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
+            hit = walk<true, STRIDE, FAR_ANY>(s.opaque, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig, best_meta);
     }
 }
 
