@@ -309,24 +309,47 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
         if (face_samples[(size_t)f].y) face_samples[(size_t)f].y -= face_samples[(size_t)f].x;
     clock.mark("patch tables");
     // VisMatrix.ReceiverOrder: cluster by cluster, leaf patches in index
-    // order (a stable counting sort on the leaves' clusters).
+    // order (a stable counting sort on the leaves' clusters), and the
+    // sky-free leaves in descending index order; both in chunks of patches
+    // on worker threads, each chunk's place found from the counts of the
+    // chunks before it.
+    constexpr int32_t kChunk = 1 << 16;
+    const int32_t nchunks = (P + kChunk - 1) / kChunk;
+    std::vector<int32_t> ccount((size_t)nchunks * (size_t)(C + 1), 0);  // per chunk: C cluster counts, sky-free leaves
+    parallel_for(nchunks, 1, [&](int64_t k) {
+        int32_t *cc = &ccount[(size_t)k * (size_t)(C + 1)];
+        for (int32_t i = (int32_t)k * kChunk; i < std::min(P, (int32_t)(k + 1) * kChunk); i++) {
+            if (leaf_cluster[(size_t)i] >= 0) cc[leaf_cluster[(size_t)i]]++;
+            if (tr[(size_t)i].y == -1 && !tr[(size_t)i].w) cc[C]++;
+        }
+    });
     std::vector<int32_t> cstart((size_t)C + 1, 0);
-    for (int32_t i = 0; i < P; i++)
-        if (leaf_cluster[(size_t)i] >= 0) cstart[(size_t)leaf_cluster[(size_t)i] + 1]++;
-    for (int32_t c = 0; c < C; c++) cstart[(size_t)c + 1] += cstart[(size_t)c];
-    std::vector<int32_t> recv((size_t)cstart[(size_t)C]);
-    {
-        std::vector<int32_t> at(cstart.begin(), cstart.end() - 1);
-        for (int32_t i = 0; i < P; i++)
-            if (leaf_cluster[(size_t)i] >= 0) recv[(size_t)at[(size_t)leaf_cluster[(size_t)i]]++] = i;
+    std::vector<int32_t> chunk_at((size_t)nchunks * (size_t)(C + 1));
+    for (int32_t c = 0; c < C; c++) {
+        int32_t at = cstart[(size_t)c];
+        for (int32_t k = 0; k < nchunks; k++) {
+            chunk_at[(size_t)k * (size_t)(C + 1) + c] = at;
+            at += ccount[(size_t)k * (size_t)(C + 1) + c];
+        }
+        cstart[(size_t)c + 1] = at;
     }
-    std::vector<int32_t> leaf_desc;
-    leaf_desc.reserve(recv.size());
-    for (int32_t i = P - 1; i >= 0; i--)
-        if (tr[(size_t)i].y == -1 && !tr[(size_t)i].w) leaf_desc.push_back(i);
-    const int32_t nleaves = (int32_t)leaf_desc.size();
-    std::vector<int32_t> leaf_rank((size_t)P, -1);
-    for (int32_t k = 0; k < nleaves; k++) leaf_rank[(size_t)leaf_desc[(size_t)k]] = k;
+    int32_t nleaves = 0;
+    for (int32_t k = nchunks - 1; k >= 0; k--) {
+        chunk_at[(size_t)k * (size_t)(C + 1) + C] = nleaves;
+        nleaves += ccount[(size_t)k * (size_t)(C + 1) + C];
+    }
+    std::vector<int32_t> recv((size_t)cstart[(size_t)C]), leaf_desc((size_t)nleaves), leaf_rank((size_t)P, -1);
+    parallel_for(nchunks, 1, [&](int64_t k) {
+        int32_t *at = &chunk_at[(size_t)k * (size_t)(C + 1)];
+        const int32_t lo = (int32_t)k * kChunk, hi = std::min(P, (int32_t)(k + 1) * kChunk);
+        for (int32_t i = lo; i < hi; i++)
+            if (leaf_cluster[(size_t)i] >= 0) recv[(size_t)at[leaf_cluster[(size_t)i]]++] = i;
+        for (int32_t i = hi - 1; i >= lo; i--)
+            if (tr[(size_t)i].y == -1 && !tr[(size_t)i].w) {
+                leaf_rank[(size_t)i] = at[C];
+                leaf_desc[(size_t)at[C]++] = i;
+            }
+    });
     // Each parent's level (1 + its deeper child's; leaves 0): a face's
     // tree is its root and its descendants, children numbered above their
     // parent, so one descending pass per face, faces in parallel; then the

@@ -349,14 +349,11 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
     for (int32_t f = 0; f < nfaces; f++) face_frame_of(faces[f], fr[(size_t)f]);
     // Neighbours (FaceNeighbours.Build, DefaultSmoothingThreshold), kept
     // for the bounce's set-up.
-    noff.assign((size_t)nfaces + 1, 0);
-    int64_t nn = 0;
-    if (vrad_build_neighbours(faces, nfaces, vertices, nvertices, 0.7071067f, noff.data(), nullptr, 0, &nn) != VRAD_OK) {
+    if (face_neighbours(faces, nfaces, vertices, nvertices, 0.7071067f, noff, nlist) != VRAD_OK) {
         why = "invalid face windings";
         return cudaErrorInvalidValue;
     }
-    nlist.assign((size_t)(nn ? nn : 1), 0);
-    vrad_build_neighbours(faces, nfaces, vertices, nvertices, 0.7071067f, noff.data(), nlist.data(), nn, &nn);
+    if (nlist.empty()) nlist.push_back(0);
     clock.mark("neighbours");
     std::vector<int32_t> lightofs((size_t)nfaces);
     int64_t total = 0;

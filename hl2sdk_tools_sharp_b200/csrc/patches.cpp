@@ -254,9 +254,20 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
     clock.mark("roots");
     // PatchSubdivider.Subdivide with bounces > 0, not -fast.  Each root's
     // subtree depends on nothing outside its face, so the roots are split
-    // on worker threads, each into its own arrays.
-    parallel_for(roots, 1, [&](int64_t i) {
-        Builder &b = subtree[(size_t)i];
+    // on worker threads, each into its own arrays; the largest faces (by
+    // luxel count, which the patch count follows) are handed out first so
+    // that no large face starts last.
+    std::vector<int32_t> by_size((size_t)roots);
+    std::vector<int64_t> luxels((size_t)roots);
+    for (int32_t i = 0; i < roots; i++) {
+        const vrad_face &fc = faces[subtree[(size_t)i].patches[0].face];
+        luxels[(size_t)i] = (int64_t)(fc.lightmap_size[0] + 1) * (fc.lightmap_size[1] + 1);
+        by_size[(size_t)i] = i;
+    }
+    std::stable_sort(by_size.begin(), by_size.end(),
+                     [&](int32_t a, int32_t b) { return luxels[(size_t)a] > luxels[(size_t)b]; });
+    parallel_for(roots, 1, [&](int64_t k) {
+        Builder &b = subtree[(size_t)by_size[(size_t)k]];
         if (!prevent_subdivision(faces[b.patches[0].face].flags)) b.subdivide(0);
     });
     clock.mark("subdivide");

@@ -281,6 +281,7 @@ bool face_row_strips(const vrad_face *faces, int32_t nfaces, const float *vertic
 
 #include <map>
 #include <tuple>
+#include <unordered_map>
 
 namespace {
 
@@ -296,24 +297,34 @@ namespace vrad {
 
 bool weld_faces(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
                 std::vector<std::vector<int32_t>> &face_verts, std::vector<std::vector<int32_t>> &vertex_face) {
-    // Weld: one vertex number per distinct position.
-    std::map<std::tuple<uint32_t, uint32_t, uint32_t>, int32_t> weld;
+    // Weld: one vertex number per distinct position, numbered in order of
+    // first appearance (faces in order, each winding in order).
+    struct Key {
+        uint32_t x, y, z;
+        bool operator==(const Key &o) const { return x == o.x && y == o.y && z == o.z; }
+    };
+    struct Hash {
+        size_t operator()(const Key &k) const {
+            uint64_t h = k.x * 0x9E3779B97F4A7C15ull;
+            h ^= (h >> 29) ^ (k.y * 0xC2B2AE3D27D4EB4Full);
+            h ^= (h >> 31) ^ (k.z * 0x165667B19E3779F9ull);
+            return (size_t)(h ^ (h >> 32));
+        }
+    };
+    std::unordered_map<Key, int32_t, Hash> weld;
+    int64_t corners = 0;
+    for (int32_t i = 0; i < nfaces; i++) corners += std::max(0, faces[i].num_vertices);
+    weld.reserve((size_t)corners);
     face_verts.assign((size_t)nfaces, {});
     for (int32_t i = 0; i < nfaces; i++) {
         const vrad_face &f = faces[i];
         if (f.first_vertex < 0 || f.num_vertices < 0 || f.first_vertex + (int64_t)f.num_vertices > nvertices) return false;
+        face_verts[(size_t)i].reserve((size_t)f.num_vertices);
         for (int32_t k = 0; k < f.num_vertices; k++) {
             const float *v = vertices + 3 * (int64_t)(f.first_vertex + k);
-            auto key = std::make_tuple(fbits(v[0] + 0.0f), fbits(v[1] + 0.0f), fbits(v[2] + 0.0f));
-            auto it = weld.find(key);
-            int32_t id;
-            if (it == weld.end()) {
-                id = (int32_t)weld.size();
-                weld.emplace(key, id);
-            } else {
-                id = it->second;
-            }
-            face_verts[(size_t)i].push_back(id);
+            const Key key = {fbits(v[0] + 0.0f), fbits(v[1] + 0.0f), fbits(v[2] + 0.0f)};
+            const auto ins = weld.emplace(key, (int32_t)weld.size());
+            face_verts[(size_t)i].push_back(ins.first->second);
         }
     }
     // vertexFace: the faces touching each vertex, in face order, once each.
@@ -331,7 +342,8 @@ bool corner_normals(const vrad_face *faces, int32_t nfaces, const float *vertice
     std::vector<std::vector<int32_t>> face_verts, vertex_face;
     if (!weld_faces(faces, nfaces, vertices, nvertices, face_verts, vertex_face)) return false;
     out.assign((size_t)nfaces, {});
-    for (int32_t i = 0; i < nfaces; i++) {
+    parallel_for(nfaces, 16, [&](int64_t ii) {
+        const int32_t i = (int32_t)ii;
         const V3 ni = {faces[i].normal[0], faces[i].normal[1], faces[i].normal[2]};
         std::vector<float> &o = out[(size_t)i];
         for (int32_t v : face_verts[(size_t)i]) {
@@ -348,7 +360,7 @@ bool corner_normals(const vrad_face *faces, int32_t nfaces, const float *vertice
             o.push_back(n.y);
             o.push_back(n.z);
         }
-    }
+    });
     return true;
 }
 
@@ -359,39 +371,59 @@ bool corner_normals(const vrad_face *faces, int32_t nfaces, const float *vertice
 // neighbours when the cosine of their normals is at least the threshold
 // (rule 2).  Vertices are identified by position, as a BSP's vertex lump
 // welds them.  Writes offsets[nfaces + 1] and the lists, in discovery order.
-extern "C" int32_t vrad_build_neighbours(const vrad_face *faces, int32_t nfaces, const float *vertices,
-                                         int64_t nvertices, float smoothing_threshold, int32_t *offsets,
-                                         int32_t *list, int64_t capacity, int64_t *count) {
-    if (nfaces < 0 || (nfaces && (!faces || !vertices)) || !offsets || !count) return VRAD_ERR_ARG;
+namespace vrad {
+
+int32_t face_neighbours(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
+                        float smoothing_threshold, std::vector<int32_t> &off, std::vector<int32_t> &list) {
     std::vector<std::vector<int32_t>> face_verts, vertex_face;
-    if (!vrad::weld_faces(faces, nfaces, vertices, nvertices, face_verts, vertex_face)) return VRAD_ERR_ARG;
-    int64_t written = 0;
-    for (int32_t i = 0; i < nfaces; i++) {
-        offsets[i] = (int32_t)written;
+    if (!weld_faces(faces, nfaces, vertices, nvertices, face_verts, vertex_face)) return VRAD_ERR_ARG;
+    std::vector<std::vector<int32_t>> found((size_t)nfaces);
+    std::atomic<bool> too_many{false};
+    parallel_for(nfaces, 16, [&](int64_t ii) {
+        const int32_t i = (int32_t)ii;
         const V3 ni = {faces[i].normal[0], faces[i].normal[1], faces[i].normal[2]};
-        std::vector<int32_t> found;
+        std::vector<int32_t> &fo = found[(size_t)i];
         for (int32_t v : face_verts[(size_t)i]) {
             for (int32_t other : vertex_face[(size_t)v]) {
                 if (other == i) continue;
                 const V3 no = {faces[other].normal[0], faces[other].normal[1], faces[other].normal[2]};
                 const double c = (double)dot(no, ni);
                 if (c < (double)smoothing_threshold) continue;
-                if (std::find(found.begin(), found.end(), other) == found.end()) {
-                    if (found.size() >= 64) return VRAD_ERR_ARG;  // MaxNeighbours
-                    found.push_back(other);
+                if (std::find(fo.begin(), fo.end(), other) == fo.end()) {
+                    if (fo.size() >= 64) {  // MaxNeighbours
+                        too_many = true;
+                        return;
+                    }
+                    fo.push_back(other);
                 }
             }
         }
-        for (int32_t o : found) {
-            if (list) {
-                if (written >= capacity) return VRAD_ERR_ARG;
-                list[written] = o;
-            }
-            written++;
-        }
+    });
+    if (too_many) return VRAD_ERR_ARG;
+    off.assign((size_t)nfaces + 1, 0);
+    for (int32_t i = 0; i < nfaces; i++) off[(size_t)i + 1] = off[(size_t)i] + (int32_t)found[(size_t)i].size();
+    list.resize((size_t)off[(size_t)nfaces]);
+    parallel_for(nfaces, 64, [&](int64_t i) {
+        std::copy(found[(size_t)i].begin(), found[(size_t)i].end(), list.begin() + off[(size_t)i]);
+    });
+    return VRAD_OK;
+}
+
+}  // namespace vrad
+
+extern "C" int32_t vrad_build_neighbours(const vrad_face *faces, int32_t nfaces, const float *vertices,
+                                         int64_t nvertices, float smoothing_threshold, int32_t *offsets,
+                                         int32_t *list, int64_t capacity, int64_t *count) {
+    if (nfaces < 0 || (nfaces && (!faces || !vertices)) || !offsets || !count) return VRAD_ERR_ARG;
+    std::vector<int32_t> off, lst;
+    const int32_t rc = vrad::face_neighbours(faces, nfaces, vertices, nvertices, smoothing_threshold, off, lst);
+    if (rc != VRAD_OK) return rc;
+    std::copy(off.begin(), off.end(), offsets);
+    *count = (int64_t)lst.size();
+    if (list) {
+        if ((int64_t)lst.size() > capacity) return VRAD_ERR_ARG;
+        std::copy(lst.begin(), lst.end(), list);
     }
-    offsets[nfaces] = (int32_t)written;
-    *count = written;
     return VRAD_OK;
 }
 

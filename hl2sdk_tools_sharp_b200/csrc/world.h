@@ -42,6 +42,12 @@ struct RowStrips {
 bool face_row_strips(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices, RowStrips &out,
                      std::string &why);
 
+// FaceNeighbours.Build's smoothing neighbours: face f's are
+// list[off[f] .. off[f + 1]), in the reference's order.  VRAD_ERR_ARG for
+// a winding outside the vertex array or more than 64 neighbours.
+int32_t face_neighbours(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
+                        float smoothing_threshold, std::vector<int32_t> &off, std::vector<int32_t> &list);
+
 // The welded vertex numbers of each face's winding (vertices identified by
 // position) and, per vertex, the faces touching it in face order.  False
 // when a face's winding lies outside the vertex array.
