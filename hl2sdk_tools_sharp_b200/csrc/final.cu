@@ -22,8 +22,11 @@
 
 #include <cuda_runtime.h>
 
+#include <cub/device/device_scan.cuh>
+
 #include <atomic>
 #include <cfloat>
+#include <climits>
 #include <vector>
 
 #include <string>
@@ -339,6 +342,146 @@ cudaError_t launch_final(const FinalView &v, const float4 *sample_light, float4 
     return cudaGetLastError();
 }
 
+namespace {
+
+// x86's truncating float-to-int conversion, which the host set-up's
+// (int) casts compile to: out of range and NaN give INT_MIN.
+__device__ __forceinline__ int trunc_x86(float x) {
+    return (x > -2147483648.0f && x < 2147483648.0f) ? __float2int_rz(x) : INT_MIN;
+}
+
+// LuxelToWorld / WorldToLuxel of the luxel frames (frames[5 f ..]: origin
+// and width, world-to-luxel s and height, world-to-luxel t and min_s,
+// luxel-to-world s and min_t, luxel-to-world t), each operation rounded
+// on its own in the host's order.
+__device__ __forceinline__ void frame_l2w(const float4 *fr, float s, float t, float out[3]) {
+    const float4 o = __ldg(&fr[0]), ls = __ldg(&fr[3]), lt = __ldg(&fr[4]);
+    s = __fadd_rn(s, (float)__float_as_int(__ldg(&fr[2].w)));
+    t = __fadd_rn(t, (float)__float_as_int(ls.w));
+    out[0] = __fadd_rn(__fadd_rn(o.x, __fmul_rn(ls.x, s)), __fmul_rn(lt.x, t));
+    out[1] = __fadd_rn(__fadd_rn(o.y, __fmul_rn(ls.y, s)), __fmul_rn(lt.y, t));
+    out[2] = __fadd_rn(__fadd_rn(o.z, __fmul_rn(ls.z, s)), __fmul_rn(lt.z, t));
+}
+
+__device__ __forceinline__ void frame_w2l(const float4 *fr, const float p[3], float &s, float &t) {
+    const float4 o = __ldg(&fr[0]), ws = __ldg(&fr[1]), wt = __ldg(&fr[2]), ls = __ldg(&fr[3]);
+    const float dx = __fsub_rn(p[0], o.x), dy = __fsub_rn(p[1], o.y), dz = __fsub_rn(p[2], o.z);
+    s = __fsub_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, ws.x), __fmul_rn(dy, ws.y)), __fmul_rn(dz, ws.z)),
+                  (float)__float_as_int(wt.w));
+    t = __fsub_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, wt.x), __fmul_rn(dy, wt.y)), __fmul_rn(dz, wt.z)),
+                  (float)__float_as_int(ls.w));
+}
+
+// One (face, neighbour) pair: the neighbour's samples whose box, moved
+// into the face's luxel space, covers a cell.  COUNT: their number into
+// counts[q]; else their indices and moved boxes at off[q]...
+template <bool COUNT>
+__global__ void k_final_cands(int32_t npairs, const int32_t *__restrict__ pair_face, const int32_t *__restrict__ nlist,
+                              const float4 *__restrict__ frames, const int64_t *__restrict__ srun,
+                              const float4 *__restrict__ sbox, int32_t *__restrict__ counts,
+                              const int64_t *__restrict__ off, int32_t *__restrict__ cand_sample,
+                              float4 *__restrict__ cand_box) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= npairs) return;
+    const int f = __ldg(&pair_face[q]), g = __ldg(&nlist[q]);
+    const float4 *me = frames + 5 * (int64_t)f, *nb = frames + 5 * (int64_t)g;
+    const int width = __float_as_int(__ldg(&me[0].w)), height = __float_as_int(__ldg(&me[1].w));
+    int64_t at = COUNT ? 0 : __ldg(&off[q]);
+    int n = 0;
+    for (int64_t k = __ldg(&srun[2 * g]); k < __ldg(&srun[2 * g + 1]); k++) {
+        const float4 b = __ldg(&sbox[k]);
+        float tmp[3], mins, mint, maxs, maxt;
+        frame_l2w(nb, b.x, b.y, tmp);
+        frame_w2l(me, tmp, mins, mint);
+        frame_l2w(nb, b.z, b.w, tmp);
+        frame_w2l(me, tmp, maxs, maxt);
+        int smin = trunc_x86(mins), tmin = trunc_x86(mint);
+        int smax = trunc_x86(__fadd_rn(maxs, 0.9999f)) + 1, tmax = trunc_x86(__fadd_rn(maxt, 0.9999f)) + 1;
+        smin = smin > 0 ? smin : 0;
+        tmin = tmin > 0 ? tmin : 0;
+        smax = smax < width ? smax : width;
+        tmax = tmax < height ? tmax : height;
+        if (smin >= smax || tmin >= tmax) continue;
+        if (!COUNT) {
+            cand_sample[at] = (int32_t)k;
+            cand_box[at] = make_float4(mins, mint, maxs, maxt);
+            at++;
+        }
+        n++;
+    }
+    if (COUNT) counts[q] = n;
+}
+
+// cand_off[f] = off[noff[f]].
+__global__ void k_final_cand_off(int32_t nfaces, const int32_t *__restrict__ noff, const int64_t *__restrict__ off,
+                                 int32_t *__restrict__ cand_off) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f <= nfaces) cand_off[f] = (int32_t)off[noff[f]];
+}
+
+unsigned blocks_of(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
+
+// The final pass's neighbour candidate tables on the device (fb.frames and
+// fb.sample_box already uploaded on `stream`): fb.cand_off, cand_sample,
+// cand_box.  Synchronises the stream once, for the total's size.
+cudaError_t neighbour_candidates(FinalBuffers &fb, int32_t nfaces, const std::vector<int32_t> &noff,
+                                 const std::vector<int32_t> &nlist, const std::vector<int64_t> &sfirst,
+                                 const std::vector<int64_t> &send, Stager &stager, cudaStream_t stream) {
+    const int32_t npairs = noff[(size_t)nfaces];
+    std::vector<int32_t> pair_face((size_t)(npairs ? npairs : 1), 0);
+    for (int32_t f = 0; f < nfaces; f++)
+        for (int32_t q = noff[(size_t)f]; q < noff[(size_t)f + 1]; q++) pair_face[(size_t)q] = f;
+    std::vector<int64_t> srun(2 * (size_t)(nfaces ? nfaces : 1), 0);
+    for (int32_t f = 0; f < nfaces; f++) {
+        srun[2 * (size_t)f] = sfirst[(size_t)f];
+        srun[2 * (size_t)f + 1] = send[(size_t)f];
+    }
+    int32_t *d_pf = nullptr, *d_nlist = nullptr, *d_noff = nullptr, *d_counts = nullptr;
+    int64_t *d_srun = nullptr, *d_off = nullptr;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0;
+    int64_t total = 0;
+    const size_t P1 = (size_t)(npairs ? npairs : 1);
+    cudaError_t e = stage_table(stager, stream, &d_pf, pair_face);
+    if (e == cudaSuccess) e = stage_table(stager, stream, &d_nlist, nlist);
+    if (e == cudaSuccess) e = stage_table(stager, stream, &d_noff, noff);
+    if (e == cudaSuccess) e = stage_table(stager, stream, &d_srun, srun);
+    if (e == cudaSuccess) e = dev_alloc(&d_counts, sizeof(int32_t) * P1);
+    if (e == cudaSuccess) e = dev_alloc(&d_off, sizeof(int64_t) * (P1 + 1));
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_off, 0, sizeof(int64_t), stream);
+    if (e == cudaSuccess && npairs > 0) {
+        k_final_cands<true><<<blocks_of(npairs, 128), 128, 0, stream>>>(npairs, d_pf, d_nlist, fb.frames, d_srun,
+                                                                       fb.sample_box, d_counts, nullptr, nullptr,
+                                                                       nullptr);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, d_counts, d_off + 1, npairs, stream);
+        if (e == cudaSuccess) e = dev_alloc(&tmp, tmp_bytes ? tmp_bytes : 1);
+        if (e == cudaSuccess) e = cub::DeviceScan::InclusiveSum(tmp, tmp_bytes, d_counts, d_off + 1, npairs, stream);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&total, d_off + npairs, sizeof total, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = stager.finish(stream);
+    if (e == cudaSuccess) e = dev_alloc(&fb.cand_off, sizeof(int32_t) * ((size_t)nfaces + 1));
+    if (e == cudaSuccess) e = dev_alloc(&fb.cand_sample, sizeof(int32_t) * (size_t)(total ? total : 1));
+    if (e == cudaSuccess) e = dev_alloc(&fb.cand_box, sizeof(float4) * (size_t)(total ? total : 1));
+    if (e == cudaSuccess && npairs > 0) {
+        k_final_cands<false><<<blocks_of(npairs, 128), 128, 0, stream>>>(npairs, d_pf, d_nlist, fb.frames, d_srun,
+                                                                        fb.sample_box, nullptr, d_off, fb.cand_sample,
+                                                                        fb.cand_box);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        k_final_cand_off<<<blocks_of((int64_t)nfaces + 1, 256), 256, 0, stream>>>(nfaces, d_noff, d_off, fb.cand_off);
+        e = cudaGetLastError();
+    }
+    // The temporaries go back to the pool once the kernels are done.
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    for (void *q : {(void *)d_pf, (void *)d_nlist, (void *)d_noff, (void *)d_counts, (void *)d_srun, (void *)d_off, tmp})
+        dev_free(q);
+    return e;
+}
+
+}  // namespace
+
 // Host-side set-up of the final pass from the uploaded world.
 cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces, const vrad_sample *samples,
                         int64_t nsamples, const float *vertices, int64_t nvertices, std::vector<int32_t> &noff,
@@ -414,50 +557,6 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
         return cudaErrorInvalidValue;
     }
     clock.mark("frames and cells");
-    // Neighbour candidates: each neighbour's samples whose box, moved into
-    // this face's luxel space as BuildLuxelRadial moves it, can cover a
-    // cell.  Faces on worker threads, lists joined in face order.
-    struct Cand {
-        int32_t sample;
-        float4 box;
-    };
-    std::vector<std::vector<Cand>> lists((size_t)nfaces);
-    parallel_for(nfaces, 4, [&](int64_t fi) {
-        const FaceFrameOut &me = fr[(size_t)fi];
-        std::vector<Cand> &out = lists[(size_t)fi];
-        for (int32_t q = noff[(size_t)fi]; q < noff[(size_t)fi + 1]; q++) {
-            const int32_t g = nlist[(size_t)q];
-            const FaceFrameOut &l = fr[(size_t)g];
-            for (int64_t k = sfirst[(size_t)g]; k < send[(size_t)g]; k++) {
-                const vrad_sample &sm = samples[k];
-                float tmp[3], mins, mint, maxs, maxt;
-                frame_luxel_to_world(l, sm.mins[0], sm.mins[1], tmp);
-                frame_world_to_luxel(me, tmp, mins, mint);
-                frame_luxel_to_world(l, sm.maxs[0], sm.maxs[1], tmp);
-                frame_world_to_luxel(me, tmp, maxs, maxt);
-                int smin = (int)mins, tmin = (int)mint, smax = (int)(maxs + 0.9999f) + 1, tmax = (int)(maxt + 0.9999f) + 1;
-                smin = smin > 0 ? smin : 0;
-                tmin = tmin > 0 ? tmin : 0;
-                smax = smax < me.width ? smax : me.width;
-                tmax = tmax < me.height ? tmax : me.height;
-                if (smin >= smax || tmin >= tmax) continue;
-                out.push_back(Cand{(int32_t)k, make_float4(mins, mint, maxs, maxt)});
-            }
-        }
-    });
-    std::vector<int32_t> cand_off((size_t)nfaces + 1, 0);
-    for (int32_t f = 0; f < nfaces; f++) cand_off[(size_t)f + 1] = cand_off[(size_t)f] + (int32_t)lists[(size_t)f].size();
-    uvector<int32_t> cand_sample((size_t)cand_off[(size_t)nfaces]);
-    uvector<float4> cand_box((size_t)cand_off[(size_t)nfaces]);
-    parallel_for(nfaces, 16, [&](int64_t f) {
-        size_t k = (size_t)cand_off[(size_t)f];
-        for (const Cand &c : lists[(size_t)f]) {
-            cand_sample[k] = c.sample;
-            cand_box[k] = c.box;
-            k++;
-        }
-    });
-    clock.mark("candidates");
     auto up = [&](auto **dst, const auto &v) { return stage_table(stager, stream, dst, v); };
     cudaError_t e = up(&fb.frames, frames);
     if (e == cudaSuccess) e = up(&fb.face_cells, face_cells);
@@ -465,9 +564,12 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
     if (e == cudaSuccess) e = up(&fb.cell_face, cell_face);
     if (e == cudaSuccess) e = up(&fb.cell_sample, cell_sample);
     if (e == cudaSuccess) e = up(&fb.sample_box, sbox);
-    if (e == cudaSuccess) e = up(&fb.cand_off, cand_off);
-    if (e == cudaSuccess) e = up(&fb.cand_sample, cand_sample);
-    if (e == cudaSuccess) e = up(&fb.cand_box, cand_box);
+    // Neighbour candidates on the device: each neighbour's samples whose
+    // box, moved into this face's luxel space as BuildLuxelRadial moves
+    // it, can cover a cell; one thread per (face, neighbour) pair, counted,
+    // scanned, then written in face, neighbour and sample order.
+    if (e == cudaSuccess) e = neighbour_candidates(fb, nfaces, noff, nlist, sfirst, send, stager, stream);
+    clock.mark("candidates");
     if (e == cudaSuccess) e = vrad::dev_alloc(&fb.rad_light, sizeof(float4) * (size_t)(ncells ? ncells : 1));
     if (e == cudaSuccess) e = vrad::dev_alloc(&fb.rad_weight, sizeof(float) * (size_t)(ncells ? ncells : 1));
     if (e == cudaSuccess) e = vrad::dev_alloc(&fb.flat, sizeof(float4) * (size_t)(ncells ? ncells : 1));
