@@ -222,7 +222,9 @@ int32_t vrad_destroy(vrad_ctx *ctx) {
         ctx->world.release();
         ctx->final_pass.release();
         ctx->bounce.release();
+        ctx->bounce.free_pinned();
         ctx->supersample.release();
+        ctx->supersample.free_pinned();
         vrad::dev_free(ctx->sample_light);
         cudaFree(ctx->status);
         cudaFree(ctx->d_rays);

@@ -685,9 +685,20 @@ void BounceBuffers::release() {
                     first, guess, feat, pred,
                     pr_off, pr_patch, pr_box, pr_coord, prad_light, prad_weight};
     for (void *q : ptrs) dev_free(q);
+    // The pinned stop-rule sums stay for the next upload (freeing pinned
+    // memory can stall); free_pinned() frees them.
+    double *sums_h = h_sums;
+    float *exact_h = h_exact;
+    *this = BounceBuffers();
+    h_sums = sums_h;
+    h_exact = exact_h;
+}
+
+void BounceBuffers::free_pinned() {
     cudaFreeHost(h_sums);
     cudaFreeHost(h_exact);
-    *this = BounceBuffers();
+    h_sums = nullptr;
+    h_exact = nullptr;
 }
 
 cudaError_t launch_patch_light(const BounceBuffers &b, const float4 *sample_light, cudaStream_t stream) {

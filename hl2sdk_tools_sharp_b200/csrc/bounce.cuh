@@ -135,7 +135,8 @@ struct BounceBuffers {
     float patch_light_ms = 0, transfer_ms = 0, bounce_ms = 0, final_ms = 0;
     unsigned long long rays = 0, blocked = 0, open_ties = 0;
 
-    void release();
+    void release();      // the device tables; the pinned sums stay
+    void free_pinned();  // the pinned sums
 };
 
 // Device phases of one bounce pass, all on `stream`.

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cstdint>
 #include <cmath>
 #include <cstring>
@@ -35,81 +36,157 @@ inline float bits_f(int32_t x) {
     return y;
 }
 
+// x86's truncating double-to-int conversion, which the host set-up's
+// (int) casts compile to: out of range and NaN give INT_MIN.
+__device__ __forceinline__ int dtrunc_x86(double x) {
+    return (x > -2147483649.0 && x < 2147483648.0) ? __double2int_rz(x) : INT_MIN;
+}
+
+// WorldToLuxel of the final pass's frame fr (5 float4: origin and width,
+// world-to-luxel s and height, world-to-luxel t and min_s, luxel-to-world
+// s and min_t, luxel-to-world t), each operation rounded on its own.
+__device__ __forceinline__ void radial_w2l(const float4 *fr, float px, float py, float pz, float &s, float &t) {
+    const float4 o = __ldg(&fr[0]), ws = __ldg(&fr[1]), wt = __ldg(&fr[2]), ls = __ldg(&fr[3]);
+    const float dx = __fsub_rn(px, o.x), dy = __fsub_rn(py, o.y), dz = __fsub_rn(pz, o.z);
+    s = __fsub_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, ws.x), __fmul_rn(dy, ws.y)), __fmul_rn(dz, ws.z)),
+                  (float)__float_as_int(wt.w));
+    t = __fsub_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, wt.x), __fmul_rn(dy, wt.y)), __fmul_rn(dz, wt.z)),
+                  (float)__float_as_int(ls.w));
+}
+
 // The per-face candidate list of the bounced light's radial grid
 // (BuildPatchRadial): the face's own leaf patches, then each smoothing
 // neighbour's, each list in FacePatches order (descendants by descending
 // index, then the root); each kept with its box in this face's cells when
-// that box holds at least one cell.  Faces are independent: each builds its
-// list on a worker thread, the lists are concatenated in face order.
-void patch_radial_tables(const std::vector<vrad_face> &faces, const PatchTree &tree, const std::vector<int32_t> &noff,
-                         const std::vector<int32_t> &nlist, std::vector<int32_t> &off, uvector<int32_t> &patch,
-                         uvector<int4> &box, uvector<float4> &coord) {
-    const int32_t nf = (int32_t)faces.size();
-    struct Entry {
-        int32_t patch;
-        int4 box;
-        float4 coord;
-    };
-    std::vector<std::vector<Entry>> lists((size_t)nf);
-    parallel_for(nf, 8, [&](int64_t fi) {
-        const int32_t f = (int32_t)fi;
-        FaceFrameOut me;
-        face_frame_of(faces[(size_t)f], me);
-        std::vector<Entry> &out = lists[(size_t)f];
-        auto visit = [&](int32_t p) {
-            const vrad_patch &pt = tree.patches[(size_t)p];
-            if (pt.child1 != -1) return;
+// that box holds at least one cell.  One thread per (face, source face)
+// pair, pairs in that order: COUNT counts into counts[q]; otherwise the
+// entries are written at off[q]...
+template <bool COUNT>
+__global__ void k_radial_pairs(int32_t npairs, const int32_t *__restrict__ pair_face,
+                               const int32_t *__restrict__ pair_src, BounceView v, const float4 *__restrict__ frames,
+                               int32_t *__restrict__ counts, const int64_t *__restrict__ off,
+                               int32_t *__restrict__ out_patch, int4 *__restrict__ out_box,
+                               float4 *__restrict__ out_coord) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= npairs) return;
+    const int f = __ldg(&pair_face[q]), g = __ldg(&pair_src[q]);
+    const float4 *me = frames + 5 * (int64_t)f;
+    const int width = __float_as_int(__ldg(&me[0].w)), height = __float_as_int(__ldg(&me[1].w));
+    const int4 fr = __ldg(&v.face_range[g]);  // root, first descendant, end
+    int64_t at = COUNT ? 0 : __ldg(&off[q]);
+    int n = 0;
+    if (fr.x >= 0) {
+        for (int k = 0; k <= fr.z - fr.y; k++) {
+            const int p = k < fr.z - fr.y ? fr.z - 1 - k : fr.x;
+            if (__ldg(&v.tree[p].y) != -1) continue;
             // PatchLightmapCoordRange.
+            const int2 w = __ldg(&v.wind[p]);
             float min_s = 1e30f, min_t = 1e30f, max_s = -1e30f, max_t = -1e30f;
-            for (int32_t k = 0; k < pt.num_points; k++) {
+            for (int i = 0; i < w.y; i++) {
+                const float4 pt = __ldg(&v.points[w.x + i]);
                 float s, t;
-                frame_world_to_luxel(me, &tree.points[3 * (size_t)(pt.first_point + k)], s, t);
+                radial_w2l(me, pt.x, pt.y, pt.z, s, t);
                 min_s = min_s < s ? min_s : s;
                 max_s = max_s > s ? max_s : s;
                 min_t = min_t < t ? min_t : t;
                 max_t = max_t > t ? max_t : t;
             }
             // LuxelRadial.AddBounced's extent and box.
+            const float4 o = __ldg(&v.origin[p]);
             float cs, ct;
-            frame_world_to_luxel(me, pt.origin, cs, ct);
-            float ds = max_s - min_s, dt = max_t - min_t;
-            ds = (float)(1.0 > (double)ds ? 1.0 : (double)ds);
-            dt = (float)(1.0 > (double)dt ? 1.0 : (double)dt);
-            int smin = (int)((double)cs - (double)ds * 1.42);
-            int tmin = (int)((double)ct - (double)dt * 1.42);
-            int smax = (int)((double)cs + (double)ds * 1.42 + 1.0);
-            int tmax = (int)((double)ct + (double)dt * 1.42 + 1.0);
-            smin = std::max(smin, 0);
-            tmin = std::max(tmin, 0);
-            smax = std::min(smax, me.width);
-            tmax = std::min(tmax, me.height);
-            if (smin >= smax || tmin >= tmax) return;
-            out.push_back(Entry{p, make_int4(smin, tmin, smax, tmax), make_float4(cs, ct, ds, dt)});
-        };
-        auto face_leaves = [&](int32_t g) {
-            const int32_t r = tree.face_root[(size_t)g];
-            if (r < 0) return;
-            for (int32_t p = tree.face_end[(size_t)g] - 1; p >= tree.face_first[(size_t)g]; p--) visit(p);
-            visit(r);
-        };
-        face_leaves(f);
-        for (int32_t q = noff[(size_t)f]; q < noff[(size_t)f + 1]; q++) face_leaves(nlist[(size_t)q]);
-    });
-    off.assign((size_t)nf + 1, 0);
-    for (int32_t f = 0; f < nf; f++) off[(size_t)f + 1] = off[(size_t)f] + (int32_t)lists[(size_t)f].size();
-    const size_t total = (size_t)off[(size_t)nf];
-    patch.resize(total);
-    box.resize(total);
-    coord.resize(total);
-    parallel_for(nf, 8, [&](int64_t f) {
-        size_t k = (size_t)off[(size_t)f];
-        for (const Entry &e : lists[(size_t)f]) {
-            patch[k] = e.patch;
-            box[k] = e.box;
-            coord[k] = e.coord;
-            k++;
+            radial_w2l(me, o.x, o.y, o.z, cs, ct);
+            float ds = __fsub_rn(max_s, min_s), dt = __fsub_rn(max_t, min_t);
+            ds = 1.0 > (double)ds ? 1.0f : ds;
+            dt = 1.0 > (double)dt ? 1.0f : dt;
+            const double es = __dmul_rn((double)ds, 1.42), et = __dmul_rn((double)dt, 1.42);
+            int smin = dtrunc_x86(__dsub_rn((double)cs, es));
+            int tmin = dtrunc_x86(__dsub_rn((double)ct, et));
+            int smax = dtrunc_x86(__dadd_rn(__dadd_rn((double)cs, es), 1.0));
+            int tmax = dtrunc_x86(__dadd_rn(__dadd_rn((double)ct, et), 1.0));
+            smin = smin > 0 ? smin : 0;
+            tmin = tmin > 0 ? tmin : 0;
+            smax = smax < width ? smax : width;
+            tmax = tmax < height ? tmax : height;
+            if (smin >= smax || tmin >= tmax) continue;
+            if (!COUNT) {
+                out_patch[at] = p;
+                out_box[at] = make_int4(smin, tmin, smax, tmax);
+                out_coord[at] = make_float4(cs, ct, ds, dt);
+                at++;
+            }
+            n++;
         }
-    });
+    }
+    if (COUNT) counts[q] = n;
+}
+
+// pr_off[f] = off[first pair of face f].
+__global__ void k_radial_off(int32_t nfaces, const int32_t *__restrict__ face_pair0, const int64_t *__restrict__ off,
+                             int32_t *__restrict__ pr_off) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f <= nfaces) pr_off[f] = (int32_t)off[face_pair0[f]];
+}
+
+unsigned grid_for(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
+
+// The radial tables on the device, from the uploaded patches (b.view) and
+// the final pass's frames, into b.pr_off, pr_patch, pr_box, pr_coord.
+// Synchronises the stream once, for the total's size.
+cudaError_t radial_tables(BounceBuffers &b, const float4 *frames, int32_t nf, const std::vector<int32_t> &noff,
+                          const std::vector<int32_t> &nlist, Stager &stager, cudaStream_t stream) {
+    const int32_t npairs = nf + noff[(size_t)nf];
+    std::vector<int32_t> pair_face((size_t)(npairs ? npairs : 1)), pair_src((size_t)(npairs ? npairs : 1)),
+        face_pair0((size_t)nf + 1);
+    int32_t q = 0;
+    for (int32_t f = 0; f < nf; f++) {
+        face_pair0[(size_t)f] = q;
+        pair_face[(size_t)q] = f;
+        pair_src[(size_t)q++] = f;
+        for (int32_t k = noff[(size_t)f]; k < noff[(size_t)f + 1]; k++) {
+            pair_face[(size_t)q] = f;
+            pair_src[(size_t)q++] = nlist[(size_t)k];
+        }
+    }
+    face_pair0[(size_t)nf] = q;
+    int32_t *d_pf = nullptr, *d_ps = nullptr, *d_p0 = nullptr, *d_counts = nullptr;
+    int64_t *d_off = nullptr;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0;
+    int64_t total = 0;
+    const size_t Q1 = (size_t)(npairs ? npairs : 1);
+    cudaError_t e = stage_table(stager, stream, &d_pf, pair_face);
+    if (e == cudaSuccess) e = stage_table(stager, stream, &d_ps, pair_src);
+    if (e == cudaSuccess) e = stage_table(stager, stream, &d_p0, face_pair0);
+    if (e == cudaSuccess) e = dev_alloc(&d_counts, sizeof(int32_t) * Q1);
+    if (e == cudaSuccess) e = dev_alloc(&d_off, sizeof(int64_t) * (Q1 + 1));
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_off, 0, sizeof(int64_t), stream);
+    if (e == cudaSuccess && npairs > 0) {
+        k_radial_pairs<true><<<grid_for(npairs, 128), 128, 0, stream>>>(npairs, d_pf, d_ps, b.view, frames, d_counts,
+                                                                       nullptr, nullptr, nullptr, nullptr);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, d_counts, d_off + 1, npairs, stream);
+        if (e == cudaSuccess) e = dev_alloc(&tmp, tmp_bytes ? tmp_bytes : 1);
+        if (e == cudaSuccess) e = cub::DeviceScan::InclusiveSum(tmp, tmp_bytes, d_counts, d_off + 1, npairs, stream);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&total, d_off + npairs, sizeof total, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    const size_t T1 = (size_t)(total ? total : 1);
+    if (e == cudaSuccess) e = dev_alloc(&b.pr_off, sizeof(int32_t) * ((size_t)nf + 1));
+    if (e == cudaSuccess) e = dev_alloc(&b.pr_patch, sizeof(int32_t) * T1);
+    if (e == cudaSuccess) e = dev_alloc(&b.pr_box, sizeof(int4) * T1);
+    if (e == cudaSuccess) e = dev_alloc(&b.pr_coord, sizeof(float4) * T1);
+    if (e == cudaSuccess && npairs > 0) {
+        k_radial_pairs<false><<<grid_for(npairs, 128), 128, 0, stream>>>(npairs, d_pf, d_ps, b.view, frames, nullptr,
+                                                                        d_off, b.pr_patch, b.pr_box, b.pr_coord);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        k_radial_off<<<grid_for((int64_t)nf + 1, 256), 256, 0, stream>>>(nf, d_p0, d_off, b.pr_off);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    for (void *x : {(void *)d_pf, (void *)d_ps, (void *)d_p0, (void *)d_counts, (void *)d_off, tmp}) dev_free(x);
+    return e;
 }
 
 }  // namespace
@@ -402,13 +479,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     if (ctx->h_noff.size() != (size_t)nf + 1) return vrad_fail(ctx, VRAD_ERR_ARG, "the world has no smoothing neighbours");
     const std::vector<int32_t> &noff = ctx->h_noff, &nlist = ctx->h_nlist;
     clock.mark("neighbours");
-    std::vector<int32_t> pr_off;
-    uvector<int32_t> pr_patch;
-    uvector<int4> pr_box;
-    uvector<float4> pr_coord;
-    patch_radial_tables(ctx->h_faces, tree, noff, nlist, pr_off, pr_patch, pr_box, pr_coord);
 
-    clock.mark("patch radial tables");
     const int32_t R = (int32_t)recv.size();
     const int64_t ncells = ctx->final_pass.view.ncells;
     if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.origin, origin);
@@ -429,10 +500,6 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.row_off, row_off);
     if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.row_faces, row_faces);
     if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.sample_area, sample_area);
-    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.pr_off, pr_off);
-    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.pr_patch, pr_patch);
-    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.pr_box, pr_box);
-    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.pr_coord, pr_coord);
     clock.mark("tables copied");
     const size_t P1 = (size_t)(P ? P : 1), R1 = (size_t)R + 1, N1 = (size_t)(ncells ? ncells : 1);
     if (e == cudaSuccess) e = dev_alloc(&b.cand_off, sizeof(int64_t) * R1);
@@ -442,8 +509,8 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     if (e == cudaSuccess) e = dev_alloc(&b.sums, kSums * sizeof(double));
     if (e == cudaSuccess) e = dev_alloc(&b.exact, 3 * sizeof(float));
     if (e == cudaSuccess) e = dev_alloc(&b.counters, 3 * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMallocHost(&b.h_sums, kSums * sizeof(double));
-    if (e == cudaSuccess) e = cudaMallocHost(&b.h_exact, 3 * sizeof(float));
+    if (e == cudaSuccess && !b.h_sums) e = cudaMallocHost(&b.h_sums, kSums * sizeof(double));
+    if (e == cudaSuccess && !b.h_exact) e = cudaMallocHost(&b.h_exact, 3 * sizeof(float));
     if (e == cudaSuccess) e = dev_alloc(&b.first, sizeof(float4) * P1);
     if (e == cudaSuccess) e = dev_alloc(&b.guess, sizeof(float4) * P1);
     if (e == cudaSuccess) e = dev_alloc(&b.feat, sizeof(uint16_t) * kFeatures * (size_t)(R ? R : 1));
@@ -487,8 +554,17 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     b.view = BounceView{P, nf, R, b.origin, b.normal, b.mins, b.maxs, b.tree, b.refl, b.wind, b.points,
                         b.face_range, b.face_samples, b.face_plane, b.recv, b.row_off, b.row_faces, b.sample_area,
                         ctx->world.sample_pos};
-    // Size the candidate and transfer arrays by one build.
     cudaStream_t s = ctx->stream;
+    // The final pass's patch tables over the smoothing neighbours, on the
+    // device from the uploaded patches.
+    e = radial_tables(b, ctx->final_pass.frames, nf, noff, nlist, ctx->stager, s);
+    if (e != cudaSuccess) {
+        ctx->stager.finish(s);
+        b.release();
+        return vrad_cuda_fail(ctx, e, "patch radial tables");
+    }
+    clock.mark("patch radial tables");
+    // Size the candidate and transfer arrays by one build.
     e = launch_transfers(b, ctx->scene.view(), ctx->status, s, true);
     int64_t ncand = 0;
     if (e == cudaSuccess && R > 0) e = cudaMemcpyAsync(&ncand, b.cand_off + R, sizeof ncand, cudaMemcpyDeviceToHost, s);

@@ -312,10 +312,21 @@ unsigned grid_of(int64_t n, int per) { return (unsigned)((n + per - 1) / per); }
 void SupersampleBuffers::release() {
     void *ptrs[] = {origin_st, cell, wind, points, intensity, processed, selected, counts, base, rows, row_out, row_bits};
     for (void *p : ptrs) dev_free(p);
-    cudaFreeHost(h_counts);
+    // The pinned counts stay for the next upload (freeing pinned memory
+    // can stall for a good part of a second); free_pinned() frees them.
     const int32_t keep = extra_passes;
+    int32_t *pinned = h_counts;
+    const size_t cap = h_counts_cap;
     *this = SupersampleBuffers();
     extra_passes = keep;
+    h_counts = pinned;
+    h_counts_cap = cap;
+}
+
+void SupersampleBuffers::free_pinned() {
+    cudaFreeHost(h_counts);
+    h_counts = nullptr;
+    h_counts_cap = 0;
 }
 
 cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_face> &faces,
@@ -350,7 +361,11 @@ cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_fac
     if (e == cudaSuccess) e = dev_alloc(&ss.rows, sizeof(int32_t) * groups);
     if (e == cudaSuccess) e = dev_alloc(&ss.row_out, sizeof(float4) * 20 * S1);
     if (e == cudaSuccess) e = dev_alloc(&ss.row_bits, sizeof(int32_t) * 5 * S1);
-    if (e == cudaSuccess) e = cudaMallocHost(&ss.h_counts, sizeof(int32_t) * (1 + (size_t)nclusters));
+    if (e == cudaSuccess && ss.h_counts_cap < 1 + (size_t)nclusters) {
+        ss.free_pinned();
+        e = cudaMallocHost(&ss.h_counts, sizeof(int32_t) * (1 + (size_t)nclusters));
+        if (e == cudaSuccess) ss.h_counts_cap = 1 + (size_t)nclusters;
+    }
     if (e != cudaSuccess) {
         ss.release();
         why = "supersampling buffers";

@@ -46,7 +46,8 @@ struct SupersampleBuffers {
     int32_t *rows = nullptr;        // group capacity: 5 * S + 16 * C
     float4 *row_out = nullptr;
     int32_t *row_bits = nullptr;
-    int32_t *h_counts = nullptr;    // pinned
+    int32_t *h_counts = nullptr;    // pinned, kept across uploads (h_counts_cap entries)
+    size_t h_counts_cap = 0;
     int64_t nsamples = 0;
     int32_t nclusters = 0;
     int32_t extra_passes = 4;       // DirectLightingSettings.ExtraPasses; 0 = -noextra
@@ -56,7 +57,8 @@ struct SupersampleBuffers {
     int32_t passes_run = 0;
     float ms = 0.0f;
 
-    void release();
+    void release();      // the device tables; the pinned counts stay
+    void free_pinned();  // the pinned counts
 };
 
 // Builds the tables from the uploaded world (host copies of its faces,
