@@ -322,46 +322,59 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     BounceBuffers &b = ctx->bounce;
     b.release();
     clock.mark("release");
+    // The patch tree, its patches written straight into the device's SoA
+    // rows (and each leaf's cluster, for the receiver order) as the merge
+    // numbers them.
+    struct SoaRows : PatchSink {
+        int32_t C = 0;
+        uvector<float4> origin, normal, mins, maxs, refl, points;
+        uvector<int4> tr;
+        uvector<int2> wind;
+        uvector<int32_t> leaf_cluster;
+        std::atomic<int32_t> bad{INT32_MAX};
+        bool prepare(int32_t n, int64_t npoints) override {
+            for (uvector<float4> *v : {&origin, &normal, &mins, &maxs, &refl}) v->resize((size_t)n);
+            tr.resize((size_t)n);
+            wind.resize((size_t)n);
+            leaf_cluster.resize((size_t)n);
+            points.resize((size_t)npoints);
+            return true;
+        }
+        void put(int32_t i, const vrad_patch &p, const float *xyz) override {
+            if (p.cluster < 0 || p.cluster >= C) {
+                int32_t cur = bad.load();
+                while (i < cur && !bad.compare_exchange_weak(cur, i)) {
+                }
+            }
+            origin[(size_t)i] = make_float4(p.origin[0], p.origin[1], p.origin[2], p.area);
+            normal[(size_t)i] = make_float4(p.normal[0], p.normal[1], p.normal[2], p.plane_dist);
+            mins[(size_t)i] = make_float4(p.mins[0], p.mins[1], p.mins[2], bits_f(p.face));
+            maxs[(size_t)i] = make_float4(p.maxs[0], p.maxs[1], p.maxs[2], bits_f(p.cluster));
+            refl[(size_t)i] = make_float4(p.reflectivity[0], p.reflectivity[1], p.reflectivity[2], 0.0f);
+            tr[(size_t)i] = make_int4(p.parent, p.child1, p.child2, p.sky);
+            wind[(size_t)i] = make_int2(p.first_point, p.num_points);
+            leaf_cluster[(size_t)i] = p.child1 == -1 ? p.cluster : -1;
+            for (int32_t k = 0; k < p.num_points; k++)
+                points[(size_t)p.first_point + (size_t)k] = make_float4(xyz[3 * k], xyz[3 * k + 1], xyz[3 * k + 2], 0.0f);
+        }
+    };
     PatchTree tree;
+    SoaRows rows;
+    rows.C = C;
     std::string why;
     const int64_t nvert = (int64_t)ctx->h_vertices.size() / 3;
     if (!build_patch_tree(ctx->h_faces.data(), nf, ctx->h_vertices.data(), nvert, d->reflectivity, d->max_chop,
-                          d->min_chop, tree, why))
+                          d->min_chop, tree, rows, why))
         return vrad_fail(ctx, VRAD_ERR_ARG, "patches: %s", why.c_str());
-    const int32_t P = (int32_t)tree.patches.size();
+    const int32_t P = tree.npatches;
     clock.mark("patch tree");
-
-    // Per patch, in parallel: the device's SoA rows, and each leaf's
-    // cluster for the receiver order.
-    uvector<float4> origin((size_t)P), normal((size_t)P), mins((size_t)P), maxs((size_t)P), refl((size_t)P);
-    uvector<int4> tr((size_t)P);
-    uvector<int2> wind((size_t)P);
-    uvector<int32_t> leaf_cluster((size_t)P);
-    std::atomic<int32_t> bad{INT32_MAX};
-    parallel_for(P, 4096, [&](int64_t ii) {
-        const size_t i = (size_t)ii;
-        const vrad_patch &p = tree.patches[i];
-        if (p.cluster < 0 || p.cluster >= C) {
-            int32_t cur = bad.load();
-            while ((int32_t)ii < cur && !bad.compare_exchange_weak(cur, (int32_t)ii)) {
-            }
-        }
-        origin[i] = make_float4(p.origin[0], p.origin[1], p.origin[2], p.area);
-        normal[i] = make_float4(p.normal[0], p.normal[1], p.normal[2], p.plane_dist);
-        mins[i] = make_float4(p.mins[0], p.mins[1], p.mins[2], bits_f(p.face));
-        maxs[i] = make_float4(p.maxs[0], p.maxs[1], p.maxs[2], bits_f(p.cluster));
-        refl[i] = make_float4(p.reflectivity[0], p.reflectivity[1], p.reflectivity[2], 0.0f);
-        tr[i] = make_int4(p.parent, p.child1, p.child2, p.sky);
-        wind[i] = make_int2(p.first_point, p.num_points);
-        leaf_cluster[i] = p.child1 == -1 ? p.cluster : -1;
-    });
-    if (bad.load() != INT32_MAX)
-        return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "patch %d lies outside every cluster", bad.load());
-    uvector<float4> points(tree.points.size() / 3);
-    parallel_for((int64_t)points.size(), 1 << 16, [&](int64_t k) {
-        const float *q = &tree.points[3 * (size_t)k];
-        points[(size_t)k] = make_float4(q[0], q[1], q[2], 0.0f);
-    });
+    if (rows.bad.load() != INT32_MAX)
+        return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "patch %d lies outside every cluster", rows.bad.load());
+    const uvector<float4> &origin = rows.origin, &normal = rows.normal, &mins = rows.mins, &maxs = rows.maxs,
+                          &refl = rows.refl, &points = rows.points;
+    const uvector<int4> &tr = rows.tr;
+    const uvector<int2> &wind = rows.wind;
+    const uvector<int32_t> &leaf_cluster = rows.leaf_cluster;
     // Per face.
     std::vector<int4> face_range((size_t)nf);
     std::vector<int2> face_samples((size_t)nf, make_int2(0, 0));

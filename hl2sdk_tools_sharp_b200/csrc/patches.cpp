@@ -186,7 +186,8 @@ bool prevent_subdivision(int32_t flags) {
 }  // namespace
 
 bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
-                      const float *reflectivity, float max_chop, float min_chop, PatchTree &out, std::string &why) {
+                      const float *reflectivity, float max_chop, float min_chop, PatchTree &out, PatchSink &sink,
+                      std::string &why) {
     SetupClock clock("patch_tree");
     std::vector<std::vector<float>> corners;
     if (!corner_normals(faces, nfaces, vertices, nvertices, kSmoothing, corners)) {
@@ -272,32 +273,40 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
     });
     clock.mark("subdivide");
     // Global indices: the roots 0..roots-1 in face order, then each root's
-    // descendants in creation order (the order SubdividePatch adds them).
+    // descendants in creation order (the order SubdividePatch adds them);
+    // the windings' points in the same order.
     std::vector<int32_t> base((size_t)roots);
+    std::vector<int64_t> root_pt((size_t)roots + 1, 0), desc_pt((size_t)roots + 1, 0);
     int32_t total = roots;
     for (int32_t i = 0; i < roots; i++) {
+        const Builder &b = subtree[(size_t)i];
         base[(size_t)i] = total;
-        total += (int32_t)subtree[(size_t)i].patches.size() - 1;
+        total += (int32_t)b.patches.size() - 1;
+        root_pt[(size_t)i + 1] = root_pt[(size_t)i] + b.wcount[0];
+        desc_pt[(size_t)i + 1] = desc_pt[(size_t)i] + (int64_t)b.pts.size() - b.wcount[0];
     }
-    out.patches.resize((size_t)total);
-    uvector<const V3 *> wind((size_t)total);  // each patch's points in its builder's array
-    uvector<int64_t> first((size_t)total + 1);
+    const int64_t npoints = root_pt[(size_t)roots] + desc_pt[(size_t)roots];
+    if (!sink.prepare(total, npoints)) {
+        why = "patch tables";
+        return false;
+    }
     out.face_first.assign((size_t)nfaces, 0);
     out.face_end.assign((size_t)nfaces, 0);
-    // Each root's block of patches, renumbered, in parallel.
+    // Each root's block of patches, renumbered, handed to the sink in
+    // parallel.
     parallel_for(roots, 8, [&](int64_t ii) {
         const int32_t i = (int32_t)ii;
         Builder &b = subtree[(size_t)i];
         auto global = [&](int32_t local) { return local < 0 ? -1 : (local == 0 ? i : base[(size_t)i] + local - 1); };
+        const int64_t desc0 = root_pt[(size_t)roots] + desc_pt[(size_t)i] - b.wcount[0];
         for (size_t k = 0; k < b.patches.size(); k++) {
             vrad_patch p = b.patches[k];
             p.parent = global(p.parent);
             p.child1 = global(p.child1);
             p.child2 = global(p.child2);
-            const int32_t g = global((int32_t)k);
-            out.patches[(size_t)g] = p;
-            wind[(size_t)g] = b.pts.data() + b.wfirst[k];
-            first[(size_t)g + 1] = (int64_t)b.wcount[k];
+            p.first_point = (int32_t)(k == 0 ? root_pt[(size_t)i] : desc0 + b.wfirst[k]);
+            p.num_points = b.wcount[k];
+            sink.put(global((int32_t)k), p, &b.pts[(size_t)b.wfirst[k]].x);
         }
     });
     for (int32_t i = 0; i < roots; i++) {
@@ -307,25 +316,9 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
         out.face_end[(size_t)f] = base[(size_t)i] + (int32_t)b.patches.size() - 1;
         out.face_root[(size_t)f] = i;
     }
+    out.npatches = total;
+    out.npoints = npoints;
     clock.mark("merge");
-    // Windings into one point array: offsets by a prefix sum, points copied
-    // in parallel.
-    first[0] = 0;
-    for (int32_t i = 0; i < total; i++) first[(size_t)i + 1] += first[(size_t)i];
-    out.points.resize((size_t)first[(size_t)total] * 3);
-    parallel_for(total, 4096, [&](int64_t i) {
-        vrad_patch &p = out.patches[(size_t)i];
-        p.first_point = (int32_t)first[(size_t)i];
-        p.num_points = (int32_t)(first[(size_t)i + 1] - first[(size_t)i]);
-        float *dst = &out.points[(size_t)first[(size_t)i] * 3];
-        const V3 *src = wind[(size_t)i];
-        for (int32_t k = 0; k < p.num_points; k++) {
-            *dst++ = src[k].x;
-            *dst++ = src[k].y;
-            *dst++ = src[k].z;
-        }
-    });
-    clock.mark("points");
     out.roots = roots;
     return true;
 }
@@ -340,14 +333,15 @@ extern "C" int32_t vrad_build_patches(const vrad_face *faces, int32_t nfaces, co
         return VRAD_ERR_ARG;
     if (!(max_chop > 0.0f) || !(min_chop > 0.0f)) return VRAD_ERR_ARG;
     vrad::PatchTree tree;
+    vrad::PatchArrays arrays;
     std::string why;
-    if (!vrad::build_patch_tree(faces, nfaces, vertices, nvertices, reflectivity, max_chop, min_chop, tree, why))
+    if (!vrad::build_patch_tree(faces, nfaces, vertices, nvertices, reflectivity, max_chop, min_chop, tree, arrays, why))
         return VRAD_ERR_ARG;
-    *count = (int64_t)tree.patches.size();
-    *point_count = (int64_t)tree.points.size() / 3;
+    *count = (int64_t)arrays.patches.size();
+    *point_count = (int64_t)arrays.points.size() / 3;
     if (!out && !points) return VRAD_OK;  // a counting pass
     if ((out && capacity < *count) || (points && point_capacity < *point_count)) return VRAD_ERR_ARG;
-    if (out) std::memcpy(out, tree.patches.data(), sizeof(vrad_patch) * tree.patches.size());
-    if (points) std::memcpy(points, tree.points.data(), sizeof(float) * tree.points.size());
+    if (out) std::memcpy(out, arrays.patches.data(), sizeof(vrad_patch) * arrays.patches.size());
+    if (points) std::memcpy(points, arrays.points.data(), sizeof(float) * arrays.points.size());
     return VRAD_OK;
 }
