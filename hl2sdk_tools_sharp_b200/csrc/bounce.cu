@@ -685,6 +685,8 @@ void BounceBuffers::release() {
                     first, guess, feat, pred,
                     pr_off, pr_patch, pr_box, pr_coord, prad_light, prad_weight};
     for (void *q : ptrs) dev_free(q);
+    for (cudaGraphExec_t &g : bounce_graph)
+        if (g) cudaGraphExecDestroy(g);
     // The pinned stop-rule sums stay for the next upload (freeing pinned
     // memory can stall); free_pinned() frees them.
     double *sums_h = h_sums;
@@ -816,6 +818,28 @@ cudaError_t launch_warm_start(BounceBuffers &b, const DeviceWorld &w, const vrad
                                                                             b.sums);
     b.last_buffer = 0;
     return cudaGetLastError();
+}
+
+cudaError_t launch_bounce_graph(BounceBuffers &b, int bounce, cudaStream_t capture, cudaStream_t stream) {
+    const int k = bounce & 1;
+    if (!b.bounce_graph[k]) {
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(capture, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        cudaError_t inside = launch_gather(b, bounce, capture);
+        if (inside == cudaSuccess)
+            inside = cudaMemcpyAsync(b.h_sums, b.sums, kSums * sizeof(double), cudaMemcpyDeviceToHost, capture);
+        e = cudaStreamEndCapture(capture, &g);
+        if (e == cudaSuccess) e = inside;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&b.bounce_graph[k], g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            b.bounce_graph[k] = nullptr;
+            return e;
+        }
+    }
+    b.last_buffer = k ^ 1;
+    return cudaGraphLaunch(b.bounce_graph[k], stream);
 }
 
 cudaError_t launch_exact_total(BounceBuffers &b, int bounce, cudaStream_t stream) {

@@ -128,6 +128,9 @@ struct BounceBuffers {
     int32_t max_bounces = 0;
     float threshold = 1.0f;
     int32_t last_buffer = 0;         // which emit/shoot half the last bounce wrote
+    // One bounce of each parity captured as a graph (gather, CollectLight's
+    // levels, the totals, their copy to h_sums), made on first use.
+    cudaGraphExec_t bounce_graph[2] = {nullptr, nullptr};
     bool ready = false;
     // Statistics of the last pass.
     int32_t bounces_run = 0, exact_totals = 0;
@@ -145,6 +148,10 @@ cudaError_t launch_transfers(BounceBuffers &b, const DeviceScene &scene, uint32_
                              bool count_only);
 cudaError_t launch_gather(BounceBuffers &b, int bounce, cudaStream_t stream);
 cudaError_t launch_exact_total(BounceBuffers &b, int bounce, cudaStream_t stream);
+// Bounce number `bounce` and the copy of its totals to h_sums as one graph
+// launch on `stream`; the graph of its parity is captured on `capture` (a
+// stream of the library's own) the first time.
+cudaError_t launch_bounce_graph(BounceBuffers &b, int bounce, cudaStream_t capture, cudaStream_t stream);
 cudaError_t launch_features(BounceBuffers &b, const DeviceWorld &w, cudaStream_t stream);
 cudaError_t launch_warm_start(BounceBuffers &b, const DeviceWorld &w, const vrad_mlp &m, cudaStream_t stream);
 

@@ -217,10 +217,14 @@ cudaError_t run_bounce(vrad_ctx *ctx, cudaStream_t s, std::string &why) {
     for (int i = 0; e == cudaSuccess && i < b.max_bounces; i++) {
         // With a network attached, the second step starts from its guess
         // (launch_warm_start) instead of bouncing the first bounce's light.
-        e = (model && i == 1) ? launch_warm_start(b, ctx->world.view, *model, s) : launch_gather(b, i, s);
+        // The later plain bounces are one captured graph each.
+        const bool graph = i > 0 && !(model && i == 1);
+        if (graph) e = launch_bounce_graph(b, i, ctx->stream, s);
+        else e = (model && i == 1) ? launch_warm_start(b, ctx->world.view, *model, s) : launch_gather(b, i, s);
         if (e == cudaSuccess && i == 0)
             e = cudaMemcpyAsync(b.first, b.total, sizeof(float4) * (size_t)b.npatches, cudaMemcpyDeviceToDevice, s);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_sums, b.sums, kSums * sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess && !graph)
+            e = cudaMemcpyAsync(b.h_sums, b.sums, kSums * sizeof(double), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) break;
         b.bounces_run = i + 1;
