@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-cpu", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-learned", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--no-batch", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--batch-maps", type=int, default=32, help=argparse.SUPPRESS)
+    ap.add_argument("--batch-workers", type=int, default=4, help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -466,6 +469,39 @@ def cpu_stage(world, inp, budget_s: float = 15.0):
             "samples_per_s": n / dt}
 
 
+def batched_run(args, device_index: int) -> dict:
+    """The batched workload: `batch_maps` seeded room grids, sides drawn
+    from 2..10 rooms, each bounced to the 8x8 map's threshold, lit by the
+    native batch runner (host buffers in and out, every map's scene, world
+    and bounce uploaded inside the timed run).  The autotuner picks the
+    gather's launch shape and the maps in flight on the first eight maps;
+    one warm-up run, then the timed run, then the same maps on one worker."""
+    from hl2sdk_tools_sharp_b200 import batch as B, roomgrid as rg
+    t = time.perf_counter()
+    cfgs = [rg.config_batch(i, seed=CONFIG_SEED) for i in range(args.batch_maps)]
+    maps = [B.map_inputs(rg.generate(c), bounces=MAX_BOUNCES, threshold=BOUNCE_THRESHOLD) for c in cfgs]
+    prep_s = time.perf_counter() - t
+    with B.LightingBatch(workers=args.batch_workers, device=device_index) as batch:
+        workers, block, tune = batch.autotune(maps[:min(8, len(maps))])
+        warm, _ = batch.run(maps)
+        results, st = batch.run(maps)
+        one, st1 = batch.run(maps, workers=1)
+    same = all(np.array_equal(a.lighting, b.lighting) and np.array_equal(a.lighting, c.lighting)
+               for a, b, c in zip(results, warm, one))
+    return {"maps": len(maps), "sides": [c.side for c in cfgs], "rooms": int(sum(c.side ** 2 for c in cfgs)),
+            "triangles": int(sum(len(m.triangles) for m in maps)),
+            "samples": int(sum(len(m.inputs.samples) for m in maps)),
+            "workers": st.workers, "threads_per_cta": st.block, "autotune_s": tune,
+            "seconds": st.seconds, "busy_seconds": st.busy_seconds, "one_worker_s": st1.seconds,
+            "rays": int(st.rays), "rays_per_s": st.rays / st.seconds, "luxels": int(st.luxels),
+            "luxels_per_s": st.luxels / st.seconds, "lighting_bytes": int(st.lighting_bytes),
+            "map_s": {"min": min(r.seconds for r in results), "max": max(r.seconds for r in results)},
+            "lumps_equal_across_runs": bool(same), "host_prep_s": prep_s,
+            "note": "wall clock of vrad_batch_run: per map the scene, world and bounce uploads from host "
+                    "arrays, the light pass, the lump read back to host memory; host_prep_s (the maps' "
+                    "generation in Python) is outside it"}
+
+
 def world_and_inputs(side):
     from hl2sdk_tools_sharp_b200 import lighting as L
     w = world_for(side)
@@ -755,6 +791,12 @@ def main_stage(args):
                                 "frac": flops / (fwd_ms / 1000.0) / 1e12 / tpeak, "rows": int(len(hx)),
                                 "ms": fwd_ms, "flops_per_row": flops / len(hx)}}
         net.close()
+    batched = None
+    if rank == 0 and world_size == 1 and not args.no_batch:
+        try:
+            batched = batched_run(args, local)
+        except Exception as exc:  # reported in the line; the headline still prints
+            batched = {"error": f"{type(exc).__name__}: {exc}"}
     # The dominant phases timed alone on the launching stream: the direct
     # gather kernel, and the transfer build (its phase events).
     a_ev = torch.cuda.Event(enable_timing=True)
@@ -817,6 +859,7 @@ def main_stage(args):
             "autotune": {"threads_per_cta": block, "ms": tune_ms},
             "check": check,
             "learned": learned,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     stage.close()

@@ -24,6 +24,7 @@
 
 #include "context.cuh"
 #include "device_pool.h"
+#include "sync_wait.h"
 
 namespace {
 
@@ -76,10 +77,11 @@ cudaError_t ensure(void **buf, size_t *cap, size_t need) {
 
 int32_t check_overflow(vrad_ctx *ctx) {
     uint32_t flag = 0;
-    cudaError_t e = cudaMemcpy(&flag, ctx->status, sizeof flag, cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpyAsync(&flag, ctx->status, sizeof flag, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = vrad::wait_stream(ctx->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "reading the traversal status");
     if (flag) {
-        cudaMemset(ctx->status, 0, sizeof(uint32_t));
+        cudaMemsetAsync(ctx->status, 0, sizeof(uint32_t), ctx->stream);
         return fail(ctx, VRAD_ERR_CUDA, "traversal stack overflow (BVH deeper than %d)",
                     vrad::kStackDepth);
     }
@@ -95,6 +97,10 @@ int32_t upload(vrad_ctx *ctx, const vrad_triangle *tris, const vrad_kd_triangle 
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
     ctx->has_scene = false;
+    // The old scene's blocks go back to the device pool once no kernel of
+    // this context reads them.
+    e = vrad::quiesce(ctx);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "waiting for the context's kernels");
     ctx->scene.release();
     ctx->report = vrad::SceneBuildReport();
     // Split by the id's sky bit (TraceId.Sky): two BVHs, so a sky test can
@@ -112,9 +118,11 @@ int32_t upload(vrad_ctx *ctx, const vrad_triangle *tris, const vrad_kd_triangle 
         if (prep) ppart[k].push_back(prep[i]);
         orig[k].push_back(i);
     }
-    e = cudaMalloc(&ctx->scene.tri_id, sizeof(int32_t) * (size_t)n);
+    e = vrad::dev_alloc(&ctx->scene.tri_id, sizeof(int32_t) * (size_t)n);
     if (e == cudaSuccess)
-        e = cudaMemcpy(ctx->scene.tri_id, ids.data(), sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(ctx->scene.tri_id, ids.data(), sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice,
+                            ctx->stream);
+    if (e == cudaSuccess) e = vrad::wait_stream(ctx->stream);
     if (e != cudaSuccess) {
         ctx->scene.release();
         return cuda_fail(ctx, e, "scene ids");
@@ -142,6 +150,7 @@ int32_t trace_device(vrad_ctx *ctx, const vrad_ray *d_rays, int64_t n,
                      cudaStream_t stream) {
     cudaError_t e = vrad::launch_trace(ctx->scene.view(), d_rays, n, params_of(opts, mode), d_bits,
                                        d_hits, ctx->status, stream);
+    if (e == cudaSuccess) e = vrad::join_stream(ctx, stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "trace launch");
     return VRAD_OK;
 }
@@ -171,6 +180,45 @@ int32_t vrad_fail(vrad_ctx *ctx, int32_t code, const char *fmt, ...) {
 
 int32_t vrad_cuda_fail(vrad_ctx *ctx, cudaError_t e, const char *what) { return cuda_fail(ctx, e, what); }
 
+namespace vrad {
+cudaError_t prioritise_uploads(vrad_ctx *ctx) {
+    std::lock_guard<std::mutex> g(ctx->mu);
+    cudaError_t e = cudaSetDevice(ctx->device);
+    int least = 0, greatest = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e == cudaSuccess) e = quiesce(ctx);
+    if (e != cudaSuccess) return e;
+    cudaStream_t up = nullptr, pass = nullptr;
+    e = cudaStreamCreateWithPriority(&up, cudaStreamNonBlocking, greatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&pass, cudaStreamNonBlocking, least);
+    if (e != cudaSuccess) {
+        if (up) cudaStreamDestroy(up);
+        return e;
+    }
+    cudaStreamDestroy(ctx->stream);
+    if (ctx->pass_stream) cudaStreamDestroy(ctx->pass_stream);
+    ctx->stream = up;
+    ctx->pass_stream = pass;
+    return cudaSuccess;
+}
+
+cudaError_t release_tables(vrad_ctx *ctx) {
+    std::lock_guard<std::mutex> g(ctx->mu);
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess) e = quiesce(ctx);
+    if (e != cudaSuccess) return e;
+    ctx->has_scene = false;
+    ctx->scene.release();
+    ctx->world.release();
+    ctx->final_pass.release();
+    ctx->bounce.release();
+    ctx->supersample.release();
+    vrad::dev_free(ctx->sample_light);
+    ctx->sample_light = nullptr;
+    return cudaSuccess;
+}
+}  // namespace vrad
+
 extern "C" {
 
 int32_t vrad_abi_version(void) { return VRAD_ABI_VERSION; }
@@ -195,8 +243,10 @@ int32_t vrad_create(int32_t device, vrad_ctx **out) {
     ctx->device = device;
     e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->status, 4 * sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMemset(ctx->status, 0, 4 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->status, 0, 4 * sizeof(uint32_t), ctx->stream);
+    if (e == cudaSuccess) e = vrad::wait_stream(ctx->stream);
     if (e != cudaSuccess) {
         int32_t rc = cuda_fail(nullptr, e, "context setup");
         vrad_destroy(ctx);
@@ -229,6 +279,8 @@ int32_t vrad_destroy(vrad_ctx *ctx) {
         cudaFree(ctx->status);
         cudaFree(ctx->d_rays);
         cudaFree(ctx->d_out);
+        if (ctx->join) cudaEventDestroy(ctx->join);
+        if (ctx->pass_stream) cudaStreamDestroy(ctx->pass_stream);
         if (ctx->stream) cudaStreamDestroy(ctx->stream);
         vrad::dev_trim(ctx->device);
     }
@@ -290,7 +342,7 @@ int32_t vrad_trace_visibility(vrad_ctx *ctx, const vrad_ray *rays, int64_t n,
                       mode, ctx->stream);
     if (rc != VRAD_OK) return rc;
     e = cudaMemcpyAsync(hit_bits, ctx->d_out, 8 * words64, cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = vrad::wait_stream(ctx->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "visibility trace");
     return check_overflow(ctx);
 }
@@ -316,7 +368,7 @@ int32_t vrad_trace_closest(vrad_ctx *ctx, const vrad_ray *rays, int64_t n,
     if (rc != VRAD_OK) return rc;
     e = cudaMemcpyAsync(hits, ctx->d_out, sizeof(vrad_hit) * (size_t)n, cudaMemcpyDeviceToHost,
                         ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = vrad::wait_stream(ctx->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "closest trace");
     return check_overflow(ctx);
 }

@@ -25,6 +25,7 @@
 #include "patches.h"
 #include "setup_clock.h"
 #include "world.h"
+#include "sync_wait.h"
 
 namespace vrad {
 
@@ -169,7 +170,7 @@ cudaError_t radial_tables(BounceBuffers &b, const float4 *frames, int32_t nf, co
         if (e == cudaSuccess) e = cub::DeviceScan::InclusiveSum(tmp, tmp_bytes, d_counts, d_off + 1, npairs, stream);
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(&total, d_off + npairs, sizeof total, cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) e = vrad::wait_stream(stream);
     const size_t T1 = (size_t)(total ? total : 1);
     if (e == cudaSuccess) e = dev_alloc(&b.pr_off, sizeof(int32_t) * ((size_t)nf + 1));
     if (e == cudaSuccess) e = dev_alloc(&b.pr_patch, sizeof(int32_t) * T1);
@@ -184,7 +185,7 @@ cudaError_t radial_tables(BounceBuffers &b, const float4 *frames, int32_t nf, co
         k_radial_off<<<grid_for((int64_t)nf + 1, 256), 256, 0, stream>>>(nf, d_p0, d_off, b.pr_off);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) e = vrad::wait_stream(stream);
     for (void *x : {(void *)d_pf, (void *)d_ps, (void *)d_p0, (void *)d_counts, (void *)d_off, tmp}) dev_free(x);
     return e;
 }
@@ -225,7 +226,7 @@ cudaError_t run_bounce(vrad_ctx *ctx, cudaStream_t s, std::string &why) {
             e = cudaMemcpyAsync(b.first, b.total, sizeof(float4) * (size_t)b.npatches, cudaMemcpyDeviceToDevice, s);
         if (e == cudaSuccess && !graph)
             e = cudaMemcpyAsync(b.h_sums, b.sums, kSums * sizeof(double), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess) e = vrad::wait_stream(s);
         if (e != cudaSuccess) break;
         b.bounces_run = i + 1;
         if (model) {
@@ -252,7 +253,7 @@ cudaError_t run_bounce(vrad_ctx *ctx, cudaStream_t s, std::string &why) {
             b.exact_totals++;
             e = launch_exact_total(b, i, s);
             if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_exact, b.exact, 3 * sizeof(float), cudaMemcpyDeviceToHost, s);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e == cudaSuccess) e = vrad::wait_stream(s);
             if (e != cudaSuccess) break;
             for (int c = 0; c < 3; c++) {
                 b.added[c] = b.h_exact[c];
@@ -267,7 +268,7 @@ cudaError_t run_bounce(vrad_ctx *ctx, cudaStream_t s, std::string &why) {
     if (e == cudaSuccess) e = cudaMemcpyAsync(counts, b.counters, sizeof counts, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess && b.nreceivers)
         e = cudaMemcpyAsync(&ntr, b.tr_off + b.nreceivers, sizeof ntr, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = vrad::wait_stream(s);
     if (e == cudaSuccess) b.ntransfers = ntr;
     if (e == cudaSuccess) {
         cudaEventElapsedTime(&b.patch_light_ms, ev[0], ev[1]);
@@ -321,7 +322,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     cudaError_t e = cudaSetDevice(ctx->device);
     // The old bounce's blocks go back to the device pool: no kernel of
     // this context, on any stream, may still read them.
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = vrad::quiesce(ctx);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
     BounceBuffers &b = ctx->bounce;
     b.release();
@@ -585,7 +586,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     e = launch_transfers(b, ctx->scene.view(), ctx->status, s, true);
     int64_t ncand = 0;
     if (e == cudaSuccess && R > 0) e = cudaMemcpyAsync(&ncand, b.cand_off + R, sizeof ncand, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = vrad::wait_stream(s);
     b.ncand = ncand;
     clock.mark("candidate count");
     if (e == cudaSuccess) e = dev_alloc(&b.cand_src, sizeof(int32_t) * (size_t)(ncand ? ncand : 1));
@@ -599,14 +600,14 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     const int64_t sell_cap = ncand + 32 * std::min<int64_t>(kMaxTransfersPerReceiver, ncand);
     if (e == cudaSuccess) e = dev_alloc(&b.sell, sizeof(int2) * (size_t)(sell_cap ? sell_cap : 1));
     if (e == cudaSuccess) e = cudaMemcpyAsync(&overflow, ctx->status, sizeof overflow, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = vrad::wait_stream(s);
     if (e != cudaSuccess) {
         ctx->stager.finish(ctx->stream);  // no copy in flight into a released block
         b.release();
         return vrad_cuda_fail(ctx, e, "transfer sizing");
     }
     if (overflow) {
-        cudaMemset(ctx->status, 0, sizeof(uint32_t));
+        cudaMemsetAsync(ctx->status, 0, sizeof(uint32_t), ctx->stream);
         ctx->stager.finish(ctx->stream);  // no copy in flight into a released block
         b.release();
         return vrad_fail(ctx, VRAD_ERR_CUDA, "stack overflow in the candidate walk (flags %u)", overflow);
@@ -709,7 +710,7 @@ extern "C" int32_t vrad_bounce_last_total(vrad_ctx *ctx, float *total) {
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e == cudaSuccess) e = vrad::launch_exact_total(b, b.bounces_run - 1, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_exact, b.exact, 3 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = vrad::wait_stream(ctx->stream);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "bounce total");
     for (int c = 0; c < 3; c++) total[c] = b.h_exact[c];
     return VRAD_OK;

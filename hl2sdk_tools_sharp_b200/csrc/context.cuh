@@ -14,10 +14,15 @@
 #include "scene.cuh"
 #include "staging.h"
 #include "supersample.cuh"
+#include "sync_wait.h"
 
 struct vrad_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaEvent_t join = nullptr;   // orders `stream` after work queued on callers' streams
+    // When set, vrad_light_pass runs on this stream instead of `stream`
+    // (a batch gives its contexts' uploads the higher priority).
+    cudaStream_t pass_stream = nullptr;
     std::mutex mu;
     vrad::SceneBuffers scene;
     vrad::SceneBuildReport report;
@@ -52,6 +57,38 @@ struct vrad_ctx {
 // The direct gather with its supersampling passes into d_out (direct.cu).
 namespace vrad {
 int32_t direct_pass(vrad_ctx *ctx, float4 *d_out, cudaStream_t s);
+
+// After an entry point queued this context's kernels on a caller's stream
+// s: the context's own stream waits for them, so that waiting for the
+// context's stream waits for every kernel of the context.  Work captured
+// into a caller's graph is not tracked (the caller waits for its graph).
+inline cudaError_t join_stream(vrad_ctx *ctx, cudaStream_t s) {
+    if (s == ctx->stream) return cudaSuccess;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess || cap != cudaStreamCaptureStatusNone) return e;
+    e = cudaEventRecord(ctx->join, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->join, 0);
+    return e;
+}
+
+// Recreates the context's stream at the device's greatest priority and
+// gives its light passes their own stream at the least: on a device shared
+// by several contexts, an upload's short kernels then take SMs ahead of the
+// long kernels of other contexts' passes (abi.cu).
+cudaError_t prioritise_uploads(vrad_ctx *ctx);
+
+// Hands every device table of the context back to the device pool (scene,
+// world, final pass, bounce, supersampling), once its kernels are done; the
+// pinned host buffers stay.  A batch worker calls it after each map, so an
+// idle worker holds no device memory that another worker's map could use.
+cudaError_t release_tables(vrad_ctx *ctx);
+
+// Waits for every kernel of this context (its stream, joined by the
+// callers' streams it ran on) and for no other context's: an upload that
+// hands the old tables back to the device pool waits here, so contexts on
+// one device run their passes side by side.
+inline cudaError_t quiesce(vrad_ctx *ctx) { return vrad::wait_stream(ctx->stream); }
 }
 
 // Shared error reporting (abi.cu).

@@ -16,6 +16,7 @@ struct Pool {
     std::mutex mu;
     std::unordered_map<void *, std::pair<int, size_t>> live;  // handed out: device, block size
     std::map<int, std::multimap<size_t, void *>> cached;      // per device: block size -> block
+    PoolCounters counters;
 };
 
 // Never destroyed: blocks may be released from static destructors after
@@ -42,6 +43,13 @@ void trim_locked(Pool &p, int device) {
     for (void *q : drop) cudaFree(q);
 }
 
+// How much larger than the request a cached block may be and still be
+// taken: a quarter below 1 MiB; up to twice the request above, so that a
+// stream of maps of different sizes (a batch) reuses the blocks of the
+// larger maps instead of mapping new memory for every map (a cudaMalloc
+// costs about 25 ms per GB).
+size_t slack(size_t want) { return want < ((size_t)1 << 20) ? want / 4 : want; }
+
 }  // namespace
 
 cudaError_t dev_alloc(void **out, size_t bytes) {
@@ -55,7 +63,7 @@ cudaError_t dev_alloc(void **out, size_t bytes) {
         std::lock_guard<std::mutex> g(p.mu);
         auto &c = p.cached[device];
         auto it = c.lower_bound(want);
-        if (it != c.end() && it->first - want <= want / 4) {
+        if (it != c.end() && it->first - want <= slack(want)) {
             *out = it->second;
             p.live[*out] = {device, it->first};
             c.erase(it);
@@ -68,6 +76,7 @@ cudaError_t dev_alloc(void **out, size_t bytes) {
         {
             std::lock_guard<std::mutex> g(p.mu);
             trim_locked(p, device);
+            p.counters.trims++;
         }
         e = cudaMalloc(out, want);
     }
@@ -77,6 +86,8 @@ cudaError_t dev_alloc(void **out, size_t bytes) {
     }
     std::lock_guard<std::mutex> g(p.mu);
     p.live[*out] = {device, want};
+    p.counters.mallocs++;
+    p.counters.malloc_bytes += (int64_t)want;
     return cudaSuccess;
 }
 
@@ -99,6 +110,12 @@ void dev_trim(int device) {
     Pool &p = pool();
     std::lock_guard<std::mutex> g(p.mu);
     trim_locked(p, device);
+}
+
+PoolCounters dev_counters() {
+    Pool &p = pool();
+    std::lock_guard<std::mutex> g(p.mu);
+    return p.counters;
 }
 
 size_t dev_cached_bytes(int device) {

@@ -2,17 +2,19 @@
 // and bounce uploads build and the light pass's per-call buffers.
 //
 // A released block goes back to a per-device cache instead of to cudaFree,
-// and a later request takes a cached block of its size class (at most a
-// quarter larger) before calling cudaMalloc: re-uploading a map of the same
+// and a later request takes the smallest cached block that holds it (at
+// most a quarter larger below 1 MiB, at most twice the request above)
+// before calling cudaMalloc: re-uploading a map of the same or a smaller
 // size maps no new memory and unmaps none.  A cudaMalloc that runs out of
 // memory empties that device's cache and tries once more.  dev_free does not
 // wait for the device: callers synchronize before releasing blocks that
-// kernels may still read (the uploads synchronize the device first).
+// kernels may still read (an upload first waits for its context's stream).
 #pragma once
 
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <cstdint>
 
 namespace vrad {
 
@@ -36,5 +38,14 @@ void dev_trim(int device);
 
 // Bytes cached (not handed out) on `device`.
 size_t dev_cached_bytes(int device);
+
+// What the pool has asked of CUDA since the library loaded: cudaMalloc
+// calls and their bytes, and the times an out-of-memory emptied a cache.
+struct PoolCounters {
+    int64_t mallocs = 0;
+    int64_t malloc_bytes = 0;
+    int64_t trims = 0;
+};
+PoolCounters dev_counters();
 
 }  // namespace vrad

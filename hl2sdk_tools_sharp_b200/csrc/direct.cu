@@ -31,6 +31,7 @@
 #include "host_parallel.h"
 #include "setup_clock.h"
 #include "supersample.cuh"
+#include "sync_wait.h"
 
 namespace vrad {
 
@@ -259,7 +260,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     cudaError_t e = cudaSetDevice(ctx->device);
     // The old world's blocks go back to the device pool: no kernel of this
     // context, on any stream, may still read them.
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = vrad::quiesce(ctx);
     vrad::WorldBuffers &wb = ctx->world;
     wb.release();
     if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.slots, slots);
@@ -373,7 +374,9 @@ extern "C" int32_t vrad_direct_lighting_device(vrad_ctx *ctx, vrad_lighting_valu
     std::lock_guard<std::mutex> g(ctx->mu);
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
-    return direct_on(ctx, reinterpret_cast<float4 *>(d_out), (cudaStream_t)stream);
+    const int32_t rc = direct_on(ctx, reinterpret_cast<float4 *>(d_out), (cudaStream_t)stream);
+    e = vrad::join_stream(ctx, (cudaStream_t)stream);
+    return rc != VRAD_OK || e == cudaSuccess ? rc : vrad_cuda_fail(ctx, e, "joining the caller's stream");
 }
 
 extern "C" int32_t vrad_direct_lighting(vrad_ctx *ctx, vrad_lighting_value *out, vrad_direct_stats *stats) {
@@ -404,11 +407,11 @@ extern "C" int32_t vrad_direct_lighting(vrad_ctx *ctx, vrad_lighting_value *out,
             e = cudaMemcpyAsync(counts, ctx->world.counters, sizeof counts, cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(&overflow, ctx->status, sizeof overflow, cudaMemcpyDeviceToHost, ctx->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e == cudaSuccess) e = vrad::wait_stream(ctx->stream);
         if (e != cudaSuccess) rc = vrad_cuda_fail(ctx, e, "direct lighting");
     }
     if (rc == VRAD_OK && overflow) {
-        cudaMemset(ctx->status, 0, sizeof(uint32_t));
+        cudaMemsetAsync(ctx->status, 0, sizeof(uint32_t), ctx->stream);
         rc = vrad_fail(ctx, VRAD_ERR_CUDA, "traversal stack overflow (BVH deeper than %d)", vrad::kStackDepth);
     }
     if (rc == VRAD_OK && stats) {

@@ -39,6 +39,7 @@
 #include "host_parallel.h"
 #include "setup_clock.h"
 #include "world.h"
+#include "sync_wait.h"
 
 namespace vrad {
 
@@ -474,7 +475,7 @@ cudaError_t neighbour_candidates(FinalBuffers &fb, int32_t nfaces, const std::ve
         e = cudaGetLastError();
     }
     // The temporaries go back to the pool once the kernels are done.
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) e = vrad::wait_stream(stream);
     for (void *q : {(void *)d_pf, (void *)d_nlist, (void *)d_noff, (void *)d_counts, (void *)d_srun, (void *)d_off, tmp})
         dev_free(q);
     return e;
@@ -635,7 +636,9 @@ extern "C" int32_t vrad_light_pass_device(vrad_ctx *ctx, uint8_t *d_lighting, vo
     std::lock_guard<std::mutex> g(ctx->mu);
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
-    return pass_on(ctx, d_lighting, (cudaStream_t)stream, nullptr, nullptr);
+    const int32_t rc = pass_on(ctx, d_lighting, (cudaStream_t)stream, nullptr, nullptr);
+    e = vrad::join_stream(ctx, (cudaStream_t)stream);
+    return rc != VRAD_OK || e == cudaSuccess ? rc : vrad_cuda_fail(ctx, e, "joining the caller's stream");
 }
 
 extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t capacity, int32_t *lightofs,
@@ -648,6 +651,7 @@ extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t cap
         return vrad_fail(ctx, VRAD_ERR_ARG, "the LIGHTING lump needs %lld bytes, %lld given", (long long)fb.lighting_bytes,
                          (long long)capacity);
     cudaError_t e = cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->pass_stream ? ctx->pass_stream : ctx->stream;
     uint8_t *d_lighting = nullptr;
     cudaEvent_t a = nullptr, m = nullptr, bm = nullptr, b = nullptr;
     if (e == cudaSuccess) e = vrad::dev_alloc(&d_lighting, (size_t)(fb.lighting_bytes ? fb.lighting_bytes : 4));
@@ -655,23 +659,23 @@ extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t cap
     if (e == cudaSuccess) e = cudaEventCreate(&m);
     if (e == cudaSuccess) e = cudaEventCreate(&bm);
     if (e == cudaSuccess) e = cudaEventCreate(&b);
-    if (e == cudaSuccess) e = cudaEventRecord(a, ctx->stream);
-    int32_t rc = e == cudaSuccess ? pass_on(ctx, d_lighting, ctx->stream, m, bm) : vrad_cuda_fail(ctx, e, "light pass set-up");
+    if (e == cudaSuccess) e = cudaEventRecord(a, s);
+    int32_t rc = e == cudaSuccess ? pass_on(ctx, d_lighting, s, m, bm) : vrad_cuda_fail(ctx, e, "light pass set-up");
     unsigned long long counts[2] = {0, 0};
     uint32_t overflow = 0;
     if (rc == VRAD_OK) {
-        e = cudaEventRecord(b, ctx->stream);
+        e = cudaEventRecord(b, s);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(lighting, d_lighting, (size_t)fb.lighting_bytes, cudaMemcpyDeviceToHost, ctx->stream);
+            e = cudaMemcpyAsync(lighting, d_lighting, (size_t)fb.lighting_bytes, cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(counts, ctx->world.counters, sizeof counts, cudaMemcpyDeviceToHost, ctx->stream);
+            e = cudaMemcpyAsync(counts, ctx->world.counters, sizeof counts, cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(&overflow, ctx->status, sizeof overflow, cudaMemcpyDeviceToHost, ctx->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+            e = cudaMemcpyAsync(&overflow, ctx->status, sizeof overflow, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = vrad::wait_stream(s);
         if (e != cudaSuccess) rc = vrad_cuda_fail(ctx, e, "light pass");
     }
     if (rc == VRAD_OK && overflow) {
-        cudaMemset(ctx->status, 0, sizeof(uint32_t));
+        cudaMemsetAsync(ctx->status, 0, sizeof(uint32_t), s);
         rc = vrad_fail(ctx, VRAD_ERR_CUDA, "traversal stack overflow (BVH deeper than %d)", vrad::kStackDepth);
     }
     if (rc == VRAD_OK) {
@@ -696,6 +700,8 @@ extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t cap
             stats->supersample_ms = ctx->supersample.ms;
         }
     }
+    if (rc != VRAD_OK) vrad::wait_stream(s);  // no kernel still writes the lump
+    if (s != ctx->stream) vrad::join_stream(ctx, s);
     vrad::dev_free(d_lighting);
     if (a) cudaEventDestroy(a);
     if (m) cudaEventDestroy(m);

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <atomic>
 #include <condition_variable>
+#include <cstddef>
 #include <cstdint>
 #include <functional>
 #include <memory>
@@ -25,8 +26,12 @@ inline unsigned host_threads() {
     return std::max(1u, std::min(32u, hw));
 }
 
-// The workers behind parallel_for.  One job at a time (a second caller
-// waits); the calling thread works on the job too.
+// The workers behind parallel_for.  Several callers (a batch's workers,
+// each setting up its own map) may run jobs at once: the jobs wait in
+// arrival order, and a free pool thread joins the oldest job that still
+// wants threads, so a job's tail (its last chunks, worked on by a few
+// threads) leaves the other threads free for the next job.  The calling
+// thread works on its own job too.
 class HostPool {
 public:
     static HostPool &get() {
@@ -34,52 +39,59 @@ public:
         return *p;
     }
 
-    // fn() on `workers` pool threads and on the caller.
+    // fn() on up to `workers` pool threads and on the caller.  fn must
+    // return at once when the job has no work left (a late joiner finds
+    // none).
     void run(unsigned workers, const std::function<void()> &fn) {
-        std::lock_guard<std::mutex> one(job_mu_);
-        workers = std::min<unsigned>(workers, (unsigned)threads_.size());
-        {
-            std::lock_guard<std::mutex> g(mu_);
-            fn_ = &fn;
-            want_ = workers;
-            taken_ = 0;
-            done_ = 0;
-            gen_++;
+        Job job;
+        job.fn = &fn;
+        job.want = std::min<unsigned>(workers, (unsigned)threads_.size());
+        if (job.want > 0) {
+            {
+                std::lock_guard<std::mutex> g(mu_);
+                queue_.push_back(&job);
+            }
+            cv_.notify_all();
         }
-        cv_.notify_all();
         fn();
         std::unique_lock<std::mutex> g(mu_);
-        done_cv_.wait(g, [&] { return done_ == want_; });
-        fn_ = nullptr;
+        // No thread joins the job after this point.
+        for (size_t k = 0; k < queue_.size(); k++)
+            if (queue_[k] == &job) {
+                queue_.erase(queue_.begin() + (std::ptrdiff_t)k);
+                break;
+            }
+        done_cv_.wait(g, [&] { return job.done == job.taken; });
     }
 
 private:
+    struct Job {
+        const std::function<void()> *fn = nullptr;
+        unsigned want = 0, taken = 0, done = 0;
+    };
+
     explicit HostPool(unsigned n) {
         for (unsigned i = 0; i < n; i++) threads_.emplace_back([this] { loop(); });
         for (auto &t : threads_) t.detach();
     }
 
     void loop() {
-        uint64_t seen = 0;
         std::unique_lock<std::mutex> g(mu_);
         while (true) {
-            cv_.wait(g, [&] { return gen_ != seen && taken_ < want_; });
-            seen = gen_;
-            taken_++;
-            const std::function<void()> *fn = fn_;
+            cv_.wait(g, [&] { return !queue_.empty(); });
+            Job *job = queue_.front();
+            if (++job->taken == job->want) queue_.erase(queue_.begin());
             g.unlock();
-            (*fn)();
+            (*job->fn)();
             g.lock();
-            if (++done_ == want_) done_cv_.notify_one();
+            if (++job->done == job->taken) done_cv_.notify_all();
         }
     }
 
     std::vector<std::thread> threads_;
-    std::mutex job_mu_, mu_;
+    std::mutex mu_;
     std::condition_variable cv_, done_cv_;
-    const std::function<void()> *fn_ = nullptr;
-    unsigned want_ = 0, taken_ = 0, done_ = 0;
-    uint64_t gen_ = 0;
+    std::vector<Job *> queue_;   // jobs that still want threads, oldest first
 };
 
 // Whether this thread is running a parallel_for body.

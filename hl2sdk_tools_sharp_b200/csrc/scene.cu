@@ -23,7 +23,9 @@
 #include <vector>
 
 #include "bvh_sah.h"
+#include "device_pool.h"
 #include "scene.cuh"
+#include "sync_wait.h"
 
 namespace vrad {
 
@@ -231,26 +233,26 @@ cudaError_t build_bvh(BvhBuffers &sb, const vrad_triangle *h_tris,
     VRAD_TRY(cudaEventCreate(&ev1));
     VRAD_TRY(cudaEventRecord(ev0, stream));
 
-    VRAD_TRY(cudaMalloc(&d_in, sizeof(vrad_triangle) * n));
+    VRAD_TRY(dev_alloc(&d_in, sizeof(vrad_triangle) * n));
     VRAD_TRY(cudaMemcpyAsync(d_in, h_tris, sizeof(vrad_triangle) * n, cudaMemcpyHostToDevice, stream));
     if (h_prepared) {
-        VRAD_TRY(cudaMalloc(&d_prep, sizeof(vrad_kd_triangle) * n));
+        VRAD_TRY(dev_alloc(&d_prep, sizeof(vrad_kd_triangle) * n));
         VRAD_TRY(cudaMemcpyAsync(d_prep, h_prepared, sizeof(vrad_kd_triangle) * n,
                                  cudaMemcpyHostToDevice, stream));
     }
-    VRAD_TRY(cudaMalloc(&d_orig, sizeof(int32_t) * n));
+    VRAD_TRY(dev_alloc(&d_orig, sizeof(int32_t) * n));
     VRAD_TRY(cudaMemcpyAsync(d_orig, h_orig, sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream));
-    VRAD_TRY(cudaMalloc(&u0, sizeof(float4) * n));
-    VRAD_TRY(cudaMalloc(&u1, sizeof(float4) * n));
-    VRAD_TRY(cudaMalloc(&u2, sizeof(float4) * n));
-    VRAD_TRY(cudaMalloc(&tri_box, sizeof(float) * 6 * n));
-    VRAD_TRY(cudaMalloc(&d_bounds, sizeof(float) * 8));
-    VRAD_TRY(cudaMalloc(&sb.tri0, sizeof(float4) * n));
-    VRAD_TRY(cudaMalloc(&sb.tri1, sizeof(float4) * n));
-    VRAD_TRY(cudaMalloc(&sb.tri2, sizeof(float4) * n));
-    VRAD_TRY(cudaMalloc(&sb.nodes, sizeof(float4) * 4 * inner));
-    VRAD_TRY(cudaMalloc(&leaf_box, sizeof(float) * 6 * n));
-    VRAD_TRY(cudaMalloc(&d_stats, sizeof(int) * 4));
+    VRAD_TRY(dev_alloc(&u0, sizeof(float4) * n));
+    VRAD_TRY(dev_alloc(&u1, sizeof(float4) * n));
+    VRAD_TRY(dev_alloc(&u2, sizeof(float4) * n));
+    VRAD_TRY(dev_alloc(&tri_box, sizeof(float) * 6 * n));
+    VRAD_TRY(dev_alloc(&d_bounds, sizeof(float) * 8));
+    VRAD_TRY(dev_alloc(&sb.tri0, sizeof(float4) * n));
+    VRAD_TRY(dev_alloc(&sb.tri1, sizeof(float4) * n));
+    VRAD_TRY(dev_alloc(&sb.tri2, sizeof(float4) * n));
+    VRAD_TRY(dev_alloc(&sb.nodes, sizeof(float4) * 4 * inner));
+    VRAD_TRY(dev_alloc(&leaf_box, sizeof(float) * 6 * n));
+    VRAD_TRY(dev_alloc(&d_stats, sizeof(int) * 4));
     VRAD_TRY(cudaMemsetAsync(d_stats, 0, sizeof(int) * 4, stream));
 
     k_prepare<<<blocks(n, 128), 128, 0, stream>>>(d_in, d_prep, d_orig, n, u0, u1, u2, tri_box);
@@ -262,7 +264,7 @@ cudaError_t build_bvh(BvhBuffers &sb, const vrad_triangle *h_tris,
 
     if (n == 1) {
         int32_t zero = 0;
-        VRAD_TRY(cudaMalloc(&order, sizeof(int32_t)));
+        VRAD_TRY(dev_alloc(&order, sizeof(int32_t)));
         VRAD_TRY(cudaMemcpyAsync(order, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, stream));
         k_pad_single<<<1, 1, 0, stream>>>(tri_box, d_bounds, leaf_box);
         k_emit_single<<<1, 1, 0, stream>>>(leaf_box, sb.nodes);
@@ -279,7 +281,7 @@ cudaError_t build_bvh(BvhBuffers &sb, const vrad_triangle *h_tris,
         std::vector<float> box((size_t)6 * n);
         VRAD_TRY(cudaMemcpyAsync(box.data(), tri_box, sizeof(float) * box.size(), cudaMemcpyDeviceToHost, stream));
         VRAD_TRY(cudaMemcpyAsync(bounds, d_bounds, sizeof(float) * 7, cudaMemcpyDeviceToHost, stream));
-        VRAD_TRY(cudaStreamSynchronize(stream));
+        VRAD_TRY(vrad::wait_stream(stream));
         const float pad = ldexpf(bounds[6], -16) + 1e-6f;
         for (int i = 0; i < n; i++)
             for (int a = 0; a < 3; a++) {
@@ -287,7 +289,7 @@ cudaError_t build_bvh(BvhBuffers &sb, const vrad_triangle *h_tris,
                 box[6 * (size_t)i + 3 + a] += pad;
             }
         build_sah(box.data(), n, tree);
-        VRAD_TRY(cudaMalloc(&order, sizeof(int32_t) * n));
+        VRAD_TRY(dev_alloc(&order, sizeof(int32_t) * n));
         VRAD_TRY(cudaMemcpyAsync(order, tree.order.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream));
         VRAD_TRY(cudaMemcpyAsync(sb.nodes, tree.nodes.data(), sizeof(float4) * tree.nodes.size(),
                                  cudaMemcpyHostToDevice, stream));
@@ -303,7 +305,7 @@ cudaError_t build_bvh(BvhBuffers &sb, const vrad_triangle *h_tris,
         VRAD_TRY(cudaMemcpyAsync(dstats, d_stats, sizeof(int) * 4, cudaMemcpyDeviceToHost, stream));
         VRAD_TRY(cudaMemcpyAsync(bounds, d_bounds, sizeof(float) * 7, cudaMemcpyDeviceToHost, stream));
         VRAD_TRY(cudaEventRecord(ev1, stream));
-        VRAD_TRY(cudaStreamSynchronize(stream));
+        VRAD_TRY(vrad::wait_stream(stream));
         stats[3] = dstats[3];
     }
     if (stats[3] != 0) {
@@ -330,17 +332,19 @@ cudaError_t build_bvh(BvhBuffers &sb, const vrad_triangle *h_tris,
     }
 
 fail:
-    cudaFree(d_in);
-    cudaFree(d_prep);
-    cudaFree(d_orig);
-    cudaFree(u0);
-    cudaFree(u1);
-    cudaFree(u2);
-    cudaFree(tri_box);
-    cudaFree(d_bounds);
-    cudaFree(leaf_box);
-    cudaFree(order);
-    cudaFree(d_stats);
+    // The scratch goes back to the device pool once the stream is done with it.
+    if (err != cudaSuccess) vrad::wait_stream(stream);
+    dev_free(d_in);
+    dev_free(d_prep);
+    dev_free(d_orig);
+    dev_free(u0);
+    dev_free(u1);
+    dev_free(u2);
+    dev_free(tri_box);
+    dev_free(d_bounds);
+    dev_free(leaf_box);
+    dev_free(order);
+    dev_free(d_stats);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (err != cudaSuccess) sb.release();
@@ -348,10 +352,10 @@ fail:
 }
 
 void BvhBuffers::release() {
-    cudaFree(tri0);
-    cudaFree(tri1);
-    cudaFree(tri2);
-    cudaFree(nodes);
+    dev_free(tri0);
+    dev_free(tri1);
+    dev_free(tri2);
+    dev_free(nodes);
     tri0 = tri1 = tri2 = nullptr;
     nodes = nullptr;
     ntris = 0;
@@ -361,7 +365,7 @@ void BvhBuffers::release() {
 void SceneBuffers::release() {
     opaque.release();
     sky.release();
-    cudaFree(tri_id);
+    dev_free(tri_id);
     tri_id = nullptr;
     ntris = 0;
 }

@@ -6,6 +6,7 @@
 #include <cstring>
 
 #include "host_parallel.h"
+#include "sync_wait.h"
 
 namespace vrad {
 
@@ -81,7 +82,7 @@ cudaError_t Stager::put(void *dst, const void *src, size_t bytes, cudaStream_t s
 }
 
 cudaError_t Stager::finish(cudaStream_t stream) {
-    const cudaError_t e = cudaStreamSynchronize(stream);
+    const cudaError_t e = vrad::wait_stream(stream);
     for (int k = 0; k < kSlots; k++) pending_[k] = false;
     cur_ = 0;
     off_ = 0;

@@ -40,6 +40,7 @@
 #include "setup_clock.h"
 #include "supersample.cuh"
 #include "world.h"
+#include "sync_wait.h"
 
 namespace vrad {
 
@@ -402,7 +403,7 @@ cudaError_t run_supersample(SupersampleBuffers &ss, const DeviceScene &scene, co
         if (e == cudaSuccess) e = cudaGetLastError();
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(ss.h_counts, ss.counts, sizeof(int32_t) * (1 + (size_t)C), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess) e = vrad::wait_stream(s);
         if (e != cudaSuccess) break;
         const int32_t nsel = ss.h_counts[0];
         if (nsel == 0) break;
@@ -433,7 +434,7 @@ cudaError_t run_supersample(SupersampleBuffers &ss, const DeviceScene &scene, co
         if (e == cudaSuccess) e = cudaGetLastError();
         // The base table is read by this pass's kernels before the next
         // pass rewrites it.
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess) e = vrad::wait_stream(s);
         ss.supersampled += nsel;
         ss.passes_run = pass;
     }

@@ -25,6 +25,7 @@
 #include "setup_clock.h"
 #include "supersample.cuh"
 #include "world.h"
+#include "sync_wait.h"
 
 namespace vrad {
 
@@ -311,7 +312,7 @@ cudaError_t device_windings(SupersampleBuffers &ss, const RowStrips &rs, const F
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaMemcpyAsync(flags, d_flags, sizeof flags, cudaMemcpyDeviceToHost, stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e == cudaSuccess) e = vrad::wait_stream(stream);
         match = e == cudaSuccess && !flags[0] && !flags[1];
     }
     if (e == cudaSuccess && !match)

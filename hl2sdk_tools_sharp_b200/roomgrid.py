@@ -70,6 +70,20 @@ def config_8x8(seed: int = 1) -> Config:
                   sky_ambient=True)
 
 
+BATCH_SIDES = (2, 10)
+
+
+def config_batch(index: int, seed: int = 1) -> Config:
+    """Map `index` of the batched workload: a side drawn uniformly from 2..10
+    rooms by (seed, index); otherwise the 8 x 8 map's settings (scale 8, 0-6
+    pillars per room, spot fraction 0.5, sun + sky), with one light per room
+    as the 8 x 8 map has."""
+    rng = np.random.default_rng([seed, index])
+    side = int(rng.integers(BATCH_SIDES[0], BATCH_SIDES[1] + 1))
+    return Config(side=side, seed=seed * 1000 + index, luxel_scale=8.0, pillars=(0, 6), lights=side * side,
+                  spot_fraction=0.5, sky_ambient=True)
+
+
 @dataclasses.dataclass
 class World:
     config: Config

@@ -537,6 +537,86 @@ int32_t vrad_bounce_features_device(vrad_ctx *ctx, uint16_t *x, float *target, i
 int32_t vrad_trace_visibility_static(vrad_ctx *ctx, const vrad_ray *rays, int64_t n,
                                      const vrad_trace_options *opts, uint64_t *hit_bits);
 
+/* ---- Batches of maps ------------------------------------------------------
+ *
+ * Many maps lit on one device.  No counterpart in the reference, which
+ * lights one map per call (Vrad.RunAsync, MapTools/Rad/Vrad.cs:160-390).
+ * A batch owns `workers` persistent host threads, each with its own context
+ * (stream, device tables, pinned staging).  The threads take maps from one
+ * shared queue, largest first.  Each map goes through the whole lighting
+ * stage: vrad_scene_upload, vrad_world_upload, vrad_set_extra_passes,
+ * vrad_bounce_upload when the map has a bounce, then vrad_light_pass.  One
+ * map's host set-up (BVH, sample slots, patch tree) therefore overlaps other
+ * maps' passes on the device, and small maps' kernels share the SMs.  Each
+ * lump is byte-identical to the one the single-map calls write. */
+
+#define VRAD_BATCH_MAX_WORKERS 8
+
+typedef struct vrad_batch vrad_batch;
+
+/* One map of a batch.  The inputs are what the single-map calls take.
+ * The run fills in the outputs. */
+typedef struct vrad_batch_map {
+    const vrad_triangle *triangles;  /* the shadow casters (vrad_scene_upload) */
+    const vrad_world_desc *world;
+    const vrad_bounce_desc *bounce;  /* NULL: the map is not bounced */
+    uint8_t *lighting;               /* host, capacity bytes: the LIGHTING lump */
+    int32_t *lightofs;               /* nfaces entries, nullable */
+    int64_t capacity;
+    int32_t ntriangles;
+    int32_t extra_passes;            /* supersampling passes; negative: the default 4 */
+    /* written by the run */
+    int32_t status;                  /* VRAD_OK, or the code of the call that failed */
+    int32_t worker;                  /* the worker that lit the map */
+    int64_t lighting_bytes;
+    double seconds;                  /* the map's time on its worker, uploads included */
+    double scene_s;                  /* of it: vrad_scene_upload */
+    double world_s;                  /* vrad_world_upload and vrad_set_extra_passes */
+    double bounce_s;                 /* vrad_bounce_upload */
+    double pass_s;                   /* vrad_light_pass, the lump read back */
+    vrad_pass_stats pass;
+    vrad_bounce_stats bounce_stats;  /* zero when the map is not bounced */
+    char error[256];                 /* the failing call's message */
+} vrad_batch_map;
+
+typedef struct vrad_batch_stats {
+    int32_t workers;        /* workers that took maps */
+    int32_t maps;
+    int32_t failed;
+    int32_t block;          /* the gather's threads per CTA; 0: each context's default */
+    double seconds;         /* wall time of the whole batch */
+    double busy_seconds;    /* sum of the maps' times */
+    int64_t rays;           /* visibility, sky and transfer rays of every map */
+    int64_t luxels;
+    int64_t lighting_bytes;
+    int64_t device_mallocs;      /* cudaMalloc calls of the library's device pool during the run */
+    int64_t device_malloc_bytes;
+    int64_t device_trims;        /* out-of-memory retries that emptied the pool's cache */
+} vrad_batch_stats;
+
+/* A batch runner on `device` with `workers` threads and contexts
+ * (1..VRAD_BATCH_MAX_WORKERS). */
+int32_t vrad_batch_create(int32_t device, int32_t workers, vrad_batch **out);
+int32_t vrad_batch_destroy(vrad_batch *batch);
+
+/* Lights every map; blocks until all are done.  workers: how many of the
+ * batch's workers take maps (0: the count the autotuner chose, else all).
+ * A worker hands its map's device tables back as soon as the map's lump is
+ * read, and a map that ran out of device memory beside the others is lit
+ * again at the end, alone.  Returns VRAD_OK when every map's status is
+ * VRAD_OK; otherwise the first failing map's code, after all maps have
+ * run. */
+int32_t vrad_batch_run(vrad_batch *batch, vrad_batch_map *maps, int32_t nmaps, int32_t workers,
+                       vrad_batch_stats *stats);
+
+/* The batch's autotuner.  It first uploads the largest map on one context
+ * and picks the gather's launch shape there (vrad_direct_autotune).  It then
+ * lights all of `maps` once per worker count 1..created and keeps the fastest
+ * count.  seconds (nullable, `created` entries) receives each count's wall
+ * time.  The maps' outputs hold the last sweep's results. */
+int32_t vrad_batch_autotune(vrad_batch *batch, vrad_batch_map *maps, int32_t nmaps, int32_t *chosen_workers,
+                            int32_t *chosen_block, double *seconds);
+
 /* DetMathF.Asin / DetMathF.Pow (MapFormats/Numerics/DetMathF.cs:141-164,
  * 265-292) as the device computes them inside the transfer build and the
  * spotlight falloff: the float nearest the exact value.  out[i] = asin a[i]
