@@ -847,9 +847,13 @@ def main_stage(args):
                          "transfers": transfer_ms, "bounces": statistics.median([p[2] for p in phases])},
             "bounce_iterations": nb,
             "e2e": e2e,
-            # direct 1, patch light 2, transfer build 5 + 2 scans (2 each),
-            # 3 per bounce, final 4 (exact totals add one each when needed).
-            "gpu_launches": (1 + 2 + 9 + 3 * nb + 4) * args.steps,
+            # Per light pass of this map (the ncu launch list in profiles/):
+            # direct 1; supersampling 4 per pass run + 1; patch light 2;
+            # transfer build 16 (candidates, rays, count, write, slices,
+            # their scans and sort); final 4; per bounce the gather, the 8
+            # tree levels of CollectLight and the totals (exact totals add
+            # one when needed).
+            "gpu_launches": (1 + 4 * int(pstats.extra_passes_run) + 1 + 2 + 16 + 4 + 10 * nb) * args.steps,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),

@@ -712,20 +712,26 @@ cudaError_t launch_patch_light(const BounceBuffers &b, const float4 *sample_ligh
 }
 
 // The transfer build.  count_only: the candidate counts and offsets alone
-// (sizing at upload).  Otherwise the candidates, their rays and form
-// factors, and the transfer lists; counters[0..1] are added to.
+// (at upload: they size the buffers, and they depend only on the patch
+// tree and the PVS rows, so they stay valid until the next upload).
+// Otherwise, with those offsets, the candidates written, their rays and
+// form factors, and the transfer lists; counters[0..1] are added to.
 cudaError_t launch_transfers(BounceBuffers &b, const DeviceScene &scene, uint32_t *overflow, cudaStream_t stream,
                              bool count_only) {
     const int R = b.nreceivers;
     if (R == 0) return cudaSuccess;
-    // Candidate counts into cand_off[1..R], then the exclusive scan.
-    k_candidates<<<blocks(R, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, nullptr, b.cand_off + 1, nullptr,
-                                                                       overflow);
-    cudaError_t e = cudaMemsetAsync(b.cand_off, 0, sizeof(int64_t), stream);
-    if (e != cudaSuccess) return e;
-    size_t tmp = b.scan_tmp_bytes;
-    e = cub::DeviceScan::InclusiveSum(b.scan_tmp, tmp, b.cand_off + 1, b.cand_off + 1, R, stream);
-    if (e != cudaSuccess || count_only) return e != cudaSuccess ? e : cudaGetLastError();
+    cudaError_t e = cudaSuccess;
+    size_t tmp = 0;
+    if (count_only) {
+        // Candidate counts into cand_off[1..R], then the exclusive scan.
+        k_candidates<<<blocks(R, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, nullptr, b.cand_off + 1, nullptr,
+                                                                           overflow);
+        e = cudaMemsetAsync(b.cand_off, 0, sizeof(int64_t), stream);
+        if (e != cudaSuccess) return e;
+        tmp = b.scan_tmp_bytes;
+        e = cub::DeviceScan::InclusiveSum(b.scan_tmp, tmp, b.cand_off + 1, b.cand_off + 1, R, stream);
+        return e != cudaSuccess ? e : cudaGetLastError();
+    }
     k_candidates<<<blocks(R, kBounceBlock), kBounceBlock, 0, stream>>>(b.view, b.cand_off, nullptr, b.cand_src,
                                                                        overflow);
     if (b.ncand > 0)
