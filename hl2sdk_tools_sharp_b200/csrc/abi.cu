@@ -207,6 +207,9 @@ cudaError_t release_tables(vrad_ctx *ctx) {
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e == cudaSuccess) e = quiesce(ctx);
     if (e != cudaSuccess) return e;
+    join_ahead(ctx);
+    ctx->ahead = PatchForest();
+    ctx->ahead_ok = false;
     ctx->has_scene = false;
     ctx->scene.release();
     ctx->world.release();
@@ -265,6 +268,7 @@ int32_t vrad_destroy(vrad_ctx *ctx) {
     if (!ctx) return VRAD_OK;
     {
         std::lock_guard<std::mutex> g(ctx->mu);
+        vrad::join_ahead(ctx);
         cudaSetDevice(ctx->device);
         // Kernels of this context may run on callers' streams too.
         cudaDeviceSynchronize();

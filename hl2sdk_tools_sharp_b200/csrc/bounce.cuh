@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "direct.cuh"
+#include "host_parallel.h"
 #include "scene.cuh"
 #include "vrad_internal.cuh"
 
@@ -123,7 +124,7 @@ struct BounceBuffers {
     float *prad_weight = nullptr;
 
     BounceView view{};
-    std::vector<int32_t> h_recv;     // host copy of the receiver order
+    uvector<int32_t> h_recv;         // host copy of the receiver order
     int32_t npatches = 0, nfaces = 0, nreceivers = 0, nleaves = 0;
     int32_t max_bounces = 0;
     float threshold = 1.0f;

@@ -368,9 +368,19 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     rows.C = C;
     std::string why;
     const int64_t nvert = (int64_t)ctx->h_vertices.size() / 3;
-    if (!build_patch_tree(ctx->h_faces.data(), nf, ctx->h_vertices.data(), nvert, d->reflectivity, d->max_chop,
-                          d->min_chop, tree, rows, why))
+    // The forest the world upload grew ahead, when its chop sizes are this
+    // upload's; otherwise grown here.
+    vrad::join_ahead(ctx);
+    PatchForest forest = std::move(ctx->ahead);
+    const bool ahead = ctx->ahead_ok && forest.grown() && forest.max_chop() == d->max_chop &&
+                       forest.min_chop() == d->min_chop;
+    ctx->ahead = PatchForest();
+    ctx->ahead_ok = false;
+    if (!(ahead || forest.grow(ctx->h_faces.data(), nf, ctx->h_vertices.data(), nvert, d->max_chop, d->min_chop,
+                               why)) ||
+        !forest.merge(d->reflectivity, tree, rows, why))
         return vrad_fail(ctx, VRAD_ERR_ARG, "patches: %s", why.c_str());
+    forest = PatchForest();
     const int32_t P = tree.npatches;
     clock.mark("patch tree");
     if (rows.bad.load() != INT32_MAX)
@@ -433,7 +443,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
         chunk_at[(size_t)k * (size_t)(C + 1) + C] = nleaves;
         nleaves += ccount[(size_t)k * (size_t)(C + 1) + C];
     }
-    std::vector<int32_t> recv((size_t)cstart[(size_t)C]), leaf_desc((size_t)nleaves), leaf_rank((size_t)P, -1);
+    uvector<int32_t> recv((size_t)cstart[(size_t)C]), leaf_desc((size_t)nleaves), leaf_rank((size_t)P, -1);
     parallel_for(nchunks, 1, [&](int64_t k) {
         int32_t *at = &chunk_at[(size_t)k * (size_t)(C + 1)];
         const int32_t lo = (int32_t)k * kChunk, hi = std::min(P, (int32_t)(k + 1) * kChunk);
@@ -449,7 +459,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     // tree is its root and its descendants, children numbered above their
     // parent, so one descending pass per face, faces in parallel; then the
     // parents grouped by level, index order within a level.
-    std::vector<uint8_t> level((size_t)P, 0);
+    uvector<uint8_t> level((size_t)P, 0);
     std::vector<int32_t> face_top((size_t)nf, 0);
     parallel_for(nf, 16, [&](int64_t f) {
         const int32_t root = tree.face_root[(size_t)f];
@@ -473,7 +483,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     for (int32_t i = 0; i < P; i++)
         if (level[(size_t)i]) level_off[(size_t)level[(size_t)i] + 1]++;
     for (int32_t h = 0; h <= top; h++) level_off[(size_t)h + 1] += level_off[(size_t)h];
-    std::vector<int32_t> level_patch((size_t)level_off[(size_t)top + 1]);
+    uvector<int32_t> level_patch((size_t)level_off[(size_t)top + 1]);
     {
         std::vector<int32_t> at(level_off.begin(), level_off.end() - 1);
         for (int32_t i = 0; i < P; i++)
@@ -621,6 +631,9 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     const int64_t ntr = 0;
     b.ntransfers = ntr;
     b.ready = true;
+    ctx->bounced = true;
+    ctx->last_max_chop = d->max_chop;
+    ctx->last_min_chop = d->min_chop;
     return VRAD_OK;
 }
 

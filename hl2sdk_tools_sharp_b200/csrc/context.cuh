@@ -5,12 +5,14 @@
 
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "bounce.cuh"
 #include "direct.cuh"
 #include "final.cuh"
 #include "host_parallel.h"
+#include "patches.h"
 #include "scene.cuh"
 #include "staging.h"
 #include "supersample.cuh"
@@ -45,6 +47,16 @@ struct vrad_ctx {
     std::vector<int32_t> h_noff, h_nlist;
     int32_t nclusters = 0;
     vrad::BounceBuffers bounce;
+    // The uploaded world's patch forest, grown ahead on a host thread while
+    // the rest of the world upload runs, with the chop sizes of this
+    // context's last bounce upload; the next bounce upload takes it when
+    // its chop sizes match.  Only a context that has bounced grows one.
+    std::thread ahead_thread;
+    vrad::PatchForest ahead;
+    bool ahead_ok = false;
+    std::string ahead_why;
+    bool bounced = false;
+    float last_max_chop = 0.0f, last_min_chop = 0.0f;
     const vrad_mlp *bounce_model = nullptr;  // the warm start's network, or none
     vrad::SupersampleBuffers supersample;
     std::string supersample_why;     // why the world's samples cannot be supersampled
@@ -83,6 +95,11 @@ cudaError_t prioritise_uploads(vrad_ctx *ctx);
 // pinned host buffers stay.  A batch worker calls it after each map, so an
 // idle worker holds no device memory that another worker's map could use.
 cudaError_t release_tables(vrad_ctx *ctx);
+
+// Waits for the patch forest growing ahead, if one is.
+inline void join_ahead(vrad_ctx *ctx) {
+    if (ctx->ahead_thread.joinable()) ctx->ahead_thread.join();
+}
 
 // Waits for every kernel of this context (its stream, joined by the
 // callers' streams it ran on) and for no other context's: an upload that

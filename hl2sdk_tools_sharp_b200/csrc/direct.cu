@@ -206,7 +206,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     // four (the last group repeating its last sample as padding), each
     // cluster's run padded to whole warps with more padding lanes, so no
     // warp mixes two light lists.
-    std::vector<int32_t> slots;
+    vrad::uvector<int32_t> slots;
     slots.reserve((size_t)(w->nsamples + 4 * (int64_t)w->nfaces + 32 * (int64_t)w->nclusters));
     std::vector<std::vector<int32_t>> by_cluster((size_t)w->nclusters);
     for (int32_t f = 0; f < w->nfaces; f++)
@@ -285,6 +285,10 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     // new world drops the old bounce.
     ctx->bounce.release();
     clock.mark("bounce released");
+    // The forest grown ahead for the previous world reads the host copies.
+    vrad::join_ahead(ctx);
+    ctx->ahead = vrad::PatchForest();
+    ctx->ahead_ok = false;
     ctx->h_faces.assign(w->faces, w->faces + w->nfaces);
     ctx->h_samples.resize((size_t)w->nsamples);
     vrad::parallel_for(w->nsamples, 1 << 16, [&](int64_t k) { ctx->h_samples[(size_t)k] = w->samples[k]; });
@@ -293,6 +297,17 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     if (w->vertices && w->nvertices > 0) ctx->h_vertices.assign(w->vertices, w->vertices + 3 * w->nvertices);
     else ctx->h_vertices.clear();
     ctx->nclusters = w->nclusters;
+    if (ctx->bounced && !ctx->h_vertices.empty()) {
+        // PatchBuilder and PatchSubdivider need only the faces and their
+        // windings: grow the forest while the final-pass and supersampling
+        // tables are built (their parallel loops and the forest's share the
+        // host pool).
+        const float mx = ctx->last_max_chop, mn = ctx->last_min_chop;
+        ctx->ahead_thread = std::thread([ctx, mx, mn]() {
+            ctx->ahead_ok = ctx->ahead.grow(ctx->h_faces.data(), (int32_t)ctx->h_faces.size(), ctx->h_vertices.data(),
+                                            (int64_t)ctx->h_vertices.size() / 3, mx, mn, ctx->ahead_why);
+        });
+    }
     ctx->final_pass.release();
     vrad::dev_free(ctx->sample_light);
     ctx->sample_light = nullptr;

@@ -130,8 +130,15 @@ void parallel_for(int64_t n, int64_t grain, F &&body) {
     HostPool::get().run(nt - 1, job);
 }
 
+// Large host blocks (host_pool.cpp): at least `bytes`, 2 MiB aligned, kept
+// when freed and handed out again, so that their pages stay mapped.
+void *host_block_alloc(size_t bytes);
+void host_block_free(void *p);
+constexpr size_t kHostBlockMin = (size_t)1 << 20;
+
 // An allocator whose value-initialising construct() default-initialises
-// instead, so resize() of a trivial type leaves the memory untouched.
+// instead, so resize() of a trivial type leaves the memory untouched, and
+// whose blocks of 1 MiB and more come from the cache of host blocks.
 template <class T, class A = std::allocator<T>>
 struct DefaultInitAllocator : A {
     using traits = std::allocator_traits<A>;
@@ -140,6 +147,14 @@ struct DefaultInitAllocator : A {
         using other = DefaultInitAllocator<U, typename traits::template rebind_alloc<U>>;
     };
     using A::A;
+    T *allocate(size_t n) {
+        if (n * sizeof(T) >= kHostBlockMin) return static_cast<T *>(host_block_alloc(n * sizeof(T)));
+        return A::allocate(n);
+    }
+    void deallocate(T *p, size_t n) {
+        if (n * sizeof(T) >= kHostBlockMin) host_block_free(p);
+        else A::deallocate(p, n);
+    }
     template <class U>
     void construct(U *p) noexcept(std::is_nothrow_default_constructible<U>::value) {
         ::new (static_cast<void *>(p)) U;

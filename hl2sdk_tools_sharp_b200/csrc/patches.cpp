@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
@@ -185,22 +186,45 @@ bool prevent_subdivision(int32_t flags) {
 
 }  // namespace
 
-bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
-                      const float *reflectivity, float max_chop, float min_chop, PatchTree &out, PatchSink &sink,
-                      std::string &why) {
-    SetupClock clock("patch_tree");
+struct PatchForest::Impl {
+    const vrad_face *faces = nullptr;
+    int32_t nfaces = 0;
+    float max_chop = 0.0f, min_chop = 0.0f;
     std::vector<std::vector<float>> corners;
-    if (!corner_normals(faces, nfaces, vertices, nvertices, kSmoothing, corners)) {
+    std::vector<V3> centroid;
+    std::vector<Builder> subtree;
+};
+
+PatchForest::PatchForest() = default;
+PatchForest::~PatchForest() = default;
+PatchForest::PatchForest(PatchForest &&) noexcept = default;
+PatchForest &PatchForest::operator=(PatchForest &&) noexcept = default;
+
+bool PatchForest::grown() const { return impl_ != nullptr; }
+float PatchForest::max_chop() const { return impl_ ? impl_->max_chop : 0.0f; }
+float PatchForest::min_chop() const { return impl_ ? impl_->min_chop : 0.0f; }
+
+bool PatchForest::grow(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
+                       float max_chop, float min_chop, std::string &why) {
+    impl_.reset();
+    SetupClock clock("patch_tree");
+    std::unique_ptr<Impl> f(new Impl);
+    f->faces = faces;
+    f->nfaces = nfaces;
+    f->max_chop = max_chop;
+    f->min_chop = min_chop;
+    if (!corner_normals(faces, nfaces, vertices, nvertices, kSmoothing, f->corners)) {
         why = "a face's winding lies outside the vertex array";
         return false;
     }
     clock.mark("corner normals");
-    std::vector<V3> centroid((size_t)nfaces, V3{0.0f, 0.0f, 0.0f});
-    out.face_root.assign((size_t)nfaces, -1);
-    // MakePatchForFace, face by face: the roots, in face order.
-    std::vector<Builder> subtree;
-    for (int32_t f = 0; f < nfaces; f++) {
-        const vrad_face &fc = faces[f];
+    f->centroid.assign((size_t)nfaces, V3{0.0f, 0.0f, 0.0f});
+    // MakePatchForFace, face by face: the roots, in face order.  The
+    // reflectivity is filled in when the forest is numbered (every patch
+    // of a face carries the face's).
+    std::vector<Builder> &subtree = f->subtree;
+    for (int32_t fi = 0; fi < nfaces; fi++) {
+        const vrad_face &fc = faces[fi];
         if (fc.num_vertices < 3) {
             why = "a face has fewer than three vertices";
             return false;
@@ -220,13 +244,13 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
         p.lux_scale = (axis_length(fc.lightmap_vecs[0]) + axis_length(fc.lightmap_vecs[1])) / 2.0f;
         p.chop = max_chop;
         p.plane_dist = fc.dist;
-        p.face = f;
+        p.face = fi;
         // ResolveClusters: the cluster of the patch's origin, which lies on
         // the face, is the cluster the face's samples lie in.
         p.cluster = fc.cluster;
         p.sky = (fc.flags & VRAD_SURF_SKY) ? 1 : 0;
         const V3 c = center(w);
-        centroid[(size_t)f] = c;
+        f->centroid[(size_t)fi] = c;
         p.origin[0] = c.x, p.origin[1] = c.y, p.origin[2] = c.z;
         for (int a = 0; a < 3; a++) p.normal[a] = fc.normal[a];
         V3 mn, mx;
@@ -237,17 +261,12 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
         p.maxs[0] = p.face_maxs[0] = mx.x;
         p.maxs[1] = p.face_maxs[1] = mx.y;
         p.maxs[2] = p.face_maxs[2] = mx.z;
-        for (int a = 0; a < 3; a++) {
-            const float r = reflectivity[3 * (int64_t)f + a];
-            p.reflectivity[a] = r < kMaxReflectivity ? r : kMaxReflectivity;
-        }
-        out.face_root[(size_t)f] = (int32_t)subtree.size();
         Builder b;
         b.faces = faces;
         b.vertices = vertices;
         b.min_chop = min_chop;
-        b.corner_normals = &corners;
-        b.centroids = &centroid;
+        b.corner_normals = &f->corners;
+        b.centroids = &f->centroid;
         b.add_patch(p, w);
         subtree.push_back(std::move(b));
     }
@@ -272,6 +291,19 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
         if (!prevent_subdivision(faces[b.patches[0].face].flags)) b.subdivide(0);
     });
     clock.mark("subdivide");
+    impl_ = std::move(f);
+    return true;
+}
+
+bool PatchForest::merge(const float *reflectivity, PatchTree &out, PatchSink &sink, std::string &why) {
+    if (!impl_) {
+        why = "no patch forest grown";
+        return false;
+    }
+    SetupClock clock("patch_tree");
+    std::vector<Builder> &subtree = impl_->subtree;
+    const int32_t nfaces = impl_->nfaces;
+    const int32_t roots = (int32_t)subtree.size();
     // Global indices: the roots 0..roots-1 in face order, then each root's
     // descendants in creation order (the order SubdividePatch adds them);
     // the windings' points in the same order.
@@ -290,15 +322,22 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
         why = "patch tables";
         return false;
     }
+    out.face_root.assign((size_t)nfaces, -1);
     out.face_first.assign((size_t)nfaces, 0);
     out.face_end.assign((size_t)nfaces, 0);
-    // Each root's block of patches, renumbered, handed to the sink in
-    // parallel.
+    // Each root's block of patches, renumbered, given the face's
+    // reflectivity (PatchBuilder clamps it to MaxReflectivity) and handed
+    // to the sink, in parallel.
     parallel_for(roots, 8, [&](int64_t ii) {
         const int32_t i = (int32_t)ii;
         Builder &b = subtree[(size_t)i];
         auto global = [&](int32_t local) { return local < 0 ? -1 : (local == 0 ? i : base[(size_t)i] + local - 1); };
         const int64_t desc0 = root_pt[(size_t)roots] + desc_pt[(size_t)i] - b.wcount[0];
+        float refl[3];
+        for (int a = 0; a < 3; a++) {
+            const float r = reflectivity[3 * (int64_t)b.patches[0].face + a];
+            refl[a] = r < kMaxReflectivity ? r : kMaxReflectivity;
+        }
         for (size_t k = 0; k < b.patches.size(); k++) {
             vrad_patch p = b.patches[k];
             p.parent = global(p.parent);
@@ -306,6 +345,7 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
             p.child2 = global(p.child2);
             p.first_point = (int32_t)(k == 0 ? root_pt[(size_t)i] : desc0 + b.wfirst[k]);
             p.num_points = b.wcount[k];
+            for (int a = 0; a < 3; a++) p.reflectivity[a] = refl[a];
             sink.put(global((int32_t)k), p, &b.pts[(size_t)b.wfirst[k]].x);
         }
     });
@@ -318,9 +358,17 @@ bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *verti
     }
     out.npatches = total;
     out.npoints = npoints;
-    clock.mark("merge");
     out.roots = roots;
+    clock.mark("merge");
     return true;
+}
+
+bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
+                      const float *reflectivity, float max_chop, float min_chop, PatchTree &out, PatchSink &sink,
+                      std::string &why) {
+    PatchForest forest;
+    return forest.grow(faces, nfaces, vertices, nvertices, max_chop, min_chop, why) &&
+           forest.merge(reflectivity, out, sink, why);
 }
 
 }  // namespace vrad

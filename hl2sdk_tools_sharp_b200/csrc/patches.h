@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -48,6 +49,35 @@ struct PatchArrays : PatchSink {
     }
 };
 
+// The first half of the patch tree: every face's root and its subdivided
+// subtree (PatchBuilder.Build, PatchSubdivider.Subdivide), before the
+// patches are numbered and given their reflectivity.  It reads only the
+// faces, their windings and the chop sizes, which the world upload already
+// has, so a context can grow it ahead of the bounce upload.  The faces and
+// vertices must outlive the forest.
+class PatchForest {
+public:
+    PatchForest();
+    ~PatchForest();
+    PatchForest(PatchForest &&) noexcept;
+    PatchForest &operator=(PatchForest &&) noexcept;
+
+    bool grow(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices, float max_chop,
+              float min_chop, std::string &why);
+    // The patches numbered as the reference numbers them, each with its
+    // face's reflectivity (nfaces x 3, clamped to 0.99), handed to the sink.
+    bool merge(const float *reflectivity, PatchTree &out, PatchSink &sink, std::string &why);
+
+    bool grown() const;
+    float max_chop() const;
+    float min_chop() const;
+
+private:
+    struct Impl;
+    std::unique_ptr<Impl> impl_;
+};
+
+// grow, then merge.
 bool build_patch_tree(const vrad_face *faces, int32_t nfaces, const float *vertices, int64_t nvertices,
                       const float *reflectivity, float max_chop, float min_chop, PatchTree &out, PatchSink &sink,
                       std::string &why);

@@ -156,3 +156,32 @@ def test_sample_runs_in_any_face_order_light_the_same_lump():
             stats.append(st.bounce_stats().bounces)
     assert stats[0] == stats[1] and stats[0] > 1
     assert np.array_equal(lumps[0], lumps[1])
+
+
+def test_reupload_grows_the_patch_forest_ahead_and_keeps_the_lump():
+    """A context that has bounced grows the next world's patch forest while
+    the world uploads, with its last chop sizes; the bounce upload takes it
+    when the sizes match and grows its own when they do not.  Either way the
+    lump is a fresh context's, and a new reflectivity still applies."""
+    w = rg.generate(rg.config_3x3(seed=2))
+    inp = L.prepare(w)
+    off, lst = L.pvs_lists(w)
+    refl = L.face_reflectivity(w)
+    dim = (refl * np.float32(0.5)).astype(np.float32)
+
+    def fresh(r, max_chop):
+        st = L.LightingStage(w, inp)
+        st.upload_bounce(r, off, lst, max_chop=max_chop)
+        lump = st.light_pass()[0].copy()
+        st.close()
+        return lump
+
+    want = {(0, 4.0): fresh(refl, 4.0), (0, 8.0): fresh(refl, 8.0), (1, 4.0): fresh(dim, 4.0)}
+    assert not np.array_equal(want[(0, 4.0)], want[(0, 8.0)])
+    st = L.LightingStage(w, inp)
+    st.upload_bounce(refl, off, lst)
+    for which, chop in ((0, 4.0), (0, 8.0), (0, 8.0), (1, 4.0), (0, 4.0)):
+        st.upload_world(inp)
+        st.upload_bounce(dim if which else refl, off, lst, max_chop=chop)
+        assert np.array_equal(st.light_pass()[0], want[(which, chop)]), (which, chop)
+    st.close()
