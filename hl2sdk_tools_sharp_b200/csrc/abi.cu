@@ -97,6 +97,7 @@ int32_t upload(vrad_ctx *ctx, const vrad_triangle *tris, const vrad_kd_triangle 
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
     ctx->has_scene = false;
+    vrad::settle_direct(ctx);
     // The old scene's blocks go back to the device pool once no kernel of
     // this context reads them.
     e = vrad::quiesce(ctx);
@@ -186,6 +187,7 @@ cudaError_t prioritise_uploads(vrad_ctx *ctx) {
     cudaError_t e = cudaSetDevice(ctx->device);
     int least = 0, greatest = 0;
     if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    settle_direct(ctx);
     if (e == cudaSuccess) e = quiesce(ctx);
     if (e != cudaSuccess) return e;
     cudaStream_t up = nullptr, pass = nullptr;
@@ -204,10 +206,11 @@ cudaError_t prioritise_uploads(vrad_ctx *ctx) {
 
 cudaError_t release_tables(vrad_ctx *ctx) {
     std::lock_guard<std::mutex> g(ctx->mu);
+    join_ahead(ctx);
+    settle_direct(ctx);
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e == cudaSuccess) e = quiesce(ctx);
     if (e != cudaSuccess) return e;
-    join_ahead(ctx);
     ctx->ahead = PatchForest();
     ctx->ahead_ok = false;
     ctx->has_scene = false;
@@ -247,6 +250,9 @@ int32_t vrad_create(int32_t device, vrad_ctx **out) {
     e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->ahead_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ahead_start);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ahead_done);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->status, 4 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemsetAsync(ctx->status, 0, 4 * sizeof(uint32_t), ctx->stream);
     if (e == cudaSuccess) e = vrad::wait_stream(ctx->stream);
@@ -269,6 +275,7 @@ int32_t vrad_destroy(vrad_ctx *ctx) {
     {
         std::lock_guard<std::mutex> g(ctx->mu);
         vrad::join_ahead(ctx);
+        vrad::settle_direct(ctx);
         cudaSetDevice(ctx->device);
         // Kernels of this context may run on callers' streams too.
         cudaDeviceSynchronize();
@@ -284,6 +291,9 @@ int32_t vrad_destroy(vrad_ctx *ctx) {
         cudaFree(ctx->d_rays);
         cudaFree(ctx->d_out);
         if (ctx->join) cudaEventDestroy(ctx->join);
+        if (ctx->ahead_start) cudaEventDestroy(ctx->ahead_start);
+        if (ctx->ahead_done) cudaEventDestroy(ctx->ahead_done);
+        if (ctx->ahead_stream) cudaStreamDestroy(ctx->ahead_stream);
         if (ctx->pass_stream) cudaStreamDestroy(ctx->pass_stream);
         if (ctx->stream) cudaStreamDestroy(ctx->stream);
         vrad::dev_trim(ctx->device);

@@ -87,14 +87,16 @@ void light_map(vrad_ctx *ctx, vrad_batch_map &m, int block) {
         into = std::chrono::duration<double>(now - t).count();
         t = now;
     };
-    int32_t rc = vrad_scene_upload(ctx, m.triangles, m.ntriangles);
-    lap(m.scene_s);
-    if (rc == VRAD_OK) rc = vrad_world_upload(ctx, m.world);
-    if (rc == VRAD_OK) rc = vrad_set_extra_passes(ctx, m.extra_passes < 0 ? 4 : m.extra_passes);
+    // The launch shape and the supersampling passes first: the world upload
+    // queues the direct gather ahead with them.
+    int32_t rc = vrad_set_extra_passes(ctx, m.extra_passes < 0 ? 4 : m.extra_passes);
     if (rc == VRAD_OK && block) {
         std::lock_guard<std::mutex> g(ctx->mu);
         ctx->world.block = block;
     }
+    if (rc == VRAD_OK) rc = vrad_scene_upload(ctx, m.triangles, m.ntriangles);
+    lap(m.scene_s);
+    if (rc == VRAD_OK) rc = vrad_world_upload(ctx, m.world);
     lap(m.world_s);
     if (rc == VRAD_OK && m.bounce) rc = vrad_bounce_upload(ctx, m.bounce);
     lap(m.bounce_s);

@@ -321,8 +321,11 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     SetupClock clock("bounce_upload");
     cudaError_t e = cudaSetDevice(ctx->device);
     // The old bounce's blocks go back to the device pool: no kernel of
-    // this context, on any stream, may still read them.
-    if (e == cudaSuccess) e = vrad::quiesce(ctx);
+    // this context may still read them.  Light passes leave none running
+    // (one on a caller's stream joined the context's stream), and the
+    // direct gather queued ahead, which this upload overlaps, reads no
+    // bounce table.
+    if (e == cudaSuccess) e = vrad::wait_stream(ctx->stream);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
     BounceBuffers &b = ctx->bounce;
     b.release();
@@ -592,8 +595,12 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
         return vrad_cuda_fail(ctx, e, "patch radial tables");
     }
     clock.mark("patch radial tables");
-    // Size the candidate and transfer arrays by one build.
-    e = launch_transfers(b, ctx->scene.view(), ctx->status, s, true);
+    // Size the candidate and transfer arrays by one build.  The walk's
+    // overflow flag is a status word of its own (status[1]): a direct
+    // gather queued ahead may be running beside this upload.
+    uint32_t *walk_flag = ctx->status + 1;
+    if (e == cudaSuccess) e = cudaMemsetAsync(walk_flag, 0, sizeof(uint32_t), s);
+    if (e == cudaSuccess) e = launch_transfers(b, ctx->scene.view(), walk_flag, s, true);
     int64_t ncand = 0;
     if (e == cudaSuccess && R > 0) e = cudaMemcpyAsync(&ncand, b.cand_off + R, sizeof ncand, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = vrad::wait_stream(s);
@@ -609,7 +616,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     // of padding.
     const int64_t sell_cap = ncand + 32 * std::min<int64_t>(kMaxTransfersPerReceiver, ncand);
     if (e == cudaSuccess) e = dev_alloc(&b.sell, sizeof(int2) * (size_t)(sell_cap ? sell_cap : 1));
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&overflow, ctx->status, sizeof overflow, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&overflow, walk_flag, sizeof overflow, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = vrad::wait_stream(s);
     if (e != cudaSuccess) {
         ctx->stager.finish(ctx->stream);  // no copy in flight into a released block
@@ -617,7 +624,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
         return vrad_cuda_fail(ctx, e, "transfer sizing");
     }
     if (overflow) {
-        cudaMemsetAsync(ctx->status, 0, sizeof(uint32_t), ctx->stream);
+        cudaMemsetAsync(walk_flag, 0, sizeof(uint32_t), ctx->stream);
         ctx->stager.finish(ctx->stream);  // no copy in flight into a released block
         b.release();
         return vrad_fail(ctx, VRAD_ERR_CUDA, "stack overflow in the candidate walk (flags %u)", overflow);

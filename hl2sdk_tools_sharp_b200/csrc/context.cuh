@@ -57,6 +57,18 @@ struct vrad_ctx {
     std::string ahead_why;
     bool bounced = false;
     float last_max_chop = 0.0f, last_min_chop = 0.0f;
+    // The light pass's first step queued ahead: at the end of a world
+    // upload a host thread runs the direct gather with its supersampling
+    // passes into sample_light on ahead_stream (the pass stream when there
+    // is one), so that it overlaps the bounce upload's host work.  The next
+    // vrad_light_pass takes it; every other call that reads or changes what
+    // it depends on first waits for it and drops it.
+    std::thread direct_thread;
+    cudaStream_t ahead_stream = nullptr;
+    cudaEvent_t ahead_start = nullptr;  // recorded before and after the gather queued ahead
+    cudaEvent_t ahead_done = nullptr;
+    bool direct_ahead = false;
+    int32_t direct_ahead_rc = 0;
     const vrad_mlp *bounce_model = nullptr;  // the warm start's network, or none
     vrad::SupersampleBuffers supersample;
     std::string supersample_why;     // why the world's samples cannot be supersampled
@@ -96,16 +108,37 @@ cudaError_t prioritise_uploads(vrad_ctx *ctx);
 // idle worker holds no device memory that another worker's map could use.
 cudaError_t release_tables(vrad_ctx *ctx);
 
+// Queues the direct gather ahead (direct.cu); nothing when the world is
+// not ready for a light pass.
+void start_direct_ahead(vrad_ctx *ctx);
+
+// Waits for the direct gather queued ahead, if one was, and drops it.
+// Returns whether it completed without error: the caller may then take its
+// sample_light (after ahead_done) instead of gathering again.
+inline bool settle_direct(vrad_ctx *ctx) {
+    if (ctx->direct_thread.joinable()) ctx->direct_thread.join();
+    const bool ok = ctx->direct_ahead && ctx->direct_ahead_rc == 0;
+    ctx->direct_ahead = false;
+    return ok;
+}
+
 // Waits for the patch forest growing ahead, if one is.
 inline void join_ahead(vrad_ctx *ctx) {
     if (ctx->ahead_thread.joinable()) ctx->ahead_thread.join();
 }
 
-// Waits for every kernel of this context (its stream, joined by the
-// callers' streams it ran on) and for no other context's: an upload that
-// hands the old tables back to the device pool waits here, so contexts on
-// one device run their passes side by side.
-inline cudaError_t quiesce(vrad_ctx *ctx) { return vrad::wait_stream(ctx->stream); }
+// Waits for every kernel of this context (its streams, the first joined by
+// the callers' streams it ran on) and for no other context's: an upload
+// that hands the old tables back to the device pool waits here, so
+// contexts on one device run their passes side by side.  A direct gather
+// queued ahead must be settled first (settle_direct), so that its thread
+// queues nothing more.
+inline cudaError_t quiesce(vrad_ctx *ctx) {
+    cudaError_t e = vrad::wait_stream(ctx->stream);
+    if (e == cudaSuccess && ctx->ahead_stream) e = vrad::wait_stream(ctx->ahead_stream);
+    if (e == cudaSuccess && ctx->pass_stream) e = vrad::wait_stream(ctx->pass_stream);
+    return e;
+}
 }
 
 // Shared error reporting (abi.cu).

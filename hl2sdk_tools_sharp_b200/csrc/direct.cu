@@ -23,6 +23,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "context.cuh"
@@ -257,6 +258,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
 
     clock.mark("slots and lights");
     std::lock_guard<std::mutex> g(ctx->mu);
+    vrad::settle_direct(ctx);
     cudaError_t e = cudaSetDevice(ctx->device);
     // The old world's blocks go back to the device pool: no kernel of this
     // context, on any stream, may still read them.
@@ -353,6 +355,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
         return vrad_cuda_fail(ctx, e, "world upload");
     }
     wb.ready = true;
+    vrad::start_direct_ahead(ctx);
     return VRAD_OK;
 }
 
@@ -379,6 +382,27 @@ int32_t direct_on(vrad_ctx *ctx, float4 *d_out, cudaStream_t s) {
 }  // namespace
 
 namespace vrad {
+void start_direct_ahead(vrad_ctx *ctx) {
+    if (!ctx->has_scene || !ctx->world.ready || !ctx->final_pass.ready || !ctx->sample_light || !ctx->ahead_stream)
+        return;
+    const cudaStream_t s = ctx->pass_stream ? ctx->pass_stream : ctx->ahead_stream;
+    ctx->direct_ahead = true;
+    ctx->direct_ahead_rc = VRAD_ERR_CUDA;
+    ctx->direct_thread = std::thread([ctx, s]() {
+        // The thread sleeps in its waits: its core goes to the bounce
+        // upload's host work meanwhile.
+        set_sleeping_waits(true);
+        int32_t rc = cudaSetDevice(ctx->device) == cudaSuccess && cudaEventRecord(ctx->ahead_start, s) == cudaSuccess
+                         ? direct_on(ctx, ctx->sample_light, s)
+                         : VRAD_ERR_CUDA;
+        if (rc == VRAD_OK && cudaEventRecord(ctx->ahead_done, s) != cudaSuccess) rc = VRAD_ERR_CUDA;
+        ctx->direct_ahead_rc = rc;
+        set_sleeping_waits(false);
+    });
+}
+}  // namespace vrad
+
+namespace vrad {
 // The direct gather with its supersampling passes (the light pass's first step).
 int32_t direct_pass(vrad_ctx *ctx, float4 *d_out, cudaStream_t s) { return direct_on(ctx, d_out, s); }
 }  // namespace vrad
@@ -387,6 +411,7 @@ extern "C" int32_t vrad_direct_lighting_device(vrad_ctx *ctx, vrad_lighting_valu
     if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
     if (!d_out && ctx->world.view.nsamples) return vrad_fail(ctx, VRAD_ERR_ARG, "null output");
     std::lock_guard<std::mutex> g(ctx->mu);
+    vrad::settle_direct(ctx);
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
     const int32_t rc = direct_on(ctx, reinterpret_cast<float4 *>(d_out), (cudaStream_t)stream);
@@ -397,6 +422,7 @@ extern "C" int32_t vrad_direct_lighting_device(vrad_ctx *ctx, vrad_lighting_valu
 extern "C" int32_t vrad_direct_lighting(vrad_ctx *ctx, vrad_lighting_value *out, vrad_direct_stats *stats) {
     if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
     std::lock_guard<std::mutex> g(ctx->mu);
+    vrad::settle_direct(ctx);
     const int64_t n = ctx->world.view.nsamples;
     if (n && !out) return vrad_fail(ctx, VRAD_ERR_ARG, "null output");
     cudaError_t e = cudaSetDevice(ctx->device);
@@ -448,6 +474,7 @@ extern "C" int32_t vrad_direct_lighting(vrad_ctx *ctx, vrad_lighting_value *out,
 extern "C" int32_t vrad_direct_autotune(vrad_ctx *ctx, int32_t *chosen_block, float *times_ms) {
     if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
     std::lock_guard<std::mutex> g(ctx->mu);
+    vrad::settle_direct(ctx);
     if (!ctx->has_scene) return vrad_fail(ctx, VRAD_ERR_NO_SCENE, "no scene uploaded");
     if (!ctx->world.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no lighting world uploaded");
     cudaError_t e = cudaSetDevice(ctx->device);
@@ -488,6 +515,7 @@ extern "C" int32_t vrad_set_extra_passes(vrad_ctx *ctx, int32_t passes) {
     if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
     if (passes < 0) return vrad_fail(ctx, VRAD_ERR_ARG, "extra passes %d < 0", passes);
     std::lock_guard<std::mutex> g(ctx->mu);
+    vrad::settle_direct(ctx);
     ctx->supersample.extra_passes = passes;
     return VRAD_OK;
 }

@@ -593,14 +593,22 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
 
 namespace {
 
-int32_t pass_on(vrad_ctx *ctx, uint8_t *d_lighting, cudaStream_t s, cudaEvent_t mid, cudaEvent_t bounce_mark) {
+// ahead: the direct gather already ran (queued at the world upload), its
+// end marked by ctx->ahead_done.
+int32_t pass_on(vrad_ctx *ctx, uint8_t *d_lighting, cudaStream_t s, cudaEvent_t mid, cudaEvent_t bounce_mark,
+                bool ahead = false) {
     if (!ctx->has_scene) return vrad_fail(ctx, VRAD_ERR_NO_SCENE, "no scene uploaded");
     if (!ctx->world.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no lighting world uploaded");
     if (!ctx->final_pass.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without face windings");
     vrad::FinalBuffers &fb = ctx->final_pass;
-    const int32_t rc = vrad::direct_pass(ctx, ctx->sample_light, s);
-    if (rc != VRAD_OK) return rc;
     cudaError_t e = cudaSuccess;
+    if (ahead) {
+        e = cudaStreamWaitEvent(s, ctx->ahead_done, 0);
+        if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "joining the direct gather");
+    } else {
+        const int32_t rc = vrad::direct_pass(ctx, ctx->sample_light, s);
+        if (rc != VRAD_OK) return rc;
+    }
     if (e == cudaSuccess && mid) e = cudaEventRecord(mid, s);
     // The bounce (patch light, transfers, bounces), when one is uploaded.
     vrad::PatchRadialView prad{};
@@ -634,6 +642,7 @@ extern "C" int32_t vrad_light_pass_device(vrad_ctx *ctx, uint8_t *d_lighting, vo
     if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
     if (!d_lighting || ((uintptr_t)d_lighting & 3)) return vrad_fail(ctx, VRAD_ERR_ARG, "lighting buffer null or not 4-byte aligned");
     std::lock_guard<std::mutex> g(ctx->mu);
+    vrad::settle_direct(ctx);  // this entry point always gathers
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
     const int32_t rc = pass_on(ctx, d_lighting, (cudaStream_t)stream, nullptr, nullptr);
@@ -645,6 +654,8 @@ extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t cap
                                    vrad_pass_stats *stats) {
     if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
     std::lock_guard<std::mutex> g(ctx->mu);
+    // The direct gather the world upload queued ahead, when there is one.
+    const bool ahead = vrad::settle_direct(ctx);
     vrad::FinalBuffers &fb = ctx->final_pass;
     if (!fb.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without face windings");
     if (!lighting || capacity < fb.lighting_bytes)
@@ -660,7 +671,7 @@ extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t cap
     if (e == cudaSuccess) e = cudaEventCreate(&bm);
     if (e == cudaSuccess) e = cudaEventCreate(&b);
     if (e == cudaSuccess) e = cudaEventRecord(a, s);
-    int32_t rc = e == cudaSuccess ? pass_on(ctx, d_lighting, s, m, bm) : vrad_cuda_fail(ctx, e, "light pass set-up");
+    int32_t rc = e == cudaSuccess ? pass_on(ctx, d_lighting, s, m, bm, ahead) : vrad_cuda_fail(ctx, e, "light pass set-up");
     unsigned long long counts[2] = {0, 0};
     uint32_t overflow = 0;
     if (rc == VRAD_OK) {
@@ -686,7 +697,9 @@ extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t cap
             for (int32_t f = 0; f < fb.nfaces; f++) lightofs[f] = fb.lightofs[(size_t)f];
         if (stats) {
             float d_ms = 0.0f, f_ms = 0.0f;
-            cudaEventElapsedTime(&d_ms, a, m);
+            // The gather's own device time, also when it ran ahead.
+            if (ahead) cudaEventElapsedTime(&d_ms, ctx->ahead_start, ctx->ahead_done);
+            else cudaEventElapsedTime(&d_ms, a, m);
             cudaEventElapsedTime(&f_ms, bm, b);
             stats->samples = ctx->world.view.nsamples;
             stats->luxels = fb.view.ncells;

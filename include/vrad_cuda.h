@@ -276,7 +276,14 @@ int32_t vrad_lightmap_layout(const vrad_face *faces, int32_t nfaces, int32_t *li
 /* Uploads the lighting world to the context's device (kept until the next
  * upload or vrad_destroy).  The scene (vrad_scene_upload) is the shadow
  * casters.  VRAD_ERR_UNSUPPORTED for a surface light (type 0) or for a
- * group of four samples that spans two clusters. */
+ * group of four samples that spans two clusters.  With the scene and the
+ * face windings present, the upload also queues the next light pass's
+ * direct gather (with its supersampling passes) on the device from a host
+ * thread, so that it runs while the caller's bounce upload builds its
+ * tables; the next vrad_light_pass takes it.  Calls that change what the
+ * gather reads (vrad_scene_upload, vrad_world_upload,
+ * vrad_set_extra_passes) or that gather themselves wait for it and drop
+ * it. */
 int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *world);
 
 /* The direct gather of every sample, style 0, flat normals: out[i] is

@@ -185,3 +185,35 @@ def test_reupload_grows_the_patch_forest_ahead_and_keeps_the_lump():
         st.upload_bounce(dim if which else refl, off, lst, max_chop=chop)
         assert np.array_equal(st.light_pass()[0], want[(which, chop)]), (which, chop)
     st.close()
+
+
+def test_direct_gather_queued_at_the_world_upload_lights_the_same_lump():
+    """The world upload queues the direct gather ahead (it overlaps the
+    bounce upload); the next host-buffer light pass takes it.  The lump is
+    the one a pass that gathers itself writes, and a setting changed after
+    the upload (the supersampling passes) drops the queued gather."""
+    import torch
+    w = rg.generate(rg.config_3x3(seed=2))
+    inp = L.prepare(w)
+    off, lst = L.pvs_lists(w)
+    refl = L.face_reflectivity(w)
+    st = L.LightingStage(w, inp)
+    st.upload_bounce(refl, off, lst)
+    ahead, _, ps = st.light_pass()                   # takes the gather queued by the world upload
+    ahead = ahead.copy()
+    d = torch.empty(len(ahead), dtype=torch.uint8, device="cuda")
+    st.light_pass_device(d)                          # gathers itself
+    torch.cuda.synchronize()
+    assert np.array_equal(d.cpu().numpy(), ahead)
+    st.upload_world(inp)
+    st.set_extra_passes(0)                           # after the upload: the queued gather is dropped
+    st.upload_bounce(refl, off, lst)
+    noextra, _, ps0 = st.light_pass()
+    assert ps0.extra_passes_run == 0 and ps.extra_passes_run > 0
+    st.close()
+    st = L.LightingStage(w, inp)
+    st.set_extra_passes(0)
+    st.upload_world(inp)                             # queued with no extra passes
+    st.upload_bounce(refl, off, lst)
+    assert np.array_equal(st.light_pass()[0], noextra)
+    st.close()
