@@ -402,19 +402,10 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
         const vrad_face &fc = ctx->h_faces[(size_t)f];
         face_plane[(size_t)f] = make_float4(fc.normal[0], fc.normal[1], fc.normal[2], fc.dist);
     }
-    // Each face's sample run (the world upload checked that a face's
-    // samples are contiguous): its first sample and count.
-    const int64_t S = (int64_t)ctx->h_samples.size();
-    const vrad_sample *sm = ctx->h_samples.data();
-    uvector<float> sample_area((size_t)S);
-    parallel_for(S, 1 << 15, [&](int64_t k) {
-        sample_area[(size_t)k] = sm[k].area;
-        const int32_t f = sm[k].face;
-        if (k == 0 || sm[k - 1].face != f) face_samples[(size_t)f].x = (int32_t)k;
-        if (k + 1 == S || sm[k + 1].face != f) face_samples[(size_t)f].y = (int32_t)(k + 1);
-    });
-    for (int32_t f = 0; f < nf; f++)
-        if (face_samples[(size_t)f].y) face_samples[(size_t)f].y -= face_samples[(size_t)f].x;
+    // Each face's sample run (first sample, count) and the samples' areas,
+    // as the world upload recorded them.
+    face_samples = ctx->h_face_samples;
+    const uvector<float> &sample_area = ctx->h_sample_area;
     clock.mark("patch tables");
     // VisMatrix.ReceiverOrder: cluster by cluster, leaf patches in index
     // order (a stable counting sort on the leaves' clusters), and the

@@ -41,7 +41,8 @@ struct vrad_ctx {
     // Host copies of the uploaded world the bounce set-up reads.
     std::vector<vrad_face> h_faces;
     std::vector<float> h_vertices;
-    vrad::uvector<vrad_sample> h_samples;
+    vrad::uvector<float> h_sample_area;     // per sample
+    std::vector<int2> h_face_samples;       // per face: first sample, count
     // The smoothing neighbours (FaceNeighbours, threshold 0.7071067) of
     // h_faces: face f's are h_nlist[h_noff[f] .. h_noff[f + 1]).
     std::vector<int32_t> h_noff, h_nlist;

@@ -175,7 +175,11 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
         run_face.push_back(face);
         i = j;
     }
-    vrad::uvector<float4> pos((size_t)w->nsamples);
+    // One pass over the samples: positions (with the face), the areas and
+    // coords the supersampling rebuild is checked against, the areas the
+    // bounce's patch light reads.
+    vrad::uvector<float4> pos((size_t)w->nsamples), area_coord((size_t)w->nsamples);
+    vrad::uvector<float> area((size_t)w->nsamples);
     std::atomic<int64_t> mixed{INT64_MAX};
     vrad::parallel_for((int64_t)run_face.size(), 16, [&](int64_t r) {
         const int32_t face = run_face[(size_t)r];
@@ -194,6 +198,8 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
             int32_t f = face;
             memcpy(&p.w, &f, 4);
             pos[(size_t)s] = p;
+            area_coord[(size_t)s] = make_float4(sm.area, sm.coord[0], sm.coord[1], 0.0f);
+            area[(size_t)s] = sm.area;
         }
     });
     if (mixed.load() != INT64_MAX) {
@@ -207,24 +213,37 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     // four (the last group repeating its last sample as padding), each
     // cluster's run padded to whole warps with more padding lanes, so no
     // warp mixes two light lists.
-    vrad::uvector<int32_t> slots;
-    slots.reserve((size_t)(w->nsamples + 4 * (int64_t)w->nfaces + 32 * (int64_t)w->nclusters));
+    // Laid out face by face first (each face's first slot, each cluster's
+    // padding run), then written in parallel.
     std::vector<std::vector<int32_t>> by_cluster((size_t)w->nclusters);
     for (int32_t f = 0; f < w->nfaces; f++)
         if (fstart[(size_t)f] >= 0) by_cluster[(size_t)w->faces[f].cluster].push_back(f);
+    std::vector<int64_t> face_slot((size_t)w->nfaces, -1), pad_from((size_t)w->nclusters), pad_to((size_t)w->nclusters);
+    std::vector<int32_t> pad_sample((size_t)w->nclusters, -1);
+    int64_t nslots = 0;
     for (int32_t c = 0; c < w->nclusters; c++) {
         int32_t last = -1;
         for (int32_t f : by_cluster[(size_t)c]) {
-            const int64_t a = fstart[(size_t)f], b = fend[(size_t)f];
-            for (int64_t g = a; g < b; g += 4)
-                for (int l = 0; l < 4; l++) {
-                    const int64_t s = g + l;
-                    slots.push_back(s < b ? (int32_t)s : (int32_t)((b - 1) | 0x80000000LL));
-                }
-            last = (int32_t)(b - 1);
+            face_slot[(size_t)f] = nslots;
+            nslots += (fend[(size_t)f] - fstart[(size_t)f] + 3) / 4 * 4;
+            last = (int32_t)(fend[(size_t)f] - 1);
         }
-        while (last >= 0 && slots.size() % 32) slots.push_back((int32_t)(last | 0x80000000LL));
+        pad_from[(size_t)c] = nslots;
+        if (last >= 0) nslots = (nslots + 31) / 32 * 32;
+        pad_to[(size_t)c] = nslots;
+        pad_sample[(size_t)c] = last;
     }
+    vrad::uvector<int32_t> slots((size_t)nslots);
+    vrad::parallel_for(w->nfaces, 64, [&](int64_t f) {
+        if (face_slot[(size_t)f] < 0) return;
+        const int64_t a = fstart[(size_t)f], b = fend[(size_t)f];
+        int32_t *o = slots.data() + face_slot[(size_t)f];
+        for (int64_t s = a; s < (b - a + 3) / 4 * 4 + a; s++)
+            *o++ = s < b ? (int32_t)s : (int32_t)((b - 1) | 0x80000000LL);
+    });
+    for (int32_t c = 0; c < w->nclusters; c++)
+        for (int64_t k = pad_from[(size_t)c]; k < pad_to[(size_t)c]; k++)
+            slots[(size_t)k] = (int32_t)(pad_sample[(size_t)c] | 0x80000000LL);
     std::vector<float4> fnorm((size_t)w->nfaces);
     for (int32_t f = 0; f < w->nfaces; f++) {
         float4 v;
@@ -292,8 +311,12 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     ctx->ahead = vrad::PatchForest();
     ctx->ahead_ok = false;
     ctx->h_faces.assign(w->faces, w->faces + w->nfaces);
-    ctx->h_samples.resize((size_t)w->nsamples);
-    vrad::parallel_for(w->nsamples, 1 << 16, [&](int64_t k) { ctx->h_samples[(size_t)k] = w->samples[k]; });
+    ctx->h_sample_area.swap(area);
+    ctx->h_face_samples.assign((size_t)w->nfaces, make_int2(0, 0));
+    for (int32_t f = 0; f < w->nfaces; f++)
+        if (fstart[(size_t)f] >= 0)
+            ctx->h_face_samples[(size_t)f] =
+                make_int2((int32_t)fstart[(size_t)f], (int32_t)(fend[(size_t)f] - fstart[(size_t)f]));
     ctx->h_noff.clear();
     ctx->h_nlist.clear();
     if (w->vertices && w->nvertices > 0) ctx->h_vertices.assign(w->vertices, w->vertices + 3 * w->nvertices);
@@ -327,7 +350,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
         clock.mark("final pass tables");
         ctx->final_pass.view.sample_pos = wb.sample_pos;
         bool have = false;
-        e = vrad::build_supersample(ctx->supersample, ctx->h_faces, ctx->h_vertices, ctx->h_samples, ctx->final_pass,
+        e = vrad::build_supersample(ctx->supersample, ctx->h_faces, ctx->h_vertices, area_coord, ctx->final_pass,
                                     w->nclusters, ctx->stager, ctx->stream, have, why);
         if (e != cudaSuccess) {
             ctx->stager.finish(ctx->stream);  // no copy in flight into a released block

@@ -249,17 +249,11 @@ unsigned blocks_of(int64_t n, int per) { return (unsigned)((n + per - 1) / per);
 }  // namespace
 
 cudaError_t device_windings(SupersampleBuffers &ss, const RowStrips &rs, const FinalView &fv,
-                            const uvector<vrad_sample> &samples, Stager &stager, cudaStream_t stream, bool &match,
+                            const uvector<float4> &check, Stager &stager, cudaStream_t stream, bool &match,
                             std::string &why) {
     match = false;
     const int32_t nrows = (int32_t)rs.face.size();
-    const int64_t S = (int64_t)samples.size();
-    // The area and coord of each given sample, for the check.
-    uvector<float4> check((size_t)S);
-    parallel_for(S, 1 << 15, [&](int64_t i) {
-        const vrad_sample &sm = samples[(size_t)i];
-        check[(size_t)i] = make_float4(sm.area, sm.coord[0], sm.coord[1], 0.0f);
-    });
+    const int64_t S = (int64_t)check.size();
     int32_t *d_face = nullptr, *d_t = nullptr, *d_ns = nullptr, *d_np = nullptr;
     int64_t *d_first = nullptr, *d_soff = nullptr, *d_poff = nullptr;
     float *d_xy = nullptr;  // (x, y) pairs
