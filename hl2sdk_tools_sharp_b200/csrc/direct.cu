@@ -340,7 +340,8 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     if (w->vertices && w->nvertices > 0) {
         std::string why;
         e = vrad::build_final(ctx->final_pass, w->faces, w->nfaces, w->samples, w->nsamples, w->vertices,
-                              w->nvertices, ctx->h_noff, ctx->h_nlist, ctx->stager, ctx->stream, why);
+                              w->nvertices, ctx->h_noff, ctx->h_nlist, ctx->stager, ctx->stream, why, fstart.data(),
+                              fend.data());
         if (e != cudaSuccess) {
             ctx->stager.finish(ctx->stream);  // no copy in flight into a released block
         wb.release();

@@ -486,7 +486,8 @@ cudaError_t neighbour_candidates(FinalBuffers &fb, int32_t nfaces, const std::ve
 // Host-side set-up of the final pass from the uploaded world.
 cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces, const vrad_sample *samples,
                         int64_t nsamples, const float *vertices, int64_t nvertices, std::vector<int32_t> &noff,
-                        std::vector<int32_t> &nlist, Stager &stager, cudaStream_t stream, std::string &why) {
+                        std::vector<int32_t> &nlist, Stager &stager, cudaStream_t stream, std::string &why,
+                        const int64_t *run_first, const int64_t *run_end) {
     fb.release();
     SetupClock clock("final_tables");
     std::vector<FaceFrameOut> fr((size_t)nfaces);
@@ -505,11 +506,19 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
     // Each face's sample run [sfirst, send) (the world upload checked
     // that a face's samples are contiguous; runs need not be in face order).
     std::vector<int64_t> sfirst((size_t)nfaces, 0), send((size_t)nfaces, 0), scount((size_t)nfaces, 0);
-    parallel_for(nsamples, 1 << 16, [&](int64_t k) {
-        const int32_t f = samples[k].face;
-        if (k == 0 || samples[k - 1].face != f) sfirst[(size_t)f] = k;
-        if (k + 1 == nsamples || samples[k + 1].face != f) send[(size_t)f] = k + 1;
-    });
+    if (run_first && run_end) {
+        for (int32_t f = 0; f < nfaces; f++)
+            if (run_first[f] >= 0) {
+                sfirst[(size_t)f] = run_first[f];
+                send[(size_t)f] = run_end[f];
+            }
+    } else {
+        parallel_for(nsamples, 1 << 16, [&](int64_t k) {
+            const int32_t f = samples[k].face;
+            if (k == 0 || samples[k - 1].face != f) sfirst[(size_t)f] = k;
+            if (k + 1 == nsamples || samples[k + 1].face != f) send[(size_t)f] = k + 1;
+        });
+    }
     for (int32_t f = 0; f < nfaces; f++) scount[(size_t)f] = send[(size_t)f] - sfirst[(size_t)f];
     // Frames, cells, own-sample cell table.
     std::vector<float4> frames((size_t)nfaces * 5);

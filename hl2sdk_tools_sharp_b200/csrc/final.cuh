@@ -60,9 +60,13 @@ struct FinalBuffers {
     void release();
 };
 
+// run_first / run_end (nullable, per face): each face's sample run as the
+// caller already found it (-1 for a face without samples); otherwise the
+// runs are found here.
 cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces, const vrad_sample *samples,
                         int64_t nsamples, const float *vertices, int64_t nvertices, std::vector<int32_t> &noff,
-                        std::vector<int32_t> &nlist, Stager &stager, cudaStream_t stream, std::string &why);
+                        std::vector<int32_t> &nlist, Stager &stager, cudaStream_t stream, std::string &why,
+                        const int64_t *run_first = nullptr, const int64_t *run_end = nullptr);
 
 // The bounced light's radial grid (FinalLightFace.BuildPatchRadial): per
 // face, the leaf patches of the face and of its smoothing neighbours whose
