@@ -286,6 +286,7 @@ int32_t vrad_destroy(vrad_ctx *ctx) {
         ctx->bounce.free_pinned();
         ctx->supersample.release();
         ctx->supersample.free_pinned();
+        ctx->shelf.release();
         vrad::dev_free(ctx->sample_light);
         cudaFree(ctx->status);
         cudaFree(ctx->d_rays);

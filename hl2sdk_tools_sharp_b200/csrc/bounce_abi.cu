@@ -333,19 +333,29 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     // The patch tree, its patches written straight into the device's SoA
     // rows (and each leaf's cluster, for the receiver order) as the merge
     // numbers them.
+    // The rows go into the context's pinned shelf, from which each reaches
+    // the device by one DMA.
     struct SoaRows : PatchSink {
         int32_t C = 0;
-        uvector<float4> origin, normal, mins, maxs, refl, points;
-        uvector<int4> tr;
-        uvector<int2> wind;
+        PinnedShelf *shelf = nullptr;
+        int32_t n = 0;
+        int64_t npoints = 0;
+        float4 *origin = nullptr, *normal = nullptr, *mins = nullptr, *maxs = nullptr, *refl = nullptr,
+               *points = nullptr;
+        int4 *tr = nullptr;
+        int2 *wind = nullptr;
         uvector<int32_t> leaf_cluster;
         std::atomic<int32_t> bad{INT32_MAX};
-        bool prepare(int32_t n, int64_t npoints) override {
-            for (uvector<float4> *v : {&origin, &normal, &mins, &maxs, &refl}) v->resize((size_t)n);
-            tr.resize((size_t)n);
-            wind.resize((size_t)n);
+        bool prepare(int32_t np, int64_t npts) override {
+            n = np;
+            npoints = npts;
+            float4 **rows[] = {&origin, &normal, &mins, &maxs, &refl};
+            for (int k = 0; k < 5; k++)
+                if (shelf->get(k, (size_t)n, rows[k]) != cudaSuccess) return false;
+            if (shelf->get(5, (size_t)npoints, &points) != cudaSuccess || shelf->get(6, (size_t)n, &tr) != cudaSuccess ||
+                shelf->get(7, (size_t)n, &wind) != cudaSuccess)
+                return false;
             leaf_cluster.resize((size_t)n);
-            points.resize((size_t)npoints);
             return true;
         }
         void put(int32_t i, const vrad_patch &p, const float *xyz) override {
@@ -369,6 +379,7 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     PatchTree tree;
     SoaRows rows;
     rows.C = C;
+    rows.shelf = &ctx->shelf;
     std::string why;
     const int64_t nvert = (int64_t)ctx->h_vertices.size() / 3;
     // The forest the world upload grew ahead, when its chop sizes are this
@@ -388,11 +399,18 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     clock.mark("patch tree");
     if (rows.bad.load() != INT32_MAX)
         return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "patch %d lies outside every cluster", rows.bad.load());
-    const uvector<float4> &origin = rows.origin, &normal = rows.normal, &mins = rows.mins, &maxs = rows.maxs,
-                          &refl = rows.refl, &points = rows.points;
-    const uvector<int4> &tr = rows.tr;
-    const uvector<int2> &wind = rows.wind;
+    const int4 *tr = rows.tr;
     const uvector<int32_t> &leaf_cluster = rows.leaf_cluster;
+    // The rows' DMAs start now and run under the host work that follows.
+    const cudaStream_t rs = ctx->stream;
+    cudaError_t e_rows = dma_table(&b.origin, rows.origin, (size_t)P, rs);
+    if (e_rows == cudaSuccess) e_rows = dma_table(&b.normal, rows.normal, (size_t)P, rs);
+    if (e_rows == cudaSuccess) e_rows = dma_table(&b.mins, rows.mins, (size_t)P, rs);
+    if (e_rows == cudaSuccess) e_rows = dma_table(&b.maxs, rows.maxs, (size_t)P, rs);
+    if (e_rows == cudaSuccess) e_rows = dma_table(&b.refl, rows.refl, (size_t)P, rs);
+    if (e_rows == cudaSuccess) e_rows = dma_table(&b.tree, rows.tr, (size_t)P, rs);
+    if (e_rows == cudaSuccess) e_rows = dma_table(&b.wind, rows.wind, (size_t)P, rs);
+    if (e_rows == cudaSuccess) e_rows = dma_table(&b.points, rows.points, (size_t)rows.npoints, rs);
     // Per face.
     std::vector<int4> face_range((size_t)nf);
     std::vector<int2> face_samples((size_t)nf, make_int2(0, 0));
@@ -472,7 +490,11 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     });
     int32_t top = 0;
     for (int32_t f = 0; f < nf; f++) top = std::max(top, face_top[(size_t)f]);
-    if (top > 255) return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "a patch's subtree is deeper than 255 levels");
+    if (top > 255) {
+        vrad::wait_stream(rs);  // no DMA still reads the shelf or writes a released block
+        b.release();
+        return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "a patch's subtree is deeper than 255 levels");
+    }
     std::vector<int32_t> level_off((size_t)top + 2, 0);
     for (int32_t i = 0; i < P; i++)
         if (level[(size_t)i]) level_off[(size_t)level[(size_t)i] + 1]++;
@@ -498,20 +520,17 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     clock.mark("receivers and rows");
     // The final pass's patch tables over the smoothing neighbours (the
     // world upload's).
-    if (ctx->h_noff.size() != (size_t)nf + 1) return vrad_fail(ctx, VRAD_ERR_ARG, "the world has no smoothing neighbours");
+    if (ctx->h_noff.size() != (size_t)nf + 1) {
+        vrad::wait_stream(rs);  // no DMA still reads the shelf or writes a released block
+        b.release();
+        return vrad_fail(ctx, VRAD_ERR_ARG, "the world has no smoothing neighbours");
+    }
     const std::vector<int32_t> &noff = ctx->h_noff, &nlist = ctx->h_nlist;
     clock.mark("neighbours");
 
     const int32_t R = (int32_t)recv.size();
     const int64_t ncells = ctx->final_pass.view.ncells;
-    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.origin, origin);
-    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.normal, normal);
-    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.mins, mins);
-    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.maxs, maxs);
-    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.refl, refl);
-    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.tree, tr);
-    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.wind, wind);
-    if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.points, points);
+    if (e == cudaSuccess) e = e_rows;
     if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.face_range, face_range);
     if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.face_samples, face_samples);
     if (e == cudaSuccess) e = stage_table(ctx->stager, ctx->stream, &b.face_plane, face_plane);

@@ -74,6 +74,7 @@ struct vrad_ctx {
     vrad::SupersampleBuffers supersample;
     std::string supersample_why;     // why the world's samples cannot be supersampled
     vrad::Stager stager;             // pinned staging of the uploads' tables
+    vrad::PinnedShelf shelf;         // pinned tables the bounce upload writes in place
     std::string last_error;
     std::string identity;
 };

@@ -10,6 +10,37 @@
 
 namespace vrad {
 
+PinnedShelf::~PinnedShelf() { release(); }
+
+cudaError_t PinnedShelf::get(int slot, size_t bytes, void **out) {
+    *out = nullptr;
+    if (slot < 0 || slot >= kSlots) return cudaErrorInvalidValue;
+    if (cap_[slot] < bytes) {
+        if (ptr_[slot]) retired_.push_back(ptr_[slot]);
+        ptr_[slot] = nullptr;
+        cap_[slot] = 0;
+        const size_t want = bytes + bytes / 4;
+        const cudaError_t e = cudaHostAlloc(&ptr_[slot], want, cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            ptr_[slot] = nullptr;
+            return e;
+        }
+        cap_[slot] = want;
+    }
+    *out = ptr_[slot];
+    return cudaSuccess;
+}
+
+void PinnedShelf::release() {
+    for (int k = 0; k < kSlots; k++) {
+        if (ptr_[k]) cudaFreeHost(ptr_[k]);
+        ptr_[k] = nullptr;
+        cap_[k] = 0;
+    }
+    for (void *p : retired_) cudaFreeHost(p);
+    retired_.clear();
+}
+
 Stager::~Stager() { release(); }
 
 void Stager::release() {
