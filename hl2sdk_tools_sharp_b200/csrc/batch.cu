@@ -316,7 +316,11 @@ extern "C" int32_t vrad_batch_autotune(vrad_batch *b, vrad_batch_map *maps, int3
         return vrad_fail(nullptr, rc, "batch autotune, map %d: %s", big, msg);
     }
     b->block = block;
-    // The maps in flight.
+    // The maps in flight.  One untimed run on every worker first: the
+    // device pool and the pinned tables then hold what the largest count
+    // needs, so no count is timed with its first allocations.
+    rc = run_locked(b, maps, nmaps, b->created, nullptr);
+    if (rc != VRAD_OK) return rc;
     double best = 1e300;
     int best_w = b->created;
     for (int w = 1; w <= b->created; w++) {

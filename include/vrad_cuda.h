@@ -110,8 +110,9 @@ int32_t vrad_create(int32_t device, vrad_ctx **out);
 int32_t vrad_destroy(vrad_ctx *ctx);
 
 /* Builds the scene on the device: intersection form (Correct-mode
- * normalise, bit-identical to KdTreeBuilder.ToIntersectionFormat), padded
- * boxes and a BVH built on the GPU.  Replaces ShadowCasterSet.BuildTracerAsync
+ * normalise, bit-identical to KdTreeBuilder.ToIntersectionFormat) and
+ * padded boxes on the GPU, the BVH's topology by the surface area
+ * heuristic on the host.  Replaces ShadowCasterSet.BuildTracerAsync
  * (src/SourceSharp.MapTools/Rad/ShadowCasterSet.cs) for the device tracer. */
 int32_t vrad_scene_upload(vrad_ctx *ctx, const vrad_triangle *tris, int32_t n);
 
@@ -618,8 +619,9 @@ int32_t vrad_batch_run(vrad_batch *batch, vrad_batch_map *maps, int32_t nmaps, i
 
 /* The batch's autotuner.  It first uploads the largest map on one context
  * and picks the gather's launch shape there (vrad_direct_autotune).  It then
- * lights all of `maps` once per worker count 1..created and keeps the fastest
- * count.  seconds (nullable, `created` entries) receives each count's wall
+ * lights all of `maps` once untimed on every worker (so that no count is
+ * timed with its first allocations), then once per worker count
+ * 1..created, and keeps the fastest count.  seconds (nullable, `created` entries) receives each count's wall
  * time.  The maps' outputs hold the last sweep's results. */
 int32_t vrad_batch_autotune(vrad_batch *batch, vrad_batch_map *maps, int32_t nmaps, int32_t *chosen_workers,
                             int32_t *chosen_block, double *seconds);
