@@ -178,7 +178,14 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     // One pass over the samples: positions (with the face), the areas and
     // coords the supersampling rebuild is checked against, the areas the
     // bounce's patch light reads.
-    vrad::uvector<float4> pos((size_t)w->nsamples), area_coord((size_t)w->nsamples);
+    // Positions and the check table go straight into the context's pinned
+    // shelf, from which one DMA each sends them (the shelf is the
+    // context's: the lock is taken here).
+    std::unique_lock<std::mutex> g(ctx->mu);
+    float4 *pos = nullptr, *area_coord = nullptr;
+    if (ctx->shelf.get(8, (size_t)w->nsamples, &pos) != cudaSuccess ||
+        ctx->shelf.get(9, (size_t)w->nsamples, &area_coord) != cudaSuccess)
+        return vrad_fail(ctx, VRAD_ERR_OOM, "pinned sample tables");
     vrad::uvector<float> area((size_t)w->nsamples);
     std::atomic<int64_t> mixed{INT64_MAX};
     vrad::parallel_for((int64_t)run_face.size(), 16, [&](int64_t r) {
@@ -276,7 +283,6 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
         jit[(size_t)d] = make_float4(w->sun_jitter[3 * d], w->sun_jitter[3 * d + 1], w->sun_jitter[3 * d + 2], 0.0f);
 
     clock.mark("slots and lights");
-    std::lock_guard<std::mutex> g(ctx->mu);
     vrad::settle_direct(ctx);
     cudaError_t e = cudaSetDevice(ctx->device);
     // The old world's blocks go back to the device pool: no kernel of this
@@ -285,7 +291,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     vrad::WorldBuffers &wb = ctx->world;
     wb.release();
     if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.slots, slots);
-    if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.sample_pos, pos);
+    if (e == cudaSuccess) e = vrad::dma_table(&wb.sample_pos, pos, (size_t)w->nsamples, ctx->stream);
     if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.face_normal, fnorm);
     if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.lights, lights);
     if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.cl_off, cl_off);
@@ -351,7 +357,8 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
         clock.mark("final pass tables");
         ctx->final_pass.view.sample_pos = wb.sample_pos;
         bool have = false;
-        e = vrad::build_supersample(ctx->supersample, ctx->h_faces, ctx->h_vertices, area_coord, ctx->final_pass,
+        e = vrad::build_supersample(ctx->supersample, ctx->h_faces, ctx->h_vertices, area_coord, w->nsamples,
+                                    ctx->final_pass,
                                     w->nclusters, ctx->stager, ctx->stream, have, why);
         if (e != cudaSuccess) {
             ctx->stager.finish(ctx->stream);  // no copy in flight into a released block

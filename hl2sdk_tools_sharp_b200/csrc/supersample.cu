@@ -331,7 +331,7 @@ void SupersampleBuffers::free_pinned() {
 }
 
 cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_face> &faces,
-                              const std::vector<float> &vertices, const uvector<float4> &area_coord,
+                              const std::vector<float> &vertices, const float4 *area_coord, int64_t nsamples,
                               const FinalBuffers &fb, int32_t nclusters, Stager &stager, cudaStream_t stream,
                               bool &have, std::string &why) {
     ss.release();
@@ -344,14 +344,14 @@ cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_fac
         return cudaSuccess;
     clock.mark("row strips");
     bool match = false;
-    cudaError_t e = device_windings(ss, rs, fb.view, area_coord, stager, stream, match, why);
+    cudaError_t e = device_windings(ss, rs, fb.view, area_coord, nsamples, stager, stream, match, why);
     if (e != cudaSuccess || !match) {
         ss.release();
         if (e != cudaSuccess) why = "supersampling windings";
         return e;
     }
     clock.mark("windings");
-    const size_t S = area_coord.size();
+    const size_t S = (size_t)nsamples;
     const size_t S1 = S ? S : 1;
     const size_t groups = 5 * S1 + 16 * (size_t)(nclusters + 1);
     e = dev_alloc(&ss.intensity, sizeof(float) * S1);

@@ -66,9 +66,9 @@ struct SupersampleBuffers {
 // and false returned when the samples are not the builder's own (their
 // windings cannot be known).
 // area_coord: each sample's area and coord (x, y, z), which the rebuilt
-// samples must match.
+// samples must match (pinned host memory, nsamples entries).
 cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_face> &faces,
-                              const std::vector<float> &vertices, const uvector<float4> &area_coord,
+                              const std::vector<float> &vertices, const float4 *area_coord, int64_t nsamples,
                               const FinalBuffers &fb, int32_t nclusters, Stager &stager, cudaStream_t stream,
                               bool &have, std::string &why);
 
@@ -77,7 +77,7 @@ cudaError_t build_supersample(SupersampleBuffers &ss, const std::vector<vrad_fac
 // ss.wind, ss.points, ss.cell and ss.origin_st; match = the world's
 // samples are the builder's own (else `why`).  Synchronises `stream`.
 cudaError_t device_windings(SupersampleBuffers &ss, const RowStrips &rs, const FinalView &fv,
-                            const uvector<float4> &area_coord, Stager &stager, cudaStream_t stream, bool &match,
+                            const float4 *check, int64_t nsamples, Stager &stager, cudaStream_t stream, bool &match,
                             std::string &why);
 
 // The supersampling passes over `light` (the direct gather's output, one

@@ -249,11 +249,11 @@ unsigned blocks_of(int64_t n, int per) { return (unsigned)((n + per - 1) / per);
 }  // namespace
 
 cudaError_t device_windings(SupersampleBuffers &ss, const RowStrips &rs, const FinalView &fv,
-                            const uvector<float4> &check, Stager &stager, cudaStream_t stream, bool &match,
+                            const float4 *check, int64_t nsamples, Stager &stager, cudaStream_t stream, bool &match,
                             std::string &why) {
     match = false;
     const int32_t nrows = (int32_t)rs.face.size();
-    const int64_t S = (int64_t)check.size();
+    const int64_t S = nsamples;
     int32_t *d_face = nullptr, *d_t = nullptr, *d_ns = nullptr, *d_np = nullptr;
     int64_t *d_first = nullptr, *d_soff = nullptr, *d_poff = nullptr;
     float *d_xy = nullptr;  // (x, y) pairs
@@ -270,7 +270,7 @@ cudaError_t device_windings(SupersampleBuffers &ss, const RowStrips &rs, const F
     if (e == cudaSuccess) e = stage_table(stager, stream, &d_first, rs.first);
     if (e == cudaSuccess) e = stage_table(stager, stream, &d_xy, rs.xy);
     if (e == cudaSuccess) e = stage_table(stager, stream, &d_apl, rs.apl);
-    if (e == cudaSuccess) e = stage_table(stager, stream, &d_check, check);
+    if (e == cudaSuccess) e = dma_table(&d_check, check, (size_t)S, stream);
     if (e == cudaSuccess) e = dev_alloc(&d_ns, sizeof(int32_t) * R1);
     if (e == cudaSuccess) e = dev_alloc(&d_np, sizeof(int32_t) * R1);
     if (e == cudaSuccess) e = dev_alloc(&d_soff, sizeof(int64_t) * (R1 + 1));
