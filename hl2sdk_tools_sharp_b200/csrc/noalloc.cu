@@ -2,10 +2,9 @@
 //
 // vrad_trace_visibility stages the caller's rays and hit bits through device
 // buffers it grows with cudaMalloc.  Some callers cannot have that happen in
-// the middle of a run: a host that records its work into a CUDA graph (an
-// allocation's implicit synchronisation is illegal while a stream is being
-// captured), or a process that reserves all of its device memory up front
-// and lets nothing else allocate.  This entry point stages through one fixed
+// the middle of a run: a process that reserves all of its device memory up
+// front and lets nothing else allocate, or a host that must not stall on
+// the device-wide synchronisation that freeing device memory can bring.  This entry point stages through one fixed
 // array instead, declared below with a stated maximum, so its calls make no
 // cudaMalloc, cudaFree or other allocating call.
 //

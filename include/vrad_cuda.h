@@ -528,9 +528,9 @@ int32_t vrad_bounce_features_device(vrad_ctx *ctx, uint16_t *x, float *target, i
 #define VRAD_STATIC_MAX_RAYS 65536
 
 /* vrad_trace_visibility for callers that must not allocate device memory
- * during a run: hosts recording work into a CUDA graph, where an
- * allocation's implicit synchronisation is not allowed, or processes that
- * reserve all their device memory at start-up.  No counterpart in the
+ * during a run: processes that reserve all their device memory at
+ * start-up, or hosts that must not stall on the device-wide synchronisation
+ * that freeing device memory can bring.  No counterpart in the
  * reference.  Same arguments, answers and errors as vrad_trace_visibility,
  * but rays and bits are staged through one fixed array inside the library
  * (about 1.8 MB, held on every GPU that loads it until the process exits)

@@ -1,8 +1,9 @@
 """vrad_trace_visibility_static: the visibility trace that allocates nothing.
 
-It serves callers that must not allocate device memory during a run (hosts
-recording into a CUDA graph, processes that reserve all device memory at
-start-up), staging rays and bits through a fixed array inside the library.
+It serves callers that must not allocate device memory during a run
+(processes that reserve all device memory at start-up, hosts that must not
+stall on the synchronisation freeing memory can bring), staging rays and
+bits through a fixed array inside the library.
 Its answers must be exactly those of vrad_trace_visibility, on two calls in
 a row (the array keeps the previous call's contents), and a batch above its
 stated maximum must be refused.  This file is collected last on purpose.
