@@ -256,6 +256,12 @@ int32_t vrad_create(int32_t device, vrad_ctx **out) {
     if (e == cudaSuccess) e = cudaMalloc(&ctx->status, 4 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemsetAsync(ctx->status, 0, 4 * sizeof(uint32_t), ctx->stream);
     if (e == cudaSuccess) e = vrad::wait_stream(ctx->stream);
+    if (e == cudaSuccess) {
+        // Places vrad_trace_visibility_static's fixed array and kernels on
+        // the device now, at set-up.  A failure here is not the context's:
+        // that entry point repeats the look-up and reports it.
+        if (vrad::prepare_static_trace(device) != cudaSuccess) (void)cudaGetLastError();
+    }
     if (e != cudaSuccess) {
         int32_t rc = cuda_fail(nullptr, e, "context setup");
         vrad_destroy(ctx);

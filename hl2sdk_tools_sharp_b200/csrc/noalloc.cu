@@ -9,10 +9,19 @@
 // cudaMalloc, cudaFree or other allocating call.
 //
 // The array is a file-scope __device__ variable: every GPU that loads the
-// library holds it (a little under 1.9 MB) until the process exits.  Host
-// code cannot use its name as a device address; its address on each device
-// is looked up once, with that device current, by cudaGetSymbolAddress, and
-// that pointer is what the kernel is given.
+// library holds it (sizeof(vrad_ray) x VRAD_STATIC_MAX_RAYS for the rays,
+// 8 KiB for the bits and 256 B for a status word: 1,843,456 bytes) until
+// the process exits.  Host code cannot use its name as a device address;
+// its address on each device is looked up by cudaGetSymbolAddress, with
+// that device current, and that pointer is what the kernel is given.
+//
+// With lazy module loading (the CUDA 12 default) the array and the trace
+// kernels' code are placed on a device only when first used, and placing
+// them takes device memory.  vrad_create therefore calls
+// prepare_static_trace for its device, so the look-up and the loads happen
+// at set-up and no later call of the entry point makes them.  The cached
+// address belongs to the device's primary context: the library does not
+// survive a cudaDeviceReset (no call of it may follow one).
 
 #include <cuda_runtime.h>
 
@@ -30,6 +39,7 @@ constexpr size_t kStatusOffset = kRayBytes + kBitBytes;
 constexpr size_t kScratchBytes = kStatusOffset + 256;
 
 static_assert(kRayBytes % 256 == 0, "bits must start 256-byte aligned");
+static_assert(kScratchBytes == 1843456, "the size the header and the comment above state");
 
 __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
@@ -55,6 +65,13 @@ cudaError_t scratch_on(int device, unsigned char **out) {
 }  // namespace
 
 namespace vrad {
+
+cudaError_t prepare_static_trace(int device) {
+    unsigned char *base = nullptr;
+    cudaError_t e = scratch_on(device, &base);
+    if (e == cudaSuccess) e = load_visibility_kernels();
+    return e;
+}
 
 // Called by vrad_trace_visibility_static in abi.cu with the context's lock
 // held and its device current.

@@ -55,10 +55,20 @@ cudaError_t launch_trace(const DeviceScene &scene, const vrad_ray *d_rays, int64
                          const TraceParams &p, uint32_t *d_bits, vrad_hit *d_hits,
                          uint32_t *d_overflow, cudaStream_t stream);
 
+// Loads the visibility trace kernels' code on the current device (with lazy
+// module loading a kernel's code is otherwise placed on the device, which
+// takes device memory, at its first launch).
+cudaError_t load_visibility_kernels();
+
 // Host-buffer visibility through the library's fixed staging array
 // (noalloc.cu); allocates nothing.  n <= VRAD_STATIC_MAX_RAYS.
 cudaError_t trace_visibility_static(const DeviceScene &scene, int device, cudaStream_t stream,
                                     const vrad_ray *h_rays, int64_t n, const TraceParams &p,
                                     uint64_t *h_bits);
+
+// Places the fixed staging array and the kernels trace_visibility_static
+// launches on `device` (current) and looks up the array's address, so that
+// no later call does either.  vrad_create calls it.
+cudaError_t prepare_static_trace(int device);
 
 }  // namespace vrad

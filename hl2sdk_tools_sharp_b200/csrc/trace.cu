@@ -98,4 +98,11 @@ cudaError_t launch_trace(const DeviceScene &scene, const vrad_ray *d_rays, int64
     return cudaGetLastError();
 }
 
+cudaError_t load_visibility_kernels() {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, k_trace<kModeAny>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, k_trace<kModeSkyPass>);
+    return e;
+}
+
 }  // namespace vrad

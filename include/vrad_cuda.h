@@ -533,15 +533,20 @@ int32_t vrad_bounce_features_device(vrad_ctx *ctx, uint16_t *x, float *target, i
  * that freeing device memory can bring.  No counterpart in the
  * reference.  Same arguments, answers and errors as vrad_trace_visibility,
  * but rays and bits are staged through one fixed array inside the library
- * (about 1.8 MB, held on every GPU that loads it until the process exits)
- * instead of buffers grown with cudaMalloc, so the call makes no allocation.
+ * (1,843,456 bytes: sizeof(vrad_ray) x VRAD_STATIC_MAX_RAYS for the rays,
+ * 8 KiB for the bits, 256 B for a status word), held on every GPU that
+ * loads the library until the process exits, instead of buffers grown with
+ * cudaMalloc, so the call makes no allocation.
  * n above VRAD_STATIC_MAX_RAYS is refused with VRAD_ERR_ARG.
  *
- * The first call on a device looks up the array's address on that device;
- * make that first call before any stream capture begins.  All calls on one
- * device share the array: calls that overlap on the GPU (two contexts on one
- * device, driven from two threads) race and must be serialised by the
- * caller.  The call blocks until the bits are written. */
+ * vrad_create places the array and the trace kernels on its device and
+ * looks up the array's address there, at set-up; later calls only use
+ * them.  (With lazy module loading that placement would otherwise happen
+ * at the first call, and it takes device memory.)  All calls on one
+ * device share the array: calls that overlap on the GPU (two contexts on
+ * one device, driven from two threads) race and must be serialised by the
+ * caller.  The call blocks until the bits are written.  The library does
+ * not survive a cudaDeviceReset of that device. */
 int32_t vrad_trace_visibility_static(vrad_ctx *ctx, const vrad_ray *rays, int64_t n,
                                      const vrad_trace_options *opts, uint64_t *hit_bits);
 

@@ -39,6 +39,40 @@ def _static_bits(tr, rays, opts):
     return bits
 
 
+def _free_device_bytes():
+    # The runtime library the vrad library itself loaded (same soname).
+    rt = ctypes.CDLL("libcudart.so.12")
+    free, total = ctypes.c_size_t(), ctypes.c_size_t()
+    assert rt.cudaMemGetInfo(ctypes.byref(free), ctypes.byref(total)) == 0
+    return free.value
+
+
+def test_static_entry_takes_no_device_memory():
+    """On a fresh context, calls of the static entry (a full batch among
+    them) leave the device's free memory exactly where it was: nothing is
+    allocated, and no kernel code is placed on the device, after set-up.
+    The allocating entry is not called before the check, so a static call
+    that fell back to the context's own buffers would show here."""
+    w = rg.generate(rg.config_3x3(seed=7))
+    r = wl.direct_rays(w, wl.luxel_samples(w, stride=3), ambient=True)
+    full = np.ascontiguousarray(r.sky[:MAX_RAYS])
+    part = np.ascontiguousarray(r.light[:777])
+    assert len(full) == MAX_RAYS
+    sky = T.RayTraceOptions(0.0, sky_does_not_block=True)
+    with T.CudaRayTracer(T.make_triangles(w.tri_verts, w.tri_ids)) as tr:
+        _static_bits(tr, part, T.RayTraceOptions.stock_exact())
+        before = _free_device_bytes()
+        a = _static_bits(tr, full, sky)
+        b = _static_bits(tr, part, T.RayTraceOptions.stock_exact())
+        c = _static_bits(tr, full, sky)
+        after = _free_device_bytes()
+        assert after == before, f"{before - after} bytes of device memory taken by static calls"
+        assert np.array_equal(a, c)
+        want = np.zeros_like(b)
+        tr.trace_visibility(part, want, T.RayTraceOptions.stock_exact())
+        assert np.array_equal(b, want)
+
+
 def test_static_entry_matches_the_allocating_one_on_two_calls():
     w = rg.generate(rg.config_3x3(seed=5))
     r = wl.direct_rays(w, wl.luxel_samples(w, stride=3), ambient=True)
