@@ -27,7 +27,7 @@ import math
 
 import numpy as np
 
-from . import tracer as T
+from . import lights as LT, roomgrid as rg, tracer as T
 from .roomgrid import World
 from .workload import ambient_directions
 
@@ -257,96 +257,24 @@ def lightmap_layout(faces: np.ndarray):
 
 # ---------------------------------------------------------------- lights
 
-def parse_intensity(color, light_scale: float = 1.0) -> np.ndarray:
-    """RadLightFile.ParseIntensity for a four-field "_light" (r g b
-    brightness): gamma 2.2 in double, narrowed to float, times
-    (float)(brightness / 255)."""
-    r, g, b, scaler = (float(c) for c in color)
-    if r < 0 or g < 0 or b < 0 or scaler < 0:
-        return np.zeros(3, np.float32)
-    x = np.float32(math.pow(r / 255.0, 2.2) * 255)
-    y = np.float32(math.pow(g / 255.0, 2.2) * 255)
-    z = np.float32(math.pow(b / 255.0, 2.2) * 255)
-    v = np.array([x, y, z], np.float32) * np.float32(scaler / 255.0)
-    return (v * np.float32(light_scale)).astype(np.float32)
+def parse_intensity(color, light_scale: float = 1.0, hdr: bool = False) -> np.ndarray:
+    """RadLightFile.ParseIntensity of a "_light" value given as its fields
+    (r g b brightness): gamma 2.2 by DetMath.Pow in double, narrowed to
+    float, times (float)(brightness / 255) (lights.parse_intensity)."""
+    text = " ".join(repr(float(c)) for c in color)
+    return LT.parse_intensity(text, hdr=hdr, light_scale=light_scale)[0]
 
 
-def _normalise(v) -> np.ndarray:
-    """Vec3.Normalise: sqrt((x*x + y*y) + z*z) in float, three divides."""
-    v = np.asarray(v, np.float32)
-    ln = np.float32(math.sqrt(float(np.float32(np.float32(v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]))))
-    if ln == 0:
-        return np.zeros(3, np.float32)
-    return np.array([v[0] / ln, v[1] / ln, v[2] / ln], np.float32)
-
-
-def _cone_cos(deg: float) -> np.float32:
-    """DetMath.CosToSingle(LightNormals.Radians(deg)): (deg / 180) in float,
-    times pi in double, cosine rounded to float."""
-    rad = float(np.float32(np.float32(deg) / np.float32(180))) * math.pi
-    return np.float32(math.cos(rad))
-
-
-def _literal_falloff(light, attn) -> None:
-    """LightFalloff.ApplyLiteralCoefficients (no _fifty_percent_distance)."""
-    c, l, q = (np.float32(a) for a in attn)
-    c = np.float32(0) if c < EQUAL_EPSILON else c
-    l = np.float32(0) if l < EQUAL_EPSILON else l
-    q = np.float32(0) if q < EQUAL_EPSILON else q
-    if c < EQUAL_EPSILON and l < EQUAL_EPSILON and q < EQUAL_EPSILON:
-        c = np.float32(1)
-    ratio = np.float32(np.float32(c + np.float32(100.0) * l) + np.float32(np.float32(100.0) * np.float32(100.0)) * q)
-    light["constant_attn"], light["linear_attn"], light["quadratic_attn"] = c, l, q
-    light["start_fade_distance"] = 0.0
-    light["end_fade_distance"] = -1.0
-    light["cap_dist"] = np.float32(1.0e22)
-    if ratio > 0:
-        light["intensity"] = (light["intensity"] * ratio).astype(np.float32)
-
-
-def build_lights(world: World):
-    """The active DirectLight list and the per-cluster light lists.
-
-    Entity order: the light_environment, then each light / light_spot.
-    Returns (lights, cluster_offsets, cluster_lights)."""
-    entities = []
-    for l in range(len(world.light_origin)):
-        e = np.zeros((), LIGHT_DTYPE)
-        e["type"] = EMIT_SPOT if world.light_type[l] == 2 else EMIT_POINT
-        e["origin"] = world.light_origin[l]
-        e["intensity"] = parse_intensity(world.light_color[l])
-        if world.light_type[l] == 2:
-            e["normal"] = _normalise(np.asarray(world.light_target[l], np.float32) - world.light_origin[l])
-            inner, outer, expo = (float(x) for x in world.light_cone[l])
-            sd = inner if inner != 0 else 10.0
-            sd2 = outer if outer != 0 else sd
-            sd2 = max(sd2, sd)
-            sd, sd2 = min(sd, 90.0), min(sd2, 90.0)
-            e["stop_dot2"] = _cone_cos(sd2)
-            e["stop_dot"] = _cone_cos(sd)
-            e["exponent"] = expo
-        _literal_falloff(e, world.light_attn[l])
-        entities.append((e, int(world.light_cluster[l])))
-    # light_environment at the origin, aimed at its target.
-    sun = np.zeros((), LIGHT_DTYPE)
-    sun["type"] = EMIT_SKY
-    sun["intensity"] = parse_intensity(world.sun_color)
-    sun["normal"] = _normalise(world.sun_target)
-    sun["cap_dist"] = np.float32(1.0e22)
-    sun["end_fade_distance"] = -1.0
-    amb = np.zeros((), LIGHT_DTYPE)
-    amb["type"] = EMIT_AMBIENT
-    amb["intensity"] = parse_intensity(world.ambient_color)
-    amb["cap_dist"] = np.float32(1.0e22)
-    amb["end_fade_distance"] = -1.0
-    # Active list: prepend in entity order (environment first: sun, then
-    # ambient), then each light.
-    active = [(sun, -1), ]
-    active.insert(0, (amb, -1))
-    for e in entities:
-        active.insert(0, e)
-    lights = np.stack([a for a, _ in active]).astype(LIGHT_DTYPE)
-    home = [c for _, c in active]
+def build_lights(world: World, hdr: bool = False):
+    """The active DirectLight list and the per-cluster light lists, for the
+    LDR pass or (hdr) the HDR pass: the map's light entities
+    (roomgrid.entities) through the restated DirectLightBuilder
+    (lights.build).  Returns (lights, cluster_offsets, cluster_lights)."""
+    ls = LT.build(rg.entities(world), lambda o: rg.cluster_of_point(world, o), hdr=hdr)
+    if ls.unsupported_class_names:
+        raise ValueError(f"unsupported light entities: {ls.unsupported_class_names}")
+    lights = LT.to_records(ls.active, LIGHT_DTYPE)
+    home = [l.cluster if l.type not in (EMIT_SKY, EMIT_AMBIENT) else -1 for l in ls.active]
     C = world.pvs.shape[0]
     lists = []
     for c in range(C):

@@ -1,0 +1,385 @@
+"""The DirectLight list from light entities: the reference's DirectLightBuilder.
+
+Restates, for the entity keys this build's maps carry, the reference's
+(muflub/hl2sdk_tools_sharp, src/SourceSharp.MapTools/Rad/Light)
+  DirectLightBuilder.Build           DirectLightBuilder.cs:84-133: the
+                                     classname dispatch ("light" prefix,
+                                     light_dynamic skipped, unknown kinds
+                                     recorded)
+  DirectLightBuilder.ParseGeneric    :198-278: style (float, truncated),
+                                     _lightHDR before _light in an HDR pass,
+                                     the target's direction or the angle keys,
+                                     _lightscaleHDR
+  ParseLightPoint / ParseLightSpot   :305-397: cones as angles, defaults,
+                                     the fully open spot, the 90-degree clamp,
+                                     DetMath.CosToSingle of the radians
+  ParseLightEnvironment              :399-505: the sun and its ambient
+                                     partner, _ambient(HDR), half the sun
+                                     when absent, _AmbientScaleHDR,
+                                     SunSpreadAngle, a second environment
+                                     orphaned
+  LightFalloff.Apply                 LightFalloff.cs:71-142, the literal
+                                     coefficients and their normalisation
+                                     at 100 units
+  LightNormals.FromProps             LightNormals.cs:66-131
+  EntityKeys                         EntityKeys.cs (last duplicate key wins,
+                                     strtod prefix scans)
+  RadLightFile.ParseIntensity        MapFormats/Text/RadLightFile.cs:344-420
+in the reference's Correct compliance mode (its default).  The active list
+is built by prepending, as DirectLightSet.AddToActiveList does, so it holds
+the entities in reverse creation order, the environment's ambient ahead of
+its sun.
+
+The _fifty_percent_distance falloff (a fitted quadratic) and texture lights
+(surface lights) are not built: an entity that asks for the first raises
+NotImplementedError, and surface lights are refused by the library.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import re
+
+import numpy as np
+
+from . import detmath as DM
+
+EMIT_SURFACE, EMIT_POINT, EMIT_SPOT, EMIT_SKY, EMIT_AMBIENT = 0, 1, 2, 3, 4
+EQUAL_EPSILON = np.float32(0.001)         # LightConstants.EqualEpsilon
+DEFAULT_INNER_CONE = np.float32(10.0)     # DirectLightBuilder.DefaultInnerCone
+MAX_CONE_ANGLE = np.float32(90.0)         # DirectLightBuilder.MaxConeAngle
+NORMALISATION_DISTANCE = np.float32(100.0)
+
+_NUM = re.compile(r"\s*([+-]?(?:\d+\.?\d*|\.\d+)(?:[eE][+-]?\d+)?)")
+
+Entity = list  # [(key, value), ...] in file order
+
+
+def entity(*pairs) -> Entity:
+    return [(str(k), str(v)) for k, v in pairs]
+
+
+# ---------------------------------------------------------------- keys
+
+def value_for_key(e: Entity, key: str) -> str:
+    """EntityKeys.ValueForKey: the LAST pair with the key wins; '' if none."""
+    v = value_for_key_with_default(e, key)
+    return "" if v is None else v
+
+
+def value_for_key_with_default(e: Entity, key: str):
+    for k, v in reversed(e):
+        if k == key:
+            return v
+    return None
+
+
+def _scan(text: str, pos: int):
+    """strtod's prefix scan from pos: (value, new pos) or (None, pos)."""
+    m = _NUM.match(text, pos)
+    if not m:
+        return None, pos
+    return float(m.group(1)), m.end()
+
+
+def atof(text: str) -> float:
+    v, _ = _scan(text, 0)
+    return 0.0 if v is None else v
+
+
+def float_for_key(e: Entity, key: str) -> np.float32:
+    """VmfValue.ParseFloat: atof in double, narrowed to float."""
+    return np.float32(atof(value_for_key(e, key)))
+
+
+def float_for_key_with_default(e: Entity, key: str, default: float) -> np.float32:
+    v = value_for_key_with_default(e, key)
+    return np.float32(default) if v is None else np.float32(atof(v))
+
+
+def int_for_key(e: Entity, key: str) -> int:
+    m = re.match(r"\s*([+-]?\d+)", value_for_key(e, key))
+    return int(m.group(1)) if m else 0
+
+
+def vector_for_key(e: Entity, key: str) -> np.ndarray:
+    """EntityKeys.GetVectorForKey: up to three doubles, stopping at the
+    first field that does not scan; each narrowed to float."""
+    text = value_for_key(e, key)
+    parts = [0.0, 0.0, 0.0]
+    pos = 0
+    for i in range(3):
+        v, pos = _scan(text, pos)
+        if v is None:
+            break
+        parts[i] = v
+    return np.array(parts, np.float32)
+
+
+def scan_doubles(text: str, maximum: int) -> list:
+    out, pos = [], 0
+    while len(out) < maximum:
+        v, pos = _scan(text, pos)
+        if v is None:
+            break
+        out.append(v)
+    return out
+
+
+# ---------------------------------------------------------------- values
+
+def parse_intensity(text: str, hdr: bool = False, light_scale: float = 1.0):
+    """RadLightFile.ParseIntensity: (intensity float32[3], parsed)."""
+    f = scan_doubles(text, 8)
+    count = len(f)
+    r = f[0] if count > 0 else 0.0
+    g = f[1] if count > 1 else 0.0
+    b = f[2] if count > 2 else 0.0
+    scaler = f[3] if count > 3 else 0.0
+    if count == 8:
+        if hdr:
+            r, g, b, scaler = f[4], f[5], f[6], f[7]
+        count = 4
+    if r < 0.0 or g < 0.0 or b < 0.0 or scaler < 0.0:
+        return np.zeros(3, np.float32), False
+    ls = np.float32(light_scale)
+    x = np.float32(DM.pow_d(r / 255.0, 2.2) * 255)
+    if count == 1:
+        return np.array([x, x, x], np.float32) * ls, True
+    if count in (3, 4):
+        y = np.float32(DM.pow_d(g / 255.0, 2.2) * 255)
+        z = np.float32(DM.pow_d(b / 255.0, 2.2) * 255)
+        v = np.array([x, y, z], np.float32)
+        if count == 4:
+            v = v * np.float32(scaler / 255.0)
+        return (v * ls).astype(np.float32), True
+    return np.array([x, 0, 0], np.float32) * ls, False
+
+
+def radians(degrees) -> float:
+    """LightNormals.Radians, Correct mode: a float divide by 180, then a
+    double multiply by pi."""
+    return float(np.float32(np.float32(degrees) / np.float32(180))) * math.pi
+
+
+def normalise(v) -> np.ndarray:
+    """Vec3.Normalise (MapFormats/Geometry/Vec3.cs:178-189): the float length
+    sqrt((x*x + y*y) + z*z), then three divides; zero stays zero."""
+    v = np.asarray(v, np.float32)
+    sq = np.float32(np.float32(v[0] * v[0] + v[1] * v[1]) + v[2] * v[2])
+    ln = np.float32(math.sqrt(float(sq)))
+    if ln == 0:
+        return np.zeros(3, np.float32)
+    return np.array([v[0] / ln, v[1] / ln, v[2] / ln], np.float32)
+
+
+def from_props(angles, angle, pitch) -> np.ndarray:
+    """LightNormals.FromProps (Correct mode)."""
+    angle, pitch = np.float32(angle), np.float32(pitch)
+    if angle == -1 or angle == -2:        # ANGLE_UP, ANGLE_DOWN
+        x = y = np.float32(0)
+    else:
+        if angle == 0:
+            angle = np.float32(angles[1])
+        x = np.float32(DM.cos_d(radians(angle)))
+        y = DM.sin_to_single(radians(angle))
+    if pitch == 0:
+        pitch = np.float32(angles[0])
+    z = DM.sin_to_single(radians(pitch))
+    cp = np.float32(DM.cos_d(radians(pitch)))
+    return np.array([x * cp, y * cp, z], np.float32)
+
+
+# ---------------------------------------------------------------- the list
+
+LIGHT_FIELDS = ("type", "style", "origin", "intensity", "normal", "stop_dot", "stop_dot2", "exponent",
+                "constant_attn", "linear_attn", "quadratic_attn", "start_fade_distance",
+                "end_fade_distance", "cap_dist")
+
+
+@dataclasses.dataclass
+class DirectLight:
+    index: int
+    origin: np.ndarray
+    cluster: int
+    type: int = EMIT_SURFACE
+    style: int = 0
+    intensity: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(3, np.float32))
+    normal: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(3, np.float32))
+    stop_dot: np.float32 = np.float32(0)
+    stop_dot2: np.float32 = np.float32(0)
+    exponent: np.float32 = np.float32(0)
+    constant_attn: np.float32 = np.float32(0)
+    linear_attn: np.float32 = np.float32(0)
+    quadratic_attn: np.float32 = np.float32(0)
+    start_fade_distance: np.float32 = np.float32(0)
+    end_fade_distance: np.float32 = np.float32(-1)      # DirectLight.cs:129
+    cap_dist: np.float32 = np.float32(1.0e22)           # DirectLight.cs:141
+
+
+@dataclasses.dataclass
+class DirectLightSet:
+    active: list = dataclasses.field(default_factory=list)
+    count: int = 0
+    sky_light: DirectLight | None = None
+    ambient: DirectLight | None = None
+    sun_angular_extent: np.float32 = np.float32(0)
+    orphaned_sky_lights: int = 0
+    unsupported_class_names: list = dataclasses.field(default_factory=list)
+    warnings: list = dataclasses.field(default_factory=list)
+
+    def alloc(self, origin, cluster: int, add: bool) -> DirectLight:
+        light = DirectLight(index=self.count, origin=np.asarray(origin, np.float32), cluster=cluster)
+        self.count += 1
+        if add:
+            self.active.insert(0, light)
+        return light
+
+
+def _find_target(entities, name: str):
+    for e in entities:
+        if value_for_key(e, "targetname") == name:
+            return e
+    return None
+
+
+def _parse_generic(entities, e, light: DirectLight, lights: DirectLightSet, hdr: bool) -> None:
+    light.style = int(float_for_key(e, "style"))
+    have = False
+    if hdr:
+        v, ok = parse_intensity(value_for_key(e, "_lightHDR"), hdr=True)
+        if ok:
+            light.intensity, have = v, True
+    if not have:
+        light.intensity, _ = parse_intensity(value_for_key(e, "_light"), hdr=hdr)
+    target = value_for_key(e, "target")
+    if target:
+        t = _find_target(entities, target)
+        if t is None:
+            o = light.origin
+            lights.warnings.append(f"WARNING: light at ({int(o[0])} {int(o[1])} {int(o[2])}) has missing target")
+        else:
+            light.normal = normalise(vector_for_key(t, "origin") - light.origin)
+    else:
+        light.normal = from_props(vector_for_key(e, "angles"), float_for_key(e, "angle"), float_for_key(e, "pitch"))
+    if hdr:
+        light.intensity = (light.intensity * float_for_key_with_default(e, "_lightscaleHDR", 1.0)).astype(np.float32)
+
+
+def _falloff(e, light: DirectLight) -> None:
+    if float_for_key(e, "_fifty_percent_distance") != 0:
+        raise NotImplementedError("_fifty_percent_distance falloff is not built")
+    light.start_fade_distance = np.float32(0)
+    light.end_fade_distance = np.float32(-1)
+    light.cap_dist = np.float32(1.0e22)
+    c, l, q = (float_for_key(e, k) for k in ("_constant_attn", "_linear_attn", "_quadratic_attn"))
+    c = np.float32(0) if c < EQUAL_EPSILON else c
+    l = np.float32(0) if l < EQUAL_EPSILON else l
+    q = np.float32(0) if q < EQUAL_EPSILON else q
+    if c < EQUAL_EPSILON and l < EQUAL_EPSILON and q < EQUAL_EPSILON:
+        c = np.float32(1)
+    light.constant_attn, light.linear_attn, light.quadratic_attn = c, l, q
+    d = NORMALISATION_DISTANCE
+    ratio = np.float32(np.float32(c + d * l) + np.float32(d * d) * q)
+    if ratio > 0:
+        light.intensity = (light.intensity * ratio).astype(np.float32)
+
+
+def _parse_point(entities, e, cluster_of, lights, hdr):
+    o = vector_for_key(e, "origin")
+    light = lights.alloc(o, cluster_of(o), True)
+    _parse_generic(entities, e, light, lights, hdr)
+    light.type = EMIT_POINT
+    _falloff(e, light)
+
+
+def _parse_spot(entities, e, cluster_of, lights, hdr):
+    o = vector_for_key(e, "origin")
+    light = lights.alloc(o, cluster_of(o), True)
+    _parse_generic(entities, e, light, lights, hdr)
+    light.type = EMIT_SPOT
+    inner = float_for_key(e, "_inner_cone")
+    if inner == 0:
+        inner = DEFAULT_INNER_CONE
+    outer = float_for_key(e, "_cone")
+    if outer == 0:
+        outer = inner
+    if outer < inner:
+        outer = inner
+    if inner == 180 and outer == 180:
+        light.stop_dot = light.stop_dot2 = np.float32(0)
+        light.type = EMIT_POINT
+        light.exponent = np.float32(0)
+    else:
+        where = f"({int(o[0])} {int(o[1])} {int(o[2])})"
+        if inner > MAX_CONE_ANGLE:
+            lights.warnings.append(f"WARNING: light_spot at {where} has inner angle larger than 90 degrees! "
+                                   "Clamping to 90...")
+            inner = MAX_CONE_ANGLE
+        if outer > MAX_CONE_ANGLE:
+            lights.warnings.append(f"WARNING: light_spot at {where} has outer angle larger than 90 degrees! "
+                                   "Clamping to 90...")
+            outer = MAX_CONE_ANGLE
+        light.stop_dot2 = DM.cos_to_single(radians(outer))
+        light.stop_dot = DM.cos_to_single(radians(inner))
+        light.exponent = float_for_key(e, "_exponent")
+    _falloff(e, light)
+
+
+def _parse_environment(entities, e, cluster_of, lights, hdr):
+    o = vector_for_key(e, "origin")
+    light = lights.alloc(o, cluster_of(o), False)
+    _parse_generic(entities, e, light, lights, hdr)
+    spread = value_for_key_with_default(e, "SunSpreadAngle")
+    if spread is not None and lights.sky_light is None:
+        lights.sun_angular_extent = DM.sin_to_single(math.pi / 180.0 * float(np.float32(atof(spread))))
+    if lights.sky_light is not None:
+        lights.orphaned_sky_lights += 1
+        return
+    lights.sky_light = light
+    light.type = EMIT_SKY
+    ambient = lights.alloc(light.origin, cluster_of(light.origin), False)
+    ambient.type = EMIT_AMBIENT
+    lights.ambient = ambient
+    have = False
+    if hdr:
+        v, ok = parse_intensity(value_for_key(e, "_ambientHDR"), hdr=True)
+        if ok:
+            ambient.intensity, have = v, True
+    if not have:
+        v, ok = parse_intensity(value_for_key(e, "_ambient"), hdr=hdr)
+        ambient.intensity = v if ok else (light.intensity * np.float32(0.5)).astype(np.float32)
+    if hdr:
+        ambient.intensity = (ambient.intensity * float_for_key_with_default(e, "_AmbientScaleHDR", 1.0)).astype(
+            np.float32)
+    # Sun, then ambient, each prepended: the ambient heads the list.
+    lights.active.insert(0, light)
+    lights.active.insert(0, ambient)
+
+
+def build(entities, cluster_of=lambda origin: 0, hdr: bool = False) -> DirectLightSet:
+    """DirectLightBuilder.Build over entity records (no surface lights).
+    cluster_of(origin) gives the cluster of a point (the tree's leaf)."""
+    lights = DirectLightSet()
+    for e in entities:
+        name = value_for_key(e, "classname")
+        if not name.startswith("light") or name == "light_dynamic":
+            continue
+        if name == "light_spot":
+            _parse_spot(entities, e, cluster_of, lights, hdr)
+        elif name == "light_environment":
+            _parse_environment(entities, e, cluster_of, lights, hdr)
+        elif name == "light":
+            _parse_point(entities, e, cluster_of, lights, hdr)
+        else:
+            lights.unsupported_class_names.append(name)
+    return lights
+
+
+def to_records(active, dtype) -> np.ndarray:
+    """The active list as the C ABI's vrad_light records."""
+    out = np.zeros(len(active), dtype)
+    for i, l in enumerate(active):
+        for f in LIGHT_FIELDS:
+            out[i][f] = getattr(l, f)
+    return out

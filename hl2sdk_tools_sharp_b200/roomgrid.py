@@ -114,6 +114,16 @@ class World:
     ambient_color: np.ndarray    # (4,) float64 "_ambient" of the light_environment
     sky_intensity: np.ndarray    # (3,) float32 nonzero when the sky ambient is on
     pvs: np.ndarray              # (C, C) bool
+    # The HDR pass's keys (drawn from a stream of their own, so the LDR map
+    # is the same with or without them): "_lightHDR" per light (a row of -1
+    # is Hammer's "-1 -1 -1 1", which falls back to "_light"),
+    # "_lightscaleHDR", and the light_environment's "_lightHDR",
+    # "_ambientHDR" and "_AmbientScaleHDR".
+    light_color_hdr: np.ndarray = None   # (L, 4) float64
+    light_scale_hdr: np.ndarray = None   # (L,) float64
+    sun_color_hdr: np.ndarray = None     # (4,) float64
+    ambient_color_hdr: np.ndarray = None  # (4,) float64
+    ambient_scale_hdr: float = 1.0
 
     @property
     def face_count(self) -> int:
@@ -420,4 +430,77 @@ def generate(cfg: Config) -> World:
         ambient_color=np.array([120.0, 150.0, 210.0, 60.0]) if cfg.sky_ambient else np.zeros(4),
         sky_intensity=np.array([1.0, 1.0, 1.0], np.float32) if cfg.sky_ambient else np.zeros(3, np.float32),
         pvs=pvs,
+        **_hdr_keys(cfg, L),
     )
+
+
+def _hdr_keys(cfg: Config, L: int) -> dict:
+    """Seeded HDR keys: half the lights fall back to "_light" ("-1 -1 -1 1"),
+    the others get an HDR colour and brightness of their own; every light a
+    "_lightscaleHDR" of 0.5 to 3; the sun and sky brighter than in LDR."""
+    rng = np.random.default_rng([cfg.seed, 0x4844])
+    color = np.full((L, 4), -1.0)
+    color[:, 3] = 1.0
+    own = rng.uniform(size=L) < 0.5
+    n = int(own.sum())
+    color[own, 0:3] = np.round(rng.uniform(160.0, 255.0, size=(n, 3)))
+    color[own, 3] = np.round(rng.uniform(cfg.intensity[0], 2.0 * cfg.intensity[1], size=n))
+    scale = rng.choice([0.5, 1.0, 1.5, 2.0, 3.0], size=L)
+    return dict(light_color_hdr=color, light_scale_hdr=scale,
+                sun_color_hdr=np.array([255.0, 235.0, 190.0, 600.0]),
+                ambient_color_hdr=np.array([110.0, 145.0, 215.0, 150.0]) if cfg.sky_ambient else np.zeros(4),
+                ambient_scale_hdr=1.5 if cfg.sky_ambient else 1.0)
+
+
+def _num(x) -> str:
+    """A key value that parses back to exactly x (a float32 or a double)."""
+    return repr(float(x))
+
+
+def entities(world: World) -> list:
+    """The map's light entities in file order, as (key, value) records the
+    reference's DirectLightBuilder reads: the light_environment at the origin
+    aimed by a target, then each light or light_spot (spots aimed by a
+    target), with "_light", the literal attenuation keys, cones, and the
+    HDR keys."""
+    def col(c):
+        return " ".join(_num(v) for v in c)
+
+    out = [[("classname", "worldspawn")]]
+    env = [("classname", "light_environment"), ("origin", "0 0 0"), ("target", "sun_target"),
+           ("_light", col(world.sun_color)), ("_ambient", col(world.ambient_color))]
+    if world.sun_color_hdr is not None:
+        env += [("_lightHDR", col(world.sun_color_hdr)), ("_ambientHDR", col(world.ambient_color_hdr)),
+                ("_AmbientScaleHDR", _num(world.ambient_scale_hdr))]
+    out.append(env)
+    out.append([("classname", "info_target"), ("targetname", "sun_target"), ("origin", col(world.sun_target))])
+    for l in range(len(world.light_origin)):
+        spot = int(world.light_type[l]) == 2
+        e = [("classname", "light_spot" if spot else "light"), ("origin", col(world.light_origin[l])),
+             ("_light", col(world.light_color[l]))]
+        if world.light_color_hdr is not None:
+            e += [("_lightHDR", col(world.light_color_hdr[l])), ("_lightscaleHDR", _num(world.light_scale_hdr[l]))]
+        a = world.light_attn[l]
+        e += [("_constant_attn", _num(a[0])), ("_linear_attn", _num(a[1])), ("_quadratic_attn", _num(a[2]))]
+        if spot:
+            inner, outer, expo = world.light_cone[l]
+            e += [("target", f"spot_{l}"), ("_inner_cone", _num(inner)), ("_cone", _num(outer)),
+                  ("_exponent", _num(expo))]
+        out.append(e)
+        if spot:
+            out.append([("classname", "info_target"), ("targetname", f"spot_{l}"),
+                        ("origin", col(world.light_target[l]))])
+    return out
+
+
+def cluster_of_point(world: World, p) -> int:
+    """The cluster (room) holding point p, or -1 outside every room."""
+    R = world.config.side
+    i = int(np.floor((float(p[0]) - WALL) / PITCH))
+    j = int(np.floor((float(p[1]) - WALL) / PITCH))
+    if not (0 <= i < R and 0 <= j < R):
+        return -1
+    x0, y0 = _room_origin(i, j)
+    if not (x0 <= p[0] <= x0 + ROOM and y0 <= p[1] <= y0 + ROOM):
+        return -1
+    return i * R + j

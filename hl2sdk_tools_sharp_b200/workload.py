@@ -20,6 +20,7 @@ face normal (FaceLightJob.ComputeIlluminationPointAndNormals).
 from __future__ import annotations
 
 import dataclasses
+import functools
 import math
 
 import numpy as np
@@ -51,17 +52,25 @@ def halton(base: int, count: int) -> np.ndarray:
 
 
 def ambient_directions(count: int = AMBIENT_DIRECTIONS) -> np.ndarray:
-    """DirectionalSampler.NextValue x count: z from Halton(2), azimuth from
-    Halton(3); trigonometry in double, rounded once to float."""
+    return _ambient_directions(count).copy()
+
+
+@functools.lru_cache(maxsize=8)
+def _ambient_directions(count: int) -> np.ndarray:
+    """DirectionalSampler.NextValue x count (DirectionalSampler.cs:96-121): z
+    from Halton(2), azimuth from Halton(3); 2z - 1 and 2 pi v in double,
+    narrowed; DetMathF.Acos, Sin and Cos (correctly rounded float functions,
+    detmath.py); the products in float."""
+    from . import detmath as DM
     z = halton(2, count)
     v = halton(3, count)
     out = np.empty((count, 3), np.float32)
     for k in range(count):
         zv = np.float32(2.0 * float(z[k]) - 1.0)
-        phi = np.float32(math.acos(float(zv)))
+        phi = DM.acos_f(zv)
         theta = np.float32(2.0 * math.pi * float(v[k]))
-        sp = np.float32(math.sin(float(phi)))
-        out[k] = (np.float32(math.cos(float(theta))) * sp, np.float32(math.sin(float(theta))) * sp, zv)
+        sp = DM.sin_f(phi)
+        out[k] = (DM.cos_f(theta) * sp, DM.sin_f(theta) * sp, zv)
     return out
 
 

@@ -11,16 +11,22 @@ Each scene is four little-endian binary files (tris, rays, tree, answers).
 They are data, not source, and the GPU test machine has no copy of the
 reference, so the bytes are committed here unchanged.
 
-It also extracts, as text, the correctly rounded single-precision arcsine
-and power rows of the reference's DetMath golden table
+It also extracts, as text, rows of the reference's DetMath golden table
 (src/SourceSharp.Tests/MapFormats/Numerics/DetMathGoldens.cs, computed by
-the reference's tools/detmath_goldens.py with mpmath at 3000 bits) into
-detmath-goldens.txt: one row per line, "function a b expected" as hex bit
-patterns.  Run from anywhere:
+the reference's tools/detmath_goldens.py with mpmath at 3000 bits):
+  detmath-goldens.txt       the single-precision arcsine and power rows
+                            (the device's asin and pow), "function a b
+                            expected" as 32-bit hex patterns;
+  detmath-goldens-host.txt  the rows of the functions the host-side tables
+                            use: single-precision Acos, Sin and Cos, double
+                            Sin, Cos and Pow, "kind function a b expected"
+                            as hex patterns of the kind's width.
+Run from anywhere, naming the reference's root (or set VRAD_REFERENCE_ROOT):
 
-    python tests/golden/make_golden.py [reference-root]
+    python tests/golden/make_golden.py <reference-root>
 """
 import hashlib
+import os
 import pathlib
 import re
 import shutil
@@ -29,12 +35,16 @@ import sys
 SRC_REL = "src/SourceSharp.Tests/MapTools/Tracing/Fixtures"
 DETMATH_REL = "src/SourceSharp.Tests/MapFormats/Numerics/DetMathGoldens.cs"
 DETMATH_ROWS = {("F1", "Asin"), ("F2", "Pow")}
+HOST_ROWS = {("F1", "Acos"), ("F1", "Sin"), ("F1", "Cos"), ("D1", "Sin"), ("D1", "Cos"), ("D2", "Pow")}
 NAMES = [f"{scene}.{part}.bin" for scene in ("kd-scene", "kd-boxes")
          for part in ("tris", "rays", "tree", "answers")]
 
 
 def main() -> None:
-    root = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    arg = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("VRAD_REFERENCE_ROOT")
+    if not arg:
+        sys.exit("usage: make_golden.py <reference-root> (or set VRAD_REFERENCE_ROOT)")
+    root = pathlib.Path(arg)
     src = root / SRC_REL
     dst = pathlib.Path(__file__).resolve().parent
     lines = []
@@ -42,15 +52,19 @@ def main() -> None:
         shutil.copyfile(src / name, dst / name)
         digest = hashlib.sha256((dst / name).read_bytes()).hexdigest()
         lines.append(f"{digest}  {name}")
-    rows = []
+    rows, host = [], []
     pat = re.compile(r'\("(\w+)", "(\w+)", 0x([0-9A-Fa-f]+)UL, 0x([0-9A-Fa-f]+)UL, 0x([0-9A-Fa-f]+)UL\)')
     for m in pat.finditer((root / DETMATH_REL).read_text()):
         kind, fn, a, b, e = m.groups()
         if (kind, fn) in DETMATH_ROWS:
             rows.append(f"{fn} {int(a, 16):08x} {int(b, 16):08x} {int(e, 16):08x}")
-    (dst / "detmath-goldens.txt").write_text("\n".join(rows) + "\n")
-    digest = hashlib.sha256((dst / "detmath-goldens.txt").read_bytes()).hexdigest()
-    lines.append(f"{digest}  detmath-goldens.txt")
+        if (kind, fn) in HOST_ROWS:
+            w = 8 if kind.startswith("F") else 16
+            host.append(f"{kind} {fn} {int(a, 16):0{w}x} {int(b, 16):0{w}x} {int(e, 16):0{w}x}")
+    for name, body in (("detmath-goldens.txt", rows), ("detmath-goldens-host.txt", host)):
+        (dst / name).write_text("\n".join(body) + "\n")
+        digest = hashlib.sha256((dst / name).read_bytes()).hexdigest()
+        lines.append(f"{digest}  {name}")
     (dst / "SHA256SUMS").write_text("\n".join(lines) + "\n")
     print("\n".join(lines))
 
