@@ -245,15 +245,23 @@ __global__ void k_candidates(BounceView v, const int64_t *__restrict__ cand_off,
     if (!out) counts[r] = n;
 }
 
-// FormFactors.PolyToDiff of source s's winding seen from (o, n).
-__device__ float poly_to_diff(const BounceView &v, int s, float area, F3 o, F3 n, unsigned long long *open) {
-    const int2 w = __ldg(&v.wind[s]);
+// FormFactors.DiffToDiff(o1, n1, o2, n2): delta = normalise(o1 - o2), then
+// -(delta . n1) * (delta . n2) / (len * len).
+__device__ __forceinline__ float diff_to_diff(F3 o1, F3 n1, F3 o2, F3 n2) {
+    float dl;
+    const F3 d = normalise3(sub3(o1, o2), dl);
+    return __fdiv_rn(__fmul_rn(-dot3(d, n1), dot3(d, n2)), __fmul_rn(dl, dl));
+}
+
+// FormFactors.PolyToDiff of a winding of `count` points seen from (o, n).
+__device__ float poly_to_diff_pts(const float4 *__restrict__ pts, int count, float area, F3 o, F3 n,
+                                  unsigned long long *open) {
     float ff = 0.0f;
-    for (int k = 0; k < w.y; k++) {
-        const int k2 = k < w.y - 1 ? k + 1 : 0;
+    for (int k = 0; k < count; k++) {
+        const int k2 = k < count - 1 ? k + 1 : 0;
         float l;
-        const F3 v1 = normalise3(sub3(f3(__ldg(&v.points[w.x + k])), o), l);
-        const F3 v2 = normalise3(sub3(f3(__ldg(&v.points[w.x + k2])), o), l);
+        const F3 v1 = normalise3(sub3(f3(__ldg(&pts[k])), o), l);
+        const F3 v2 = normalise3(sub3(f3(__ldg(&pts[k2])), o), l);
         float sin_alpha;
         F3 gamma = normalise3(cross3(v1, v2), sin_alpha);
         if (sin_alpha < -1.0f || sin_alpha > 1.0f) sin_alpha = sin_alpha > 1.0f ? 1.0f : -1.0f;
@@ -261,6 +269,13 @@ __device__ float poly_to_diff(const BounceView &v, int s, float area, F3 o, F3 n
         ff = __fadd_rn(ff, dot3(gamma, n));
     }
     return __fmul_rn(ff, __fdiv_rn(0.5f, area));
+}
+
+// PolyToDiff of source s's winding seen from (o, n).
+__device__ __forceinline__ float poly_to_diff(const BounceView &v, int s, float area, F3 o, F3 n,
+                                              unsigned long long *open) {
+    const int2 w = __ldg(&v.wind[s]);
+    return poly_to_diff_pts(v.points + w.x, w.y, area, o, n, open);
 }
 
 // One candidate pair: VisMatrix.TransferRay traced (StockExact: every
@@ -314,9 +329,7 @@ __global__ void __launch_bounds__(BLOCK, 12) k_transfer(BounceView v, DeviceScen
         if (!blocked && __ldg(&v.tree[s].w) == 0 && so.w > 0.0f) {
             // MakeTransfer: DiffToDiff(source, receiver), the polygon form
             // factor for a near source, trans = area * scale > 1e-7.
-            float dl;
-            const F3 d = normalise3(sub3(f3(so), f3(po)), dl);
-            float scale = __fdiv_rn(__fmul_rn(-dot3(d, f3(sn)), dot3(d, f3(pn))), __fmul_rn(dl, dl));
+            float scale = diff_to_diff(f3(so), f3(sn), f3(po), f3(pn));
             if (!(scale <= 0.0f)) {
                 const F3 dd = sub3(f3(po), f3(so));
                 const float threshold = (float)__dmul_rn(3.141592653589793 * 0.04, (double)dot3(dd, dd));
@@ -854,3 +867,91 @@ cudaError_t launch_exact_total(BounceBuffers &b, int bounce, cudaStream_t stream
 }
 
 }  // namespace vrad
+
+// ---- form factors on their own (inspection) ----------------------------------
+//
+// The transfer build's DiffToDiff and PolyToDiff, evaluated for caller-given
+// cases by the same device functions k_transfer calls, so the reference's
+// known-answer cases (Tests/MapTools/Rad/Bounce/FormFactorsTests.cs) run on
+// the device's own arithmetic.
+
+namespace {
+
+__global__ void k_ff_diff(const float *__restrict__ c, int64_t n, float *__restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float *q = c + 12 * i;
+    out[i] = vrad::diff_to_diff({q[0], q[1], q[2]}, {q[3], q[4], q[5]}, {q[6], q[7], q[8]}, {q[9], q[10], q[11]});
+}
+
+__global__ void k_ff_poly(const float4 *__restrict__ pts, const int32_t *__restrict__ first,
+                          const float *__restrict__ c, int64_t n, float *__restrict__ out,
+                          unsigned long long *open) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float *q = c + 7 * i;
+    out[i] = vrad::poly_to_diff_pts(pts + first[i], first[i + 1] - first[i], q[0], {q[1], q[2], q[3]},
+                                    {q[4], q[5], q[6]}, open);
+}
+
+// Copies `bytes` from host to a fresh device block (the inspection calls'
+// own small temporaries).
+cudaError_t upload_tmp(void **d, const void *h, size_t bytes, cudaStream_t s) {
+    cudaError_t e = cudaMalloc(d, bytes ? bytes : 16);
+    if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(*d, h, bytes, cudaMemcpyHostToDevice, s);
+    return e;
+}
+
+}  // namespace
+
+extern "C" int32_t vrad_form_factor_diff(vrad_ctx *ctx, const float *cases, int64_t n, float *out) {
+    if (!ctx || n < 0 || (n && (!cases || !out))) return vrad_fail(ctx, VRAD_ERR_ARG, "invalid form factor cases");
+    if (n == 0) return VRAD_OK;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    void *dc = nullptr, *dout = nullptr;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess) e = upload_tmp(&dc, cases, sizeof(float) * 12 * (size_t)n, ctx->stream);
+    if (e == cudaSuccess) e = cudaMalloc(&dout, sizeof(float) * (size_t)n);
+    if (e == cudaSuccess) {
+        k_ff_diff<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(static_cast<const float *>(dc), n,
+                                                                      static_cast<float *>(dout));
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = vrad::wait_stream(ctx->stream);
+    cudaFree(dc);
+    cudaFree(dout);
+    return e == cudaSuccess ? VRAD_OK : vrad_cuda_fail(ctx, e, "form factors");
+}
+
+extern "C" int32_t vrad_form_factor_poly(vrad_ctx *ctx, const float *points, const int32_t *first,
+                                         const float *cases, int64_t n, float *out) {
+    if (!ctx || n < 0 || (n && (!points || !first || !cases || !out)))
+        return vrad_fail(ctx, VRAD_ERR_ARG, "invalid form factor cases");
+    if (n == 0) return VRAD_OK;
+    for (int64_t i = 0; i < n; i++)
+        if (first[i] < 0 || first[i + 1] < first[i] + 3)
+            return vrad_fail(ctx, VRAD_ERR_ARG, "winding %lld has fewer than three points", (long long)i);
+    const int64_t np = first[n];
+    std::vector<float4> pts((size_t)np);
+    for (int64_t k = 0; k < np; k++) pts[(size_t)k] = make_float4(points[3 * k], points[3 * k + 1], points[3 * k + 2], 0.0f);
+    std::lock_guard<std::mutex> g(ctx->mu);
+    void *dp = nullptr, *df = nullptr, *dc = nullptr, *dout = nullptr, *dopen = nullptr;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess) e = upload_tmp(&dp, pts.data(), sizeof(float4) * (size_t)np, ctx->stream);
+    if (e == cudaSuccess) e = upload_tmp(&df, first, sizeof(int32_t) * (size_t)(n + 1), ctx->stream);
+    if (e == cudaSuccess) e = upload_tmp(&dc, cases, sizeof(float) * 7 * (size_t)n, ctx->stream);
+    if (e == cudaSuccess) e = cudaMalloc(&dout, sizeof(float) * (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&dopen, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemsetAsync(dopen, 0, sizeof(unsigned long long), ctx->stream);
+    if (e == cudaSuccess) {
+        k_ff_poly<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(
+            static_cast<const float4 *>(dp), static_cast<const int32_t *>(df), static_cast<const float *>(dc), n,
+            static_cast<float *>(dout), static_cast<unsigned long long *>(dopen));
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = vrad::wait_stream(ctx->stream);
+    for (void *q : {dp, df, dc, dout, dopen}) cudaFree(q);
+    return e == cudaSuccess ? VRAD_OK : vrad_cuda_fail(ctx, e, "form factors");
+}

@@ -143,6 +143,10 @@ def _lib():
         lib.vrad_bounce_last_total.restype = i32
         lib.vrad_bounce_transfers.argtypes = [P, P, i64, P, i64, ctypes.POINTER(i64)]
         lib.vrad_bounce_transfers.restype = i32
+        lib.vrad_form_factor_diff.argtypes = [P, P, i64, P]
+        lib.vrad_form_factor_diff.restype = i32
+        lib.vrad_form_factor_poly.argtypes = [P, P, P, P, i64, P]
+        lib.vrad_form_factor_poly.restype = i32
         lib._lighting_bound = True
     return lib
 
@@ -214,6 +218,28 @@ def build_patches(faces: np.ndarray, verts: np.ndarray, reflectivity: np.ndarray
 def face_reflectivity(world: World) -> np.ndarray:
     """Each lit face's material reflectivity (F, 3)."""
     return np.ascontiguousarray(world.reflectivity[world.face_material], np.float32)
+
+
+def form_factors_diff(ctx_owner, cases) -> np.ndarray:
+    """vrad_form_factor_diff on the device of ctx_owner (a tracer or a
+    stage): cases (n, 12) = o1, n1, o2, n2."""
+    c = np.ascontiguousarray(cases, np.float32).reshape(-1, 12)
+    out = np.zeros(len(c), np.float32)
+    T._check(_lib().vrad_form_factor_diff(ctx_owner._ctx, c.ctypes.data, len(c), out.ctypes.data), ctx_owner._ctx)
+    return out
+
+
+def form_factors_poly(ctx_owner, windings, cases) -> np.ndarray:
+    """vrad_form_factor_poly: windings a list of (k, 3) point arrays, cases
+    (n, 7) = area, receiving point, normal."""
+    pts = np.ascontiguousarray(np.concatenate([np.asarray(w, np.float32).reshape(-1, 3) for w in windings]))
+    first = np.zeros(len(windings) + 1, np.int32)
+    first[1:] = np.cumsum([len(w) for w in windings])
+    c = np.ascontiguousarray(cases, np.float32).reshape(-1, 7)
+    out = np.zeros(len(c), np.float32)
+    T._check(_lib().vrad_form_factor_poly(ctx_owner._ctx, pts.ctypes.data, first.ctypes.data, c.ctypes.data, len(c),
+                                          out.ctypes.data), ctx_owner._ctx)
+    return out
 
 
 def pvs_lists(world: World):

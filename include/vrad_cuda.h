@@ -452,6 +452,22 @@ int32_t vrad_bounce_patch_light(vrad_ctx *ctx, float *total_light, float *direct
  * value its stop rule compares), xyz. */
 int32_t vrad_bounce_last_total(vrad_ctx *ctx, float *total);
 
+/* The transfer build's form factors on their own, evaluated on the device by
+ * the functions the transfer kernel calls; they replace
+ * FormFactors.DiffToDiff and FormFactors.PolyToDiff
+ * (MapTools/Rad/Bounce/FormFactors.cs:58-140, Correct mode) for inspection.
+ *   vrad_form_factor_diff: cases are n x 12 floats (o1, n1, o2, n2); out[i]
+ *     = -(d . n1)(d . n2) / len^2 with d, len = normalise(o1 - o2).
+ *   vrad_form_factor_poly: winding i is points[first[i] .. first[i+1]) (xyz
+ *     triples, at least three); cases are n x 7 floats (the winding's area,
+ *     the receiving point, its normal); out[i] the polygon form factor
+ *     (Sum gamma_k asin|v_k x v_k+1| . n) * 0.5 / area, with the correctly
+ *     rounded arcsine.
+ * Both block and allocate their own small device temporaries. */
+int32_t vrad_form_factor_diff(vrad_ctx *ctx, const float *cases, int64_t n, float *out);
+int32_t vrad_form_factor_poly(vrad_ctx *ctx, const float *points, const int32_t *first, const float *cases,
+                              int64_t n, float *out);
+
 /* Transfer (MapTools/Rad/Bounce/TransferSet.cs:26): source patch, weight. */
 typedef struct vrad_transfer {
     int32_t patch;

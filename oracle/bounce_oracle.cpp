@@ -890,6 +890,18 @@ int64_t orc_bounce_stats(void *h, int64_t *blocked) {
 
 float orc_asin(float x) { return AsinCR(x); }
 
+// FormFactors.DiffToDiff(o1, n1, o2, n2); q = 12 floats.
+float orc_diff_to_diff(const float *q) {
+    return DiffToDiff(V{q[0], q[1], q[2]}, V{q[3], q[4], q[5]}, V{q[6], q[7], q[8]}, V{q[9], q[10], q[11]});
+}
+
+// FormFactors.PolyToDiff of a winding of `count` xyz points.
+float orc_poly_to_diff(const float *points, int32_t count, float area, const float *origin, const float *normal) {
+    Winding w;
+    for (int32_t k = 0; k < count; k++) w.push_back(V{points[3 * k], points[3 * k + 1], points[3 * k + 2]});
+    return PolyToDiff(w, area, V{origin[0], origin[1], origin[2]}, V{normal[0], normal[1], normal[2]});
+}
+
 // Drops every built transfer list, so the next build traces again.
 void orc_bounce_forget_transfers(void *h) {
     World &w = *static_cast<World *>(h);

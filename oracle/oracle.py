@@ -319,6 +319,10 @@ def _bounce_lib():
         L.orc_bounce_count_candidates.restype = i64
         L.orc_asin.argtypes = [f32]
         L.orc_asin.restype = f32
+        L.orc_diff_to_diff.argtypes = [P]
+        L.orc_diff_to_diff.restype = f32
+        L.orc_poly_to_diff.argtypes = [P, i32, f32, P, P]
+        L.orc_poly_to_diff.restype = f32
         L._bounce_typed = True
     return L
 
@@ -334,6 +338,20 @@ def powf(x: float, y: float) -> float:
 def asin(x: float) -> float:
     """DetMathF.Asin as the oracle computes it."""
     return _bounce_lib().orc_asin(float(x))
+
+
+def diff_to_diff(o1, n1, o2, n2) -> np.float32:
+    """FormFactors.DiffToDiff as the oracle computes it."""
+    q = np.ascontiguousarray(np.concatenate([o1, n1, o2, n2]), np.float32)
+    return np.float32(_bounce_lib().orc_diff_to_diff(_p(q)))
+
+
+def poly_to_diff(points, area, origin, normal) -> np.float32:
+    """FormFactors.PolyToDiff as the oracle computes it."""
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    o = np.ascontiguousarray(origin, np.float32)
+    n = np.ascontiguousarray(normal, np.float32)
+    return np.float32(_bounce_lib().orc_poly_to_diff(_p(pts), len(pts), float(area), _p(o), _p(n)))
 
 
 class Bounce:

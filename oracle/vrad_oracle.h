@@ -245,6 +245,10 @@ int64_t orc_bounce_count_candidates(void *h);
 float orc_powf(float x, float y);
 /* DetMathF.Asin as the oracle computes it. */
 float orc_asin(float x);
+/* FormFactors.DiffToDiff (o1, n1, o2, n2 as 12 floats) and PolyToDiff
+ * (MapTools/Rad/Bounce/FormFactors.cs:58-140). */
+float orc_diff_to_diff(const float *q);
+float orc_poly_to_diff(const float *points, int32_t count, float area, const float *origin, const float *normal);
 
 #ifdef __cplusplus
 }
