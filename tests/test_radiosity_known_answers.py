@@ -26,7 +26,7 @@ S = 256.0
 TRACE_ID_SKY = 0x01000000
 
 
-def _box(ceiling_sky=False):
+def _box(ceiling_sky=False, occluder=False):
     # LightBox.Map: (texinfo s axis, t axis, normal, corners) per face.
     floor_st = ((1, 0, 0), (0, -1, 0))
     wall_st = ((0, 1, 0), (0, 0, -1))
@@ -64,6 +64,12 @@ def _box(ceiling_sky=False):
         ident = TRACE_ID_SKY if sky else 0
         tris += [np.concatenate([c[0], c[1], c[2]]), np.concatenate([c[0], c[2], c[3]])]
         ids += [ident, ident]
+    if occluder:
+        # AnOccluderRemovesTransfers: map.AddOccluder((8 8 128) (248 8 128)
+        # (248 248 128) (8 248 128)), a caster that is no face.
+        c = np.array([(8, 8, 128), (248, 8, 128), (248, 248, 128), (8, 248, 128)], np.float32)
+        tris += [np.concatenate([c[0], c[1], c[2]]), np.concatenate([c[0], c[2], c[3]])]
+        ids += [0, 0]
     verts = np.array(verts, np.float32)
     samples, first = L.build_samples(faces, verts)
     ls = LT.build([LT.entity(("classname", "worldspawn")),
@@ -77,23 +83,25 @@ def _box(ceiling_sky=False):
 
 
 PVS = (np.array([0, 1], np.int32), np.array([0], np.int32))
+NO_SELF = (np.array([0, 0], np.int32), np.array([], np.int32))   # BounceBox.Map(seesItself: false)
 
 
-def _oracle(O, world, inp, refl, bounces, threshold=1.0):
+def _oracle(O, world, inp, refl, bounces, threshold=1.0, pvs=PVS):
     tree = O.kd_build(world.tri_verts, world.tri_ids)
     light = O.direct(tree, inp.faces, inp.samples, inp.face_first, inp.lights, inp.cluster_offsets,
                      inp.cluster_lights, inp.sky_directions, verts=inp.verts)
-    ob = O.Bounce(tree, inp.faces, inp.verts, inp.samples, inp.face_first, refl, *PVS, bounces=bounces,
+    ob = O.Bounce(tree, inp.faces, inp.verts, inp.samples, inp.face_first, refl, *pvs, bounces=bounces,
                   threshold=threshold)
     patches, _ = ob.patches()
-    off, src, w, _ = ob.transfers()
+    off, src, w, rays = ob.transfers()
     total, direct, n, added = ob.run(light)
-    return dict(patches=patches, off=off, src=src, w=w, total=total, direct=direct, bounces=n, last=added)
+    return dict(patches=patches, off=off, src=src, w=w, total=total, direct=direct, bounces=n, last=added,
+                rays=rays)
 
 
-def _device(world, inp, refl, bounces, threshold=1.0):
+def _device(world, inp, refl, bounces, threshold=1.0, pvs=PVS):
     with L.LightingStage(world, inp) as st:
-        st.upload_bounce(refl, *PVS, bounces=bounces, threshold=threshold)
+        st.upload_bounce(refl, *pvs, bounces=bounces, threshold=threshold)
         st.light_pass()
         total, direct = st.patch_light()
         off, tr = st.transfers()
@@ -101,7 +109,7 @@ def _device(world, inp, refl, bounces, threshold=1.0):
         last = st.last_total() if bs.bounces > 0 else None
     patches, _ = L.build_patches(inp.faces, inp.verts, refl)
     return dict(patches=patches, off=off, src=tr["patch"], w=tr["weight"], total=total, direct=direct,
-                bounces=bs.bounces, last=last)
+                bounces=bs.bounces, last=last, rays=bs.transfer_rays, blocked=getattr(bs, "blocked_rays", None))
 
 
 def _leaves(r):
@@ -199,3 +207,50 @@ def test_device_sky_patch_emits_nothing():
     r = _device(world, inp, refl, bounces=100)
     sky = np.flatnonzero(r["patches"]["sky"] != 0)
     assert len(sky) and not r["total"][sky].any()
+
+
+# ---- VisMatrixTests (Tests/MapTools/Rad/Bounce/VisMatrixTests.cs) on the box
+
+def _check_transfer_lists(r):
+    p = r["patches"]
+    counts = np.diff(r["off"])
+    leaves = set(_leaves(r).tolist())
+    assert counts.sum() > 0
+    for j in range(len(p)):
+        if j not in leaves:
+            assert counts[j] == 0, j                 # OnlyClusterChildrenHaveTransfers
+            continue
+        src = r["src"][r["off"][j]:r["off"][j + 1]]
+        assert not (p["face"][src] == p["face"][j]).any(), j   # NoPatchTakesLightFromItsOwnFace
+        acc = np.float32(0)
+        for x in r["w"][r["off"][j]:r["off"][j + 1]]:
+            acc = np.float32(acc + x)
+        assert acc <= np.float32(1.0001), (j, acc)    # EveryListSumsToAtMostOne
+    floor = [j for j in leaves if p["face"][j] == 0]
+    assert all((p["face"][r["src"][r["off"][j]:r["off"][j + 1]]] == 1).any() for j in floor)  # floor sees ceiling
+
+
+def _visibility_cases(run):
+    world, inp, refl = _box()
+    open_ = run(world, inp, refl)
+    _check_transfer_lists(open_)
+    world, inp, refl = _box(occluder=True)
+    shut = run(world, inp, refl)
+    assert len(shut["src"]) < len(open_["src"])       # AnOccluderRemovesTransfers
+    world, inp, refl = _box()
+    none = run(world, inp, refl, pvs=NO_SELF)
+    assert len(none["src"]) == 0 and none["rays"] == 0  # APvsThatExcludesTheClusterMakesNoTransfers
+    return open_
+
+
+def test_oracle_transfer_lists(oracle_mod):
+    _visibility_cases(lambda w, i, r, pvs=PVS: _oracle(oracle_mod, w, i, r, bounces=1, pvs=pvs))
+
+
+@pytest.mark.gpu
+def test_device_transfer_lists(oracle_mod):
+    d = _visibility_cases(lambda w, i, r, pvs=PVS: _device(w, i, r, bounces=1, pvs=pvs))
+    world, inp, refl = _box()
+    o = _oracle(oracle_mod, world, inp, refl, bounces=1)
+    assert np.array_equal(d["off"], o["off"]) and np.array_equal(d["src"], o["src"])
+    assert np.array_equal(d["w"].view(np.uint32), o["w"].view(np.uint32))
