@@ -221,6 +221,8 @@ cudaError_t release_tables(vrad_ctx *ctx) {
     ctx->supersample.release();
     vrad::dev_free(ctx->sample_light);
     ctx->sample_light = nullptr;
+    vrad::dev_free(ctx->sample_light_hdr);
+    ctx->sample_light_hdr = nullptr;
     return cudaSuccess;
 }
 }  // namespace vrad
@@ -294,6 +296,7 @@ int32_t vrad_destroy(vrad_ctx *ctx) {
         ctx->supersample.free_pinned();
         ctx->shelf.release();
         vrad::dev_free(ctx->sample_light);
+        vrad::dev_free(ctx->sample_light_hdr);
         cudaFree(ctx->status);
         cudaFree(ctx->d_rays);
         cudaFree(ctx->d_out);

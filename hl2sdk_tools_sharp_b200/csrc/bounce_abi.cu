@@ -193,19 +193,21 @@ cudaError_t radial_tables(BounceBuffers &b, const float4 *frames, int32_t nf, co
 }  // namespace
 
 // The bounce of one light pass, after the direct gather wrote
-// sample_light: patch light, transfers, bounces to the stop rule.  Leaves
-// the bounced light in b.total.  Blocks on the stream once per bounce (the
-// stop rule is decided on the host).
-cudaError_t run_bounce(vrad_ctx *ctx, cudaStream_t s, std::string &why) {
+// sample_light: patch light, transfers (unless the pass's previous range
+// built them), bounces to the stop rule.  Leaves the bounced light in
+// b.total.  Blocks on the stream once per bounce (the stop rule is decided
+// on the host).
+cudaError_t run_bounce(vrad_ctx *ctx, cudaStream_t s, const float4 *sample_light, bool build_transfers,
+                       std::string &why) {
     BounceBuffers &b = ctx->bounce;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaError_t e = cudaSuccess;
     for (int k = 0; k < 4 && e == cudaSuccess; k++) e = cudaEventCreate(&ev[k]);
     if (e == cudaSuccess) e = cudaEventRecord(ev[0], s);
-    if (e == cudaSuccess) e = launch_patch_light(b, ctx->sample_light, s);
+    if (e == cudaSuccess) e = launch_patch_light(b, sample_light, s);
     if (e == cudaSuccess) e = cudaEventRecord(ev[1], s);
     if (e == cudaSuccess) e = cudaMemsetAsync(b.counters, 0, 3 * sizeof(unsigned long long), s);
-    if (e == cudaSuccess) e = launch_transfers(b, ctx->scene.view(), ctx->status, s, false);
+    if (e == cudaSuccess && build_transfers) e = launch_transfers(b, ctx->scene.view(), ctx->status, s, false);
     if (e == cudaSuccess) e = cudaEventRecord(ev[2], s);
     b.bounces_run = 0;
     b.exact_totals = 0;
@@ -654,11 +656,9 @@ extern "C" int32_t vrad_bounce_upload(vrad_ctx *ctx, const vrad_bounce_desc *d) 
     return VRAD_OK;
 }
 
-extern "C" int32_t vrad_bounce_stats_get(vrad_ctx *ctx, vrad_bounce_stats *st) {
-    if (!ctx || !st) return vrad_fail(ctx, VRAD_ERR_ARG, "null argument");
-    std::lock_guard<std::mutex> g(ctx->mu);
+namespace vrad {
+void fill_bounce_stats(const vrad_ctx *ctx, vrad_bounce_stats *st) {
     const vrad::BounceBuffers &b = ctx->bounce;
-    if (!b.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no bounce uploaded");
     std::memset(st, 0, sizeof *st);
     st->patches = b.npatches;
     st->receivers = b.nreceivers;
@@ -673,6 +673,14 @@ extern "C" int32_t vrad_bounce_stats_get(vrad_ctx *ctx, vrad_bounce_stats *st) {
     st->bounce_ms = b.bounce_ms;
     st->final_ms = b.final_ms;
     st->unsettled_asin = (int64_t)b.open_ties;
+}
+}  // namespace vrad
+
+extern "C" int32_t vrad_bounce_stats_get(vrad_ctx *ctx, vrad_bounce_stats *st) {
+    if (!ctx || !st) return vrad_fail(ctx, VRAD_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (!ctx->bounce.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no bounce uploaded");
+    vrad::fill_bounce_stats(ctx, st);
     return VRAD_OK;
 }
 

@@ -18,6 +18,15 @@
 #include "supersample.cuh"
 #include "sync_wait.h"
 
+namespace vrad {
+// One range's supersampling passes in the last direct gather.
+struct RangeSupersample {
+    int32_t passes_run = 0;
+    int64_t supersampled = 0;
+    float ms = 0.0f;
+};
+}  // namespace vrad
+
 struct vrad_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -37,7 +46,9 @@ struct vrad_ctx {
     size_t d_out_cap = 0;
     vrad::WorldBuffers world;
     vrad::FinalBuffers final_pass;
-    float4 *sample_light = nullptr;  // the direct gather's output, one per sample
+    float4 *sample_light = nullptr;      // the direct gather's output, one per sample (LDR)
+    float4 *sample_light_hdr = nullptr;  // the HDR range's, when the world has an HDR list
+    vrad::RangeSupersample range_ss[2];  // the last gather's supersampling, LDR and HDR
     // Host copies of the uploaded world the bounce set-up reads.
     std::vector<vrad_face> h_faces;
     std::vector<float> h_vertices;
@@ -70,6 +81,7 @@ struct vrad_ctx {
     cudaEvent_t ahead_done = nullptr;
     bool direct_ahead = false;
     int32_t direct_ahead_rc = 0;
+    int32_t ahead_ranges = 0;           // the ranges the gather queued ahead lights
     const vrad_mlp *bounce_model = nullptr;  // the warm start's network, or none
     vrad::SupersampleBuffers supersample;
     std::string supersample_why;     // why the world's samples cannot be supersampled
@@ -82,7 +94,7 @@ struct vrad_ctx {
 
 // The direct gather with its supersampling passes into d_out (direct.cu).
 namespace vrad {
-int32_t direct_pass(vrad_ctx *ctx, float4 *d_out, cudaStream_t s);
+int32_t direct_pass(vrad_ctx *ctx, float4 *ldr_out, float4 *hdr_out, cudaStream_t s);
 
 // After an entry point queued this context's kernels on a caller's stream
 // s: the context's own stream waits for them, so that waiting for the

@@ -41,8 +41,11 @@ namespace {
 // BLOCK threads per CTA (32, 64 or 128, chosen by vrad_direct_autotune):
 // every thread traces its samples' whole light list, so a small CTA frees
 // its SM slot as soon as its own warps are done.
-template <int BLOCK>
+// DUAL: one traversal lights both ranges (out from w.lights, out_hdr from
+// w.lights_hdr).
+template <int BLOCK, bool DUAL>
 __global__ void __launch_bounds__(BLOCK) k_direct(DeviceScene sc, DeviceWorld w, float4 *__restrict__ out,
+                                                  float4 *__restrict__ out_hdr,
                                                   unsigned long long *__restrict__ counters,
                                                   uint32_t *__restrict__ overflow) {
     extern __shared__ int stack_mem[];  // sc.stack_depth() entries per thread
@@ -68,10 +71,13 @@ __global__ void __launch_bounds__(BLOCK) k_direct(DeviceScene sc, DeviceWorld w,
     const float px = __fadd_rn(sp.x, nx), py = __fadd_rn(sp.y, ny), pz = __fadd_rn(sp.z, nz);
 
     unsigned long long vis_rays = 0, sky_rays = 0;
-    const float4 r = gather_point<BLOCK>(sc, w, cluster, px, py, pz, nx, ny, nz, real, gmask, kAllLights, stack,
-                                         overflow, counters, vis_rays, sky_rays);
-    const float ax = r.x, ay = r.y, az = r.z, sun = r.w;
-    if (real) out[si] = make_float4(ax, ay, az, sun);
+    float4 h;
+    const float4 r = gather_point<BLOCK, DUAL>(sc, w, cluster, px, py, pz, nx, ny, nz, real, gmask, kAllLights,
+                                               stack, overflow, counters, vis_rays, sky_rays, &h);
+    if (real) {
+        out[si] = r;
+        if (DUAL) out_hdr[si] = h;
+    }
 
     // Ray counts: one atomic per warp.
     __syncwarp();
@@ -92,34 +98,40 @@ void WorldBuffers::release() {
     dev_free(sample_pos);
     dev_free(face_normal);
     dev_free(lights);
+    dev_free(lights_hdr);
     dev_free(cl_off);
     dev_free(cl_list);
     dev_free(dirs);
     dev_free(jitter);
     dev_free(counters);
     slots = nullptr;
-    sample_pos = face_normal = lights = dirs = jitter = nullptr;
+    sample_pos = face_normal = lights = lights_hdr = dirs = jitter = nullptr;
     cl_off = cl_list = nullptr;
     counters = nullptr;
     view = DeviceWorld{};
     ready = false;
 }
 
-cudaError_t launch_direct(const DeviceScene &scene, const DeviceWorld &world, float4 *out,
+cudaError_t launch_direct(const DeviceScene &scene, const DeviceWorld &world, float4 *out, float4 *out_hdr,
                           unsigned long long *counters, uint32_t *overflow, cudaStream_t stream,
                           int block) {
     if (world.nslots == 0) return cudaSuccess;
+    if (out_hdr && !world.lights_hdr) return cudaErrorInvalidValue;
     const size_t smem = sizeof(int) * (size_t)scene.stack_depth();  // per thread
-    switch (block) {
-        case 32:
-            k_direct<32><<<(unsigned)((world.nslots + 31) / 32), 32, smem * 32, stream>>>(scene, world, out, counters, overflow);
-            break;
-        case 64:
-            k_direct<64><<<(unsigned)((world.nslots + 63) / 64), 64, smem * 64, stream>>>(scene, world, out, counters, overflow);
-            break;
-        default:
-            k_direct<128><<<(unsigned)((world.nslots + 127) / 128), 128, smem * 128, stream>>>(scene, world, out, counters, overflow);
-            break;
+    const unsigned g32 = (unsigned)((world.nslots + 31) / 32), g64 = (unsigned)((world.nslots + 63) / 64),
+                   g128 = (unsigned)((world.nslots + 127) / 128);
+    if (out_hdr) {
+        switch (block) {
+            case 32: k_direct<32, true><<<g32, 32, smem * 32, stream>>>(scene, world, out, out_hdr, counters, overflow); break;
+            case 64: k_direct<64, true><<<g64, 64, smem * 64, stream>>>(scene, world, out, out_hdr, counters, overflow); break;
+            default: k_direct<128, true><<<g128, 128, smem * 128, stream>>>(scene, world, out, out_hdr, counters, overflow); break;
+        }
+    } else {
+        switch (block) {
+            case 32: k_direct<32, false><<<g32, 32, smem * 32, stream>>>(scene, world, out, nullptr, counters, overflow); break;
+            case 64: k_direct<64, false><<<g64, 64, smem * 64, stream>>>(scene, world, out, nullptr, counters, overflow); break;
+            default: k_direct<128, false><<<g128, 128, smem * 128, stream>>>(scene, world, out, nullptr, counters, overflow); break;
+        }
     }
     return cudaGetLastError();
 }
@@ -261,18 +273,35 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
         memcpy(&v.w, &c, 4);
         fnorm[(size_t)f] = v;
     }
-    std::vector<float4> lights((size_t)nl * vrad::kLightF4);
-    for (int32_t l = 0; l < nl; l++) {
-        const vrad_light &s = w->lights[l];
-        float4 *o = &lights[(size_t)l * vrad::kLightF4];
-        int32_t type = s.type, style = s.style;
-        o[0] = make_float4(s.origin[0], s.origin[1], s.origin[2], 0.0f);
-        memcpy(&o[0].w, &type, 4);
-        o[1] = make_float4(s.intensity[0], s.intensity[1], s.intensity[2], 0.0f);
-        memcpy(&o[1].w, &style, 4);
-        o[2] = make_float4(s.normal[0], s.normal[1], s.normal[2], s.exponent);
-        o[3] = make_float4(s.stop_dot, s.stop_dot2, s.constant_attn, s.linear_attn);
-        o[4] = make_float4(s.quadratic_attn, s.start_fade_distance, s.end_fade_distance, s.cap_dist);
+    auto pack = [nl](const vrad_light *src) {
+        std::vector<float4> lights((size_t)nl * vrad::kLightF4);
+        for (int32_t l = 0; l < nl; l++) {
+            const vrad_light &s = src[l];
+            float4 *o = &lights[(size_t)l * vrad::kLightF4];
+            int32_t type = s.type, style = s.style;
+            o[0] = make_float4(s.origin[0], s.origin[1], s.origin[2], 0.0f);
+            memcpy(&o[0].w, &type, 4);
+            o[1] = make_float4(s.intensity[0], s.intensity[1], s.intensity[2], 0.0f);
+            memcpy(&o[1].w, &style, 4);
+            o[2] = make_float4(s.normal[0], s.normal[1], s.normal[2], s.exponent);
+            o[3] = make_float4(s.stop_dot, s.stop_dot2, s.constant_attn, s.linear_attn);
+            o[4] = make_float4(s.quadratic_attn, s.start_fade_distance, s.end_fade_distance, s.cap_dist);
+        }
+        return lights;
+    };
+    const std::vector<float4> lights = pack(w->lights);
+    // The HDR list differs from the LDR one in intensity alone (both come
+    // from the same entities): every other word must match.
+    std::vector<float4> lights_hdr;
+    if (w->lights_hdr) {
+        lights_hdr = pack(w->lights_hdr);
+        for (int32_t l = 0; l < nl; l++)
+            for (int k = 0; k < vrad::kLightF4; k++) {
+                const float4 &a = lights[(size_t)l * vrad::kLightF4 + k], &b = lights_hdr[(size_t)l * vrad::kLightF4 + k];
+                const bool intensity = k == 1;
+                if ((!intensity && memcmp(&a, &b, sizeof a) != 0) || (intensity && memcmp(&a.w, &b.w, 4) != 0))
+                    return vrad_fail(ctx, VRAD_ERR_ARG, "HDR light %d differs from the LDR light in more than intensity", l);
+            }
     }
     std::vector<int32_t> cl_off(w->cluster_light_offsets, w->cluster_light_offsets + w->nclusters + 1);
     std::vector<int32_t> cl_list(w->cluster_lights, w->cluster_lights + total);
@@ -294,6 +323,8 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     if (e == cudaSuccess) e = vrad::dma_table(&wb.sample_pos, pos, (size_t)w->nsamples, ctx->stream);
     if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.face_normal, fnorm);
     if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.lights, lights);
+    if (e == cudaSuccess && !lights_hdr.empty())
+        e = vrad::stage_table(ctx->stager, ctx->stream, &wb.lights_hdr, lights_hdr);
     if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.cl_off, cl_off);
     if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.cl_list, cl_list);
     if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.dirs, dirs);
@@ -306,7 +337,8 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     }
     wb.view = vrad::DeviceWorld{wb.slots, (int64_t)slots.size(), wb.sample_pos, wb.face_normal, wb.lights, nl,
                                 wb.cl_off, wb.cl_list, w->nclusters, wb.dirs, w->nsky_directions, wb.jitter,
-                                w->nsun_jitter, w->sun_angular_extent, w->sun_samples, w->nsamples};
+                                w->nsun_jitter, w->sun_angular_extent, w->sun_samples, w->nsamples,
+                                wb.lights_hdr};
     clock.mark("world buffers");
     // The final pass's tables, and the direct gather's output buffer.  A
     // new world drops the old bounce.
@@ -342,6 +374,8 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     ctx->final_pass.release();
     vrad::dev_free(ctx->sample_light);
     ctx->sample_light = nullptr;
+    vrad::dev_free(ctx->sample_light_hdr);
+    ctx->sample_light_hdr = nullptr;
     clock.mark("host copies");
     if (w->vertices && w->nvertices > 0) {
         std::string why;
@@ -373,6 +407,8 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
         ctx->supersample_why = "the world was uploaded without face windings";
     }
     e = vrad::dev_alloc(&ctx->sample_light, sizeof(float4) * (size_t)(w->nsamples ? w->nsamples : 1));
+    if (e == cudaSuccess && wb.lights_hdr)
+        e = vrad::dev_alloc(&ctx->sample_light_hdr, sizeof(float4) * (size_t)(w->nsamples ? w->nsamples : 1));
     if (e != cudaSuccess) {
         ctx->stager.finish(ctx->stream);  // no copy in flight into a released block
         wb.release();
@@ -392,20 +428,40 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
 
 namespace {
 
-int32_t direct_on(vrad_ctx *ctx, float4 *d_out, cudaStream_t s) {
+// The direct gather with its supersampling passes: LDR into ldr_out, HDR
+// into hdr_out (either may be null, not both).  With both, the first round
+// is one traversal for the two ranges; each range then has its own
+// supersampling passes (their selections follow each range's gradients).
+int32_t direct_on(vrad_ctx *ctx, float4 *ldr_out, float4 *hdr_out, cudaStream_t s) {
     if (!ctx->has_scene) return vrad_fail(ctx, VRAD_ERR_NO_SCENE, "no scene uploaded");
     if (!ctx->world.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no lighting world uploaded");
-    cudaError_t e = cudaMemsetAsync(ctx->world.counters, 0, 3 * sizeof(unsigned long long), s);
-    if (e == cudaSuccess)
-        e = vrad::launch_direct(ctx->scene.view(), ctx->world.view, d_out, ctx->world.counters, ctx->status, s,
-                                ctx->world.block);
-    // The supersampling passes (FaceLightJob's rounds after the first).
-    if (e == cudaSuccess && ctx->supersample.extra_passes > 0 && !ctx->supersample.ready && ctx->world.view.nsamples)
+    if (hdr_out && !ctx->world.view.lights_hdr)
+        return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without an HDR light list");
+    if (ctx->supersample.extra_passes > 0 && !ctx->supersample.ready && ctx->world.view.nsamples)
         return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "supersampling: %s (vrad_set_extra_passes 0 turns it off)",
                          ctx->supersample_why.c_str());
-    if (e == cudaSuccess)
-        e = vrad::run_supersample(ctx->supersample, ctx->scene.view(), ctx->world.view, ctx->final_pass.view, d_out,
+    const vrad::DeviceWorld ldr = vrad::range_view(ctx->world.view, false);
+    const vrad::DeviceWorld hdr = hdr_out ? vrad::range_view(ctx->world.view, true) : ldr;
+    cudaError_t e = cudaMemsetAsync(ctx->world.counters, 0, 3 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess) {
+        if (ldr_out && hdr_out)
+            e = vrad::launch_direct(ctx->scene.view(), ctx->world.view, ldr_out, hdr_out, ctx->world.counters,
+                                    ctx->status, s, ctx->world.block);
+        else
+            e = vrad::launch_direct(ctx->scene.view(), ldr_out ? ldr : hdr, ldr_out ? ldr_out : hdr_out, nullptr,
+                                    ctx->world.counters, ctx->status, s, ctx->world.block);
+    }
+    // The supersampling passes (FaceLightJob's rounds after the first),
+    // per range.
+    for (int r = 0; r < 2; r++) {
+        float4 *out = r == 0 ? ldr_out : hdr_out;
+        vrad::SupersampleBuffers &ss = ctx->supersample;
+        ctx->range_ss[r] = vrad::RangeSupersample{};
+        if (!out || e != cudaSuccess) continue;
+        e = vrad::run_supersample(ss, ctx->scene.view(), r == 0 ? ldr : hdr, ctx->final_pass.view, out,
                                   ctx->world.counters, ctx->status, s);
+        ctx->range_ss[r] = vrad::RangeSupersample{ss.passes_run, ss.supersampled, ss.ms};
+    }
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "direct lighting launch");
     return VRAD_OK;
 }
@@ -419,12 +475,14 @@ void start_direct_ahead(vrad_ctx *ctx) {
     const cudaStream_t s = ctx->pass_stream ? ctx->pass_stream : ctx->ahead_stream;
     ctx->direct_ahead = true;
     ctx->direct_ahead_rc = VRAD_ERR_CUDA;
+    // Every range the world has: a world with an HDR list is lit in both.
+    ctx->ahead_ranges = VRAD_RANGE_LDR | (ctx->sample_light_hdr ? VRAD_RANGE_HDR : 0);
     ctx->direct_thread = std::thread([ctx, s]() {
         // The thread sleeps in its waits: its core goes to the bounce
         // upload's host work meanwhile.
         set_sleeping_waits(true);
         int32_t rc = cudaSetDevice(ctx->device) == cudaSuccess && cudaEventRecord(ctx->ahead_start, s) == cudaSuccess
-                         ? direct_on(ctx, ctx->sample_light, s)
+                         ? direct_on(ctx, ctx->sample_light, ctx->sample_light_hdr, s)
                          : VRAD_ERR_CUDA;
         if (rc == VRAD_OK && cudaEventRecord(ctx->ahead_done, s) != cudaSuccess) rc = VRAD_ERR_CUDA;
         ctx->direct_ahead_rc = rc;
@@ -434,8 +492,11 @@ void start_direct_ahead(vrad_ctx *ctx) {
 }  // namespace vrad
 
 namespace vrad {
-// The direct gather with its supersampling passes (the light pass's first step).
-int32_t direct_pass(vrad_ctx *ctx, float4 *d_out, cudaStream_t s) { return direct_on(ctx, d_out, s); }
+// The direct gather with its supersampling passes (the light pass's first
+// step), for the ranges whose outputs are given.
+int32_t direct_pass(vrad_ctx *ctx, float4 *ldr_out, float4 *hdr_out, cudaStream_t s) {
+    return direct_on(ctx, ldr_out, hdr_out, s);
+}
 }  // namespace vrad
 
 extern "C" int32_t vrad_direct_lighting_device(vrad_ctx *ctx, vrad_lighting_value *d_out, void *stream) {
@@ -445,7 +506,7 @@ extern "C" int32_t vrad_direct_lighting_device(vrad_ctx *ctx, vrad_lighting_valu
     vrad::settle_direct(ctx);
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
-    const int32_t rc = direct_on(ctx, reinterpret_cast<float4 *>(d_out), (cudaStream_t)stream);
+    const int32_t rc = direct_on(ctx, reinterpret_cast<float4 *>(d_out), nullptr, (cudaStream_t)stream);
     e = vrad::join_stream(ctx, (cudaStream_t)stream);
     return rc != VRAD_OK || e == cudaSuccess ? rc : vrad_cuda_fail(ctx, e, "joining the caller's stream");
 }
@@ -468,7 +529,7 @@ extern "C" int32_t vrad_direct_lighting(vrad_ctx *ctx, vrad_lighting_value *out,
         if (a) cudaEventDestroy(a);
         return vrad_cuda_fail(ctx, e, "direct lighting set-up");
     }
-    int32_t rc = direct_on(ctx, d_out, ctx->stream);
+    int32_t rc = direct_on(ctx, d_out, nullptr, ctx->stream);
     unsigned long long counts[2] = {0, 0};
     uint32_t overflow = 0;
     if (rc == VRAD_OK) {
@@ -510,9 +571,13 @@ extern "C" int32_t vrad_direct_autotune(vrad_ctx *ctx, int32_t *chosen_block, fl
     if (!ctx->world.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no lighting world uploaded");
     cudaError_t e = cudaSetDevice(ctx->device);
     const int64_t n = ctx->world.view.nsamples;
-    float4 *d_out = nullptr;
+    float4 *d_out = nullptr, *d_hdr = nullptr;
     cudaEvent_t a = nullptr, b = nullptr;
+    // A world with an HDR list is gathered for both ranges at once: the
+    // shape is tuned on that kernel.
+    const bool dual = ctx->world.view.lights_hdr != nullptr;
     if (e == cudaSuccess) e = vrad::dev_alloc(&d_out, sizeof(float4) * (size_t)(n ? n : 1));
+    if (e == cudaSuccess && dual) e = vrad::dev_alloc(&d_hdr, sizeof(float4) * (size_t)(n ? n : 1));
     if (e == cudaSuccess) e = cudaEventCreate(&a);
     if (e == cudaSuccess) e = cudaEventCreate(&b);
     const int candidates[3] = {32, 64, 128};
@@ -521,8 +586,8 @@ extern "C" int32_t vrad_direct_autotune(vrad_ctx *ctx, int32_t *chosen_block, fl
     for (int k = 0; k < 3 && e == cudaSuccess; k++) {
         e = cudaEventRecord(a, ctx->stream);
         if (e == cudaSuccess)
-            e = vrad::launch_direct(ctx->scene.view(), ctx->world.view, d_out, ctx->world.counters, ctx->status,
-                                    ctx->stream, candidates[k]);
+            e = vrad::launch_direct(ctx->scene.view(), dual ? ctx->world.view : vrad::range_view(ctx->world.view, false),
+                                    d_out, d_hdr, ctx->world.counters, ctx->status, ctx->stream, candidates[k]);
         if (e == cudaSuccess) e = cudaEventRecord(b, ctx->stream);
         if (e == cudaSuccess) e = cudaEventSynchronize(b);
         float ms = 0.0f;
@@ -534,6 +599,7 @@ extern "C" int32_t vrad_direct_autotune(vrad_ctx *ctx, int32_t *chosen_block, fl
         }
     }
     vrad::dev_free(d_out);
+    vrad::dev_free(d_hdr);
     if (a) cudaEventDestroy(a);
     if (b) cudaEventDestroy(b);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "direct autotune");

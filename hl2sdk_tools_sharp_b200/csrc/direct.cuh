@@ -16,6 +16,8 @@
 //                   (origin, type) (intensity, style) (normal, exponent)
 //                   (stop_dot, stop_dot2, constant, linear)
 //                   (quadratic, start_fade, end_fade, cap_dist)
+//   lights_hdr[l]   the same 5 x float4 for the HDR range (intensity the
+//                   only difference), or null for a world without one
 //   cl_off, cl_list per-cluster light lists in gather order (CSR)
 //   dirs[d]         float4 sky-ambient directions; jitter[d] sun jitter
 #pragma once
@@ -47,6 +49,7 @@ struct DeviceWorld {
     float sun_extent;
     int32_t sun_samples;
     int64_t nsamples;
+    const float4 *lights_hdr;  // null: the world has one range
 };
 
 struct WorldBuffers {
@@ -54,6 +57,7 @@ struct WorldBuffers {
     float4 *sample_pos = nullptr;
     float4 *face_normal = nullptr;
     float4 *lights = nullptr;
+    float4 *lights_hdr = nullptr;
     int32_t *cl_off = nullptr;
     int32_t *cl_list = nullptr;
     float4 *dirs = nullptr;
@@ -67,8 +71,18 @@ struct WorldBuffers {
 };
 
 // Launches the fused gather: out[i] = (lighting xyz, direct sun amount).
-cudaError_t launch_direct(const DeviceScene &scene, const DeviceWorld &world, float4 *out,
+// With out_hdr (and world.lights_hdr) one traversal lights both ranges:
+// out from world.lights, out_hdr from world.lights_hdr.
+cudaError_t launch_direct(const DeviceScene &scene, const DeviceWorld &world, float4 *out, float4 *out_hdr,
                           unsigned long long *counters, uint32_t *overflow, cudaStream_t stream,
                           int block);
+
+// The world as one range sees it: lights = that range's table, no second.
+inline DeviceWorld range_view(const DeviceWorld &w, bool hdr) {
+    DeviceWorld v = w;
+    if (hdr) v.lights = w.lights_hdr;
+    v.lights_hdr = nullptr;
+    return v;
+}
 
 }  // namespace vrad

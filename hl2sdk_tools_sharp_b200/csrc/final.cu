@@ -24,9 +24,11 @@
 
 #include <cub/device/device_scan.cuh>
 
+#include <algorithm>
 #include <atomic>
 #include <cfloat>
 #include <climits>
+#include <cstring>
 #include <vector>
 
 #include <string>
@@ -602,39 +604,174 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
 
 namespace {
 
-// ahead: the direct gather already ran (queued at the world upload), its
-// end marked by ctx->ahead_done.
-int32_t pass_on(vrad_ctx *ctx, uint8_t *d_lighting, cudaStream_t s, cudaEvent_t mid, cudaEvent_t bounce_mark,
-                bool ahead = false) {
+// One light pass's events: its start, the end of the direct gather, and
+// per range the end of its bounce and of its final pass.
+struct PassEvents {
+    cudaEvent_t start = nullptr, direct = nullptr, bounce[2] = {nullptr, nullptr}, final_[2] = {nullptr, nullptr};
+    cudaError_t create() {
+        cudaError_t e = cudaSuccess;
+        for (cudaEvent_t *x : {&start, &direct, &bounce[0], &bounce[1], &final_[0], &final_[1]})
+            if (e == cudaSuccess) e = cudaEventCreate(x);
+        return e;
+    }
+    ~PassEvents() {
+        for (cudaEvent_t x : {start, direct, bounce[0], bounce[1], final_[0], final_[1]})
+            if (x) cudaEventDestroy(x);
+    }
+};
+
+// The light pass for `ranges` (VRAD_RANGE_*) on stream s: the direct
+// gather (or, with ahead, the one queued at the world upload, its end
+// marked by ctx->ahead_done), then per range, LDR first, its bounce (the
+// first range builds the transfers, the second reuses them) and its final
+// pass into d_out[range].  ev (nullable) marks the steps; bstats
+// (nullable, two records) receives each range's bounce statistics.
+int32_t pass_on(vrad_ctx *ctx, int32_t ranges, uint8_t *d_ldr, uint8_t *d_hdr, cudaStream_t s, PassEvents *ev,
+                vrad_bounce_stats *bstats, bool ahead = false) {
     if (!ctx->has_scene) return vrad_fail(ctx, VRAD_ERR_NO_SCENE, "no scene uploaded");
     if (!ctx->world.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no lighting world uploaded");
     if (!ctx->final_pass.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without face windings");
+    if ((ranges & VRAD_RANGE_HDR) && !ctx->sample_light_hdr)
+        return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without an HDR light list");
     vrad::FinalBuffers &fb = ctx->final_pass;
     cudaError_t e = cudaSuccess;
-    if (ahead) {
+    if (ev) e = cudaEventRecord(ev->start, s);
+    if (e == cudaSuccess && ahead) {
         e = cudaStreamWaitEvent(s, ctx->ahead_done, 0);
         if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "joining the direct gather");
-    } else {
-        const int32_t rc = vrad::direct_pass(ctx, ctx->sample_light, s);
+    } else if (e == cudaSuccess) {
+        const int32_t rc = vrad::direct_pass(ctx, (ranges & VRAD_RANGE_LDR) ? ctx->sample_light : nullptr,
+                                             (ranges & VRAD_RANGE_HDR) ? ctx->sample_light_hdr : nullptr, s);
         if (rc != VRAD_OK) return rc;
     }
-    if (e == cudaSuccess && mid) e = cudaEventRecord(mid, s);
-    // The bounce (patch light, transfers, bounces), when one is uploaded.
-    vrad::PatchRadialView prad{};
+    if (e == cudaSuccess && ev) e = cudaEventRecord(ev->direct, s);
     const bool bounce = vrad::bounce_active(ctx);
-    if (e == cudaSuccess && bounce) {
-        std::string why;
-        e = vrad::run_bounce(ctx, s, why);
-        if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, why.c_str());
-        prad = vrad::patch_radial_view(ctx);
+    bool built = false;
+    for (int r = 0; r < 2 && e == cudaSuccess; r++) {
+        if (bstats) std::memset(&bstats[r], 0, sizeof bstats[r]);
+        if (!(ranges & (1 << r))) continue;
+        const float4 *light = r == 0 ? ctx->sample_light : ctx->sample_light_hdr;
+        uint8_t *out = r == 0 ? d_ldr : d_hdr;
+        // The bounce (patch light, transfers, bounces), when one is uploaded.
+        vrad::PatchRadialView prad{};
+        if (bounce) {
+            std::string why;
+            e = vrad::run_bounce(ctx, s, light, !built, why);
+            if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, why.c_str());
+            built = true;
+            prad = vrad::patch_radial_view(ctx);
+            if (bstats) vrad::fill_bounce_stats(ctx, &bstats[r]);
+        }
+        if (e == cudaSuccess && ev) e = cudaEventRecord(ev->bounce[r], s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(out, 0, (size_t)fb.lighting_bytes, s);
+        if (e == cudaSuccess)
+            e = vrad::launch_final(fb.view, light, fb.rad_light, fb.rad_weight, fb.flat, out, fb.nfaces,
+                                   bounce ? &prad : nullptr, s);
+        if (e == cudaSuccess && ev) e = cudaEventRecord(ev->final_[r], s);
     }
-    if (e == cudaSuccess && bounce_mark) e = cudaEventRecord(bounce_mark, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d_lighting, 0, (size_t)fb.lighting_bytes, s);
-    if (e == cudaSuccess)
-        e = vrad::launch_final(fb.view, ctx->sample_light, fb.rad_light, fb.rad_weight, fb.flat, d_lighting, fb.nfaces,
-                               bounce ? &prad : nullptr, s);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "light pass launch");
     return VRAD_OK;
+}
+
+// The device-buffer pass: always gathers (the gather queued ahead is
+// dropped).
+int32_t pass_device(vrad_ctx *ctx, int32_t ranges, uint8_t *d_ldr, uint8_t *d_hdr, void *stream) {
+    if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
+    if (ranges < 1 || ranges > 3) return vrad_fail(ctx, VRAD_ERR_ARG, "ranges %d is not LDR, HDR or both", ranges);
+    for (int r = 0; r < 2; r++) {
+        uint8_t *d = r == 0 ? d_ldr : d_hdr;
+        if ((ranges & (1 << r)) && (!d || ((uintptr_t)d & 3)))
+            return vrad_fail(ctx, VRAD_ERR_ARG, "lighting buffer null or not 4-byte aligned");
+    }
+    std::lock_guard<std::mutex> g(ctx->mu);
+    vrad::settle_direct(ctx);
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
+    const int32_t rc = pass_on(ctx, ranges, d_ldr, d_hdr, (cudaStream_t)stream, nullptr, nullptr);
+    e = vrad::join_stream(ctx, (cudaStream_t)stream);
+    return rc != VRAD_OK || e == cudaSuccess ? rc : vrad_cuda_fail(ctx, e, "joining the caller's stream");
+}
+
+// The host-buffer pass: takes the gather queued ahead when it lit every
+// range asked for.
+int32_t pass_host(vrad_ctx *ctx, int32_t ranges, uint8_t *ldr, int64_t ldr_capacity, uint8_t *hdr,
+                  int64_t hdr_capacity, int32_t *lightofs, vrad_pass_stats *stats, vrad_bounce_stats *bstats) {
+    if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
+    if (ranges < 1 || ranges > 3) return vrad_fail(ctx, VRAD_ERR_ARG, "ranges %d is not LDR, HDR or both", ranges);
+    std::lock_guard<std::mutex> g(ctx->mu);
+    // The direct gather the world upload queued ahead, when there is one.
+    const bool ahead = vrad::settle_direct(ctx) && (ctx->ahead_ranges & ranges) == ranges;
+    vrad::FinalBuffers &fb = ctx->final_pass;
+    if (!fb.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without face windings");
+    for (int r = 0; r < 2; r++) {
+        if (!(ranges & (1 << r))) continue;
+        const uint8_t *h = r == 0 ? ldr : hdr;
+        const int64_t cap = r == 0 ? ldr_capacity : hdr_capacity;
+        if (!h || cap < fb.lighting_bytes)
+            return vrad_fail(ctx, VRAD_ERR_ARG, "the %s lump needs %lld bytes, %lld given",
+                             r == 0 ? "LIGHTING" : "LIGHTING_HDR", (long long)fb.lighting_bytes, (long long)cap);
+    }
+    cudaError_t e = cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->pass_stream ? ctx->pass_stream : ctx->stream;
+    uint8_t *d_out[2] = {nullptr, nullptr};
+    PassEvents ev;
+    for (int r = 0; r < 2 && e == cudaSuccess; r++)
+        if (ranges & (1 << r)) e = vrad::dev_alloc(&d_out[r], (size_t)(fb.lighting_bytes ? fb.lighting_bytes : 4));
+    if (e == cudaSuccess) e = ev.create();
+    int32_t rc = e == cudaSuccess ? pass_on(ctx, ranges, d_out[0], d_out[1], s, &ev, bstats, ahead)
+                                  : vrad_cuda_fail(ctx, e, "light pass set-up");
+    unsigned long long counts[2] = {0, 0};
+    uint32_t overflow = 0;
+    if (rc == VRAD_OK) {
+        for (int r = 0; r < 2 && e == cudaSuccess; r++)
+            if (ranges & (1 << r))
+                e = cudaMemcpyAsync(r == 0 ? ldr : hdr, d_out[r], (size_t)fb.lighting_bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(counts, ctx->world.counters, sizeof counts, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&overflow, ctx->status, sizeof overflow, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = vrad::wait_stream(s);
+        if (e != cudaSuccess) rc = vrad_cuda_fail(ctx, e, "light pass");
+    }
+    if (rc == VRAD_OK && overflow) {
+        cudaMemsetAsync(ctx->status, 0, sizeof(uint32_t), s);
+        rc = vrad_fail(ctx, VRAD_ERR_CUDA, "traversal stack overflow (BVH deeper than %d)", vrad::kStackDepth);
+    }
+    if (rc == VRAD_OK) {
+        float final_ms[2] = {0.0f, 0.0f};
+        for (int r = 0; r < 2; r++)
+            if (ranges & (1 << r)) cudaEventElapsedTime(&final_ms[r], ev.bounce[r], ev.final_[r]);
+        ctx->bounce.final_ms = (ranges & VRAD_RANGE_HDR) ? final_ms[1] : final_ms[0];
+        if (bstats)
+            for (int r = 0; r < 2; r++) bstats[r].final_ms = final_ms[r];
+        if (lightofs)
+            for (int32_t f = 0; f < fb.nfaces; f++) lightofs[f] = fb.lightofs[(size_t)f];
+        if (stats) {
+            float d_ms = 0.0f;
+            // The gather's own device time, also when it ran ahead.
+            if (ahead) cudaEventElapsedTime(&d_ms, ctx->ahead_start, ctx->ahead_done);
+            else cudaEventElapsedTime(&d_ms, ev.start, ev.direct);
+            std::memset(stats, 0, sizeof *stats);
+            stats->samples = ctx->world.view.nsamples;
+            stats->luxels = fb.view.ncells;
+            stats->visibility_rays = (int64_t)counts[0];
+            stats->sky_rays = (int64_t)counts[1];
+            stats->lighting_bytes = fb.lighting_bytes;
+            stats->direct_ms = d_ms;
+            stats->final_ms = final_ms[0] + final_ms[1];
+            for (int r = 0; r < 2; r++) {
+                if (!(ranges & (1 << r))) continue;
+                stats->extra_passes_run = std::max(stats->extra_passes_run, ctx->range_ss[r].passes_run);
+                stats->supersampled += ctx->range_ss[r].supersampled;
+                stats->supersample_ms += ctx->range_ss[r].ms;
+            }
+        }
+    }
+    if (rc != VRAD_OK) vrad::wait_stream(s);  // no kernel still writes the lumps
+    if (s != ctx->stream) vrad::join_stream(ctx, s);
+    vrad::dev_free(d_out[0]);
+    vrad::dev_free(d_out[1]);
+    return rc;
 }
 
 }  // namespace
@@ -648,86 +785,36 @@ extern "C" int32_t vrad_lighting_size(vrad_ctx *ctx, int64_t *bytes) {
 }
 
 extern "C" int32_t vrad_light_pass_device(vrad_ctx *ctx, uint8_t *d_lighting, void *stream) {
-    if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
-    if (!d_lighting || ((uintptr_t)d_lighting & 3)) return vrad_fail(ctx, VRAD_ERR_ARG, "lighting buffer null or not 4-byte aligned");
-    std::lock_guard<std::mutex> g(ctx->mu);
-    vrad::settle_direct(ctx);  // this entry point always gathers
-    cudaError_t e = cudaSetDevice(ctx->device);
-    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
-    const int32_t rc = pass_on(ctx, d_lighting, (cudaStream_t)stream, nullptr, nullptr);
-    e = vrad::join_stream(ctx, (cudaStream_t)stream);
-    return rc != VRAD_OK || e == cudaSuccess ? rc : vrad_cuda_fail(ctx, e, "joining the caller's stream");
+    return pass_device(ctx, VRAD_RANGE_LDR, d_lighting, nullptr, stream);
 }
 
 extern "C" int32_t vrad_light_pass(vrad_ctx *ctx, uint8_t *lighting, int64_t capacity, int32_t *lightofs,
                                    vrad_pass_stats *stats) {
+    return pass_host(ctx, VRAD_RANGE_LDR, lighting, capacity, nullptr, 0, lightofs, stats, nullptr);
+}
+
+extern "C" int32_t vrad_light_pass_ranges(vrad_ctx *ctx, int32_t ranges, uint8_t *ldr, int64_t ldr_capacity,
+                                          uint8_t *hdr, int64_t hdr_capacity, int32_t *lightofs,
+                                          vrad_pass_stats *stats, vrad_bounce_stats *bounce_stats) {
+    return pass_host(ctx, ranges, ldr, ldr_capacity, hdr, hdr_capacity, lightofs, stats, bounce_stats);
+}
+
+extern "C" int32_t vrad_light_pass_ranges_device(vrad_ctx *ctx, int32_t ranges, uint8_t *d_ldr, uint8_t *d_hdr,
+                                                 void *stream) {
+    return pass_device(ctx, ranges, d_ldr, d_hdr, stream);
+}
+
+extern "C" int32_t vrad_pass_sample_light(vrad_ctx *ctx, int32_t range, vrad_lighting_value *out, int64_t n) {
     if (!ctx) return vrad_fail(nullptr, VRAD_ERR_ARG, "null context");
+    if (range != VRAD_RANGE_LDR && range != VRAD_RANGE_HDR) return vrad_fail(ctx, VRAD_ERR_ARG, "range %d", range);
     std::lock_guard<std::mutex> g(ctx->mu);
-    // The direct gather the world upload queued ahead, when there is one.
-    const bool ahead = vrad::settle_direct(ctx);
-    vrad::FinalBuffers &fb = ctx->final_pass;
-    if (!fb.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without face windings");
-    if (!lighting || capacity < fb.lighting_bytes)
-        return vrad_fail(ctx, VRAD_ERR_ARG, "the LIGHTING lump needs %lld bytes, %lld given", (long long)fb.lighting_bytes,
-                         (long long)capacity);
+    vrad::settle_direct(ctx);
+    const float4 *src = range == VRAD_RANGE_LDR ? ctx->sample_light : ctx->sample_light_hdr;
+    if (!ctx->world.ready || !src) return vrad_fail(ctx, VRAD_ERR_ARG, "no light pass of that range");
+    if (!out || n != ctx->world.view.nsamples)
+        return vrad_fail(ctx, VRAD_ERR_ARG, "%lld samples, %lld asked", (long long)ctx->world.view.nsamples, (long long)n);
     cudaError_t e = cudaSetDevice(ctx->device);
-    cudaStream_t s = ctx->pass_stream ? ctx->pass_stream : ctx->stream;
-    uint8_t *d_lighting = nullptr;
-    cudaEvent_t a = nullptr, m = nullptr, bm = nullptr, b = nullptr;
-    if (e == cudaSuccess) e = vrad::dev_alloc(&d_lighting, (size_t)(fb.lighting_bytes ? fb.lighting_bytes : 4));
-    if (e == cudaSuccess) e = cudaEventCreate(&a);
-    if (e == cudaSuccess) e = cudaEventCreate(&m);
-    if (e == cudaSuccess) e = cudaEventCreate(&bm);
-    if (e == cudaSuccess) e = cudaEventCreate(&b);
-    if (e == cudaSuccess) e = cudaEventRecord(a, s);
-    int32_t rc = e == cudaSuccess ? pass_on(ctx, d_lighting, s, m, bm, ahead) : vrad_cuda_fail(ctx, e, "light pass set-up");
-    unsigned long long counts[2] = {0, 0};
-    uint32_t overflow = 0;
-    if (rc == VRAD_OK) {
-        e = cudaEventRecord(b, s);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(lighting, d_lighting, (size_t)fb.lighting_bytes, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(counts, ctx->world.counters, sizeof counts, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(&overflow, ctx->status, sizeof overflow, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = vrad::wait_stream(s);
-        if (e != cudaSuccess) rc = vrad_cuda_fail(ctx, e, "light pass");
-    }
-    if (rc == VRAD_OK && overflow) {
-        cudaMemsetAsync(ctx->status, 0, sizeof(uint32_t), s);
-        rc = vrad_fail(ctx, VRAD_ERR_CUDA, "traversal stack overflow (BVH deeper than %d)", vrad::kStackDepth);
-    }
-    if (rc == VRAD_OK) {
-        float f_ms = 0.0f;
-        cudaEventElapsedTime(&f_ms, bm, b);
-        ctx->bounce.final_ms = f_ms;
-        if (lightofs)
-            for (int32_t f = 0; f < fb.nfaces; f++) lightofs[f] = fb.lightofs[(size_t)f];
-        if (stats) {
-            float d_ms = 0.0f, f_ms = 0.0f;
-            // The gather's own device time, also when it ran ahead.
-            if (ahead) cudaEventElapsedTime(&d_ms, ctx->ahead_start, ctx->ahead_done);
-            else cudaEventElapsedTime(&d_ms, a, m);
-            cudaEventElapsedTime(&f_ms, bm, b);
-            stats->samples = ctx->world.view.nsamples;
-            stats->luxels = fb.view.ncells;
-            stats->visibility_rays = (int64_t)counts[0];
-            stats->sky_rays = (int64_t)counts[1];
-            stats->lighting_bytes = fb.lighting_bytes;
-            stats->direct_ms = d_ms;
-            stats->final_ms = f_ms;
-            stats->extra_passes_run = ctx->supersample.passes_run;
-            stats->supersampled = ctx->supersample.supersampled;
-            stats->supersample_ms = ctx->supersample.ms;
-        }
-    }
-    if (rc != VRAD_OK) vrad::wait_stream(s);  // no kernel still writes the lump
-    if (s != ctx->stream) vrad::join_stream(ctx, s);
-    vrad::dev_free(d_lighting);
-    if (a) cudaEventDestroy(a);
-    if (m) cudaEventDestroy(m);
-    if (bm) cudaEventDestroy(bm);
-    if (b) cudaEventDestroy(b);
-    return rc;
+    if (e == cudaSuccess) e = vrad::quiesce(ctx);
+    if (e == cudaSuccess && n) e = cudaMemcpy(out, src, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? VRAD_OK : vrad_cuda_fail(ctx, e, "sample light");
 }

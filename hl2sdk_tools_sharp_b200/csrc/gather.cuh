@@ -93,14 +93,19 @@ enum : int { kAllLights = 0, kAmbientOnly = 1, kDirectOnly = 2 };
 
 // The light of one point (px, py, pz already one unit off the face, flat
 // normal n): (lighting xyz, direct sun amount).  Lanes with real = false
-// follow the group's decisions but trace nothing and add nothing.
-template <int BLOCK>
+// follow the group's decisions but trace nothing and add nothing.  With
+// DUAL the same segments also light the HDR range: `second` receives its
+// value from w.lights_hdr's intensities (every decision and every traced
+// segment is the range-independent one, so each range gets its own pass's
+// bits).
+template <int BLOCK, bool DUAL = false>
 __device__ __forceinline__ float4 gather_point(const DeviceScene &sc, const DeviceWorld &w, int cluster, float px,
                                                float py, float pz, float nx, float ny, float nz, bool real,
                                                unsigned gmask, int filter, int *stack, uint32_t *overflow,
                                                unsigned long long *counters, unsigned long long &vis_rays,
-                                               unsigned long long &sky_rays) {
+                                               unsigned long long &sky_rays, float4 *second = nullptr) {
     float ax = 0.0f, ay = 0.0f, az = 0.0f, sun = 0.0f;
+    float hx = 0.0f, hy = 0.0f, hz = 0.0f;
 
     const int l0 = __ldg(&w.cl_off[cluster]), l1 = __ldg(&w.cl_off[cluster + 1]);
     for (int k = l0; k < l1; k++) {
@@ -234,8 +239,15 @@ __device__ __forceinline__ float4 gather_point(const DeviceScene &sc, const Devi
             ay = __fadd_rn(ay, __fmul_rn(fx, B.y));
             az = __fadd_rn(az, __fmul_rn(fx, B.z));
             sun = __fadd_rn(sun, sun_amount);
+            if (DUAL) {
+                const float4 H = __ldg(w.lights_hdr + kLightF4 * li + 1);
+                hx = __fadd_rn(hx, __fmul_rn(fx, H.x));
+                hy = __fadd_rn(hy, __fmul_rn(fx, H.y));
+                hz = __fadd_rn(hz, __fmul_rn(fx, H.z));
+            }
         }
     }
+    if (DUAL) *second = make_float4(hx, hy, hz, sun);
     return make_float4(ax, ay, az, sun);
 }
 

@@ -70,7 +70,8 @@ class _WorldDesc(ctypes.Structure):
                 ("nclusters", ctypes.c_int32), ("sky_directions", ctypes.c_void_p),
                 ("nsky_directions", ctypes.c_int32), ("sun_jitter", ctypes.c_void_p),
                 ("nsun_jitter", ctypes.c_int32), ("sun_angular_extent", ctypes.c_float),
-                ("sun_samples", ctypes.c_int32), ("vertices", ctypes.c_void_p), ("nvertices", ctypes.c_int64)]
+                ("sun_samples", ctypes.c_int32), ("vertices", ctypes.c_void_p), ("nvertices", ctypes.c_int64),
+                ("lights_hdr", ctypes.c_void_p)]
 
 
 class PassStats(ctypes.Structure):
@@ -124,6 +125,13 @@ def _lib():
         lib.vrad_light_pass.restype = i32
         lib.vrad_light_pass_device.argtypes = [P, P, P]
         lib.vrad_light_pass_device.restype = i32
+        lib.vrad_light_pass_ranges.argtypes = [P, i32, P, i64, P, i64, P, ctypes.POINTER(PassStats),
+                                               ctypes.POINTER(BounceStats)]
+        lib.vrad_light_pass_ranges.restype = i32
+        lib.vrad_light_pass_ranges_device.argtypes = [P, i32, P, P, P]
+        lib.vrad_light_pass_ranges_device.restype = i32
+        lib.vrad_pass_sample_light.argtypes = [P, i32, P, i64]
+        lib.vrad_pass_sample_light.restype = i32
         lib.vrad_set_extra_passes.argtypes = [P, i32]
         lib.vrad_set_extra_passes.restype = i32
         lib.vrad_build_patches.argtypes = [P, i32, P, i64, P, ctypes.c_float, ctypes.c_float, P, i64,
@@ -327,14 +335,23 @@ class LightingInputs:
     sun_jitter: np.ndarray
     sun_samples: int = 1
     sun_angular_extent: float = 0.0
+    lights_hdr: np.ndarray | None = None    # the HDR range's list (intensities differ), or none
 
 
-def prepare(world: World) -> LightingInputs:
+RANGE_LDR, RANGE_HDR = 1, 2      # VRAD_RANGE_*
+
+
+def prepare(world: World, hdr: bool = False) -> LightingInputs:
+    """The lighting stage's inputs; with hdr, also the HDR range's light list."""
     faces, verts = faces_of(world)
     samples, first = build_samples(faces, verts)
     lights, off, flat = build_lights(world)
-    return LightingInputs(faces, verts, samples, first, lights, off, flat,
-                          ambient_directions().astype(np.float32), np.zeros((0, 3), np.float32))
+    inp = LightingInputs(faces, verts, samples, first, lights, off, flat,
+                         ambient_directions().astype(np.float32), np.zeros((0, 3), np.float32))
+    if hdr:
+        inp.lights_hdr, off_h, flat_h = build_lights(world, hdr=True)
+        assert np.array_equal(off, off_h) and np.array_equal(flat, flat_h)
+    return inp
 
 
 class LightingStage:
@@ -352,10 +369,12 @@ class LightingStage:
         keep = [np.ascontiguousarray(a) for a in (i.faces, i.samples, i.lights, i.cluster_offsets,
                                                   i.cluster_lights, i.sky_directions, i.sun_jitter, i.verts)]
         f, s, l, off, cl, dirs, jit, vv = keep
+        lh = None if i.lights_hdr is None else np.ascontiguousarray(i.lights_hdr, LIGHT_DTYPE)
+        keep.append(lh)
         d = _WorldDesc(f.ctypes.data, len(f), s.ctypes.data, len(s), l.ctypes.data, len(l),
                        off.ctypes.data, cl.ctypes.data, len(off) - 1, dirs.ctypes.data, len(dirs),
                        jit.ctypes.data if len(jit) else None, len(jit), i.sun_angular_extent, i.sun_samples,
-                       vv.ctypes.data, len(vv))
+                       vv.ctypes.data, len(vv), None if lh is None else lh.ctypes.data)
         T._check(_lib().vrad_world_upload(self._ctx, ctypes.byref(d)), self._ctx)
         self.inputs = i
 
@@ -466,6 +485,39 @@ class LightingStage:
         T._check(_lib().vrad_light_pass(self._ctx, lighting.ctypes.data, len(lighting), ofs.ctypes.data,
                                         ctypes.byref(st)), self._ctx)
         return lighting, ofs, st
+
+    def light_pass_ranges(self, ranges: int = RANGE_LDR | RANGE_HDR, ldr: np.ndarray | None = None,
+                          hdr: np.ndarray | None = None):
+        """vrad_light_pass_ranges: (LIGHTING bytes or None, LIGHTING_HDR bytes
+        or None, lightofs, PassStats, [BounceStats LDR, BounceStats HDR])."""
+        n = self.lighting_size()
+        if ranges & RANGE_LDR and ldr is None:
+            ldr = np.zeros(n, np.uint8)
+        if ranges & RANGE_HDR and hdr is None:
+            hdr = np.zeros(n, np.uint8)
+        ofs = np.zeros(len(self.inputs.faces), np.int32)
+        st = PassStats()
+        bs = (BounceStats * 2)()
+        T._check(_lib().vrad_light_pass_ranges(
+            self._ctx, ranges, ldr.ctypes.data if ranges & RANGE_LDR else None, len(ldr) if ranges & RANGE_LDR else 0,
+            hdr.ctypes.data if ranges & RANGE_HDR else None, len(hdr) if ranges & RANGE_HDR else 0,
+            ofs.ctypes.data, ctypes.byref(st), bs), self._ctx)
+        return (ldr if ranges & RANGE_LDR else None, hdr if ranges & RANGE_HDR else None, ofs, st, [bs[0], bs[1]])
+
+    def pass_sample_light(self, rng: int) -> np.ndarray:
+        """vrad_pass_sample_light: the last pass's direct light of one range
+        (LIGHTING_DTYPE per sample)."""
+        out = np.zeros(len(self.inputs.samples), LIGHTING_DTYPE)
+        T._check(_lib().vrad_pass_sample_light(self._ctx, rng, out.ctypes.data, len(out)), self._ctx)
+        return out
+
+    def light_pass_ranges_device(self, d_ldr, d_hdr, ranges: int = RANGE_LDR | RANGE_HDR, stream=None):
+        """vrad_light_pass_ranges_device into CUDA tensors (uint8)."""
+        import torch
+        s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        T._check(_lib().vrad_light_pass_ranges_device(
+            self._ctx, ranges, d_ldr.data_ptr() if d_ldr is not None else None,
+            d_hdr.data_ptr() if d_hdr is not None else None, ctypes.c_void_p(s)), self._ctx)
 
     def light_pass_device(self, d_lighting, stream=None):
         import torch

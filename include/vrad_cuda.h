@@ -241,6 +241,13 @@ typedef struct vrad_world_desc {
     int32_t sun_samples;
     const float *vertices;                 /* face windings, xyz each (vrad_face.first_vertex) */
     int64_t nvertices;
+    /* The HDR pass's light list (nullable): the same nlights lights in the
+     * same order, parsed for the HDR range (DirectLightBuilder.ParseGeneric
+     * with the HDR flag, MapTools/Rad/Light/DirectLightBuilder.cs:198-278:
+     * _lightHDR, _lightscaleHDR, _ambientHDR), which differs from the LDR
+     * list in intensity alone; any other difference is VRAD_ERR_ARG.  With
+     * it the world can be lit in both ranges (vrad_light_pass_ranges). */
+    const vrad_light *lights_hdr;
 } vrad_world_desc;
 
 typedef struct vrad_direct_stats {
@@ -442,6 +449,41 @@ typedef struct vrad_bounce_stats {
 
 /* The statistics of the last light pass's bounce. */
 int32_t vrad_bounce_stats_get(vrad_ctx *ctx, vrad_bounce_stats *stats);
+
+/* The ranges a compile lights (Vrad.Passes, MapTools/Rad/Vrad.cs:150-158):
+ * LDR, HDR, or both (-both: LDR first). */
+#define VRAD_RANGE_LDR 1
+#define VRAD_RANGE_HDR 2
+
+/* The lighting stage for one or both ranges, as the reference runs its
+ * passes (Vrad.LightTakenAsync / RunPassAsync, MapTools/Rad/Vrad.cs:262-285,
+ * 392-590): each range's direct gather, supersampling, bounce and final
+ * pass, writing LIGHTING (ldr) and LIGHTING_HDR (hdr), each
+ * vrad_lighting_size bytes.  The second range reuses the first's transfers
+ * (they are geometry; Rad/Vrad.cs:261-263, RadWorld.BounceAsync), so one
+ * transfer build serves both.  With both ranges the first round of the
+ * direct gather is one traversal: every shadow, sun and sky segment is
+ * traced once and lights both ranges (the ranges differ in intensity
+ * only), so each range's sample light is the bits its own pass would give.
+ * FACES and FACES_HDR share the layout: lightofs (nullable) is written
+ * once.  bounce_stats (nullable) receives two records, LDR then HDR (a
+ * range not lit is zeroed); afterwards vrad_bounce_patch_light and the
+ * other bounce inspections report the last range lit.  HDR needs a world
+ * uploaded with lights_hdr.  Host buffers; blocks. */
+int32_t vrad_light_pass_ranges(vrad_ctx *ctx, int32_t ranges, uint8_t *ldr, int64_t ldr_capacity, uint8_t *hdr,
+                               int64_t hdr_capacity, int32_t *lightofs, vrad_pass_stats *stats,
+                               vrad_bounce_stats *bounce_stats);
+
+/* vrad_light_pass_ranges into device buffers (4-byte aligned, each
+ * vrad_lighting_size bytes; the one of a range not lit may be NULL),
+ * queued on `stream` (NULL: the default stream). */
+int32_t vrad_light_pass_ranges_device(vrad_ctx *ctx, int32_t ranges, uint8_t *d_ldr, uint8_t *d_hdr, void *stream);
+
+/* After a light pass: one range's per-sample direct light (LightingValue,
+ * FaceLight's sample values after the supersampling rounds) as that pass's
+ * patch light and final pass read it; n = the world's sample count.  The
+ * reference keeps it per range in RadPass.LightData (FaceLight). */
+int32_t vrad_pass_sample_light(vrad_ctx *ctx, int32_t range, vrad_lighting_value *out, int64_t n);
 
 /* After a light pass: each patch's bounced light (TotalLight.Flat) and
  * direct light (DirectLight), npatches x 3 each; either may be NULL. */
