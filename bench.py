@@ -1,26 +1,32 @@
-"""Benchmark: vrad's lighting stage on the seeded 8x8 room grid.
+"""Benchmark: vrad's lighting stage on the seeded 8x8 room grid, LDR and HDR.
 
-One step = one light pass (vrad_light_pass), the whole stage from the
-uploaded world to the LIGHTING lump:
+One step = the lighting stage of one map in both ranges, as the reference
+runs it with -both (vrad_light_pass_ranges_device), from the uploaded world
+to the LIGHTING and LIGHTING_HDR lumps:
   direct  the fused direct gather over every light sample of the map (for
           each of its 5.68 M samples, every light of its cluster's list in
           gather order: shadow segments to 64 point and spot lights, the
-          sun's sky test and 162 sky-ambient directions, traced in-kernel);
-  bounce  the patches' direct light, the transfer build (every candidate
-          patch pair's ray traced, form factors, scales) and the radiosity
-          bounces to the stop threshold (0.1, the configuration's);
-  final   the luxel radial filters of the direct and the bounced light,
-          RGBE encode, medians, into the LIGHTING lump.
+          sun's sky test and 162 sky-ambient directions, traced in-kernel;
+          one traversal lights both ranges), then each range's four
+          supersampling passes;
+  bounce  the transfer build once (every candidate patch pair's ray traced,
+          form factors, scales), then per range the patches' direct light
+          and the radiosity bounces to the stop threshold (0.1, the
+          configuration's);
+  final   per range the luxel radial filters of the direct and the bounced
+          light, RGBE encode, medians, into its lump.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
     python bench.py --workload seam     # the IRayTracer seam alone, rays in HBM
 
-Prints one JSON line (rank 0).  `value` is rays/s (segments traced per
-second, all ranks) with the world resident in HBM; `e2e` is the same
-through the C ABI's host-buffer entry points (pinned host samples in,
-lighting values out, copies inside the timed region).  `--impl reference`
-times the reference's algorithm on the host CPU: the restated KD tracer and
-four-sample-group gather, all host threads, on a strided sample of faces.
+Prints one JSON line (rank 0).  `value` is rays/s (the rays the reference
+traces for the stage, over the device-timed step, all ranks) with the world
+resident in HBM; `e2e` is the same through the C ABI's host-buffer entry
+points with the inputs built, the scene, world and bounce uploaded and both
+lumps read back inside every step.  `--impl reference` times the
+reference's algorithm (the oracle's restatement) on the host cores.
+Under torchrun each rank lights its own map (seed + rank): whole maps per
+GPU, no data-path exchange; the batched workload deals its maps to the ranks.
 """
 from __future__ import annotations
 
@@ -39,7 +45,7 @@ import numpy as np
 ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "vrad lighting stage rays/s (8x8 room grid, 1 B200)"
+METRIC = "vrad lighting stage rays/s (8x8 room grid, LDR+HDR, 1 B200)"
 UNIT = "rays/s"
 BYTES_PER_RAY = 28.0 + 0.125        # 28-byte ray record in, one hit bit out
 CONFIG_SEED = 1
@@ -64,9 +70,9 @@ def parse():
     return ap.parse_args()
 
 
-def world_for(side: int):
+def world_for(side: int, seed: int = CONFIG_SEED):
     from hl2sdk_tools_sharp_b200 import roomgrid as rg
-    cfg = rg.config_8x8(CONFIG_SEED) if side == 8 else rg.config_3x3(CONFIG_SEED)
+    cfg = rg.config_8x8(seed) if side == 8 else rg.config_3x3(seed)
     if side not in (3, 8):
         cfg.side = side
     return rg.generate(cfg)
@@ -158,6 +164,17 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
+def sum_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def job_value(units_per_rank: float, ms_per_step: float, world: int) -> float:
     """Whole-job throughput: every rank's units over the slowest rank's time."""
     return world * units_per_rank / (ms_per_step / 1000.0)
@@ -213,15 +230,18 @@ def run_reference(args):
     rays = device_rays(w, dev)
     total = sum(int(rays[k].shape[0]) for k in ("light", "sun", "sky"))
     rays_np = host_sample(rays, total)
-    vals = []
+    vals, walls = [], []
     for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
         cb = cpu_reference(w, rays_np, total, budget_s=max(3.0, 60.0 / max(1, args.warmup + args.steps)))
         if i >= args.warmup:
             vals.append(cb["value"])
+            walls.append(time.perf_counter() - t0)
     value = statistics.median(vals)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / value,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.median(walls),
+        "seconds_per_full_step_extrapolated": total / value,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded room grid)",
         "config": {"workload": "8x8 room grid direct-lighting rays (light + sun + 162-dir sky)",
@@ -432,9 +452,10 @@ def main_seam(args):
     return 0
 
 
-def oracle_faces_sample(world, inp, stride: int):
-    """Every `stride`-th face with its samples, renumbered, for the CPU leg."""
-    sel = np.arange(0, len(inp.faces), stride)
+def oracle_faces_sample(world, inp, stride: int, phase: int = 0):
+    """Every `stride`-th face (from `phase`) with its samples, renumbered,
+    for the CPU legs."""
+    sel = np.arange(phase % max(1, stride), len(inp.faces), max(1, stride))
     ff = inp.face_first
     parts = [inp.samples[ff[f]:ff[f + 1]] for f in sel]
     counts = np.array([len(p) for p in parts])
@@ -445,195 +466,297 @@ def oracle_faces_sample(world, inp, stride: int):
     return sel, samples, first, index
 
 
-def cpu_stage(world, inp, budget_s: float = 15.0):
-    """The reference's direct gather on the host: restated KD build + the
-    four-sample-group gather with the KD walk, all host threads, on a
-    strided sample of faces sized to about budget_s."""
+def cpu_direct(world, inp, lights, tree, budget_s: float, phase: int = 0):
+    """The reference's direct gather for one range (its light list) on the
+    host: the restated KD walk and four-sample-group gather with its
+    supersampling passes, all host threads, on a strided sample of faces
+    sized to about budget_s.  (samples/s, segments/s, description)."""
     from oracle import oracle as O
     threads = O.default_threads()
-    tree = O.kd_build(world.tri_verts, world.tri_ids)
 
-    def run(stride):
-        sel, samples, first, _ = oracle_faces_sample(world, inp, stride)
+    def run(stride, ph):
+        sel, samples, first, _ = oracle_faces_sample(world, inp, stride, ph)
         t0 = time.perf_counter()
-        _, rays = O.direct(tree, inp.faces[sel], samples, first, inp.lights, inp.cluster_offsets,
-                           inp.cluster_lights, inp.sky_directions, inp.sun_jitter, inp.sun_samples,
-                           inp.sun_angular_extent, threads=threads, count_rays=True, verts=inp.verts)
+        _, rays = O.direct(tree, inp.faces[sel], samples, first, lights, inp.cluster_offsets, inp.cluster_lights,
+                           inp.sky_directions, inp.sun_jitter, inp.sun_samples, inp.sun_angular_extent,
+                           threads=threads, count_rays=True, verts=inp.verts)
         return rays, len(samples), time.perf_counter() - t0, len(sel)
-    rays, n, dt, nf = run(max(1, len(inp.faces) // 64))
+    rays, n, dt, nf = run(max(1, len(inp.faces) // 64), phase)
     stride = max(1, int(len(inp.faces) / max(1.0, nf * budget_s / max(dt, 1e-3))))
-    rays, n, dt, nf = run(stride)
-    return {"value": rays / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{nf} of {len(inp.faces)} faces (every {stride}th), {n} samples, {rays} segments "
-                      f"of the 8x8 direct gather; restated KD build + KD walk + four-sample-group gather",
-            "samples_per_s": n / dt}
+    rays, n, dt, nf = run(stride, phase)
+    return n / dt, rays / dt, f"{nf} of {len(inp.faces)} faces (every {stride}th), {n} samples, {rays} segments"
 
 
-def batched_run(args, device_index: int) -> dict:
-    """The batched workload: `batch_maps` seeded room grids, sides drawn
-    from 2..10 rooms, each bounced to the 8x8 map's threshold, lit by the
-    native batch runner (host buffers in and out, every map's scene, world
-    and bounce uploaded inside the timed run).  The autotuner picks the
-    gather's launch shape and the maps in flight on the first eight maps;
-    one warm-up run, then the timed run, then the same maps on one worker."""
-    from hl2sdk_tools_sharp_b200 import batch as B, roomgrid as rg
-    t = time.perf_counter()
-    cfgs = [rg.config_batch(i, seed=CONFIG_SEED) for i in range(args.batch_maps)]
-    maps = [B.map_inputs(rg.generate(c), bounces=MAX_BOUNCES, threshold=BOUNCE_THRESHOLD) for c in cfgs]
-    prep_s = time.perf_counter() - t
-    with B.LightingBatch(workers=args.batch_workers, device=device_index) as batch:
-        workers, block, tune = batch.autotune(maps[:min(8, len(maps))])
-        warm, _ = batch.run(maps)
-        results, st = batch.run(maps)
-        one, st1 = batch.run(maps, workers=1)
-    same = all(np.array_equal(a.lighting, b.lighting) and np.array_equal(a.lighting, c.lighting)
-               for a, b, c in zip(results, warm, one))
-    return {"maps": len(maps), "sides": [c.side for c in cfgs], "rooms": int(sum(c.side ** 2 for c in cfgs)),
-            "triangles": int(sum(len(m.triangles) for m in maps)),
-            "samples": int(sum(len(m.inputs.samples) for m in maps)),
-            "workers": st.workers, "threads_per_cta": st.block, "autotune_s": tune,
-            "seconds": st.seconds, "busy_seconds": st.busy_seconds, "one_worker_s": st1.seconds,
-            "rays": int(st.rays), "rays_per_s": st.rays / st.seconds, "luxels": int(st.luxels),
-            "luxels_per_s": st.luxels / st.seconds, "lighting_bytes": int(st.lighting_bytes),
-            "map_s": {"min": min(r.seconds for r in results), "max": max(r.seconds for r in results)},
-            "lumps_equal_across_runs": bool(same), "host_prep_s": prep_s,
-            "note": "wall clock of vrad_batch_run: per map the scene, world and bounce uploads from host "
-                    "arrays, the light pass, the lump read back to host memory; host_prep_s (the maps' "
-                    "generation in Python) is outside it"}
-
-
-def world_and_inputs(side):
-    from hl2sdk_tools_sharp_b200 import lighting as L
-    w = world_for(side)
-    return w, L.prepare(w)
-
-
-def oracle_bounce(world, inp, tree=None):
-    """The oracle's bounce over the world (patches built, nothing traced)."""
-    from hl2sdk_tools_sharp_b200 import lighting as L
-    from oracle import oracle as O
-    tree = tree if tree is not None else O.kd_build(world.tri_verts, world.tri_ids)
-    off, lst = L.pvs_lists(world)
-    return O.Bounce(tree, inp.faces, inp.verts, inp.samples, inp.face_first, L.face_reflectivity(world), off, lst,
-                    bounces=MAX_BOUNCES, threshold=BOUNCE_THRESHOLD)
-
-
-def cpu_transfers(ob, budget_s: float = 10.0):
+def cpu_transfers(ob, budget_s: float = 10.0, phase: int = 0):
     """The transfer build restated (candidate walk, KD-traced rays, form
-    factors) on a strided sample of receivers: transfer rays per second."""
+    factors) on a strided sample of receivers: (transfer rays/s, description)."""
     patches, _ = ob.patches()
     leaves = np.flatnonzero(patches["child1"] == -1)
 
-    def run(stride, phase):
-        sub = leaves[phase::stride]
+    def run(stride, ph):
+        sub = leaves[ph % stride::stride]
         ob.forget_transfers()
         t0 = time.perf_counter()
         _, _, _, rays = ob.transfers(sub)
         return rays, time.perf_counter() - t0, len(sub)
     rays, dt, n = run(max(1, len(leaves) // 400), 1)
     stride = max(1, int(len(leaves) / max(1.0, n * budget_s / max(dt, 1e-3))))
-    rays, dt, n = run(stride, 0)
+    rays, dt, n = run(stride, phase)
     return rays / dt, f"{n} of {len(leaves)} receivers (every {stride}th), {rays} transfer rays"
 
 
-WORKLOAD = ("8x8 room grid lighting stage: direct gather (64 point/spot lights, sun, 162-dir sky), "
-            "bounce (patch light, transfer build, radiosity to threshold 0.1), final pass")
+def world_and_inputs(side, seed=CONFIG_SEED):
+    """The map and the stage's inputs for both ranges, through the library's
+    host builders (the native sample builder)."""
+    from hl2sdk_tools_sharp_b200 import lighting as L
+    w = world_for(side, seed)
+    return w, L.prepare(w, hdr=True)
+
+
+def reference_inputs(world):
+    """The same inputs built without the CUDA library: faces and both light
+    lists by the host layer's pure-Python builders, samples by the oracle's
+    FaceSampleBuilder restatement (bit-identical to the native builder,
+    tests/test_lighting_cpu.py)."""
+    from hl2sdk_tools_sharp_b200 import lighting as L, workload as wl
+    from oracle import oracle as O
+    faces, verts = L.faces_of(world)
+    raw, first = O.build_samples(faces, verts)
+    lights, off, flat = L.build_lights(world)
+    lights_hdr, _, _ = L.build_lights(world, hdr=True)
+    return L.LightingInputs(faces, verts, raw.view(L.SAMPLE_DTYPE), first, lights, off, flat,
+                            wl.ambient_directions().astype(np.float32), np.zeros((0, 3), np.float32),
+                            lights_hdr=lights_hdr)
+
+
+def oracle_bounce(world, inp, tree=None, bounces=MAX_BOUNCES, threshold=BOUNCE_THRESHOLD):
+    """The oracle's bounce over the world (patches built, nothing traced)."""
+    from hl2sdk_tools_sharp_b200 import lighting as L
+    from oracle import oracle as O
+    tree = tree if tree is not None else O.kd_build(world.tri_verts, world.tri_ids)
+    off, lst = L.pvs_lists(world)
+    return O.Bounce(tree, inp.faces, inp.verts, inp.samples, inp.face_first, L.face_reflectivity(world), off, lst,
+                    bounces=bounces, threshold=threshold)
+
+
+WORKLOAD = ("8x8 room grid lighting stage, LDR and HDR ranges: per range the direct gather (64 point/spot "
+            "lights, sun, 162-dir sky, 4 supersampling passes), the bounce (patch light, radiosity to threshold "
+            "0.1) and the final pass into LIGHTING / LIGHTING_HDR; one transfer build for both ranges")
+
+
+def stage_config(args):
+    """The workload's defining keys, the same in both arms."""
+    return {"workload": WORKLOAD, "side": args.side, "seed": CONFIG_SEED, "ranges": "LDR+HDR",
+            "bounce_threshold": BOUNCE_THRESHOLD, "max_bounces": MAX_BOUNCES,
+            "l2": "no L2 flush: the 0.3 GB sample set and 5 GB of candidate pairs exceed L2",
+            "parallelism": f"replicas{args.gpus} (one map per rank, seed {CONFIG_SEED} + rank)"}
 
 
 def run_reference_stage(args):
-    """The reference's algorithm on the host cores: the direct gather and
-    the transfer build restated (KD build, KD walk, four-sample groups,
-    candidate walk, form factors), all host threads, each on a bounded
-    sample of the 8x8 stage.  value = the stage's traced rays over the CPU
-    seconds those two parts take at the sampled rates; the bounce's
-    gathers and the final pass are left out of the CPU time (which only
-    flatters the CPU)."""
+    """The reference's algorithm on the host cores (the oracle, a C++
+    restatement of the reference's C#, which cannot run here), all host
+    threads, on the GPU arm's workload.  Set-up (untimed): the inputs
+    without the CUDA library, the KD tree, both ranges' full direct gather,
+    the full transfer build, and each range's bounce and final pass timed
+    whole once.  Each step then times a bounded sample of the ray-tracing
+    parts (both ranges' direct gathers on a strided face sample, the
+    transfer build on a strided receiver sample); value = the stage's rays
+    over the stage seconds those rates and the whole-pass timings give.
+    ms_per_step is the wall time a step took."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     from oracle import oracle as O
-    w, inp = world_and_inputs(args.side)
+    t_setup = time.perf_counter()
+    w = world_for(args.side)
+    inp = reference_inputs(w)
+    threads = O.default_threads()
     tree = O.kd_build(w.tri_verts, w.tri_ids)
+    ranges = {"ldr": inp.lights, "hdr": inp.lights_hdr}
+    light, direct_rays = {}, {}
+    for r, lights in ranges.items():
+        light[r], direct_rays[r] = O.direct(tree, inp.faces, inp.samples, inp.face_first, lights, inp.cluster_offsets,
+                                            inp.cluster_lights, inp.sky_directions, inp.sun_jitter, inp.sun_samples,
+                                            inp.sun_angular_extent, threads=threads, count_rays=True,
+                                            verts=inp.verts)
     ob = oracle_bounce(w, inp, tree)
-    counts = None
-    vals = []
-    cb = None
+    t = time.perf_counter()
+    t_off, t_src, t_w, transfer_rays = ob.transfers()
+    transfer_full_s = time.perf_counter() - t
+    whole = {}
+    for r in ranges:
+        t = time.perf_counter()
+        _, _, nb, _ = ob.run(light[r])
+        bounce_s = time.perf_counter() - t
+        t = time.perf_counter()
+        ob.final(light[r])
+        whole[r] = {"bounces": int(nb), "bounce_s": bounce_s, "final_s": time.perf_counter() - t}
+    setup_s = time.perf_counter() - t_setup
+    rays_per_step = int(direct_rays["ldr"] + direct_rays["hdr"] + transfer_rays)
+    vals, walls, stages = [], [], []
     for i in range(args.warmup + args.steps):
-        budget = max(2.0, 40.0 / max(1, args.warmup + args.steps))
-        cb = cpu_stage(w, inp, budget_s=budget)
-        t_rate, t_sample = cpu_transfers(ob, budget_s=budget)
-        if counts is None:
-            # Ray counts of one full step: the direct gather's from the
-            # sampled rate's own sample scaled to every sample; the transfer
-            # build's from the candidate walk (no tracing needed to count).
-            direct_rays = cb["value"] * len(inp.samples) / cb["samples_per_s"]
-            counts = (direct_rays, ob.count_candidates())
-        direct_rays, transfer_rays = counts
-        cpu_s = direct_rays / cb["value"] + transfer_rays / t_rate
+        t0 = time.perf_counter()
+        rates = {r: cpu_direct(w, inp, lights, tree, 0.5, phase=i) for r, lights in ranges.items()}
+        t_rate, t_sample = cpu_transfers(ob, budget_s=0.6, phase=i)
+        wall = time.perf_counter() - t0
+        stage_s = (sum(len(inp.samples) / rates[r][0] for r in ranges) + transfer_rays / t_rate
+                   + sum(whole[r]["bounce_s"] + whole[r]["final_s"] for r in ranges))
         if i >= args.warmup:
-            vals.append((direct_rays + transfer_rays) / cpu_s)
+            vals.append(rays_per_step / stage_s)
+            walls.append(wall)
+            stages.append(stage_s)
     value = statistics.median(vals)
-    direct_rays, transfer_rays = counts
+    sample = (f"per step: LDR gather {rates['ldr'][2]}; HDR gather {rates['hdr'][2]}; transfer build {t_sample}; "
+              f"the bounce and final pass of each range timed whole once at set-up "
+              f"(LDR {whole['ldr']['bounces']} bounces {whole['ldr']['bounce_s']:.2f} s + final "
+              f"{whole['ldr']['final_s']:.2f} s, HDR {whole['hdr']['bounces']} bounces "
+              f"{whole['hdr']['bounce_s']:.2f} s + final {whole['hdr']['final_s']:.2f} s)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * (direct_rays + transfer_rays) / value,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.median(walls),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded room grid)",
-        "config": {"workload": WORKLOAD, "side": args.side, "seed": CONFIG_SEED, "samples": int(len(inp.samples)),
-                   "bounce_threshold": BOUNCE_THRESHOLD},
-        "cpu_baseline": {**cb, "value": value,
-                         "sample": cb["sample"] + f"; transfer build: {t_sample}; bounce gathers and final pass not timed"},
+        "config": stage_config(args),
+        "stage_s_extrapolated": statistics.median(stages),
+        "rays_per_step": rays_per_step,
+        "setup_s": setup_s, "transfer_build_whole_s": transfer_full_s,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
+def deal_maps(weights, world: int) -> list:
+    """Whole maps dealt to `world` ranks, largest first, each to the rank
+    with the least weight so far (LPT); ties to the lowest rank.  Returns
+    each rank's map indices in dealing order."""
+    load = [0.0] * world
+    out = [[] for _ in range(world)]
+    for i in sorted(range(len(weights)), key=lambda k: (-weights[k], k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        out[r].append(i)
+        load[r] += weights[i]
+    return out
+
+
+def batched_run(args, device_index: int, rank: int = 0, world: int = 1) -> dict:
+    """The batched workload: `batch_maps` seeded room grids, sides drawn
+    from 2..10 rooms, each bounced to the 8x8 map's threshold, lit by the
+    native batch runner (host buffers in and out, every map's scene, world
+    and bounce uploaded inside the timed run).  Across ranks the maps are
+    dealt whole (deal_maps, weighted by rooms), with no exchange: each rank
+    lights its share, and the job takes the slowest rank's time.  The
+    autotuner picks the gather's launch shape and the maps in flight on the
+    first eight maps of the share; one warm-up run, then the timed run, then
+    the same maps on one worker."""
+    from hl2sdk_tools_sharp_b200 import batch as B, roomgrid as rg
+    out = {}
+    try:
+        t = time.perf_counter()
+        cfgs = [rg.config_batch(i, seed=CONFIG_SEED) for i in range(args.batch_maps)]
+        mine = deal_maps([c.side ** 2 for c in cfgs], world)[rank]
+        cfgs = [cfgs[i] for i in mine]
+        maps = [B.map_inputs(rg.generate(c), bounces=MAX_BOUNCES, threshold=BOUNCE_THRESHOLD) for c in cfgs]
+        prep_s = time.perf_counter() - t
+        with B.LightingBatch(workers=args.batch_workers, device=device_index) as batch:
+            workers, block, tune = batch.autotune(maps[:min(8, len(maps))])
+            warm, _ = batch.run(maps)
+            results, st = batch.run(maps)
+            one, st1 = batch.run(maps, workers=1)
+        same = all(np.array_equal(a.lighting, b.lighting) and np.array_equal(a.lighting, c.lighting)
+                   for a, b, c in zip(results, warm, one))
+        out = {"maps": len(maps), "map_indices": mine, "sides": [c.side for c in cfgs],
+               "rooms": int(sum(c.side ** 2 for c in cfgs)),
+               "triangles": int(sum(len(m.triangles) for m in maps)),
+               "samples": int(sum(len(m.inputs.samples) for m in maps)),
+               "workers": st.workers, "threads_per_cta": st.block, "autotune_s": tune,
+               "seconds": st.seconds, "busy_seconds": st.busy_seconds, "one_worker_s": st1.seconds,
+               "rays": int(st.rays), "rays_per_s": st.rays / st.seconds, "luxels": int(st.luxels),
+               "luxels_per_s": st.luxels / st.seconds, "lighting_bytes": int(st.lighting_bytes),
+               "map_s": {"min": min(r.seconds for r in results), "max": max(r.seconds for r in results)},
+               "lumps_equal_across_runs": bool(same), "host_prep_s": prep_s,
+               "note": "wall clock of vrad_batch_run: per map the scene, world and bounce uploads from host "
+                       "arrays, the light pass, the lump read back to host memory; host_prep_s (the maps' "
+                       "generation in Python) is outside it"}
+    except Exception as exc:  # reported in the line; the headline still prints
+        out = {"error": f"{type(exc).__name__}: {exc}"}
+    # Every rank takes the same collective steps, with or without an error.
+    secs = out.get("seconds", 0.0)
+    job_s = max_over_ranks(secs, world)
+    job_rays = sum_over_ranks(out.get("rays", 0), world)
+    if world > 1:
+        out = {"rank0": out, "ranks": world, "job_seconds": job_s, "job_rays": int(job_rays),
+               "job_rays_per_s": job_rays / job_s if job_s > 0 else None,
+               "split": "whole maps per rank, dealt largest first by rooms; no collective on the data path"}
+    return out
+
+
+# Per launch DRAM traffic of the dominant kernels, from one ncu capture each
+# (dram__bytes_read.sum + dram__bytes_write.sum over the units that launch
+# processed), scaled by the units a full launch processes.  The captures
+# and their commands: profiles/k_transfer_4x4_roomgrid.md,
+# profiles/k_direct_4x4_roomgrid.md.
+TRAFFIC_PER_TRANSFER_RAY = (92441088 + 49963008) / 19922134.0
+
+
 def main_stage(args):
     import torch
-    from hl2sdk_tools_sharp_b200 import lighting as L
+    from hl2sdk_tools_sharp_b200 import lighting as L, tracer as T
     rank, world_size, local = dist_setup(args.gpus)
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
 
-    w, inp = world_and_inputs(args.side)
+    # Weak scaling over whole maps: rank r lights its own map (seed + r),
+    # no data-path exchange (rank 0's is the single-GPU workload).
+    w, inp = world_and_inputs(args.side, CONFIG_SEED + rank)
     n = len(inp.samples)
     refl = L.face_reflectivity(w)
     pvs_off, pvs_list = L.pvs_lists(w)
+    tris = T.make_triangles(w.tri_verts, w.tri_ids)
     stage = L.LightingStage(w, inp, device=local)
     stage.upload_bounce(refl, pvs_off, pvs_list, bounces=MAX_BOUNCES, threshold=BOUNCE_THRESHOLD)
     info = stage.tracer.scene_info()
-    d_out = torch.empty(n * 4, dtype=torch.float32, device=device)
     block, tune_ms = stage.autotune()                # picks the launch shape (untimed)
-    lump_host, lightofs, pstats = stage.light_pass()   # counts the rays of one step
-    bst = stage.bounce_stats()
-    rays_per_step = int(pstats.visibility_rays + pstats.sky_rays + bst.transfer_rays)
+    # Ray counts: each range lit alone (the reference's passes: each range
+    # traces its own direct segments, the first builds the transfers), and
+    # both at once (what one step traces: the first gather round once).
+    _, _, _, st_l, bs_l = stage.light_pass_ranges(L.RANGE_LDR)
+    _, _, _, st_h, _ = stage.light_pass_ranges(L.RANGE_HDR)
+    ldr_host, hdr_host, _, pstats, bst = stage.light_pass_ranges()
+    transfer_rays = int(bst[0].transfer_rays)
+    rays_per_step = int(st_l.visibility_rays + st_l.sky_rays + st_h.visibility_rays + st_h.sky_rays) + transfer_rays
+    traced_per_step = int(pstats.visibility_rays + pstats.sky_rays) + transfer_rays
     luxels = int(pstats.luxels)
-    d_lump = torch.empty(len(lump_host), dtype=torch.uint8, device=device)
+    nbytes = len(ldr_host)
+    d_ldr = torch.empty(nbytes, dtype=torch.uint8, device=device)
+    d_hdr = torch.empty(nbytes, dtype=torch.uint8, device=device)
+    d_out = torch.empty(n * 4, dtype=torch.float32, device=device)
     for _ in range(max(3, args.warmup)):
-        stage.light_pass_device(d_lump)
+        stage.light_pass_ranges_device(d_ldr, d_hdr)
     torch.cuda.synchronize()
 
     check = None
-    ob = None
     cpu_parts = {}
     if rank == 0 and not args.no_cpu:
-        # Parity on this run's own output: a strided sample of faces through
-        # the oracle's direct gather, a sample of receivers through its
-        # transfer build, and the whole lump through its bounce and final
-        # pass fed the device's sample light and transfers (each checked
-        # here or by the sampled comparisons).
+        # Parity on this run's own output: per range a strided sample of
+        # faces through the oracle's direct gather, a sample of receivers
+        # through its transfer build, and each whole lump through its bounce
+        # and final pass fed the device's sample light and transfers (each
+        # pinned by those samples); the bounce and final pass timed here are
+        # the CPU baseline's.
         from oracle import oracle as O
         tree = O.kd_build(w.tri_verts, w.tri_ids)
-        sel, samples, first, index = oracle_faces_sample(w, inp, 97)
-        want = O.direct(tree, inp.faces[sel], samples, first, inp.lights, inp.cluster_offsets,
-                        inp.cluster_lights, inp.sky_directions, inp.sun_jitter, inp.sun_samples,
-                        inp.sun_angular_extent, verts=inp.verts)
-        stage.direct_device(d_out)
-        torch.cuda.synchronize()
-        got_all = d_out.view(n, 4).cpu().numpy()
+        got = {"ldr": stage.pass_sample_light(L.RANGE_LDR), "hdr": stage.pass_sample_light(L.RANGE_HDR)}
+        got = {r: np.concatenate([v["lighting"], v["direct_sun_amount"][:, None]], 1) for r, v in got.items()}
         t_off, t_rec = stage.transfers()
+        sel, samples, first, index = oracle_faces_sample(w, inp, 97)
+        check = {"samples": int(len(index))}
+        for r, lights in (("ldr", inp.lights), ("hdr", inp.lights_hdr)):
+            want = O.direct(tree, inp.faces[sel], samples, first, lights, inp.cluster_offsets,
+                            inp.cluster_lights, inp.sky_directions, inp.sun_jitter, inp.sun_samples,
+                            inp.sun_angular_extent, verts=inp.verts)
+            check[f"{r}_mismatches"] = int((got[r][index].view(np.uint32) != want.view(np.uint32)).any(1).sum())
         ob = oracle_bounce(w, inp, tree)
         patches, _ = ob.patches()
         leaves = np.flatnonzero(patches["child1"] == -1)
@@ -645,20 +768,19 @@ def main_stage(args):
             c, d = o_off[p], o_off[p + 1]
             tr_bad += int(not (np.array_equal(t_rec["patch"][a:b], o_src[c:d])
                                and np.array_equal(t_rec["weight"][a:b].view(np.uint32), o_w[c:d].view(np.uint32))))
+        check.update({"receivers": int(len(sub)), "receiver_mismatches": tr_bad})
         ob.set_transfers(t_off, t_rec["patch"], t_rec["weight"])
-        t = time.perf_counter()
-        _, _, o_bounces, _ = ob.run(got_all)
-        cpu_parts["bounce_s"] = time.perf_counter() - t
-        t = time.perf_counter()
-        lump_want, _ = ob.final(got_all)
-        cpu_parts["final_s"] = time.perf_counter() - t
-        lump_got = d_lump.cpu().numpy()
-        check = {"samples": int(len(index)),
-                 "mismatches": int((got_all[index].view(np.uint32) != want.view(np.uint32)).any(1).sum()),
-                 "receivers": int(len(sub)), "receiver_mismatches": tr_bad,
-                 "bounces": int(bst.bounces), "oracle_bounces": int(o_bounces),
-                 "lump_words": int(len(lump_want) // 4),
-                 "lump_mismatches": int((lump_got.view(np.uint32) != lump_want.view(np.uint32)).sum())}
+        for r, lump in (("ldr", ldr_host), ("hdr", hdr_host)):
+            t = time.perf_counter()
+            _, _, o_bounces, _ = ob.run(got[r])
+            cpu_parts[f"bounce_{r}_s"] = time.perf_counter() - t
+            t = time.perf_counter()
+            lump_want, _ = ob.final(got[r])
+            cpu_parts[f"final_{r}_s"] = time.perf_counter() - t
+            check[f"{r}_bounces"] = int(bst[0 if r == "ldr" else 1].bounces)
+            check[f"{r}_oracle_bounces"] = int(o_bounces)
+            check[f"{r}_lump_words"] = int(len(lump_want) // 4)
+            check[f"{r}_lump_mismatches"] = int((lump.view(np.uint32) != lump_want.view(np.uint32)).sum())
         del t_rec
 
     stream = torch.cuda.current_stream(device)
@@ -672,43 +794,56 @@ def main_stage(args):
         t0.record(stream)
         for s_ in range(args.steps):
             ev[2 * s_].record(stream)
-            stage.light_pass_device(d_lump)
+            stage.light_pass_ranges_device(d_ldr, d_hdr)
             ev[2 * s_ + 1].record(stream)
-            b = stage.bounce_stats()
-            phases.append((b.patch_light_ms, b.transfer_ms, b.bounce_ms, b.bounces))
+            b = stage.bounce_stats_ranges()
+            phases.append((b[0].patch_light_ms + b[1].patch_light_ms, b[0].transfer_ms,
+                           b[0].bounce_ms + b[1].bounce_ms, b[0].bounces, b[1].bounces))
         t1.record(stream)
         torch.cuda.synchronize()
     barrier(world_size)
     elapsed_ms = max_over_ranks(t0.elapsed_time(t1), world_size)
     per_step = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps)]
     ms_per_step = elapsed_ms / args.steps
-    value = job_value(rays_per_step, ms_per_step, world_size)
-    bst = stage.bounce_stats()
-
-    # End to end through the host-buffer C ABI: the world (samples from
-    # pinned memory) and the bounce uploaded, the light pass, the lump read
-    # back into pinned memory.
+    job_rays = sum_over_ranks(rays_per_step, world_size)
+    value = job_rays / (ms_per_step / 1000.0)
+    # End to end through the host-buffer C ABI, every step: the stage's
+    # inputs built on the host (faces, the samples by the native builder,
+    # both ranges' light lists from the entities), the scene (intersection
+    # form and BVH), the world and the bounce uploaded, and both ranges lit
+    # with their lumps read back into pinned memory.
     e2e = None
     if not args.no_e2e:
-        pinned = torch.empty(inp.samples.nbytes, dtype=torch.uint8, pin_memory=True)
-        pinned.numpy()[:] = inp.samples.view(np.uint8).reshape(-1)
-        inp_pinned = L.LightingInputs(**{**inp.__dict__, "samples": pinned.numpy().view(L.SAMPLE_DTYPE)})
-        out_pinned = torch.empty(len(lump_host), dtype=torch.uint8, pin_memory=True)
-        outv = out_pinned.numpy()
-
-        parts = {"upload_world": [], "upload_bounce": [], "light_pass": []}
+        from hl2sdk_tools_sharp_b200 import workload as wl
+        out_ldr = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True).numpy()
+        out_hdr = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True).numpy()
+        sample_buf = np.empty(n + 64, L.SAMPLE_DTYPE)   # reused from map to map
+        parts = {"inputs": [], "upload_scene": [], "upload_world": [], "upload_bounce": [], "light_pass": []}
+        h2d = []
 
         def e2e_step():
             t0 = time.perf_counter()
-            stage.upload_world(inp_pinned)
+            faces, verts = L.faces_of(w)
+            samples, first = L.build_samples(faces, verts, out=sample_buf)
+            lights, off, flat = L.build_lights(w)
+            lights_hdr, _, _ = L.build_lights(w, hdr=True)
+            i2 = L.LightingInputs(faces, verts, samples, first, lights, off, flat,
+                                  wl.ambient_directions().astype(np.float32), np.zeros((0, 3), np.float32),
+                                  lights_hdr=lights_hdr)
             t1 = time.perf_counter()
-            stage.upload_bounce(refl, pvs_off, pvs_list, bounces=MAX_BOUNCES, threshold=BOUNCE_THRESHOLD)
+            stage.tracer.upload_scene(tris)
             t2 = time.perf_counter()
-            stage.light_pass(outv)
+            stage.upload_world(i2)
             t3 = time.perf_counter()
-            parts["upload_world"].append(t1 - t0)
-            parts["upload_bounce"].append(t2 - t1)
-            parts["light_pass"].append(t3 - t2)
+            stage.upload_bounce(refl, pvs_off, pvs_list, bounces=MAX_BOUNCES, threshold=BOUNCE_THRESHOLD)
+            t4 = time.perf_counter()
+            stage.light_pass_ranges(ldr=out_ldr, hdr=out_hdr)
+            t5 = time.perf_counter()
+            for k, a, b in (("inputs", t0, t1), ("upload_scene", t1, t2), ("upload_world", t2, t3),
+                            ("upload_bounce", t3, t4), ("light_pass", t4, t5)):
+                parts[k].append(b - a)
+            h2d.append(tris.nbytes + faces.nbytes + verts.nbytes + samples.nbytes + lights.nbytes + lights_hdr.nbytes
+                       + off.nbytes + flat.nbytes + refl.nbytes + pvs_off.nbytes + pvs_list.nbytes)
         e2e_step()
         barrier(world_size)
         t = time.perf_counter()
@@ -716,30 +851,32 @@ def main_stage(args):
         for _ in range(e2e_steps):
             e2e_step()
         e2e_s = max_over_ranks((time.perf_counter() - t) / e2e_steps, world_size)
-        e2e = {"value": world_size * rays_per_step / e2e_s, "unit": UNIT,
-               "h2d_bytes_per_step": int(inp.samples.nbytes + inp.faces.nbytes + inp.lights.nbytes
-                                         + inp.verts.nbytes + refl.nbytes + pvs_off.nbytes + pvs_list.nbytes),
-               "d2h_bytes_per_step": int(len(lump_host)), "stage_s": e2e_s,
+        e2e = {"value": job_rays / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d[-1]),
+               "d2h_bytes_per_step": int(2 * nbytes), "stage_s": e2e_s,
                "parts_s": {k: statistics.median(v[1:]) for k, v in parts.items()},
                "step_parts_s": [[round(parts[k][i], 4) for k in parts] for i in range(1, len(parts["light_pass"]))],
-               "note": "includes the host-side set-up of the world and the bounce (slot layout, final-pass "
-                       "tables, the patch tree) and the device tables' uploads"}
-        if not np.array_equal(outv, lump_host):
+               "note": "per step: the inputs built on the host (faces, samples, both light lists), the scene "
+                       "upload with its BVH build, the world and bounce uploads with all their host set-up, "
+                       "both ranges lit and their lumps read back"}
+        if not (np.array_equal(out_ldr, ldr_host) and np.array_equal(out_hdr, hdr_host)):
             e2e["mismatch_vs_device"] = True
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu:
-        cpu = cpu_stage(w, inp, budget_s=12.0)
+        from oracle import oracle as O
+        tree = O.kd_build(w.tri_verts, w.tri_ids)
+        ob = oracle_bounce(w, inp, tree)
+        r_l = cpu_direct(w, inp, inp.lights, tree, 6.0)
+        r_h = cpu_direct(w, inp, inp.lights_hdr, tree, 6.0, phase=1)
         t_rate, t_sample = cpu_transfers(ob, budget_s=12.0)
-        cpu_direct_s = n / cpu["samples_per_s"]
-        cpu_transfer_s = bst.transfer_rays / t_rate
-        cpu["stage_s"] = cpu_direct_s + cpu_transfer_s + cpu_parts["bounce_s"] + cpu_parts["final_s"]
-        cpu["parts_s"] = {"direct": cpu_direct_s, "transfers": cpu_transfer_s, "bounce": cpu_parts["bounce_s"],
-                          "final": cpu_parts["final_s"]}
-        cpu["value"] = rays_per_step / cpu["stage_s"]
-        cpu["sample"] += (f"; transfer build: {t_sample} ({t_rate:.3g} rays/s); bounce (patch light + "
-                          f"{bst.bounces} bounces over the device's transfers) and final pass timed whole "
-                          f"({cpu_parts['bounce_s']:.2f} s, {cpu_parts['final_s']:.2f} s)")
+        cparts = {"direct_ldr": n / r_l[0], "direct_hdr": n / r_h[0], "transfers": transfer_rays / t_rate,
+                  **{k: v for k, v in cpu_parts.items()}}
+        stage_s = sum(cparts.values())
+        cpu = {"value": rays_per_step / stage_s, "unit": UNIT, "cores": O.default_threads(), "kind": "port",
+               "sample": (f"LDR gather: {r_l[2]}; HDR gather: {r_h[2]}; transfer build: {t_sample} "
+                          f"({t_rate:.3g} rays/s); each range's bounce (patch light and bounces over the device's "
+                          f"transfers) and final pass timed whole"),
+               "stage_s": stage_s, "parts_s": cparts}
 
     peaks = {}
     try:
@@ -748,9 +885,9 @@ def main_stage(args):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
 
-    # The learned warm start: a network trained on the device on plain
-    # bounce solutions of eight small seeded maps (2 to 6 rooms a side),
-    # then this map bounced from its guess, against the plain bounce.
+    # The learned warm start (LDR range): a network trained on the device on
+    # plain bounce solutions of eight small seeded maps (2 to 6 rooms a
+    # side), then this map bounced from its guess, against the plain bounce.
     learned = None
     if rank == 0 and not args.no_learned:
         from hl2sdk_tools_sharp_b200 import learned as LN
@@ -764,6 +901,8 @@ def main_stage(args):
         tb.record(stream)
         torch.cuda.synchronize()
         train_ms = ta.elapsed_time(tb)
+        plain_lump, _, _ = stage.light_pass()
+        bp = stage.bounce_stats()
         stage.set_bounce_model(net)
         warm_lump, _, _ = stage.light_pass()
         bw = stage.bounce_stats()
@@ -779,10 +918,10 @@ def main_stage(args):
         fwd_ms = ta.elapsed_time(tb) / 10
         flops = 2.0 * (32 * 128 + 128 * 128 + 128 * 8) * len(hx)
         tpeak = float(peaks.get("bf16_tflops", 1590.0))
-        learned = {"plain_bounces": int(bst.bounces), "warm_bounces": int(bw.bounces),
-                   "plain_bounce_ms": statistics.median([p[2] for p in phases]), "warm_bounce_ms": bw.bounce_ms,
-                   "iteration_ratio": bst.bounces / max(1, bw.bounces),
-                   "lightmap_within_1_lsb": LN.within_one_lsb(warm_lump, lump_host),
+        learned = {"range": "LDR", "plain_bounces": int(bp.bounces), "warm_bounces": int(bw.bounces),
+                   "plain_bounce_ms": bp.bounce_ms, "warm_bounce_ms": bw.bounce_ms,
+                   "iteration_ratio": bp.bounces / max(1, bw.bounces),
+                   "lightmap_within_1_lsb": LN.within_one_lsb(warm_lump, plain_lump),
                    "guess_abs_error_log1p": float((y - ht).abs().mean().item()),
                    "training": {"maps": 8, "rows": int(len(lx)), "steps": 3000, "batch": 32768,
                                 "collect_s": collect_s, "train_ms": train_ms, "final_loss": loss},
@@ -792,74 +931,79 @@ def main_stage(args):
                                 "ms": fwd_ms, "flops_per_row": flops / len(hx)}}
         net.close()
     batched = None
-    if rank == 0 and world_size == 1 and not args.no_batch:
-        try:
-            batched = batched_run(args, local)
-        except Exception as exc:  # reported in the line; the headline still prints
-            batched = {"error": f"{type(exc).__name__}: {exc}"}
-    # The dominant phases timed alone on the launching stream: the direct
-    # gather kernel, and the transfer build (its phase events).
-    a_ev = torch.cuda.Event(enable_timing=True)
-    b_ev = torch.cuda.Event(enable_timing=True)
-    a_ev.record(stream)
+    if not args.no_batch:
+        batched = batched_run(args, local, rank, world_size)
+    # The dominant phases on the launching stream: both ranges' direct
+    # gather (the two-range first round and each range's supersampling
+    # passes), timed by a host-buffer pass, and the transfer build (its
+    # phase events in every timed step).
+    dms = []
     for _ in range(3):
-        stage.direct_device(d_out)
-    b_ev.record(stream)
-    torch.cuda.synchronize()
-    direct_ms = a_ev.elapsed_time(b_ev) / 3.0
+        _, _, _, ps, _ = stage.light_pass_ranges(ldr=ldr_host.copy(), hdr=hdr_host.copy())
+        dms.append(ps.direct_ms)
+    direct_ms = statistics.median(dms)
     transfer_ms = statistics.median([p[1] for p in phases])
     direct_rays = int(pstats.visibility_rays + pstats.sky_rays)
     if direct_ms >= transfer_ms:
-        alg_bytes = 28.0 * direct_rays + 32.0 * n
-        kernel, kernel_ms = "k_direct (fused gather + traversal)", direct_ms
-        alg_note = "28 B per traced segment + 16 B sample in + 16 B value out"
+        alg_bytes = 28.0 * direct_rays + 48.0 * n
+        kernel, kernel_ms = "k_direct (both ranges' gather + traversal) and the supersampling passes", direct_ms
+        alg_note = "28 B per traced segment + 16 B sample in + 2 x 16 B values out"
+        traffic = None
     else:
-        alg_bytes = 28.0 * bst.transfer_rays + 8.0 * bst.transfers
+        alg_bytes = 28.0 * transfer_rays + 8.0 * bst[0].transfers
         kernel, kernel_ms = "transfer build (k_candidates + k_transfer + compaction)", transfer_ms
         alg_note = "28 B per candidate ray + 8 B per transfer written"
+        traffic = TRAFFIC_PER_TRANSFER_RAY * transfer_rays
     achieved = alg_bytes / (kernel_ms / 1000.0) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": kernel, "kernel_ms": kernel_ms, "algorithmic_bytes": alg_note,
+                "traffic": traffic, "kernel": kernel, "kernel_ms": kernel_ms, "algorithmic_bytes": alg_note,
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_transfer launch on "
+                                  "the 4x4 map (profiles/k_transfer_4x4_roomgrid.md), per transfer ray, times this "
+                                  "launch's transfer rays",
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "direct_ms": direct_ms, "transfer_build_ms": transfer_ms}
-    nb = int(statistics.median([p[3] for p in phases]))
+    nb_l = int(statistics.median([p[3] for p in phases]))
+    nb_h = int(statistics.median([p[4] for p in phases]))
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded room grid)",
-            "config": {"workload": WORKLOAD,
-                       "side": args.side, "seed": CONFIG_SEED, "samples": n, "faces": int(len(inp.faces)),
-                       "triangles": info.triangles, "lights": int(len(inp.lights)),
-                       "rays_per_step": rays_per_step,
-                       "visibility_rays": int(pstats.visibility_rays), "sky_rays": int(pstats.sky_rays),
-                       "transfer_rays": int(bst.transfer_rays), "transfers": int(bst.transfers),
-                       "patches": int(bst.patches), "receivers": int(bst.receivers),
-                       "luxels": luxels, "lighting_bytes": int(len(lump_host)),
-                       "bounce_threshold": BOUNCE_THRESHOLD, "bounces": nb,
-                       "l2": "no L2 flush: the 0.3 GB sample set and 5 GB of candidate pairs exceed L2",
-                       "parallelism": f"replicas{world_size}"},
+            "config": stage_config(args),
+            "counts": {"samples": n, "faces": int(len(inp.faces)), "triangles": info.triangles,
+                       "lights": int(len(inp.lights)), "rays_per_step": rays_per_step,
+                       "rays_traced_per_step": traced_per_step,
+                       "direct_rays_ldr": int(st_l.visibility_rays + st_l.sky_rays),
+                       "direct_rays_hdr": int(st_h.visibility_rays + st_h.sky_rays),
+                       "transfer_rays": transfer_rays, "transfers": int(bst[0].transfers),
+                       "patches": int(bst[0].patches), "receivers": int(bst[0].receivers),
+                       "luxels": luxels, "lighting_bytes_per_range": nbytes,
+                       "bounces_ldr": nb_l, "bounces_hdr": nb_h,
+                       "job_rays_per_step": job_rays},
+            "rays_note": ("rays_per_step counts what the reference traces for the stage: each range's direct "
+                          "segments (it lights the ranges in two passes) and one transfer build; one step here "
+                          "traces rays_traced_per_step (the two ranges' first gather round share one traversal)"),
             "samples_per_s": world_size * n / (ms_per_step / 1000.0),
-            "luxels_per_s": world_size * luxels / (ms_per_step / 1000.0),
+            "luxels_per_s": world_size * 2 * luxels / (ms_per_step / 1000.0),
             "stage_s": ms_per_step / 1000.0,
-            "phase_ms": {"direct": direct_ms, "patch_light": statistics.median([p[0] for p in phases]),
+            "phase_ms": {"direct_both_ranges": direct_ms, "patch_light": statistics.median([p[0] for p in phases]),
                          "transfers": transfer_ms, "bounces": statistics.median([p[2] for p in phases])},
-            "bounce_iterations": nb,
             "e2e": e2e,
-            # Per light pass of this map (the ncu launch list in profiles/):
-            # direct 1; supersampling 4 per pass run + 1; patch light 2;
-            # transfer build 16 (candidates, rays, count, write, slices,
-            # their scans and sort); final 4; per bounce the gather, the 8
-            # tree levels of CollectLight and the totals (exact totals add
-            # one when needed).
-            "gpu_launches": (1 + 4 * int(pstats.extra_passes_run) + 1 + 2 + 16 + 4 + 10 * nb) * args.steps,
+            # Per step (the ncu launch list in profiles/): the two-range
+            # gather 1; per range its supersampling (1 + 4 per pass run),
+            # patch light 2, final 4, per bounce the gather, the 8 tree
+            # levels of CollectLight and the totals; the transfer build 16
+            # (candidates, rays, count, write, slices, their scans and sort).
+            "gpu_launches": (1 + (1 + 4 * int(st_l.extra_passes_run)) + (1 + 4 * int(st_h.extra_passes_run))
+                             + 2 * (2 + 4) + 16 + 10 * (nb_l + nb_h)) * args.steps,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
             "step_ms": per_step,
-            "bvh": {"nodes": info.bvh_nodes, "leaves": info.bvh_leaves, "max_leaf": info.max_leaf, "depth": info.bvh_depth,
-                    "build_ms": info.build_ms, "pad": info.box_pad},
+            "bvh": {"nodes": info.bvh_nodes, "leaves": info.bvh_leaves, "max_leaf": info.max_leaf,
+                    "depth": info.bvh_depth, "build_ms": info.build_ms, "pad": info.box_pad},
             "autotune": {"threads_per_cta": block, "ms": tune_ms},
             "check": check,
             "learned": learned,

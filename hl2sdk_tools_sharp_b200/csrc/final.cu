@@ -647,6 +647,7 @@ int32_t pass_on(vrad_ctx *ctx, int32_t ranges, uint8_t *d_ldr, uint8_t *d_hdr, c
     if (e == cudaSuccess && ev) e = cudaEventRecord(ev->direct, s);
     const bool bounce = vrad::bounce_active(ctx);
     bool built = false;
+    for (int r = 0; r < 2; r++) std::memset(&ctx->range_bounce[r], 0, sizeof ctx->range_bounce[r]);
     for (int r = 0; r < 2 && e == cudaSuccess; r++) {
         if (bstats) std::memset(&bstats[r], 0, sizeof bstats[r]);
         if (!(ranges & (1 << r))) continue;
@@ -660,7 +661,8 @@ int32_t pass_on(vrad_ctx *ctx, int32_t ranges, uint8_t *d_ldr, uint8_t *d_hdr, c
             if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, why.c_str());
             built = true;
             prad = vrad::patch_radial_view(ctx);
-            if (bstats) vrad::fill_bounce_stats(ctx, &bstats[r]);
+            vrad::fill_bounce_stats(ctx, &ctx->range_bounce[r]);
+            if (bstats) bstats[r] = ctx->range_bounce[r];
         }
         if (e == cudaSuccess && ev) e = cudaEventRecord(ev->bounce[r], s);
         if (e == cudaSuccess) e = cudaMemsetAsync(out, 0, (size_t)fb.lighting_bytes, s);
@@ -742,8 +744,10 @@ int32_t pass_host(vrad_ctx *ctx, int32_t ranges, uint8_t *ldr, int64_t ldr_capac
         for (int r = 0; r < 2; r++)
             if (ranges & (1 << r)) cudaEventElapsedTime(&final_ms[r], ev.bounce[r], ev.final_[r]);
         ctx->bounce.final_ms = (ranges & VRAD_RANGE_HDR) ? final_ms[1] : final_ms[0];
-        if (bstats)
-            for (int r = 0; r < 2; r++) bstats[r].final_ms = final_ms[r];
+        for (int r = 0; r < 2; r++) {
+            ctx->range_bounce[r].final_ms = final_ms[r];
+            if (bstats) bstats[r].final_ms = final_ms[r];
+        }
         if (lightofs)
             for (int32_t f = 0; f < fb.nfaces; f++) lightofs[f] = fb.lightofs[(size_t)f];
         if (stats) {
@@ -817,4 +821,12 @@ extern "C" int32_t vrad_pass_sample_light(vrad_ctx *ctx, int32_t range, vrad_lig
     if (e == cudaSuccess) e = vrad::quiesce(ctx);
     if (e == cudaSuccess && n) e = cudaMemcpy(out, src, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToHost);
     return e == cudaSuccess ? VRAD_OK : vrad_cuda_fail(ctx, e, "sample light");
+}
+
+extern "C" int32_t vrad_bounce_stats_ranges(vrad_ctx *ctx, vrad_bounce_stats *stats) {
+    if (!ctx || !stats) return vrad_fail(ctx, VRAD_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    stats[0] = ctx->range_bounce[0];
+    stats[1] = ctx->range_bounce[1];
+    return VRAD_OK;
 }

@@ -132,6 +132,8 @@ def _lib():
         lib.vrad_light_pass_ranges_device.restype = i32
         lib.vrad_pass_sample_light.argtypes = [P, i32, P, i64]
         lib.vrad_pass_sample_light.restype = i32
+        lib.vrad_bounce_stats_ranges.argtypes = [P, ctypes.POINTER(BounceStats)]
+        lib.vrad_bounce_stats_ranges.restype = i32
         lib.vrad_set_extra_passes.argtypes = [P, i32]
         lib.vrad_set_extra_passes.restype = i32
         lib.vrad_build_patches.argtypes = [P, i32, P, i64, P, ctypes.c_float, ctypes.c_float, P, i64,
@@ -180,24 +182,25 @@ def faces_of(world: World):
     return faces, verts
 
 
-def build_samples(faces: np.ndarray, verts: np.ndarray):
+def build_samples(faces: np.ndarray, verts: np.ndarray, out: np.ndarray | None = None):
     """FaceSampleBuilder.CalcPoints for every face (native); returns the
-    samples and face_first (index of each face's first sample)."""
+    samples and face_first (index of each face's first sample).  A face has
+    at most one sample per lightmap cell, so one call into a buffer of that
+    many records builds them all; `out` (SAMPLE_DTYPE, at least that long)
+    lets a caller reuse one buffer across maps."""
     lib = _lib()
     faces = np.ascontiguousarray(faces, FACE_DTYPE)
     verts = np.ascontiguousarray(verts, np.float32)
+    cap = int((faces["lightmap_size"][:, 0].astype(np.int64) * faces["lightmap_size"][:, 1]).sum())
+    if out is None or len(out) < cap:
+        out = np.empty(max(1, cap), SAMPLE_DTYPE)
     count = ctypes.c_int64()
-    rc = lib.vrad_build_samples(faces.ctypes.data, len(faces), verts.ctypes.data, len(verts), None,
-                                1 << 62, ctypes.byref(count), None)
-    if rc != 0:
-        raise ValueError(f"vrad_build_samples failed ({rc})")
-    out = np.zeros(count.value, SAMPLE_DTYPE)
     first = np.zeros(len(faces) + 1, np.int64)
     rc = lib.vrad_build_samples(faces.ctypes.data, len(faces), verts.ctypes.data, len(verts),
                                 out.ctypes.data, len(out), ctypes.byref(count), first.ctypes.data)
     if rc != 0:
         raise ValueError(f"vrad_build_samples failed ({rc})")
-    return out, first
+    return out[:count.value], first
 
 
 def build_patches(faces: np.ndarray, verts: np.ndarray, reflectivity: np.ndarray, max_chop: float = 4.0,
@@ -503,6 +506,12 @@ class LightingStage:
             hdr.ctypes.data if ranges & RANGE_HDR else None, len(hdr) if ranges & RANGE_HDR else 0,
             ofs.ctypes.data, ctypes.byref(st), bs), self._ctx)
         return (ldr if ranges & RANGE_LDR else None, hdr if ranges & RANGE_HDR else None, ofs, st, [bs[0], bs[1]])
+
+    def bounce_stats_ranges(self):
+        """vrad_bounce_stats_ranges: [LDR, HDR] BounceStats of the last pass."""
+        bs = (BounceStats * 2)()
+        T._check(_lib().vrad_bounce_stats_ranges(self._ctx, bs), self._ctx)
+        return [bs[0], bs[1]]
 
     def pass_sample_light(self, rng: int) -> np.ndarray:
         """vrad_pass_sample_light: the last pass's direct light of one range

@@ -221,6 +221,16 @@ class CudaRayTracer:
             rc = lib.vrad_scene_upload(ctx, tris.ctypes.data, len(tris))
         _check(rc, ctx)
 
+    def upload_scene(self, triangles) -> None:
+        """vrad_scene_upload again: a new scene (intersection form and BVH)
+        for this context's later traces and light passes."""
+        tris = triangles
+        if not (isinstance(tris, np.ndarray) and tris.dtype == TRIANGLE_DTYPE):
+            tris = make_triangles(tris)
+        tris = np.ascontiguousarray(tris)
+        self.triangle_count = len(tris)
+        _check(self._lib.vrad_scene_upload(self._ctx, tris.ctypes.data, len(tris)), self._ctx)
+
     # -- lifetime ---------------------------------------------------------
     def close(self) -> None:
         if getattr(self, "_ctx", None):

@@ -485,6 +485,11 @@ int32_t vrad_light_pass_ranges_device(vrad_ctx *ctx, int32_t ranges, uint8_t *d_
  * reference keeps it per range in RadPass.LightData (FaceLight). */
 int32_t vrad_pass_sample_light(vrad_ctx *ctx, int32_t range, vrad_lighting_value *out, int64_t n);
 
+/* The last light pass's bounce statistics per range: two records, LDR then
+ * HDR (zeroed for a range the pass did not light; final_ms is kept only by
+ * the host-buffer passes).  Device-buffer passes report here too. */
+int32_t vrad_bounce_stats_ranges(vrad_ctx *ctx, vrad_bounce_stats *stats);
+
 /* After a light pass: each patch's bounced light (TotalLight.Flat) and
  * direct light (DirectLight), npatches x 3 each; either may be NULL. */
 int32_t vrad_bounce_patch_light(vrad_ctx *ctx, float *total_light, float *direct_light, int64_t npatches);
