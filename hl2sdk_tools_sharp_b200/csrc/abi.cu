@@ -219,6 +219,7 @@ cudaError_t release_tables(vrad_ctx *ctx) {
     ctx->final_pass.release();
     ctx->bounce.release();
     ctx->supersample.release();
+    ctx->bsp.release();
     vrad::dev_free(ctx->sample_light);
     ctx->sample_light = nullptr;
     vrad::dev_free(ctx->sample_light_hdr);
@@ -295,6 +296,7 @@ int32_t vrad_destroy(vrad_ctx *ctx) {
         ctx->supersample.release();
         ctx->supersample.free_pinned();
         ctx->shelf.release();
+        ctx->bsp.release();
         vrad::dev_free(ctx->sample_light);
         vrad::dev_free(ctx->sample_light_hdr);
         cudaFree(ctx->status);

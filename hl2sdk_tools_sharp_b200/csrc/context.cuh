@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "bounce.cuh"
+#include "bsp_trace.cuh"
 #include "direct.cuh"
 #include "final.cuh"
 #include "host_parallel.h"
@@ -60,6 +61,7 @@ struct vrad_ctx {
     std::vector<int32_t> h_noff, h_nlist;
     int32_t nclusters = 0;
     vrad::BounceBuffers bounce;
+    vrad::BspBuffers bsp;            // a map's BSP tree for the surface walk (vrad_bsp_upload)
     // The uploaded world's patch forest, grown ahead on a host thread while
     // the rest of the world upload runs, with the chop sizes of this
     // context's last bounce upload; the next bounce upload takes it when

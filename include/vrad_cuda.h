@@ -613,6 +613,60 @@ int32_t vrad_bounce_features_device(vrad_ctx *ctx, uint16_t *x, float *target, i
 int32_t vrad_trace_visibility_static(vrad_ctx *ctx, const vrad_ray *rays, int64_t n,
                                      const vrad_trace_options *opts, uint64_t *hit_bits);
 
+/* ---- The BSP surface walk -------------------------------------------------
+ *
+ * Stock vrad's other tracer: CLightSurface over EnumerateNodesAlongRay, a
+ * front-to-back walk of the map's own BSP tree that tests lit faces in
+ * lightmap space and sky faces by their windings, stopping at the first hit.
+ * Leaf ambient traces with it.  Replaces BspSurfaceTracer.TraceClosest
+ * (MapTools/Tracing/BspSurfaceTracer.cs:166-199, 233-357) over the arrays
+ * BspTraceGeometry.Build makes (MapTools/Tracing/BspTraceGeometry.cs:291-
+ * 899; hl2sdk_tools_sharp_b200/bsp.py builds them from a BSP file):
+ *   nodes       8 words per node: plane normal xyz, dist, then as int32
+ *               child0, child1 (a leaf is -1 - index), first node face,
+ *               packed (lit face count | sky face count << 15 | axis << 30,
+ *               axis 3 for a plane that is not axial);
+ *   surfaces    16 floats per face: plane normal xyz, dist, lightmap s
+ *               (xyz, offset), t (xyz, offset), lightmap mins s, t and
+ *               sizes s, t (sizes -1 for a face with no lightmap);
+ *   node_faces  every node's on-node candidates, lit then sky;
+ *   leaf_faces  every leaf's candidates; leaf_start / leaf_count per leaf;
+ *   sky_points  the sky faces' windings (xyz), sky_start / sky_count per face.
+ * Every index is checked at upload; the context keeps the tree until the
+ * next upload or vrad_destroy. */
+typedef struct vrad_bsp_geometry {
+    const float *nodes;
+    int32_t nnodes;
+    const float *surfaces;
+    int32_t nsurfaces;
+    const int32_t *node_faces;
+    int32_t nnode_faces;
+    const int32_t *leaf_faces;
+    int32_t nleaf_faces;
+    const int32_t *leaf_start;
+    const int32_t *leaf_count;
+    int32_t nleaves;
+    const float *sky_points;
+    int32_t nsky_points;
+    const int32_t *sky_start;
+    const int32_t *sky_count;
+} vrad_bsp_geometry;
+
+int32_t vrad_bsp_upload(vrad_ctx *ctx, const vrad_bsp_geometry *bsp);
+
+/* The walk for n rays: the segment from origin along direction x reach
+ * (stock's start + delta over the fraction 0..1).  hits[i] = the face hit
+ * and the fraction along the segment, or -1 and 1 for none.  min_distance
+ * is the smallest fraction a leaf face may be hit at (RayTraceOptions'
+ * MinDistance); a skip id is VRAD_ERR_UNSUPPORTED.  A walk deeper than 64
+ * pending splits fails the call with VRAD_ERR_CUDA, as the reference's
+ * throws.  Host buffers; blocks.  The _device form takes device buffers and
+ * queues on `stream`. */
+int32_t vrad_bsp_trace_closest(vrad_ctx *ctx, const vrad_ray *rays, int64_t n, const vrad_trace_options *opts,
+                               vrad_hit *hits);
+int32_t vrad_bsp_trace_closest_device(vrad_ctx *ctx, const vrad_ray *d_rays, int64_t n, float min_distance,
+                                      vrad_hit *d_hits, void *stream);
+
 /* ---- Batches of maps ------------------------------------------------------
  *
  * Many maps lit on one device.  No counterpart in the reference, which

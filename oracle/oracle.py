@@ -182,6 +182,31 @@ def fp64_classify(verts: np.ndarray, rays: np.ndarray, rel_margin: float = 1e-6,
     return out
 
 
+def bsp_trace(geom, rays: np.ndarray, min_frac: float = 0.0, threads: int | None = None):
+    """The reference's BSP surface tracer (bsp_oracle.cpp) over a
+    hl2sdk_tools_sharp_b200.bsp.TraceGeometry: (face per ray, -1 for none;
+    fraction along the ray's delta, 1 for none)."""
+    L = lib()
+    if not getattr(L, "_bsp_typed", False):
+        P = ctypes.c_void_p
+        L.orc_bsp_trace.argtypes = [P, P, P, P, P, P, ctypes.c_int32, P, P, P, P, ctypes.c_int64, ctypes.c_float,
+                                    P, P, ctypes.c_int32]
+        L.orc_bsp_trace.restype = ctypes.c_int
+        L._bsp_typed = True
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 7)
+    keep = [np.ascontiguousarray(a) for a in (geom.nodes, geom.surfaces, geom.node_faces, geom.leaf_faces,
+                                               geom.leaf_start, geom.leaf_count, geom.sky_points, geom.sky_start,
+                                               geom.sky_count)]
+    face = np.empty(len(rays), np.int32)
+    frac = np.empty(len(rays), np.float32)
+    rc = L.orc_bsp_trace(_p(keep[0]), _p(keep[1]), _p(keep[2]), _p(keep[3]), _p(keep[4]), _p(keep[5]),
+                         len(geom.leaf_start), _p(keep[6]), _p(keep[7]), _p(keep[8]), _p(rays), len(rays), min_frac,
+                         _p(face), _p(frac), threads if threads is not None else default_threads())
+    if rc != 0:
+        raise RuntimeError("orc_bsp_trace: the walk outgrew its stack")
+    return face, frac
+
+
 def bits_to_bool(bits: np.ndarray, n: int) -> np.ndarray:
     """Unpack LSB-first u64 words into n booleans."""
     b = np.ascontiguousarray(bits, dtype="<u8").view(np.uint8)

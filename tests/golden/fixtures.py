@@ -88,3 +88,38 @@ def detmath(function: str):
     b = np.array([int(r[2], 16) for r in sel], np.uint32)
     e = np.array([int(r[3], 16) for r in sel], np.uint32)
     return a, b, e
+
+
+def lockdown_lumps() -> dict:
+    """dm_lockdown's geometry lumps as {id: (version, bytes)} (the layout
+    make_golden.py writes: "VLMP", count, then id, version, length, bytes)."""
+    blob = (HERE / "dm_lockdown.lumps.bin").read_bytes()
+    assert blob[:4] == b"VLMP"
+    n = int(np.frombuffer(blob, "<i4", 1, 4)[0])
+    p, out = 8, {}
+    for _ in range(n):
+        i, ver, ln = (int(x) for x in np.frombuffer(blob, "<i4", 3, p))
+        p += 12
+        out[i] = (ver, blob[p:p + ln])
+        p += ln
+    assert p == len(blob)
+    return out
+
+
+def lockdown_rays():
+    """The reference's recorded BSP surface tracer set: (rays (n, 7) as
+    start + (end - start) x 1, stock's face per ray (-1 none), its fraction,
+    its m_bHasLuxel)."""
+    rb = (HERE / "rays-lockdown-leafambient.bin").read_bytes()
+    ab = (HERE / "stock-lockdown-leafambient.bin").read_bytes()
+    n = int(np.frombuffer(rb, "<i4", 1)[0])
+    se = np.frombuffer(rb, "<f4", 6 * n, 4).reshape(n, 6)
+    rays = np.empty((n, 7), np.float32)
+    rays[:, 0:3] = se[:, 0:3]
+    rays[:, 3:6] = se[:, 3:6] - se[:, 0:3]
+    rays[:, 6] = 1.0
+    assert int(np.frombuffer(ab, "<i4", 1)[0]) == n and len(ab) == 4 + 9 * n
+    face = np.frombuffer(ab, "<i4", n, 4).copy()
+    frac = np.frombuffer(ab, "<f4", n, 4 + 4 * n).copy()
+    lux = np.frombuffer(ab, "u1", n, 4 + 8 * n) != 0
+    return rays, face, frac, lux

@@ -11,6 +11,13 @@ Each scene is four little-endian binary files (tris, rays, tree, answers).
 They are data, not source, and the GPU test machine has no copy of the
 reference, so the bytes are committed here unchanged.
 
+It also copies the reference's BSP surface tracer fixtures
+(rays-lockdown-leafambient.bin: 8,100 rays; stock-lockdown-leafambient.bin:
+stock's CLightSurface answers for them; README-bsp-rays.md there) and, from
+game/mod_sharp/maps/dm_lockdown.bsp, the geometry lumps that tracer reads
+(planes, vertexes, nodes, texinfo, faces, leafs, edges, surfedges,
+leaffaces), unchanged, into dm_lockdown.lumps.bin.
+
 It also extracts, as text, rows of the reference's DetMath golden table
 (src/SourceSharp.Tests/MapFormats/Numerics/DetMathGoldens.cs, computed by
 the reference's tools/detmath_goldens.py with mpmath at 3000 bits):
@@ -30,6 +37,7 @@ import os
 import pathlib
 import re
 import shutil
+import struct
 import sys
 
 SRC_REL = "src/SourceSharp.Tests/MapTools/Tracing/Fixtures"
@@ -37,7 +45,9 @@ DETMATH_REL = "src/SourceSharp.Tests/MapFormats/Numerics/DetMathGoldens.cs"
 DETMATH_ROWS = {("F1", "Asin"), ("F2", "Pow")}
 HOST_ROWS = {("F1", "Acos"), ("F1", "Sin"), ("F1", "Cos"), ("D1", "Sin"), ("D1", "Cos"), ("D2", "Pow")}
 NAMES = [f"{scene}.{part}.bin" for scene in ("kd-scene", "kd-boxes")
-         for part in ("tris", "rays", "tree", "answers")]
+         for part in ("tris", "rays", "tree", "answers")] + ["rays-lockdown-leafambient.bin",
+                                                             "stock-lockdown-leafambient.bin"]
+BSP_REL = "game/mod_sharp/maps/dm_lockdown.bsp"
 
 
 def main() -> None:
@@ -52,6 +62,19 @@ def main() -> None:
         shutil.copyfile(src / name, dst / name)
         digest = hashlib.sha256((dst / name).read_bytes()).hexdigest()
         lines.append(f"{digest}  {name}")
+    # dm_lockdown's geometry lumps (the BSP surface tracer's inputs), each
+    # copied unchanged: "VLMP", lump count, then per lump its id, version,
+    # length and bytes.
+    sys.path.insert(0, str(dst.parent.parent))
+    from hl2sdk_tools_sharp_b200 import bsp as B
+    lumps = B.lumps_of(str(root / BSP_REL))
+    blob = [b"VLMP", struct.pack("<i", len(lumps))]
+    for i in sorted(lumps):
+        ver, data = lumps[i]
+        blob += [struct.pack("<iii", i, ver, len(data)), data]
+    (dst / "dm_lockdown.lumps.bin").write_bytes(b"".join(blob))
+    lines.append(f"{hashlib.sha256((dst / 'dm_lockdown.lumps.bin').read_bytes()).hexdigest()}  dm_lockdown.lumps.bin")
+    lines.append(f"{hashlib.sha256((root / BSP_REL).read_bytes()).hexdigest()}  (source) {BSP_REL}")
     rows, host = [], []
     pat = re.compile(r'\("(\w+)", "(\w+)", 0x([0-9A-Fa-f]+)UL, 0x([0-9A-Fa-f]+)UL, 0x([0-9A-Fa-f]+)UL\)')
     for m in pat.finditer((root / DETMATH_REL).read_text()):
