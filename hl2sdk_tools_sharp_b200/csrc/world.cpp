@@ -109,9 +109,10 @@ bool luxel_winding(const vrad_face &f, const float *vertices, int64_t nvertices,
 
 // FaceSampleBuilder.BuildFacesamples for one face (number fi): its samples
 // appended to `out`.
-int32_t face_samples(const vrad_face &f, int32_t fi, const float *vertices, int64_t nvertices,
-                     std::vector<vrad_sample> &out) {
-    Winding cell_front, cell_back, row_front, row_back, w;
+// emit(sample) is called for each of the face's samples in order.
+template <class Emit>
+int32_t face_samples_to(const vrad_face &f, int32_t fi, const float *vertices, int64_t nvertices, Emit &&emit) {
+    Winding cell_front, cell_back, row_front, row_back, w, row;
     const FaceFrame fr = face_frame(f);
     const float area_per_luxel = world_area_per_luxel(f);
     if (!luxel_winding(f, vertices, nvertices, fr, w)) return VRAD_ERR_ARG;
@@ -119,7 +120,7 @@ int32_t face_samples(const vrad_face &f, int32_t fi, const float *vertices, int6
     Winding lm = w;
     for (int t = 0; t < fr.height && !lm.empty(); t++) {
         clip_axis(lm, 1, (float)t + 1.0f, kLightmapOnEpsilon, row_front, row_back);
-        Winding row = row_back;
+        row.swap(row_back);
         for (int s = 0; s < fr.width && !row.empty(); s++) {
             clip_axis(row, 0, (float)s + 1.0f, kLightmapOnEpsilon, cell_front, cell_back);
             if (!cell_back.empty()) {
@@ -148,13 +149,18 @@ int32_t face_samples(const vrad_face &f, int32_t fi, const float *vertices, int6
                 o.t = t;
                 o.face = fi;
                 o.cluster = f.cluster;
-                out.push_back(o);
+                emit(o);
             }
-            row = cell_front;
+            row.swap(cell_front);
         }
-        lm = row_front;
+        lm.swap(row_front);
     }
     return VRAD_OK;
+}
+
+int32_t face_samples(const vrad_face &f, int32_t fi, const float *vertices, int64_t nvertices,
+                     std::vector<vrad_sample> &out) {
+    return face_samples_to(f, fi, vertices, nvertices, [&](const vrad_sample &o) { out.push_back(o); });
 }
 
 // Every face's samples, faces built in parallel (each face's samples
@@ -177,6 +183,42 @@ extern "C" int32_t vrad_build_samples(const vrad_face *faces, int32_t nfaces, co
                                       int64_t nvertices, vrad_sample *out, int64_t capacity,
                                       int64_t *count, int64_t *face_first) {
     if (!count) return VRAD_ERR_ARG;
+    if (nfaces < 0 || (nfaces > 0 && (!faces || !vertices))) return VRAD_ERR_ARG;
+    // A face has at most one sample per lightmap cell.  With room for that
+    // many, each face writes its samples straight into `out` at its bound's
+    // offset (in parallel), and the runs are then closed up in face order
+    // (no move at all when every cell has its sample).
+    std::vector<int64_t> ub((size_t)nfaces + 1, 0);
+    for (int32_t f = 0; f < nfaces; f++)
+        ub[(size_t)f + 1] = ub[(size_t)f] + (int64_t)std::max(0, faces[f].lightmap_size[0]) *
+                                                std::max(0, faces[f].lightmap_size[1]);
+    if (out && capacity >= ub[(size_t)nfaces]) {
+        std::vector<int64_t> n((size_t)nfaces, 0);
+        std::atomic<int32_t> rc{VRAD_OK};
+        std::atomic<bool> over{false};
+        vrad::parallel_for(nfaces, 1, [&](int64_t f) {
+            const int64_t cap = ub[(size_t)f + 1] - ub[(size_t)f];
+            int64_t k = 0;
+            const int32_t r = face_samples_to(faces[f], (int32_t)f, vertices, nvertices, [&](const vrad_sample &o) {
+                if (k < cap) out[ub[(size_t)f] + k] = o;
+                k++;
+            });
+            if (r != VRAD_OK) rc = r;
+            if (k > cap) over = true;
+            n[(size_t)f] = k;
+        });
+        if (rc != VRAD_OK) return rc;
+        if (!over) {
+            std::vector<int64_t> first((size_t)nfaces + 1, 0);
+            for (int32_t f = 0; f < nfaces; f++) first[(size_t)f + 1] = first[(size_t)f] + n[(size_t)f];
+            for (int32_t f = 0; f < nfaces; f++)
+                if (first[(size_t)f] != ub[(size_t)f] && n[(size_t)f])
+                    std::memmove(out + first[(size_t)f], out + ub[(size_t)f], sizeof(vrad_sample) * (size_t)n[(size_t)f]);
+            if (face_first) std::copy(first.begin(), first.end(), face_first);
+            *count = first[(size_t)nfaces];
+            return VRAD_OK;
+        }
+    }
     std::vector<std::vector<vrad_sample>> all;
     const int32_t rc = build_all_samples(faces, nfaces, vertices, nvertices, all);
     if (rc != VRAD_OK) return rc;

@@ -143,6 +143,7 @@ def _exact(x) -> Decimal:
 
 # ---------------------------------------------------------------- DetMath (double)
 
+@functools.lru_cache(maxsize=1 << 16)
 def sin_d(x: float) -> float:
     """DetMath.Sin: the double nearest sin x."""
     x = float(x)
@@ -151,6 +152,7 @@ def sin_d(x: float) -> float:
     return to_double(_sin_cos(_exact(x))[0])
 
 
+@functools.lru_cache(maxsize=1 << 16)
 def cos_d(x: float) -> float:
     """DetMath.Cos: the double nearest cos x."""
     x = float(x)
@@ -159,6 +161,7 @@ def cos_d(x: float) -> float:
     return to_double(_sin_cos(_exact(x))[1])
 
 
+@functools.lru_cache(maxsize=1 << 16)
 def pow_d(x: float, y: float) -> float:
     """DetMath.Pow for the arguments the lighting tables use (x >= 0):
     the double nearest x**y."""
