@@ -72,6 +72,8 @@ def parse():
 
 def world_for(side: int, seed: int = CONFIG_SEED):
     from hl2sdk_tools_sharp_b200 import roomgrid as rg
+    if side == 16:
+        return rg.generate(rg.config_large(seed))
     cfg = rg.config_8x8(seed) if side == 8 else rg.config_3x3(seed)
     if side not in (3, 8):
         cfg.side = side

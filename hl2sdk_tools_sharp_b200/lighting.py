@@ -302,12 +302,17 @@ def parse_intensity(color, light_scale: float = 1.0, hdr: bool = False) -> np.nd
     return LT.parse_intensity(text, hdr=hdr, light_scale=light_scale)[0]
 
 
+def light_set(world: World, hdr: bool = False) -> LT.DirectLightSet:
+    """The map's light entities through the restated DirectLightBuilder."""
+    return LT.build(rg.entities(world), lambda o: rg.cluster_of_point(world, o), hdr=hdr)
+
+
 def build_lights(world: World, hdr: bool = False):
     """The active DirectLight list and the per-cluster light lists, for the
     LDR pass or (hdr) the HDR pass: the map's light entities
     (roomgrid.entities) through the restated DirectLightBuilder
     (lights.build).  Returns (lights, cluster_offsets, cluster_lights)."""
-    ls = LT.build(rg.entities(world), lambda o: rg.cluster_of_point(world, o), hdr=hdr)
+    ls = light_set(world, hdr)
     if ls.unsupported_class_names:
         raise ValueError(f"unsupported light entities: {ls.unsupported_class_names}")
     lights = LT.to_records(ls.active, LIGHT_DTYPE)
@@ -351,6 +356,14 @@ def prepare(world: World, hdr: bool = False) -> LightingInputs:
     lights, off, flat = build_lights(world)
     inp = LightingInputs(faces, verts, samples, first, lights, off, flat,
                          ambient_directions().astype(np.float32), np.zeros((0, 3), np.float32))
+    extent = light_set(world).sun_angular_extent
+    if extent > 0:
+        # A sun with a spread: the configured count of jittered rays, ray d
+        # jittered by the sampler's direction d - 1 (DirectLightGatherer's
+        # SamplerPrefix).
+        inp.sun_angular_extent = np.float32(extent)
+        inp.sun_samples = int(world.config.sun_samples)
+        inp.sun_jitter = ambient_directions(max(1, inp.sun_samples - 1)).astype(np.float32)
     if hdr:
         inp.lights_hdr, off_h, flat_h = build_lights(world, hdr=True)
         assert np.array_equal(off, off_h) and np.array_equal(flat, flat_h)

@@ -55,12 +55,22 @@ class Config:
     reflectivity: tuple[float, float] = (0.1, 0.7)
     materials: int = 8
     sky_ambient: bool = False
+    sun_spread: float = 0.0          # the light_environment's SunSpreadAngle (degrees); 0: one sun ray
+    sun_samples: int = 30            # jittered sun rays with a spread (the reference fixes 30)
 
 
 def config_3x3(seed: int = 1) -> Config:
     """Plain vrad, CPU-runnable: 3 x 3 rooms, scale 16, 4 point lights + sun."""
     return Config(side=3, seed=seed, luxel_scale=16.0, pillars=(0, 0), lights=4, spot_fraction=0.0,
                   sky_ambient=False)
+
+
+def config_large(seed: int = 1) -> Config:
+    """The Large configuration without its displaced floors and AO (neither
+    is built): 16 x 16 rooms + 0-6 pillars each, scale 8, 256 point and spot
+    lights, a sun of 256 jittered rays (spread 2 degrees) + sky, HDR."""
+    return Config(side=16, seed=seed, luxel_scale=8.0, pillars=(0, 6), lights=256, spot_fraction=0.5,
+                  sky_ambient=True, sun_spread=2.0, sun_samples=256)
 
 
 def config_8x8(seed: int = 1) -> Config:
@@ -469,6 +479,8 @@ def entities(world: World) -> list:
     out = [[("classname", "worldspawn")]]
     env = [("classname", "light_environment"), ("origin", "0 0 0"), ("target", "sun_target"),
            ("_light", col(world.sun_color)), ("_ambient", col(world.ambient_color))]
+    if world.config.sun_spread > 0:
+        env.append(("SunSpreadAngle", _num(world.config.sun_spread)))
     if world.sun_color_hdr is not None:
         env += [("_lightHDR", col(world.sun_color_hdr)), ("_ambientHDR", col(world.ambient_color_hdr)),
                 ("_AmbientScaleHDR", _num(world.ambient_scale_hdr))]

@@ -74,7 +74,7 @@ def main() -> None:
         blob += [struct.pack("<iii", i, ver, len(data)), data]
     (dst / "dm_lockdown.lumps.bin").write_bytes(b"".join(blob))
     lines.append(f"{hashlib.sha256((dst / 'dm_lockdown.lumps.bin').read_bytes()).hexdigest()}  dm_lockdown.lumps.bin")
-    lines.append(f"{hashlib.sha256((root / BSP_REL).read_bytes()).hexdigest()}  (source) {BSP_REL}")
+    lines.append(f"# the lumps' source, {BSP_REL}: {hashlib.sha256((root / BSP_REL).read_bytes()).hexdigest()}")
     rows, host = [], []
     pat = re.compile(r'\("(\w+)", "(\w+)", 0x([0-9A-Fa-f]+)UL, 0x([0-9A-Fa-f]+)UL, 0x([0-9A-Fa-f]+)UL\)')
     for m in pat.finditer((root / DETMATH_REL).read_text()):

@@ -22,7 +22,7 @@ def test_fixture_hashes():
     import pathlib
     here = pathlib.Path(fixtures.__file__).parent
     for line in (here / "SHA256SUMS").read_text().split("\n"):
-        if not line.strip():
+        if not line.strip() or line.startswith("#"):
             continue
         digest, name = line.split()
         assert hashlib.sha256((here / name).read_bytes()).hexdigest() == digest, name
