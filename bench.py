@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-learned", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-batch", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--no-ambient", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--batch-maps", type=int, default=32, help=argparse.SUPPRESS)
     ap.add_argument("--batch-workers", type=int, default=4, help=argparse.SUPPRESS)
     return ap.parse_args()
@@ -702,6 +703,92 @@ def batched_run(args, device_index: int, rank: int = 0, world: int = 1) -> dict:
 TRAFFIC_PER_TRANSFER_RAY = (92441088 + 49963008) / 19922134.0
 
 
+def lockdown_ambient_lumps(seed: int = 3) -> dict:
+    """dm_lockdown's geometry lumps (the committed fixture) with a seeded
+    synthetic lighting lump, texture reflectivities and a sky ambient light:
+    the fixture keeps the map's geometry, not its 6 MB lighting."""
+    from hl2sdk_tools_sharp_b200 import ambient as A, bsp as B
+    from tests.golden import fixtures as F
+    lumps = dict(F.lockdown_lumps())
+    rng = np.random.default_rng(seed)
+    faces = np.frombuffer(lumps[B.LUMP_FACES][1], B.FACE)
+    texinfo = np.frombuffer(lumps[B.LUMP_TEXINFO][1], B.TEXINFO)
+    ntex = int(texinfo["texdata"].max()) + 1
+    td = np.zeros(ntex, A.TEXDATA)
+    td["reflectivity"] = rng.uniform(0.05, 0.9, (ntex, 3)).astype(np.float32)
+    styles = (faces["styles"] != 255).sum(1)
+    size = (faces["lm_size"][:, 0].astype(np.int64) + 1) * (faces["lm_size"][:, 1] + 1) * 4 * np.maximum(styles, 1)
+    end = int(np.max(np.where(faces["lightofs"] >= 0, faces["lightofs"] + 4 * size, 0)))
+    light = rng.integers(0, 256, end + 64, dtype=np.uint8)
+    light[3::4] = rng.integers(-9, 3, len(light[3::4])).astype(np.int8).view(np.uint8)
+    wl = np.zeros(2, A.WORLDLIGHT)
+    wl["type"] = (1, A.EMIT_SKYAMBIENT)
+    wl["intensity"][1] = (0.25, 0.5, 0.75)
+    lumps[B.LUMP_TEXDATA] = (0, td.tobytes())
+    lumps[B.LUMP_LIGHTING] = (1, light.tobytes())
+    lumps[A.LUMP_WORLDLIGHTS] = (0, wl.tobytes())
+    return lumps
+
+
+def ambient_run(args, samples: int = 131072) -> dict:
+    """The leaf ambient ray cubes (vrad_ambient_cubes) on dm_lockdown's
+    geometry: `samples` seeded points in its open leaves, 162 rays each,
+    timed on the device (inputs resident) and end to end through the host
+    call; the first 2,048 cubes checked against the oracle, which is also
+    timed on a bounded sample on the host's cores."""
+    import torch
+    from hl2sdk_tools_sharp_b200 import ambient as A, bsp as B
+    lumps = lockdown_ambient_lumps()
+    leaves = np.frombuffer(lumps[B.LUMP_LEAFS][1], B.LEAF_V0 if lumps[B.LUMP_LEAFS][0] == 0 else B.LEAF_V1)
+    open_ = leaves[(leaves["contents"] & A.CONTENTS_SOLID) == 0]
+    rng = np.random.default_rng(17)
+    pick = open_[rng.integers(0, len(open_), samples)]
+    u = rng.uniform(0.02, 0.98, (samples, 3))
+    pos = (pick["mins"] + u * (pick["maxs"].astype(np.float64) - pick["mins"])).astype(np.float32)
+    out = {"workload": f"dm_lockdown geometry ({len(np.frombuffer(lumps[B.LUMP_NODES][1], B.NODE))} nodes, "
+                       f"{len(np.frombuffer(lumps[B.LUMP_FACES][1], B.FACE))} faces), seeded synthetic lighting, "
+                       f"{samples} seeded points in open leaves x 162 rays",
+           "samples": samples, "rays": samples * A.DIRECTIONS}
+    with A.CudaAmbientSampler(lumps) as s:
+        stream = torch.cuda.current_stream()
+        d_pos = torch.from_numpy(pos).cuda()
+        d_out = torch.empty((samples, A.SIDES, 3), dtype=torch.float32, device="cuda")
+        for _ in range(2):
+            s.cubes_device(d_pos, out=d_out, stream=stream.cuda_stream)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 5
+        a.record(stream)
+        for _ in range(reps):
+            s.cubes_device(d_pos, out=d_out, stream=stream.cuda_stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        s.status()
+        ms = a.elapsed_time(b) / reps
+        t = time.perf_counter()
+        host = s.cubes(pos)
+        e2e_s = time.perf_counter() - t
+    out.update({"ms": ms, "rays_per_s": out["rays"] / (ms / 1000.0), "samples_per_s": samples / (ms / 1000.0),
+                "e2e": {"s": e2e_s, "rays_per_s": out["rays"] / e2e_s, "h2d_bytes": int(pos.nbytes),
+                        "d2h_bytes": int(host.nbytes)},
+                "gpu_launches_per_call": 2 * ((samples + 16383) // 16384)})
+    if not args.no_cpu:
+        from oracle import oracle as O
+        geom = B.trace_geometry(lumps)
+        r = A.ambient_range(lumps, False)
+        check = 2048
+        threads = O.default_threads()
+        t = time.perf_counter()
+        want = O.ambient_cubes(geom, r.faces, r.lighting, A.anorms(), float(A.cone_tan()), r.sky_ambient,
+                               pos[:check], threads=threads)
+        cpu_s = time.perf_counter() - t
+        out["check"] = {"samples": check,
+                        "mismatched_samples": int((host[:check].view(np.uint32) != want.view(np.uint32))
+                                                  .any(axis=(1, 2)).sum())}
+        out["cpu_baseline"] = {"kind": "port", "cores": threads, "sample": f"{check} samples x 162 rays",
+                               "rays_per_s": check * A.DIRECTIONS / cpu_s}
+    return out
+
+
 def main_stage(args):
     import torch
     from hl2sdk_tools_sharp_b200 import lighting as L, tracer as T
@@ -888,13 +975,15 @@ def main_stage(args):
     peak = float(peaks.get("hbm_gbs", 6650.0))
 
     # The learned warm start (LDR range): a network trained on the device on
-    # plain bounce solutions of eight small seeded maps (2 to 6 rooms a
-    # side), then this map bounced from its guess, against the plain bounce.
+    # plain bounce solutions of 32 seeded maps (2 to 8 rooms a side), then
+    # this map and three held-out maps bounced from its guess, against the
+    # plain bounce, with each held-out map's guess error and contraction.
     learned = None
     if rank == 0 and not args.no_learned:
         from hl2sdk_tools_sharp_b200 import learned as LN
+        train_maps = 32
         t = time.perf_counter()
-        lx, lt = LN.collect([LN.training_config(k) for k in range(8)], threshold=BOUNCE_THRESHOLD)
+        lx, lt = LN.collect([LN.training_config(k) for k in range(train_maps)], threshold=BOUNCE_THRESHOLD)
         collect_s = time.perf_counter() - t
         net = LN.Network(stage.tracer, seed=7)
         ta, tb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -920,12 +1009,19 @@ def main_stage(args):
         fwd_ms = ta.elapsed_time(tb) / 10
         flops = 2.0 * (32 * 128 + 128 * 128 + 128 * 8) * len(hx)
         tpeak = float(peaks.get("bf16_tflops", 1590.0))
+        guess = y.float().expm1().clamp_min(0)
+        conv = ht.float().expm1()
+        t = time.perf_counter()
+        held_out = LN.evaluate(net, [LN.heldout_config(k) for k in range(3)], threshold=BOUNCE_THRESHOLD)
+        held_s = time.perf_counter() - t
         learned = {"range": "LDR", "plain_bounces": int(bp.bounces), "warm_bounces": int(bw.bounces),
+                   "eps": float((guess - conv).abs().mean() / conv.abs().mean()),
+                   "held_out": held_out, "held_out_s": held_s,
                    "plain_bounce_ms": bp.bounce_ms, "warm_bounce_ms": bw.bounce_ms,
                    "iteration_ratio": bp.bounces / max(1, bw.bounces),
                    "lightmap_within_1_lsb": LN.within_one_lsb(warm_lump, plain_lump),
                    "guess_abs_error_log1p": float((y - ht).abs().mean().item()),
-                   "training": {"maps": 8, "rows": int(len(lx)), "steps": 3000, "batch": 32768,
+                   "training": {"maps": train_maps, "rows": int(len(lx)), "steps": 3000, "batch": 32768,
                                 "collect_s": collect_s, "train_ms": train_ms, "final_loss": loss},
                    "roofline": {"bound": "tensor", "kernel": "k_mlp_forward (mma.sync bf16, fp32 accumulate)",
                                 "achieved": flops / (fwd_ms / 1000.0) / 1e12, "peak": tpeak, "unit": "TFLOP/s",
@@ -935,6 +1031,7 @@ def main_stage(args):
     batched = None
     if not args.no_batch:
         batched = batched_run(args, local, rank, world_size)
+    leaf_ambient = ambient_run(args) if rank == 0 and not args.no_ambient else None
     # The dominant phases on the launching stream: both ranges' direct
     # gather (the two-range first round and each range's supersampling
     # passes), timed by a host-buffer pass, and the transfer build (its
@@ -1010,6 +1107,7 @@ def main_stage(args):
             "check": check,
             "learned": learned,
             "batched": batched,
+            "leaf_ambient": leaf_ambient,
         }
         print(json.dumps(line), flush=True)
     stage.close()

@@ -220,6 +220,7 @@ cudaError_t release_tables(vrad_ctx *ctx) {
     ctx->bounce.release();
     ctx->supersample.release();
     ctx->bsp.release();
+    ctx->ambient.release();
     vrad::dev_free(ctx->sample_light);
     ctx->sample_light = nullptr;
     vrad::dev_free(ctx->sample_light_hdr);
@@ -297,6 +298,7 @@ int32_t vrad_destroy(vrad_ctx *ctx) {
         ctx->supersample.free_pinned();
         ctx->shelf.release();
         ctx->bsp.release();
+        ctx->ambient.release();
         vrad::dev_free(ctx->sample_light);
         vrad::dev_free(ctx->sample_light_hdr);
         cudaFree(ctx->status);

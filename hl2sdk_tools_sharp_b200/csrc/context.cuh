@@ -8,6 +8,7 @@
 #include <thread>
 #include <vector>
 
+#include "ambient.cuh"
 #include "bounce.cuh"
 #include "bsp_trace.cuh"
 #include "direct.cuh"
@@ -62,6 +63,7 @@ struct vrad_ctx {
     int32_t nclusters = 0;
     vrad::BounceBuffers bounce;
     vrad::BspBuffers bsp;            // a map's BSP tree for the surface walk (vrad_bsp_upload)
+    vrad::AmbientBuffers ambient;    // its lighting for the leaf ambient sample (vrad_ambient_upload)
     // The uploaded world's patch forest, grown ahead on a host thread while
     // the rest of the world upload runs, with the chop sizes of this
     // context's last bounce upload; the next bounce upload takes it when

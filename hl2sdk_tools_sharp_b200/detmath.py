@@ -13,7 +13,9 @@ that every machine builds the same bits:
     (DetMath.cs:151-187);
   * the light colours' gamma, RadLightFile.ParseIntensity
     (MapFormats/Text/RadLightFile.cs:383-396): DetMath.Pow in double;
-  * LightNormals.FromProps (Rad/Light/LightNormals.cs:66-107).
+  * LightNormals.FromProps (Rad/Light/LightNormals.cs:66-107);
+  * the leaf ambient cone's tangent (Rad/Ambient/AmbientSampler.cs:142):
+    DetMathF.Tan of a float.
 
 These tables are made once per map on the host, so the functions here are
 written for exactness, not speed: each value is evaluated in decimal at 60
@@ -206,6 +208,17 @@ def cos_f(x) -> np.float32:
     if not np.isfinite(x):
         return np.float32(np.cos(x))
     return to_single(_sin_cos(_exact(x))[1])
+
+
+def tan_f(x) -> np.float32:
+    """DetMathF.Tan: the float nearest tan x, x a float."""
+    x = np.float32(x)
+    if x == 0 or not np.isfinite(x):
+        return np.float32(np.tan(x))
+    s, c = _sin_cos(_exact(x))
+    with localcontext() as ctx:
+        ctx.prec = _PREC + 20
+        return to_single(s / c)
 
 
 def acos_f(x) -> np.float32:

@@ -116,10 +116,10 @@ class Network:
 
 def training_config(k: int, seed0: int = 100):
     """The k-th training map: an 8x8-style room grid (pillars, point and
-    spot lights, sun and sky) of 2 to 6 rooms a side, one light per room."""
+    spot lights, sun and sky) of 2 to 8 rooms a side, one light per room."""
     import dataclasses
     from . import roomgrid as rg
-    side = 2 + k % 5
+    side = 2 + k % 7
     return dataclasses.replace(rg.config_8x8(seed0 + k), side=side, lights=side * side)
 
 
@@ -168,3 +168,53 @@ def within_one_lsb(a: np.ndarray, b: np.ndarray) -> float:
     fb = vb[:, :3] * np.exp2(eb)[:, None]
     lsb = np.exp2(np.maximum(ea, eb))[:, None]
     return float((np.abs(fa - fb) <= lsb).all(1).mean())
+
+
+def heldout_config(k: int, seed0: int = 900):
+    """The k-th held-out map: the training maps' kind, seeds no training map
+    uses, sides 3, 5 and 7 rooms."""
+    import dataclasses
+    from . import roomgrid as rg
+    side = (3, 5, 7)[k % 3]
+    return dataclasses.replace(rg.config_8x8(seed0 + k), side=side, lights=side * side)
+
+
+def evaluate(net: Network, configs, threshold: float = 0.1, bounces: int = 100) -> list:
+    """Per map: the plain and the warm bounce counts, the guess's relative
+    error eps (mean |G - T| over mean T, G the network's converged-light
+    guess, T the plain bounce's converged light, per receiver and channel),
+    the plain iteration's contraction rho (the geometric mean of the ratio
+    between successive bounces' added light: (A_n / A_1)^(1 / (n - 1)),
+    A_k the light bounce k adds), the savings the bound log(1/eps) /
+    log(1/rho) predicts, and whether the warm lump is within 1 LSB of the
+    plain one."""
+    import math
+    from . import lighting as L, roomgrid as rg
+    out = []
+    for cfg in configs:
+        w = rg.generate(cfg)
+        off, lst = L.pvs_lists(w)
+        refl = L.face_reflectivity(w)
+        with L.LightingStage(w) as st:
+            st.upload_bounce(refl, off, lst, bounces=1, threshold=0.0)
+            st.light_pass()
+            a1 = sum(st.bounce_stats().added)
+            st.upload_bounce(refl, off, lst, bounces=bounces, threshold=threshold)
+            plain_lump, _, _ = st.light_pass()
+            bp = st.bounce_stats()
+            an = sum(bp.added)
+            x, t = st.bounce_features()
+            y = net.forward(x)
+            g, tt = y.float().expm1().clamp_min(0), t.float().expm1()
+            eps = float((g - tt).abs().mean() / tt.abs().mean().clamp_min(1e-30))
+            st.set_bounce_model(net)
+            warm_lump, _, _ = st.light_pass()
+            bw = st.bounce_stats()
+            st.set_bounce_model(None)
+        n = int(bp.bounces)
+        rho = (an / a1) ** (1.0 / (n - 1)) if n > 1 and a1 > 0 and an > 0 else float("nan")
+        pred = math.log(1.0 / eps) / math.log(1.0 / rho) if 0 < eps < 1 and 0 < rho < 1 else float("nan")
+        out.append({"side": cfg.side, "seed": cfg.seed, "receivers": int(len(x)), "plain_bounces": n,
+                    "warm_bounces": int(bw.bounces), "eps": eps, "rho": rho, "bound_savings": pred,
+                    "within_1_lsb": within_one_lsb(warm_lump, plain_lump)})
+    return out

@@ -667,6 +667,106 @@ int32_t vrad_bsp_trace_closest(vrad_ctx *ctx, const vrad_ray *rays, int64_t n, c
 int32_t vrad_bsp_trace_closest_device(vrad_ctx *ctx, const vrad_ray *d_rays, int64_t n, float min_distance,
                                       vrad_hit *d_hits, void *stream);
 
+/* ---- Leaf ambient ---------------------------------------------------------
+ *
+ * Stock vrad's per-leaf ambient cubes (ComputePerLeafAmbientLighting,
+ * MapTools/Rad/Ambient/LeafAmbientBuilder.cs:22-688), the stage that is
+ * 51.6 % of stock vrad's wall clock.  Two parts live here:
+ *   vrad_leaf_ambient_positions  each leaf's candidate sample positions
+ *     (host code: LeafAmbientBuilder.PlanSamples, :252-276, over
+ *     LeafSampler.Generate, LeafSampler.cs:38-148);
+ *   vrad_ambient_cubes  at each position the 162 rays into the map through
+ *     the BSP surface walk, each hit's lightmap colour blended by the cone
+ *     (RayAmbientLighting.Accumulate, RayAmbientLighting.cs:89-134), and
+ *     the colours projected onto the six cube sides (AmbientCube.Project,
+ *     AmbientCube.cs:80-103): AmbientSampler.ComputeRayCube
+ *     (AmbientSampler.cs:211-227), on the device.
+ * The baked surface lights (AmbientSampler.AddSurfaceLights), the 16-sample
+ * list and the lump encoding are not part of these calls, and neither are
+ * displacements: a map with displacement faces is the caller's to refuse. */
+
+/* The BSP pieces the sampler reads, one int32 array per lump, widened:
+ *   planes        nplanes x 4 floats: normal xyz, dist
+ *   nodes         nnodes x 3: plane, child 0, child 1 (a leaf is -1 - leaf)
+ *   leaves        nleaves x 9: contents, mins xyz, maxs xyz, first leaf
+ *                 brush, leaf brush count
+ *   leaf_brushes  nleaf_brushes brush numbers
+ *   brushes       nbrushes x 3: first side, side count, contents
+ *   brush_sides   nbrush_sides x 2: plane, bevel */
+typedef struct vrad_ambient_tree {
+    const float *planes;
+    int32_t nplanes;
+    const int32_t *nodes;
+    int32_t nnodes;
+    const int32_t *leaves;
+    int32_t nleaves;
+    const int32_t *leaf_brushes;
+    int32_t nleaf_brushes;
+    const int32_t *brushes;
+    int32_t nbrushes;
+    const int32_t *brush_sides;
+    int32_t nbrush_sides;
+} vrad_ambient_tree;
+
+/* Every leaf's candidate sample positions in leaf order: counts[l] = the
+ * leaf's candidate count (stock's, with the sample-count quirk that sizes
+ * all three axes by x: LeafAmbientBuilder.CandidateSampleCount, :420-454;
+ * 0 for a solid leaf), positions = the positions, 3 floats each, leaf after
+ * leaf.  Each leaf draws from its own stream seeded 0, as stock's
+ * per-leaf CLeafSampler does.  With positions NULL only counts and *total
+ * are filled; otherwise capacity (in positions) must hold *total.  Host
+ * code on `threads` threads (0: all); needs no device. */
+int32_t vrad_leaf_ambient_positions(const vrad_ambient_tree *tree, int32_t *counts, float *positions,
+                                    int64_t capacity, int64_t *total, int32_t threads);
+
+/* One BSP face's lightmap lookups (AmbientScene's FaceShade,
+ * AmbientScene.cs:247-318).  styles packs the four style bytes, slot 0 in
+ * the low byte; averages[k] is slot k's average colour (the four bytes
+ * before the lightmap, counting back) decoded and tinted by reflectivity. */
+#define VRAD_AMBIENT_SKY 1          /* SURF_SKY: a hit reads the sky ambient  */
+#define VRAD_AMBIENT_BAD_AVERAGE 2  /* a slot's average lies outside the lump */
+typedef struct vrad_ambient_face {
+    int32_t lightofs;    /* byte offset of the face's lightmap; -1: none */
+    int32_t smax, tmax;  /* luxels a row, rows */
+    int32_t stride;      /* luxels between style slots (x4 when bumped) */
+    int32_t nstyles;     /* slots in use, up to 4 */
+    uint32_t styles;
+    int32_t flags;       /* VRAD_AMBIENT_* */
+    float reflectivity[3];
+    float averages[4][3];
+} vrad_ambient_face;
+
+/* The lighting the cubes read: one range's lighting lump (LDR or HDR), the
+ * faces' records (the range's face lump), the 162 sample directions
+ * (VertexNormals; 3 floats each), tan of the cone's inner half-angle, and
+ * the sky ambient (the range's first emit_skyambient world light's
+ * intensity) when the map has one.  Needs vrad_bsp_upload of the same map;
+ * nfaces must equal its surface count. */
+typedef struct vrad_ambient_lighting {
+    const uint8_t *lighting;
+    int64_t lighting_bytes;
+    const vrad_ambient_face *faces;
+    int32_t nfaces;
+    const float *directions;
+    int32_t ndirections;  /* 162 */
+    float tan_theta;
+    int32_t has_sky_ambient;
+    float sky_ambient[3];
+} vrad_ambient_lighting;
+
+int32_t vrad_ambient_upload(vrad_ctx *ctx, const vrad_ambient_lighting *lighting);
+
+/* The ray cubes at n positions (3 floats each): cubes[6 n] colours (3
+ * floats each), sides +x, -x, +y, -y, +z, -z.  Fails with VRAD_ERR_ARG
+ * when a ray hits a face whose lightmap or averages lie outside the lump
+ * (the reference's InvalidOperationException) and with VRAD_ERR_CUDA when a
+ * walk goes deeper than 64 pending splits.  Host buffers; blocks.  The
+ * _device form takes device buffers and queues on `stream`; its faults
+ * are reported by the next vrad_ambient_status. */
+int32_t vrad_ambient_cubes(vrad_ctx *ctx, const float *positions, int64_t n, float *cubes);
+int32_t vrad_ambient_cubes_device(vrad_ctx *ctx, const float *d_positions, int64_t n, float *d_cubes, void *stream);
+int32_t vrad_ambient_status(vrad_ctx *ctx);
+
 /* ---- Batches of maps ------------------------------------------------------
  *
  * Many maps lit on one device.  No counterpart in the reference, which

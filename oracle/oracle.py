@@ -207,6 +207,200 @@ def bsp_trace(geom, rays: np.ndarray, min_frac: float = 0.0, threads: int | None
     return face, frac
 
 
+def ambient_cubes(geom, faces: np.ndarray, light: np.ndarray, dirs: np.ndarray, tan_theta: float, sky,
+                  positions: np.ndarray, threads: int | None = None) -> np.ndarray:
+    """AmbientSampler.ComputeRayCube restated (bsp_oracle.cpp) at each
+    position: (n, 6, 3) float32.  faces is the product's 88-byte face record
+    array; sky the sky ambient (3 floats) or None."""
+    L = lib()
+    if not getattr(L, "_ambient_typed", False):
+        P, i32, i64, f32 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_float
+        L.orc_ambient_cubes.argtypes = [P, P, P, P, P, P, i32, P, P, P, P, P, i64, P, f32, i32, P, P, i64, P, i32]
+        L.orc_ambient_cubes.restype = ctypes.c_int
+        L._ambient_typed = True
+    keep = [np.ascontiguousarray(a) for a in (geom.nodes, geom.surfaces, geom.node_faces, geom.leaf_faces,
+                                               geom.leaf_start, geom.leaf_count, geom.sky_points, geom.sky_start,
+                                               geom.sky_count)]
+    faces = np.ascontiguousarray(faces)
+    assert faces.dtype.itemsize == 88
+    light = np.ascontiguousarray(light, np.uint8)
+    dirs = np.ascontiguousarray(dirs, np.float32)
+    pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+    skyv = np.zeros(3, np.float32) if sky is None else np.asarray(sky, np.float32)
+    out = np.zeros((len(pos), 6, 3), np.float32)
+    rc = L.orc_ambient_cubes(_p(keep[0]), _p(keep[1]), _p(keep[2]), _p(keep[3]), _p(keep[4]), _p(keep[5]),
+                             len(geom.leaf_start), _p(keep[6]), _p(keep[7]), _p(keep[8]), _p(faces),
+                             _p(light) if len(light) else None, len(light), _p(dirs), tan_theta,
+                             int(sky is not None), _p(skyv), _p(pos), len(pos), _p(out),
+                             threads if threads is not None else default_threads())
+    if rc != 0:
+        raise RuntimeError(f"orc_ambient_cubes failed: {rc}")
+    return out
+
+
+class Ran1:
+    """Stock's uniform random stream (MapTools/Rad/Ambient/StockRandomStream.cs:
+    13-234): Park-Miller minimal standard draws through a 32-entry
+    Bays-Durham shuffle; RandomFloat = (float)(AM * draw), capped at
+    RNMX, scaled into [lo, hi] in float."""
+    NTAB, IA, IM, IQ, IR = 32, 16807, 2147483647, 127773, 2836
+    NDIV = 1 + (IM - 1) // NTAB
+    AM = 1.0 / IM
+    RNMX = 1.0 - 1.2e-7
+
+    def __init__(self, seed: int = 0):
+        self.idum = seed if seed < 0 else -seed
+        self.iy = 0
+        self.iv = [0] * self.NTAB
+
+    def _step(self):
+        k = int(self.idum / self.IQ)          # C# int division truncates toward zero
+        self.idum = self.IA * (self.idum - k * self.IQ) - self.IR * k
+        if self.idum < 0:
+            self.idum += self.IM
+
+    def draw(self) -> int:
+        if self.idum <= 0 or self.iy == 0:
+            self.idum = 1 if -self.idum < 1 else -self.idum
+            for j in range(self.NTAB + 7, -1, -1):
+                self._step()
+                if j < self.NTAB:
+                    self.iv[j] = self.idum
+            self.iy = self.iv[0]
+        self._step()
+        slot = self.iy // self.NDIV
+        self.iy = self.iv[slot]
+        self.iv[slot] = self.idum
+        return self.iy
+
+    def uniform(self, lo=0.0, hi=1.0) -> np.float32:
+        fl = np.float32(self.AM * self.draw())
+        if float(fl) > self.RNMX:
+            fl = np.float32(self.RNMX)
+        lo, hi = np.float32(lo), np.float32(hi)
+        return np.float32(np.float32(fl * np.float32(hi - lo)) + lo)
+
+
+def leaf_positions(planes, nodes, leaves, leaf_brushes, brushes, brush_sides):
+    """Every leaf's candidate ambient sample positions, restated in Python
+    (MapTools/Rad/Ambient: LeafAmbientBuilder.CandidateSampleCount :420-454
+    with stock's all-axes-by-x quirk, BspParents :31-96,
+    LeafBoundaryPlanes.Gather :32-70, LeafBrushTrace :43-265,
+    LeafSampler.Generate :38-148); the arrays are the product's
+    vrad_ambient_tree layout.  Returns (counts, (n, 3) float32)."""
+    f32 = np.float32
+
+    def dot(a, b):
+        return f32(f32(f32(a[0] * b[0]) + f32(a[1] * b[1])) + f32(a[2] * b[2]))
+
+    node_parent = [0] * len(nodes)
+    leaf_parent = [0] * len(leaves)
+    if len(nodes):
+        node_parent[0] = -1
+        stack = [0]
+        while stack:
+            n = stack.pop()
+            for ch in (int(nodes[n][1]), int(nodes[n][2])):
+                if ch < 0:
+                    leaf_parent[-ch - 1] = n
+                else:
+                    node_parent[ch] = n
+                    stack.append(ch)
+
+    def clip(brush, p1, p2):
+        first, count = int(brushes[brush][0]), int(brushes[brush][1])
+        if count == 0:
+            return f32(1), None, False
+        enter, leave, clip_plane, start_out = f32(-9999.0), f32(1.0), -1, False
+        for i in range(count):
+            pnum, bevel = int(brush_sides[first + i][0]), int(brush_sides[first + i][1])
+            if bevel == 1:
+                continue
+            nrm, dist = planes[pnum][:3], planes[pnum][3]
+            d1 = f32(dot(p1, nrm) - dist)
+            d2 = f32(dot(p2, nrm) - dist)
+            if d1 > 0 and d2 > 0:
+                return f32(1), None, False
+            if d1 > 0:
+                start_out = True
+            if d1 <= 0 and d2 <= 0:
+                continue
+            if d1 > d2:
+                f = f32((float(d1) - 0.03125) / float(f32(d1 - d2)))
+                if f > enter:
+                    enter, clip_plane = f, pnum
+            else:
+                f = f32((float(d1) + 0.03125) / float(f32(d1 - d2)))
+                if f < leave:
+                    leave = f
+        if not start_out:
+            return f32(1), None, True
+        if enter < leave and enter > f32(-9999.0) and enter < f32(1.0):
+            return max(enter, f32(0)), planes[clip_plane][:3], False
+        return f32(1), None, False
+
+    def brush_trace(leaf, start, end):
+        L = leaves[leaf]
+        for i in range(int(L[8])):
+            b = int(leaf_brushes[int(L[7]) + i])
+            if (int(brushes[b][2]) & (0x1 | 0x4000 | 0x80)) == 0:
+                continue
+            frac, nrm, solid = clip(b, start, end)
+            if frac != 1 or solid:
+                return (f32(0) if solid else frac), nrm, solid
+        return f32(1), None, False
+
+    counts = np.zeros(len(leaves), np.int32)
+    out = []
+    for l, L in enumerate(leaves):
+        if int(L[0]) & 1:
+            continue
+        x = max((int(L[4]) - int(L[1])) // 32 if int(L[4]) >= int(L[1]) else -((int(L[1]) - int(L[4])) // 32), 1)
+        v = (x * x * x) & 0xFFFFFFFF
+        v = v - (1 << 32) if v >= 1 << 31 else v
+        counts[l] = min(max(v, 1), 128)
+        bound_planes = []
+        node, child = leaf_parent[l], -(l + 1)
+        while node >= 0:
+            p = planes[int(nodes[node][0])]
+            if int(nodes[node][1]) == child:
+                bound_planes.append((p[:3].astype(f32), f32(p[3])))
+            else:
+                bound_planes.append(((-p[:3]).astype(f32), f32(-p[3])))
+            child, node = node, node_parent[node]
+        mn = [f32(L[1]), f32(L[2]), f32(L[3])]
+        mx = [f32(L[4]), f32(L[5]), f32(L[6])]
+        ext = [f32(int(L[4]) - int(L[1])), f32(int(L[5]) - int(L[2])), f32(int(L[6]) - int(L[3]))]
+        rng = Ran1()
+        for _ in range(int(counts[l])):
+            pos, valid = None, False
+            for _try in range(1000):
+                a, b, c = rng.uniform(0, ext[0]), rng.uniform(0, ext[1]), rng.uniform(0, ext[2])
+                pos = [f32(mn[0] + a), f32(mn[1] + b), f32(mn[2] + c)]
+                valid = all(f32(dot(n, pos) - d) >= f32(0.03125) for n, d in bound_planes)
+                if not valid:
+                    continue
+                for j in range(6):
+                    axis = j % 3
+                    end = list(pos)
+                    end[axis] = mn[axis] if j < 3 else mx[axis]
+                    t, nrm, _solid = brush_trace(l, pos, end)
+                    if t == 0:
+                        valid = False
+                        break
+                    if t != 1:
+                        delta = [f32(end[k] - pos[k]) for k in range(3)]
+                        if dot(delta, nrm) > 0:
+                            valid = False
+                            break
+                if valid:
+                    break
+            if not valid:
+                pos = [f32(f32(mn[k] + mx[k]) * f32(0.5)) for k in range(3)]
+            out.append(pos)
+    return counts, np.array(out, np.float32).reshape(-1, 3)
+
+
 def bits_to_bool(bits: np.ndarray, n: int) -> np.ndarray:
     """Unpack LSB-first u64 words into n booleans."""
     b = np.ascontiguousarray(bits, dtype="<u8").view(np.uint8)

@@ -28,6 +28,17 @@ the reference's tools/detmath_goldens.py with mpmath at 3000 bits):
                             use: single-precision Acos, Sin and Cos, double
                             Sin, Cos and Pow, "kind function a b expected"
                             as hex patterns of the kind's width.
+It also copies the reference's leaf-ambient fixture map
+src/SourceSharp.Tests/MapTools/Rad/Ambient/Fixtures/p4g_detail.bsp
+(gen_ambient_fixture.py --detail there: one sealed room, a func_detail
+pillar, a sky section, a point and a spot light, no displacements; run
+through stock vbsp, vvis and vrad -both, so it holds stock's own leaf
+ambient lumps), unchanged, and extracts as text the reference's golden
+vectors of stock's random stream (StockRandomStreamVectors.cs there, made
+by gen_stock_random_vectors.py from the stock stream): ran1-vectors.txt,
+one "name low high" header line per set and then its 512 float results as
+32-bit hex patterns.
+
 Run from anywhere, naming the reference's root (or set VRAD_REFERENCE_ROOT):
 
     python tests/golden/make_golden.py <reference-root>
@@ -43,7 +54,16 @@ import sys
 SRC_REL = "src/SourceSharp.Tests/MapTools/Tracing/Fixtures"
 DETMATH_REL = "src/SourceSharp.Tests/MapFormats/Numerics/DetMathGoldens.cs"
 DETMATH_ROWS = {("F1", "Asin"), ("F2", "Pow")}
-HOST_ROWS = {("F1", "Acos"), ("F1", "Sin"), ("F1", "Cos"), ("D1", "Sin"), ("D1", "Cos"), ("D2", "Pow")}
+HOST_ROWS = {("F1", "Acos"), ("F1", "Sin"), ("F1", "Cos"), ("F1", "Tan"), ("D1", "Sin"), ("D1", "Cos"),
+             ("D2", "Pow")}
+AMBIENT_REL = "src/SourceSharp.Tests/MapTools/Rad/Ambient"
+AMBIENT_NAMES = ["p4g_detail.bsp"]
+# StockRandomStreamVectors' sets: (seed, low, high); seed None is the stream
+# as constructed (SetSeed(0) in its constructor).
+RAN1_SETS = {"DefaultUnit": (None, 0.0, 1.0), "DefaultRanged1024": (None, 0.0, 1024.0),
+             "Seed0": (0, 0.0, 1.0), "Seed1": (1, 0.0, 1.0), "Seed7": (7, 0.0, 1.0),
+             "Seed12345": (12345, 0.0, 1.0), "SeedMinus3": (-3, 0.0, 1.0),
+             "Seed2147483647": (2147483647, 0.0, 1.0)}
 NAMES = [f"{scene}.{part}.bin" for scene in ("kd-scene", "kd-boxes")
          for part in ("tris", "rays", "tree", "answers")] + ["rays-lockdown-leafambient.bin",
                                                              "stock-lockdown-leafambient.bin"]
@@ -62,6 +82,19 @@ def main() -> None:
         shutil.copyfile(src / name, dst / name)
         digest = hashlib.sha256((dst / name).read_bytes()).hexdigest()
         lines.append(f"{digest}  {name}")
+    for name in AMBIENT_NAMES:
+        shutil.copyfile(root / AMBIENT_REL / "Fixtures" / name, dst / name)
+        lines.append(f"{hashlib.sha256((dst / name).read_bytes()).hexdigest()}  {name}")
+    text = (root / AMBIENT_REL / "StockRandomStreamVectors.cs").read_text()
+    body = []
+    for set_name, (seed, lo, hi) in RAN1_SETS.items():
+        m = re.search(rf"ReadOnlySpan<uint> {set_name} =>\s*\[(.*?)\]", text, re.S)
+        vals = re.findall(r"0x([0-9A-Fa-f]{8})", m.group(1))
+        assert len(vals) == 512, (set_name, len(vals))
+        body.append(f"{set_name} {'default' if seed is None else seed} {lo!r} {hi!r}")
+        body += [" ".join(v.lower() for v in vals[k:k + 8]) for k in range(0, 512, 8)]
+    (dst / "ran1-vectors.txt").write_text("\n".join(body) + "\n")
+    lines.append(f"{hashlib.sha256((dst / 'ran1-vectors.txt').read_bytes()).hexdigest()}  ran1-vectors.txt")
     # dm_lockdown's geometry lumps (the BSP surface tracer's inputs), each
     # copied unchanged: "VLMP", lump count, then per lump its id, version,
     # length and bytes.

@@ -1,6 +1,6 @@
 """The host-side correctly rounded functions (hl2sdk_tools_sharp_b200/detmath.py)
 against the reference's DetMath golden table (DetMathGoldens.cs, computed
-with mpmath at 3000 bits): every single-precision Acos, Sin and Cos row and
+with mpmath at 3000 bits): every single-precision Acos, Sin, Cos and Tan row and
 every double Sin, Cos and Pow row, bit for bit."""
 import pathlib
 import struct
@@ -34,7 +34,7 @@ def _dbits(x):
     return struct.unpack("<Q", struct.pack("<d", x))[0]
 
 
-FUNCS = {("F1", "Acos"): DM.acos_f, ("F1", "Sin"): DM.sin_f, ("F1", "Cos"): DM.cos_f,
+FUNCS = {("F1", "Acos"): DM.acos_f, ("F1", "Sin"): DM.sin_f, ("F1", "Cos"): DM.cos_f, ("F1", "Tan"): DM.tan_f,
          ("D1", "Sin"): DM.sin_d, ("D1", "Cos"): DM.cos_d, ("D2", "Pow"): DM.pow_d}
 
 

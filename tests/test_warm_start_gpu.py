@@ -34,9 +34,13 @@ def test_trained_warm_start_beats_plain_and_untrained():
         warm_bounces = st.bounce_stats().bounces
         st.set_bounce_model(None)
         again, _, _ = st.light_pass()
+        held_out = LN.evaluate(trained, [LN.heldout_config(0)])
         untrained.close()
         trained.close()
     assert err_trained < 0.5 * err_untrained and err_trained < 0.25, (err_trained, err_untrained)
     assert warm_bounces <= plain_bounces, (warm_bounces, plain_bounces)
     assert LN.within_one_lsb(warm, plain) >= 0.999
     assert np.array_equal(again, plain)                # detaching restores the plain bounce exactly
+    (ev,) = held_out
+    assert 0.0 < ev["rho"] < 1.0 and 0.0 < ev["eps"] < 1.0, ev
+    assert ev["warm_bounces"] <= ev["plain_bounces"] and ev["within_1_lsb"] >= 0.999, ev
