@@ -422,11 +422,7 @@ cudaError_t allow_smem(int device) {
 }  // namespace
 
 cudaError_t mlp_forward(const vrad_mlp &m, const uint16_t *x, int64_t n, float *y, cudaStream_t s) {
-    if (n == 0) return cudaSuccess;
-    cudaError_t e = allow_smem(m.device);
-    if (e != cudaSuccess) return e;
-    k_mlp_forward<<<blocks_for(n), kMlpThreads, sizeof(FwdSmem), s>>>(m, x, n, y, nullptr, nullptr);
-    return cudaGetLastError();
+    return mlp_forward_tc(m, x, n, y, s);
 }
 
 }  // namespace vrad
@@ -435,7 +431,8 @@ namespace {
 
 void release_mlp(vrad_mlp *m) {
     for (void *p : {(void *)m->master, (void *)m->adam_m, (void *)m->adam_v, (void *)m->grad, (void *)m->w1t,
-                    (void *)m->w2t, (void *)m->w3t, (void *)m->w2, (void *)m->w3, (void *)m->loss, (void *)m->h1,
+                    (void *)m->w2t, (void *)m->w3t, (void *)m->w2, (void *)m->w3, (void *)m->loss, (void *)m->flags,
+                    (void *)m->h1,
                     (void *)m->h2, (void *)m->dz1, (void *)m->dz2, (void *)m->dy, (void *)m->y})
         cudaFree(p);
     delete m;
@@ -460,6 +457,8 @@ extern "C" int32_t vrad_mlp_create(vrad_ctx *ctx, uint64_t seed, vrad_mlp **out)
     for (uint16_t **p : {&m->w1t, &m->w2t, &m->w3t, &m->w2, &m->w3})
         if (e == cudaSuccess) e = cudaMalloc(p, sizeof(uint16_t) * kW2);
     if (e == cudaSuccess) e = cudaMalloc(&m->loss, sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&m->flags, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(m->flags, 0, sizeof(uint32_t));
     if (e == cudaSuccess) e = allow_smem(ctx->device);
     // He initialisation from a seeded generator; biases zero.
     std::vector<float> w((size_t)kMlpParams, 0.0f);
@@ -549,5 +548,16 @@ extern "C" int32_t vrad_mlp_loss(vrad_mlp *m, float *loss) {
     cudaError_t e = cudaSetDevice(m->device);
     if (e == cudaSuccess) e = cudaMemcpy(loss, m->loss, sizeof(float), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return vrad_cuda_fail(nullptr, e, "network loss");
+    return VRAD_OK;
+}
+
+extern "C" int32_t vrad_mlp_status(vrad_mlp *m) {
+    if (!m) return vrad_fail(nullptr, VRAD_ERR_ARG, "null network");
+    uint32_t f = 0;
+    cudaError_t e = cudaSetDevice(m->device);
+    if (e == cudaSuccess) e = cudaMemcpy(&f, m->flags, sizeof f, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && f) e = cudaMemset(m->flags, 0, sizeof f);
+    if (e != cudaSuccess) return vrad_cuda_fail(nullptr, e, "network status");
+    if (f) return vrad_fail(nullptr, VRAD_ERR_TIMEOUT, "a network forward's tensor-core wait ran out");
     return VRAD_OK;
 }

@@ -1,5 +1,6 @@
 // mlp.cuh -- the learned warm start's network: 32 -> 128 -> 128 -> 3 with
-// ReLU, BF16 weights and activations, FP32 accumulation (mlp.cu).
+// ReLU, BF16 weights and activations, FP32 accumulation (mlp.cu: training
+// on mma.sync; mlp_tc.cu: the forward on tcgen05 with TMEM accumulators).
 //
 // Device layout of one network (struct vrad_mlp):
 //   master  float  FP32 parameters, the order of kMlpParams (w1 [32][128],
@@ -39,6 +40,7 @@ struct vrad_mlp {
     float *master = nullptr, *adam_m = nullptr, *adam_v = nullptr, *grad = nullptr;
     uint16_t *w1t = nullptr, *w2t = nullptr, *w3t = nullptr, *w2 = nullptr, *w3 = nullptr;
     float *loss = nullptr;        // device scalar of the last step
+    uint32_t *flags = nullptr;    // device word: bit 0, a forward's MMA wait ran out (sticky)
     // Training scratch, grown on demand: activations and their gradients.
     uint16_t *h1 = nullptr, *h2 = nullptr, *dz1 = nullptr, *dz2 = nullptr, *dy = nullptr;
     float *y = nullptr;
@@ -48,7 +50,9 @@ struct vrad_mlp {
 
 namespace vrad {
 
-// y[n][3] = the network on x[n][32] (bf16 bits), on `stream`.
+// y[n][3] = the network on x[n][32] (bf16 bits), on `stream`: the
+// tcgen05 forward (mlp_tc.cu).
 cudaError_t mlp_forward(const vrad_mlp &m, const uint16_t *x, int64_t n, float *y, cudaStream_t stream);
+cudaError_t mlp_forward_tc(const vrad_mlp &m, const uint16_t *x, int64_t n, float *y, cudaStream_t stream);
 
 }  // namespace vrad

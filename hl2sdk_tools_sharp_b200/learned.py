@@ -2,7 +2,8 @@
 
 A 32 -> 128 -> 128 -> 3 network (ReLU, BF16 weights and activations, FP32
 accumulation) trained and run on the device by the library's own tensor-core
-kernels.  Inputs are (n, 32) torch.bfloat16 CUDA tensors, targets and
+kernels: the forward on tcgen05 with TMEM accumulators, the training on
+mma.sync.  Inputs are (n, 32) torch.bfloat16 CUDA tensors, targets and
 outputs (n, 3) float32 CUDA tensors; torch is only the allocator.
 """
 from __future__ import annotations
@@ -36,8 +37,9 @@ def _lib():
         lib.vrad_mlp_gradient_device.argtypes = [P, P, P, i64, P, P, P]
         lib.vrad_mlp_train_step_device.argtypes = [P, P, P, i64, f32, P]
         lib.vrad_mlp_loss.argtypes = [P, P]
+        lib.vrad_mlp_status.argtypes = [P]
         for n in ("vrad_mlp_create", "vrad_mlp_destroy", "vrad_mlp_params", "vrad_mlp_forward_device",
-                  "vrad_mlp_gradient_device", "vrad_mlp_train_step_device", "vrad_mlp_loss"):
+                  "vrad_mlp_gradient_device", "vrad_mlp_train_step_device", "vrad_mlp_loss", "vrad_mlp_status"):
             getattr(lib, n).restype = i32
         lib._mlp_bound = True
     return lib
@@ -107,6 +109,11 @@ class Network:
     def train_step(self, x, target, lr: float, stream=None) -> None:
         T._check(_lib().vrad_mlp_train_step_device(self._h, x.data_ptr(), target.data_ptr(), x.shape[0], lr,
                                                    ctypes.c_void_p(self._stream(stream))), None)
+
+    def status(self) -> None:
+        """Raises when a forward since the last call gave up on a bounded
+        tensor-core wait (vrad_mlp_status)."""
+        T._check(_lib().vrad_mlp_status(self._h), None)
 
     def loss(self) -> float:
         v = np.zeros(1, np.float32)

@@ -570,6 +570,12 @@ int32_t vrad_mlp_train_step_device(vrad_mlp *m, const uint16_t *x, const float *
                                    void *stream);
 int32_t vrad_mlp_loss(vrad_mlp *m, float *loss);
 
+/* The forward runs on the fifth-generation tensor cores (tcgen05.mma, TMEM
+ * accumulators); each of its MMA waits is bounded, and a wait that runs out
+ * is recorded on the device.  This call reads and clears that record:
+ * VRAD_ERR_TIMEOUT when a forward since the last call gave up. */
+int32_t vrad_mlp_status(vrad_mlp *m);
+
 /* Attaches a network to the bounce (NULL detaches it: the plain bounce).
  * With one attached, a light pass bounces once from the direct light (B1),
  * asks the network for each patch's converged bounced light G from its

@@ -70,3 +70,34 @@ def test_training_fits_a_function(net):
     torch.cuda.synchronize()
     last = n.loss()
     assert last < first / 10, (first, last)
+
+
+def test_tcgen05_forward_at_scale_and_alignment(net):
+    """The tcgen05 forward over a million rows (7,813 tiles on 2 CTAs per SM,
+    the last tile partial) against the oracle on a spread of rows, and the
+    same rows from a 4-byte-aligned (not 16-byte-aligned) input."""
+    from oracle import mlp_oracle as MO
+    n, torch = net
+    rows = 1_000_003
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11)
+    xt = torch.randn((rows, LN.INPUTS), device="cuda", generator=g).to(torch.bfloat16).contiguous()
+    y = n.forward(xt)
+    torch.cuda.synchronize()
+    n.status()
+    pick = np.unique(np.concatenate([np.arange(0, 300), np.linspace(0, rows - 1, 3000).astype(np.int64),
+                                     np.arange(rows - 300, rows)]))
+    idx = torch.from_numpy(pick).cuda()
+    bits = xt[idx].cpu().view(torch.int16).numpy().view(np.uint16)
+    want, _, _ = MO.forward(n.params(), bits)
+    got = y[idx].cpu().numpy()
+    assert np.isfinite(got).all()
+    assert _rel(got, want) < 2e-3
+    # A view two elements in: rows start 4 bytes past a 16-byte boundary.
+    buf = torch.zeros((4096 * LN.INPUTS + 2,), dtype=torch.bfloat16, device="cuda")
+    view = buf[2:].view(4096, LN.INPUTS)
+    view.copy_(xt[:4096])
+    assert view.data_ptr() % 16 == 4
+    y2 = n.forward(view)
+    torch.cuda.synchronize()
+    assert torch.equal(y2, y[:4096])
