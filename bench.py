@@ -411,7 +411,7 @@ def main_seam(args):
                    "guess_abs_error_log1p": float((y - ht).abs().mean().item()),
                    "training": {"maps": 8, "rows": int(len(lx)), "steps": 3000, "batch": 32768,
                                 "collect_s": collect_s, "train_ms": train_ms, "final_loss": loss},
-                   "roofline": {"bound": "tensor", "kernel": "k_mlp_forward (mma.sync bf16, fp32 accumulate)",
+                   "roofline": {"bound": "tensor", "kernel": "k_mlp_forward_tc (tcgen05.mma kind::f16, bf16 in, fp32 in TMEM)",
                                 "achieved": flops / (fwd_ms / 1000.0) / 1e12, "peak": tpeak, "unit": "TFLOP/s",
                                 "frac": flops / (fwd_ms / 1000.0) / 1e12 / tpeak, "rows": int(len(hx)),
                                 "ms": fwd_ms, "flops_per_row": flops / len(hx)}}
@@ -547,9 +547,17 @@ WORKLOAD = ("8x8 room grid lighting stage, LDR and HDR ranges: per range the dir
             "0.1) and the final pass into LIGHTING / LIGHTING_HDR; one transfer build for both ranges")
 
 
+WORKLOAD_LARGE = ("16x16 room grid lighting stage (the large configuration without displacements or ambient "
+                  "occlusion), LDR and HDR ranges: per range the direct gather (256 point/spot lights, a sun of 256 "
+                  "jittered rays, 162-dir sky, 4 supersampling passes), the bounce (patch light, radiosity to "
+                  "threshold 0.1) and the final pass into LIGHTING / LIGHTING_HDR; one transfer build for both ranges")
+
+
 def stage_config(args):
     """The workload's defining keys, the same in both arms."""
-    return {"workload": WORKLOAD, "side": args.side, "seed": CONFIG_SEED, "ranges": "LDR+HDR",
+    work = WORKLOAD_LARGE if args.side == 16 else (WORKLOAD if args.side == 8 else f"{args.side}x{args.side} "
+                                                   "room grid lighting stage, LDR and HDR ranges")
+    return {"workload": work, "side": args.side, "seed": CONFIG_SEED, "ranges": "LDR+HDR",
             "bounce_threshold": BOUNCE_THRESHOLD, "max_bounces": MAX_BOUNCES,
             "l2": "no L2 flush: the 0.3 GB sample set and 5 GB of candidate pairs exceed L2",
             "parallelism": f"replicas{args.gpus} (one map per rank, seed {CONFIG_SEED} + rank)"}
@@ -789,6 +797,23 @@ def ambient_run(args, samples: int = 131072) -> dict:
     return out
 
 
+def recheck_run(world, stride: int = 7) -> dict:
+    """The FP64 recheck (vrad_trace_visibility_recheck) over the light rays
+    of every `stride`-th luxel of the map (point, spot and sun segments;
+    the sky pass-through mode is outside the recheck): how many rays the
+    FP32 values flag, their FP64 classes, and the FP32/FP64 disagreements."""
+    from hl2sdk_tools_sharp_b200 import tracer as T, workload as wl
+    s = wl.luxel_samples(world, stride=stride)
+    rays = np.ascontiguousarray(wl.direct_rays(world, s, ambient=False).light)
+    with T.CudaRayTracer(T.make_triangles(world.tri_verts, world.tri_ids)) as tr:
+        t = time.perf_counter()
+        vis, _, st = tr.visibility_recheck(rays, T.RayTraceOptions.stock_exact())
+        wall = time.perf_counter() - t
+    st.update({"sample": f"light rays of every {stride}th luxel", "blocked": int(vis.sum()), "call_s": wall,
+               "flag_margin": 1e-5, "fp64_margin": 1e-6})
+    return st
+
+
 def main_stage(args):
     import torch
     from hl2sdk_tools_sharp_b200 import lighting as L, tracer as T
@@ -912,13 +937,9 @@ def main_stage(args):
 
         def e2e_step():
             t0 = time.perf_counter()
-            faces, verts = L.faces_of(w)
-            samples, first = L.build_samples(faces, verts, out=sample_buf)
-            lights, off, flat = L.build_lights(w)
-            lights_hdr, _, _ = L.build_lights(w, hdr=True)
-            i2 = L.LightingInputs(faces, verts, samples, first, lights, off, flat,
-                                  wl.ambient_directions().astype(np.float32), np.zeros((0, 3), np.float32),
-                                  lights_hdr=lights_hdr)
+            i2 = L.prepare(w, hdr=True, sample_out=sample_buf)
+            faces, verts, samples, lights, lights_hdr = i2.faces, i2.verts, i2.samples, i2.lights, i2.lights_hdr
+            off, flat = i2.cluster_offsets, i2.cluster_lights
             t1 = time.perf_counter()
             stage.tracer.upload_scene(tris)
             t2 = time.perf_counter()
@@ -932,7 +953,8 @@ def main_stage(args):
                             ("upload_bounce", t3, t4), ("light_pass", t4, t5)):
                 parts[k].append(b - a)
             h2d.append(tris.nbytes + faces.nbytes + verts.nbytes + samples.nbytes + lights.nbytes + lights_hdr.nbytes
-                       + off.nbytes + flat.nbytes + refl.nbytes + pvs_off.nbytes + pvs_list.nbytes)
+                       + off.nbytes + flat.nbytes + i2.sun_jitter.nbytes + refl.nbytes + pvs_off.nbytes
+                       + pvs_list.nbytes)
         e2e_step()
         barrier(world_size)
         t = time.perf_counter()
@@ -1023,7 +1045,7 @@ def main_stage(args):
                    "guess_abs_error_log1p": float((y - ht).abs().mean().item()),
                    "training": {"maps": train_maps, "rows": int(len(lx)), "steps": 3000, "batch": 32768,
                                 "collect_s": collect_s, "train_ms": train_ms, "final_loss": loss},
-                   "roofline": {"bound": "tensor", "kernel": "k_mlp_forward (mma.sync bf16, fp32 accumulate)",
+                   "roofline": {"bound": "tensor", "kernel": "k_mlp_forward_tc (tcgen05.mma kind::f16, bf16 in, fp32 in TMEM)",
                                 "achieved": flops / (fwd_ms / 1000.0) / 1e12, "peak": tpeak, "unit": "TFLOP/s",
                                 "frac": flops / (fwd_ms / 1000.0) / 1e12 / tpeak, "rows": int(len(hx)),
                                 "ms": fwd_ms, "flops_per_row": flops / len(hx)}}
@@ -1032,6 +1054,7 @@ def main_stage(args):
     if not args.no_batch:
         batched = batched_run(args, local, rank, world_size)
     leaf_ambient = ambient_run(args) if rank == 0 and not args.no_ambient else None
+    recheck = recheck_run(w) if rank == 0 and not args.no_ambient else None
     # The dominant phases on the launching stream: both ranges' direct
     # gather (the two-range first round and each range's supersampling
     # passes), timed by a host-buffer pass, and the transfer build (its
@@ -1108,6 +1131,7 @@ def main_stage(args):
             "learned": learned,
             "batched": batched,
             "leaf_ambient": leaf_ambient,
+            "fp64_recheck": recheck,
         }
         print(json.dumps(line), flush=True)
     stage.close()

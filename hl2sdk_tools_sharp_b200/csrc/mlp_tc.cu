@@ -11,7 +11,8 @@
 //   bytes, core (row group g, K chunk k) at (k x row groups + g) x 128 B;
 // and 128 TMEM columns (128 lanes x 128 FP32) that each layer's
 // accumulator reuses.  Per tile:
-//   x -> shared memory (each thread 32 bytes of a row)
+//   x -> shared memory (each thread 32 bytes of a row, loaded from global
+//     memory while the previous tile ran)
 //   layer 1: 2 x tcgen05.mma M128 N128 K16 -> TMEM, commit -> mbarrier
 //   epilogue: tcgen05.ld (warp w reads lanes 32 (w % 4) .., columns
 //     64 (w / 4) ..), + bias, ReLU, BF16 -> h in shared memory
@@ -148,25 +149,24 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
 }
 
 // Bias, ReLU and BF16 of this thread's 64 accumulator columns of row r into h.
+// Both 32-column loads are in flight before the one wait.
 __device__ __forceinline__ void hidden_epilogue(TcSmem &s, uint32_t taddr, const float *bias, int r, int c0) {
+    float v[64];
+    tmem_ld32(taddr + (uint32_t)c0, v);
+    tmem_ld32(taddr + (uint32_t)(c0 + 32), v + 32);
+    tmem_wait_ld();
 #pragma unroll
-    for (int half = 0; half < 2; half++) {
-        float v[32];
-        tmem_ld32(taddr + (uint32_t)(c0 + 32 * half), v);
-        tmem_wait_ld();
+    for (int q = 0; q < 8; q++) {
+        const int c = c0 + 8 * q;
+        uint4 w;
+        uint32_t *pw = reinterpret_cast<uint32_t *>(&w);
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int c = c0 + 32 * half + 8 * q;
-            uint4 w;
-            uint32_t *pw = reinterpret_cast<uint32_t *>(&w);
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-                const float a = fmaxf(__fadd_rn(v[8 * q + 2 * e], bias[c + 2 * e]), 0.0f);
-                const float b = fmaxf(__fadd_rn(v[8 * q + 2 * e + 1], bias[c + 2 * e + 1]), 0.0f);
-                pw[e] = pack2(a, b);
-            }
-            *reinterpret_cast<uint4 *>(s.h + canon(r, c, kTcRows / 8)) = w;
+        for (int e = 0; e < 4; e++) {
+            const float a = fmaxf(__fadd_rn(v[8 * q + 2 * e], bias[c + 2 * e]), 0.0f);
+            const float b = fmaxf(__fadd_rn(v[8 * q + 2 * e + 1], bias[c + 2 * e + 1]), 0.0f);
+            pw[e] = pack2(a, b);
         }
+        *reinterpret_cast<uint4 *>(s.h + canon(r, c, kTcRows / 8)) = w;
     }
 }
 
@@ -237,27 +237,32 @@ __global__ void __launch_bounds__(kTcThreads) k_mlp_forward_tc(vrad_mlp m, const
         return s.abort == 0;
     };
 
-    for (int64_t tile = blockIdx.x; ok && tile * kTcRows < n; tile += gridDim.x) {
-        const int64_t r0 = tile * kTcRows;
-        // x: thread t fills half of row t / 2 (two 16-byte chunks).
-        {
-            const int r = tid >> 1, kc0 = 2 * (tid & 1);
-            const int64_t gr = r0 + r;
+    // x: thread t holds half of row t / 2 (two 16-byte chunks) of a tile;
+    // the next tile's are loaded while this tile's layers run.
+    const int xr_row = tid >> 1, xr_kc = 2 * (tid & 1);
+    uint4 xr[2];
+    auto load_x = [&](int64_t tile) {
+        const int64_t gr = tile * kTcRows + xr_row;
 #pragma unroll
-            for (int q = 0; q < 2; q++) {
-                uint4 w = make_uint4(0, 0, 0, 0);
-                if (gr < n) {
-                    const uint16_t *src = x + gr * kMlpIn + 8 * (kc0 + q);
-                    if (x16) {
-                        w = *reinterpret_cast<const uint4 *>(src);
-                    } else {
-                        const uint32_t *s32 = reinterpret_cast<const uint32_t *>(src);
-                        w = make_uint4(s32[0], s32[1], s32[2], s32[3]);
-                    }
+        for (int q = 0; q < 2; q++) {
+            xr[q] = make_uint4(0, 0, 0, 0);
+            if (gr < n) {
+                const uint16_t *src = x + gr * kMlpIn + 8 * (xr_kc + q);
+                if (x16) {
+                    xr[q] = *reinterpret_cast<const uint4 *>(src);
+                } else {
+                    const uint32_t *s32 = reinterpret_cast<const uint32_t *>(src);
+                    xr[q] = make_uint4(s32[0], s32[1], s32[2], s32[3]);
                 }
-                *reinterpret_cast<uint4 *>(s.x + canon(r, 8 * (kc0 + q), kTcRows / 8)) = w;
             }
         }
+    };
+    load_x(blockIdx.x);
+
+    for (int64_t tile = blockIdx.x; ok && tile * kTcRows < n; tile += gridDim.x) {
+        const int64_t r0 = tile * kTcRows;
+#pragma unroll
+        for (int q = 0; q < 2; q++) *reinterpret_cast<uint4 *>(s.x + canon(xr_row, 8 * (xr_kc + q), kTcRows / 8)) = xr[q];
         fence_async_smem();
         __syncthreads();
         if (tid == 0) {
@@ -268,6 +273,7 @@ __global__ void __launch_bounds__(kTcThreads) k_mlp_forward_tc(vrad_mlp m, const
                     idesc(kMlpHidden), k > 0);
             commit(bar);
         }
+        load_x(tile + gridDim.x);
         if (!(ok = wait_all())) break;
         hidden_epilogue(s, taddr, s.b1, row, c0);
         fence_before();

@@ -33,11 +33,22 @@ __device__ inline float sel3(int axis, float x, float y, float z) {
     return axis == 0 ? x : (axis == 1 ? y : z);
 }
 
+// The FP64 recheck's flag (vrad_trace_visibility_recheck): set when a
+// triangle's FP32 predicate values lie within `m` of a decision boundary --
+// an edge value near 0, their sum near 1, or t near either end of the
+// segment [tlo, thi] -- and no farther than `m` outside on the others.
+struct NearCheck {
+    float m, tlo, thi;
+    bool near;
+};
+
 // The predicate.  Returns true with the exact t when the triangle accepts
 // the ray (|d.n| > eps, eps < t < 1e23, both edge values >= eps, their sum
-// <= 1).
+// <= 1).  With FLAG the near-boundary test runs first; the decision itself
+// is the same arithmetic either way.
+template <bool FLAG = false>
 __device__ __forceinline__ bool kd_hit(const DeviceBvh &s, int k, const RayState &r, float &t_out,
-                                       uint32_t &meta_out, int32_t &orig_out) {
+                                       uint32_t &meta_out, int32_t &orig_out, NearCheck *nc = nullptr) {
     const float4 A = __ldg(&s.tri0[k]);
     float ddotn = __fmul_rn(r.dx, A.x);
     ddotn = __fadd_rn(__fmul_rn(r.dy, A.y), ddotn);
@@ -49,6 +60,23 @@ __device__ __forceinline__ bool kd_hit(const DeviceBvh &s, int k, const RayState
     // t > eps needs num and ddotn of one sign; this rejects without the
     // divide exactly where the divide's sign would (|ddotn| > eps > 0).
     if (!(ddotn > kKdEps || ddotn < -kKdEps)) return false;
+    if constexpr (FLAG) {
+        const float4 B = __ldg(&s.tri1[k]);
+        const float4 C = __ldg(&s.tri2[k]);
+        const int drop = __float_as_uint(C.w) & 3;
+        const int c0 = drop == 2 ? 0 : drop + 1;
+        const int c1 = drop == 0 ? 2 : drop - 1;
+        const float t = __fdiv_rn(num, ddotn);
+        const float h1 = __fadd_rn(sel3(c0, r.ox, r.oy, r.oz), __fmul_rn(t, sel3(c0, r.dx, r.dy, r.dz)));
+        const float h2 = __fadd_rn(sel3(c1, r.ox, r.oy, r.oz), __fmul_rn(t, sel3(c1, r.dx, r.dy, r.dz)));
+        const float b0 = __fadd_rn(__fadd_rn(__fmul_rn(B.x, h1), __fmul_rn(B.y, h2)), B.z);
+        const float b1 = __fadd_rn(__fadd_rn(__fmul_rn(B.w, h1), __fmul_rn(C.x, h2)), C.y);
+        const float m = nc->m, tm = m * fmaxf(1.0f, fabsf(nc->thi));
+        const float sum = __fadd_rn(b0, b1);
+        const bool out = b0 < -m || b1 < -m || sum > 1.0f + m || t < nc->tlo - tm || t > nc->thi + tm;
+        const bool in = b0 > m && b1 > m && sum < 1.0f - m && t > nc->tlo + tm && t < nc->thi - tm;
+        if (!out && !in) nc->near = true;
+    }
     if ((__float_as_uint(num) ^ __float_as_uint(ddotn)) & 0x80000000u) return false;
     const float t = __fdiv_rn(num, ddotn);
     if (!(t > kKdEps) || !(t < kKdHuge)) return false;
@@ -103,11 +131,11 @@ __device__ __forceinline__ void slab2(const float4 &a, const float4 &b, const fl
 // Of two children the segment meets, the nearer is entered first, or with
 // FAR the farther (an any-hit walk may find its blocker sooner from the far
 // end; which order pays is measured per caller).
-template <bool ANY, int STRIDE = kBlock, bool FAR = false>
+template <bool ANY, int STRIDE = kBlock, bool FAR = false, bool FLAG = false>
 __device__ __forceinline__ bool walk(const DeviceBvh &s, const int32_t *__restrict__ tri_id,
                                      const RayState &r, float tmin, int32_t skip_id, int *stack,
                                      uint32_t *overflow, float &thi, int32_t &best_orig,
-                                     uint32_t &best_meta) {
+                                     uint32_t &best_meta, NearCheck *nc = nullptr) {
     bool hit = false;
     int sp = 0;
     int ref = 0;
@@ -117,7 +145,13 @@ __device__ __forceinline__ bool walk(const DeviceBvh &s, const int32_t *__restri
             const float4 a = __ldg(nd), b = __ldg(nd + 1), c = __ldg(nd + 2), d = __ldg(nd + 3);
             bool h0, h1;
             float n0, n1;
-            slab2(a, b, c, r, tmin, thi, h0, h1, n0, n1);
+            if constexpr (FLAG) {
+                // The recheck also wants the triangles just past either end.
+                const float tm = nc->m * fmaxf(1.0f, fabsf(thi));
+                slab2(a, b, c, r, tmin - tm, thi + tm, h0, h1, n0, n1);
+            } else {
+                slab2(a, b, c, r, tmin, thi, h0, h1, n0, n1);
+            }
             const int r0 = __float_as_int(d.x), r1 = __float_as_int(d.y);
             if (h0 && h1) {
                 int near_ref = r0, far_ref = r1;
@@ -150,7 +184,7 @@ __device__ __forceinline__ bool walk(const DeviceBvh &s, const int32_t *__restri
                 float t;
                 uint32_t meta;
                 int32_t orig;
-                if (!kd_hit(s, k, r, t, meta, orig)) continue;
+                if (!kd_hit<FLAG>(s, k, r, t, meta, orig, nc)) continue;
                 if (!(t >= tmin)) continue;
                 if (!(t < thi || (t == thi && orig < best_orig))) continue;
                 if (skip_id != -1 && __ldg(&tri_id[orig]) == skip_id) continue;
@@ -203,6 +237,24 @@ __device__ __forceinline__ void trace_ray(const DeviceScene &s, const RayState &
     }
 }
 
+
+// kModeAny with the FP64 recheck's flag: the same walks and answer as
+// trace_ray<kModeAny>, every box widened by the margin at both ends.
+template <int STRIDE = kBlock>
+__device__ __forceinline__ void trace_ray_flagged(const DeviceScene &s, const RayState &r, float tmin, float reach,
+                                                  int32_t skip_id, int *stack, uint32_t *overflow, bool &hit,
+                                                  NearCheck &nc) {
+    float best_t = reach;
+    int32_t best_orig = -1;
+    uint32_t best_meta = 0;
+    hit = false;
+    if (s.opaque.ntris)
+        hit = walk<true, STRIDE, false, true>(s.opaque, s.tri_id, r, tmin, skip_id, stack, overflow, best_t,
+                                              best_orig, best_meta, &nc);
+    if (!hit && s.sky.ntris)
+        hit = walk<true, STRIDE, false, true>(s.sky, s.tri_id, r, tmin, skip_id, stack, overflow, best_t, best_orig,
+                                              best_meta, &nc);
+}
 
 __device__ __forceinline__ RayState make_ray(float ox, float oy, float oz, float dx, float dy, float dz) {
     RayState r;

@@ -349,10 +349,11 @@ class LightingInputs:
 RANGE_LDR, RANGE_HDR = 1, 2      # VRAD_RANGE_*
 
 
-def prepare(world: World, hdr: bool = False) -> LightingInputs:
-    """The lighting stage's inputs; with hdr, also the HDR range's light list."""
+def prepare(world: World, hdr: bool = False, sample_out: np.ndarray | None = None) -> LightingInputs:
+    """The lighting stage's inputs; with hdr, also the HDR range's light
+    list.  sample_out: a caller's buffer for the samples (build_samples)."""
     faces, verts = faces_of(world)
-    samples, first = build_samples(faces, verts)
+    samples, first = build_samples(faces, verts, out=sample_out)
     lights, off, flat = build_lights(world)
     inp = LightingInputs(faces, verts, samples, first, lights, off, flat,
                          ambient_directions().astype(np.float32), np.zeros((0, 3), np.float32))

@@ -107,6 +107,12 @@ class RayTraceOptions:
                         int(bool(self.sky_does_not_block)), int(bool(self.isolated_rays)))
 
 
+class RecheckStats(ctypes.Structure):
+    _fields_ = [("rays", ctypes.c_int64), ("flagged", ctypes.c_int64), ("fp64_hit", ctypes.c_int64),
+                ("fp64_miss", ctypes.c_int64), ("fp64_ambiguous", ctypes.c_int64),
+                ("disagreements", ctypes.c_int64)]
+
+
 _lib = None
 
 
@@ -131,6 +137,8 @@ def load_library() -> ctypes.CDLL:
         "vrad_trace_closest": ([P, P, i64, ctypes.POINTER(_Options), P], i32),
         "vrad_trace_visibility_device": ([P, P, i64, ctypes.POINTER(_Options), P, P], i32),
         "vrad_trace_closest_device": ([P, P, i64, ctypes.POINTER(_Options), P, P], i32),
+        "vrad_trace_visibility_recheck": ([P, P, i64, ctypes.POINTER(_Options), P, i32, ctypes.c_float,
+                                           ctypes.c_double, P, P, ctypes.POINTER(RecheckStats)], i32),
         "vrad_tracer_identity": ([P, ctypes.c_char_p, i32], i32),
         "vrad_last_error": ([P, ctypes.c_char_p, i32], i32),
     }
@@ -212,6 +220,7 @@ class CudaRayTracer:
             tris = make_triangles(tris)
         tris = np.ascontiguousarray(tris)
         self.triangle_count = len(tris)
+        self._tris = tris
         if prepared is not None:
             prepared = np.ascontiguousarray(prepared, KD_TRIANGLE_DTYPE)
             if len(prepared) != len(tris):
@@ -229,6 +238,7 @@ class CudaRayTracer:
             tris = make_triangles(tris)
         tris = np.ascontiguousarray(tris)
         self.triangle_count = len(tris)
+        self._tris = tris
         _check(self._lib.vrad_scene_upload(self._ctx, tris.ctypes.data, len(tris)), self._ctx)
 
     # -- lifetime ---------------------------------------------------------
@@ -321,6 +331,24 @@ class CudaRayTracer:
         bits = np.zeros((n + 63) // 64, np.uint64)
         self.trace_visibility(rays, bits, options)
         return np.unpackbits(bits.view(np.uint8), bitorder="little")[:n].astype(bool)
+
+    def visibility_recheck(self, rays, options: RayTraceOptions = RayTraceOptions(), flag_margin: float = 1e-5,
+                           fp64_margin: float = 1e-6):
+        """vrad_trace_visibility_recheck: (the FP32 visibility, as visibility
+        gives it; per ray the FP64 class of a flagged ray, 0 miss, 1 hit,
+        2 ambiguous, -1 not flagged; the counts as a dict)."""
+        rays = np.ascontiguousarray(rays)
+        n = rays.nbytes // 28
+        bits = np.zeros((n + 63) // 64 or 1, np.uint64)
+        cls = np.zeros(n or 1, np.int8)
+        st = RecheckStats()
+        o = options._c()
+        _check(self._lib.vrad_trace_visibility_recheck(self._ctx, rays.ctypes.data, n, ctypes.byref(o),
+                                                       self._tris.ctypes.data, len(self._tris), flag_margin,
+                                                       fp64_margin, bits.ctypes.data, cls.ctypes.data,
+                                                       ctypes.byref(st)), self._ctx)
+        vis = np.unpackbits(bits.view(np.uint8), bitorder="little")[:n].astype(bool)
+        return vis, cls[:n], {k: int(getattr(st, k)) for k, _ in RecheckStats._fields_}
 
     def closest(self, rays, options: RayTraceOptions = RayTraceOptions()) -> np.ndarray:
         rays = np.ascontiguousarray(rays)

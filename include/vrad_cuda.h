@@ -151,6 +151,33 @@ int32_t vrad_trace_closest_device(vrad_ctx *ctx, const vrad_ray *d_rays, int64_t
                                   const vrad_trace_options *opts, vrad_hit *d_hits,
                                   void *stream);
 
+/* ---- FP64 recheck ---------------------------------------------------------
+ *
+ * The check the reference's own GPU tracer is held to
+ * (Tests/MapTools/Tracing/VulkanRayTracerFacts.cs:1215-1300), on the device.
+ * The visibility bits are vrad_trace_visibility's (the reference's FP32
+ * answer, opts as there; the sky pass-through mode is VRAD_ERR_UNSUPPORTED).
+ * A ray is flagged when some triangle's FP32 edge values, their sum or t lie
+ * within flag_margin of a boundary (an edge, 1, either end of the segment);
+ * each flagged ray is re-tested in FP64 against every triangle of `tris` (the
+ * array given to vrad_scene_upload, for the original vertices):
+ * fp64_class[i] = 0 miss, 1 hit, 2 within fp64_margin of a boundary
+ * (ambiguous), -1 not flagged.  A flagged ray whose clear FP64 class differs
+ * from its FP32 bit is a disagreement.  Host buffers; blocks. */
+typedef struct vrad_recheck_stats {
+    int64_t rays;
+    int64_t flagged;
+    int64_t fp64_hit;
+    int64_t fp64_miss;
+    int64_t fp64_ambiguous;
+    int64_t disagreements;
+} vrad_recheck_stats;
+
+int32_t vrad_trace_visibility_recheck(vrad_ctx *ctx, const vrad_ray *rays, int64_t n,
+                                      const vrad_trace_options *opts, const vrad_triangle *tris, int32_t ntris,
+                                      float flag_margin, double fp64_margin, uint64_t *hit_bits,
+                                      int8_t *fp64_class, vrad_recheck_stats *stats);
+
 /* ---- Lighting stage ------------------------------------------------------
  *
  * The direct-lighting gather of vrad's lighting stage (the reference's

@@ -162,3 +162,31 @@ def test_device_equals_brute_force_on_adversarial_rays(oracle_mod):
                 assert np.array_equal(hits["surface"], np.where(bt >= 0, ids[np.maximum(bt, 0)], -1)), (name, kind)
                 hit = bt >= 0
                 assert np.array_equal(hits["fraction"][hit].view(np.uint32), bd[hit].view(np.uint32)), (name, kind)
+
+
+@pytest.mark.gpu
+def test_fp64_recheck_flags_every_questionable_ray(oracle_mod):
+    """vrad_trace_visibility_recheck on the adversarial sets: its visibility
+    bits are the FP32 trace's; every flagged ray's FP64 class is the oracle's
+    (the same FP64 arithmetic); and every ray it does not flag has an FP64
+    class that is clear and agrees with its FP32 bit, so the flag misses no
+    ray an FP64 test would question."""
+    O = oracle_mod
+    totals = {"flagged": 0, "fp64_ambiguous": 0, "disagreements": 0, "rays": 0}
+    for name, verts, ids, tree in _scenes():
+        tree = tree if tree is not None else O.kd_build(verts, ids)
+        with T.CudaRayTracer(T.make_triangles(verts, ids)) as tr:
+            for kind, rays in _adversarial(verts, tree, np.random.default_rng(7)).items():
+                rr = np.ascontiguousarray(rays).view(T.RAY_DTYPE).reshape(-1)
+                vis, cls, st = tr.visibility_recheck(rr, T.RayTraceOptions.stock_exact())
+                assert np.array_equal(vis, tr.visibility(rr, T.RayTraceOptions.stock_exact())), (name, kind)
+                want = O.fp64_classify(verts, rays, MARGIN)
+                flagged = cls >= 0
+                assert st["flagged"] == int(flagged.sum())
+                assert np.array_equal(cls[flagged], want[flagged]), (name, kind)
+                quiet = ~flagged
+                assert (want[quiet] != 2).all(), (name, kind, int((want[quiet] == 2).sum()))
+                assert np.array_equal(want[quiet] == 1, vis[quiet]), (name, kind)
+                for k in totals:
+                    totals[k] += st[k]
+    assert totals["flagged"] > 0 and totals["fp64_ambiguous"] > 0, totals
