@@ -60,7 +60,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--side", type=int, default=8, help=argparse.SUPPRESS)
-    ap.add_argument("--workload", default="stage", choices=["stage", "seam"])
+    ap.add_argument("--workload", default="stage", choices=["stage", "seam", "ambient", "forward"])
+    ap.add_argument("--ambient-samples", type=int, default=131072, help=argparse.SUPPRESS)
     ap.add_argument("--no-e2e", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-cpu", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-learned", action="store_true", help=argparse.SUPPRESS)
@@ -1141,8 +1142,50 @@ def main_stage(args):
     return 0
 
 
+def forward_run(rows: int = 999080, reps: int = 20) -> dict:
+    """The learned warm start's tcgen05 forward alone on `rows` seeded rows
+    (the 8x8 map's receiver count by default), timed on the device."""
+    import torch
+    from hl2sdk_tools_sharp_b200 import learned as LN, tracer as T
+    with T.CudaRayTracer(T.make_triangles(np.zeros((1, 9), np.float32), np.zeros(1, np.int32))) as tr:
+        net = LN.Network(tr, seed=7)
+        g = torch.Generator(device="cuda")
+        g.manual_seed(3)
+        x = torch.randn((rows, LN.INPUTS), device="cuda", generator=g).to(torch.bfloat16).contiguous()
+        y = torch.empty((rows, LN.OUTPUTS), device="cuda")
+        for _ in range(3):
+            net.forward(x, out=y)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            net.forward(x, out=y)
+        b.record()
+        torch.cuda.synchronize()
+        net.status()
+        ms = a.elapsed_time(b) / reps
+        net.close()
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    flops = 2.0 * (32 * 128 + 128 * 128 + 128 * 8) * rows
+    tf = flops / (ms / 1000.0) / 1e12
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    return {"kernel": "k_mlp_forward_tc", "rows": rows, "ms": ms, "achieved_tflops": tf, "peak_tflops": peak,
+            "frac": tf / peak, "peak_source": "measured" if "bf16_tflops" in peaks else "fallback"}
+
+
 def main():
     args = parse()
+    if args.workload == "forward":
+        print(json.dumps(forward_run()), flush=True)
+        return 0
+    if args.workload == "ambient":
+        # The leaf ambient section alone (also the small case its ncu
+        # capture runs): one JSON line of ambient_run's figures.
+        print(json.dumps(ambient_run(args, samples=args.ambient_samples)), flush=True)
+        return 0
     if args.workload == "seam":
         return run_reference(args) if args.impl == "reference" else main_seam(args)
     return run_reference_stage(args) if args.impl == "reference" else main_stage(args)

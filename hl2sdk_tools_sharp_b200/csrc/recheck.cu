@@ -110,7 +110,21 @@ __global__ void __launch_bounds__(32 * kClassWarps) k_fp64_class(const vrad_ray 
         const double scale = __dmul_rn(__dmul_rn(dn, e1n), e2n);
         if (scale == 0.0) continue;
         if (fabs(det) <= __dmul_rn(m, scale)) {
-            if (fabs(det) > 0.0) ambiguous = true;  // grazing
+            // Grazing: ambiguous when the segment runs within the margin of
+            // the triangle's plane (or crosses it).
+            const double nx = __dsub_rn(__dmul_rn(e1y, e2z), __dmul_rn(e1z, e2y));
+            const double ny = __dsub_rn(__dmul_rn(e1z, e2x), __dmul_rn(e1x, e2z));
+            const double nz = __dsub_rn(__dmul_rn(e1x, e2y), __dmul_rn(e1y, e2x));
+            const double nn = __dsqrt_rn(dot3d(nx, ny, nz, nx, ny, nz));
+            if (nn == 0.0 || !(fabs(det) > 0.0)) continue;
+            const double wx = __dsub_rn(ox, ax), wy = __dsub_rn(oy, ay), wz = __dsub_rn(oz, az);
+            const double d0 = __ddiv_rn(dot3d(wx, wy, wz, nx, ny, nz), nn);
+            const double d1 = __dadd_rn(d0, __dmul_rn(reach, __ddiv_rn(dot3d(dx, dy, dz, nx, ny, nz), nn)));
+            const double el = e1n > e2n ? e1n : e2n;
+            const double rl = __dmul_rn(reach, dn);
+            const double lim = __dmul_rn(m, el > rl ? el : rl);
+            const bool clear = (d0 > lim && d1 > lim) || (d0 < -lim && d1 < -lim);
+            if (!clear) ambiguous = true;
             continue;
         }
         const double inv = __ddiv_rn(1.0, det);

@@ -504,9 +504,22 @@ extern "C" int orc_fp64_classify(const float *v9, int32_t ntris, const orc_ray *
                 double scale = dn * e1n * e2n;
                 if (scale == 0.0) continue;
                 if (std::fabs(det) <= rel_margin * scale) {
-                    // Grazing: parallel within margin.  Ambiguous only if the
-                    // ray passes near the triangle; keep it simple and flag.
-                    if (std::fabs(det) > 0) cls = cls == 1 ? 1 : 2;
+                    // Grazing: parallel within margin.  Ambiguous when the
+                    // segment runs within the margin of the triangle's plane
+                    // (or crosses it); a segment clear of the plane on one
+                    // side misses.
+                    double nv[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                                    e1[0] * e2[1] - e1[1] * e2[0]};
+                    double nn = std::sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+                    if (nn == 0.0 || !(std::fabs(det) > 0)) continue;
+                    double w[3] = {o[0] - a[0], o[1] - a[1], o[2] - a[2]};
+                    double d0 = (w[0] * nv[0] + w[1] * nv[1] + w[2] * nv[2]) / nn;
+                    double d1 = d0 + reach * ((d[0] * nv[0] + d[1] * nv[1] + d[2] * nv[2]) / nn);
+                    double lim = e1n > e2n ? e1n : e2n;
+                    double rl = reach * dn;
+                    lim = rel_margin * (lim > rl ? lim : rl);
+                    bool clear = (d0 > lim && d1 > lim) || (d0 < -lim && d1 < -lim);
+                    if (!clear) cls = cls == 1 ? 1 : 2;
                     continue;
                 }
                 double inv = 1.0 / det;
