@@ -332,7 +332,7 @@ class CudaRayTracer:
         self.trace_visibility(rays, bits, options)
         return np.unpackbits(bits.view(np.uint8), bitorder="little")[:n].astype(bool)
 
-    def visibility_recheck(self, rays, options: RayTraceOptions = RayTraceOptions(), flag_margin: float = 1e-5,
+    def visibility_recheck(self, rays, options: RayTraceOptions = RayTraceOptions(), flag_margin: float = 1e-3,
                            fp64_margin: float = 1e-6):
         """vrad_trace_visibility_recheck: (the FP32 visibility, as visibility
         gives it; per ray the FP64 class of a flagged ray, 0 miss, 1 hit,
