@@ -318,3 +318,56 @@ def fixed8(t, lo, hi) -> int:
     cv = np.float32(min(max(cv, np.float32(0.0)), np.float32(1.0)))
     frac = np.float32(np.float32(0.0) + np.float32(np.float32(255.0) * cv))
     return int(np.float32(frac + np.float32(0.5)))
+
+
+def gamma_table() -> np.ndarray:
+    """StockLightColor's linear-to-screen table (StockLightColor.cs:186-250):
+    1,024 ints, entry i = (int)(255 x DetMath.Pow(f, 1 / 2.2)) of the
+    piecewise-remapped (float)(i / 1023)."""
+    g = np.float32(1.0 / float(np.float32(2.2)))
+    g3 = np.float32(0.125)
+    out = np.zeros(1024, np.int32)
+    for i in range(1024):
+        f = np.float32(i / 1023.0)
+        if f <= g3:
+            f = np.float32(float(np.float32(f / g3)) * 0.125)
+        else:
+            f = np.float32(0.125 + ((float(np.float32(f - g3)) / (1.0 - float(g3))) * 0.875))
+        v = int(255 * DM.pow_d(float(f), float(g)))
+        out[i] = min(max(v, 0), 255)
+    return out
+
+
+def leaf_ambient_lumps(tree: AmbientTree, counts, positions, cubes, correct_tiebreak: bool = False):
+    """vrad_leaf_ambient_lumps: every leaf's samples (counts and positions
+    as candidate_positions gives them, cubes (n, 6, 3)) through the 16-sample
+    list and its compression into (LEAF_AMBIENT_INDEX bytes,
+    LEAF_AMBIENT_LIGHTING bytes, bad leaf count)."""
+    from . import tracer as T
+    lib = _lib()
+    if not getattr(lib, "_lumps_bound", False):
+        P, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+        lib.vrad_leaf_ambient_lumps.argtypes = [ctypes.POINTER(lib._AmbientTree), P, P, P, P, i32, P, P, i64,
+                                                ctypes.POINTER(i64), ctypes.POINTER(i32)]
+        lib.vrad_leaf_ambient_lumps.restype = i32
+        lib._lumps_bound = True
+    keep = [np.ascontiguousarray(a) for a in (tree.planes, tree.nodes, tree.leaves, tree.leaf_brushes,
+                                               tree.brushes, tree.brush_sides)]
+    pl, nd, lv, lb, br, bs = keep
+    ptr = lambda a: a.ctypes.data if a is not None and a.size else None  # noqa: E731
+    t = lib._AmbientTree(ptr(pl), len(pl), ptr(nd), len(nd), ptr(lv), len(lv), ptr(lb), len(lb), ptr(br), len(br),
+                         ptr(bs), len(bs))
+    c = np.ascontiguousarray(counts, np.int32)
+    p = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+    q = np.ascontiguousarray(cubes, np.float32).reshape(-1, 18)
+    table = gamma_table()
+    index = np.zeros(4 * len(lv), np.uint8)
+    recs, bad = ctypes.c_int64(), ctypes.c_int32()
+    T._check(lib.vrad_leaf_ambient_lumps(ctypes.byref(t), c.ctypes.data, ptr(p), ptr(q), table.ctypes.data,
+                                         int(correct_tiebreak), index.ctypes.data, None, 0, ctypes.byref(recs),
+                                         ctypes.byref(bad)), None)
+    light = np.zeros(max(1, 28 * recs.value), np.uint8)
+    T._check(lib.vrad_leaf_ambient_lumps(ctypes.byref(t), c.ctypes.data, ptr(p), ptr(q), table.ctypes.data,
+                                         int(correct_tiebreak), index.ctypes.data, light.ctypes.data, recs.value,
+                                         ctypes.byref(recs), ctypes.byref(bad)), None)
+    return index.tobytes(), light[:28 * recs.value].tobytes(), int(bad.value)

@@ -752,6 +752,22 @@ typedef struct vrad_ambient_tree {
 int32_t vrad_leaf_ambient_positions(const vrad_ambient_tree *tree, int32_t *counts, float *positions,
                                     int64_t capacity, int64_t *total, int32_t threads);
 
+/* The stage's last steps (host code): every leaf's samples, in order, into
+ * the 16-sample list (AmbientSampleList.Add; stock's tie-break, which never
+ * fires, unless correct_tiebreak), compressed (AmbientSampleList.Compress,
+ * over gamma_table: StockLightColor's 1,024-entry linear-to-screen table),
+ * and encoded (LeafAmbientBuilder.Encode): index_out = nleaves records of
+ * (uint16 count, uint16 first), an empty leaf's first naming its nearest
+ * neighbour with samples; lighting_out = *records records of 28 bytes (six
+ * RGBE colours, the 8-bit position fractions, a zero pad).  counts and
+ * positions are vrad_leaf_ambient_positions', cubes the samples' cubes (18
+ * floats each: with the baked surface lights added, when the caller has
+ * them).  With lighting_out NULL only *records is filled. */
+int32_t vrad_leaf_ambient_lumps(const vrad_ambient_tree *tree, const int32_t *counts, const float *positions,
+                                const float *cubes, const int32_t *gamma_table, int32_t correct_tiebreak,
+                                uint8_t *index_out, uint8_t *lighting_out, int64_t capacity, int64_t *records,
+                                int32_t *bad_leaves);
+
 /* One BSP face's lightmap lookups (AmbientScene's FaceShade,
  * AmbientScene.cs:247-318).  styles packs the four style bytes, slot 0 in
  * the low byte; averages[k] is slot k's average colour (the four bytes

@@ -672,3 +672,182 @@ class Bounce:
         if rc != 0:
             raise RuntimeError(f"orc_bounce_final failed: {rc}")
         return out, ofs
+
+
+# ---- Leaf ambient: the 16-sample list and the lumps (restated in Python) ----
+#
+# Follows MapTools/Rad/Ambient: AmbientSampleList.cs:40-222 (Add, Compress,
+# ColorAtPosition, CubeDeltaGammaSpace), LeafAmbientBuilder.cs:503-670
+# (Encode, NearestNeighborWithLight, AabbDistance, Fixed8Fraction),
+# ToolBspTree.cs:20-90 (EnumerateLeavesInBox), StockLightColor.cs:110-150
+# (Encode).  A sample is (position, cube): three float32 and 6 x 3 float32.
+
+def _f32(x):
+    return np.float32(x)
+
+
+def _len(v):
+    return _f32(np.sqrt(_f32(_f32(_f32(v[0] * v[0]) + _f32(v[1] * v[1])) + _f32(v[2] * v[2]))))
+
+
+def _len_sq(v):
+    return _f32(_f32(_f32(v[0] * v[0]) + _f32(v[1] * v[1])) + _f32(v[2] * v[2]))
+
+
+def sample_list_add(samples: list, pos, cube, dead_tiebreak: bool = True) -> None:
+    """AmbientSampleList.Add; samples is a list of (pos (3,), cube (6, 3))
+    float32 arrays, changed in place."""
+    samples.append((np.asarray(pos, np.float32), np.asarray(cube, np.float32).reshape(6, 3)))
+    if len(samples) <= 16:
+        return
+    nearest, nearest_dist, nearest_total = 0, _f32(3.4028234663852886e38), _f32(0)
+    for i, (pa, ca) in enumerate(samples):
+        closest, total = _f32(3.4028234663852886e38), _f32(0)
+        for j, (pb, cb) in enumerate(samples):
+            if j == i:
+                continue
+            dist = _len((pa - pb).astype(np.float32))
+            max_dc = _f32(0)
+            for k in range(6):
+                for c in range(3):
+                    d = _f32(abs(_f32(ca[k, c] - cb[k, c])))
+                    max_dc = max_dc if max_dc > d else d
+                total = _f32(total + max_dc)
+            if max_dc < _f32(1e-4):
+                max_dc = _f32(0)
+            elif max_dc > _f32(1):
+                max_dc = _f32(1)
+            dist = _f32(dist * _f32(_f32(0.1) + _f32(max_dc * _f32(0.9))))
+            if dist < closest:
+                closest = dist
+        if closest < nearest_dist or (not dead_tiebreak and closest == nearest_dist and total < nearest_total):
+            nearest_dist, nearest = closest, i
+            if not dead_tiebreak:
+                nearest_total = total
+    samples[nearest] = samples[-1]
+    samples.pop()
+
+
+def color_at_position(samples: list, pos, skip: int) -> np.ndarray:
+    """AmbientSampleList.ColorAtPosition: (6, 3) float32."""
+    into = np.zeros((6, 3), np.float32)
+    total = _f32(0)
+    for i, (p, c) in enumerate(samples):
+        if i == skip:
+            continue
+        factor = _f32(_f32(1) / _f32(_len_sq((p - np.asarray(pos, np.float32)).astype(np.float32)) + _f32(1)))
+        total = _f32(total + factor)
+        into = (into + (c * factor).astype(np.float32)).astype(np.float32)
+    return (into * _f32(_f32(1) / total)).astype(np.float32)
+
+
+def gamma_delta(a, b, table) -> int:
+    """AmbientSampleList.CubeDeltaGammaSpace over the 1,024-entry table."""
+    def g(f):
+        i = int(np.trunc(np.float32(np.float32(f) * np.float32(1023)))) if np.isfinite(f) else 0
+        return int(table[min(max(i, 0), 1023)])
+    return max(abs(g(x) - g(y)) for x, y in zip(np.asarray(a).ravel(), np.asarray(b).ravel()))
+
+
+def sample_list_compress(samples: list, table) -> None:
+    """AmbientSampleList.Compress, in place."""
+    i = 0
+    while i < len(samples):
+        if len(samples) > 1:
+            test = color_at_position(samples, samples[i][0], i)
+            if gamma_delta(test, samples[i][1], table) < 3:
+                samples[i] = samples[-1]
+                samples.pop()
+                i -= 1
+        i += 1
+
+
+def encode_rgbe(v) -> bytes:
+    """StockLightColor.Encode of one colour."""
+    x, y, z = (np.float32(c) for c in v)
+    mx = (x if x > z else z) if x > y else (y if y > z else z)
+    e = 0 if mx == 0 else int((int(np.float32(mx).view(np.uint32)) & 0x7F800000) >> 23) - (7 + 127)
+    sc = np.uint32(((127 - e) << 23) & 0xFFFFFFFF).view(np.float32)
+    return bytes([int(np.float32(c * sc)) & 0xFF for c in (x, y, z)] + [e & 0xFF])
+
+
+def fixed8(t, lo, hi) -> int:
+    t, lo, hi = np.float32(t), np.float32(lo), np.float32(hi)
+    if hi <= lo:
+        return 0
+    cv = np.float32(np.float32(t - lo) / np.float32(hi - lo))
+    cv = np.float32(min(max(cv, np.float32(0)), np.float32(1)))
+    return int(np.float32(np.float32(np.float32(0) + np.float32(np.float32(255) * cv)) + np.float32(0.5))) & 0xFF
+
+
+def leaves_in_box(planes, nodes, mins, maxs) -> list:
+    out, pending = [], [0]
+    while pending:
+        node = pending.pop()
+        while node >= 0:
+            p = planes[int(nodes[node][0])]
+            cmin = [mins[i] if p[i] >= 0 else maxs[i] for i in range(3)]
+            cmax = [maxs[i] if p[i] >= 0 else mins[i] for i in range(3)]
+            dmax = _f32(_f32(_f32(p[0] * cmax[0]) + _f32(p[1] * cmax[1])) + _f32(p[2] * cmax[2]))
+            dmin = _f32(_f32(_f32(p[0] * cmin[0]) + _f32(p[1] * cmin[1])) + _f32(p[2] * cmin[2]))
+            if _f32(dmax - p[3]) <= _f32(-0.03125):
+                node = int(nodes[node][2])
+            elif _f32(dmin - p[3]) >= _f32(0.03125):
+                node = int(nodes[node][1])
+            else:
+                pending.append(int(nodes[node][2]))
+                node = int(nodes[node][1])
+        out.append(-node - 1)
+    return out
+
+
+def leaf_ambient_lumps(planes, nodes, leaves, counts, positions, cubes, table, dead_tiebreak: bool = True):
+    """The leaf ambient lumps from every leaf's samples: (index bytes,
+    lighting bytes, bad leaves)."""
+    first = np.concatenate([[0], np.cumsum(counts)])
+    lists = []
+    for l in range(len(leaves)):
+        s = []
+        for k in range(int(first[l]), int(first[l + 1])):
+            sample_list_add(s, positions[k], cubes[k], dead_tiebreak)
+        sample_list_compress(s, table)
+        lists.append(s)
+    count = [len(s) for s in lists]
+    firstrec, lighting, at = [0] * len(leaves), bytearray(), 0
+    for l, s in enumerate(lists):
+        L = leaves[l]
+        mn, mx = [np.float32(L[1 + a]) for a in range(3)], [np.float32(L[4 + a]) for a in range(3)]
+        firstrec[l] = at if s else 0
+        for p, c in s:
+            lighting += b"".join(encode_rgbe(c[j]) for j in range(6))
+            lighting += bytes([fixed8(p[a], mn[a], mx[a]) for a in range(3)] + [0])
+            at += 1
+    bad = 0
+    for l in range(len(leaves)):
+        if count[l]:
+            continue
+        L = leaves[l]
+        if (int(L[0]) & 1) == 0:
+            bad += 1
+        mn = [np.float32(L[1 + a]) for a in range(3)]
+        mx = [np.float32(L[4 + a]) for a in range(3)]
+        size = [_f32(mx[a] - mn[a]) for a in range(3)]
+        near = leaves_in_box(planes, nodes, [_f32(mn[a] - size[a]) for a in range(3)],
+                             [_f32(mx[a] + size[a]) for a in range(3)])
+        best, best_leaf = _f32(3.4028234663852886e38), l
+        for o in near:
+            if count[o] == 0:
+                continue
+            M = leaves[o]
+            d = []
+            for a in range(3):
+                g = max(mn[a], np.float32(M[1 + a]))
+                s_ = min(mx[a], np.float32(M[4 + a]))
+                d.append(_f32(0) if g < s_ else _f32(s_ - g))
+            dist = _len(np.array(d, np.float32))
+            if dist < best:
+                best, best_leaf = dist, o
+        firstrec[l] = best_leaf
+    index = b"".join(int(c).to_bytes(2, "little") + int(f & 0xFFFF).to_bytes(2, "little")
+                     for c, f in zip(count, firstrec))
+    return index, bytes(lighting), bad
