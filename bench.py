@@ -18,6 +18,7 @@ to the LIGHTING and LIGHTING_HDR lumps:
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
     python bench.py --workload seam     # the IRayTracer seam alone, rays in HBM
+    python bench.py --workload transfer-cache   # the transfer cache's store and hit
 
 Prints one JSON line (rank 0).  `value` is rays/s (the rays the reference
 traces for the stage, over the device-timed step, all ranks) with the world
@@ -60,7 +61,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--side", type=int, default=8, help=argparse.SUPPRESS)
-    ap.add_argument("--workload", default="stage", choices=["stage", "seam", "ambient", "forward"])
+    ap.add_argument("--workload", default="stage", choices=["stage", "seam", "ambient", "forward", "transfer-cache"])
     ap.add_argument("--ambient-samples", type=int, default=131072, help=argparse.SUPPRESS)
     ap.add_argument("--no-e2e", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-cpu", action="store_true", help=argparse.SUPPRESS)
@@ -1176,8 +1177,54 @@ def forward_run(rows: int = 999080, reps: int = 20) -> dict:
             "frac": tf / peak, "peak_source": "measured" if "bf16_tflops" in peaks else "fallback"}
 
 
+def transfer_cache_run(args, reps: int = 3) -> dict:
+    """The transfer cache on the map of --side (default 8x8): the store
+    (vrad_transfer_export: the set put in patch order and shuffled into
+    planes on the device, deflated on the host's threads) and the hit
+    (vrad_transfer_install: inflated on the host's threads, decoded and put
+    in receiver order on the device, sliced for the gather), each timed
+    around its blocking library call (best of `reps`), beside the transfer
+    build they stand in for; then a pass lit with the installed set checked
+    against one that built its own."""
+    from hl2sdk_tools_sharp_b200 import lighting as L, transfer_cache as C
+    w, inp = world_and_inputs(args.side, CONFIG_SEED)
+    refl = L.face_reflectivity(w)
+    pvs_off, pvs_list = L.pvs_lists(w)
+    with L.LightingStage(w, inp) as st:
+        st.upload_bounce(refl, pvs_off, pvs_list, bounces=MAX_BOUNCES, threshold=BOUNCE_THRESHOLD)
+        ldr, hdr, _, _, bst = st.light_pass_ranges()
+        build_ms, total = float(bst[0].transfer_ms), int(bst[0].transfers)
+        store = []
+        for _ in range(reps):
+            t = {}
+            idx, packed = C.export(st, timing=t)
+            store.append(t["abi_s"])
+    packed_bytes = int(sum(memoryview(p).nbytes for p in packed))
+    with L.LightingStage(w, inp) as st:
+        st.upload_bounce(refl, pvs_off, pvs_list, bounces=MAX_BOUNCES, threshold=BOUNCE_THRESHOLD)
+        hit = []
+        for _ in range(reps):
+            t = {}
+            assert C.install(st, idx, packed, timing=t)
+            hit.append(t["abi_s"])
+        ldr2, hdr2, _, _, bst2 = st.light_pass_ranges()
+    raw = 8 * total
+    return {"workload": f"{args.side}x{args.side} room grid transfer set ({total} transfers, {len(packed)} chunks "
+                        f"of at most {C.DEFAULT_MAX_CHUNK_BYTES} bytes)",
+            "transfers": total, "raw_bytes": raw, "packed_bytes": packed_bytes + len(idx),
+            "ratio": (packed_bytes + len(idx)) / raw if raw else None,
+            "build_ms": build_ms, "store_ms": 1000 * min(store), "hit_ms": 1000 * min(hit),
+            "store_gbs": raw / min(store) / 1e9, "hit_gbs": raw / min(hit) / 1e9,
+            "host_threads": os.cpu_count(),
+            "replay": {"transfers_cached": int(bst2[0].transfers_cached), "transfer_rays": int(bst2[0].transfer_rays),
+                       "lumps_equal": bool(np.array_equal(ldr, ldr2) and np.array_equal(hdr, hdr2))}}
+
+
 def main():
     args = parse()
+    if args.workload == "transfer-cache":
+        print(json.dumps(transfer_cache_run(args)), flush=True)
+        return 0
     if args.workload == "forward":
         print(json.dumps(forward_run()), flush=True)
         return 0

@@ -760,7 +760,16 @@ cudaError_t launch_transfers(BounceBuffers &b, const DeviceScene &scene, uint32_
     if (!b.tr) return cudaGetLastError();
     k_transfer_write<<<blocks((int64_t)R * 32, kBounceBlock), kBounceBlock, 0, stream>>>(
         R, b.cand_off, b.cand_src, b.cand_w, b.tr_off, b.tr);
-    // The gather's slices.
+    e = cudaGetLastError();
+    return e != cudaSuccess ? e : launch_sell(b, stream);
+}
+
+// The gather's slices (SELL-32) from the transfer lists tr_off / tr.
+cudaError_t launch_sell(BounceBuffers &b, cudaStream_t stream) {
+    const int R = b.nreceivers;
+    if (R == 0) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    size_t tmp = 0;
     const int nslices = (R + 31) / 32;
     k_sell_keys<<<blocks(R, kBounceBlock), kBounceBlock, 0, stream>>>(R, b.tr_off, b.sell_key, b.sell_idx);
     tmp = b.sort_tmp_bytes;

@@ -133,6 +133,11 @@ struct BounceBuffers {
     // levels, the totals, their copy to h_sums), made on first use.
     cudaGraphExec_t bounce_graph[2] = {nullptr, nullptr};
     bool ready = false;
+    // The transfer lists came from vrad_transfer_install: every light pass
+    // bounces with them instead of building, until the next upload.
+    bool installed = false;
+    // tr_off / tr hold a set (a light pass bounced, or one was installed).
+    bool lists_ready = false;
     // Statistics of the last pass.
     int32_t bounces_run = 0, exact_totals = 0;
     double added[3] = {0, 0, 0};
@@ -147,6 +152,9 @@ struct BounceBuffers {
 cudaError_t launch_patch_light(const BounceBuffers &b, const float4 *sample_light, cudaStream_t stream);
 cudaError_t launch_transfers(BounceBuffers &b, const DeviceScene &scene, uint32_t *overflow, cudaStream_t stream,
                              bool count_only);
+// The gather's slices from the transfer lists (the transfer build's last
+// step; also after the lists are installed from a cache).
+cudaError_t launch_sell(BounceBuffers &b, cudaStream_t stream);
 cudaError_t launch_gather(BounceBuffers &b, int bounce, cudaStream_t stream);
 cudaError_t launch_exact_total(BounceBuffers &b, int bounce, cudaStream_t stream);
 // Bounce number `bounce` and the copy of its totals to h_sums as one graph

@@ -271,7 +271,10 @@ cudaError_t run_bounce(vrad_ctx *ctx, cudaStream_t s, const float4 *sample_light
     if (e == cudaSuccess && b.nreceivers)
         e = cudaMemcpyAsync(&ntr, b.tr_off + b.nreceivers, sizeof ntr, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = vrad::wait_stream(s);
-    if (e == cudaSuccess) b.ntransfers = ntr;
+    if (e == cudaSuccess) {
+        b.ntransfers = ntr;
+        b.lists_ready = true;
+    }
     if (e == cudaSuccess) {
         cudaEventElapsedTime(&b.patch_light_ms, ev[0], ev[1]);
         cudaEventElapsedTime(&b.transfer_ms, ev[1], ev[2]);
@@ -673,6 +676,7 @@ void fill_bounce_stats(const vrad_ctx *ctx, vrad_bounce_stats *st) {
     st->bounce_ms = b.bounce_ms;
     st->final_ms = b.final_ms;
     st->unsettled_asin = (int64_t)b.open_ties;
+    st->transfers_cached = b.installed ? 1 : 0;
 }
 }  // namespace vrad
 

@@ -657,7 +657,7 @@ int32_t pass_on(vrad_ctx *ctx, int32_t ranges, uint8_t *d_ldr, uint8_t *d_hdr, c
         vrad::PatchRadialView prad{};
         if (bounce) {
             std::string why;
-            e = vrad::run_bounce(ctx, s, light, !built, why);
+            e = vrad::run_bounce(ctx, s, light, !built && !ctx->bounce.installed, why);
             if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, why.c_str());
             built = true;
             prad = vrad::patch_radial_view(ctx);

@@ -92,7 +92,8 @@ class BounceStats(ctypes.Structure):
                 ("blocked", ctypes.c_int64), ("transfers", ctypes.c_int64), ("bounces", ctypes.c_int32),
                 ("exact_totals", ctypes.c_int32), ("added", ctypes.c_double * 3),
                 ("patch_light_ms", ctypes.c_float), ("transfer_ms", ctypes.c_float),
-                ("bounce_ms", ctypes.c_float), ("final_ms", ctypes.c_float), ("unsettled_asin", ctypes.c_int64)]
+                ("bounce_ms", ctypes.c_float), ("final_ms", ctypes.c_float), ("unsettled_asin", ctypes.c_int64),
+                ("transfers_cached", ctypes.c_int32)]
 
 
 class DirectStats(ctypes.Structure):

@@ -35,7 +35,7 @@ LIB_PATH = HERE / "libvrad_cuda.so"
 VRAD_OK = 0
 ERRORS = {
     -1: "VRAD_ERR_ARG", -2: "VRAD_ERR_CUDA", -3: "VRAD_ERR_OOM", -4: "VRAD_ERR_TIMEOUT",
-    -5: "VRAD_ERR_NO_SCENE", -6: "VRAD_ERR_UNSUPPORTED", -7: "VRAD_ERR_NO_DEVICE",
+    -5: "VRAD_ERR_NO_SCENE", -6: "VRAD_ERR_UNSUPPORTED", -7: "VRAD_ERR_NO_DEVICE", -8: "VRAD_ERR_FORMAT",
 }
 
 TRACE_ID_SKY = 0x01000000   # TraceId.Sky (MapTools/Rad/TraceId.cs)

@@ -37,6 +37,7 @@ extern "C" {
 #define VRAD_ERR_NO_SCENE (-5)     /* trace before vrad_scene_upload                     */
 #define VRAD_ERR_UNSUPPORTED (-6)  /* option this tracer cannot honour (NotSupported)    */
 #define VRAD_ERR_NO_DEVICE (-7)    /* no CUDA device / wrong architecture                */
+#define VRAD_ERR_FORMAT (-8)       /* bytes that do not decode (the codec's null result) */
 
 /* Ray: origin, direction (need not be unit length), reach in units of the
  * direction's length.  28 bytes, the reference's wire format. */
@@ -472,6 +473,8 @@ typedef struct vrad_bounce_stats {
     float bounce_ms;
     float final_ms;
     int64_t unsettled_asin;   /* form-factor arcsines left at the plain rounding (expected 0) */
+    int32_t transfers_cached; /* 1: the pass bounced with transfers from vrad_transfer_install
+                                 (RadWorld.TransfersWereCached); transfer_rays and blocked are 0 */
 } vrad_bounce_stats;
 
 /* The statistics of the last light pass's bounce. */
@@ -553,6 +556,79 @@ typedef struct vrad_transfer {
  * offsets[p + 1])).  With transfers NULL it only fills offsets and count. */
 int32_t vrad_bounce_transfers(vrad_ctx *ctx, int64_t *offsets, int64_t npatches, vrad_transfer *transfers,
                               int64_t capacity, int64_t *count);
+
+/* ---- Transfer cache: a transfer set as bytes ------------------------------
+ *
+ * TransferSetCodec (MapTools/Rad/Bounce/TransferSetCodec.cs:23-447), the
+ * format the reference's cross-compile transfer cache stores
+ * (Compile/Cache/StoreTransferCache.cs:241-262, 360-378):
+ *   index: "TRF1" (u32 0x31465254), the patch count (i32), the longest list
+ *     (i32), the total (i64), then every patch's count (i32), little-endian;
+ *   chunks: the transfers patch after patch as (patch i32, weight's f32
+ *     bits), cut every max(1, max_chunk_bytes / 8) transfers (a list may
+ *     straddle two chunks; an empty set has no chunk);
+ *   packed chunk: the chunk's transfer count n (i32), then a zlib stream
+ *     (RFC 1950, deflate level 1) of 8n bytes: byte b of every patch delta
+ *     (the patch minus the one before it in the chunk, the first minus 0,
+ *     wrapping) as plane b, then byte b of every weight as plane 4 + b.
+ * The planes are the reference's byte for byte; the deflate stream is
+ * zlib's own, so the packed bytes are not necessarily those of another
+ * deflater, and any zlib stream of the right bytes reads back. */
+#define VRAD_TRANSFER_MAGIC 0x31465254u
+
+/* Index(set) from the lists' offsets (offsets[npatches + 1], as
+ * vrad_bounce_transfers fills them) into out (20 + 4 npatches bytes).
+ * VRAD_ERR_ARG when a list is longer than an int or the offsets fall. */
+int32_t vrad_transfer_index(const int64_t *offsets, int32_t npatches, uint8_t *out, int64_t capacity);
+
+/* Pack(chunk) on host bytes: len a multiple of 8.  *written = the packed
+ * size; vrad_transfer_pack_bound(len) bytes always suffice. */
+int64_t vrad_transfer_pack_bound(int64_t len);
+int32_t vrad_transfer_pack(const uint8_t *chunk, int64_t len, uint8_t *out, int64_t capacity, int64_t *written);
+
+/* Unpack(packed) on host bytes.  VRAD_ERR_FORMAT (the reference's null)
+ * when the bytes are not a packed chunk: shorter than 4, a count out of
+ * range, a stream that does not inflate to exactly 8n bytes. */
+int32_t vrad_transfer_unpack(const uint8_t *packed, int64_t len, uint8_t *out, int64_t capacity, int64_t *written);
+
+/* The context's transfer set (after a light pass that bounced, or an
+ * install) as the index and its packed chunks, for a store: the set is put
+ * in patch order and shuffled into planes on the device, then each chunk is
+ * deflated on the host's threads.  vrad_transfer_export_size reports the
+ * index size, the chunk count and a packed size that always suffices;
+ * vrad_transfer_export writes the index, the packed chunks back to back
+ * into packed, their sizes into chunk_sizes[nchunks], and the bytes used
+ * into *packed_len.  Blocks. */
+int32_t vrad_transfer_export_size(vrad_ctx *ctx, int64_t max_chunk_bytes, int64_t *index_len, int64_t *nchunks,
+                                  int64_t *packed_bound);
+int32_t vrad_transfer_export(vrad_ctx *ctx, int64_t max_chunk_bytes, uint8_t *index, int64_t index_capacity,
+                             uint8_t *packed, int64_t packed_capacity, int64_t *chunk_sizes, int64_t chunk_capacity,
+                             int64_t *packed_len);
+
+/* ReadPacked(index, chunks, patch_count) into host arrays: chunk k is
+ * packed[at_k .. at_k + chunk_sizes[k]) with at_k the sum of the sizes
+ * before it.  The chunks inflate on the host's threads and their planes are
+ * turned back into transfers on ctx's device; offsets[patch_count + 1] and
+ * *total are filled, transfers (nullable: offsets only) needs room for the
+ * total.  VRAD_ERR_FORMAT (the reference's null) when they do not fit
+ * together: the index's magic, patch count, size, counts, total and
+ * longest list; the chunks' counts adding up to the total; every chunk
+ * inflating to exactly its count; every patch in range.  Blocks. */
+int32_t vrad_transfer_read_packed(vrad_ctx *ctx, const uint8_t *index, int64_t index_len, const uint8_t *packed,
+                                  const int64_t *chunk_sizes, int64_t nchunks, int32_t patch_count,
+                                  int64_t *offsets, vrad_transfer *transfers, int64_t capacity, int64_t *total);
+
+/* A cache hit (RadWorld.BounceAsync's TryGetAsync branch,
+ * MapTools/Rad/Light/RadWorld.Bounce.cs:364-374): ReadPacked with the
+ * uploaded bounce's patch count, straight into the bounce's transfer
+ * lists; every later light pass bounces with them instead of building its
+ * own (vrad_bounce_stats.transfers_cached), until the next
+ * vrad_bounce_upload.  VRAD_ERR_FORMAT as vrad_transfer_read_packed, and
+ * when the set cannot be this bounce's: a list on a patch that receives
+ * none here, or more transfers than the bounce's candidate pairs.  A
+ * refused set leaves the context's transfers as they were.  Blocks. */
+int32_t vrad_transfer_install(vrad_ctx *ctx, const uint8_t *index, int64_t index_len, const uint8_t *packed,
+                              const int64_t *chunk_sizes, int64_t nchunks);
 
 /* ---- Learned warm start ---------------------------------------------------
  *
