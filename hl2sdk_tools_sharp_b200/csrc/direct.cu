@@ -152,6 +152,11 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
         if (t == 0)
             return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "surface lights are not supported by this build");
         if (t < 1 || t > 4) return vrad_fail(ctx, VRAD_ERR_ARG, "light %d has type %d", l, t);
+        // Every light lands in style 0's lightmap: a styled light would
+        // need a slot of its own (FaceLight.FindOrAllocateStyle).
+        if (w->lights[l].style != 0 || (w->lights_hdr && w->lights_hdr[l].style != 0))
+            return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "light %d has style %d: light styles above 0 are not supported",
+                             l, w->lights[l].style);
     }
     const int32_t total = w->cluster_light_offsets[w->nclusters];
     for (int32_t c = 0; c < w->nclusters; c++)

@@ -156,3 +156,16 @@ def test_supersampling_refuses_samples_not_the_builders(change):
         assert stats.supersampled == 0 and len(plain) == len(s)
     with L.LightingStage(w, inp) as st:
         st.direct()
+
+
+def test_a_styled_light_is_refused():
+    """Light styles above 0 need their own lightmap slots
+    (FaceLight.FindOrAllocateStyle, Rad/Light/FaceLightJob.cs:435-445),
+    which this build does not make: the world upload refuses such a light
+    instead of lighting it into style 0."""
+    w = rg.generate(rg.config_3x3(seed=2))
+    inp = L.prepare(w)
+    lights = inp.lights.copy()
+    lights["style"][len(lights) // 2] = 5
+    with pytest.raises(NotImplementedError, match="style 5"):
+        L.LightingStage(w, L.LightingInputs(**{**inp.__dict__, "lights": lights}))
