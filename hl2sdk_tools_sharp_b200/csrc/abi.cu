@@ -216,6 +216,7 @@ cudaError_t release_tables(vrad_ctx *ctx) {
     ctx->has_scene = false;
     ctx->scene.release();
     ctx->world.release();
+    ctx->styles.release();
     ctx->final_pass.release();
     ctx->bounce.release();
     ctx->supersample.release();
@@ -291,6 +292,7 @@ int32_t vrad_destroy(vrad_ctx *ctx) {
         cudaDeviceSynchronize();
         ctx->scene.release();
         ctx->world.release();
+        ctx->styles.release();
         ctx->final_pass.release();
         ctx->bounce.release();
         ctx->bounce.free_pinned();

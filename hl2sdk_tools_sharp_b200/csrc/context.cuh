@@ -51,6 +51,7 @@ struct vrad_ctx {
     float4 *sample_light = nullptr;      // the direct gather's output, one per sample (LDR)
     float4 *sample_light_hdr = nullptr;  // the HDR range's, when the world has an HDR list
     vrad::RangeSupersample range_ss[2];  // the last gather's supersampling, LDR and HDR
+    vrad::StyleState styles;             // light styles above 0, when the world has any
     vrad_bounce_stats range_bounce[2] = {};  // the last pass's bounce per range (zero: not lit)
     // Host copies of the uploaded world the bounce set-up reads.
     std::vector<vrad_face> h_faces;

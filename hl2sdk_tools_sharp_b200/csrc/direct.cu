@@ -19,6 +19,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <cstring>
@@ -72,8 +73,11 @@ __global__ void __launch_bounds__(BLOCK) k_direct(DeviceScene sc, DeviceWorld w,
 
     unsigned long long vis_rays = 0, sky_rays = 0;
     float4 h;
+    // The group's first sample (a face's groups start on lanes 0, 4, ...):
+    // groups in sample order are ResolveGroup's order.
+    const unsigned long long key_group = (unsigned long long)(uint32_t)__shfl_sync(kFull, si, lane & ~3) << 32;
     const float4 r = gather_point<BLOCK, DUAL>(sc, w, cluster, px, py, pz, nx, ny, nz, real, gmask, kAllLights,
-                                               stack, overflow, counters, vis_rays, sky_rays, &h);
+                                               stack, overflow, counters, vis_rays, sky_rays, &h, face, key_group);
     if (real) {
         out[si] = r;
         if (DUAL) out_hdr[si] = h;
@@ -92,6 +96,21 @@ __global__ void __launch_bounds__(BLOCK) k_direct(DeviceScene sc, DeviceWorld w,
 }
 
 }  // namespace
+
+void StyleState::release() {
+    for (int r = 0; r < 2; r++) {
+        for (float4 *p : light[r]) dev_free(p);
+        light[r].clear();
+    }
+    dev_free(keys);
+    dev_free(slots);
+    keys = nullptr;
+    slots = nullptr;
+    styles.clear();
+    face_styles.clear();
+    dropped = 0;
+    ready = false;
+}
 
 void WorldBuffers::release() {
     dev_free(slots);
@@ -152,11 +171,9 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
         if (t == 0)
             return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "surface lights are not supported by this build");
         if (t < 1 || t > 4) return vrad_fail(ctx, VRAD_ERR_ARG, "light %d has type %d", l, t);
-        // Every light lands in style 0's lightmap: a styled light would
-        // need a slot of its own (FaceLight.FindOrAllocateStyle).
-        if (w->lights[l].style != 0 || (w->lights_hdr && w->lights_hdr[l].style != 0))
-            return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "light %d has style %d: light styles above 0 are not supported",
-                             l, w->lights[l].style);
+        // A face's style slots are bytes, 255 meaning none.
+        if (w->lights[l].style < 0 || w->lights[l].style > 254)
+            return vrad_fail(ctx, VRAD_ERR_ARG, "light %d has style %d (0 to 254)", l, w->lights[l].style);
     }
     const int32_t total = w->cluster_light_offsets[w->nclusters];
     for (int32_t c = 0; c < w->nclusters; c++)
@@ -324,6 +341,12 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     if (e == cudaSuccess) e = vrad::quiesce(ctx);
     vrad::WorldBuffers &wb = ctx->world;
     wb.release();
+    ctx->styles.release();
+    for (int32_t l = 0; l < nl; l++)
+        if (w->lights[l].style != 0) ctx->styles.styles.push_back(w->lights[l].style);
+    std::sort(ctx->styles.styles.begin(), ctx->styles.styles.end());
+    ctx->styles.styles.erase(std::unique(ctx->styles.styles.begin(), ctx->styles.styles.end()),
+                             ctx->styles.styles.end());
     if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.slots, slots);
     if (e == cudaSuccess) e = vrad::dma_table(&wb.sample_pos, pos, (size_t)w->nsamples, ctx->stream);
     if (e == cudaSuccess) e = vrad::stage_table(ctx->stager, ctx->stream, &wb.face_normal, fnorm);

@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 #include "vrad_internal.cuh"
 
@@ -50,6 +51,15 @@ struct DeviceWorld {
     int32_t sun_samples;
     int64_t nsamples;
     const float4 *lights_hdr;  // null: the world has one range
+    // Light styles (FaceLight.Styles): a launch gathers the lights of one
+    // style alone.  With face_key set, the gather also records, per face,
+    // the first (sample group, light) that the style lights: the key that
+    // orders the face's style slots (FaceLight.FindOrAllocateStyle).  With
+    // face_slot set, the supersampling passes skip the faces whose slot for
+    // this style is negative (the style is not the face's).
+    int32_t style;
+    unsigned long long *face_key;
+    const int8_t *face_slot;
 };
 
 struct WorldBuffers {
@@ -66,6 +76,24 @@ struct WorldBuffers {
     DeviceWorld view{};
     bool ready = false;
     int block = 64;  // threads per CTA of the gather; vrad_direct_autotune picks it
+
+    void release();
+};
+
+// Light styles above 0 (FaceLight.Styles, MapTools/Rad/Light/FaceLight.cs):
+// each style's lights are gathered apart into a sample light of their own;
+// a face keeps style 0 in slot 0 and takes up to three more styles in the
+// order its sample groups first light them (FaceLightJob.ResolveGroup), a
+// fifth being warned and dropped.  The slots decide the lightmap layout, so
+// they are made once per world, before the first light pass.
+struct StyleState {
+    std::vector<int32_t> styles;         // the world's light styles above 0, ascending
+    std::vector<float4 *> light[2];      // per style, its sample light (LDR, HDR)
+    unsigned long long *keys = nullptr;  // styles x faces: (first group's sample, light position)
+    int8_t *slots = nullptr;             // styles x faces: the style's slot on the face, -1 none
+    std::vector<uint8_t> face_styles;    // faces x 4 (FaceLight.Styles; 255: empty)
+    int64_t dropped = 0;                 // faces warned of a fifth style
+    bool ready = false;                  // slots and layout made for the uploaded world
 
     void release();
 };

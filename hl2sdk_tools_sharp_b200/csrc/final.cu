@@ -116,6 +116,7 @@ __global__ void k_radial(FinalView v, const float4 *__restrict__ sample_light, f
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= v.ncells) return;
     const int f = __ldg(&v.cell_face[c]);
+    if (v.style_slot && __ldg(&v.style_slot[f]) < 0) return;
     const Frame fr = load_frame(v.frames, f);
     const int base = __ldg(&v.face_cells[f]);
     const int local = (int)(c - base);
@@ -133,12 +134,15 @@ __global__ void k_radial(FinalView v, const float4 *__restrict__ sample_light, f
                        lz, lsun, weight);
         }
     }
-    // Then every neighbour's samples that can reach this face, in order.
+    // Then every neighbour's samples that can reach this face, in order
+    // (of a neighbour that has this light style: BuildLuxelRadial matches
+    // the style number, FinalLightFace.cs:339-360).
     const int c0 = __ldg(&v.cand_off[f]), c1 = __ldg(&v.cand_off[f + 1]);
     for (int q = c0; q < c1; q++) {
         const int k = __ldg(&v.cand_sample[q]);
-        add_direct(fr, s, t, __ldg(&v.sample_pos[k]), __ldg(&v.cand_box[q]), __ldg(&sample_light[k]), lx, ly, lz,
-                   lsun, weight);
+        const float4 pos = __ldg(&v.sample_pos[k]);
+        if (v.style_slot && __ldg(&v.style_slot[__float_as_int(pos.w)]) < 0) continue;
+        add_direct(fr, s, t, pos, __ldg(&v.cand_box[q]), __ldg(&sample_light[k]), lx, ly, lz, lsun, weight);
     }
     rad_light[c] = make_float4(lx, ly, lz, lsun);
     rad_weight[c] = weight;
@@ -197,6 +201,8 @@ __global__ void k_luxel(FinalView v, const float4 *__restrict__ rad_light, const
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= v.ncells) return;
     const int f = __ldg(&v.cell_face[c]);
+    const int slot = v.style_slot ? __ldg(&v.style_slot[f]) : 0;
+    if (slot < 0) return;
     const Frame fr = load_frame(v.frames, f);
     const int base = __ldg(&v.face_cells[f]);
     const int j = (int)(c - base);
@@ -258,7 +264,8 @@ __global__ void k_luxel(FinalView v, const float4 *__restrict__ rad_light, const
     lx = lx > 0.0f ? lx : 0.0f;
     ly = ly > 0.0f ? ly : 0.0f;
     lz = lz > 0.0f ? lz : 0.0f;
-    lighting[fr.lightofs / 4 + j] = encode(lx, ly, lz);
+    // Slot k's luxels follow slot k - 1's.
+    lighting[fr.lightofs / 4 + slot * fr.w * fr.h + j] = encode(lx, ly, lz);
     flat[c] = make_float4(lx, ly, lz, ok ? 1.0f : 0.0f);
 }
 
@@ -286,6 +293,8 @@ __global__ void __launch_bounds__(kMedianThreads) k_median(FinalView v, const fl
     __shared__ float ch[3][kMedianMax];
     __shared__ int count;
     const int f = blockIdx.x;
+    const int style_slot = v.style_slot ? __ldg(&v.style_slot[f]) : 0;
+    if (style_slot < 0) return;  // the whole block
     const Frame fr = load_frame(v.frames, f);
     const int base = __ldg(&v.face_cells[f]);
     const int n = fr.w * fr.h;
@@ -310,7 +319,8 @@ __global__ void __launch_bounds__(kMedianThreads) k_median(FinalView v, const fl
     if (threadIdx.x == 0) {
         const int m = count >> 1;
         const float x = count ? ch[0][m] : 0.0f, y = count ? ch[1][m] : 0.0f, z = count ? ch[2][m] : 0.0f;
-        lighting[fr.lightofs / 4 - 1] = encode(x, y, z);
+        // Before lightofs, in reverse style order.
+        lighting[fr.lightofs / 4 - 1 - style_slot] = encode(x, y, z);
     }
 }
 
@@ -594,6 +604,7 @@ cudaError_t build_final(FinalBuffers &fb, const vrad_face *faces, int32_t nfaces
     fb.lighting_bytes = total;
     fb.nfaces = nfaces;
     fb.lightofs = lightofs;
+    fb.h_frames = frames;
     fb.view = FinalView{fb.frames, fb.face_cells, fb.face_nsamples, fb.cell_face, fb.cell_sample, nullptr,
                         fb.sample_box, fb.cand_off, fb.cand_sample, fb.cand_box, ncells};
     fb.ready = true;
@@ -620,6 +631,91 @@ struct PassEvents {
     }
 };
 
+// The style slots and the lightmap layout of a world with light styles
+// above 0, made once per world on stream s: each style's lights gathered
+// (LDR) with the first-lit keys, then per face style 0 in slot 0 and the
+// styles its groups light, in key order, three at most (FaceLightJob's
+// FindOrAllocateStyle; a fifth style is dropped and counted), then the
+// layout (LightmapOffsets.Compute) and the frames' lightofs words.
+int32_t ensure_style_layout(vrad_ctx *ctx, cudaStream_t s) {
+    vrad::StyleState &st = ctx->styles;
+    if (st.styles.empty() || st.ready) return VRAD_OK;
+    vrad::FinalBuffers &fb = ctx->final_pass;
+    if (!fb.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without face windings");
+    const int32_t nf = fb.nfaces, S = (int32_t)st.styles.size();
+    const int64_t ns = ctx->world.view.nsamples;
+    cudaError_t e = cudaSuccess;
+    for (int r = 0; r < 2 && e == cudaSuccess; r++) {
+        if (r == 1 && !ctx->world.view.lights_hdr) break;
+        st.light[r].assign((size_t)S, nullptr);
+        for (int32_t i = 0; i < S && e == cudaSuccess; i++)
+            e = vrad::dev_alloc(&st.light[r][(size_t)i], sizeof(float4) * (size_t)(ns ? ns : 1));
+    }
+    if (e == cudaSuccess) e = vrad::dev_alloc(&st.keys, sizeof(unsigned long long) * (size_t)S * (size_t)(nf ? nf : 1));
+    if (e == cudaSuccess) e = vrad::dev_alloc(&st.slots, (size_t)S * (size_t)(nf ? nf : 1));
+    // The ray counts of these gathers go to a scratch counter: a light
+    // pass's statistics count its own rays.
+    unsigned long long *scratch = nullptr;
+    if (e == cudaSuccess) e = vrad::dev_alloc(&scratch, 3 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemsetAsync(st.keys, 0xFF, sizeof(unsigned long long) * (size_t)S * nf, s);
+    for (int32_t i = 0; i < S && e == cudaSuccess; i++) {
+        vrad::DeviceWorld v = vrad::range_view(ctx->world.view, false);
+        v.style = st.styles[(size_t)i];
+        v.face_key = st.keys + (size_t)i * nf;
+        e = vrad::launch_direct(ctx->scene.view(), v, st.light[0][(size_t)i], nullptr, scratch, ctx->status, s,
+                                ctx->world.block);
+    }
+    std::vector<unsigned long long> keys((size_t)S * nf);
+    if (e == cudaSuccess && nf)
+        e = cudaMemcpyAsync(keys.data(), st.keys, sizeof(unsigned long long) * keys.size(), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = vrad::wait_stream(s);
+    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "light style slots");  // (scratch kept: kernels may run)
+    vrad::dev_free(scratch);
+    std::vector<int8_t> slots((size_t)S * nf, -1);
+    st.face_styles.assign((size_t)nf * 4, 255);
+    st.dropped = 0;
+    for (int32_t f = 0; f < nf; f++) {
+        std::vector<std::pair<unsigned long long, int32_t>> lit;
+        for (int32_t i = 0; i < S; i++)
+            if (keys[(size_t)i * nf + f] != ~0ull) lit.push_back({keys[(size_t)i * nf + f], i});
+        std::sort(lit.begin(), lit.end());
+        st.face_styles[(size_t)f * 4] = 0;
+        for (size_t k = 0; k < lit.size(); k++) {
+            if (k >= 3) {
+                st.dropped++;
+                break;
+            }
+            st.face_styles[(size_t)f * 4 + 1 + k] = (uint8_t)st.styles[(size_t)lit[k].second];
+            slots[(size_t)lit[k].second * nf + f] = (int8_t)(1 + k);
+        }
+    }
+    int64_t total = 0;
+    std::vector<int32_t> ofs((size_t)nf);
+    vrad_lightmap_layout_styles(ctx->h_faces.data(), nf, st.face_styles.data(), ofs.data(), &total);
+    for (int32_t f = 0; f < nf; f++) std::memcpy(&fb.h_frames[(size_t)f * 5 + 4].w, &ofs[(size_t)f], 4);
+    if (e == cudaSuccess && nf)
+        e = cudaMemcpyAsync(st.slots, slots.data(), slots.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && nf)
+        e = cudaMemcpyAsync(fb.frames, fb.h_frames.data(), sizeof(float4) * fb.h_frames.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = vrad::wait_stream(s);
+    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "light style layout");
+    fb.lightofs = ofs;
+    fb.lighting_bytes = total;
+    st.ready = true;
+    return VRAD_OK;
+}
+
+// A world with light styles above 0 first makes its style slots (they
+// decide the layout): the call then gathers each such style once.
+int32_t style_layout_now(vrad_ctx *ctx) {
+    if (ctx->styles.styles.empty() || ctx->styles.ready) return VRAD_OK;
+    if (!ctx->has_scene) return vrad_fail(ctx, VRAD_ERR_NO_SCENE, "no scene uploaded");
+    if (!ctx->world.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "no lighting world uploaded");
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
+    return ensure_style_layout(ctx, ctx->stream);
+}
+
 // The light pass for `ranges` (VRAD_RANGE_*) on stream s: the direct
 // gather (or, with ahead, the one queued at the world upload, its end
 // marked by ctx->ahead_done), then per range, LDR first, its bounce (the
@@ -643,6 +739,31 @@ int32_t pass_on(vrad_ctx *ctx, int32_t ranges, uint8_t *d_ldr, uint8_t *d_hdr, c
         const int32_t rc = vrad::direct_pass(ctx, (ranges & VRAD_RANGE_LDR) ? ctx->sample_light : nullptr,
                                              (ranges & VRAD_RANGE_HDR) ? ctx->sample_light_hdr : nullptr, s);
         if (rc != VRAD_OK) return rc;
+    }
+    // Light styles above 0: each style's gather (both ranges in one
+    // traversal) and its supersampling passes on the faces that hold it.
+    vrad::StyleState &st = ctx->styles;
+    if (!st.styles.empty() && !st.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "light style slots not made");
+    for (size_t i = 0; i < st.styles.size() && e == cudaSuccess; i++) {
+        vrad::DeviceWorld v = ctx->world.view;
+        v.style = st.styles[i];
+        v.face_slot = st.slots + i * (size_t)fb.nfaces;
+        float4 *lo = (ranges & VRAD_RANGE_LDR) ? st.light[0][i] : nullptr;
+        float4 *hi = (ranges & VRAD_RANGE_HDR) ? st.light[1][i] : nullptr;
+        if (lo && hi)
+            e = vrad::launch_direct(ctx->scene.view(), v, lo, hi, ctx->world.counters, ctx->status, s, ctx->world.block);
+        else
+            e = vrad::launch_direct(ctx->scene.view(), vrad::range_view(v, hi != nullptr), lo ? lo : hi, nullptr,
+                                    ctx->world.counters, ctx->status, s, ctx->world.block);
+        for (int r = 0; r < 2 && e == cudaSuccess; r++) {
+            float4 *out = r == 0 ? lo : hi;
+            if (!out) continue;
+            vrad::SupersampleBuffers &ss = ctx->supersample;
+            e = vrad::run_supersample(ss, ctx->scene.view(), vrad::range_view(v, r == 1), fb.view, out,
+                                      ctx->world.counters, ctx->status, s);
+            ctx->range_ss[r].supersampled += ss.supersampled;
+            ctx->range_ss[r].ms += ss.ms;
+        }
     }
     if (e == cudaSuccess && ev) e = cudaEventRecord(ev->direct, s);
     const bool bounce = vrad::bounce_active(ctx);
@@ -669,6 +790,13 @@ int32_t pass_on(vrad_ctx *ctx, int32_t ranges, uint8_t *d_ldr, uint8_t *d_hdr, c
         if (e == cudaSuccess)
             e = vrad::launch_final(fb.view, light, fb.rad_light, fb.rad_weight, fb.flat, out, fb.nfaces,
                                    bounce ? &prad : nullptr, s);
+        // Each further style into its slots (the bounce goes into style 0's
+        // alone).
+        for (size_t i = 0; i < st.styles.size() && e == cudaSuccess; i++) {
+            vrad::FinalView v = fb.view;
+            v.style_slot = st.slots + i * (size_t)fb.nfaces;
+            e = vrad::launch_final(v, st.light[r][i], fb.rad_light, fb.rad_weight, fb.flat, out, fb.nfaces, nullptr, s);
+        }
         if (e == cudaSuccess && ev) e = cudaEventRecord(ev->final_[r], s);
     }
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "light pass launch");
@@ -689,7 +817,9 @@ int32_t pass_device(vrad_ctx *ctx, int32_t ranges, uint8_t *d_ldr, uint8_t *d_hd
     vrad::settle_direct(ctx);
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return vrad_cuda_fail(ctx, e, "cudaSetDevice");
-    const int32_t rc = pass_on(ctx, ranges, d_ldr, d_hdr, (cudaStream_t)stream, nullptr, nullptr);
+    int32_t rc = style_layout_now(ctx);
+    if (rc != VRAD_OK) return rc;
+    rc = pass_on(ctx, ranges, d_ldr, d_hdr, (cudaStream_t)stream, nullptr, nullptr);
     e = vrad::join_stream(ctx, (cudaStream_t)stream);
     return rc != VRAD_OK || e == cudaSuccess ? rc : vrad_cuda_fail(ctx, e, "joining the caller's stream");
 }
@@ -705,6 +835,8 @@ int32_t pass_host(vrad_ctx *ctx, int32_t ranges, uint8_t *ldr, int64_t ldr_capac
     const bool ahead = vrad::settle_direct(ctx) && (ctx->ahead_ranges & ranges) == ranges;
     vrad::FinalBuffers &fb = ctx->final_pass;
     if (!fb.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without face windings");
+    const int32_t lrc = style_layout_now(ctx);
+    if (lrc != VRAD_OK) return lrc;
     for (int r = 0; r < 2; r++) {
         if (!(ranges & (1 << r))) continue;
         const uint8_t *h = r == 0 ? ldr : hdr;
@@ -784,7 +916,25 @@ extern "C" int32_t vrad_lighting_size(vrad_ctx *ctx, int64_t *bytes) {
     if (!ctx || !bytes) return vrad_fail(ctx, VRAD_ERR_ARG, "null argument");
     std::lock_guard<std::mutex> g(ctx->mu);
     if (!ctx->final_pass.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without face windings");
+    const int32_t rc = style_layout_now(ctx);
+    if (rc != VRAD_OK) return rc;
     *bytes = ctx->final_pass.lighting_bytes;
+    return VRAD_OK;
+}
+
+extern "C" int32_t vrad_face_styles(vrad_ctx *ctx, uint8_t *styles, int32_t nfaces, int64_t *dropped) {
+    if (!ctx || !styles) return vrad_fail(ctx, VRAD_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    vrad::FinalBuffers &fb = ctx->final_pass;
+    if (!fb.ready) return vrad_fail(ctx, VRAD_ERR_ARG, "the world was uploaded without face windings");
+    if (nfaces != fb.nfaces) return vrad_fail(ctx, VRAD_ERR_ARG, "%d faces, %d asked", fb.nfaces, nfaces);
+    const int32_t rc = style_layout_now(ctx);
+    if (rc != VRAD_OK) return rc;
+    const vrad::StyleState &st = ctx->styles;
+    for (int32_t f = 0; f < nfaces; f++)
+        for (int k = 0; k < 4; k++)
+            styles[4 * (int64_t)f + k] = st.styles.empty() ? (k == 0 ? 0 : 255) : st.face_styles[(size_t)f * 4 + k];
+    if (dropped) *dropped = st.dropped;
     return VRAD_OK;
 }
 

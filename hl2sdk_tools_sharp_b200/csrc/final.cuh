@@ -36,6 +36,10 @@ struct FinalView {
     const int32_t *cand_sample;
     const float4 *cand_box;
     int64_t ncells;
+    // The pass's light style: each face's slot for it (-1: not the face's
+    // style, the face is skipped and its samples reach no neighbour); null:
+    // style 0, slot 0 on every face.
+    const int8_t *style_slot;
 };
 
 struct FinalBuffers {
@@ -54,6 +58,7 @@ struct FinalBuffers {
     int64_t lighting_bytes = 0;
     int32_t nfaces = 0;
     std::vector<int32_t> lightofs;
+    std::vector<float4> h_frames;   // host copy of frames (its lightofs words change with the styles)
     FinalView view{};
     bool ready = false;
 

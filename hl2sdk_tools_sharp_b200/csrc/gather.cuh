@@ -103,7 +103,8 @@ __device__ __forceinline__ float4 gather_point(const DeviceScene &sc, const Devi
                                                float py, float pz, float nx, float ny, float nz, bool real,
                                                unsigned gmask, int filter, int *stack, uint32_t *overflow,
                                                unsigned long long *counters, unsigned long long &vis_rays,
-                                               unsigned long long &sky_rays, float4 *second = nullptr) {
+                                               unsigned long long &sky_rays, float4 *second = nullptr,
+                                               int face = 0, unsigned long long key_group = 0) {
     float ax = 0.0f, ay = 0.0f, az = 0.0f, sun = 0.0f;
     float hx = 0.0f, hy = 0.0f, hz = 0.0f;
 
@@ -113,6 +114,9 @@ __device__ __forceinline__ float4 gather_point(const DeviceScene &sc, const Devi
         const float4 *L = w.lights + kLightF4 * li;
         const float4 A = __ldg(L), B = __ldg(L + 1), C = __ldg(L + 2), D = __ldg(L + 3), E = __ldg(L + 4);
         const int type = __float_as_int(A.w);
+        // Each style's lights are gathered apart (its own slot); the test
+        // is warp-uniform.
+        if (__float_as_int(B.w) != w.style) continue;
         // The resampling passes gather the sky ambient and the other
         // lights apart (EmitResample); the filter is warp-uniform.
         if (filter == kAmbientOnly && type != kSkyAmbient) continue;
@@ -234,6 +238,11 @@ __device__ __forceinline__ float4 gather_point(const DeviceScene &sc, const Devi
         dot = maxps(dot, 0.0f);
         const float fx = __fmul_rn(real ? dot : 0.0f, falloff);
         if (!group_any(fx != 0.0f, gmask)) continue;
+        // ResolveGroup's FindOrAllocateStyle point: this group lights the
+        // face in this style; its first lane keeps the earliest (group,
+        // position in the light list) per face.
+        if (w.face_key && (threadIdx.x & 3) == 0)
+            atomicMin(&w.face_key[face], key_group | (unsigned long long)(k - l0));
         if (real) {
             ax = __fadd_rn(ax, __fmul_rn(fx, B.x));
             ay = __fadd_rn(ay, __fmul_rn(fx, B.y));

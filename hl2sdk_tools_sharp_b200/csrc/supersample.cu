@@ -89,6 +89,8 @@ __global__ void k_ss_select(int64_t n, FinalView fv, DeviceWorld w, const int32_
     if (i >= n || processed[i]) return;
     const int c = __ldg(&cell[i]);
     const int f = __ldg(&fv.cell_face[c]);
+    // A style that is not this face's has no supersampling state here.
+    if (w.face_slot && __ldg(&w.face_slot[f]) < 0) return;
     const int base = __ldg(&fv.face_cells[f]);
     const int wd = __float_as_int(__ldg(&fv.frames[5 * f].w)), ht = __float_as_int(__ldg(&fv.frames[5 * f + 1].w));
     const int s = (c - base) % wd, t = (c - base) / wd;

@@ -469,15 +469,23 @@ extern "C" int32_t vrad_build_neighbours(const vrad_face *faces, int32_t nfaces,
     return VRAD_OK;
 }
 
-// LightmapOffsets.Compute (MapTools/Rad/Light/LightmapOffsets.cs:54-126)
-// for faces lit in style 0 only (every lit face has style 0): four bytes of
-// median before each face's lightofs, then (w + 1) * (h + 1) luxels.
-extern "C" int32_t vrad_lightmap_layout(const vrad_face *faces, int32_t nfaces, int32_t *lightofs,
-                                        int64_t *total) {
+// LightmapOffsets.Compute (MapTools/Rad/Light/LightmapOffsets.cs:54-126):
+// per face its styles' four-byte medians before its lightofs, then each
+// style's (w + 1) * (h + 1) luxels.  styles (nullable): four bytes per face,
+// 255 ending the list; without it every face has style 0 alone.
+extern "C" int32_t vrad_lightmap_layout_styles(const vrad_face *faces, int32_t nfaces, const uint8_t *styles,
+                                               int32_t *lightofs, int64_t *total) {
     if (nfaces < 0 || (nfaces && !faces) || !lightofs || !total) return VRAD_ERR_ARG;
     int64_t size = 0;
     for (int32_t f = 0; f < nfaces; f++) {
-        const int lightstyles = 1;
+        int lightstyles = 1;
+        if (styles)
+            for (lightstyles = 0; lightstyles < 4 && styles[4 * (int64_t)f + lightstyles] != 255; lightstyles++) {
+            }
+        if (lightstyles == 0) {
+            lightofs[f] = -1;  // a face without styles gets no lightmap
+            continue;
+        }
         size += lightstyles * 4;
         lightofs[f] = (int32_t)size;
         const int64_t luxels = (int64_t)(faces[f].lightmap_size[0] + 1) * (faces[f].lightmap_size[1] + 1);
@@ -485,6 +493,11 @@ extern "C" int32_t vrad_lightmap_layout(const vrad_face *faces, int32_t nfaces, 
     }
     *total = size;
     return VRAD_OK;
+}
+
+extern "C" int32_t vrad_lightmap_layout(const vrad_face *faces, int32_t nfaces, int32_t *lightofs,
+                                        int64_t *total) {
+    return vrad_lightmap_layout_styles(faces, nfaces, nullptr, lightofs, total);
 }
 
 // ---- frames for the other translation units --------------------------------

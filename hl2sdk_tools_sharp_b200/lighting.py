@@ -122,6 +122,10 @@ def _lib():
         lib.vrad_lightmap_layout.restype = i32
         lib.vrad_lighting_size.argtypes = [P, ctypes.POINTER(i64)]
         lib.vrad_lighting_size.restype = i32
+        lib.vrad_lightmap_layout_styles.argtypes = [P, i32, P, P, ctypes.POINTER(i64)]
+        lib.vrad_lightmap_layout_styles.restype = i32
+        lib.vrad_face_styles.argtypes = [P, P, i32, ctypes.POINTER(i64)]
+        lib.vrad_face_styles.restype = i32
         lib.vrad_light_pass.argtypes = [P, P, i64, P, ctypes.POINTER(PassStats)]
         lib.vrad_light_pass.restype = i32
         lib.vrad_light_pass_device.argtypes = [P, P, P]
@@ -282,12 +286,18 @@ def build_neighbours(faces: np.ndarray, verts: np.ndarray, threshold: float = 0.
     return off, lst[:count.value]
 
 
-def lightmap_layout(faces: np.ndarray):
-    """vrad_lightmap_layout: (lightofs per face, LIGHTING size)."""
+def lightmap_layout(faces: np.ndarray, styles: np.ndarray | None = None):
+    """vrad_lightmap_layout: (lightofs per face, LIGHTING size); with styles
+    ((nfaces, 4) style bytes, 255 an empty slot), vrad_lightmap_layout_styles."""
     faces = np.ascontiguousarray(faces, FACE_DTYPE)
     ofs = np.zeros(len(faces), np.int32)
     total = ctypes.c_int64()
-    rc = _lib().vrad_lightmap_layout(faces.ctypes.data, len(faces), ofs.ctypes.data, ctypes.byref(total))
+    if styles is None:
+        rc = _lib().vrad_lightmap_layout(faces.ctypes.data, len(faces), ofs.ctypes.data, ctypes.byref(total))
+    else:
+        st = np.ascontiguousarray(styles, np.uint8).reshape(len(faces), 4)
+        rc = _lib().vrad_lightmap_layout_styles(faces.ctypes.data, len(faces), st.ctypes.data, ofs.ctypes.data,
+                                                ctypes.byref(total))
     if rc != 0:
         raise ValueError(f"vrad_lightmap_layout failed ({rc})")
     return ofs, total.value
@@ -463,6 +473,15 @@ class LightingStage:
         T._check(_lib().vrad_bounce_transfers(self._ctx, off.ctypes.data, n, tr.ctypes.data, len(tr),
                                               ctypes.byref(count)), self._ctx)
         return off, tr[:count.value]
+
+    def face_styles(self):
+        """vrad_face_styles: each face's four style bytes ((nfaces, 4) uint8,
+        255 an empty slot) and the number of faces that dropped a fifth style."""
+        n = len(self.inputs.faces)
+        out = np.zeros((n, 4), np.uint8)
+        dropped = ctypes.c_int64()
+        T._check(_lib().vrad_face_styles(self._ctx, out.ctypes.data, n, ctypes.byref(dropped)), self._ctx)
+        return out, dropped.value
 
     def close(self):
         self.tracer.close()

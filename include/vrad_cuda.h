@@ -308,6 +308,12 @@ int32_t vrad_build_neighbours(const vrad_face *faces, int32_t nfaces, const floa
  * for faces lit in style 0: each face's lightofs (its median's four bytes
  * sit just before it) and the LIGHTING lump's total size.  Host-side. */
 int32_t vrad_lightmap_layout(const vrad_face *faces, int32_t nfaces, int32_t *lightofs, int64_t *total);
+/* The layout with light styles: styles holds four bytes per face (its
+ * FaceLight.Styles, 255 ending the list; vrad_face_styles gives a lit
+ * world's); each face's style medians precede its lightofs, in reverse
+ * style order, and its styles' luxels follow it, style after style. */
+int32_t vrad_lightmap_layout_styles(const vrad_face *faces, int32_t nfaces, const uint8_t *styles,
+                                    int32_t *lightofs, int64_t *total);
 
 /* Uploads the lighting world to the context's device (kept until the next
  * upload or vrad_destroy).  The scene (vrad_scene_upload) is the shadow
@@ -353,6 +359,17 @@ typedef struct vrad_pass_stats {
 /* Size in bytes of the LIGHTING lump the uploaded world produces
  * (LightmapOffsets.Compute's LightDataSize). */
 int32_t vrad_lighting_size(vrad_ctx *ctx, int64_t *bytes);
+
+/* Light styles (FaceLight.Styles): lights of a style other than 0 light
+ * their own lightmap of the face.  A face holds style 0 in its first slot
+ * and up to three more styles, in the order its first sample groups light
+ * them (FaceLightJob.ResolveGroup's FindOrAllocateStyle); a fifth style is
+ * dropped from the face ("Too many light styles on a face").  The slots
+ * decide the layout: for a world with styled lights, vrad_lighting_size and
+ * the first light pass make them (each such style gathered once).
+ * vrad_face_styles gives each face's four style bytes (FACES' styles, 255 an
+ * empty slot; nfaces x 4) and the number of faces that dropped a style. */
+int32_t vrad_face_styles(vrad_ctx *ctx, uint8_t *styles, int32_t nfaces, int64_t *dropped);
 
 /* The lighting stage with -bounce 0 (the reference's Vrad.RunPassAsync
  * without the bounce, MapTools/Rad/Vrad.cs:392-530): the direct gather, then

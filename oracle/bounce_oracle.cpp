@@ -861,6 +861,11 @@ int orc_bounce_run(void *h, const float *sample_light, float *total_light, float
 
 int orc_bounce_final(void *h, const float *sample_light, uint8_t *lighting, int64_t capacity, int32_t *lightofs,
                      int64_t *total) {
+    return orc_bounce_final_styles(h, sample_light, nullptr, nullptr, lighting, capacity, lightofs, total);
+}
+
+int orc_bounce_final_styles(void *h, const float *sample_light, const float *slots_light, const uint8_t *face_styles,
+                            uint8_t *lighting, int64_t capacity, int32_t *lightofs, int64_t *total) {
     World &w = *static_cast<World *>(h);
     OrcBounced b;
     b.face_leaves.assign(w.faces.size(), {});
@@ -879,7 +884,8 @@ int orc_bounce_final(void *h, const float *sample_light, uint8_t *lighting, int6
             b.face_leaves[f].push_back(bp);
         }
     return orc_final_impl(w.faces.data(), (int32_t)w.faces.size(), w.verts.data(), w.samples.data(), w.face_first.data(),
-                          sample_light, lighting, capacity, lightofs, total, w.bounces > 0 ? &b : nullptr);
+                          sample_light, lighting, capacity, lightofs, total, w.bounces > 0 ? &b : nullptr,
+                          slots_light, face_styles);
 }
 
 int64_t orc_bounce_stats(void *h, int64_t *blocked) {

@@ -456,15 +456,17 @@ bool PointsInWinding(const F3 pts[4], const W &winding, int &invalidBits) {
 }
 
 // EmitResample + ResolveResample for one row of four points: the ambient
-// light alone or every other light, each added with AddLight (no skip).
+// light alone or every other light, of one style (FaceLightJob.cs:465-550),
+// each added with AddLight (no skip).
 void Resample(const Ctx &c, const F3 pts[4], F3 n, int cl, const int32_t *cl_off, const int32_t *cl_list,
-              bool ambientOnly, float result[4][4]) {
+              bool ambientOnly, int style, float result[4][4]) {
     std::memset(result, 0, sizeof(float) * 16);
     F3 nrm[4] = {n, n, n, n};
     for (int k = cl_off[cl]; k < cl_off[cl + 1]; k++) {
         const orc_light &L = c.lights[cl_list[k]];
         if (ambientOnly && L.type != 4) continue;
         if (!ambientOnly && L.type == 4) continue;
+        if (L.style != style) continue;
         Out4 o;
         gather(c, L, pts, nrm, 4, o);
         for (int l = 0; l < 4; l++) {
@@ -477,10 +479,11 @@ void Resample(const Ctx &c, const F3 pts[4], F3 n, int cl, const int32_t *cl_off
     }
 }
 
-// The supersampling passes of one face (FaceLightJob.AdvanceAfterRound and
-// StyleSupersample), over its samples' light (4 floats each).
+// The supersampling passes of one style slot of one face
+// (FaceLightJob.AdvanceAfterRound and StyleSupersample), over its samples'
+// light in that slot (4 floats each).
 int64_t Supersample(const Ctx &c, const orc_face &f, const orc_sample *samples, int64_t nsamp, const std::vector<W> &wind,
-                    const int32_t *cl_off, const int32_t *cl_list, int extra_passes, float *light) {
+                    const int32_t *cl_off, const int32_t *cl_list, int extra_passes, int style, float *light) {
     const Info in = face_info(f);
     const int w = in.width, h = in.height, size = w * h;
     std::vector<float> inten((size_t)size, 0.0f);
@@ -581,7 +584,7 @@ int64_t Supersample(const Ctx &c, const orc_face &f, const orc_sample *samples, 
                     F3 pts[4];
                     for (int l = 0; l < 4; l++) pts[l] = pos[l] + n;
                     float res[4][4];
-                    Resample(c, pts, n, f.cluster, cl_off, cl_list, ambientOnly, res);
+                    Resample(c, pts, n, f.cluster, cl_off, cl_list, ambientOnly, style, res);
                     float *acc = ambientOnly ? amb : dir;
                     int &cnt = ambientOnly ? ac : dc;
                     for (int l = 0; l < 4; l++) {
@@ -614,15 +617,39 @@ int64_t Supersample(const Ctx &c, const orc_face &f, const orc_sample *samples, 
     return done;
 }
 
+// FaceLight.FindOrAllocateStyle (FaceLight.cs:200-223): the slot holding
+// `style`, a free slot taken for it, or -1 when all four are taken.
+int FindOrAllocateStyle(uint8_t styles[4], int style) {
+    for (int k = 0; k < 4; k++) {
+        if (styles[k] == style) return k;
+        if (styles[k] == 255) {
+            styles[k] = (uint8_t)style;
+            return k;
+        }
+    }
+    return -1;
+}
+
 }  // namespace
 
-extern "C" int orc_direct(const orc_kdnode *nodes, const int32_t *indices, const orc_tri *tris,
-                          const float *bounds6, const orc_face *faces, int32_t nfaces, const float *verts,
-                          const orc_sample *samples, const int64_t *face_first, const orc_light *lights,
-                          const int32_t *cl_off, const int32_t *cl_list, const float *dirs, int32_t ndirs,
-                          const float *jitter, int32_t sun_samples, float sun_extent, int32_t extra_passes,
-                          float *out, int32_t threads, int64_t *rays_out, int64_t *supersampled_out) {
-    std::atomic<int64_t> rays(0), supersampled(0);
+// The direct gather with light styles: per face, style 0 in slot 0 from the
+// start (FaceLightJob.cs:184-186), every other style given the next free
+// slot by the first four-sample group it lights (ResolveGroup,
+// FaceLightJob.cs:399-455; a fifth style is warned and dropped), then the
+// supersampling passes of each slot with that style's lights alone.
+// out: slot 0 (4 floats per sample); out_slots (nullable): slots 1..3, each
+// nsamples x 4 floats, zero where the slot is not the face's;
+// face_styles (nullable): 4 bytes per face (255: no style); dropped
+// (nullable): faces warned of a fifth style.
+extern "C" int orc_direct_styles(const orc_kdnode *nodes, const int32_t *indices, const orc_tri *tris,
+                                 const float *bounds6, const orc_face *faces, int32_t nfaces, const float *verts,
+                                 const orc_sample *samples, const int64_t *face_first, const orc_light *lights,
+                                 const int32_t *cl_off, const int32_t *cl_list, const float *dirs, int32_t ndirs,
+                                 const float *jitter, int32_t sun_samples, float sun_extent, int32_t extra_passes,
+                                 float *out, float *out_slots, uint8_t *face_styles, int64_t *dropped,
+                                 int32_t threads, int64_t *rays_out, int64_t *supersampled_out) {
+    std::atomic<int64_t> rays(0), supersampled(0), warned(0);
+    const int64_t nsamples = face_first[nfaces];
     std::atomic<bool> mismatch(false);
     Ctx c;
     c.kd = OrcKd{nodes, indices, tris, {bounds6[0], bounds6[1], bounds6[2], bounds6[3], bounds6[4], bounds6[5]}};
@@ -638,6 +665,13 @@ extern "C" int orc_direct(const orc_kdnode *nodes, const int32_t *indices, const
             const int64_t a = face_first[fi], b = face_first[fi + 1];
             const F3 n = {faces[fi].normal[0], faces[fi].normal[1], faces[fi].normal[2]};
             const int cl = faces[fi].cluster;
+            uint8_t st[4] = {0, 255, 255, 255};
+            bool warn = false;
+            // The face's light per slot (slot 0 in out); zero until a slot is taken.
+            std::vector<float> mine_slots((size_t)(3 * 4 * (b - a)), 0.0f);
+            auto slot_light = [&](int k, int64_t i) {
+                return k == 0 ? out + 4 * i : mine_slots.data() + 4 * ((k - 1) * (b - a) + (i - a));
+            };
             for (int64_t g = a; g < b; g += 4) {
                 int count = (int)((b - g) < 4 ? (b - g) : 4);
                 F3 pts[4], nrm[4];
@@ -646,7 +680,7 @@ extern "C" int orc_direct(const orc_kdnode *nodes, const int32_t *indices, const
                     pts[l] = F3{s.position[0], s.position[1], s.position[2]} + n;
                     nrm[l] = n;
                 }
-                float acc[4][4];
+                float acc[4][4][4];
                 std::memset(acc, 0, sizeof acc);
                 for (int k = cl_off[cl]; k < cl_off[cl + 1]; k++) {
                     const orc_light &L = lights[cl_list[k]];
@@ -660,15 +694,28 @@ extern "C" int orc_direct(const orc_kdnode *nodes, const int32_t *indices, const
                         skip &= fx[l] == 0.0f;
                     }
                     if (skip) continue;
+                    const int slot = FindOrAllocateStyle(st, L.style);
+                    if (slot < 0) {
+                        warn = true;
+                        continue;
+                    }
                     for (int l = 0; l < count; l++) {
-                        acc[l][0] = acc[l][0] + (fx[l] * L.intensity[0]);
-                        acc[l][1] = acc[l][1] + (fx[l] * L.intensity[1]);
-                        acc[l][2] = acc[l][2] + (fx[l] * L.intensity[2]);
-                        acc[l][3] += o.sun[l];
+                        acc[slot][l][0] = acc[slot][l][0] + (fx[l] * L.intensity[0]);
+                        acc[slot][l][1] = acc[slot][l][1] + (fx[l] * L.intensity[1]);
+                        acc[slot][l][2] = acc[slot][l][2] + (fx[l] * L.intensity[2]);
+                        acc[slot][l][3] += o.sun[l];
                     }
                 }
-                for (int l = 0; l < count; l++) std::memcpy(out + 4 * (g + l), acc[l], 16);
+                for (int k = 0; k < 4; k++)
+                    for (int l = 0; l < count; l++) std::memcpy(slot_light(k, g + l), acc[k][l], 16);
             }
+            if (warn) warned++;
+            if (face_styles) std::memcpy(face_styles + 4 * (int64_t)fi, st, 4);
+            auto keep_slots = [&]() {
+                if (!out_slots) return;
+                for (int k = 1; k < 4; k++)
+                    std::memcpy(out_slots + 4 * ((k - 1) * nsamples + a), slot_light(k, a), sizeof(float) * 4 * (b - a));
+            };
             if (extra_passes > 0 && b > a) {
                 // The face's own samples and their windings (the caller's
                 // samples must be the builder's: checked, not assumed).
@@ -683,11 +730,14 @@ extern "C" int orc_direct(const orc_kdnode *nodes, const int32_t *indices, const
                 }
                 if (!same) {
                     mismatch = true;
+                    keep_slots();
                     continue;
                 }
-                supersampled += Supersample(c, faces[fi], samples + a, b - a, wind, cl_off, cl_list, extra_passes,
-                                            out + 4 * a);
+                for (int k = 0; k < 4 && st[k] != 255; k++)
+                    supersampled += Supersample(c, faces[fi], samples + a, b - a, wind, cl_off, cl_list, extra_passes,
+                                                st[k], slot_light(k, a));
             }
+            keep_slots();
         }
         rays += t_rays;
     };
@@ -709,7 +759,21 @@ extern "C" int orc_direct(const orc_kdnode *nodes, const int32_t *indices, const
     }
     if (rays_out) *rays_out = rays.load();
     if (supersampled_out) *supersampled_out = supersampled.load();
+    if (dropped) *dropped = warned.load();
     return mismatch ? -2 : 0;
+}
+
+// The gather's slot 0 alone (every light of the maps this was first written
+// for is style 0).
+extern "C" int orc_direct(const orc_kdnode *nodes, const int32_t *indices, const orc_tri *tris,
+                          const float *bounds6, const orc_face *faces, int32_t nfaces, const float *verts,
+                          const orc_sample *samples, const int64_t *face_first, const orc_light *lights,
+                          const int32_t *cl_off, const int32_t *cl_list, const float *dirs, int32_t ndirs,
+                          const float *jitter, int32_t sun_samples, float sun_extent, int32_t extra_passes,
+                          float *out, int32_t threads, int64_t *rays_out, int64_t *supersampled_out) {
+    return orc_direct_styles(nodes, indices, tris, bounds6, faces, nfaces, verts, samples, face_first, lights,
+                             cl_off, cl_list, dirs, ndirs, jitter, sun_samples, sun_extent, extra_passes, out,
+                             nullptr, nullptr, nullptr, threads, rays_out, supersampled_out);
 }
 
 // DetMathF.Pow as the oracle computes it (the spotlight cone's power).

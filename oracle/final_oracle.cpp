@@ -238,14 +238,31 @@ extern "C" int orc_neighbours(const orc_face *faces, int32_t nfaces, const float
 
 int orc_final_impl(const orc_face *faces, int32_t nfaces, const float *verts, const orc_sample *samples,
                    const int64_t *face_first, const float *sample_light, uint8_t *lighting, int64_t capacity,
-                   int32_t *lightofs, int64_t *total, const OrcBounced *bounced) {
-    // LightmapOffsets.Compute: style 0 on every lit face.
+                   int32_t *lightofs, int64_t *total, const OrcBounced *bounced, const float *slots_light,
+                   const uint8_t *face_styles) {
+    // Each face's styles (FaceLight.Styles; style 0 alone without a table)
+    // and a sample's light in one slot (slot 0 in sample_light, slots 1..3
+    // in slots_light).
+    const int64_t nsamples = face_first[nfaces];
+    static const uint8_t kStyle0[4] = {0, 255, 255, 255};
+    auto styles_of = [&](int f) { return face_styles ? face_styles + 4 * (int64_t)f : kStyle0; };
+    auto light_of = [&](int k, int64_t i) {
+        return k == 0 ? sample_light + 4 * i : slots_light + 4 * ((k - 1) * nsamples + i);
+    };
+    auto nstyles = [&](int f) {
+        int n = 0;
+        while (n < 4 && styles_of(f)[n] != 255) n++;
+        return n;
+    };
+    // LightmapOffsets.Compute (LightmapOffsets.cs:84-123): per lit face its
+    // styles' four-byte averages, then each style's luxels.
     int64_t size = 0;
     std::vector<int32_t> ofs((size_t)nfaces);
     for (int f = 0; f < nfaces; f++) {
-        size += 4;
+        const int ls = nstyles(f);
+        size += 4 * ls;
         ofs[(size_t)f] = (int32_t)size;
-        size += (int64_t)(faces[f].size[0] + 1) * (faces[f].size[1] + 1) * 4;
+        size += (int64_t)(faces[f].size[0] + 1) * (faces[f].size[1] + 1) * 4 * ls;
     }
     *total = size;
     if (lightofs) std::memcpy(lightofs, ofs.data(), sizeof(int32_t) * (size_t)nfaces);
@@ -261,17 +278,24 @@ int orc_final_impl(const orc_face *faces, int32_t nfaces, const float *verts, co
     for (int f = 0; f < nfaces; f++) frames[(size_t)f] = frame(faces[f]);
     Radial rad, prad;
     std::vector<float> red, green, blue;
-    for (int f = 0; f < nfaces; f++) {
+    for (int f = 0; f < nfaces; f++)
+    for (int slot = 0; slot < nstyles(f); slot++) {
         const Frame &fr = frames[(size_t)f];
         rad.reset(fr);
-        // BuildLuxelRadial: own samples, then each neighbour's, in order.
+        // BuildLuxelRadial: own samples of this slot, then each neighbour's
+        // samples of the same style NUMBER, in order; a neighbour without
+        // that style adds nothing (FinalLightFace.cs:339-380).
         for (int64_t k = face_first[f]; k < face_first[f + 1]; k++) {
             const orc_sample &sm = samples[k];
             rad.add_direct({sm.position[0], sm.position[1], sm.position[2]}, sm.mins[0], sm.mins[1], sm.maxs[0],
-                           sm.maxs[1], sample_light + 4 * k);
+                           sm.maxs[1], light_of(slot, k));
         }
+        const uint8_t wanted = styles_of(f)[slot];
         for (int q = noff[(size_t)f]; q < noff[(size_t)f + 1]; q++) {
             const int g = nlist[(size_t)q];
+            int ns = 0;
+            while (ns < 4 && styles_of(g)[ns] != wanted) ns++;
+            if (ns >= 4) continue;
             const Frame &l = frames[(size_t)g];
             for (int64_t k = face_first[g]; k < face_first[g + 1]; k++) {
                 const orc_sample &sm = samples[k];
@@ -279,12 +303,14 @@ int orc_final_impl(const orc_face *faces, int32_t nfaces, const float *verts, co
                 w2l(fr, l2w(l, sm.mins[0], sm.mins[1]), mins, mint);
                 w2l(fr, l2w(l, sm.maxs[0], sm.maxs[1]), maxs, maxt);
                 rad.add_direct({sm.position[0], sm.position[1], sm.position[2]}, mins, mint, maxs, maxt,
-                               sample_light + 4 * k);
+                               light_of(ns, k));
             }
         }
-        // BuildPatchRadial: the leaf patches of the face, then of each
-        // neighbour (AddFacePatches), splatted with their bounced light.
-        if (bounced) {
+        // BuildPatchRadial (style 0 only): the leaf patches of the face,
+        // then of each neighbour (AddFacePatches), splatted with their
+        // bounced light.
+        const bool bounce_here = bounced && slot == 0;
+        if (bounce_here) {
             prad.reset(fr);
             std::vector<int> order = {f};
             for (int q = noff[(size_t)f]; q < noff[(size_t)f + 1]; q++) order.push_back(nlist[(size_t)q]);
@@ -313,7 +339,7 @@ int orc_final_impl(const orc_face *faces, int32_t nfaces, const float *verts, co
             const int s = j % fr.w, t = j / fr.w;
             float lb[3];
             bool ok = rad.sample(l2w(fr, (float)s, (float)t), lb);
-            if (bounced) {
+            if (bounce_here) {
                 float v[3];
                 (void)prad.sample(l2w(fr, (float)s, (float)t), v);
                 for (int c = 0; c < 3; c++) lb[c] = lb[c] + v[c];
@@ -330,7 +356,7 @@ int orc_final_impl(const orc_face *faces, int32_t nfaces, const float *verts, co
                 blue.push_back(lb[2]);
             }
             uint32_t w = encode(lb[0], lb[1], lb[2]);
-            std::memcpy(lighting + ofs[(size_t)f] + 4 * j, &w, 4);
+            std::memcpy(lighting + ofs[(size_t)f] + 4 * ((int64_t)slot * n + j), &w, 4);
         }
         float med[3] = {0.0f, 0.0f, 0.0f};
         if (!red.empty()) {
@@ -341,10 +367,21 @@ int orc_final_impl(const orc_face *faces, int32_t nfaces, const float *verts, co
             med[1] = green[green.size() >> 1];
             med[2] = blue[blue.size() >> 1];
         }
+        // Before lightofs, in reverse style order.
         uint32_t w = encode(med[0], med[1], med[2]);
-        std::memcpy(lighting + ofs[(size_t)f] - 4, &w, 4);
+        std::memcpy(lighting + ofs[(size_t)f] - 4 * (slot + 1), &w, 4);
     }
     return 0;
+}
+
+// The final pass of a map with light styles: slots_light holds slots 1..3
+// (nsamples x 4 floats each), face_styles 4 bytes per face.
+extern "C" int orc_final_styles(const orc_face *faces, int32_t nfaces, const float *verts, const orc_sample *samples,
+                                const int64_t *face_first, const float *sample_light, const float *slots_light,
+                                const uint8_t *face_styles, uint8_t *lighting, int64_t capacity, int32_t *lightofs,
+                                int64_t *total) {
+    return orc_final_impl(faces, nfaces, verts, samples, face_first, sample_light, lighting, capacity, lightofs,
+                          total, nullptr, slots_light, face_styles);
 }
 
 extern "C" int orc_final(const orc_face *faces, int32_t nfaces, const float *verts, const orc_sample *samples,

@@ -65,6 +65,11 @@ def lib() -> ctypes.CDLL:
         _lib.orc_neighbours.restype = ctypes.c_int
         _lib.orc_final.argtypes = [P, i32, P, P, P, P, P, ctypes.c_int64, P, P]
         _lib.orc_final.restype = ctypes.c_int
+        _lib.orc_direct_styles.argtypes = [P, P, P, P, P, i32, P, P, P, P, P, P, P, i32, P, i32, f32, i32, P, P, P,
+                                           P, i32, P, P]
+        _lib.orc_direct_styles.restype = ctypes.c_int
+        _lib.orc_final_styles.argtypes = [P, i32, P, P, P, P, P, P, P, ctypes.c_int64, P, P]
+        _lib.orc_final_styles.restype = ctypes.c_int
         if hasattr(_lib, "orc_kd_build"):
             _lib.orc_kd_build.argtypes = [P, P, P, i32, P]
             _lib.orc_kd_build.restype = ctypes.c_int
@@ -463,6 +468,60 @@ def direct(tree: dict, faces, samples, face_first, lights, cl_off, cl_list, dirs
     return (out, rays.value) if count_rays else out
 
 
+def direct_styles(tree, faces, samples, face_first, lights, cl_off, cl_list, dirs, jitter=None, sun_samples: int = 1,
+                  sun_extent: float = 0.0, threads: int | None = None, verts=None, extra_passes: int = 4):
+    """The direct gather with light styles (FaceLightJob's slots): (slot 0
+    (nsamples, 4), slots 1..3 (3, nsamples, 4), face styles (nfaces, 4)
+    uint8 with 255 for an empty slot, faces warned of a fifth style)."""
+    nodes = np.ascontiguousarray(tree["nodes"], dtype=NODE_DTYPE)
+    idx = np.ascontiguousarray(tree["indices"], dtype=np.int32)
+    tris = np.ascontiguousarray(tree["tris"], dtype=TRI_DTYPE)
+    bounds = np.ascontiguousarray(tree["bounds"], dtype=np.float32)
+    faces = np.ascontiguousarray(faces)
+    samples = np.ascontiguousarray(samples)
+    face_first = np.ascontiguousarray(face_first, np.int64)
+    lights = np.ascontiguousarray(lights)
+    cl_off = np.ascontiguousarray(cl_off, np.int32)
+    cl_list = np.ascontiguousarray(cl_list, np.int32)
+    dirs = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+    jit = np.ascontiguousarray(jitter if jitter is not None and len(jitter) else np.zeros((1, 3)), np.float32)
+    vv = None if verts is None else np.ascontiguousarray(verts, np.float32)
+    n = int(face_first[-1])
+    out = np.zeros((n, 4), np.float32)
+    slots = np.zeros((3, n, 4), np.float32)
+    styles = np.zeros((len(faces), 4), np.uint8)
+    dropped, rays, ss = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+    rc = lib().orc_direct_styles(_p(nodes), _p(idx), _p(tris), _p(bounds), _p(faces), len(faces), _p(vv),
+                                 _p(samples), _p(face_first), _p(lights), _p(cl_off), _p(cl_list), _p(dirs), len(dirs),
+                                 _p(jit), sun_samples, sun_extent, extra_passes if vv is not None else 0, _p(out),
+                                 _p(slots), _p(styles), ctypes.byref(dropped),
+                                 threads if threads is not None else default_threads(), ctypes.byref(rays),
+                                 ctypes.byref(ss))
+    if rc != 0:
+        raise RuntimeError(f"orc_direct_styles failed: {rc}")
+    return out, slots, styles, dropped.value
+
+
+def final_styles(faces, verts, samples, face_first, sample_light, slots_light, face_styles):
+    """FinalLightFace restated with light styles: (LIGHTING bytes, lightofs)."""
+    faces = np.ascontiguousarray(faces)
+    verts = np.ascontiguousarray(verts, np.float32)
+    samples = np.ascontiguousarray(samples)
+    face_first = np.ascontiguousarray(face_first, np.int64)
+    light = np.ascontiguousarray(sample_light, np.float32).reshape(-1, 4)
+    slots = np.ascontiguousarray(slots_light, np.float32).reshape(3, -1, 4)
+    styles = np.ascontiguousarray(face_styles, np.uint8).reshape(-1, 4)
+    total = ctypes.c_int64()
+    ofs = np.zeros(len(faces), np.int32)
+    args = (_p(faces), len(faces), _p(verts), _p(samples), _p(face_first), _p(light), _p(slots), _p(styles))
+    lib().orc_final_styles(*args, None, 0, _p(ofs), ctypes.byref(total))
+    out = np.zeros(total.value, np.uint8)
+    rc = lib().orc_final_styles(*args, _p(out), len(out), _p(ofs), ctypes.byref(total))
+    if rc != 0:
+        raise RuntimeError(f"orc_final_styles failed: {rc}")
+    return out, ofs
+
+
 def neighbours(faces, verts, threshold: float = 0.7071067):
     faces = np.ascontiguousarray(faces)
     verts = np.ascontiguousarray(verts, np.float32)
@@ -530,6 +589,7 @@ def _bounce_lib():
         L.orc_bounce_set_transfers.argtypes = [P, P, P, P]
         L.orc_bounce_run.argtypes = [P, P, P, P, P, P]
         L.orc_bounce_final.argtypes = [P, P, P, i64, P, P]
+        L.orc_bounce_final_styles.argtypes = [P, P, P, P, P, i64, P, P]
         L.orc_bounce_stats.argtypes = [P, P]
         L.orc_bounce_stats.restype = i64
         L.orc_bounce_forget_transfers.argtypes = [P]
@@ -659,16 +719,21 @@ class Bounce:
             raise RuntimeError(f"orc_bounce_run failed: {rc}")
         return total, direct, n.value, added
 
-    def final(self, sample_light):
-        """FinalLightFace with the last run's bounced light: (LIGHTING, lightofs)."""
+    def final(self, sample_light, slots_light=None, face_styles=None):
+        """FinalLightFace with the last run's bounced light: (LIGHTING, lightofs).
+        With light styles, slots 1..3 and the faces' style bytes as
+        direct_styles returns them (the bounce goes into slot 0)."""
         L = _bounce_lib()
         light = np.ascontiguousarray(sample_light, np.float32).reshape(-1, 4)
+        slots = None if slots_light is None else np.ascontiguousarray(slots_light, np.float32).reshape(3, -1, 4)
+        styles = None if face_styles is None else np.ascontiguousarray(face_styles, np.uint8).reshape(-1, 4)
         total = ctypes.c_int64()
         nf = len(self._keep["faces"])
         ofs = np.zeros(nf, np.int32)
-        L.orc_bounce_final(self._h, _p(light), None, 0, _p(ofs), ctypes.byref(total))
+        L.orc_bounce_final_styles(self._h, _p(light), _p(slots), _p(styles), None, 0, _p(ofs), ctypes.byref(total))
         out = np.zeros(total.value, np.uint8)
-        rc = L.orc_bounce_final(self._h, _p(light), _p(out), len(out), _p(ofs), ctypes.byref(total))
+        rc = L.orc_bounce_final_styles(self._h, _p(light), _p(slots), _p(styles), _p(out), len(out), _p(ofs),
+                                       ctypes.byref(total))
         if rc != 0:
             raise RuntimeError(f"orc_bounce_final failed: {rc}")
         return out, ofs

@@ -31,4 +31,5 @@ struct OrcBounced {
 // FinalLightFace over every face; bounced = nullptr for -bounce 0.
 int orc_final_impl(const orc_face *faces, int32_t nfaces, const float *verts, const orc_sample *samples,
                    const int64_t *face_first, const float *sample_light, uint8_t *lighting, int64_t capacity,
-                   int32_t *lightofs, int64_t *total, const OrcBounced *bounced);
+                   int32_t *lightofs, int64_t *total, const OrcBounced *bounced,
+                   const float *slots_light = nullptr, const uint8_t *face_styles = nullptr);

@@ -151,6 +151,18 @@ int orc_direct(const orc_kdnode *nodes, const int32_t *indices, const orc_tri *t
                const float *jitter, int32_t sun_samples, float sun_extent, int32_t extra_passes,
                float *out, int32_t threads, int64_t *rays_out, int64_t *supersampled_out);
 
+/* orc_direct with light styles: out is slot 0; out_slots (nullable) slots
+ * 1..3 (each nsamples x 4 floats, zero where the face has no such slot);
+ * face_styles (nullable) 4 bytes per face, 255 for an empty slot; dropped
+ * (nullable) the faces warned of a fifth style. */
+int orc_direct_styles(const orc_kdnode *nodes, const int32_t *indices, const orc_tri *tris,
+                      const float *bounds6, const orc_face *faces, int32_t nfaces, const float *verts,
+                      const orc_sample *samples, const int64_t *face_first, const orc_light *lights,
+                      const int32_t *cl_off, const int32_t *cl_list, const float *dirs, int32_t ndirs,
+                      const float *jitter, int32_t sun_samples, float sun_extent, int32_t extra_passes,
+                      float *out, float *out_slots, uint8_t *face_styles, int64_t *dropped, int32_t threads,
+                      int64_t *rays_out, int64_t *supersampled_out);
+
 /* FaceNeighbours.Build for smoothing groups 0 (vertices welded by position). */
 int orc_neighbours(const orc_face *faces, int32_t nfaces, const float *verts, float threshold,
                    int32_t *offsets, int32_t *list, int64_t capacity, int64_t *count);
@@ -234,6 +246,15 @@ int orc_bounce_run(void *h, const float *sample_light, float *total_light, float
                    int32_t *bounces_run, float *added);
 /* FinalLightFace for every face with the bounced light of the last run. */
 int orc_bounce_final(void *h, const float *sample_light, uint8_t *lighting, int64_t capacity, int32_t *lightofs,
+                     int64_t *total);
+/* orc_bounce_final with light styles (slots 1..3 and 4 style bytes per
+ * face, as orc_direct_styles gives them); the bounce goes into slot 0. */
+int orc_bounce_final_styles(void *h, const float *sample_light, const float *slots_light, const uint8_t *face_styles,
+                            uint8_t *lighting, int64_t capacity, int32_t *lightofs, int64_t *total);
+/* orc_final with light styles. */
+int orc_final_styles(const orc_face *faces, int32_t nfaces, const float *verts, const orc_sample *samples,
+                     const int64_t *face_first, const float *sample_light, const float *slots_light,
+                     const uint8_t *face_styles, uint8_t *lighting, int64_t capacity, int32_t *lightofs,
                      int64_t *total);
 /* Rays traced so far; *blocked of them blocked. */
 int64_t orc_bounce_stats(void *h, int64_t *blocked);

@@ -158,14 +158,12 @@ def test_supersampling_refuses_samples_not_the_builders(change):
         st.direct()
 
 
-def test_a_styled_light_is_refused():
-    """Light styles above 0 need their own lightmap slots
-    (FaceLight.FindOrAllocateStyle, Rad/Light/FaceLightJob.cs:435-445),
-    which this build does not make: the world upload refuses such a light
-    instead of lighting it into style 0."""
+def test_a_style_outside_a_byte_is_refused():
+    """A face's style slots are bytes and 255 marks an empty one
+    (FaceLight.Styles), so a light's style must lie in 0..254."""
     w = rg.generate(rg.config_3x3(seed=2))
     inp = L.prepare(w)
     lights = inp.lights.copy()
-    lights["style"][len(lights) // 2] = 5
-    with pytest.raises(NotImplementedError, match="style 5"):
+    lights["style"][len(lights) // 2] = 255
+    with pytest.raises(ValueError, match="style 255"):
         L.LightingStage(w, L.LightingInputs(**{**inp.__dict__, "lights": lights}))
