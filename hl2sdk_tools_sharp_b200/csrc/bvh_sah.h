@@ -1,5 +1,5 @@
 // bvh_sah.h -- the scene BVH's topology, built on the host by the surface
-// area heuristic over the triangles' padded boxes (bvh_sah.cpp).
+// area heuristic over the triangles' padded boxes (bvh_sah.cu).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -23,6 +23,8 @@ struct SahTree {
 // hi xyz).  The root is always an inner node; leaves hold at most kMaxLeaf
 // triangles; the depth stays within kStackDepth (ranges that would go
 // deeper are split at their median).
-void build_sah(const float *box, int32_t n, SahTree &out);
+// parallel: the subtrees below the top few splits are built on the host's
+// threads; the tree is the same either way.
+void build_sah(const float *box, int32_t n, SahTree &out, bool parallel = true);
 
 }  // namespace vrad
