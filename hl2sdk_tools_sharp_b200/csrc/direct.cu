@@ -168,9 +168,7 @@ extern "C" int32_t vrad_world_upload(vrad_ctx *ctx, const vrad_world_desc *w) {
     const int32_t nl = w->nlights;
     for (int32_t l = 0; l < nl; l++) {
         const int t = w->lights[l].type;
-        if (t == 0)
-            return vrad_fail(ctx, VRAD_ERR_UNSUPPORTED, "surface lights are not supported by this build");
-        if (t < 1 || t > 4) return vrad_fail(ctx, VRAD_ERR_ARG, "light %d has type %d", l, t);
+        if (t < 0 || t > 4) return vrad_fail(ctx, VRAD_ERR_ARG, "light %d has type %d", l, t);
         // A face's style slots are bytes, 255 meaning none.
         if (w->lights[l].style < 0 || w->lights[l].style > 254)
             return vrad_fail(ctx, VRAD_ERR_ARG, "light %d has style %d (0 to 254)", l, w->lights[l].style);

@@ -34,6 +34,8 @@ constexpr float kMaxTraceLength = (float)(1.732050807569 * (2 * 16384));  // Lig
 constexpr float kEqualEpsilon = 0.001f;                                   // LightConstants.EqualEpsilon
 
 enum : int { kSurface = 0, kPoint = 1, kSpot = 2, kSkyLight = 3, kSkyAmbient = 4 };
+// LightConstants.DistEpsilon: how far a surface light's rays end off its patch.
+constexpr float kDistEpsilon = 0.03125f;
 
 // The any-hit walks' child order for the gather's segments: the farther
 // child first (measured faster for these rays than nearest first).
@@ -166,6 +168,37 @@ __device__ __forceinline__ float4 gather_point(const DeviceScene &sc, const Devi
             if (real && dot != 0.0f && falloff != 0.0f) {
                 vis_rays++;
                 if (segment_blocked<kModeAny, BLOCK, kFarPoint>(sc, px, py, pz, A.x, A.y, A.z, stack, overflow)) dot = 0.0f;
+            }
+        } else if (type == kSurface) {
+            // GatherSurfaceFour (DirectLightGatherer.cs:1452-1545): the
+            // patch's cosine over the squared distance, the segment to the
+            // patch origin pushed off the emitter by DistEpsilon.
+            const bool hard = E.z > E.y;
+            float dx = __fsub_rn(A.x, px), dy = __fsub_rn(A.y, py), dz = __fsub_rn(A.z, pz);
+            const float dist2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+            float dist = __fsqrt_rn(dist2);
+            const float rpc = __fdiv_rn(1.0f, dist);
+            dx = __fmul_rn(dx, rpc);
+            dy = __fmul_rn(dy, rpc);
+            dz = __fmul_rn(dz, rpc);
+            float d = __fadd_rn(__fadd_rn(__fmul_rn(dx, nx), __fmul_rn(dy, ny)), __fmul_rn(dz, nz));
+            d = maxps(0.0f, d);
+            bool live = !hard || dist <= E.z;
+            dist = maxps(dist, 1.0f);
+            // The negation flips the sign bit (a -0 survives maxps).
+            float dot2 = -__fadd_rn(__fadd_rn(__fmul_rn(dx, C.x), __fmul_rn(dy, C.y)), __fmul_rn(dz, C.z));
+            dot2 = maxps(0.0f, dot2);
+            live = live && !(d == 0.0f);
+            float f = __fdiv_rn(dot2, dist2);
+            if (hard) f = __fmul_rn(fade(dist, E.y, __fsub_rn(E.z, E.y)), f);
+            dot = live ? d : 0.0f;
+            falloff = live ? f : 0.0f;
+            if (real && dot != 0.0f && falloff != 0.0f) {
+                vis_rays++;
+                const float ex = __fadd_rn(A.x, __fmul_rn(C.x, kDistEpsilon)),
+                            ey = __fadd_rn(A.y, __fmul_rn(C.y, kDistEpsilon)),
+                            ez = __fadd_rn(A.z, __fmul_rn(C.z, kDistEpsilon));
+                if (segment_blocked<kModeAny, BLOCK, kFarPoint>(sc, px, py, pz, ex, ey, ez, stack, overflow)) dot = 0.0f;
             }
         } else if (type == kSkyLight) {
             // EmitSkyLight / ResolveSkyLight.

@@ -113,9 +113,11 @@ struct Builder {
         bounds(w, mn, mx);
         ch.mins[0] = mn.x, ch.mins[1] = mn.y, ch.mins[2] = mn.z;
         ch.maxs[0] = mx.x, ch.maxs[1] = mx.y, ch.maxs[2] = mx.z;
-        // No surface lights here (base light zero), so the face-edge rule
-        // applies: a child already under chop on every axis that touches
-        // the face's bounds has its chop halved once.
+        // A surface light's patches are never refined by the face-edge
+        // rule (PatchSubdivider.cs:375-380).  Otherwise a child already
+        // under chop on every axis that touches the face's bounds has its
+        // chop halved once.
+        if (faces[ch.face].flags & VRAD_FACE_EMITS) return add_patch(ch, w);
         const V3 total = mul(sub(mx, mn), ch.lux_scale);
         if (ch.chop > min_chop && total.x < ch.chop && total.y < ch.chop && total.z < ch.chop) {
             for (int i = 0; i < 3; i++) {

@@ -59,6 +59,7 @@ assert FACE_DTYPE.itemsize == 80 and SAMPLE_DTYPE.itemsize == 56 and LIGHT_DTYPE
 assert PATCH_DTYPE.itemsize == 144 and TRANSFER_DTYPE.itemsize == 8
 
 EMIT_POINT, EMIT_SPOT, EMIT_SKY, EMIT_AMBIENT = 1, 2, 3, 4
+SURF_LIGHT, FACE_EMITS = 0x0001, 0x40000000     # VRAD_SURF_LIGHT, VRAD_FACE_EMITS
 EQUAL_EPSILON = np.float32(0.001)
 
 
@@ -183,6 +184,11 @@ def faces_of(world: World):
     faces["first_vertex"] = first
     faces["num_vertices"] = counts
     faces["cluster"] = world.face_cluster
+    if world.face_emit is not None:
+        # An emitting texture: SURF_LIGHT (PatchBuilder.MakePatchForFace)
+        # and the library's emitting-face bit.
+        emits = world.face_emit[:, 3] > 0
+        faces["flags"][emits] |= SURF_LIGHT | FACE_EMITS
     verts = np.concatenate(world.face_verts).astype(np.float32)
     return faces, verts
 
@@ -313,9 +319,31 @@ def parse_intensity(color, light_scale: float = 1.0, hdr: bool = False) -> np.nd
     return LT.parse_intensity(text, hdr=hdr, light_scale=light_scale)[0]
 
 
+def surface_patches(world: World, hdr: bool = False, max_chop: float = 4.0, min_chop: float = 4.0):
+    """The patch set's part that AddSurfaceLights reads, for a map with
+    texlights (None without): the patches at the bounce's chop sizes
+    (vrad_build_patches) and each face's emission, parsed from its
+    texlight value as the lights file's are (ParseIntensity, HDR keys for
+    the HDR range)."""
+    if world.face_emit is None or not (world.face_emit[:, 3] > 0).any():
+        return None
+    faces, verts = faces_of(world)
+    patches, _ = build_patches(faces, verts, face_reflectivity(world), max_chop, min_chop)
+    base = np.zeros((world.face_count, 3), np.float32)
+    for f in np.flatnonzero(world.face_emit[:, 3] > 0):
+        base[f] = parse_intensity(world.face_emit[f], hdr=hdr)
+    F = world.face_count
+    return LT.SurfacePatches(origin=patches["origin"], normal=patches["normal"], area=patches["area"],
+                             face=patches["face"], leaf=patches["child1"] == -1, base_light=base,
+                             base_area=np.full(F, world.texel_area, np.float32),
+                             scale=np.tile(np.array(world.texel_scale, np.float32), (F, 1)))
+
+
 def light_set(world: World, hdr: bool = False) -> LT.DirectLightSet:
-    """The map's light entities through the restated DirectLightBuilder."""
-    return LT.build(rg.entities(world), lambda o: rg.cluster_of_point(world, o), hdr=hdr)
+    """The map's lights through the restated DirectLightBuilder: its
+    texlights' surface lights, then its light entities."""
+    return LT.build(rg.entities(world), lambda o: rg.cluster_of_point(world, o), hdr=hdr,
+                    surface=surface_patches(world, hdr))
 
 
 def build_lights(world: World, hdr: bool = False):

@@ -30,9 +30,10 @@ is built by prepending, as DirectLightSet.AddToActiveList does, so it holds
 the entities in reverse creation order, the environment's ambient ahead of
 its sun.
 
-The _fifty_percent_distance falloff (a fitted quadratic) and texture lights
-(surface lights) are not built: an entity that asks for the first raises
-NotImplementedError, and surface lights are refused by the library.
+Surface lights come from the emitting textures' leaf patches
+(add_surface_lights).  The _fifty_percent_distance falloff (a fitted
+quadratic) is not built: an entity that asks for it raises
+NotImplementedError.
 """
 from __future__ import annotations
 
@@ -357,10 +358,58 @@ def _parse_environment(entities, e, cluster_of, lights, hdr):
     lights.active.insert(0, ambient)
 
 
-def build(entities, cluster_of=lambda origin: 0, hdr: bool = False) -> DirectLightSet:
-    """DirectLightBuilder.Build over entity records (no surface lights).
-    cluster_of(origin) gives the cluster of a point (the tree's leaf)."""
+# LightConstants.DirectScale and DirectLightingSettings.DLightThreshold.
+DIRECT_SCALE = np.float32(100.0 * 100.0)
+DLIGHT_THRESHOLD = np.float32(0.1)
+
+
+@dataclasses.dataclass
+class SurfacePatches:
+    """What AddSurfaceLights reads of the patch set: per patch its origin,
+    shading normal, area, face and whether it has children (patch index
+    order), and per face its texture's emission (BaseLight), texel area
+    (BaseArea) and texels per world unit (ScaleS, ScaleT)."""
+    origin: np.ndarray       # (P, 3) float32
+    normal: np.ndarray       # (P, 3) float32
+    area: np.ndarray         # (P,) float32
+    face: np.ndarray         # (P,) int32
+    leaf: np.ndarray         # (P,) bool
+    base_light: np.ndarray   # (F, 3) float32
+    base_area: np.ndarray    # (F,) float32
+    scale: np.ndarray        # (F, 2) float32
+
+
+def add_surface_lights(lights: DirectLightSet, sp: SurfacePatches, cluster_of, light_scale: float = 1.0,
+                       threshold=DLIGHT_THRESHOLD) -> None:
+    """DirectLightBuilder.AddSurfaceLights (DirectLightBuilder.cs:145-189):
+    every leaf patch of an emitting texture, in patch index order (each
+    prepended, so the list ends in reverse patch order), whose emission
+    averages at least the threshold, becomes a surface light at the
+    patch's origin with its normal and intensity BaseLight * (LightScale *
+    Area * ScaleS * ScaleT / BaseArea) * DirectScale, float by float."""
+    f32 = np.float32
+    for i in range(len(sp.area)):
+        f = int(sp.face[i])
+        if not sp.leaf[i] or float(sp.base_area[f]) < 1e-6:
+            continue
+        bl = sp.base_light[f].astype(f32)
+        average = f32(f32(bl[0] + bl[1]) + bl[2]) / f32(3.0)
+        if average < threshold:
+            continue
+        light = lights.alloc(sp.origin[i], cluster_of(sp.origin[i]), True)
+        light.type = EMIT_SURFACE
+        light.normal = sp.normal[i].astype(f32)
+        scale = f32(f32(f32(f32(light_scale) * sp.area[i]) * sp.scale[f, 0]) * sp.scale[f, 1]) / sp.base_area[f]
+        light.intensity = (bl * f32(scale)).astype(f32) * DIRECT_SCALE
+
+
+def build(entities, cluster_of=lambda origin: 0, hdr: bool = False, surface: SurfacePatches | None = None) -> DirectLightSet:
+    """DirectLightBuilder.Build (DirectLightBuilder.cs:88-140): the surface
+    lights (with surface given), then the light entities.  cluster_of(origin)
+    gives the cluster of a point (the tree's leaf)."""
     lights = DirectLightSet()
+    if surface is not None:
+        add_surface_lights(lights, surface, cluster_of)
     for e in entities:
         name = value_for_key(e, "classname")
         if not name.startswith("light") or name == "light_dynamic":

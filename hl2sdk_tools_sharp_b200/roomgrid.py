@@ -57,6 +57,7 @@ class Config:
     sky_ambient: bool = False
     sun_spread: float = 0.0          # the light_environment's SunSpreadAngle (degrees); 0: one sun ray
     sun_samples: int = 30            # jittered sun rays with a spread (the reference fixes 30)
+    texlights: int = 0               # faces whose texture emits (surface lights)
 
 
 def config_3x3(seed: int = 1) -> Config:
@@ -134,6 +135,13 @@ class World:
     sun_color_hdr: np.ndarray = None     # (4,) float64
     ambient_color_hdr: np.ndarray = None  # (4,) float64
     ambient_scale_hdr: float = 1.0
+    # Texlights (the level's lights file, TextureLightTable): per face the
+    # emitting texture's "r g b brightness" (a zero row: the face does not
+    # emit), and every face's texture: its texel area (texdata width x
+    # height) and texels per world unit along s and t.
+    face_emit: np.ndarray = None         # (F, 4) float64
+    texel_area: float = 256.0 * 256.0
+    texel_scale: tuple = (4.0, 4.0)
 
     @property
     def face_count(self) -> int:
@@ -440,8 +448,24 @@ def generate(cfg: Config) -> World:
         ambient_color=np.array([120.0, 150.0, 210.0, 60.0]) if cfg.sky_ambient else np.zeros(4),
         sky_intensity=np.array([1.0, 1.0, 1.0], np.float32) if cfg.sky_ambient else np.zeros(3, np.float32),
         pvs=pvs,
+        face_emit=_texlights(cfg, np.stack(fext)),
         **_hdr_keys(cfg, L),
     )
+
+
+def _texlights(cfg: Config, extents: np.ndarray) -> np.ndarray:
+    """cfg.texlights panels: faces of at least 8 x 8 luxels (the rooms are
+    open to the sky, so these are walls and pillar sides) drawn from a
+    stream of their own, each with a texlight value "r g b brightness"."""
+    emit = np.zeros((len(extents), 4))
+    if cfg.texlights <= 0:
+        return emit
+    rng = np.random.default_rng([cfg.seed, 0x544C])
+    large = np.flatnonzero((extents[:, 0] >= 7) & (extents[:, 1] >= 7))
+    pick = rng.choice(large, size=min(cfg.texlights, len(large)), replace=False)
+    emit[pick, 0:3] = np.round(rng.uniform(180.0, 255.0, size=(len(pick), 3)))
+    emit[pick, 3] = np.round(rng.uniform(100.0, 400.0, size=len(pick)))
+    return emit
 
 
 def _hdr_keys(cfg: Config, L: int) -> dict:

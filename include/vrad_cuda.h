@@ -414,6 +414,12 @@ int32_t vrad_direct_autotune(vrad_ctx *ctx, int32_t *chosen_block, float *times_
 #define VRAD_SURF_NOLIGHT 0x0400
 #define VRAD_SURF_BUMPLIGHT 0x0800
 #define VRAD_SURF_NOCHOP 0x4000
+/* Not a SurfaceFlags bit: the face's texture emits (PatchBuilder's
+ * BaseLightForFace is nonzero), so its patches are surface lights' and skip
+ * the face-edge refinement (PatchSubdivider.cs:375-380).  The caller makes
+ * the surface lights themselves (DirectLightBuilder.AddSurfaceLights) from
+ * the leaf patches, as type 0 lights. */
+#define VRAD_FACE_EMITS 0x40000000
 
 /* Patch (MapTools/Rad/Light/Patch.cs:44-234), the fields the bounce reads.
  * normal is the shading normal (the plane normal for a root, the phong

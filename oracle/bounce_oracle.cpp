@@ -329,6 +329,13 @@ int CreateChildPatch(World &w, int parentIndex, const Winding &winding, float ar
     Bounds(winding, mins, maxs);
     child.mins = mins;
     child.maxs = maxs;
+    // A surface light's patches skip the face-edge rule ("don't check
+    // edges on surf lights", PatchSubdivider.cs:375-380): a face whose
+    // texture emits carries the library's emitting-face bit.
+    if (w.faces[(size_t)child.face].flags & 0x40000000) {
+        w.patches.push_back(child);
+        return (int)w.patches.size() - 1;
+    }
     V total = (maxs - mins) * child.lux_scale;
     if (child.chop > w.min_chop && total.x < child.chop && total.y < child.chop && total.z < child.chop) {
         for (int i = 0; i < 3; i++) {

@@ -329,6 +329,33 @@ void gather(const Ctx &c, const orc_light &L, const F3 pts[4], const F3 nrm[4], 
             if (l < count && o.dot[l] != 0.0f && o.falloff[l] != 0.0f)
                 o.dot[l] = (visible(c, pts[l], src, false) ? 1.0f : 0.0f) * o.dot[l];
         }
+    } else if (L.type == 0) {
+        // GatherSurfaceFour (DirectLightGatherer.cs:1452-1545): the
+        // emitter's cosine over the squared distance; the segment ends
+        // DistEpsilon off the emitting patch.
+        const F3 end = src + ln * 0.03125f;
+        for (int l = 0; l < kLanes; l++) {
+            float dx = src.x - pts[l].x, dy = src.y - pts[l].y, dz = src.z - pts[l].z;
+            float d2 = ((dx * dx) + (dy * dy)) + (dz * dz);
+            float dist = std::sqrt(d2);
+            float r = 1.0f / dist;
+            dx *= r;
+            dy *= r;
+            dz *= r;
+            float dot = ((dx * nrm[l].x) + (dy * nrm[l].y)) + (dz * nrm[l].z);
+            dot = MaxPs(0.0f, dot);
+            bool live = !hard || dist <= L.end_fade;
+            dist = MaxPs(dist, 1.0f);
+            float dot2 = -(((dx * ln.x) + (dy * ln.y)) + (dz * ln.z));
+            dot2 = MaxPs(0.0f, dot2);
+            live = live && !(dot == 0.0f);
+            float fall = dot2 / d2;
+            if (hard) fall = quintic(dist, L) * fall;
+            o.dot[l] = live ? dot : 0.0f;
+            o.falloff[l] = live ? fall : 0.0f;
+            if (l < count && o.dot[l] != 0.0f && o.falloff[l] != 0.0f)
+                o.dot[l] = (visible(c, pts[l], end, false) ? 1.0f : 0.0f) * o.dot[l];
+        }
     } else if (L.type == 2) {
         // GatherStandardLane (Spotlight) for the real lanes; the resolve
         // copies the last real lane into the padding.

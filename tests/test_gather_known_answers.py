@@ -78,6 +78,18 @@ CASES = {
     "sun_hitting_geometry_shadowed": (_light(3, (0, 0, 0), normal=(0, 0, -1)), 50.0, 1, lambda v: v == 0.0, 0, 1),
     "soft_sun_thirty_rays": (_light(3, (0, 0, 0), normal=(0, 0, -1)), None, 30, lambda v: v == 1.0, 0, 30),
     "open_sky_ambient_unit_dot": (_light(4, (0, 0, 0)), None, 1, lambda v: abs(v - 1.0) < 5e-7, 0, None),
+    # GatherTests.ASurfaceLightFallsOffAsItsNormalDotOverDistanceSquared
+    # (GatherTests.cs:197-210): the emitter's cosine over the squared
+    # distance; its ray ends DistEpsilon (1/32) short of the emitter: a
+    # blocker below that end shadows, one between it and the emitter does not.
+    "surface_dot_over_distance_squared": (_light(0, (0, 0, 10), normal=(0, 0, -1)), None, 1,
+                                          lambda v: v == np.float32(0.01), 1, 0),
+    "surface_blocked_below_the_ray_end": (_light(0, (0, 0, 10), normal=(0, 0, -1)), 9.9, 1,
+                                          lambda v: v == 0.0, 1, 0),
+    "surface_not_blocked_past_the_ray_end": (_light(0, (0, 0, 10), normal=(0, 0, -1)), 9.99, 1,
+                                             lambda v: v == np.float32(0.01), 1, 0),
+    "surface_facing_away_lights_nothing": (_light(0, (0, 0, 10), normal=(0, 0, 1)), None, 1,
+                                           lambda v: v == 0.0, 0, 0),
     "closed_sky_ambient_nothing": (_light(4, (0, 0, 0)), 10.0, 1, lambda v: v == 0.0, 0, None),
 }
 
