@@ -31,9 +31,8 @@ the entities in reverse creation order, the environment's ambient ahead of
 its sun.
 
 Surface lights come from the emitting textures' leaf patches
-(add_surface_lights).  The _fifty_percent_distance falloff (a fitted
-quadratic) is not built: an entity that asks for it raises
-NotImplementedError.
+(add_surface_lights); the _fifty_percent_distance falloff is the fitted
+quadratic of LightFalloff.ApplySolvedCurve (solve_inverse_quadratic*).
 """
 from __future__ import annotations
 
@@ -267,12 +266,93 @@ def _parse_generic(entities, e, light: DirectLight, lights: DirectLightSet, hdr:
         light.intensity = (light.intensity * float_for_key_with_default(e, "_lightscaleHDR", 1.0)).astype(np.float32)
 
 
-def _falloff(e, light: DirectLight) -> None:
-    if float_for_key(e, "_fifty_percent_distance") != 0:
-        raise NotImplementedError("_fifty_percent_distance falloff is not built")
+def solve_inverse_quadratic(x1, y1, x2, y2, x3, y3):
+    """MathSolvers.SolveInverseQuadratic (MathSolvers.cs): the quadratic
+    a x^2 + b x + c through three points, float by float in the reference's
+    order; None when two x coincide."""
+    f = np.float32
+    x1, y1, x2, y2, x3, y3 = (f(v) for v in (x1, y1, x2, y2, x3, y3))
+    det = f(f(x1 - x2) * f(x1 - x3)) * f(x2 - x3)
+    if det == f(0):
+        return None
+    na = f(f(x3 * f(-y1 + y2)) + f(x2 * f(y1 - y3))) + f(x1 * f(-y2 + y3))
+    nb = f(f(f(x3 * x3) * f(y1 - y2)) + f(f(x1 * x1) * f(y2 - y3))) + f(f(x2 * x2) * f(-y1 + y3))
+    nc = f(f(f(f(x1 * x3) * f(-x1 + x3)) * y2) + f(f(x2 * x2) * f(f(x3 * y1) - f(x1 * y3)))) + \
+        f(x2 * f(-f(f(x3 * x3) * y1) + f(f(x1 * x1) * y3)))
+    return f(na / det), f(nb / det), f(nc / det)
+
+
+def solve_inverse_quadratic_monotonic(x1, y1, x2, y2, x3, y3, a, b, c):
+    """MathSolvers.SolveInverseQuadraticMonotonic: the points sorted by x,
+    then the middle point blended toward the straight line in float steps
+    of (double) 0.05 until the slope at the first point agrees with the
+    data's direction.  (ok, a, b, c); a failed solve keeps a, b, c."""
+    f = np.float32
+    x1, y1, x2, y2, x3, y3 = (f(v) for v in (x1, y1, x2, y2, x3, y3))
+    if x1 > x2:
+        x1, x2, y1, y2 = x2, x1, y2, y1
+    if x2 > x3:
+        x2, x3, y2, y3 = x3, x2, y3, y2
+    if x1 > x2:
+        x1, x2, y1, y2 = x2, x1, y2, y1
+    blend = f(0)
+    while blend <= f(1):
+        linear = f(y1 + f(f(f(y3 - y1) * f(x2 - x1)) / f(x3 - x1)))       # FLerp
+        temp_y2 = f(f(f(1) - blend) * y2) + f(blend * linear)
+        sol = solve_inverse_quadratic(x1, y1, x2, temp_y2, x3, y3)
+        if sol is None:
+            return False, a, b, c
+        a, b, c = sol
+        derivative = f((2.0 * float(a) * float(x1)) + float(b))
+        if y1 < y2 < y3:
+            if derivative >= f(0):
+                return True, a, b, c
+        elif y1 > y2 > y3:
+            if derivative <= f(0):
+                return True, a, b, c
+        else:
+            return True, a, b, c
+        blend = f(float(blend) + 0.05)
+    return True, a, b, c
+
+
+def _solved_falloff(e, light: DirectLight, d50, warnings) -> None:
+    """LightFalloff.ApplySolvedCurve (LightFalloff.cs:116-200): a falloff
+    whose reciprocal brightness is 1 at the light, 2 at
+    _fifty_percent_distance and 256 at _zero_percent_distance; the
+    constants are double literals, so their expressions narrow from double."""
+    f = np.float32
+    d0 = float_for_key(e, "_zero_percent_distance")
+    if d0 < d50:
+        warnings.append(f"light has _fifty_percent_distance of {d50} but _zero_percent_distance of {d0}")
+        d0 = f(2.0 * float(d50))
+    ok, a, b, c = solve_inverse_quadratic_monotonic(f(0), f(1), d50, f(2), d0, f(256), f(0), f(1), f(0))
+    if not ok:
+        warnings.append(f"can't solve quadratic for light {d50} {d0}")
+    v50 = f(c + f(d50 * f(b + f(d50 * a))))
+    scale = f(2.0 / float(v50))
+    a, b, c = f(a * scale), f(b * scale), f(c * scale)
+    light.quadratic_attn, light.linear_attn, light.constant_attn = a, b, c
+    if int_for_key(e, "_hardfalloff") != 0:
+        light.end_fade_distance = f(d0)
+        light.start_fade_distance = f((0.75 * float(d0)) + (0.25 * float(d50)))
+        return
+    if abs(float(a)) > 0.0:
+        top = f(float(b) / (-2.0 * float(a)))
+        if top > f(0):
+            light.cap_dist = top
+            light.start_fade_distance = top
+            light.end_fade_distance = f(10.0 * float(top))
+
+
+def _falloff(e, light: DirectLight, warnings=None) -> None:
     light.start_fade_distance = np.float32(0)
     light.end_fade_distance = np.float32(-1)
     light.cap_dist = np.float32(1.0e22)
+    d50 = float_for_key(e, "_fifty_percent_distance")
+    if d50 != 0:
+        _solved_falloff(e, light, d50, warnings if warnings is not None else [])
+        return
     c, l, q = (float_for_key(e, k) for k in ("_constant_attn", "_linear_attn", "_quadratic_attn"))
     c = np.float32(0) if c < EQUAL_EPSILON else c
     l = np.float32(0) if l < EQUAL_EPSILON else l
@@ -291,7 +371,7 @@ def _parse_point(entities, e, cluster_of, lights, hdr):
     light = lights.alloc(o, cluster_of(o), True)
     _parse_generic(entities, e, light, lights, hdr)
     light.type = EMIT_POINT
-    _falloff(e, light)
+    _falloff(e, light, lights.warnings)
 
 
 def _parse_spot(entities, e, cluster_of, lights, hdr):
@@ -324,7 +404,7 @@ def _parse_spot(entities, e, cluster_of, lights, hdr):
         light.stop_dot2 = DM.cos_to_single(radians(outer))
         light.stop_dot = DM.cos_to_single(radians(inner))
         light.exponent = float_for_key(e, "_exponent")
-    _falloff(e, light)
+    _falloff(e, light, lights.warnings)
 
 
 def _parse_environment(entities, e, cluster_of, lights, hdr):
