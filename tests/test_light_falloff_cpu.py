@@ -1,11 +1,14 @@
-"""The solved light falloff (_fifty_percent_distance) and its solver: the
-reference's LightFalloffTests and MathSolverTests
-(src/SourceSharp.Tests/MapTools/Rad/Light/LightMathTests.cs:148-244, 90-146)
-restated on the host layer (lights._falloff, lights.solve_inverse_quadratic*),
-in the reference's Correct mode (divides, the slope at the first point)."""
+"""The solved light falloff (_fifty_percent_distance), its solver and a
+light's direction: the reference's LightFalloffTests, MathSolverTests and
+LightNormalTests (src/SourceSharp.Tests/MapTools/Rad/Light/
+LightMathTests.cs:90-289) restated on the host layer (lights._falloff,
+lights.solve_inverse_quadratic*, lights.from_props), in the reference's
+Correct mode (divides, the slope at the first point, the double cosine)."""
+import math
+
 import numpy as np
 
-from hl2sdk_tools_sharp_b200 import lights as LT
+from hl2sdk_tools_sharp_b200 import detmath as DM, lights as LT
 
 f32 = np.float32
 
@@ -79,3 +82,22 @@ def test_a_solved_light_goes_through_the_builder():
     (light,) = ls.active
     assert light.linear_attn == f32(0.00250157318) and light.quadratic_attn == f32(0.000185510071)
     assert not ls.warnings
+
+
+# LightNormalTests (LightMathTests.cs:246-289): a light's direction from its
+# angle keys (LightNormals.FromProps, Correct mode).
+
+def test_zero_angle_falls_back_to_the_angles_yaw():
+    assert LT.from_props((0, 180, 0), 0, 0)[0] == f32(-1)
+
+
+def test_zero_pitch_falls_back_to_the_angles_pitch():
+    assert LT.from_props((-90, 0, 0), 0, 0)[2] == f32(-1)
+
+
+def test_angle_up_is_overwritten_by_the_pitch():
+    assert np.array_equal(LT.from_props((0, 0, 0), -1, 0), [0, 0, 0])
+
+
+def test_the_correct_cosine_of_a_right_angle_is_the_doubles_distance_from_pi():
+    assert f32(DM.cos_d(math.pi / 2)) == f32(6.123234e-17)
