@@ -78,13 +78,13 @@ def test_autotune_keeps_the_bytes(maps_and_singles):
 
 def test_a_failing_map_leaves_the_others(maps_and_singles):
     maps, singles = maps_and_singles
-    bad_inputs = dataclasses.replace(maps[1].inputs, lights=maps[1].inputs.lights.copy())
-    bad_inputs.lights["type"][0] = 0                  # a surface light: unsupported
-    bad = dataclasses.replace(maps[1], inputs=bad_inputs)
+    bad_inputs = dataclasses.replace(maps[0].inputs, faces=maps[0].inputs.faces.copy())
+    bad_inputs.faces["flags"][0] |= 0x0800            # a bump-mapped face: unsupported by the bounce
+    bad = dataclasses.replace(maps[0], inputs=bad_inputs)
     with B.LightingBatch(workers=2) as batch:
-        results, st = batch.run([maps[0], bad, maps[2]], raise_on_error=False)
-        assert st.failed == 1 and results[1].status == -6 and "surface" in results[1].error.lower()
-        _same([results[0], results[2]], [singles[0], singles[2]])
+        results, st = batch.run([maps[1], bad, maps[2]], raise_on_error=False)
+        assert st.failed == 1 and results[1].status == -6 and "bump" in results[1].error.lower()
+        _same([results[0], results[2]], [singles[1], singles[2]])
         with pytest.raises(NotImplementedError):
             batch.run([bad])
         _same(batch.run(maps)[0], singles)
