@@ -339,19 +339,20 @@ def surface_patches(world: World, hdr: bool = False, max_chop: float = 4.0, min_
                              scale=np.tile(np.array(world.texel_scale, np.float32), (F, 1)))
 
 
-def light_set(world: World, hdr: bool = False) -> LT.DirectLightSet:
+def light_set(world: World, hdr: bool = False, max_chop: float = 4.0, min_chop: float = 4.0) -> LT.DirectLightSet:
     """The map's lights through the restated DirectLightBuilder: its
-    texlights' surface lights, then its light entities."""
+    texlights' surface lights (from the patches at the bounce's chop sizes),
+    then its light entities."""
     return LT.build(rg.entities(world), lambda o: rg.cluster_of_point(world, o), hdr=hdr,
-                    surface=surface_patches(world, hdr))
+                    surface=surface_patches(world, hdr, max_chop, min_chop))
 
 
-def build_lights(world: World, hdr: bool = False):
+def build_lights(world: World, hdr: bool = False, max_chop: float = 4.0, min_chop: float = 4.0):
     """The active DirectLight list and the per-cluster light lists, for the
     LDR pass or (hdr) the HDR pass: the map's light entities
     (roomgrid.entities) through the restated DirectLightBuilder
     (lights.build).  Returns (lights, cluster_offsets, cluster_lights)."""
-    ls = light_set(world, hdr)
+    ls = light_set(world, hdr, max_chop, min_chop)
     if ls.unsupported_class_names:
         raise ValueError(f"unsupported light entities: {ls.unsupported_class_names}")
     lights = LT.to_records(ls.active, LIGHT_DTYPE)
@@ -388,15 +389,18 @@ class LightingInputs:
 RANGE_LDR, RANGE_HDR = 1, 2      # VRAD_RANGE_*
 
 
-def prepare(world: World, hdr: bool = False, sample_out: np.ndarray | None = None) -> LightingInputs:
+def prepare(world: World, hdr: bool = False, sample_out: np.ndarray | None = None, max_chop: float = 4.0,
+            min_chop: float = 4.0) -> LightingInputs:
     """The lighting stage's inputs; with hdr, also the HDR range's light
-    list.  sample_out: a caller's buffer for the samples (build_samples)."""
+    list.  sample_out: a caller's buffer for the samples (build_samples).
+    A map with texlights takes its surface lights from the patch tree at
+    max_chop / min_chop: the chop sizes its bounce is uploaded with."""
     faces, verts = faces_of(world)
     samples, first = build_samples(faces, verts, out=sample_out)
-    lights, off, flat = build_lights(world)
+    lights, off, flat = build_lights(world, max_chop=max_chop, min_chop=min_chop)
     inp = LightingInputs(faces, verts, samples, first, lights, off, flat,
                          ambient_directions().astype(np.float32), np.zeros((0, 3), np.float32))
-    extent = light_set(world).sun_angular_extent
+    extent = LT.build(rg.entities(world)).sun_angular_extent   # the light_environment's alone
     if extent > 0:
         # A sun with a spread: the configured count of jittered rays, ray d
         # jittered by the sampler's direction d - 1 (DirectLightGatherer's
@@ -405,7 +409,7 @@ def prepare(world: World, hdr: bool = False, sample_out: np.ndarray | None = Non
         inp.sun_samples = int(world.config.sun_samples)
         inp.sun_jitter = ambient_directions(max(1, inp.sun_samples - 1)).astype(np.float32)
     if hdr:
-        inp.lights_hdr, off_h, flat_h = build_lights(world, hdr=True)
+        inp.lights_hdr, off_h, flat_h = build_lights(world, hdr=True, max_chop=max_chop, min_chop=min_chop)
         assert np.array_equal(off, off_h) and np.array_equal(flat, flat_h)
     return inp
 
