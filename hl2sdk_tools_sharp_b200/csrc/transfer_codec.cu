@@ -494,7 +494,9 @@ extern "C" int32_t vrad_transfer_unpack(const uint8_t *packed, int64_t len, uint
         return vrad_fail(nullptr, VRAD_ERR_FORMAT, "a packed chunk's count out of range");
     if (capacity < kTransferBytes * n || (!out && n))
         return vrad_fail(nullptr, VRAD_ERR_ARG, "the chunk takes %lld bytes", (long long)(kTransferBytes * n));
-    std::vector<uint8_t> planes((size_t)(kTransferBytes * n));
+    // Uninitialised: junk that claims a large count fails in the inflate
+    // without touching the pages.
+    uvector<uint8_t> planes((size_t)(kTransferBytes * n));
     if (!inflate_exact(packed + 4, len - 4, planes.data(), kTransferBytes * n))
         return vrad_fail(nullptr, VRAD_ERR_FORMAT, "the stream does not inflate to exactly its count");
     unshuffle_host(planes.data(), n, out);
