@@ -77,3 +77,13 @@ def test_styled_bounce_both_ranges_equal_the_oracle(oracle_mod):
         bad = np.flatnonzero(got.view(np.uint32) != lump.view(np.uint32))
         assert len(bad) == 0, f"{r}: {len(bad)} of {len(lump) // 4} words differ"
     assert bst[0].bounces > 1
+
+
+def test_a_map_without_styled_lights_keeps_style_zero_alone():
+    w = rg.generate(rg.config_3x3(seed=2))
+    inp = L.prepare(w)
+    with L.LightingStage(w, inp) as st:
+        styles, dropped = st.face_styles()
+        size = st.lighting_size()
+    assert (styles == [0, 255, 255, 255]).all() and dropped == 0
+    assert size == L.lightmap_layout(inp.faces)[1]
