@@ -317,8 +317,9 @@ int32_t vrad_lightmap_layout_styles(const vrad_face *faces, int32_t nfaces, cons
 
 /* Uploads the lighting world to the context's device (kept until the next
  * upload or vrad_destroy).  The scene (vrad_scene_upload) is the shadow
- * casters.  VRAD_ERR_UNSUPPORTED for a surface light (type 0) or for a
- * group of four samples that spans two clusters.  With the scene and the
+ * casters.  Lights of every type (0 surface, 1 point, 2 spot, 3 sun, 4 sky
+ * ambient) and style (0 to 254) are lit; VRAD_ERR_UNSUPPORTED for a group
+ * of four samples that spans two clusters.  With the scene and the
  * face windings present, the upload also queues the next light pass's
  * direct gather (with its supersampling passes) on the device from a host
  * thread, so that it runs while the caller's bounce upload builds its
